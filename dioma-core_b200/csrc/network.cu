@@ -1,0 +1,1345 @@
+// network.cu — host side of the SiMuse Network on one B200: builder, device
+// layout, step launches, readbacks, and the extern "C" ABI of
+// include/simuse_b200.h.
+//
+// Device layout (HBM).  Populations are placed at 32-aligned offsets of a
+// padded device index space (Nd neurons) so that every warp of a neuron
+// kernel covers one whole spike-bitmask word; padding neurons never spike and
+// own no synapses.  State and params stay SoA, [col][cap] per population
+// (P/core/exec/population.rs:16-25).  The delay ring is [n_rings][32][Nd]
+// floats (P/api/net/delay.rs:26-35), ring 0 static, ring k the k-th kinetic
+// profile.  The CSR keeps the reference's u32 row_ptr/col (graph.rs:67-80),
+// f32 weights, and one code byte per edge (delay | syn_type | STDP flag).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "models.cuh"
+#include "step_kernels.cuh"
+
+namespace sg {
+
+thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+template <typename T> struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    if (count == 0) return;
+    SG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void zero(cudaStream_t s) {
+    if (p) SG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+};
+
+// growable device array for staged edges
+template <typename T> struct DVec {
+  T *p = nullptr;
+  size_t n = 0, cap = 0;
+  ~DVec() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = cap = 0;
+  }
+  void reserve(size_t c, cudaStream_t s) {
+    if (c <= cap) return;
+    size_t nc = std::max(c, cap + cap / 2);
+    T *q = nullptr;
+    SG_CUDA(cudaMalloc(&q, nc * sizeof(T)));
+    if (n) SG_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    if (p) cudaFree(p);
+    p = q;
+    cap = nc;
+  }
+};
+
+struct HostPop {
+  int model;
+  uint32_t n, cap, dev_off, np, ns;
+  std::vector<float> params, state;  // before build
+  DBuf<float> d_params, d_state;     // after build
+};
+
+struct HostSrc {
+  float p;
+  uint32_t seed;
+  std::vector<uint32_t> post;  // device indices
+  std::vector<float> w;
+  std::vector<uint8_t> code;
+};
+
+struct Kin {
+  float a_decay, erev;
+};
+
+}  // namespace sg
+
+using namespace sg;
+
+struct sg_net {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool built = false;
+  std::vector<HostPop> pops;
+  std::vector<uint32_t> offsets{0};  // reference global offsets
+  uint64_t total = 0;                // reference neuron count
+  uint32_t Nd = 0;                   // padded device neuron count
+  // staged edges (device)
+  DVec<uint32_t> e_pre, e_post;
+  DVec<float> e_w;
+  DVec<uint8_t> e_code;
+  std::vector<Kin> kin;
+  std::vector<HostSrc> srcs;
+  bool stdp_on = false;
+  float stdp_dt = 0, tau_pre = 0, tau_post = 0, a_plus = 0, a_minus = 0, w_min = 0, w_max = 0;
+  int deterministic = 1;
+  int weight_format = SG_W_F32;
+
+  // device state
+  DBuf<unsigned long long> d_step, d_ev_step, d_ev_total, d_clamp, d_stat_ev;
+  DBuf<uint32_t> d_n_active, d_active, d_last_bits, d_raster, d_done, d_stat_spk;
+  DBuf<float> d_ring, d_kin_g;
+  DBuf<uint32_t> d_row_ptr, d_col;
+  DBuf<float> d_w;
+  DBuf<uint8_t> d_code;
+  uint64_t n_edges = 0;
+  DBuf<float> d_src_p, d_src_w;
+  DBuf<uint32_t> d_src_seed, d_src_ptr, d_src_post;
+  DBuf<uint8_t> d_src_code;
+  uint64_t n_src_edges = 0;
+  DBuf<unsigned long long> d_bin_base;
+  DBuf<uint32_t> d_bin_cnt, d_bkey, d_bcell;
+  DBuf<float> d_bw;
+  uint32_t tshift = 11, n_tiles = 0, hbits = 13;
+  DBuf<float> d_x_pre, d_x_post;
+  DBuf<uint32_t> d_in_ptr, d_in_edge, d_in_pre;
+  DBuf<double> d_drift;
+  DBuf<uint32_t> d_inj_idx;
+  DBuf<float> d_inj_val;
+  uint32_t raster_cap = 0;
+  uint64_t raster_read_step = 0;
+  uint32_t stat_cap = 1u << 16;
+  uint64_t stat_read_step = 0;
+  uint64_t host_step = 0;  // steps issued
+  int apply_blocks = 0, expand_blocks = 0, src_blocks = 0;
+  size_t apply_smem = 0;
+  // CUDA graph of `graph_steps` steps
+  cudaGraphExec_t graph = nullptr;
+  uint32_t graph_steps = 0;
+  std::vector<float> ln_consts{0, 0};
+
+  uint32_t dev_index(uint32_t pop, uint32_t i) const { return pops[pop].dev_off + i; }
+};
+
+namespace {
+
+int run(const std::function<void()> &f) {
+  try {
+    f();
+    return SG_OK;
+  } catch (const Fail &e) {
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_error("host allocation failed");
+    return SG_E_NOMEM;
+  } catch (const std::exception &e) {
+    set_error(e.what());
+    return SG_E_INVALID;
+  }
+}
+
+#define NET_CHECK(net)                                                     \
+  do {                                                                     \
+    if (!(net)) {                                                          \
+      set_error("null network handle");                                    \
+      return SG_E_INVALID;                                                 \
+    }                                                                      \
+  } while (0)
+
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DevGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+void require_pop(const sg_net *net, uint32_t pop) {
+  SG_REQUIRE(pop < net->pops.size(), SG_E_INVALID,
+             "population " + std::to_string(pop) + " out of range (have " +
+                 std::to_string(net->pops.size()) + ")");
+}
+
+StepArgs make_args(sg_net *net) {
+  StepArgs a{};
+  a.step = net->d_step.p;
+  a.n_active = net->d_n_active.p;
+  a.active = net->d_active.p;
+  a.last_bits = net->d_last_bits.p;
+  a.raster = net->raster_cap ? net->d_raster.p : nullptr;
+  a.raster_cap = net->raster_cap ? net->raster_cap : 1;
+  a.words = net->Nd / 32;
+  a.done = net->d_done.p;
+  a.ev_step = net->d_ev_step.p;
+  a.ev_total = net->d_ev_total.p;
+  a.stat_spk = net->d_stat_spk.p;
+  a.stat_ev = net->d_stat_ev.p;
+  a.stat_cap = net->stat_cap;
+  a.clamp_hits = net->d_clamp.p;
+  a.ring = net->d_ring.p;
+  a.Nd = net->Nd;
+  a.n_kin = (int)net->kin.size();
+  for (size_t k = 0; k < net->kin.size() && k < 3; ++k) {
+    a.kin_a[k] = net->kin[k].a_decay;
+    a.kin_erev[k] = net->kin[k].erev;
+  }
+  a.kin_g = net->d_kin_g.p;
+  a.row_ptr = net->d_row_ptr.p;
+  a.col = net->d_col.p;
+  a.w = net->d_w.p;
+  a.code = net->d_code.p;
+  a.n_edges = (uint32_t)net->n_edges;
+  a.n_src = (uint32_t)net->srcs.size();
+  a.src_p = net->d_src_p.p;
+  a.src_seed = net->d_src_seed.p;
+  a.src_ptr = net->d_src_ptr.p;
+  a.src_post = net->d_src_post.p;
+  a.src_w = net->d_src_w.p;
+  a.src_code = net->d_src_code.p;
+  a.tshift = net->tshift;
+  a.n_tiles = net->n_tiles;
+  a.hbits = net->hbits;
+  a.bin_base = net->d_bin_base.p;
+  a.bin_cnt = net->d_bin_cnt.p;
+  a.bkey = net->d_bkey.p;
+  a.bw = net->d_bw.p;
+  a.bcell = net->d_bcell.p;
+  a.deterministic = net->deterministic;
+  a.stdp = net->stdp_on ? 1 : 0;
+  a.x_pre = net->d_x_pre.p;
+  a.x_post = net->d_x_post.p;
+  if (net->stdp_on) {
+    a.d_pre = net->ln_consts.size() > 2 ? net->ln_consts[2] : 0.f;
+    a.d_post = net->ln_consts.size() > 3 ? net->ln_consts[3] : 0.f;
+  }
+  a.a_plus = net->a_plus;
+  a.a_minus = net->a_minus;
+  a.w_min = net->w_min;
+  a.w_max = net->w_max;
+  a.in_ptr = net->d_in_ptr.p;
+  a.in_edge = net->d_in_edge.p;
+  a.in_pre = net->d_in_pre.p;
+  a.drift = net->d_drift.p;
+  return a;
+}
+
+// Host restatement of P/math/fast_exp.rs:23-68 (fused flavour), used for the
+// per-step STDP trace decay constants (brain.rs:208-209).
+float host_fast_exp(float x) {
+  const float log2e = 1.44269504088896340736f;
+  float t = x * log2e;
+  float tf = std::floor(t);
+  int n = std::isnan(tf) ? 0 : (tf >= 2147483647.0f ? 2147483647 : (tf <= -2147483648.0f ? INT32_MIN : (int)tf));
+  float f = t - (float)n;
+  float poly = std::fma(0.0001540353f, f, 0.001333356f);
+  poly = std::fma(poly, f, 0.009618129f);
+  poly = std::fma(poly, f, 0.05550411f);
+  poly = std::fma(poly, f, 0.2402265f);
+  poly = std::fma(poly, f, 0.693147180559945309417f);
+  poly = std::fma(poly, f, 1.0f);
+  if (n < -126) return 0.0f;
+  if (n > 127) return INFINITY;
+  uint32_t bits = (uint32_t)(n + 127) << 23;
+  float s;
+  std::memcpy(&s, &bits, 4);
+  return s * poly;
+}
+
+// ---------------------------------------------------------------------------
+// build kernels
+// ---------------------------------------------------------------------------
+__global__ void iota_kernel(uint32_t *v, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+__global__ void gather_edges_kernel(const uint32_t *perm, const uint32_t *post_in, const float *w_in,
+                                    const uint8_t *code_in, uint32_t *col, float *w, uint8_t *code,
+                                    uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = perm[i];
+    col[i] = post_in[j];
+    w[i] = w_in[j];
+    code[i] = code_in[j];
+  }
+}
+__global__ void histogram_kernel(const uint32_t *keys, uint64_t n, uint32_t shift, unsigned long long *cnt) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(cnt + (keys[i] >> shift), 1ull);
+}
+__global__ void to_u32_kernel(const unsigned long long *in, uint32_t *out, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)in[i];
+}
+// Plastic in-edges grouped by post.
+__global__ void csc_count_kernel(const uint32_t *row_ptr, const uint32_t *col, const uint8_t *code,
+                                 uint32_t Nd, unsigned long long *cnt) {
+  for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x)
+    for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e)
+      if (code_stdp(code[e])) atomicAdd(cnt + col[e], 1ull);
+}
+__global__ void csc_fill_kernel(const uint32_t *row_ptr, const uint32_t *col, const uint8_t *code,
+                                uint32_t Nd, uint32_t *cursor, uint32_t *in_edge, uint32_t *in_pre) {
+  for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x)
+    for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e)
+      if (code_stdp(code[e])) {
+        const uint32_t k = atomicAdd(cursor + col[e], 1u);
+        in_edge[k] = e;
+        in_pre[k] = pre;
+      }
+}
+__global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, uint8_t *code,
+                                      uint64_t base, uint32_t n_post, uint32_t k_in, uint64_t seed,
+                                      uint32_t from_off, uint32_t n_from, uint32_t to_off,
+                                      uint32_t n_exc, float w_exc, float w_inh, uint32_t d_min,
+                                      uint32_t d_span, uint8_t st_e, uint8_t st_i, uint32_t flags_e) {
+  const uint64_t total = (uint64_t)n_post * k_in;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t h = splitmix64(seed ^ (t * 0x9E3779B97F4A7C15ull));
+    const uint32_t j = (uint32_t)(t / k_in);
+    const uint32_t src = (uint32_t)(((h >> 32) * (uint64_t)n_from) >> 32);
+    const uint32_t d = d_min + (uint32_t)((h & 0xffffffffull) % d_span);
+    const bool exc = src < n_exc;
+    pre[base + t] = from_off + src;
+    post[base + t] = to_off + j;
+    w[base + t] = exc ? w_exc : w_inh;
+    code[base + t] = edge_code((uint8_t)d, exc ? st_e : st_i, exc && (flags_e & SG_EDGE_STDP));
+  }
+}
+
+template <typename F> void launch_grid(uint64_t n, F f) {
+  uint64_t blocks = (n + 255) / 256;
+  if (blocks > 148ull * 32) blocks = 148ull * 32;
+  if (blocks == 0) blocks = 1;
+  f((unsigned)blocks);
+}
+
+void upload_staged_edges(sg_net *net, const uint32_t *pre, const uint32_t *post, const float *w,
+                         const uint8_t *code, uint64_t n) {
+  const size_t n0 = net->e_pre.n;
+  net->e_pre.reserve(n0 + n, net->stream);
+  net->e_post.reserve(n0 + n, net->stream);
+  net->e_w.reserve(n0 + n, net->stream);
+  net->e_code.reserve(n0 + n, net->stream);
+  SG_CUDA(cudaMemcpyAsync(net->e_pre.p + n0, pre, n * 4, cudaMemcpyHostToDevice, net->stream));
+  SG_CUDA(cudaMemcpyAsync(net->e_post.p + n0, post, n * 4, cudaMemcpyHostToDevice, net->stream));
+  SG_CUDA(cudaMemcpyAsync(net->e_w.p + n0, w, n * 4, cudaMemcpyHostToDevice, net->stream));
+  SG_CUDA(cudaMemcpyAsync(net->e_code.p + n0, code, n, cudaMemcpyHostToDevice, net->stream));
+  SG_CUDA(cudaStreamSynchronize(net->stream));
+  net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
+}
+
+// Stable sort of the staged edges by pre (graph.rs:142-147; the reference
+// sort is unstable, this one keeps insertion order inside a row), then the
+// u32 row_ptr (graph.rs:149-180).
+void build_graph(sg_net *net) {
+  cudaStream_t s = net->stream;
+  const uint64_t E = net->e_pre.n;
+  net->n_edges = E;
+  const uint32_t Nd = net->Nd;
+  net->d_row_ptr.alloc((size_t)Nd + 1);
+  net->d_col.alloc(std::max<uint64_t>(E, 1));
+  net->d_w.alloc(std::max<uint64_t>(E, 1));
+  net->d_code.alloc(std::max<uint64_t>(E, 1));
+  DBuf<unsigned long long> cnt;
+  cnt.alloc((size_t)Nd + 1);
+  cnt.zero(s);
+  if (E > 0) {
+    DBuf<uint32_t> keys_out, vals_in, vals_out;
+    keys_out.alloc(E);
+    vals_in.alloc(E);
+    vals_out.alloc(E);
+    launch_grid(E, [&](unsigned b) { iota_kernel<<<b, 256, 0, s>>>(vals_in.p, E); });
+    int end_bit = 1;
+    while (end_bit < 32 && (1ull << end_bit) < (uint64_t)Nd) ++end_bit;
+    size_t temp_bytes = 0;
+    SG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, net->e_pre.p, keys_out.p, vals_in.p,
+                                            vals_out.p, (int64_t)E, 0, end_bit, s));
+    DBuf<uint8_t> temp;
+    temp.alloc(std::max<size_t>(temp_bytes, 1));
+    SG_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, temp_bytes, net->e_pre.p, keys_out.p, vals_in.p,
+                                            vals_out.p, (int64_t)E, 0, end_bit, s));
+    temp.release();
+    vals_in.release();
+    launch_grid(E, [&](unsigned b) {
+      gather_edges_kernel<<<b, 256, 0, s>>>(vals_out.p, net->e_post.p, net->e_w.p, net->e_code.p,
+                                            net->d_col.p, net->d_w.p, net->d_code.p, E);
+    });
+    launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(keys_out.p, E, 0, cnt.p); });
+    SG_CUDA(cudaStreamSynchronize(s));
+  }
+  net->e_pre.release();
+  net->e_post.release();
+  net->e_w.release();
+  net->e_code.release();
+  // exclusive scan in u64 -> u32 row_ptr
+  DBuf<unsigned long long> rp64;
+  rp64.alloc((size_t)Nd + 1);
+  size_t tb = 0;
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, rp64.p, (int64_t)Nd + 1, s));
+  DBuf<uint8_t> temp;
+  temp.alloc(std::max<size_t>(tb, 1));
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, rp64.p, (int64_t)Nd + 1, s));
+  launch_grid((uint64_t)Nd + 1, [&](unsigned b) { to_u32_kernel<<<b, 256, 0, s>>>(rp64.p, net->d_row_ptr.p, (uint64_t)Nd + 1); });
+  SG_CUDA(cudaStreamSynchronize(s));
+}
+
+// Bins: tile t holds at most (in-degree of its posts, neuron + source
+// synapses) events per step, since every synapse fires at most once per step.
+void build_bins(sg_net *net) {
+  cudaStream_t s = net->stream;
+  const uint32_t Nd = net->Nd;
+  // tile size: 2^tshift posts (whole network when small)
+  uint32_t ts = 11;
+  while (ts > 5 && (1u << ts) > Nd * 2) --ts;
+  net->tshift = ts;
+  net->n_tiles = (Nd + (1u << ts) - 1) >> ts;
+  net->hbits = 13;
+  DBuf<unsigned long long> cnt;
+  cnt.alloc((size_t)net->n_tiles + 1);
+  cnt.zero(s);
+  if (net->n_edges)
+    launch_grid(net->n_edges, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->d_col.p, net->n_edges, ts, cnt.p); });
+  if (net->n_src_edges)
+    launch_grid(net->n_src_edges, [&](unsigned b) {
+      histogram_kernel<<<b, 256, 0, s>>>(net->d_src_post.p, net->n_src_edges, ts, cnt.p);
+    });
+  net->d_bin_base.alloc((size_t)net->n_tiles + 1);
+  size_t tb = 0;
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, net->d_bin_base.p, (int64_t)net->n_tiles + 1, s));
+  DBuf<uint8_t> temp;
+  temp.alloc(std::max<size_t>(tb, 1));
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, net->d_bin_base.p, (int64_t)net->n_tiles + 1, s));
+  const uint64_t tot = net->n_edges + net->n_src_edges;
+  net->d_bin_cnt.alloc(net->n_tiles);
+  net->d_bin_cnt.zero(s);
+  net->d_bkey.alloc(std::max<uint64_t>(tot, 1));
+  net->d_bw.alloc(std::max<uint64_t>(tot, 1));
+  net->d_bcell.alloc(std::max<uint64_t>(tot, 1));
+  SG_CUDA(cudaStreamSynchronize(s));
+}
+
+void build_sources(sg_net *net) {
+  const size_t S = net->srcs.size();
+  std::vector<float> p(S), w;
+  std::vector<uint32_t> seed(S), ptr(S + 1, 0), post;
+  std::vector<uint8_t> code;
+  uint64_t tot = 0;
+  for (size_t i = 0; i < S; ++i) {
+    p[i] = net->srcs[i].p;
+    seed[i] = net->srcs[i].seed;
+    ptr[i] = (uint32_t)tot;
+    tot += net->srcs[i].post.size();
+  }
+  SG_REQUIRE(tot < 0xFFFFFFFFull, SG_E_OVERFLOW, "too many Poisson-source synapses");
+  ptr[S] = (uint32_t)tot;
+  post.reserve(tot);
+  w.reserve(tot);
+  code.reserve(tot);
+  for (auto &sr : net->srcs) {
+    post.insert(post.end(), sr.post.begin(), sr.post.end());
+    w.insert(w.end(), sr.w.begin(), sr.w.end());
+    code.insert(code.end(), sr.code.begin(), sr.code.end());
+  }
+  net->n_src_edges = tot;
+  auto up = [&](auto &buf, const auto &vec) {
+    using T = typename std::decay_t<decltype(vec)>::value_type;
+    buf.alloc(std::max<size_t>(vec.size(), 1));
+    if (!vec.empty()) SG_CUDA(cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice, net->stream));
+  };
+  up(net->d_src_p, p);
+  up(net->d_src_seed, seed);
+  up(net->d_src_ptr, ptr);
+  up(net->d_src_post, post);
+  up(net->d_src_w, w);
+  up(net->d_src_code, code);
+  SG_CUDA(cudaStreamSynchronize(net->stream));
+  for (auto &sr : net->srcs) {  // host copies are no longer needed
+    std::vector<uint32_t>().swap(sr.post);
+    std::vector<float>().swap(sr.w);
+    std::vector<uint8_t>().swap(sr.code);
+  }
+}
+
+void build_stdp(sg_net *net) {
+  cudaStream_t s = net->stream;
+  const uint32_t Nd = net->Nd;
+  net->d_x_pre.alloc(Nd);
+  net->d_x_pre.zero(s);
+  net->d_x_post.alloc(Nd);
+  net->d_x_post.zero(s);
+  net->d_drift.alloc(1);
+  net->d_drift.zero(s);
+  DBuf<unsigned long long> cnt, ip64;
+  cnt.alloc((size_t)Nd + 1);
+  cnt.zero(s);
+  launch_grid(Nd, [&](unsigned b) {
+    csc_count_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, net->d_code.p, Nd, cnt.p);
+  });
+  ip64.alloc((size_t)Nd + 1);
+  size_t tb = 0;
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, ip64.p, (int64_t)Nd + 1, s));
+  DBuf<uint8_t> temp;
+  temp.alloc(std::max<size_t>(tb, 1));
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, ip64.p, (int64_t)Nd + 1, s));
+  net->d_in_ptr.alloc((size_t)Nd + 1);
+  launch_grid((uint64_t)Nd + 1, [&](unsigned b) { to_u32_kernel<<<b, 256, 0, s>>>(ip64.p, net->d_in_ptr.p, (uint64_t)Nd + 1); });
+  unsigned long long n_in = 0;
+  SG_CUDA(cudaMemcpyAsync(&n_in, ip64.p + Nd, 8, cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  net->d_in_edge.alloc(std::max<unsigned long long>(n_in, 1));
+  net->d_in_pre.alloc(std::max<unsigned long long>(n_in, 1));
+  DBuf<uint32_t> cursor;
+  cursor.alloc((size_t)Nd + 1);
+  SG_CUDA(cudaMemcpyAsync(cursor.p, net->d_in_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  launch_grid(Nd, [&](unsigned b) {
+    csc_fill_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, net->d_code.p, Nd, cursor.p,
+                                      net->d_in_edge.p, net->d_in_pre.p);
+  });
+  SG_CUDA(cudaStreamSynchronize(s));
+  net->ln_consts.resize(4);
+  net->ln_consts[2] = host_fast_exp(-net->stdp_dt / net->tau_pre);
+  net->ln_consts[3] = host_fast_exp(-net->stdp_dt / net->tau_post);
+}
+
+void finish_build(sg_net *net) {
+  cudaStream_t s = net->stream;
+  const uint32_t Nd = net->Nd;
+  SG_REQUIRE(net->kin.size() <= 3, SG_E_INVALID, "at most 3 kinetic profiles are supported on the device path");
+  // populations -> device
+  for (auto &p : net->pops) {
+    p.d_params.alloc(std::max<size_t>(p.params.size(), 1));
+    p.d_state.alloc(std::max<size_t>(p.state.size(), 1));
+    if (!p.params.empty())
+      SG_CUDA(cudaMemcpyAsync(p.d_params.p, p.params.data(), p.params.size() * 4, cudaMemcpyHostToDevice, s));
+    if (!p.state.empty())
+      SG_CUDA(cudaMemcpyAsync(p.d_state.p, p.state.data(), p.state.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  SG_CUDA(cudaStreamSynchronize(s));
+  for (auto &p : net->pops) {
+    std::vector<float>().swap(p.params);
+    std::vector<float>().swap(p.state);
+  }
+  const size_t n_rings = 1 + net->kin.size();
+  net->d_ring.alloc(std::max<size_t>(n_rings * kSlots * Nd, 1));
+  net->d_ring.zero(s);
+  net->d_kin_g.alloc(std::max<size_t>(net->kin.size() * Nd, 1));
+  net->d_kin_g.zero(s);
+  net->d_step.alloc(1);
+  net->d_step.zero(s);
+  net->d_n_active.alloc(1);
+  net->d_n_active.zero(s);
+  net->d_active.alloc(std::max<uint32_t>(Nd, 1));
+  net->d_last_bits.alloc(std::max<uint32_t>(Nd / 32, 1));
+  net->d_last_bits.zero(s);
+  net->d_done.alloc(1);
+  net->d_done.zero(s);
+  net->d_ev_step.alloc(1);
+  net->d_ev_step.zero(s);
+  net->d_ev_total.alloc(1);
+  net->d_ev_total.zero(s);
+  net->d_clamp.alloc(1);
+  net->d_clamp.zero(s);
+  net->d_stat_spk.alloc(net->stat_cap);
+  net->d_stat_spk.zero(s);
+  net->d_stat_ev.alloc(net->stat_cap);
+  net->d_stat_ev.zero(s);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  net->apply_blocks = (int)std::min<uint32_t>(net->n_tiles, (uint32_t)sms * 4);
+  net->apply_smem = (size_t)4 << net->hbits;
+  SG_CUDA(cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)net->apply_smem));
+  net->src_blocks = (int)((net->srcs.size() + 255) / 256);
+  net->expand_blocks = sms * 8;
+  SG_CUDA(cudaStreamSynchronize(s));
+  net->built = true;
+}
+
+template <int M> void launch_neuron(sg_net *net, const StepArgs &a, HostPop &p) {
+  PopArgs pa{p.d_state.p, p.d_params.p, p.n, p.cap, p.dev_off, net->ln_consts[0], net->ln_consts[1]};
+  const unsigned blocks = (p.cap + 255) / 256;
+  neuron_kernel<M><<<blocks, 256, 0, net->stream>>>(a, pa);
+}
+
+void enqueue_step(sg_net *net, const StepArgs &a) {
+  cudaStream_t s = net->stream;
+  for (auto &p : net->pops) {
+    if (p.n == 0) continue;
+    switch (p.model) {
+      case kLIF: launch_neuron<kLIF>(net, a, p); break;
+      case kIZH: launch_neuron<kIZH>(net, a, p); break;
+      case kGPEA: launch_neuron<kGPEA>(net, a, p); break;
+      case kHH: launch_neuron<kHH>(net, a, p); break;
+    }
+  }
+  expand_kernel<<<net->src_blocks + net->expand_blocks, 256, 0, s>>>(a, (uint32_t)net->src_blocks);
+  if (net->stdp_on) stdp_ltp_kernel<<<net->expand_blocks, 256, 0, s>>>(a);
+  apply_kernel<<<net->apply_blocks, 512, net->apply_smem, s>>>(a);
+}
+
+void drop_graph(sg_net *net) {
+  if (net->graph) cudaGraphExecDestroy(net->graph);
+  net->graph = nullptr;
+  net->graph_steps = 0;
+}
+
+void do_steps(sg_net *net, uint32_t n) {
+  if (net->total == 0) {
+    // empty network: only the counter advances (step.rs:22-25)
+    unsigned long long st = 0;
+    SG_CUDA(cudaMemcpyAsync(&st, net->d_step.p, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    st += n;
+    SG_CUDA(cudaMemcpyAsync(net->d_step.p, &st, 8, cudaMemcpyHostToDevice, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    net->host_step += n;
+    return;
+  }
+  const StepArgs a = make_args(net);
+  const uint32_t G = 32;  // steps per graph launch
+  uint32_t done = 0;
+  if (n >= G) {
+    if (!net->graph || net->graph_steps != G) {
+      drop_graph(net);
+      cudaGraph_t g;
+      SG_CUDA(cudaStreamBeginCapture(net->stream, cudaStreamCaptureModeThreadLocal));
+      for (uint32_t k = 0; k < G; ++k) enqueue_step(net, a);
+      SG_CUDA(cudaStreamEndCapture(net->stream, &g));
+      SG_CUDA(cudaGraphInstantiate(&net->graph, g, 0));
+      cudaGraphDestroy(g);
+      net->graph_steps = G;
+    }
+    for (; done + G <= n; done += G) SG_CUDA(cudaGraphLaunch(net->graph, net->stream));
+  }
+  for (; done < n; ++done) enqueue_step(net, a);
+  SG_CUDA(cudaGetLastError());
+  net->host_step += n;
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C"
+// ===========================================================================
+extern "C" {
+
+int sg_abi_version(void) { return SG_ABI_VERSION; }
+
+int sg_last_error(char *buf, size_t len) {
+  if (!buf || len == 0) return SG_E_INVALID;
+  std::strncpy(buf, g_last_error.c_str(), len - 1);
+  buf[len - 1] = 0;
+  return (int)std::min(g_last_error.size(), len - 1);
+}
+
+int sg_device_count(int *out) {
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    SG_CUDA(cudaGetDeviceCount(out));
+  });
+}
+
+int sg_net_create(sg_net **out, int device) {
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = nullptr;
+    int n = 0;
+    SG_CUDA(cudaGetDeviceCount(&n));
+    SG_REQUIRE(device >= 0 && device < n, SG_E_INVALID, "device ordinal out of range");
+    DevGuard g(device);
+    auto *net = new sg_net();
+    net->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete net;
+      SG_CUDA(e);
+    }
+    *out = net;
+  });
+}
+
+int sg_net_destroy(sg_net *net) {
+  if (!net) return SG_OK;
+  {
+    DevGuard g(net->device);
+    cudaStreamSynchronize(net->stream);
+    drop_graph(net);
+    cudaStream_t s = net->stream;
+    delete net;  // DBufs free their memory
+    cudaStreamDestroy(s);
+  }
+  return SG_OK;
+}
+
+int sg_synchronize(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    DevGuard g(net->device);
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+int sg_pop_add(sg_net *net, int model, uint32_t n, uint32_t *out_pop) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot add populations after build()");
+    SG_REQUIRE(n_params(model) > 0, SG_E_INVALID, "unknown model");
+    SG_REQUIRE(net->total + n <= 0xFFFFFFFFull, SG_E_INVALID, "Network: total neuron count exceeds u32::MAX");
+    HostPop p;
+    p.model = model;
+    p.n = n;
+    p.cap = (uint32_t)align_up(n, 32);
+    p.dev_off = net->Nd;
+    p.np = n_params(model);
+    p.ns = n_state(model);
+    p.params.assign((size_t)p.cap * p.np, 0.0f);
+    p.state.assign((size_t)p.cap * p.ns, 0.0f);
+    SG_REQUIRE((uint64_t)net->Nd + p.cap <= 0xFFFFFFFFull, SG_E_INVALID, "device neuron count exceeds u32");
+    net->Nd += p.cap;
+    net->pops.push_back(std::move(p));
+    net->total += n;
+    net->offsets.push_back((uint32_t)net->total);
+    if (out_pop) *out_pop = (uint32_t)net->pops.size() - 1;
+  });
+}
+
+static int pop_col(sg_net *net, uint32_t pop, uint32_t col, bool param) {
+  require_pop(net, pop);
+  const auto &p = net->pops[pop];
+  SG_REQUIRE(col < (param ? p.np : p.ns), SG_E_INVALID,
+             std::string(param ? "fill_param" : "fill_state") + ": column " + std::to_string(col) + " out of range");
+  return 0;
+}
+
+static int pop_write(sg_net *net, uint32_t pop, uint32_t col, bool param, const float *vals, float fill, uint32_t n) {
+  return run([&] {
+    pop_col(net, pop, col, param);
+    auto &p = net->pops[pop];
+    if (vals) SG_REQUIRE(n == p.n, SG_E_INVALID, "slice length does not match population size");
+    if (!net->built) {
+      auto &v = param ? p.params : p.state;
+      for (uint32_t i = 0; i < p.n; ++i) v[(size_t)col * p.cap + i] = vals ? vals[i] : fill;
+      return;
+    }
+    DevGuard g(net->device);
+    std::vector<float> tmp;
+    const float *src = vals;
+    if (!vals) {
+      tmp.assign(p.n, fill);
+      src = tmp.data();
+    }
+    float *dst = (param ? p.d_params.p : p.d_state.p) + (size_t)col * p.cap;
+    SG_CUDA(cudaMemcpyAsync(dst, src, (size_t)p.n * 4, cudaMemcpyHostToDevice, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+static int pop_read(sg_net *net, uint32_t pop, uint32_t col, bool param, float *out, uint32_t n) {
+  return run([&] {
+    pop_col(net, pop, col, param);
+    auto &p = net->pops[pop];
+    SG_REQUIRE(out && n == p.n, SG_E_INVALID, "output length does not match population size");
+    if (!net->built) {
+      const auto &v = param ? p.params : p.state;
+      std::memcpy(out, v.data() + (size_t)col * p.cap, (size_t)p.n * 4);
+      return;
+    }
+    DevGuard g(net->device);
+    const float *src = (param ? p.d_params.p : p.d_state.p) + (size_t)col * p.cap;
+    SG_CUDA(cudaMemcpyAsync(out, src, (size_t)p.n * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+int sg_pop_fill_param(sg_net *net, uint32_t pop, uint32_t col, float value) {
+  NET_CHECK(net);
+  return pop_write(net, pop, col, true, nullptr, value, 0);
+}
+int sg_pop_fill_state(sg_net *net, uint32_t pop, uint32_t col, float value) {
+  NET_CHECK(net);
+  return pop_write(net, pop, col, false, nullptr, value, 0);
+}
+int sg_pop_set_param(sg_net *net, uint32_t pop, uint32_t col, const float *vals, uint32_t n) {
+  NET_CHECK(net);
+  if (!vals) return (set_error("null values"), SG_E_INVALID);
+  return pop_write(net, pop, col, true, vals, 0, n);
+}
+int sg_pop_set_state(sg_net *net, uint32_t pop, uint32_t col, const float *vals, uint32_t n) {
+  NET_CHECK(net);
+  if (!vals) return (set_error("null values"), SG_E_INVALID);
+  return pop_write(net, pop, col, false, vals, 0, n);
+}
+int sg_pop_get_state(sg_net *net, uint32_t pop, uint32_t col, float *out, uint32_t n) {
+  NET_CHECK(net);
+  return pop_read(net, pop, col, false, out, n);
+}
+int sg_pop_get_param(sg_net *net, uint32_t pop, uint32_t col, float *out, uint32_t n) {
+  NET_CHECK(net);
+  return pop_read(net, pop, col, true, out, n);
+}
+
+int sg_connect_ex(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, const uint32_t *ti,
+                  const float *w, const uint8_t *d, const uint8_t *st, uint64_t n, uint32_t flags) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+    require_pop(net, from);
+    require_pop(net, to);
+    if (n == 0) return;
+    SG_REQUIRE(fi && ti && w && d, SG_E_INVALID, "null slice");
+    const auto &pf = net->pops[from];
+    const auto &pt = net->pops[to];
+    std::vector<uint32_t> pre(n), post(n);
+    std::vector<uint8_t> code(n);
+    for (uint64_t i = 0; i < n; ++i) {
+      SG_REQUIRE(fi[i] < pf.n, SG_E_INVALID, "from index " + std::to_string(fi[i]) + " out of bounds");
+      SG_REQUIRE(ti[i] < pt.n, SG_E_INVALID, "to index " + std::to_string(ti[i]) + " out of bounds");
+      SG_REQUIRE(std::isfinite(w[i]), SG_E_INVALID, "Network::connect: weight " + std::to_string(i) + " must be finite");
+      SG_REQUIRE(d[i] < kSlots, SG_E_INVALID, "delay " + std::to_string(d[i]) + " >= MAX_DELAY_SLOTS (32)");
+      const uint8_t s = st ? st[i] : 0;
+      SG_REQUIRE(s <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
+      pre[i] = pf.dev_off + fi[i];
+      post[i] = pt.dev_off + ti[i];
+      code[i] = edge_code(d[i], s, (flags & SG_EDGE_STDP) != 0);
+    }
+    DevGuard g(net->device);
+    upload_staged_edges(net, pre.data(), post.data(), w, code.data(), n);
+  });
+}
+
+int sg_connect(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, const uint32_t *ti,
+               const float *w, const uint8_t *d, uint64_t n) {
+  return sg_connect_ex(net, from, fi, to, ti, w, d, nullptr, n, 0);
+}
+
+int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k_in, uint64_t seed,
+                              uint32_t n_exc, float w_exc, float w_inh, uint8_t d_min, uint8_t d_max,
+                              uint8_t st_e, uint8_t st_i, uint32_t flags_e) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+    require_pop(net, from);
+    require_pop(net, to);
+    SG_REQUIRE(d_min <= d_max && d_max < kSlots, SG_E_INVALID, "delay range invalid");
+    SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
+    SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
+    const auto &pf = net->pops[from];
+    const auto &pt = net->pops[to];
+    SG_REQUIRE(pf.n > 0 || k_in == 0, SG_E_INVALID, "empty source population");
+    const uint64_t n = (uint64_t)pt.n * k_in;
+    if (n == 0) return;
+    DevGuard g(net->device);
+    const size_t n0 = net->e_pre.n;
+    net->e_pre.reserve(n0 + n, net->stream);
+    net->e_post.reserve(n0 + n, net->stream);
+    net->e_w.reserve(n0 + n, net->stream);
+    net->e_code.reserve(n0 + n, net->stream);
+    launch_grid(n, [&](unsigned b) {
+      synth_indegree_kernel<<<b, 256, 0, net->stream>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p, n0,
+                                                        pt.n, k_in, seed, pf.dev_off, pf.n, pt.dev_off, n_exc, w_exc,
+                                                        w_inh, d_min, (uint32_t)(d_max - d_min + 1), st_e, st_i, flags_e);
+    });
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
+  });
+}
+
+int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "register_kinetics must be called before build()");
+    SG_REQUIRE(std::isfinite(dt) && dt > 0, SG_E_INVALID, "register_kinetics: dt must be finite and > 0");
+    SG_REQUIRE(std::isfinite(tau_decay) && tau_decay > 0, SG_E_INVALID, "tau_decay must be finite and > 0");
+    SG_REQUIRE(std::isfinite(erev), SG_E_INVALID, "erev must be finite");
+    SG_REQUIRE(net->kin.size() < 3, SG_E_INVALID, "at most 3 kinetic profiles are supported on the device path");
+    net->kin.push_back(Kin{std::exp(-dt / tau_decay), erev});  // step.rs:252-254 (f32 exp)
+    if (out_id) *out_id = (uint32_t)net->kin.size();
+  });
+}
+
+int sg_poisson_add_many(sg_net *net, uint32_t n, float rate_hz, float dt_ms, const uint32_t *seeds, uint32_t seed0,
+                        uint32_t *out_first) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "add_poisson_source must be called before build()");
+    SG_REQUIRE(std::isfinite(rate_hz) && rate_hz >= 0, SG_E_INVALID, "add_poisson_source: rate_hz must be finite and >= 0");
+    SG_REQUIRE(std::isfinite(dt_ms) && dt_ms > 0, SG_E_INVALID, "add_poisson_source: dt_ms must be finite and > 0");
+    float p = rate_hz * dt_ms / 1000.0f;  // core.rs:301
+    p = std::fmin(std::fmax(p, 0.0f), 1.0f);
+    if (out_first) *out_first = (uint32_t)net->srcs.size();
+    net->srcs.reserve(net->srcs.size() + n);
+    for (uint32_t i = 0; i < n; ++i) {
+      HostSrc s;
+      s.p = p;
+      s.seed = seeds ? seeds[i] : seed0 + i;
+      net->srcs.push_back(std::move(s));
+    }
+  });
+}
+
+int sg_poisson_add(sg_net *net, float rate_hz, float dt_ms, uint32_t seed, uint32_t *out_id) {
+  return sg_poisson_add_many(net, 1, rate_hz, dt_ms, nullptr, seed, out_id);
+}
+
+int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts, const float *w,
+                       const uint8_t *d, const uint8_t *st, uint64_t n) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+    SG_REQUIRE(src < net->srcs.size(), SG_E_INVALID, "poisson source out of range");
+    require_pop(net, to);
+    const auto &pt = net->pops[to];
+    auto &s = net->srcs[src];
+    for (uint64_t i = 0; i < n; ++i) {
+      SG_REQUIRE(posts[i] < pt.n, SG_E_INVALID, "post index out of bounds");
+      SG_REQUIRE(std::isfinite(w[i]), SG_E_INVALID, "connect_poisson_source: weight must be finite");
+      SG_REQUIRE(d[i] < kSlots, SG_E_INVALID, "connect_poisson_source: delay >= MAX_DELAY_SLOTS (32)");
+      const uint8_t t = st ? st[i] : 0;
+      SG_REQUIRE(t <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
+      s.post.push_back(pt.dev_off + posts[i]);
+      s.w.push_back(w[i]);
+      s.code.push_back(edge_code(d[i], t, false));
+    }
+  });
+}
+
+int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint32_t to, const uint32_t *posts,
+                                  float weight, uint8_t delay) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+    SG_REQUIRE((uint64_t)first + n <= net->srcs.size(), SG_E_INVALID, "poisson source out of range");
+    require_pop(net, to);
+    SG_REQUIRE(std::isfinite(weight), SG_E_INVALID, "weight must be finite");
+    SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
+    const auto &pt = net->pops[to];
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t q = posts ? posts[i] : i;
+      SG_REQUIRE(q < pt.n, SG_E_INVALID, "post index out of bounds");
+      auto &s = net->srcs[first + i];
+      s.post.push_back(pt.dev_off + q);
+      s.w.push_back(weight);
+      s.code.push_back(edge_code(delay, 0, false));
+    }
+  });
+}
+
+int sg_stdp_config(sg_net *net, float dt, float tau_pre, float tau_post, float a_plus, float a_minus, float w_min,
+                   float w_max) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "stdp must be configured before build()");
+    SG_REQUIRE(dt > 0 && tau_pre > 0 && tau_post > 0 && w_min <= w_max, SG_E_INVALID, "invalid STDP config");
+    net->stdp_on = true;
+    net->stdp_dt = dt;
+    net->tau_pre = tau_pre;
+    net->tau_post = tau_post;
+    net->a_plus = a_plus;
+    net->a_minus = a_minus;
+    net->w_min = w_min;
+    net->w_max = w_max;
+  });
+}
+
+int sg_set_weight_format(sg_net *net, int format) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "weight format must be set before build()");
+    SG_REQUIRE(format == SG_W_F32, SG_E_INVALID, "only FP32 weights are available in this build");
+    net->weight_format = format;
+  });
+}
+
+int sg_set_deterministic(sg_net *net, int on) {
+  NET_CHECK(net);
+  return run([&] {
+    net->deterministic = on ? 1 : 0;
+    drop_graph(net);
+  });
+}
+
+int sg_build(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Network::build() called twice — the graph is already built");
+    DevGuard g(net->device);
+    // GPEA Nernst constants with the host libm ln (gpea.rs:277-278)
+    net->ln_consts = {std::log(10.0f / 140.0f), std::log(5.0f / 140.0f)};
+    const uint64_t E = net->e_pre.n;
+    uint64_t src_e = 0;
+    for (auto &s : net->srcs) src_e += s.post.size();
+    SG_REQUIRE(E + src_e < 0xFFFFFFFFull, SG_E_OVERFLOW,
+               "SparseGraph: too many synapses for a u32 CSR row_ptr / event key");
+    build_graph(net);
+    build_sources(net);
+    build_bins(net);
+    if (net->stdp_on) build_stdp(net);
+    finish_build(net);
+  });
+}
+
+int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col, const float *w, const uint8_t *d) {
+  NET_CHECK(net);
+  const int rc = run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Network::build() called twice");
+    SG_REQUIRE(net->e_pre.n == 0, SG_E_STATE, "from_csr: edges were already added");
+    SG_REQUIRE(row_ptr && row_ptr[0] == 0, SG_E_INVALID, "CSR row_ptr must start at 0");
+    const uint64_t N = net->total;
+    for (uint64_t i = 0; i < N; ++i)
+      SG_REQUIRE(row_ptr[i] <= row_ptr[i + 1], SG_E_INVALID, "CSR row_ptr must be monotonically non-decreasing");
+    const uint64_t E = row_ptr[N];
+    // global -> device index
+    std::vector<uint32_t> g2d(N);
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      for (uint32_t i = 0; i < net->pops[p].n; ++i) g2d[net->offsets[p] + i] = net->pops[p].dev_off + i;
+    std::vector<uint32_t> pre(E), post(E);
+    std::vector<uint8_t> code(E);
+    for (uint64_t i = 0; i < N; ++i)
+      for (uint64_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+        SG_REQUIRE(col[e] < N, SG_E_INVALID, "col index out of range");
+        SG_REQUIRE(std::isfinite(w[e]), SG_E_INVALID, "weight must be finite");
+        SG_REQUIRE(d[e] < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
+        pre[e] = g2d[i];
+        post[e] = g2d[col[e]];
+        code[e] = edge_code(d[e], 0, false);
+      }
+    DevGuard g(net->device);
+    if (E) upload_staged_edges(net, pre.data(), post.data(), w, code.data(), E);
+  });
+  return rc != SG_OK ? rc : sg_build(net);
+}
+
+int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals, uint64_t n) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "inject_current() called before build()");
+    require_pop(net, pop);
+    if (n == 0) return;
+    SG_REQUIRE(idx && vals, SG_E_INVALID, "null slice");
+    const auto &p = net->pops[pop];
+    std::vector<uint8_t> seen(p.n, 0);
+    bool dup = false;
+    for (uint64_t i = 0; i < n; ++i) {
+      SG_REQUIRE(idx[i] < p.n, SG_E_INVALID,
+                 "inject_current: neuron index " + std::to_string(idx[i]) + " out of bounds (population has " +
+                     std::to_string(p.n) + ")");
+      SG_REQUIRE(std::isfinite(vals[i]), SG_E_INVALID, "inject_current: value must be finite");
+      dup |= seen[idx[i]] != 0;
+      seen[idx[i]] = 1;
+    }
+    DevGuard g(net->device);
+    if (net->d_inj_idx.n < n) {
+      net->d_inj_idx.alloc(n);
+      net->d_inj_val.alloc(n);
+    }
+    SG_CUDA(cudaMemcpyAsync(net->d_inj_idx.p, idx, n * 4, cudaMemcpyHostToDevice, net->stream));
+    SG_CUDA(cudaMemcpyAsync(net->d_inj_val.p, vals, n * 4, cudaMemcpyHostToDevice, net->stream));
+    unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 8);
+    inject_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->d_step.p, net->d_inj_idx.p,
+                                                   net->d_inj_val.p, n, p.dev_off, dup ? 1 : 0);
+    SG_CUDA(cudaGetLastError());
+    // the staging buffers are reused by the next call
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+int sg_step(sg_net *net, uint32_t n_steps) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "Network::step() called before build()");
+    DevGuard g(net->device);
+    do_steps(net, n_steps);
+  });
+}
+
+int sg_raster_enable(sg_net *net, uint32_t cap) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "raster recording needs a built network");
+    DevGuard g(net->device);
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    drop_graph(net);
+    net->raster_cap = cap;
+    if (cap) {
+      net->d_raster.alloc((size_t)cap * (net->Nd / 32));
+      net->d_raster.zero(net->stream);
+    } else {
+      net->d_raster.release();
+    }
+    net->raster_read_step = net->host_step;
+  });
+}
+
+int sg_raster_read(sg_net *net, uint8_t *out, uint64_t cap_bytes, uint32_t *n_steps) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->raster_cap > 0, SG_E_STATE, "raster recording is not enabled");
+    DevGuard g(net->device);
+    const uint64_t k = net->host_step - net->raster_read_step;
+    SG_REQUIRE(k <= net->raster_cap, SG_E_OVERFLOW,
+               "raster overflow: " + std::to_string(k) + " steps since the last read, capacity " +
+                   std::to_string(net->raster_cap));
+    const uint64_t N = net->total;
+    SG_REQUIRE(k * N <= cap_bytes, SG_E_INVALID, "output buffer too small");
+    const uint32_t words = net->Nd / 32;
+    std::vector<uint32_t> bits((size_t)net->raster_cap * words);
+    SG_CUDA(cudaMemcpyAsync(bits.data(), net->d_raster.p, bits.size() * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (uint64_t t = 0; t < k; ++t) {
+      const uint64_t step = net->raster_read_step + t;
+      const uint32_t *row = bits.data() + (size_t)(step % net->raster_cap) * words;
+      uint8_t *o = out + t * N;
+      for (size_t p = 0; p < net->pops.size(); ++p) {
+        const auto &pp = net->pops[p];
+        for (uint32_t i = 0; i < pp.n; ++i) {
+          const uint32_t di = pp.dev_off + i;
+          o[net->offsets[p] + i] = (uint8_t)((row[di >> 5] >> (di & 31)) & 1u);
+        }
+      }
+    }
+    if (n_steps) *n_steps = (uint32_t)k;
+    net->raster_read_step = net->host_step;
+  });
+}
+
+int sg_stats_read(sg_net *net, uint32_t *spikes, uint64_t *events, uint32_t cap, uint32_t *n_steps) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    DevGuard g(net->device);
+    const uint64_t k = net->host_step - net->stat_read_step;
+    SG_REQUIRE(k <= net->stat_cap, SG_E_OVERFLOW, "stats overflow");
+    SG_REQUIRE(k <= cap, SG_E_INVALID, "output buffer too small");
+    std::vector<uint32_t> s(net->stat_cap);
+    std::vector<unsigned long long> e(net->stat_cap);
+    SG_CUDA(cudaMemcpyAsync(s.data(), net->d_stat_spk.p, s.size() * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(e.data(), net->d_stat_ev.p, e.size() * 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (uint64_t t = 0; t < k; ++t) {
+      const uint64_t st = net->stat_read_step + t;
+      if (spikes) spikes[t] = s[st % net->stat_cap];
+      if (events) events[t] = e[st % net->stat_cap];
+    }
+    if (n_steps) *n_steps = (uint32_t)k;
+    net->stat_read_step = net->host_step;
+  });
+}
+
+int sg_spikes(sg_net *net, uint32_t pop, int32_t *out, uint32_t n) {
+  NET_CHECK(net);
+  return run([&] {
+    require_pop(net, pop);
+    const auto &p = net->pops[pop];
+    SG_REQUIRE(out && n == p.n, SG_E_INVALID, "output length does not match population size");
+    if (!net->built) {
+      std::memset(out, 0, (size_t)n * 4);
+      return;
+    }
+    DevGuard g(net->device);
+    const uint32_t w0 = p.dev_off / 32, nw = p.cap / 32;
+    std::vector<uint32_t> bits(std::max<uint32_t>(nw, 1));
+    if (nw) SG_CUDA(cudaMemcpyAsync(bits.data(), net->d_last_bits.p + w0, (size_t)nw * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (uint32_t i = 0; i < p.n; ++i) out[i] = (int32_t)((bits[i >> 5] >> (i & 31)) & 1u);
+  });
+}
+
+int sg_step_counter(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = net->host_step;
+  });
+}
+
+int sg_total_neurons(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = net->total;
+  });
+}
+
+int sg_num_synapses(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = net->built ? net->n_edges : net->e_pre.n;
+  });
+}
+
+int sg_events_total(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    if (!net->built) {
+      *out = 0;
+      return;
+    }
+    DevGuard g(net->device);
+    unsigned long long v = 0;
+    SG_CUDA(cudaMemcpyAsync(&v, net->d_ev_total.p, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    *out = v;
+  });
+}
+
+static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *d, bool only_w) {
+  const uint32_t Nd = net->Nd;
+  const uint64_t E = net->n_edges;
+  std::vector<uint32_t> rp(Nd + 1), c(E);
+  std::vector<uint8_t> code(E);
+  SG_CUDA(cudaMemcpyAsync(rp.data(), net->d_row_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToHost, net->stream));
+  if (E) {
+    if (!only_w) SG_CUDA(cudaMemcpyAsync(c.data(), net->d_col.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(w, net->d_w.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
+    if (!only_w) SG_CUDA(cudaMemcpyAsync(code.data(), net->d_code.p, E, cudaMemcpyDeviceToHost, net->stream));
+  }
+  SG_CUDA(cudaStreamSynchronize(net->stream));
+  if (only_w) return;
+  // device index -> global index
+  std::vector<uint32_t> d2g(Nd, 0xFFFFFFFFu);
+  for (size_t p = 0; p < net->pops.size(); ++p)
+    for (uint32_t i = 0; i < net->pops[p].n; ++i) d2g[net->pops[p].dev_off + i] = net->offsets[p] + i;
+  // padding rows are empty, so the global row_ptr is the device one restricted
+  for (size_t p = 0; p < net->pops.size(); ++p)
+    for (uint32_t i = 0; i < net->pops[p].n; ++i) row_ptr[net->offsets[p] + i] = rp[net->pops[p].dev_off + i];
+  row_ptr[net->total] = (uint32_t)E;
+  for (uint64_t e = 0; e < E; ++e) {
+    col[e] = d2g[c[e]];
+    d[e] = (uint8_t)code_delay(code[e]);
+  }
+}
+
+int sg_graph_read(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *d) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(row_ptr && col && w && d, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    read_csr_global(net, row_ptr, col, w, d, false);
+  });
+}
+
+int sg_weights_read(sg_net *net, float *w) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(w, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    read_csr_global(net, nullptr, nullptr, w, nullptr, true);
+  });
+}
+
+int sg_ring_read(sg_net *net, uint32_t ring, float *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(ring <= net->kin.size(), SG_E_INVALID, "ring out of range");
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    const uint32_t Nd = net->Nd;
+    std::vector<float> r((size_t)kSlots * Nd);
+    SG_CUDA(cudaMemcpyAsync(r.data(), net->d_ring.p + (size_t)ring * kSlots * Nd, r.size() * 4,
+                            cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    const uint64_t N = net->total;
+    for (uint32_t s = 0; s < kSlots; ++s)
+      for (size_t p = 0; p < net->pops.size(); ++p)
+        for (uint32_t i = 0; i < net->pops[p].n; ++i)
+          out[(size_t)s * N + net->offsets[p] + i] = r[(size_t)s * Nd + net->pops[p].dev_off + i];
+  });
+}
+
+int sg_stdp_drift(sg_net *net, double *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built && net->stdp_on, SG_E_STATE, "STDP is not enabled");
+    DevGuard g(net->device);
+    SG_CUDA(cudaMemcpyAsync(out, net->d_drift.p, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+int sg_stdp_traces(sg_net *net, float *x_pre, float *x_post) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built && net->stdp_on, SG_E_STATE, "STDP is not enabled");
+    DevGuard g(net->device);
+    std::vector<float> a(net->Nd), b(net->Nd);
+    SG_CUDA(cudaMemcpyAsync(a.data(), net->d_x_pre.p, a.size() * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(b.data(), net->d_x_post.p, b.size() * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      for (uint32_t i = 0; i < net->pops[p].n; ++i) {
+        x_pre[net->offsets[p] + i] = a[net->pops[p].dev_off + i];
+        x_post[net->offsets[p] + i] = b[net->pops[p].dev_off + i];
+      }
+  });
+}
+
+int sg_clamp_hits(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    DevGuard g(net->device);
+    unsigned long long v = 0;
+    SG_CUDA(cudaMemcpyAsync(&v, net->d_clamp.p, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    *out = v;
+  });
+}
+
+int sg_footprint(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    uint64_t b = 0;
+    for (auto &p : net->pops) b += (p.d_params.n + p.d_state.n) * 4;
+    b += net->d_ring.n * 4 + net->d_kin_g.n * 4 + net->d_row_ptr.n * 4 + net->d_col.n * 4 + net->d_w.n * 4 +
+         net->d_code.n + net->d_bkey.n * 4 + net->d_bw.n * 4 + net->d_bcell.n * 4 + net->d_active.n * 4 +
+         net->d_src_post.n * 4 + net->d_src_w.n * 4 + net->d_src_code.n + net->d_src_p.n * 4 +
+         net->d_src_seed.n * 4 + net->d_src_ptr.n * 4 + net->d_raster.n * 4 + net->d_in_edge.n * 8;
+    *out = b;
+  });
+}
+
+int sg_stream(sg_net *net, void **out) {
+  NET_CHECK(net);
+  if (!out) return SG_E_INVALID;
+  *out = (void *)net->stream;
+  return SG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+"""Loading and binding of libsimuse_b200.so (the C ABI of include/simuse_b200.h)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+_PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+_ROOT = os.path.dirname(_PKG_DIR)  # dioma-core_b200/
+library_path = os.path.join(_ROOT, "libsimuse_b200.so")
+header_path = os.path.join(os.path.dirname(_ROOT), "include", "simuse_b200.h")
+
+
+class SimuseError(RuntimeError):
+    """A non-zero status from the C ABI (the reference panics in these cases)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+vp, i32, u32, u64, f32, f64, sz = (
+    C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_float, C.c_double, C.c_size_t)
+u8 = C.c_uint8
+
+# name -> argument types (all return int status)
+SIGNATURES = {
+    "sg_abi_version": [],
+    "sg_last_error": [C.c_char_p, sz],
+    "sg_device_count": [vp],
+    "sg_net_create": [vp, i32],
+    "sg_net_destroy": [vp],
+    "sg_synchronize": [vp],
+    "sg_pop_add": [vp, i32, u32, vp],
+    "sg_pop_fill_param": [vp, u32, u32, f32],
+    "sg_pop_fill_state": [vp, u32, u32, f32],
+    "sg_pop_set_param": [vp, u32, u32, vp, u32],
+    "sg_pop_set_state": [vp, u32, u32, vp, u32],
+    "sg_pop_get_state": [vp, u32, u32, vp, u32],
+    "sg_pop_get_param": [vp, u32, u32, vp, u32],
+    "sg_connect": [vp, u32, vp, u32, vp, vp, vp, u64],
+    "sg_connect_ex": [vp, u32, vp, u32, vp, vp, vp, vp, u64, u32],
+    "sg_connect_fixed_indegree": [vp, u32, u32, u32, u64, u32, f32, f32, u8, u8, u8, u8, u32],
+    "sg_register_expone": [vp, f32, f32, f32, vp],
+    "sg_poisson_add": [vp, f32, f32, u32, vp],
+    "sg_poisson_add_many": [vp, u32, f32, f32, vp, u32, vp],
+    "sg_poisson_connect": [vp, u32, u32, vp, vp, vp, vp, u64],
+    "sg_poisson_connect_one_to_one": [vp, u32, u32, u32, vp, f32, u8],
+    "sg_stdp_config": [vp, f32, f32, f32, f32, f32, f32, f32],
+    "sg_set_weight_format": [vp, i32],
+    "sg_set_deterministic": [vp, i32],
+    "sg_build": [vp],
+    "sg_build_from_csr": [vp, vp, vp, vp, vp],
+    "sg_inject": [vp, u32, vp, vp, u64],
+    "sg_step": [vp, u32],
+    "sg_raster_enable": [vp, u32],
+    "sg_raster_read": [vp, vp, u64, vp],
+    "sg_stats_read": [vp, vp, vp, u32, vp],
+    "sg_spikes": [vp, u32, vp, u32],
+    "sg_step_counter": [vp, vp],
+    "sg_total_neurons": [vp, vp],
+    "sg_num_synapses": [vp, vp],
+    "sg_events_total": [vp, vp],
+    "sg_graph_read": [vp, vp, vp, vp, vp],
+    "sg_weights_read": [vp, vp],
+    "sg_ring_read": [vp, u32, vp],
+    "sg_stdp_drift": [vp, vp],
+    "sg_stdp_traces": [vp, vp, vp],
+    "sg_clamp_hits": [vp, vp],
+    "sg_footprint": [vp, vp],
+    "sg_stream": [vp, vp],
+}
+
+_lib = None
+
+
+def declared_symbols() -> list[str]:
+    """Every function declared in include/simuse_b200.h."""
+    txt = open(header_path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\bint\s+(sg_\w+)\s*\(", txt)))
+
+
+def lib():
+    """The loaded library; raises when it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(library_path):
+            raise ImportError(
+                f"{library_path} is missing: build it with `make -C dioma-core_b200` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(library_path)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = i32
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(4096)
+    lib().sg_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        raise SimuseError(rc, last_error())
+    return rc

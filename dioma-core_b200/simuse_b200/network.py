@@ -1,0 +1,261 @@
+"""``Network`` — the reference's builder/step API over the B200 C ABI.
+
+Method names, argument meaning and error behaviour follow
+``pillars::api::Network`` (crates/SiMuse/crates/pillars/src/api/net/network/
+core.rs:87-622, build.rs:18-276, step.rs:18-189): populations in creation
+order, neuron indices within a population, delays in steps (< 32), errors
+where the reference panics (raised here as SimuseError).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, lib
+
+LIF, IZH, GPEA, HH = 1, 2, 3, 4
+W_F32, W_BF16, W_FP8 = 0, 1, 2
+EDGE_STDP = 1
+
+N_PARAMS = {LIF: 6, IZH: 7, GPEA: 14, HH: 10}
+N_STATE = {LIF: 2, IZH: 3, GPEA: 9, HH: 4}
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Network:
+    """One simulated network resident on one GPU (one CUDA stream)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().sg_net_create(C.byref(h), device))
+        self._h = h
+        self._sizes: list[int] = []
+        self._models: list[int] = []
+        self.device = device
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().sg_net_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- builder (core.rs) ---------------------------------------------------
+    def add_population(self, model: int, n: int) -> int:
+        out = C.c_uint32()
+        check(lib().sg_pop_add(self._h, model, n, C.byref(out)))
+        self._sizes.append(n)
+        self._models.append(model)
+        return out.value
+
+    def fill_param(self, pop: int, col: int, value: float):
+        check(lib().sg_pop_fill_param(self._h, pop, col, float(value)))
+
+    def fill_state(self, pop: int, col: int, value: float):
+        check(lib().sg_pop_fill_state(self._h, pop, col, float(value)))
+
+    def set_param(self, pop: int, col: int, values):
+        a = np.ascontiguousarray(values, np.float32)
+        check(lib().sg_pop_set_param(self._h, pop, col, _p(a), a.size))
+
+    def set_state(self, pop: int, col: int, values):
+        a = np.ascontiguousarray(values, np.float32)
+        check(lib().sg_pop_set_state(self._h, pop, col, _p(a), a.size))
+
+    def state(self, pop: int, col: int) -> np.ndarray:
+        out = np.empty(self._sizes[pop], np.float32)
+        check(lib().sg_pop_get_state(self._h, pop, col, _p(out), out.size))
+        return out
+
+    def param_slice(self, pop: int, col: int) -> np.ndarray:
+        out = np.empty(self._sizes[pop], np.float32)
+        check(lib().sg_pop_get_param(self._h, pop, col, _p(out), out.size))
+        return out
+
+    def connect(self, frm, from_idx, to, to_idx, weights, delays, syn_types=None, stdp=False):
+        fi = np.ascontiguousarray(from_idx, np.uint32)
+        ti = np.ascontiguousarray(to_idx, np.uint32)
+        w = np.ascontiguousarray(weights, np.float32)
+        d = np.ascontiguousarray(delays, np.uint8)
+        st = None if syn_types is None else np.ascontiguousarray(syn_types, np.uint8)
+        if not (fi.size == ti.size == w.size == d.size) or (st is not None and st.size != fi.size):
+            from ._lib import SimuseError
+            raise SimuseError(-1, "connect: slice length mismatch")
+        check(lib().sg_connect_ex(self._h, frm, _p(fi), to, _p(ti), _p(w), _p(d), _p(st), fi.size,
+                                  EDGE_STDP if stdp else 0))
+
+    def connect_fixed_indegree(self, frm, to, k_in, seed, n_exc, w_exc, w_inh, d_min, d_max,
+                               syn_type_exc=0, syn_type_inh=0, stdp_exc=False):
+        check(lib().sg_connect_fixed_indegree(self._h, frm, to, k_in, seed, n_exc, w_exc, w_inh,
+                                              d_min, d_max, syn_type_exc, syn_type_inh,
+                                              EDGE_STDP if stdp_exc else 0))
+
+    def register_expone(self, tau_decay: float, erev: float, dt: float) -> int:
+        out = C.c_uint32()
+        check(lib().sg_register_expone(self._h, tau_decay, erev, dt, C.byref(out)))
+        return out.value
+
+    def add_poisson_source(self, rate_hz: float, dt_ms: float, seed: int) -> int:
+        out = C.c_uint32()
+        check(lib().sg_poisson_add(self._h, rate_hz, dt_ms, seed, C.byref(out)))
+        return out.value
+
+    def add_poisson_sources(self, n: int, rate_hz: float, dt_ms: float, seeds=None, seed0: int = 0) -> int:
+        out = C.c_uint32()
+        s = None if seeds is None else np.ascontiguousarray(seeds, np.uint32)
+        check(lib().sg_poisson_add_many(self._h, n, rate_hz, dt_ms, _p(s), seed0, C.byref(out)))
+        return out.value
+
+    def connect_poisson_source(self, src, to, posts, weights, delays, syn_types=None):
+        p = np.ascontiguousarray(posts, np.uint32)
+        w = np.ascontiguousarray(weights, np.float32)
+        d = np.ascontiguousarray(delays, np.uint8)
+        st = None if syn_types is None else np.ascontiguousarray(syn_types, np.uint8)
+        check(lib().sg_poisson_connect(self._h, src, to, _p(p), _p(w), _p(d), _p(st), p.size))
+
+    def connect_poisson_one_to_one(self, first_src, n, to, weight, delay, posts=None):
+        p = None if posts is None else np.ascontiguousarray(posts, np.uint32)
+        check(lib().sg_poisson_connect_one_to_one(self._h, first_src, n, to, _p(p), weight, delay))
+
+    def stdp_config(self, dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max):
+        check(lib().sg_stdp_config(self._h, dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max))
+
+    def set_weight_format(self, fmt: int):
+        check(lib().sg_set_weight_format(self._h, fmt))
+
+    def set_deterministic(self, on: bool):
+        check(lib().sg_set_deterministic(self._h, 1 if on else 0))
+
+    def build(self):
+        check(lib().sg_build(self._h))
+
+    def build_from_csr(self, row_ptr, col, weights, delays):
+        rp = np.ascontiguousarray(row_ptr, np.uint32)
+        c = np.ascontiguousarray(col, np.uint32)
+        w = np.ascontiguousarray(weights, np.float32)
+        d = np.ascontiguousarray(delays, np.uint8)
+        check(lib().sg_build_from_csr(self._h, _p(rp), _p(c), _p(w), _p(d)))
+
+    # -- run (build.rs / step.rs) -----------------------------------------------
+    def inject_current(self, pop, indices, values):
+        i = np.ascontiguousarray(indices, np.uint32)
+        v = np.ascontiguousarray(values, np.float32)
+        if i.size != v.size:
+            from ._lib import SimuseError
+            raise SimuseError(-1, "inject_current: indices/values length mismatch")
+        check(lib().sg_inject(self._h, pop, _p(i), _p(v), i.size))
+
+    def step(self, n_steps: int = 1):
+        check(lib().sg_step(self._h, n_steps))
+
+    def synchronize(self):
+        check(lib().sg_synchronize(self._h))
+
+    def enable_raster(self, capacity_steps: int):
+        check(lib().sg_raster_enable(self._h, capacity_steps))
+        self._raster_mark = self.step_counter
+
+    def read_raster(self) -> np.ndarray:
+        """Spike raster [steps since the last read][total_neurons] as uint8."""
+        n = C.c_uint32()
+        k = self.step_counter - getattr(self, "_raster_mark", 0)
+        out = np.zeros(max(k * self.total_neurons, 1), np.uint8)
+        check(lib().sg_raster_read(self._h, _p(out), out.size, C.byref(n)))
+        self._raster_mark = self.step_counter
+        return out[: n.value * self.total_neurons].reshape(n.value, self.total_neurons)
+
+    def read_stats(self):
+        k = C.c_uint32()
+        n = max(1, self.step_counter - getattr(self, "_stats_mark", 0))
+        spk = np.zeros(n, np.uint32)
+        ev = np.zeros(n, np.uint64)
+        check(lib().sg_stats_read(self._h, _p(spk), _p(ev), n, C.byref(k)))
+        self._stats_mark = self.step_counter
+        return spk[: k.value], ev[: k.value]
+
+    # -- readback -----------------------------------------------------------
+    def spikes(self, pop: int) -> np.ndarray:
+        out = np.empty(self._sizes[pop], np.int32)
+        check(lib().sg_spikes(self._h, pop, _p(out), out.size))
+        return out
+
+    def _u64(self, fn) -> int:
+        out = C.c_uint64()
+        check(fn(self._h, C.byref(out)))
+        return out.value
+
+    @property
+    def step_counter(self) -> int:
+        return self._u64(lib().sg_step_counter)
+
+    @property
+    def total_neurons(self) -> int:
+        return self._u64(lib().sg_total_neurons)
+
+    @property
+    def num_synapses(self) -> int:
+        return self._u64(lib().sg_num_synapses)
+
+    @property
+    def events_total(self) -> int:
+        return self._u64(lib().sg_events_total)
+
+    @property
+    def clamp_hits(self) -> int:
+        return self._u64(lib().sg_clamp_hits)
+
+    @property
+    def footprint(self) -> int:
+        return self._u64(lib().sg_footprint)
+
+    def graph(self):
+        n, e = self.total_neurons, self.num_synapses
+        rp = np.empty(n + 1, np.uint32)
+        c = np.empty(e, np.uint32)
+        w = np.empty(e, np.float32)
+        d = np.empty(e, np.uint8)
+        check(lib().sg_graph_read(self._h, _p(rp), _p(c), _p(w), _p(d)))
+        return rp, c, w, d
+
+    def weights(self) -> np.ndarray:
+        w = np.empty(self.num_synapses, np.float32)
+        check(lib().sg_weights_read(self._h, _p(w)))
+        return w
+
+    def ring(self, ring: int = 0) -> np.ndarray:
+        out = np.empty((32, self.total_neurons), np.float32)
+        check(lib().sg_ring_read(self._h, ring, _p(out)))
+        return out
+
+    @property
+    def stdp_drift(self) -> float:
+        out = C.c_double()
+        check(lib().sg_stdp_drift(self._h, C.byref(out)))
+        return out.value
+
+    def stdp_traces(self):
+        a = np.empty(self.total_neurons, np.float32)
+        b = np.empty(self.total_neurons, np.float32)
+        check(lib().sg_stdp_traces(self._h, _p(a), _p(b)))
+        return a, b
+
+    @property
+    def stream(self) -> int:
+        out = C.c_void_p()
+        check(lib().sg_stream(self._h, C.byref(out)))
+        return out.value or 0

@@ -1,0 +1,201 @@
+"""Seeded synthetic workloads (the benchmark configurations).
+
+Every random number comes from a counter-based SplitMix64 hash, so the same
+seed gives the same network on any machine and in any build order; the
+arrays produced here feed both the GPU ``Network`` and, in tests, the CPU
+oracle (which exposes the same builder method names).
+
+* ``izhikevich_pulse`` — the plain Izhikevich pulse-coupled network: N=1000,
+  800 excitatory (a=0.02, b=0.2, c=-65+15r^2, d=8-6r^2) and 200 inhibitory
+  (a=0.02+0.08r, b=0.25-0.05r, c=-65, d=2), 100 distinct random targets per
+  neuron without self-loops, weights 0.5U (exc) / -U (inh), delay 1, dt=1 ms
+  as two 0.5 ms half-steps, thalamic input 5N(0,1) / 2N(0,1) per step fed by
+  inject_current, v0=-65, u0=b*v0, seed 0.
+* ``lif_balanced`` — the balanced current-based LIF network: N neurons (80 %
+  excitatory), tau_m=20 ms, V_th=20 mV, V_reset=10 mV, refractory 2 ms,
+  dt=0.1 ms, fixed in-degree K with uniformly drawn presynaptic sources,
+  weights J / -gJ (g=5), delays uniform in 1..20 steps, one Poisson source
+  per neuron.  The reference LIF integrates dv = (v_rest - v + I)*dt/tau, so
+  a PSP of J mV needs a ring weight of J*tau/dt: J=0.1 mV -> 20, -gJ -> -100.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PHI = np.uint64(0x9E3779B97F4A7C15)
+M1 = np.uint64(0xBF58476D1CE4E5B9)
+M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(z):
+    """Vectorised SplitMix64 finaliser (uint64 in, uint64 out)."""
+    z = np.asarray(z, np.uint64)
+    with np.errstate(over="ignore"):
+        z = z + PHI
+        z = (z ^ (z >> np.uint64(30))) * M1
+        z = (z ^ (z >> np.uint64(27))) * M2
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform01(seed: int, stream: int, counter) -> np.ndarray:
+    """U[0,1) doubles for (seed, stream, counter) with 53 random bits."""
+    c = np.asarray(counter, np.uint64)
+    with np.errstate(over="ignore"):
+        key = (np.uint64(seed) * PHI) ^ (np.uint64(stream) << np.uint64(40)) ^ c
+    h = splitmix64(splitmix64(key))
+    return (h >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def std_normal(seed: int, stream: int, counter) -> np.ndarray:
+    """Box-Muller N(0,1) in FP64 from two uniform draws per value."""
+    c = np.asarray(counter, np.uint64)
+    u1 = 1.0 - uniform01(seed, stream, c * np.uint64(2))  # (0, 1]
+    u2 = uniform01(seed, stream, c * np.uint64(2) + np.uint64(1))
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+
+
+# ---------------------------------------------------------------------------
+# Izhikevich pulse-coupled network
+# ---------------------------------------------------------------------------
+IZH_STREAM_R, IZH_STREAM_TARGETS, IZH_STREAM_W, IZH_STREAM_NOISE = 1, 2, 3, 4
+
+
+def izhikevich_pulse(n: int = 1000, n_exc: int | None = None, k_out: int = 100,
+                     steps: int = 1000, seed: int = 0, noise: bool = True) -> dict:
+    if n_exc is None:
+        n_exc = n * 4 // 5
+    idx = np.arange(n, dtype=np.uint64)
+    r = uniform01(seed, IZH_STREAM_R, idx)
+    exc = np.arange(n) < n_exc
+    a = np.where(exc, 0.02, 0.02 + 0.08 * r).astype(np.float32)
+    b = np.where(exc, 0.2, 0.25 - 0.05 * r).astype(np.float32)
+    c = np.where(exc, -65.0 + 15.0 * r * r, -65.0).astype(np.float32)
+    d = np.where(exc, 8.0 - 6.0 * r * r, 2.0).astype(np.float32)
+    v0 = np.full(n, -65.0, np.float32)
+    u0 = (b * v0).astype(np.float32)
+    # 100 distinct targets per pre, no self-loop: partial Fisher-Yates over the
+    # other n-1 neurons driven by the hash stream of that pre.
+    k = min(k_out, n - 1)
+    pre = np.repeat(np.arange(n, dtype=np.uint32), k)
+    post = np.empty(n * k, np.uint32)
+    for i in range(n):
+        pool = np.concatenate([np.arange(0, i), np.arange(i + 1, n)]).astype(np.uint32)
+        u = uniform01(seed, IZH_STREAM_TARGETS, np.arange(k, dtype=np.uint64) + np.uint64(i * k))
+        m = pool.size
+        for j in range(k):
+            s = j + int(u[j] * (m - j))
+            pool[j], pool[s] = pool[s], pool[j]
+        post[i * k:(i + 1) * k] = pool[:k]
+    uw = uniform01(seed, IZH_STREAM_W, np.arange(n * k, dtype=np.uint64))
+    w = np.where(exc[pre], 0.5 * uw, -uw).astype(np.float32)
+    delay = np.ones(n * k, np.uint8)
+    spec = dict(n=n, n_exc=n_exc, a=a, b=b, c=c, d=d, v0=v0, u0=u0, pre=pre, post=post, w=w,
+                delay=delay, steps=steps, seed=seed, noise=noise)
+    return spec
+
+
+def izhikevich_input(spec: dict, step: int) -> np.ndarray:
+    """Thalamic input of one step: 5N(0,1) excitatory, 2N(0,1) inhibitory (f32)."""
+    n = spec["n"]
+    if not spec["noise"]:
+        return np.zeros(n, np.float32)
+    ctr = np.arange(n, dtype=np.uint64) + np.uint64(step) * np.uint64(n)
+    z = std_normal(spec["seed"], IZH_STREAM_NOISE, ctr)
+    scale = np.where(np.arange(n) < spec["n_exc"], 5.0, 2.0)
+    return (scale * z).astype(np.float32)
+
+
+def build_izhikevich(net, spec: dict, model_izh: int = 2) -> int:
+    """Apply the spec through the reference builder API; returns the population."""
+    n = spec["n"]
+    pop = net.add_population(model_izh, n)
+    net.fill_param(pop, 0, 1.0)   # dt
+    net.set_param(pop, 1, spec["a"])
+    net.set_param(pop, 2, spec["b"])
+    net.set_param(pop, 3, spec["c"])
+    net.set_param(pop, 4, spec["d"])
+    net.fill_param(pop, 5, 0.0)   # tau_ref: none
+    net.fill_param(pop, 6, 30.0)  # v_thresh
+    net.set_state(pop, 0, spec["v0"])
+    net.set_state(pop, 1, spec["u0"])
+    net.connect(pop, spec["pre"], pop, spec["post"], spec["w"], spec["delay"])
+    net.build()
+    return pop
+
+
+def run_izhikevich(net, pop: int, spec: dict, steps: int | None = None, start: int = 0):
+    """Drive the network step by step (inject then step); returns spike counts per step."""
+    n = spec["n"]
+    idx = np.arange(n, dtype=np.uint32)
+    steps = spec["steps"] if steps is None else steps
+    for t in range(start, start + steps):
+        net.inject_current(pop, idx, izhikevich_input(spec, t))
+        net.step(1)
+
+
+# ---------------------------------------------------------------------------
+# balanced LIF network
+# ---------------------------------------------------------------------------
+LIF_STREAM_V0 = 5
+
+
+def fixed_indegree_edges(n_from: int, n_post: int, k_in: int, seed: int, n_exc: int,
+                         w_exc: float, w_inh: float, d_min: int, d_max: int,
+                         from_off: int = 0, to_off: int = 0):
+    """numpy restatement of the device generator of sg_connect_fixed_indegree
+    (edge t = (post j, draw q) = j*k_in + q, in that order)."""
+    t = np.arange(n_post * k_in, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        h = splitmix64(np.uint64(seed) ^ (t * PHI))
+    src = (((h >> np.uint64(32)) * np.uint64(n_from)) >> np.uint64(32)).astype(np.uint32)
+    span = np.uint64(d_max - d_min + 1)
+    d = (np.uint64(d_min) + (h & np.uint64(0xFFFFFFFF)) % span).astype(np.uint8)
+    post = (t // np.uint64(k_in)).astype(np.uint32)
+    exc = src < n_exc
+    w = np.where(exc, np.float32(w_exc), np.float32(w_inh)).astype(np.float32)
+    return src + np.uint32(from_off), post + np.uint32(to_off), w, d
+
+
+def lif_balanced(n: int = 1_000_000, k_in: int = 1000, seed: int = 1, ext_rate_hz: float = 2000.0,
+                 ext_weight: float = 20.0, w_exc: float = 20.0, g: float = 5.0,
+                 d_min: int = 1, d_max: int = 20) -> dict:
+    """The balanced LIF network; the literal configuration is the default
+    (external Poisson 2000 Hz with weight J)."""
+    n_exc = n * 4 // 5
+    v0 = (10.0 + 10.0 * uniform01(seed, LIF_STREAM_V0, np.arange(n, dtype=np.uint64))).astype(np.float32)
+    return dict(n=n, n_exc=n_exc, k_in=k_in, seed=seed, ext_rate_hz=ext_rate_hz,
+                ext_weight=ext_weight, w_exc=w_exc, w_inh=-g * w_exc, d_min=d_min, d_max=d_max,
+                dt=0.1, v0=v0)
+
+
+LIF_PARAMS = (0.1, 0.05, 0.0, 20.0, 10.0, 2.0)  # dt inv_tau v_rest v_th v_reset tau_ref
+
+
+def build_lif(net, spec: dict, model_lif: int = 1, device_generator: bool = True) -> int:
+    """Apply the LIF spec; the GPU network generates its synapses on the
+    device, the oracle receives the identical numpy-generated edge list."""
+    n = spec["n"]
+    pop = net.add_population(model_lif, n)
+    for col, v in enumerate(LIF_PARAMS):
+        net.fill_param(pop, col, v)
+    net.set_state(pop, 0, spec["v0"])
+    if device_generator:
+        net.connect_fixed_indegree(pop, pop, spec["k_in"], spec["seed"], spec["n_exc"],
+                                   spec["w_exc"], spec["w_inh"], spec["d_min"], spec["d_max"])
+    else:
+        pre, post, w, d = fixed_indegree_edges(n, n, spec["k_in"], spec["seed"], spec["n_exc"],
+                                               spec["w_exc"], spec["w_inh"], spec["d_min"],
+                                               spec["d_max"])
+        net.connect(pop, pre, pop, post, w, d)
+    # one Poisson source per neuron, seed = neuron index, delay 1
+    if hasattr(net, "add_poisson_sources"):
+        first = net.add_poisson_sources(n, spec["ext_rate_hz"], spec["dt"], seed0=0)
+        net.connect_poisson_one_to_one(first, n, pop, spec["ext_weight"], 1)
+    else:
+        ones_w = np.array([spec["ext_weight"]], np.float32)
+        one_d = np.array([1], np.uint8)
+        for i in range(n):
+            s = net.add_poisson_source(spec["ext_rate_hz"], spec["dt"], i)
+            net.connect_poisson_source(s, pop, np.array([i], np.uint32), ones_w, one_d)
+    return pop

@@ -1,0 +1,176 @@
+/*
+ * simuse_b200.h — C ABI of the B200-native SiMuse simulation step.
+ *
+ * A drop-in for the reference's `pillars::api::Network` builder/step API
+ * (crates/SiMuse/crates/pillars/src/api/net/network/core.rs:87-622,
+ * build.rs:18-276, step.rs:18-189).  The ABI is Rust-callable by design:
+ * opaque handle, plain pointers and sizes, int status codes, no C++ or torch
+ * types.  Each entry point names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns SG_OK (0) or a negative SG_E_* code; the message
+ *    is available from sg_last_error() (thread-local), as the Unity bridge
+ *    does (src/unity_bridge.rs:8-64).  Nothing aborts the process: the
+ *    reference's assert!/panic! contract violations become SG_E_INVALID.
+ *  - Host pointers are read during the call only; the caller keeps
+ *    ownership.  Readbacks copy into caller-provided buffers (as
+ *    CompiledNetwork::download_* does, pillars-cuda/src/network.rs:471-491).
+ *  - One handle owns one CUDA stream on one device.  Calls on different
+ *    handles are thread-safe; calls on one handle must be serialised by the
+ *    caller.
+ *  - Indices are the reference's: population ids in creation order, neuron
+ *    indices within a population, global neuron index = population offset +
+ *    index (core.rs:236-239).
+ */
+#ifndef SIMUSE_B200_H
+#define SIMUSE_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_ABI_VERSION 1
+
+enum sg_status {
+  SG_OK = 0,
+  SG_E_INVALID = -1,  /* contract violation (reference: assert!/panic!) */
+  SG_E_STATE = -2,    /* wrong lifecycle stage (e.g. connect after build) */
+  SG_E_CUDA = -3,     /* CUDA runtime error */
+  SG_E_NOMEM = -4,    /* device allocation failed or over budget */
+  SG_E_OVERFLOW = -5, /* a fixed-capacity device buffer would overflow */
+  SG_E_TIMEOUT = -6   /* a bounded device wait gave up */
+};
+
+/* Neuron models (reference: pillars::zoo::neurons::*). */
+enum sg_model {
+  SG_LIF = 1,  /* LIFModel, P/zoo/neurons/lif.rs:22-78; params dt inv_tau_m v_rest v_thresh v_reset tau_ref; state v refr */
+  SG_IZH = 2,  /* IzhikevichModel, P/zoo/neurons/izhikevich.rs:42-125; params dt a b c d tau_ref v_thresh; state v u refr */
+  SG_GPEA = 3, /* GpeaModel, P/zoo/neurons/gpea.rs:211-360; 14 params, 9 states */
+  SG_HH = 4    /* Hodgkin-Huxley, RK4 (no reference: P/zoo/neurons/hh.rs is a stub);
+                  params dt c_m g_na g_k g_l e_na e_k e_l i_bias v_thresh; state v m h n */
+};
+
+/* Edge flags for sg_connect_ex. */
+#define SG_EDGE_STDP 1u /* the synapse takes part in pair STDP */
+
+/* Weight storage precision (scatter bytes), sg_set_weight_format. */
+enum sg_weight_format { SG_W_F32 = 0, SG_W_BF16 = 1, SG_W_FP8 = 2 };
+
+typedef struct sg_net sg_net;
+
+/* ---- library ---------------------------------------------------------- */
+int sg_abi_version(void);                       /* src/unity_bridge.rs:207-241 (*_abi_version) */
+int sg_last_error(char *buf, size_t len);       /* src/unity_bridge.rs:58-64 (last_error) */
+int sg_device_count(int *out);
+
+/* ---- Network lifecycle ------------------------------------------------ */
+int sg_net_create(sg_net **out, int device);    /* Network::new, core.rs:87-113 */
+int sg_net_destroy(sg_net *net);                /* Drop for Network */
+int sg_synchronize(sg_net *net);
+
+/* ---- builder (before sg_build) ---------------------------------------- */
+/* Network::add_population::<M>(n) -> PopulationId, core.rs:149-155 */
+int sg_pop_add(sg_net *net, int model, uint32_t n, uint32_t *out_pop);
+/* NeuralPopulation::fill_param / fill_state, P/core/exec/population.rs:166-197 */
+int sg_pop_fill_param(sg_net *net, uint32_t pop, uint32_t col, float value);
+int sg_pop_fill_state(sg_net *net, uint32_t pop, uint32_t col, float value);
+/* param_slice_mut / state_slice_mut then a copy, population.rs:209-220 (any time) */
+int sg_pop_set_param(sg_net *net, uint32_t pop, uint32_t col, const float *vals, uint32_t n);
+int sg_pop_set_state(sg_net *net, uint32_t pop, uint32_t col, const float *vals, uint32_t n);
+/* Network::state(pop, col) / param_slice(pop, col), build.rs:155-182 */
+int sg_pop_get_state(sg_net *net, uint32_t pop, uint32_t col, float *out, uint32_t n);
+int sg_pop_get_param(sg_net *net, uint32_t pop, uint32_t col, float *out, uint32_t n);
+
+/* Network::connect(from, &[u32], to, &[u32], &[f32], &[u8]), core.rs:166-249 */
+int sg_connect(sg_net *net, uint32_t from, const uint32_t *from_idx, uint32_t to,
+               const uint32_t *to_idx, const float *weights, const uint8_t *delays, uint64_t n);
+/* connect_edges with per-edge syn_type (0 static, k = kinetic profile k) and
+   flags (SG_EDGE_STDP), core.rs:254-279; syn_types may be NULL. */
+int sg_connect_ex(sg_net *net, uint32_t from, const uint32_t *from_idx, uint32_t to,
+                  const uint32_t *to_idx, const float *weights, const uint8_t *delays,
+                  const uint8_t *syn_types, uint64_t n, uint32_t flags);
+/* Seeded synthetic projection generated on the device: every post of `to`
+   receives exactly `k_in` synapses from pres drawn uniformly (with
+   replacement) from `from`; weight w_exc for pre index < n_exc else w_inh;
+   delay uniform in [d_min, d_max].  Edge (post j, draw q) uses
+   h = splitmix64(seed ^ (j*k_in + q)*0x9E3779B97F4A7C15), pre = (h>>32)*n_from>>32,
+   delay = d_min + (h & 0xffffffff) % (d_max-d_min+1); edges are appended in
+   (post, draw) order. */
+int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k_in,
+                              uint64_t seed, uint32_t n_exc, float w_exc, float w_inh,
+                              uint8_t d_min, uint8_t d_max, uint8_t syn_type_exc,
+                              uint8_t syn_type_inh, uint32_t flags_exc);
+
+/* Network::register_kinetics(SynapseKinetics::ExpOne{tau_decay, erev}, dt)
+   -> profile id (1-based), core.rs:564-584; step.rs:248-345 */
+int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id);
+
+/* Network::add_poisson_source(rate_hz, dt_ms, seed) -> id, core.rs:288-312 */
+int sg_poisson_add(sg_net *net, float rate_hz, float dt_ms, uint32_t seed, uint32_t *out_id);
+/* n sources at once with seeds[i] (or seed0 + i when seeds == NULL); ids are consecutive */
+int sg_poisson_add_many(sg_net *net, uint32_t n, float rate_hz, float dt_ms,
+                        const uint32_t *seeds, uint32_t seed0, uint32_t *out_first_id);
+/* Network::connect_poisson_source(src, to, posts, w, d, st, pt), core.rs:323-381 */
+int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts,
+                       const float *weights, const uint8_t *delays, const uint8_t *syn_types,
+                       uint64_t n);
+/* Source first_src + i gets one synapse to post posts[i] (posts == NULL:
+   post i), weight w, delay d: the "one source per neuron" drive. */
+int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first_src, uint32_t n, uint32_t to,
+                                  const uint32_t *posts, float weight, uint8_t delay);
+
+/* Pair STDP on edges flagged SG_EDGE_STDP (no reference function; the trace
+   arithmetic follows P/api/learn/brain.rs:204-222). */
+int sg_stdp_config(sg_net *net, float dt, float tau_pre, float tau_post, float a_plus,
+                   float a_minus, float w_min, float w_max);
+
+/* Weight storage format for the scatter (FP32 default). */
+int sg_set_weight_format(sg_net *net, int format);
+/* Scatter mode: 1 = deterministic (reference summation order, default),
+   0 = atomic accumulation (tolerance mode, order not fixed). */
+int sg_set_deterministic(sg_net *net, int on);
+
+/* Network::build(), build.rs:18-109 (a second call is SG_E_STATE) */
+int sg_build(sg_net *net);
+/* SparseGraph::from_csr + build (graph.rs:217-275): all-static, not plastic */
+int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col,
+                      const float *weights, const uint8_t *delays);
+
+/* ---- run -------------------------------------------------------------- */
+/* Network::inject_current(pop, idx, vals), build.rs:243-275: same-step slot */
+int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals, uint64_t n);
+/* n_steps x Network::step(), step.rs:18-189 (asynchronous; CUDA-graph replay) */
+int sg_step(sg_net *net, uint32_t n_steps);
+/* Spike raster: keep the last `capacity_steps` steps as bitmasks (0 disables). */
+int sg_raster_enable(sg_net *net, uint32_t capacity_steps);
+/* Copy the spike raster of the steps recorded since the last read into
+   `out` as bytes [n_steps][total_neurons]; returns the step count in *n_steps. */
+int sg_raster_read(sg_net *net, uint8_t *out, uint64_t cap_bytes, uint32_t *n_steps);
+/* Per-step counters since the last read: spikes and synaptic events. */
+int sg_stats_read(sg_net *net, uint32_t *spikes, uint64_t *events, uint32_t cap, uint32_t *n_steps);
+
+/* ---- readback --------------------------------------------------------- */
+int sg_spikes(sg_net *net, uint32_t pop, int32_t *out, uint32_t n); /* build.rs:145-152 */
+int sg_step_counter(sg_net *net, uint64_t *out);                    /* build.rs:136-140 */
+int sg_total_neurons(sg_net *net, uint64_t *out);                   /* build.rs:130-134 */
+int sg_num_synapses(sg_net *net, uint64_t *out);                    /* graph.rs:285-287 */
+int sg_events_total(sg_net *net, uint64_t *out);
+/* Network::graph() -> SparseGraph CSR arrays, build.rs:186-188 */
+int sg_graph_read(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *weights, uint8_t *delays);
+int sg_weights_read(sg_net *net, float *weights); /* current CSR weights (STDP) */
+/* DelayBuffer contents [32][total_neurons] of ring 0 (static) or kinetic k */
+int sg_ring_read(sg_net *net, uint32_t ring, float *out);
+int sg_stdp_drift(sg_net *net, double *out);
+int sg_stdp_traces(sg_net *net, float *x_pre, float *x_post);
+int sg_clamp_hits(sg_net *net, uint64_t *out); /* i_syn values that hit the +-100 clamp */
+/* Device bytes held by this network (state + CSR + rings + scratch). */
+int sg_footprint(sg_net *net, uint64_t *out);
+/* Device stream of the handle (cudaStream_t), for event timing. */
+int sg_stream(sg_net *net, void **out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

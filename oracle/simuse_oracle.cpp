@@ -1,0 +1,1098 @@
+// simuse_oracle.cpp — CPU oracle: a plain C++ restatement of the reference's
+// SiMuse simulation step.  TEST INFRASTRUCTURE ONLY (see simuse_oracle.h).
+//
+// Every function cites the reference file:line it restates, paths relative
+// to crates/SiMuse/crates/ (P/ = pillars/src/).  FP32 arithmetic follows the
+// reference operation by operation: left-to-right evaluation, no FMA
+// contraction (Rust never contracts; this file is built with
+// -ffp-contract=off), and explicit fused multiply-add exactly where the
+// reference calls mul_add.  Where the reference has no implementation
+// (HH with RK4, pair STDP with immediate weight updates, Kuramoto with RK4)
+// the formulas here define the behaviour; a templated FP64 twin of every
+// model runs the same formulas in double precision.
+#include "simuse_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <thread>
+
+namespace {
+
+thread_local std::string g_err;
+int fail(const std::string &m) {
+  g_err = m;
+  return -1;
+}
+
+constexpr uint32_t kSlots = 32;  // P/api/net/graph.rs:33 MAX_DELAY_SLOTS
+
+enum Model { LIF = 1, IZH = 2, GPEA = 3, HH = 4 };
+int n_params_of(int m) {
+  switch (m) {
+    case LIF: return 6;    // P/zoo/neurons/lif.rs:28-39
+    case IZH: return 7;    // P/zoo/neurons/izhikevich.rs:50-63
+    case GPEA: return 14;  // P/zoo/neurons/gpea.rs:231-258
+    case HH: return 10;    // dt c_m g_na g_k g_l e_na e_k e_l i_bias v_thresh
+  }
+  return -1;
+}
+int n_state_of(int m) {
+  switch (m) {
+    case LIF: return 2;
+    case IZH: return 3;
+    case GPEA: return 9;
+    case HH: return 4;  // v m h n
+  }
+  return -1;
+}
+bool clamps_input(int m) {
+  // P/core/exec/population.rs:69-86: CLAMP_I_SYN defaults to true; GPEA is
+  // #[no_clamp] (P/zoo/neurons/gpea.rs:210).  HH here is a conductance model
+  // and is defined without the clamp as well.
+  return m == LIF || m == IZH;
+}
+
+// ---------------------------------------------------------------------------
+// Math
+// ---------------------------------------------------------------------------
+
+// P/math/fast_exp.rs:23-68, the fused (x86_64 + fma) flavour.
+float fast_exp_f(float x) {
+  const float log2e = 1.44269504088896340736f;
+  float t = x * log2e;
+  float tf = std::floor(t);
+  int n;
+  if (std::isnan(tf)) n = 0;
+  else if (tf >= 2147483647.0f) n = 2147483647;
+  else if (tf <= -2147483648.0f) n = (-2147483647 - 1);
+  else n = (int)tf;
+  float f = t - (float)n;
+  const float c1 = 0.693147180559945309417f;
+  const float c2 = 0.2402265f;
+  const float c3 = 0.05550411f;
+  const float c4 = 0.009618129f;
+  const float c5 = 0.001333356f;
+  const float c6 = 0.0001540353f;
+  float poly = std::fma(c6, f, c5);
+  poly = std::fma(poly, f, c4);
+  poly = std::fma(poly, f, c3);
+  poly = std::fma(poly, f, c2);
+  poly = std::fma(poly, f, c1);
+  poly = std::fma(poly, f, 1.0f);
+  if (n < -126) return 0.0f;
+  if (n > 127) return INFINITY;
+  uint32_t bits = (uint32_t)(n + 127) << 23;
+  float s;
+  std::memcpy(&s, &bits, 4);
+  return s * poly;
+}
+
+// Exponential used by the HH model in FP32 (shared definition with the CUDA
+// kernel: Cody-Waite reduction by ln 2 split into a short high part and a
+// low part, degree-7 Taylor polynomial of e^r on |r| <= ln2/2, exponent
+// scaling by bit construction).  Written from the mathematics.
+float sg_expf(float x) {
+  if (x > 88.0f) x = 88.0f;
+  if (x < -87.0f) x = -87.0f;
+  const float log2e = 1.44269504088896340736f;
+  const float ln2_hi = 0.693145751953125f;
+  const float ln2_lo = 1.428606820309417232e-6f;
+  float k = std::nearbyint(x * log2e);
+  float r = std::fma(-k, ln2_hi, x);
+  r = std::fma(-k, ln2_lo, r);
+  float p = 1.0f / 5040.0f;
+  p = std::fma(p, r, 1.0f / 720.0f);
+  p = std::fma(p, r, 1.0f / 120.0f);
+  p = std::fma(p, r, 1.0f / 24.0f);
+  p = std::fma(p, r, 1.0f / 6.0f);
+  p = std::fma(p, r, 0.5f);
+  p = std::fma(p, r, 1.0f);
+  p = std::fma(p, r, 1.0f);
+  int ki = (int)k;
+  // 2^k split in two factors so that k in [-126, 127] never leaves the
+  // normal range of either factor.
+  int k1 = ki / 2, k2 = ki - k1;
+  uint32_t b1 = (uint32_t)(k1 + 127) << 23, b2 = (uint32_t)(k2 + 127) << 23;
+  float s1, s2;
+  std::memcpy(&s1, &b1, 4);
+  std::memcpy(&s2, &b2, 4);
+  return (p * s1) * s2;
+}
+
+template <typename T> struct M;
+template <> struct M<float> {
+  static float fexp(float x) { return fast_exp_f(x); }  // GPEA, STDP decay
+  static float hexp(float x) { return sg_expf(x); }     // HH rates
+  static float ln(float x) { return std::log(x); }
+  static float fma(float a, float b, float c) { return std::fma(a, b, c); }
+};
+template <> struct M<double> {
+  static double fexp(double x) { return std::exp(x); }
+  static double hexp(double x) { return std::exp(x); }
+  static double ln(double x) { return std::log(x); }
+  static double fma(double a, double b, double c) { return std::fma(a, b, c); }
+};
+
+// P/api/net/network/sources.rs:5-14
+bool poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p) {
+  uint64_t z = ((uint64_t)seed << 32) | (uint64_t)stream;
+  z ^= step * 0x9E3779B97F4A7C15ull;
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  float u = (float)(z >> 40) / (float)(1ull << 24);
+  return u < p;
+}
+
+// ---------------------------------------------------------------------------
+// Neuron models (one neuron, SoA accessors)
+// ---------------------------------------------------------------------------
+
+template <typename T> struct Cols {
+  T *s;
+  const T *p;
+  uint32_t cap, i;
+  T &st(int c) const { return s[(size_t)c * cap + i]; }
+  T pr(int c) const { return p[(size_t)c * cap + i]; }
+};
+
+// P/zoo/neurons/lif.rs:47-78
+template <typename T> bool lif_step(const Cols<T> &c, T i_syn, T dt) {
+  const T zero = 0;
+  T v = c.st(0), refr = c.st(1);
+  const T inv_tau = c.pr(1), v_rest = c.pr(2), v_th = c.pr(3), v_reset = c.pr(4),
+          tau_ref = c.pr(5);
+  bool is_refr = refr > zero;
+  T dv = ((v_rest - v) + i_syn) * inv_tau * dt;
+  T v_new = v + dv;
+  bool spike = is_refr ? false : (v_new >= v_th);
+  T v_final = spike ? v_reset : v_new;
+  c.st(0) = is_refr ? v : v_final;
+  T refr_dec = refr - dt;
+  T refr_set = spike ? tau_ref : refr_dec;
+  c.st(1) = std::fmax(refr_set, zero);
+  return spike;
+}
+
+// P/zoo/neurons/izhikevich.rs:71-125
+template <typename T> bool izh_step(const Cols<T> &c, T i_syn, T dt) {
+  const T zero = 0;
+  T vs = c.st(0), u = c.st(1), refr = c.st(2);
+  const T a = c.pr(1), b = c.pr(2), cc = c.pr(3), d = c.pr(4), tau_ref = c.pr(5),
+          v_th = c.pr(6);
+  bool is_refr = refr > zero;
+  T v = is_refr ? cc : vs;
+  T half_dt = dt * (T)0.5;
+  const T c04 = (T)0.04f, c5 = 5, c140 = 140;
+  T v_poly1 = v * (c04 * v + c5);
+  T dv1 = (v_poly1 + c140 - u + i_syn) * half_dt;
+  T v_mid = v + dv1;
+  T v_poly2 = v_mid * (c04 * v_mid + c5);
+  T dv2 = (v_poly2 + c140 - u + i_syn) * half_dt;
+  T dv_total = is_refr ? zero : dv1 + dv2;
+  T v_new = v + dv_total;
+  T du = a * (b * v - u) * dt;
+  T u_new = is_refr ? u : u + du;
+  bool spike = v_new >= v_th;
+  c.st(0) = spike ? cc : v_new;
+  c.st(1) = spike ? u_new + d : u_new;
+  T refr_dec = refr - dt;
+  T refr_set = spike ? tau_ref : refr_dec;
+  c.st(2) = std::fmax(refr_set, zero);
+  return spike;
+}
+
+// P/zoo/neurons/gpea.rs:53-123 constants, :129-179 helpers, :266-360 step.
+namespace gp {
+constexpr float NA_TH_M = -38.0f, NA_TH_H = -45.5f, NA_K_M = -7.0f, NA_K_H = 6.4f;
+constexpr float NA_TAU_M0 = 0.001f, NA_TAU_M1 = 0.1f, NA_THT_M = -53.0f, NA_SIG_M = -0.7f;
+constexpr float NA_TAU_H0 = 0.0f, NA_TAU_H1 = 4.5f, NA_THT_H1 = -50.0f, NA_SIG_H1 = -15.0f;
+constexpr float NA_THT_H2 = -50.0f, NA_SIG_H2 = 16.0f;
+constexpr float K_TH_N = -42.0f, K_K_N = -14.0f, K_TAU_N0 = 0.0f, K_TAU_N1 = 2.4f;
+constexpr float K_THT_N1 = -40.0f, K_SIG_N1 = -40.0f, K_THT_N2 = -40.0f, K_SIG_N2 = 50.0f;
+constexpr float CAT_TH_P = -56.0f, CAT_TH_Q = -85.0f, CAT_K_P = -6.7f, CAT_K_Q = 5.8f;
+constexpr float CAT_TAU_P0 = 5.0f, CAT_TAU_P1 = 0.33f, CAT_TAU_Q0 = 0.0f, CAT_TAU_Q1 = 400.0f;
+constexpr float CAT_THT_P1 = -27.0f, CAT_SIG_P1 = -10.0f, CAT_THT_P2 = -102.0f, CAT_SIG_P2 = 15.0f;
+constexpr float CAT_THT_Q1 = -50.0f, CAT_SIG_Q1 = -15.0f, CAT_THT_Q2 = -50.0f, CAT_SIG_Q2 = 16.0f;
+constexpr float AHP_TH_R = 0.17e-3f, AHP_K_R = -0.08e-3f, AHP_TAU_R = 2.0f;
+constexpr float CA_FARADAY = 96485.0f;
+constexpr float NA_NAI = 10.0f, NA_NAO = 140.0f, K_KI = 140.0f, K_KO = 5.0f, CA_CAO = 2.0f;
+constexpr float GAS_R = 8.31441f;
+}  // namespace gp
+
+template <typename T> T g_sigmoid(T x, float th, float k) {
+  return (T)1 / ((T)1 + M<T>::fexp((x - (T)th) * (T)(1.0f / k)));
+}
+template <typename T> T g_exp_euler(T x, T x_inf, T tau, T dt) {
+  T decay = M<T>::fexp(-dt / tau);
+  return M<T>::fma(decay, x - x_inf, x_inf);
+}
+template <typename T> T g_tau2(T v, float t0, float t1, float th1, float s1, float th2, float s2) {
+  T e1 = M<T>::fexp((v - (T)th1) * (T)(-1.0f / s1));
+  T e2 = M<T>::fexp((-(v - (T)th2)) * (T)(1.0f / s2));
+  return (T)t0 + (T)t1 / (e1 + e2);
+}
+
+template <typename T> bool gpea_step(const Cols<T> &c, T i_syn, T dt) {
+  using namespace gp;
+  T celsius = c.pr(1), inv_cm = c.pr(2), v_thresh = c.pr(3), area = c.pr(4), gnabar = c.pr(5),
+    gkdrbar = c.pr(6), gl = c.pr(7), el = c.pr(8), gcatbar = c.pr(9), gkcabar = c.pr(10),
+    kca = c.pr(11), vol = c.pr(12), caGain = c.pr(13);
+  T rt = (T)GAS_R * ((T)273.0f + celsius - (T)9.5f) / (T)CA_FARADAY * (T)1000.0f;
+  T ena = -rt * M<T>::ln((T)NA_NAI / (T)NA_NAO);
+  T ek = rt * M<T>::ln((T)K_KO / (T)K_KI);
+  T v = c.st(0), m = c.st(1), h = c.st(2), n = c.st(3), p = c.st(4), q = c.st(5), cai = c.st(6),
+    r = c.st(7), was_below = c.st(8);
+
+  T m_inf = g_sigmoid(v, NA_TH_M, NA_K_M);
+  T m_tau;
+  {
+    T denom = (T)1 + M<T>::fexp((v - (T)NA_THT_M) * (T)(-1.0f / NA_SIG_M));
+    m_tau = (T)NA_TAU_M0 + (T)NA_TAU_M1 / denom;
+  }
+  T m_new = g_exp_euler(m, m_inf, m_tau, dt);
+  T h_inf = g_sigmoid(v, NA_TH_H, NA_K_H);
+  T h_tau = g_tau2(v, NA_TAU_H0, NA_TAU_H1, NA_THT_H1, NA_SIG_H1, NA_THT_H2, NA_SIG_H2);
+  T h_new = g_exp_euler(h, h_inf, h_tau, dt);
+  T n_inf = g_sigmoid(v, K_TH_N, K_K_N);
+  T n_tau = g_tau2(v, K_TAU_N0, K_TAU_N1, K_THT_N1, K_SIG_N1, K_THT_N2, K_SIG_N2);
+  T n_new = g_exp_euler(n, n_inf, n_tau, dt);
+  T p_inf = g_sigmoid(v, CAT_TH_P, CAT_K_P);
+  T p_tau = g_tau2(v, CAT_TAU_P0, CAT_TAU_P1, CAT_THT_P1, CAT_SIG_P1, CAT_THT_P2, CAT_SIG_P2);
+  T p_new = g_exp_euler(p, p_inf, p_tau, dt);
+  T q_inf = g_sigmoid(v, CAT_TH_Q, CAT_K_Q);
+  T q_tau = g_tau2(v, CAT_TAU_Q0, CAT_TAU_Q1, CAT_THT_Q1, CAT_SIG_Q1, CAT_THT_Q2, CAT_SIG_Q2);
+  T q_new = g_exp_euler(q, q_inf, q_tau, dt);
+  T r_inf = g_sigmoid(cai, AHP_TH_R, AHP_K_R);
+  T r_new = g_exp_euler(r, r_inf, (T)AHP_TAU_R, dt);
+
+  T eca_old = -rt * M<T>::ln(cai / (T)CA_CAO) / (T)2.0f;
+  T gcat_old = gcatbar * p * p * q;
+  T ica_old = gcat_old * (v - eca_old);
+  T j = -ica_old * area * (T)1e-14f / ((T)2.0f * (T)CA_FARADAY * vol);
+  T k_ca = caGain * kca;
+  T cai_decay = M<T>::fexp(-dt * k_ca);
+  T cai_new = cai + ((T)1 - cai_decay) * (caGain * j / k_ca - cai);
+  T eca = -rt * M<T>::ln(cai_new / (T)CA_CAO) / (T)2.0f;
+
+  T g_na = gnabar * (m_new * m_new * m_new) * h_new;
+  T n2 = n_new * n_new;
+  T g_k = gkdrbar * (n2 * n2);
+  T g_cat = gcatbar * p_new * p_new * q_new;
+  T g_ahp = gkcabar * r_new * r_new;
+  T g_leak = gl;
+  T g_sum = g_na + g_k + g_cat + g_ahp + g_leak;
+  T g_e_sum = g_na * ena + (g_k + g_ahp) * ek + g_cat * eca + g_leak * el;
+  T c_over_dt = (T)1 / (inv_cm * dt);
+  T v_new = (c_over_dt * v + i_syn + g_e_sum) / (c_over_dt + g_sum);
+  bool is_above = v_new >= v_thresh;
+  bool spike = is_above && (was_below > (T)0);  // P/ops/spike.rs:70-74
+  c.st(0) = v_new;
+  c.st(1) = m_new;
+  c.st(2) = h_new;
+  c.st(3) = n_new;
+  c.st(4) = p_new;
+  c.st(5) = q_new;
+  c.st(6) = cai_new;
+  c.st(7) = r_new;
+  c.st(8) = is_above ? (T)0 : (T)1;
+  return spike;
+}
+
+// Hodgkin-Huxley with classic RK4 over (V, m, h, n).  The reference's HH
+// model is a stub (P/zoo/neurons/hh.rs:1-43); the rate functions follow the
+// reference CUDA kernel's vtrap form (pillars-cuda/kernels/hh.cu:40-63).
+// The synaptic current i_syn is held fixed over the step (the reference
+// computes conductance currents from V at the start of the step,
+// P/api/net/network/step.rs:36-70).
+template <typename T> T hh_vtrap(T x, T y) {
+  T r = x / y;
+  if (std::fabs(r) < (T)1e-6f) return y - x * (T)0.5f;
+  return x / (M<T>::hexp(r) - (T)1);
+}
+template <typename T> struct HHp { T c_m, g_na, g_k, g_l, e_na, e_k, e_l, i_ext; };
+template <typename T>
+void hh_deriv(const HHp<T> &P, T v, T m, T h, T n, T &dv, T &dm, T &dh, T &dn) {
+  T am = (T)0.1f * hh_vtrap(-(v + (T)40), (T)10);
+  T bm = (T)4 * M<T>::hexp(-(v + (T)65) / (T)18);
+  T ah = (T)0.07f * M<T>::hexp(-(v + (T)65) / (T)20);
+  T bh = (T)1 / ((T)1 + M<T>::hexp(-(v + (T)35) / (T)10));
+  T an = (T)0.01f * hh_vtrap(-(v + (T)55), (T)10);
+  T bn = (T)0.125f * M<T>::hexp(-(v + (T)65) / (T)80);
+  T n2 = n * n;
+  T i_na = P.g_na * (m * m * m) * h * (v - P.e_na);
+  T i_k = P.g_k * (n2 * n2) * (v - P.e_k);
+  T i_l = P.g_l * (v - P.e_l);
+  dv = (P.i_ext - ((i_na + i_k) + i_l)) / P.c_m;
+  dm = am * ((T)1 - m) - bm * m;
+  dh = ah * ((T)1 - h) - bh * h;
+  dn = an * ((T)1 - n) - bn * n;
+}
+template <typename T> bool hh_step(const Cols<T> &c, T i_syn, T dt) {
+  HHp<T> P{c.pr(1), c.pr(2), c.pr(3), c.pr(4), c.pr(5), c.pr(6), c.pr(7), c.pr(8) + i_syn};
+  T v_th = c.pr(9);
+  T v = c.st(0), m = c.st(1), h = c.st(2), n = c.st(3);
+  T hdt = dt * (T)0.5f;
+  T k1v, k1m, k1h, k1n, k2v, k2m, k2h, k2n, k3v, k3m, k3h, k3n, k4v, k4m, k4h, k4n;
+  hh_deriv(P, v, m, h, n, k1v, k1m, k1h, k1n);
+  hh_deriv(P, v + hdt * k1v, m + hdt * k1m, h + hdt * k1h, n + hdt * k1n, k2v, k2m, k2h, k2n);
+  hh_deriv(P, v + hdt * k2v, m + hdt * k2m, h + hdt * k2h, n + hdt * k2n, k3v, k3m, k3h, k3n);
+  hh_deriv(P, v + dt * k3v, m + dt * k3m, h + dt * k3h, n + dt * k3n, k4v, k4m, k4h, k4n);
+  T w = dt / (T)6;
+  T v_new = v + w * (((k1v + (T)2 * k2v) + (T)2 * k3v) + k4v);
+  c.st(0) = v_new;
+  c.st(1) = m + w * (((k1m + (T)2 * k2m) + (T)2 * k3m) + k4m);
+  c.st(2) = h + w * (((k1h + (T)2 * k2h) + (T)2 * k3h) + k4h);
+  c.st(3) = n + w * (((k1n + (T)2 * k2n) + (T)2 * k3n) + k4n);
+  return v < v_th && v_new >= v_th;
+}
+
+// ---------------------------------------------------------------------------
+// Network
+// ---------------------------------------------------------------------------
+
+template <typename T> struct Pop {
+  int model;
+  uint32_t n, cap, np, ns;
+  std::vector<T> params, state;  // SoA [col][cap], P/core/exec/population.rs:106-127
+};
+
+struct EdgeIn {
+  uint32_t pre, post;
+  float w;
+  uint8_t d, st, flags;
+};
+
+struct Kin {
+  float a_decay, erev;  // P/api/net/network/step.rs:248-302 (ExpOne)
+};
+
+template <typename T> struct Src {
+  float p;
+  uint32_t seed;
+  std::vector<uint32_t> post;
+  std::vector<T> w;
+  std::vector<uint8_t> d, st;
+};
+
+struct Stdp {
+  bool on = false;
+  float dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max;
+};
+
+struct NetBase {
+  virtual ~NetBase() {}
+};
+
+template <typename T> struct Net : NetBase {
+  std::vector<Pop<T>> pops;
+  std::vector<uint32_t> offsets{0};
+  uint64_t total = 0;
+  bool built = false;
+  std::vector<EdgeIn> edges;
+  std::vector<uint32_t> row_ptr, col;
+  std::vector<T> w;
+  std::vector<uint8_t> d, st, plastic;
+  std::vector<Kin> kin;
+  std::vector<T> g;     // [nk][N] kinetic conductances
+  std::vector<T> ring;  // [1 + nk][32][N]
+  std::vector<Src<T>> srcs;
+  uint64_t step = 0, events = 0;
+  std::vector<T> i_in, v_scr, scratch;
+  std::vector<int32_t> spikes;
+  std::vector<uint32_t> active;
+  Stdp stdp;
+  std::vector<T> x_pre, x_post;
+  std::vector<uint32_t> in_ptr, in_edge, in_pre;  // CSC of plastic edges
+  double drift = 0.0;
+
+  T *ring_slot(uint32_t r, uint32_t slot) { return &ring[((size_t)r * kSlots + slot) * total]; }
+};
+
+// P/api/net/graph.rs:104-206 from_triplets_with_types: validate, sort by pre
+// (the reference's sort is unstable; this one is stable so that edges of one
+// row keep insertion order), count, prefix-sum a u32 row_ptr, place.
+template <typename T> int build_csr(Net<T> &net) {
+  const uint64_t E = net.edges.size();
+  const uint64_t N = net.total;
+  std::vector<uint64_t> counts(N + 1, 0);
+  for (auto &e : net.edges) counts[e.pre]++;
+  net.row_ptr.assign(N + 1, 0);
+  uint64_t cum = 0;
+  for (uint64_t i = 0; i < N; ++i) {
+    if (cum > 0xFFFFFFFFull) return fail("SparseGraph: too many synapses for a u32 CSR row_ptr");
+    net.row_ptr[i] = (uint32_t)cum;
+    cum += counts[i];
+  }
+  if (cum > 0xFFFFFFFFull) return fail("SparseGraph: too many synapses for a u32 CSR row_ptr");
+  net.row_ptr[N] = (uint32_t)cum;
+  net.col.assign(E, 0);
+  net.w.assign(E, 0);
+  net.d.assign(E, 0);
+  net.st.assign(E, 0);
+  net.plastic.assign(E, 0);
+  std::vector<uint64_t> cursor(net.row_ptr.begin(), net.row_ptr.end() - 1);
+  for (auto &e : net.edges) {
+    uint64_t pos = cursor[e.pre]++;
+    net.col[pos] = e.post;
+    net.w[pos] = (T)e.w;
+    net.d[pos] = e.d;
+    net.st[pos] = e.st;
+    net.plastic[pos] = e.flags & 1;
+  }
+  net.edges.clear();
+  net.edges.shrink_to_fit();
+  return 0;
+}
+
+template <typename T> void alloc_runtime(Net<T> &net) {
+  const size_t N = net.total;
+  net.ring.assign((1 + net.kin.size()) * kSlots * N, (T)0);
+  net.g.assign(net.kin.size() * N, (T)0);
+  net.i_in.assign(N, (T)0);
+  net.v_scr.assign(N, (T)0);
+  net.scratch.assign(N, (T)0);
+  net.spikes.assign(N, 0);
+  net.active.reserve(N / 20 + 8);
+  if (net.stdp.on) {
+    net.x_pre.assign(N, (T)0);
+    net.x_post.assign(N, (T)0);
+    // in-edges of plastic synapses, grouped by post (Brain keeps in_edges,
+    // P/api/learn/brain.rs:79-80,113-118)
+    std::vector<uint64_t> cnt(N + 1, 0);
+    for (uint64_t pre = 0; pre < N; ++pre)
+      for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e)
+        if (net.plastic[e]) cnt[net.col[e]]++;
+    net.in_ptr.assign(N + 1, 0);
+    uint64_t c = 0;
+    for (uint64_t i = 0; i < N; ++i) {
+      net.in_ptr[i] = (uint32_t)c;
+      c += cnt[i];
+    }
+    net.in_ptr[N] = (uint32_t)c;
+    net.in_edge.assign(c, 0);
+    net.in_pre.assign(c, 0);
+    std::vector<uint64_t> cur(net.in_ptr.begin(), net.in_ptr.end() - 1);
+    for (uint64_t pre = 0; pre < N; ++pre)
+      for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e)
+        if (net.plastic[e]) {
+          uint64_t k = cur[net.col[e]]++;
+          net.in_edge[k] = (uint32_t)e;
+          net.in_pre[k] = (uint32_t)pre;
+        }
+  }
+  net.built = true;
+}
+
+int g_threads = 1;
+
+// P/api/net/network/step.rs:18-189 Network::step, then (when configured) the
+// pair-STDP update of the plastic weights.
+template <typename T> void net_step(Net<T> &net) {
+  const size_t N = net.total;
+  if (N == 0) {
+    net.step++;
+    return;
+  }
+  const uint32_t slot = (uint32_t)(net.step % kSlots);
+  // 1-2. read the current slot into i_in, clear it (step.rs:27-34)
+  T *rs = net.ring_slot(0, slot);
+  std::memcpy(net.i_in.data(), rs, N * sizeof(T));
+  std::memset(rs, 0, N * sizeof(T));
+  // 2b. kinetic synapses (step.rs:36-70; ExpOne at :338-345)
+  if (!net.kin.empty()) {
+    for (size_t p = 0; p < net.pops.size(); ++p) {
+      auto &pop = net.pops[p];
+      for (uint32_t i = 0; i < pop.n; ++i) net.v_scr[net.offsets[p] + i] = pop.state[i];
+    }
+    for (size_t k = 0; k < net.kin.size(); ++k) {
+      T *ks = net.ring_slot((uint32_t)k + 1, slot);
+      std::memcpy(net.scratch.data(), ks, N * sizeof(T));
+      std::memset(ks, 0, N * sizeof(T));
+      const T a = (T)net.kin[k].a_decay, erev = (T)net.kin[k].erev;
+      T *g = &net.g[k * N];
+      for (size_t i = 0; i < N; ++i) {
+        T gn = g[i] * a + net.scratch[i];
+        g[i] = gn;
+        net.i_in[i] += gn * (erev - net.v_scr[i]);
+      }
+    }
+  }
+  // 3. populations (P/core/exec/population.rs:284-465).  dt is param column 0
+  // of neuron 0, broadcast to the population (:307,:361).
+  for (size_t p = 0; p < net.pops.size(); ++p) {
+    auto &pop = net.pops[p];
+    if (pop.n == 0) continue;
+    const T dt = pop.params[0];
+    const bool clamp = clamps_input(pop.model);
+    const uint32_t off = net.offsets[p];
+    for (uint32_t i = 0; i < pop.n; ++i) {
+      T x = net.i_in[off + i];
+      if (clamp) x = std::fmin(std::fmax(x, (T)-100.0f), (T)100.0f);
+      Cols<T> c{pop.state.data(), pop.params.data(), pop.cap, i};
+      bool s = false;
+      switch (pop.model) {
+        case LIF: s = lif_step(c, x, dt); break;
+        case IZH: s = izh_step(c, x, dt); break;
+        case GPEA: s = gpea_step(c, x, dt); break;
+        case HH: s = hh_step(c, x, dt); break;
+      }
+      net.spikes[off + i] = s ? 1 : 0;
+    }
+  }
+  // 4. compaction, ascending (P/api/net/compact.rs:30-61)
+  net.active.clear();
+  for (size_t i = 0; i < N; ++i)
+    if (net.spikes[i] != 0) net.active.push_back((uint32_t)i);
+  // 5. push (P/api/net/push.rs:126-173; the rayon variant :184-237 collects
+  // (post, slot, w, type) per chunk in chunk order and scatters them
+  // sequentially, which is the same per-cell order).
+  const uint64_t s = net.step;
+  auto deliver = [&](uint32_t post, uint8_t dl, uint8_t st, T wv) {
+    uint32_t ts = (uint32_t)((s + std::max<uint32_t>(dl, 1)) % kSlots);
+    net.ring_slot(st, ts)[post] += wv;
+  };
+  if (g_threads > 1 && net.active.size() > 64) {
+    struct Tri {
+      uint32_t post;
+      uint8_t d, st;
+      T w;
+    };
+    const size_t A = net.active.size();
+    const int nt = g_threads;
+    const size_t chunk = std::max<size_t>((A + nt - 1) / nt, 8);
+    std::vector<std::vector<Tri>> parts(nt);
+    auto work = [&](int t) {
+      size_t a0 = std::min(A, (size_t)t * chunk), a1 = std::min(A, a0 + chunk);
+      auto &out = parts[t];
+      for (size_t a = a0; a < a1; ++a) {
+        uint32_t pre = net.active[a];
+        for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e)
+          out.push_back(Tri{net.col[e], net.d[e], net.st[e], net.w[e]});
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (auto &part : parts)
+      for (auto &t : part) deliver(t.post, t.d, t.st, t.w);
+  } else {
+    for (uint32_t pre : net.active)
+      for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e)
+        deliver(net.col[e], net.d[e], net.st[e], net.w[e]);
+  }
+  for (uint32_t pre : net.active) net.events += net.row_ptr[pre + 1] - net.row_ptr[pre];
+  // 5b. Poisson sources (step.rs:163-185)
+  for (auto &src : net.srcs) {
+    if (src.p <= 0.0f || !poisson_spike(src.seed, 0, s, src.p)) continue;
+    for (size_t i = 0; i < src.post.size(); ++i) deliver(src.post[i], src.d[i], src.st[i], src.w[i]);
+    net.events += src.post.size();
+  }
+  // Pair STDP with immediate weight updates (oracle-defined; trace order
+  // from P/api/learn/brain.rs:204-222: decay then add, fused mul_add,
+  // d = fast_exp(-dt/tau)).  Depression on the out-edges of every spiking
+  // pre, then potentiation on the in-edges of every spiking post; each
+  // update is clipped to [w_min, w_max].  The push above used the weights
+  // from before this step's update.
+  if (net.stdp.on) {
+    const Stdp &c = net.stdp;
+    const T d_pre = M<T>::fexp(-(T)c.dt / (T)c.tau_pre);
+    const T d_post = M<T>::fexp(-(T)c.dt / (T)c.tau_post);
+    for (size_t i = 0; i < N; ++i) {
+      T add = net.spikes[i] > 0 ? (T)1 : (T)0;
+      net.x_pre[i] = M<T>::fma(net.x_pre[i], d_pre, add);
+      net.x_post[i] = M<T>::fma(net.x_post[i], d_post, add);
+    }
+    const T wmin = (T)c.w_min, wmax = (T)c.w_max, am = (T)c.a_minus, ap = (T)c.a_plus;
+    for (uint32_t pre : net.active)
+      for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e) {
+        if (!net.plastic[e]) continue;
+        T w0 = net.w[e];
+        T w1 = std::fmin(std::fmax(w0 - am * net.x_post[net.col[e]], wmin), wmax);
+        net.w[e] = w1;
+        net.drift += (double)w1 - (double)w0;
+      }
+    for (uint32_t post : net.active)
+      for (uint64_t k = net.in_ptr[post]; k < net.in_ptr[post + 1]; ++k) {
+        uint32_t e = net.in_edge[k];
+        uint32_t pre = net.in_pre[k];
+        T w0 = net.w[e];
+        T w1 = std::fmin(std::fmax(w0 + ap * net.x_pre[pre], wmin), wmax);
+        net.w[e] = w1;
+        net.drift += (double)w1 - (double)w0;
+      }
+  }
+  net.step++;
+}
+
+struct Handle {
+  int precision;
+  NetBase *net;
+};
+
+template <typename T> Net<T> &N_(const or_net *h) {
+  return *static_cast<Net<T> *>(((Handle *)const_cast<or_net *>(h))->net);
+}
+
+#define DISPATCH(h, ...)                           \
+  do {                                             \
+    if (((const Handle *)(h))->precision == 0) {   \
+      auto &net = N_<float>(h);                    \
+      __VA_ARGS__;                                 \
+    } else {                                       \
+      auto &net = N_<double>(h);                   \
+      __VA_ARGS__;                                 \
+    }                                              \
+  } while (0)
+
+template <typename T> int pop_check(Net<T> &net, int pop, int col, bool param) {
+  if (pop < 0 || (size_t)pop >= net.pops.size()) return fail("population out of range");
+  auto &p = net.pops[pop];
+  int lim = param ? (int)p.np : (int)p.ns;
+  if (col < 0 || col >= lim) return fail("column out of range");
+  return 0;
+}
+
+template <typename T> int kuramoto_rk4(uint32_t n, const float *th0, const float *om, float kf,
+                                       float dtf, uint32_t steps, float *th_out, double *r_out) {
+  std::vector<T> th(n), omg(n), k1(n), k2(n), k3(n), k4(n), tmp(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    th[i] = (T)th0[i];
+    omg[i] = (T)om[i];
+  }
+  const T K = (T)kf, dt = (T)dtf, hdt = dt * (T)0.5f, inv_n = (T)1 / (T)n;
+  const T two_pi = (T)6.28318530717958647692;
+  auto field = [&](const std::vector<T> &x, std::vector<T> &k) {
+    double cs = 0, sn = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      cs += std::cos((double)x[i]);
+      sn += std::sin((double)x[i]);
+    }
+    T C = (T)(cs / n), S = (T)(sn / n);
+    for (uint32_t i = 0; i < n; ++i) k[i] = omg[i] + K * (S * std::cos(x[i]) - C * std::sin(x[i]));
+  };
+  (void)inv_n;
+  for (uint32_t s = 0; s < steps; ++s) {
+    field(th, k1);
+    for (uint32_t i = 0; i < n; ++i) tmp[i] = th[i] + hdt * k1[i];
+    field(tmp, k2);
+    for (uint32_t i = 0; i < n; ++i) tmp[i] = th[i] + hdt * k2[i];
+    field(tmp, k3);
+    for (uint32_t i = 0; i < n; ++i) tmp[i] = th[i] + dt * k3[i];
+    field(tmp, k4);
+    const T w6 = dt / (T)6;
+    for (uint32_t i = 0; i < n; ++i) {
+      T x = th[i] + w6 * (((k1[i] + (T)2 * k2[i]) + (T)2 * k3[i]) + k4[i]);
+      th[i] = x - two_pi * std::round(x / two_pi);  // P/kernels/mod.rs:74-77
+    }
+    if (r_out) {
+      double cs = 0, sn = 0;
+      for (uint32_t i = 0; i < n; ++i) {
+        cs += std::cos((double)th[i]);
+        sn += std::sin((double)th[i]);
+      }
+      r_out[s] = std::sqrt(cs * cs + sn * sn) / n;
+    }
+  }
+  for (uint32_t i = 0; i < n; ++i) th_out[i] = (float)th[i];
+  return 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C API
+// ===========================================================================
+extern "C" {
+
+const char *or_last_error(void) { return g_err.c_str(); }
+
+or_net *or_net_new(int precision) {
+  Handle *h = new Handle;
+  h->precision = precision ? 1 : 0;
+  if (h->precision == 0) h->net = new Net<float>();
+  else h->net = new Net<double>();
+  return (or_net *)h;
+}
+
+void or_net_free(or_net *h) {
+  if (!h) return;
+  delete ((Handle *)h)->net;
+  delete (Handle *)h;
+}
+
+int or_set_threads(int n) {
+  g_threads = n < 1 ? 1 : n;
+  return g_threads;
+}
+
+// P/api/net/network/core.rs:124-155 add_population; capacity = ceil(n/8)*8
+int or_pop_add(or_net *h, int model, uint32_t n) {
+  int np = n_params_of(model), ns = n_state_of(model);
+  if (np < 0) return fail("unknown model");
+  int id = -1;
+  DISPATCH(h, {
+    if (net.built) return fail("Cannot add populations after build()");
+    if (net.total + n > 0xFFFFFFFFull) return fail("Network: total neuron count exceeds u32::MAX");
+    Pop<std::remove_reference_t<decltype(net.w[0])>> p;
+    p.model = model;
+    p.n = n;
+    p.cap = (n + 7) / 8 * 8;
+    p.np = np;
+    p.ns = ns;
+    p.params.assign((size_t)p.cap * np, 0);
+    p.state.assign((size_t)p.cap * ns, 0);
+    net.pops.push_back(std::move(p));
+    net.total += n;
+    net.offsets.push_back((uint32_t)net.total);
+    id = (int)net.pops.size() - 1;
+  });
+  return id;
+}
+
+int or_pop_fill_param(or_net *h, int pop, int col, double v) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, true)) return -1;
+    auto &p = net.pops[pop];
+    for (uint32_t i = 0; i < p.n; ++i) p.params[(size_t)col * p.cap + i] = (decltype(p.params[0] + 0))(float)v;
+  });
+  return 0;
+}
+int or_pop_fill_state(or_net *h, int pop, int col, double v) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, false)) return -1;
+    auto &p = net.pops[pop];
+    for (uint32_t i = 0; i < p.n; ++i) p.state[(size_t)col * p.cap + i] = (decltype(p.state[0] + 0))(float)v;
+  });
+  return 0;
+}
+int or_pop_set_param(or_net *h, int pop, int col, const float *v, uint32_t n) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, true)) return -1;
+    auto &p = net.pops[pop];
+    if (n != p.n) return fail("length mismatch");
+    for (uint32_t i = 0; i < p.n; ++i) p.params[(size_t)col * p.cap + i] = v[i];
+  });
+  return 0;
+}
+int or_pop_set_state(or_net *h, int pop, int col, const float *v, uint32_t n) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, false)) return -1;
+    auto &p = net.pops[pop];
+    if (n != p.n) return fail("length mismatch");
+    for (uint32_t i = 0; i < p.n; ++i) p.state[(size_t)col * p.cap + i] = v[i];
+  });
+  return 0;
+}
+int or_pop_get_state(or_net *h, int pop, int col, float *out, uint32_t n) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, false)) return -1;
+    auto &p = net.pops[pop];
+    if (n != p.n) return fail("length mismatch");
+    for (uint32_t i = 0; i < p.n; ++i) out[i] = (float)p.state[(size_t)col * p.cap + i];
+  });
+  return 0;
+}
+int or_pop_get_state_f64(or_net *h, int pop, int col, double *out, uint32_t n) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, false)) return -1;
+    auto &p = net.pops[pop];
+    if (n != p.n) return fail("length mismatch");
+    for (uint32_t i = 0; i < p.n; ++i) out[i] = (double)p.state[(size_t)col * p.cap + i];
+  });
+  return 0;
+}
+int or_pop_get_param(or_net *h, int pop, int col, float *out, uint32_t n) {
+  DISPATCH(h, {
+    if (pop_check(net, pop, col, true)) return -1;
+    auto &p = net.pops[pop];
+    if (n != p.n) return fail("length mismatch");
+    for (uint32_t i = 0; i < p.n; ++i) out[i] = (float)p.params[(size_t)col * p.cap + i];
+  });
+  return 0;
+}
+
+// P/api/net/network/core.rs:166-249 connect / connect_inner
+int or_connect(or_net *h, int from, const uint32_t *fi, int to, const uint32_t *ti, const float *w,
+               const uint8_t *dl, const uint8_t *st, uint64_t n, uint32_t flags) {
+  DISPATCH(h, {
+    if (net.built) return fail("Cannot connect after build()");
+    if (from < 0 || (size_t)from >= net.pops.size()) return fail("from population out of range");
+    if (to < 0 || (size_t)to >= net.pops.size()) return fail("to population out of range");
+    const uint32_t fo = net.offsets[from], fc = net.offsets[from + 1] - fo;
+    const uint32_t tof = net.offsets[to], tc = net.offsets[to + 1] - tof;
+    for (uint64_t i = 0; i < n; ++i) {
+      if (fi[i] >= fc) return fail("from index out of bounds");
+      if (ti[i] >= tc) return fail("to index out of bounds");
+      if (!std::isfinite(w[i])) return fail("Network::connect: weight must be finite");
+      if (dl[i] >= kSlots) return fail("delay >= MAX_DELAY_SLOTS");
+      uint8_t s = st ? st[i] : 0;
+      net.edges.push_back(EdgeIn{fo + fi[i], tof + ti[i], w[i], dl[i], s, (uint8_t)(flags & 1)});
+    }
+  });
+  return 0;
+}
+
+// P/api/net/network/core.rs:564-584 register_kinetics (ExpOne profile,
+// a_decay = exp(-dt/tau) in f32, step.rs:252-254)
+int or_register_expone(or_net *h, float tau_decay, float erev, float dt) {
+  int id = -1;
+  if (!(tau_decay > 0) || !std::isfinite(tau_decay)) return fail("tau_decay must be finite and > 0");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail("register_kinetics: dt must be finite and > 0");
+  DISPATCH(h, {
+    if (net.built) return fail("register_kinetics must be called before build()");
+    if (net.kin.size() >= 255) return fail("profile id overflow");
+    net.kin.push_back(Kin{std::exp(-dt / tau_decay), erev});
+    id = (int)net.kin.size();
+  });
+  return id;
+}
+
+// P/api/net/network/core.rs:288-312
+int or_poisson_add(or_net *h, float rate_hz, float dt_ms, uint32_t seed) {
+  if (!std::isfinite(rate_hz) || rate_hz < 0) return fail("add_poisson_source: rate_hz must be finite and >= 0");
+  if (!std::isfinite(dt_ms) || !(dt_ms > 0)) return fail("add_poisson_source: dt_ms must be finite and > 0");
+  int id = -1;
+  DISPATCH(h, {
+    if (net.built) return fail("add_poisson_source must be called before build()");
+    float p = rate_hz * dt_ms / 1000.0f;
+    p = std::fmin(std::fmax(p, 0.0f), 1.0f);
+    Src<std::remove_reference_t<decltype(net.w[0])>> s;
+    s.p = p;
+    s.seed = seed;
+    net.srcs.push_back(std::move(s));
+    id = (int)net.srcs.size() - 1;
+  });
+  return id;
+}
+
+int or_poisson_add_many(or_net *h, uint32_t n, float rate_hz, float dt_ms, uint32_t seed0) {
+  int first = -1;
+  for (uint32_t i = 0; i < n; ++i) {
+    int id = or_poisson_add(h, rate_hz, dt_ms, seed0 + i);
+    if (id < 0) return id;
+    if (i == 0) first = id;
+  }
+  return first;
+}
+
+// P/api/net/network/core.rs:323-381
+int or_poisson_connect(or_net *h, int src, int to, const uint32_t *posts, const float *w,
+                       const uint8_t *dl, const uint8_t *st, uint64_t n) {
+  DISPATCH(h, {
+    if (net.built) return fail("Cannot connect after build()");
+    if (src < 0 || (size_t)src >= net.srcs.size()) return fail("poisson source out of range");
+    if (to < 0 || (size_t)to >= net.pops.size()) return fail("to population out of range");
+    const uint32_t tof = net.offsets[to], tc = net.offsets[to + 1] - tof;
+    auto &s = net.srcs[src];
+    for (uint64_t i = 0; i < n; ++i) {
+      if (posts[i] >= tc) return fail("post index out of bounds");
+      if (!std::isfinite(w[i])) return fail("connect_poisson_source: weight must be finite");
+      if (dl[i] >= kSlots) return fail("connect_poisson_source: delay >= MAX_DELAY_SLOTS");
+      s.post.push_back(tof + posts[i]);
+      s.w.push_back(w[i]);
+      s.d.push_back(dl[i]);
+      s.st.push_back(st ? st[i] : 0);
+    }
+  });
+  return 0;
+}
+
+int or_poisson_connect_one_to_one(or_net *h, int first, uint32_t n, int to, float w, uint8_t dl) {
+  for (uint32_t i = 0; i < n; ++i) {
+    uint8_t st = 0;
+    int rc = or_poisson_connect(h, first + (int)i, to, &i, &w, &dl, &st, 1);
+    if (rc < 0) return rc;
+  }
+  return 0;
+}
+
+int or_stdp_config(or_net *h, float dt, float tau_pre, float tau_post, float a_plus, float a_minus,
+                   float w_min, float w_max) {
+  DISPATCH(h, {
+    if (net.built) return fail("stdp must be configured before build()");
+    net.stdp = Stdp{true, dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max};
+  });
+  return 0;
+}
+
+// P/api/net/network/build.rs:18-109
+int or_build(or_net *h) {
+  DISPATCH(h, {
+    if (net.built) return fail("Network::build() called twice");
+    for (auto &e : net.edges)
+      if (e.st > net.kin.size()) return fail("Network::build: syn_type exceeds registered kinetics");
+    for (auto &s : net.srcs)
+      for (auto st : s.st)
+        if (st > net.kin.size()) return fail("Network::build: Poisson-source syn_type exceeds registered kinetics");
+    if (build_csr(net)) return -1;
+    alloc_runtime(net);
+  });
+  return 0;
+}
+
+// P/api/net/graph.rs:217-275 from_csr (all edges static, not plastic)
+int or_build_from_csr(or_net *h, const uint32_t *row_ptr, const uint32_t *col, const float *w,
+                      const uint8_t *dl) {
+  DISPATCH(h, {
+    if (net.built) return fail("Network::build() called twice");
+    if (!net.edges.empty()) return fail("from_csr: edges were already added");
+    const uint64_t N = net.total;
+    if (row_ptr[0] != 0) return fail("CSR row_ptr must start at 0");
+    for (uint64_t i = 0; i < N; ++i)
+      if (row_ptr[i] > row_ptr[i + 1]) return fail("CSR row_ptr must be monotonically non-decreasing");
+    const uint64_t E = row_ptr[N];
+    net.row_ptr.assign(row_ptr, row_ptr + N + 1);
+    net.col.assign(col, col + E);
+    net.w.resize(E);
+    for (uint64_t e = 0; e < E; ++e) {
+      if (col[e] >= N) return fail("col index out of range");
+      if (!std::isfinite(w[e])) return fail("weight must be finite");
+      if (dl[e] >= kSlots) return fail("delay >= MAX_DELAY_SLOTS");
+      net.w[e] = w[e];
+    }
+    net.d.assign(dl, dl + E);
+    net.st.assign(E, 0);
+    net.plastic.assign(E, 0);
+    alloc_runtime(net);
+  });
+  return 0;
+}
+
+// P/api/net/network/build.rs:243-275 inject_current (same-step slot)
+int or_inject(or_net *h, int pop, const uint32_t *idx, const float *v, uint64_t n) {
+  DISPATCH(h, {
+    if (!net.built) return fail("inject_current() called before build()");
+    if (pop < 0 || (size_t)pop >= net.pops.size()) return fail("inject_current: population out of range");
+    const uint32_t start = net.offsets[pop], count = net.offsets[pop + 1] - start;
+    for (uint64_t i = 0; i < n; ++i) {
+      if (idx[i] >= count) return fail("inject_current: neuron index out of bounds");
+      if (!std::isfinite(v[i])) return fail("inject_current: value must be finite");
+    }
+    auto *s = net.ring_slot(0, (uint32_t)(net.step % kSlots));
+    for (uint64_t i = 0; i < n; ++i) s[start + idx[i]] += v[i];
+  });
+  return 0;
+}
+
+int or_step(or_net *h, uint32_t n_steps, uint8_t *raster) {
+  DISPATCH(h, {
+    if (!net.built) return fail("Network::step() called before build()");
+    for (uint32_t k = 0; k < n_steps; ++k) {
+      net_step(net);
+      if (raster)
+        for (uint64_t i = 0; i < net.total; ++i) raster[(size_t)k * net.total + i] = (uint8_t)net.spikes[i];
+    }
+  });
+  return 0;
+}
+
+int or_spikes(or_net *h, int pop, int32_t *out, uint32_t n) {
+  DISPATCH(h, {
+    if (pop < 0 || (size_t)pop >= net.pops.size()) return fail("population out of range");
+    uint32_t s = net.offsets[pop], c = net.offsets[pop + 1] - s;
+    if (n != c) return fail("length mismatch");
+    if (!net.built) {
+      std::memset(out, 0, n * 4);
+      return 0;
+    }
+    std::memcpy(out, &net.spikes[s], (size_t)c * 4);
+  });
+  return 0;
+}
+
+uint64_t or_step_counter(const or_net *h) {
+  uint64_t r = 0;
+  DISPATCH(h, { r = net.step; });
+  return r;
+}
+uint64_t or_total_neurons(const or_net *h) {
+  uint64_t r = 0;
+  DISPATCH(h, { r = net.total; });
+  return r;
+}
+uint64_t or_num_synapses(const or_net *h) {
+  uint64_t r = 0;
+  DISPATCH(h, { r = net.built ? net.col.size() : net.edges.size(); });
+  return r;
+}
+uint64_t or_events(const or_net *h) {
+  uint64_t r = 0;
+  DISPATCH(h, { r = net.events; });
+  return r;
+}
+
+int or_ring_read(or_net *h, int ring, float *out) {
+  DISPATCH(h, {
+    if (!net.built) return fail("not built");
+    if (ring < 0 || (size_t)ring > net.kin.size()) return fail("ring out of range");
+    const size_t cnt = (size_t)kSlots * net.total;
+    const auto *src = &net.ring[(size_t)ring * cnt];
+    for (size_t i = 0; i < cnt; ++i) out[i] = (float)src[i];
+  });
+  return 0;
+}
+
+int or_graph_read(or_net *h, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *dl) {
+  DISPATCH(h, {
+    if (!net.built) return fail("not built");
+    std::memcpy(row_ptr, net.row_ptr.data(), net.row_ptr.size() * 4);
+    std::memcpy(col, net.col.data(), net.col.size() * 4);
+    for (size_t i = 0; i < net.w.size(); ++i) w[i] = (float)net.w[i];
+    std::memcpy(dl, net.d.data(), net.d.size());
+  });
+  return 0;
+}
+
+int or_weights_read(or_net *h, float *w) {
+  DISPATCH(h, {
+    if (!net.built) return fail("not built");
+    for (size_t i = 0; i < net.w.size(); ++i) w[i] = (float)net.w[i];
+  });
+  return 0;
+}
+
+double or_stdp_drift(const or_net *h) {
+  double r = 0;
+  DISPATCH(h, { r = net.drift; });
+  return r;
+}
+
+int or_traces_read(or_net *h, float *x_pre, float *x_post) {
+  DISPATCH(h, {
+    if (!net.stdp.on || !net.built) return fail("stdp not enabled");
+    for (size_t i = 0; i < net.total; ++i) {
+      x_pre[i] = (float)net.x_pre[i];
+      x_post[i] = (float)net.x_post[i];
+    }
+  });
+  return 0;
+}
+
+float or_fast_exp(float x) { return fast_exp_f(x); }
+float or_sg_expf(float x) { return sg_expf(x); }
+int or_poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p) {
+  return poisson_spike(seed, stream, step, p) ? 1 : 0;
+}
+uint64_t or_compact(const int32_t *spikes, uint64_t n, uint32_t *out) {
+  uint64_t k = 0;
+  for (uint64_t i = 0; i < n; ++i)
+    if (spikes[i] != 0) out[k++] = (uint32_t)i;
+  return k;
+}
+
+int or_kuramoto_rk4(int precision, uint32_t n, const float *theta0, const float *omega, float k,
+                    float dt, uint32_t n_steps, float *theta_out, double *r_out) {
+  if (n == 0) return fail("empty population");
+  if (precision) return kuramoto_rk4<double>(n, theta0, omega, k, dt, n_steps, theta_out, r_out);
+  return kuramoto_rk4<float>(n, theta0, omega, k, dt, n_steps, theta_out, r_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+"""The oracle against every golden vector the reference's own tests hold for
+the simulation step (CPU only).  The pins are parsed from the reference test
+files by tests/golden/make_reference_pins.py; each case cites its source."""
+import numpy as np
+import pytest
+
+import oracle as O
+import scenarios as S
+
+PINS = S.PINS
+
+
+def make_oracle():
+    return O.Network(0)
+
+
+@pytest.mark.parametrize("cfg", PINS["lif_spike_counts"]["configs"], ids=lambda c: c["label"])
+def test_lif_golden_spike_counts(cfg):
+    # tests/lif_vs_neuron.rs:77-140: mean count within 2 of 0 / 51 / 83
+    pin = PINS["lif_spike_counts"]
+    counts = S.lif_pin_counts(make_oracle, cfg, n=pin["n"], t_ms=pin["t_ms"], on_ms=pin["on_ms"])
+    assert abs(counts.mean() - cfg["ref_spikes"]) <= pin["tolerance"]
+    # the restatement is exact: every neuron gives the pinned count
+    assert np.all(counts == int(cfg["ref_spikes"]))
+
+
+@pytest.mark.parametrize("cfg", PINS["izh_patterns"]["configs"], ids=lambda c: c["label"])
+def test_izhikevich_pattern_ranges(cfg):
+    # tests/izhikevich_vs_neuron.rs:30-75,152-190
+    per, cv = S.izh_pattern(make_oracle, cfg, PINS["izh_patterns"])
+    avg = per.mean()
+    assert cfg["min_spikes"] <= avg <= cfg["max_spikes"], avg
+    assert cv >= cfg["min_isi_cv"]
+
+
+@pytest.mark.parametrize("n", PINS["delay_arrival"]["sizes"])
+def test_delay_arrival_exact(n):
+    # tests/network_delays.rs:114-160: arrival exactly max(delay, 1) steps later
+    delays = PINS["delay_arrival"]["delays"]
+    d = [delays[i % len(delays)] for i in range(n)]
+    a0, raster = S.delay_arrival(make_oracle, n, d)
+    assert np.all(a0 == 1)
+    for i, dl in enumerate(d):
+        arrival = max(dl, 1)
+        expect = np.zeros(raster.shape[0], np.int32)
+        expect[arrival] = 1
+        assert np.array_equal(raster[:, i], expect), (i, dl)
+    assert raster.sum() == n
+
+
+@pytest.mark.parametrize("case", PINS["push"]["cases"], ids=lambda c: c["name"])
+def test_push_slot_arithmetic(case):
+    # P/api/net/push.rs:300-499
+    ring, spikes = S.push_case(make_oracle, case)
+    assert sorted(np.nonzero(spikes)[0].tolist()) == sorted(case["active"])
+    expect = np.zeros_like(ring)
+    for slot, post, val in case["expect"]:
+        expect[slot, post] += val
+    assert np.array_equal(ring, expect)
+
+
+def test_delay_ring_accumulate():
+    # P/api/net/delay.rs:139-145: 3 + 4 accumulate to 7 in one cell
+    case = dict(n=3, **{"from": [0, 1], "to": [2, 2]}, w=[3.0, 4.0], d=[2, 2], active=[0, 1], step=0)
+    ring, _ = S.push_case(make_oracle, case)
+    assert ring[2, 2] == 7.0
+
+
+def test_compaction_pins():
+    pin = PINS["compact"]
+    s = [1 if i % pin["some"]["every"] == 0 else 0 for i in range(pin["some"]["n"])]
+    assert O.compact(s).tolist() == pin["some"]["expect"]
+    assert O.compact(pin["alternating"]["spikes"]).tolist() == pin["alternating"]["expect"]
+    h = pin["hashed"]
+    spikes = [1 if (i * h["mul"]) % (1 << 64) % h["mod"] < h["lt"] else 0 for i in range(h["n"])]
+    out = O.compact(spikes)
+    assert out.tolist() == [i for i, x in enumerate(spikes) if x]
+    assert out.size >= h["min_len"]
+    assert O.compact(np.zeros(100, np.int32)).size == 0
+    assert O.compact(np.ones(64, np.int32)).tolist() == list(range(64))
+
+
+def test_poisson_hash_properties():
+    # P/api/net/network/sources.rs:5-14: deterministic, rate ~ p
+    hits = sum(O.poisson_spike(7, 0, s, 0.2) for s in range(20000))
+    assert abs(hits / 20000 - 0.2) < 0.01
+    assert [O.poisson_spike(3, 0, s, 0.5) for s in range(50)] == [O.poisson_spike(3, 0, s, 0.5) for s in range(50)]
+    assert not any(O.poisson_spike(1, 0, s, 0.0) for s in range(1000))
+    assert all(O.poisson_spike(1, 0, s, 1.0) for s in range(1000))
+
+
+def test_fast_exp_accuracy():
+    # P/math/fast_exp.rs:20-22: rel. error < 0.001 for |x| < 80
+    for x in np.linspace(-80, 80, 2001):
+        assert abs(O.fast_exp(x) / np.exp(x) - 1) < 1e-3
+
+
+def test_hh_exp_accuracy():
+    for x in np.linspace(-80, 80, 4001, dtype=np.float32):
+        e = np.exp(np.float64(x))
+        assert abs(O.sg_expf(float(x)) / e - 1) < 4e-7
+
+
+def test_contract_violations_raise():
+    net = make_oracle()
+    p = net.add_population(S.LIF, 4)
+    with pytest.raises(O.OracleError):
+        net.connect(p, [0], p, [9], [1.0], [0])  # to index out of bounds
+    with pytest.raises(O.OracleError):
+        net.connect(p, [0], p, [1], [1.0], [32])  # delay >= 32
+    with pytest.raises(O.OracleError):
+        net.connect(p, [0], p, [1], [float("nan")], [0])
+    with pytest.raises(O.OracleError):
+        net.step(1)  # before build
+    net.build()
+    with pytest.raises(O.OracleError):
+        net.build()
+    with pytest.raises(O.OracleError):
+        net.connect(p, [0], p, [1], [1.0], [0])
+    with pytest.raises(O.OracleError):
+        net.inject_current(p, [4], [1.0])
+
+
+def test_empty_network_advances_counter():
+    # P/api/net/network/step.rs:22-25
+    net = make_oracle()
+    net.build()
+    net.step(5)
+    assert net.step_counter == 5
+
+
+def test_izhikevich_pulse_network_activity():
+    # the pulse-coupled network settles into the known ~5-10 Hz activity
+    import simuse_b200.workloads as W
+    spec = W.izhikevich_pulse(steps=300)
+    net = make_oracle()
+    pop = W.build_izhikevich(net, spec)
+    idx = np.arange(spec["n"], dtype=np.uint32)
+    tot = 0
+    for t in range(300):
+        net.inject_current(pop, idx, W.izhikevich_input(spec, t))
+        net.step(1)
+        tot += net.spikes(pop).sum()
+    rate = tot / spec["n"] / 0.3
+    assert 2.0 < rate < 20.0, rate
+
+
+def test_fixed_indegree_generator_shape():
+    import simuse_b200.workloads as W
+    pre, post, w, d = W.fixed_indegree_edges(1000, 500, 50, 9, 800, 20.0, -100.0, 1, 20)
+    assert pre.size == 500 * 50
+    assert np.all(np.bincount(post, minlength=500) == 50)
+    assert pre.max() < 1000 and d.min() >= 1 and d.max() <= 20
+    assert np.all((w == 20.0) == (pre < 800))
+
+
+def test_hh_fp32_vs_fp64_close():
+    # HH-RK4 FP32 restatement stays close to its FP64 twin over 20 ms
+    out = []
+    for prec in (0, 1):
+        net = O.Network(prec)
+        p = net.add_population(S.HH, 16)
+        for col, v in enumerate([0.01, 1.0, 120.0, 36.0, 0.3, 50.0, -77.0, -54.4, 10.0, 0.0]):
+            net.fill_param(p, col, v)
+        net.fill_state(p, 0, -65.0)
+        net.fill_state(p, 1, 0.0529)
+        net.fill_state(p, 2, 0.5961)
+        net.fill_state(p, 3, 0.3177)
+        net.build()
+        r = net.step(2000, record=True)
+        out.append((r, net.state_f64(p, 0)))
+    (r32, v32), (r64, v64) = out
+    assert np.array_equal(r32, r64)
+    assert r32.sum() > 0
+    assert np.max(np.abs(v32 - v64)) < 1e-2
