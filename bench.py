@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Headline benchmark: synaptic events/s of the SiMuse simulation step on a
+balanced LIF network of 1,000,000 neurons and 1e9 synapses.
+
+One bench "step" = `--sim-steps` simulation steps (default 1000 = 100 ms of
+simulated time at dt = 0.1 ms) of the whole network: neuron update, spike
+compaction, deterministic CSR scatter into the delay rings, Poisson drive.
+
+Workloads (`--variant`):
+  driven   external Poisson drive 4000 Hz x 0.5 mV (ring weight 100) per
+           neuron; the network settles at ~34 Hz and the recurrent scatter
+           carries ~3.8e6 synaptic events per step.  Headline.
+  literal  the configuration as stated (2000 Hz x J = 0.1 mV): mean drive
+           4 mV < threshold 20 mV, so the network is silent and only the
+           2e5 Poisson events per step reach the rings.
+
+Reported, one JSON line on rank 0:
+  value   events/s over K bench steps, CUDA events on the network's stream
+          (inputs resident in HBM; the 9 GB CSR exceeds L2 on every step).
+  e2e     the same metric through the C ABI with host buffers: each bench
+          step calls sg_step and then reads the step's spike raster back to
+          pinned host memory (sg_raster_read_events), wall clock.
+  roofline  dominant kernel: algorithmic bytes per launch / average launch
+          time (CUDA events around each phase in a profiled pass of K bench
+          steps) against MEASURED_PEAKS.json's copy bandwidth.
+  cpu_baseline  the CPU restatement of the reference step (oracle/) on this
+          host's cores, on a bounded sample of the same network.
+`--impl reference` times that CPU path alone as the reference arm.
+Multi-GPU (`--gpus N` under torchrun): each rank simulates its own replica
+(seed + rank); no data-path collective (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dioma-core_b200"))
+
+METRIC = "synaptic events/s"
+UNIT = "events/s"
+
+# algorithmic bytes: LIF neuron = v, refr read+write (16 B),
+# ring slot read + clear (8 B), spike bit (1/8 B); per event col 4 + weight 4
+# + delay 1 (expand) and ring read-modify-write 8 (apply); per spike the
+# active-list write+read and two row_ptr reads (16 B); per Poisson source
+# rate + seed reads (8 B).
+B_NEURON = 24.125
+B_EVENT_EXPAND = 9.0
+B_EVENT_APPLY = 8.0
+B_SPIKE = 16.0
+B_SOURCE = 8.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="driven", choices=["driven", "literal"])
+    ap.add_argument("--sim-steps", type=int, default=1000)
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--k-in", type=int, default=1000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args, rank=0):
+    from simuse_b200 import workloads as W
+    kw = (dict(ext_rate_hz=4000.0, ext_weight=100.0) if args.variant == "driven"
+          else dict(ext_rate_hz=2000.0, ext_weight=20.0))
+    spec = W.lif_balanced(n=args.n, k_in=args.k_in, seed=1 + rank, **kw)
+    name = f"lif_balanced_{args.n // 1000}k_in{args.k_in}_{args.variant}"
+    return spec, name
+
+
+def config(args, name, spec):
+    return {
+        "workload": name,
+        "neurons": spec["n"],
+        "synapses": spec["n"] * spec["k_in"],
+        "dt_ms": spec["dt"],
+        "sim_steps_per_bench_step": args.sim_steps,
+        "external_drive": {"rate_hz": spec["ext_rate_hz"], "ring_weight": spec["ext_weight"]},
+        "weights": "fp32", "scatter": "deterministic (reference summation order)",
+        "l2": "inputs larger than L2 (9 GB CSR streamed every step)",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(args, spec, seconds):
+    """The CPU restatement of the reference step on this host's cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    net = O.Network(0)
+    pop = net.add_population(O.LIF, spec["n"])
+    from simuse_b200.workloads import LIF_PARAMS
+    for col, v in enumerate(LIF_PARAMS):
+        net.fill_param(pop, col, v)
+    net.set_state(pop, 0, spec["v0"])
+    first = net.add_poisson_sources(spec["n"], spec["ext_rate_hz"], spec["dt"], seed0=0)
+    net.connect_poisson_one_to_one(first, spec["n"], pop, spec["ext_weight"], 1)
+    t0 = time.time()
+    net.build_fixed_indegree(pop, pop, spec["k_in"], spec["seed"], spec["n_exc"], spec["w_exc"],
+                             spec["w_inh"], spec["d_min"], spec["d_max"])
+    build_s = time.time() - t0
+    return net, cores, build_s
+
+
+def run_cpu_sample(net, seconds, min_steps=5, chunk=5):
+    ev0 = net.events
+    s0 = net.step_counter
+    t0 = time.perf_counter()
+    while True:
+        net.step(chunk)
+        el = time.perf_counter() - t0
+        if el >= seconds and net.step_counter - s0 >= min_steps:
+            break
+    return net.events - ev0, net.step_counter - s0, el
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        v = d.get(kernel)
+        return None if v is None else float(v["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+
+    spec, name = workload(args, rank)
+    net = sg.Network(local)
+    W.build_lif(net, spec)
+    net.build()
+    net.synchronize()
+    stream = torch.cuda.ExternalStream(net.stream, device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        net.synchronize()
+
+    S = args.sim_steps
+    for _ in range(args.warmup):
+        net.step(S)
+    barrier()
+
+    # ---- (A) device-timed value ---------------------------------------------
+    ev0 = net.events_total
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            net.step(S)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    events = net.events_total - ev0
+    spk, evs = net.read_stats()
+    spk = spk[-args.steps * S:]
+    t_max = ms
+    ev_all = events
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        e = torch.tensor([float(events)], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        ev_all = float(e.item())
+    value = ev_all / (t_max / 1e3)
+
+    # ---- (B) end to end through the C ABI with host buffers --------------------
+    net.enable_raster(S)
+    cap = int(max(spk.max() if spk.size else 1, 1) * S * 1.5) + 1024
+    h_steps = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    h_idx = torch.empty(cap, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    net.step(S)
+    net.read_spike_events_into(h_steps, h_idx)  # warm
+    barrier()
+    ev0 = net.events_total
+    d2h = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.step(S)
+        n_sp = net.read_spike_events_into(h_steps, h_idx)
+        d2h += n_sp * 8
+    t_e2e = time.perf_counter() - t0
+    ev_e2e = net.events_total - ev0
+    if dist is not None:
+        t = torch.tensor([t_e2e], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+        e = torch.tensor([float(ev_e2e)], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        ev_e2e = float(e.item())
+    net.enable_raster(0)
+
+    # ---- (C) per-kernel timing: CUDA events around each phase --------------------
+    net.profile(True)
+    p_steps = min(S, 1000)
+    sp_before = net.step_counter
+    ev0 = net.events_total
+    net.step(p_steps)
+    ph_ms, ph_launch = net.profile_read()
+    net.profile(False)
+    p_events = (net.events_total - ev0) / p_steps
+    sp, _ = net.read_stats()
+    p_spikes = float(sp[-p_steps:].mean()) if sp.size else 0.0
+    phases = ["neuron_kernel<LIF>", "expand_kernel", "stdp_ltp_kernel", "apply_kernel"]
+    n_src = spec["n"]
+    alg = [spec["n"] * B_NEURON,
+           p_events * B_EVENT_EXPAND + p_spikes * B_SPIKE + n_src * B_SOURCE,
+           0.0,
+           p_events * B_EVENT_APPLY]
+    per_launch_ms = [ph_ms[i] / max(int(ph_launch[i]), 1) for i in range(4)]
+    dom = int(np.argmax(ph_ms))
+    peak, peak_kind = measured_peak()
+    achieved = alg[dom] / (per_launch_ms[dom] / 1e3) / 1e9
+    step_alg = sum(alg)
+    step_ms = ms / (args.steps * S)
+
+    if dist is not None:
+        net.close()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    mean_spk = float(spk.mean()) if spk.size else 0.0
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config(args, name, spec),
+        "sim": {"ms_per_sim_step": step_ms, "events_per_sim_step": events / (args.steps * S),
+                "spikes_per_sim_step": mean_spk, "rate_hz": mean_spk / spec["n"] / (spec["dt"] * 1e-3),
+                "neuron_updates_per_s": spec["n"] * args.steps * S / (ms / 1e3) * world,
+                "step_roofline_frac": step_alg / (step_ms / 1e3) / 1e9 / peak},
+        "e2e": {"value": ev_e2e / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(d2h / args.steps),
+                "path": "sg_step + sg_raster_read_events into pinned host buffers, wall clock"},
+        "roofline": {"bound": "hbm", "kernel": phases[dom], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": profiled_traffic(phases[dom]),
+                     "alg_bytes_per_launch": alg[dom], "launch_ms": per_launch_ms[dom],
+                     "phases_ms_per_launch": dict(zip(phases, per_launch_ms))},
+        "clocks": clk.summary(),
+        "gpu_launches": int(args.steps * S * 3),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        cnet, cores, build_s = cpu_baseline(args, spec, args.cpu_seconds)
+        ev, nsteps, el = run_cpu_sample(cnet, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": ev / el, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"first {nsteps} steps of the same network from its initial state "
+                                         f"({el:.1f} s; oracle/ C++ restatement, push collected on {cores} threads)"}
+    print(json.dumps(out), flush=True)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    spec, name = workload(args, 0)
+    net, cores, build_s = cpu_baseline(args, spec, args.cpu_seconds)
+    per_step_s = 1.0
+    for _ in range(args.warmup):
+        run_cpu_sample(net, per_step_s, min_steps=5)
+    tot_ev, tot_t, tot_steps = 0, 0.0, 0
+    for _ in range(args.steps):
+        ev, ns, el = run_cpu_sample(net, per_step_s, min_steps=5)
+        tot_ev += ev
+        tot_t += el
+        tot_steps += ns
+    value = tot_ev / tot_t
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_t / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)", "impl": "reference", "config": config(args, name, spec),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{tot_steps} simulation steps in {args.steps} samples of ~{per_step_s:.0f} s "
+                                   f"(oracle/ C++ restatement of the reference step; build {build_s:.1f} s)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -146,6 +146,11 @@ struct sg_net {
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_steps = 0;
   std::vector<float> ln_consts{0, 0};
+  // per-phase CUDA-event timing (neuron, expand, stdp_ltp, apply)
+  bool profile = false;
+  std::vector<cudaEvent_t> prof_ev;
+  double prof_ms[4] = {0, 0, 0, 0};
+  uint64_t prof_launches[4] = {0, 0, 0, 0};
 
   uint32_t dev_index(uint32_t pop, uint32_t i) const { return pops[pop].dev_off + i; }
 };
@@ -335,6 +340,87 @@ __global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, u
     post[base + t] = to_off + j;
     w[base + t] = exc ? w_exc : w_inh;
     code[base + t] = edge_code((uint8_t)d, exc ? st_e : st_i, exc && (flags_e & SG_EDGE_STDP));
+  }
+}
+
+// Raster compaction: bitmask rows (one per recorded step) -> (step, global
+// index) pairs in step-then-index order.  1024 words per block.
+constexpr uint32_t kRasterWordsPerBlock = 1024;
+
+__device__ __forceinline__ uint32_t raster_word(const uint32_t *bits, uint32_t cap, uint32_t words, uint64_t t0,
+                                                uint64_t w) {
+  const uint64_t t = t0 + w / words;
+  return bits[(size_t)(t % cap) * words + (w % words)];
+}
+
+__global__ void raster_count_kernel(const uint32_t *bits, uint32_t cap, uint32_t words, uint64_t t0, uint64_t nw,
+                                    unsigned long long *block_cnt) {
+  const uint64_t w0 = (uint64_t)blockIdx.x * kRasterWordsPerBlock;
+  uint32_t c = 0;
+  for (uint32_t j = threadIdx.x; j < kRasterWordsPerBlock; j += blockDim.x)
+    if (w0 + j < nw) c += __popc(raster_word(bits, cap, words, t0, w0 + j));
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  __shared__ uint32_t part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (uint32_t i = 0; i < blockDim.x / 32; ++i) tot += part[i];
+    block_cnt[blockIdx.x] = tot;
+  }
+}
+
+__global__ void raster_write_kernel(const uint32_t *bits, uint32_t cap, uint32_t words, uint64_t t0, uint64_t nw,
+                                    const unsigned long long *block_off, const uint32_t *pop_dev, const uint32_t *pop_glob,
+                                    int npops, uint32_t *out_step, uint32_t *out_idx) {
+  // each thread owns 4 consecutive words of the block's 1024
+  __shared__ uint32_t warp_tot[32];
+  const uint64_t w0 = (uint64_t)blockIdx.x * kRasterWordsPerBlock + threadIdx.x * 4;
+  uint32_t v[4], c = 0;
+  for (int q = 0; q < 4; ++q) {
+    v[q] = (w0 + q < nw) ? raster_word(bits, cap, words, t0, w0 + q) : 0u;
+    c += __popc(v[q]);
+  }
+  // block exclusive scan of c
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t t = lane < blockDim.x / 32 ? warp_tot[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= (uint32_t)o) t += y;
+    }
+    warp_tot[lane] = t;  // inclusive
+  }
+  __syncthreads();
+  unsigned long long pos = block_off[blockIdx.x] + (x - c) + (wid ? warp_tot[wid - 1] : 0);
+  for (int q = 0; q < 4; ++q) {
+    uint32_t m = v[q];
+    if (!m) continue;
+    const uint64_t w = w0 + q;
+    const uint32_t step = (uint32_t)(t0 + w / words);
+    const uint32_t dbase = (uint32_t)(w % words) * 32;
+    // population of this word (populations are 32-aligned: one per word)
+    int lo = 0, hi = npops - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pop_dev[mid] <= dbase) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t gbase = pop_glob[lo] + (dbase - pop_dev[lo]);
+    while (m) {
+      const uint32_t b = __ffs(m) - 1;
+      m &= m - 1;
+      out_step[pos] = step;
+      out_idx[pos] = gbase + b;
+      ++pos;
+    }
   }
 }
 
@@ -592,8 +678,9 @@ template <int M> void launch_neuron(sg_net *net, const StepArgs &a, HostPop &p) 
   neuron_kernel<M><<<blocks, 256, 0, net->stream>>>(a, pa);
 }
 
-void enqueue_step(sg_net *net, const StepArgs &a) {
+void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
   cudaStream_t s = net->stream;
+  if (ev) SG_CUDA(cudaEventRecord(ev[0], s));
   for (auto &p : net->pops) {
     if (p.n == 0) continue;
     switch (p.model) {
@@ -603,9 +690,35 @@ void enqueue_step(sg_net *net, const StepArgs &a) {
       case kHH: launch_neuron<kHH>(net, a, p); break;
     }
   }
+  if (ev) SG_CUDA(cudaEventRecord(ev[1], s));
   expand_kernel<<<net->src_blocks + net->expand_blocks, 256, 0, s>>>(a, (uint32_t)net->src_blocks);
+  if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
   if (net->stdp_on) stdp_ltp_kernel<<<net->expand_blocks, 256, 0, s>>>(a);
+  if (ev) SG_CUDA(cudaEventRecord(ev[3], s));
   apply_kernel<<<net->apply_blocks, 512, net->apply_smem, s>>>(a);
+  if (ev) SG_CUDA(cudaEventRecord(ev[4], s));
+}
+
+// Profiled steps: eager launches with CUDA events between the phases, read
+// back after every step (adds host synchronisation; for measurement only).
+void do_steps_profiled(sg_net *net, uint32_t n) {
+  const StepArgs a = make_args(net);
+  if (net->prof_ev.empty()) {
+    net->prof_ev.resize(5);
+    for (auto &e : net->prof_ev) SG_CUDA(cudaEventCreate(&e));
+  }
+  for (uint32_t k = 0; k < n; ++k) {
+    enqueue_step(net, a, net->prof_ev.data());
+    SG_CUDA(cudaEventSynchronize(net->prof_ev[4]));
+    for (int ph = 0; ph < 4; ++ph) {
+      float ms = 0;
+      SG_CUDA(cudaEventElapsedTime(&ms, net->prof_ev[ph], net->prof_ev[ph + 1]));
+      net->prof_ms[ph] += ms;
+      if (ph != 2 || net->stdp_on) net->prof_launches[ph] += (ph == 0 ? net->pops.size() : 1);
+    }
+  }
+  SG_CUDA(cudaGetLastError());
+  net->host_step += n;
 }
 
 void drop_graph(sg_net *net) {
@@ -695,6 +808,7 @@ int sg_net_destroy(sg_net *net) {
     DevGuard g(net->device);
     cudaStreamSynchronize(net->stream);
     drop_graph(net);
+    for (auto e : net->prof_ev) cudaEventDestroy(e);
     cudaStream_t s = net->stream;
     delete net;  // DBufs free their memory
     cudaStreamDestroy(s);
@@ -1080,7 +1194,30 @@ int sg_step(sg_net *net, uint32_t n_steps) {
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "Network::step() called before build()");
     DevGuard g(net->device);
-    do_steps(net, n_steps);
+    if (net->profile && net->total > 0) do_steps_profiled(net, n_steps);
+    else do_steps(net, n_steps);
+  });
+}
+
+int sg_profile_enable(sg_net *net, int on) {
+  NET_CHECK(net);
+  return run([&] {
+    net->profile = on != 0;
+    for (int i = 0; i < 4; ++i) {
+      net->prof_ms[i] = 0;
+      net->prof_launches[i] = 0;
+    }
+  });
+}
+
+int sg_profile_read(sg_net *net, double *ms, uint64_t *launches) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(ms && launches, SG_E_INVALID, "null output");
+    for (int i = 0; i < 4; ++i) {
+      ms[i] = net->prof_ms[i];
+      launches[i] = net->prof_launches[i];
+    }
   });
 }
 
@@ -1130,6 +1267,67 @@ int sg_raster_read(sg_net *net, uint8_t *out, uint64_t cap_bytes, uint32_t *n_st
       }
     }
     if (n_steps) *n_steps = (uint32_t)k;
+    net->raster_read_step = net->host_step;
+  });
+}
+
+int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap, uint64_t *n_out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->raster_cap > 0, SG_E_STATE, "raster recording is not enabled");
+    SG_REQUIRE(n_out, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    cudaStream_t s = net->stream;
+    const uint64_t k = net->host_step - net->raster_read_step;
+    SG_REQUIRE(k <= net->raster_cap, SG_E_OVERFLOW,
+               "raster overflow: " + std::to_string(k) + " steps since the last read, capacity " +
+                   std::to_string(net->raster_cap));
+    const uint32_t words = net->Nd / 32;
+    const uint64_t nw = k * words;
+    const uint64_t nb = (nw + kRasterWordsPerBlock - 1) / kRasterWordsPerBlock;
+    *n_out = 0;
+    if (nb == 0) {
+      net->raster_read_step = net->host_step;
+      return;
+    }
+    DBuf<unsigned long long> cnt, off;
+    cnt.alloc(nb + 1);
+    off.alloc(nb + 1);
+    cnt.zero(s);
+    raster_count_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, net->raster_read_step, nw,
+                                                     cnt.p);
+    size_t tb = 0;
+    SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, off.p, (int64_t)nb + 1, s));
+    DBuf<uint8_t> temp;
+    temp.alloc(std::max<size_t>(tb, 1));
+    SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, off.p, (int64_t)nb + 1, s));
+    unsigned long long total = 0;
+    SG_CUDA(cudaMemcpyAsync(&total, off.p + nb, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    *n_out = total;
+    SG_REQUIRE(total <= cap, SG_E_INVALID, "output buffer too small: " + std::to_string(total) + " spikes");
+    if (total == 0) {
+      net->raster_read_step = net->host_step;
+      return;
+    }
+    std::vector<uint32_t> pd, pgl;
+    for (size_t p = 0; p < net->pops.size(); ++p) {
+      pd.push_back(net->pops[p].dev_off);
+      pgl.push_back(net->offsets[p]);
+    }
+    DBuf<uint32_t> d_pd, d_pg, o_step, o_idx;
+    d_pd.alloc(pd.size());
+    d_pg.alloc(pgl.size());
+    SG_CUDA(cudaMemcpyAsync(d_pd.p, pd.data(), pd.size() * 4, cudaMemcpyHostToDevice, s));
+    SG_CUDA(cudaMemcpyAsync(d_pg.p, pgl.data(), pgl.size() * 4, cudaMemcpyHostToDevice, s));
+    o_step.alloc(total);
+    o_idx.alloc(total);
+    raster_write_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, net->raster_read_step, nw,
+                                                     off.p, d_pd.p, d_pg.p, (int)pd.size(), o_step.p, o_idx.p);
+    SG_CUDA(cudaGetLastError());
+    if (steps) SG_CUDA(cudaMemcpyAsync(steps, o_step.p, total * 4, cudaMemcpyDeviceToHost, s));
+    if (idx) SG_CUDA(cudaMemcpyAsync(idx, o_idx.p, total * 4, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
     net->raster_read_step = net->host_step;
   });
 }

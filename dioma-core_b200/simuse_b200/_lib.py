@@ -56,6 +56,9 @@ SIGNATURES = {
     "sg_raster_enable": [vp, u32],
     "sg_raster_read": [vp, vp, u64, vp],
     "sg_stats_read": [vp, vp, vp, u32, vp],
+    "sg_raster_read_events": [vp, vp, vp, u64, vp],
+    "sg_profile_enable": [vp, i32],
+    "sg_profile_read": [vp, vp, vp],
     "sg_spikes": [vp, u32, vp, u32],
     "sg_step_counter": [vp, vp],
     "sg_total_neurons": [vp, vp],

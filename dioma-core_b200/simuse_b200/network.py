@@ -179,6 +179,35 @@ class Network:
         self._raster_mark = self.step_counter
         return out[: n.value * self.total_neurons].reshape(n.value, self.total_neurons)
 
+    def read_spike_events(self, capacity: int | None = None):
+        """(steps, indices) of every spike recorded since the last read,
+        ordered by step then neuron (compacted on the device)."""
+        n = C.c_uint64()
+        if capacity is None:
+            k = self.step_counter - getattr(self, "_raster_mark", 0)
+            capacity = max(1, k * self.total_neurons)
+        st = np.empty(capacity, np.uint32)
+        ix = np.empty(capacity, np.uint32)
+        check(lib().sg_raster_read_events(self._h, _p(st), _p(ix), capacity, C.byref(n)))
+        self._raster_mark = self.step_counter
+        return st[: n.value], ix[: n.value]
+
+    def read_spike_events_into(self, steps: np.ndarray, idx: np.ndarray) -> int:
+        """Zero-allocation variant for preallocated (pinned) host buffers."""
+        n = C.c_uint64()
+        check(lib().sg_raster_read_events(self._h, _p(steps), _p(idx), steps.size, C.byref(n)))
+        self._raster_mark = self.step_counter
+        return n.value
+
+    def profile(self, on: bool):
+        check(lib().sg_profile_enable(self._h, 1 if on else 0))
+
+    def profile_read(self):
+        ms = np.zeros(4, np.float64)
+        launches = np.zeros(4, np.uint64)
+        check(lib().sg_profile_read(self._h, _p(ms), _p(launches)))
+        return ms, launches
+
     def read_stats(self):
         k = C.c_uint32()
         n = max(1, self.step_counter - getattr(self, "_stats_mark", 0))

@@ -151,6 +151,17 @@ int sg_raster_read(sg_net *net, uint8_t *out, uint64_t cap_bytes, uint32_t *n_st
 /* Per-step counters since the last read: spikes and synaptic events. */
 int sg_stats_read(sg_net *net, uint32_t *spikes, uint64_t *events, uint32_t cap, uint32_t *n_steps);
 
+/* Spike raster of the steps recorded since the last read, as a list of
+   (step, global neuron index) pairs ordered by step then index; the list is
+   compacted on the device so only the spikes cross PCIe.  *n_out = spikes. */
+int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap,
+                          uint64_t *n_out);
+/* Phase timing: when enabled, sg_step launches each step eagerly with CUDA
+   events around its phases (0 neuron update, 1 expand, 2 STDP potentiation,
+   3 apply) and accumulates the device time per phase. */
+int sg_profile_enable(sg_net *net, int on);
+int sg_profile_read(sg_net *net, double *ms, uint64_t *launches); /* 4 entries each */
+
 /* ---- readback --------------------------------------------------------- */
 int sg_spikes(sg_net *net, uint32_t pop, int32_t *out, uint32_t n); /* build.rs:145-152 */
 int sg_step_counter(sg_net *net, uint64_t *out);                    /* build.rs:136-140 */

@@ -65,6 +65,7 @@ def lib():
             "or_poisson_connect_one_to_one": (i32, [vp, i32, u32, i32, f32, C.c_uint8]),
             "or_stdp_config": (i32, [vp, f32, f32, f32, f32, f32, f32, f32]),
             "or_build": (i32, [vp]),
+            "or_build_fixed_indegree": (i32, [vp, i32, i32, u32, u64, u32, f32, f32, u32, u32]),
             "or_build_from_csr": (i32, [vp, vp, vp, vp, vp]),
             "or_inject": (i32, [vp, i32, vp, vp, u64]),
             "or_step": (i32, [vp, u32, vp]),
@@ -199,6 +200,10 @@ class Network:
 
     def build(self):
         _chk(lib().or_build(self._h))
+
+    def build_fixed_indegree(self, frm, to, k_in, seed, n_exc, w_exc, w_inh, d_min, d_max):
+        """Fixed in-degree projection + build in one pass (see simuse_oracle.h)."""
+        _chk(lib().or_build_fixed_indegree(self._h, frm, to, k_in, seed, n_exc, w_exc, w_inh, d_min, d_max))
 
     def build_from_csr(self, row_ptr, col, w, d):
         rp = np.ascontiguousarray(row_ptr, np.uint32)

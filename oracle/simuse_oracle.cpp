@@ -923,6 +923,100 @@ int or_stdp_config(or_net *h, float dt, float tau_pre, float tau_post, float a_p
   return 0;
 }
 
+static inline uint64_t splitmix64_h(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// connect(fixed in-degree projection, same generator as the product's
+// sg_connect_fixed_indegree: edge t = (post j, draw q) = j*k_in + q) followed
+// by build(), writing the stable-sorted CSR directly (no triplet list), in
+// parallel over post ranges with per-thread row offsets so that every row
+// keeps (post, draw) order.  Only for a network with no other synapses.
+int or_build_fixed_indegree(or_net *h, int from, int to, uint32_t k_in, uint64_t seed, uint32_t n_exc,
+                            float w_exc, float w_inh, uint32_t d_min, uint32_t d_max) {
+  DISPATCH(h, {
+    if (net.built) return fail("Network::build() called twice");
+    if (!net.edges.empty()) return fail("fixed in-degree build needs a network without other edges");
+    if (from < 0 || (size_t)from >= net.pops.size() || to < 0 || (size_t)to >= net.pops.size())
+      return fail("population out of range");
+    if (d_min > d_max || d_max >= kSlots) return fail("delay range invalid");
+    const uint32_t fo = net.offsets[from], nf = net.offsets[from + 1] - fo;
+    const uint32_t tof = net.offsets[to], nt = net.offsets[to + 1] - tof;
+    const uint64_t N = net.total, E = (uint64_t)nt * k_in;
+    if (E > 0xFFFFFFFFull) return fail("SparseGraph: too many synapses for a u32 CSR row_ptr");
+    const uint32_t span = d_max - d_min + 1;
+    const int T = std::max(1, g_threads);
+    auto edge = [&](uint64_t t, uint32_t &pre, uint32_t &dl) {
+      const uint64_t hh = splitmix64_h(seed ^ (t * 0x9E3779B97F4A7C15ull));
+      pre = (uint32_t)(((hh >> 32) * (uint64_t)nf) >> 32);
+      dl = d_min + (uint32_t)((hh & 0xffffffffull) % span);
+    };
+    std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(N, 0));
+    auto range = [&](int t, uint32_t &j0, uint32_t &j1) {
+      j0 = (uint32_t)((uint64_t)nt * t / T);
+      j1 = (uint32_t)((uint64_t)nt * (t + 1) / T);
+    };
+    auto count = [&](int t) {
+      uint32_t j0, j1;
+      range(t, j0, j1);
+      for (uint64_t e = (uint64_t)j0 * k_in; e < (uint64_t)j1 * k_in; ++e) {
+        uint32_t pre, dl;
+        edge(e, pre, dl);
+        cnt[t][fo + pre]++;
+      }
+    };
+    {
+      std::vector<std::thread> pool;
+      for (int t = 1; t < T; ++t) pool.emplace_back(count, t);
+      count(0);
+      for (auto &th : pool) th.join();
+    }
+    net.row_ptr.assign(N + 1, 0);
+    uint64_t cum = 0;
+    for (uint64_t i = 0; i < N; ++i) {
+      net.row_ptr[i] = (uint32_t)cum;
+      for (int t = 0; t < T; ++t) {
+        const uint32_t c = cnt[t][i];
+        cnt[t][i] = (uint32_t)cum;  // becomes the thread's write cursor
+        cum += c;
+      }
+    }
+    net.row_ptr[N] = (uint32_t)cum;
+    using TT = std::remove_reference_t<decltype(net.w[0])>;
+    net.col.assign(E, 0);
+    net.w.assign(E, (TT)0);
+    net.d.assign(E, 0);
+    net.st.assign(E, 0);
+    net.plastic.assign(E, 0);
+    auto fill = [&](int t) {
+      uint32_t j0, j1;
+      range(t, j0, j1);
+      for (uint64_t e = (uint64_t)j0 * k_in; e < (uint64_t)j1 * k_in; ++e) {
+        uint32_t pre, dl;
+        edge(e, pre, dl);
+        const uint64_t pos = cnt[t][fo + pre]++;
+        net.col[pos] = tof + (uint32_t)(e / k_in);
+        net.w[pos] = (TT)(pre < n_exc ? w_exc : w_inh);
+        net.d[pos] = (uint8_t)dl;
+      }
+    };
+    {
+      std::vector<std::thread> pool;
+      for (int t = 1; t < T; ++t) pool.emplace_back(fill, t);
+      fill(0);
+      for (auto &th : pool) th.join();
+    }
+    for (auto &sr : net.srcs)
+      for (auto st : sr.st)
+        if (st > net.kin.size()) return fail("Network::build: Poisson-source syn_type exceeds registered kinetics");
+    alloc_runtime(net);
+  });
+  return 0;
+}
+
 // P/api/net/network/build.rs:18-109
 int or_build(or_net *h) {
   DISPATCH(h, {

@@ -55,6 +55,11 @@ int or_poisson_connect(or_net *net, int src, int to, const uint32_t *posts,
 int or_stdp_config(or_net *net, float dt, float tau_pre, float tau_post,
                    float a_plus, float a_minus, float w_min, float w_max);
 int or_build(or_net *net);
+/* Fixed in-degree projection (the product's sg_connect_fixed_indegree
+   generator) + build, straight into the CSR; network must have no other edges. */
+int or_build_fixed_indegree(or_net *net, int from, int to, uint32_t k_in, uint64_t seed,
+                            uint32_t n_exc, float w_exc, float w_inh, uint32_t d_min,
+                            uint32_t d_max);
 /* Build straight from a CSR (reference: SparseGraph::from_csr). */
 int or_build_from_csr(or_net *net, const uint32_t *row_ptr, const uint32_t *col,
                       const float *w, const uint8_t *delay);
