@@ -181,6 +181,20 @@ int sg_footprint(sg_net *net, uint64_t *out);
 /* Device stream of the handle (cudaStream_t), for event timing. */
 int sg_stream(sg_net *net, void **out);
 
+/* ---- stand-alone operators on device buffers ------------------------------ */
+/* push_spikes(active, graph, delay, step), P/api/net/push.rs:126-173: for every
+   neuron in `active` (device, strictly ascending, as compact_spikes_into
+   returns) add each outgoing synapse's weight to
+   ring[(step + max(delay,1)) % 32][post], each ring cell in the reference's
+   order (bit-identical sums).  All arrays are device memory: a valid CSR
+   (row_ptr[n_neurons+1], col/weights/delays[row_ptr[n_neurons]]) and the
+   ring [32][n_neurons] floats.  `stream` is a cudaStream_t (NULL: legacy
+   default stream).  Scratch is allocated per call (cudaMalloc/cudaFree);
+   the call returns after the ring is updated. */
+int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
+                   const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
+                   uint32_t n_active, uint64_t step, float *ring, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

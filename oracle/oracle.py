@@ -83,6 +83,7 @@ def lib():
             "or_sg_expf": (f32, [f32]),
             "or_poisson_spike": (i32, [u32, u32, u64, f32]),
             "or_compact": (u64, [vp, u64, vp]),
+            "or_push_spikes": (i32, [vp, vp, vp, vp, u32, vp, u32, u64, vp]),
             "or_kuramoto_rk4": (i32, [i32, u32, vp, vp, f32, f32, u32, vp, vp]),
         }
         for name, (res, args) in sig.items():
@@ -296,6 +297,18 @@ def compact(spikes) -> np.ndarray:
     out = np.empty(s.size, np.uint32)
     k = lib().or_compact(_p(s), s.size, _p(out))
     return out[:k]
+
+
+def push_spikes(row_ptr, col, w, d, n_neurons, active, step, ring):
+    """push_spikes on plain arrays; `ring` ([32][n] float32) is updated in place."""
+    rp = np.ascontiguousarray(row_ptr, np.uint32)
+    c = np.ascontiguousarray(col, np.uint32)
+    ww = np.ascontiguousarray(w, np.float32)
+    dd = np.ascontiguousarray(d, np.uint8)
+    a = np.ascontiguousarray(active, np.uint32)
+    assert ring.dtype == np.float32 and ring.flags.c_contiguous
+    _chk(lib().or_push_spikes(_p(rp), _p(c), _p(ww), _p(dd), n_neurons, _p(a), a.size, step, _p(ring)))
+    return ring
 
 
 def kuramoto_rk4(theta0, omega, k, dt, n_steps, precision=1):

@@ -1175,6 +1175,23 @@ float or_sg_expf(float x) { return sg_expf(x); }
 int or_poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p) {
   return poisson_spike(seed, stream, step, p) ? 1 : 0;
 }
+// P/api/net/push.rs:126-173 push_spikes on plain arrays (static ring)
+int or_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *w, const uint8_t *dl,
+                   uint32_t n_neurons, const uint32_t *active, uint32_t n_active, uint64_t step,
+                   float *ring) {
+  for (uint32_t a = 0; a < n_active; ++a) {
+    const uint32_t pre = active[a];
+    if (pre >= n_neurons) return fail("push_spikes: active index out of range");
+    for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e) {
+      const uint32_t post = col[e];
+      if (post >= n_neurons) return fail("DelayBuffer::add: post index out of range");
+      const uint32_t slot = (uint32_t)((step + std::max<uint32_t>(dl[e], 1)) % kSlots);
+      ring[(size_t)slot * n_neurons + post] += w[e];
+    }
+  }
+  return 0;
+}
+
 uint64_t or_compact(const int32_t *spikes, uint64_t n, uint32_t *out) {
   uint64_t k = 0;
   for (uint64_t i = 0; i < n; ++i)

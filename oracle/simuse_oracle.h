@@ -84,6 +84,9 @@ float or_fast_exp(float x);
 float or_sg_expf(float x);
 int or_poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p);
 uint64_t or_compact(const int32_t *spikes, uint64_t n, uint32_t *out);
+int or_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *w,
+                   const uint8_t *delay, uint32_t n_neurons, const uint32_t *active,
+                   uint32_t n_active, uint64_t step, float *ring);
 
 /* ---- Kuramoto, mean-field RK4 (FP32 and FP64 twins) ---- */
 int or_kuramoto_rk4(int precision, uint32_t n, const float *theta0,
