@@ -267,3 +267,82 @@ extern "C" int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, cons
   });
 }
 
+// ---------------------------------------------------------------------------
+// sg_push_spikes_noalloc: the same operator for callers that cannot allocate
+// device memory while they run (a host inside a CUDA-graph capture that must
+// stay allocation-free, a real-time loop that forbids cudaMalloc, an embedding
+// with a fixed memory budget).  Its scratch is one file-scope __device__
+// array of fixed size that every GPU loading this library keeps until exit.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kNoAllocMaxEvents = 1u << 20;   // synaptic events per call
+constexpr uint32_t kNoAllocMaxNeurons = 1u << 23;  // 8,388,608 neurons
+constexpr uint32_t kNoAllocTiles = kNoAllocMaxNeurons >> kPushTileShift;  // 4096
+constexpr size_t kNoAllocCounterBytes = ((size_t)kNoAllocTiles * 3 + 1) * 4;
+constexpr size_t kNoAllocTotalOff = (kNoAllocCounterBytes + 255) & ~(size_t)255;
+constexpr size_t kNoAllocBinsOff = kNoAllocTotalOff + 256;
+constexpr size_t kNoAllocBytes = kNoAllocBinsOff + (size_t)kNoAllocMaxEvents * 12;  // ~12.1 MiB
+
+// In host code this name is only a stand-in: the device address comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_push_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Resolve the scratch array's device address on the current device (first
+// call per device only).
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  SG_CUDA(cudaGetDevice(&dev));
+  SG_REQUIRE(dev >= 0 && dev < kMaxDevices, SG_E_INVALID, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_push_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error(std::string("sg_push_spikes_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+      return SG_E_CUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return SG_OK;
+}
+
+}  // namespace
+
+extern "C" int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
+                                      const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
+                                      uint32_t n_active, uint64_t step, float *ring, void *stream) {
+  return guarded([&]() -> int {
+    push_check_args(row_ptr, col, weights, delays, n_neurons, active, n_active, ring);
+    SG_REQUIRE(n_neurons <= kNoAllocMaxNeurons, SG_E_INVALID,
+               "sg_push_spikes_noalloc: n_neurons " + std::to_string(n_neurons) + " exceeds the maximum " +
+                   std::to_string(kNoAllocMaxNeurons));
+    void *base = nullptr;
+    const int rc0 = noalloc_scratch(&base);
+    if (rc0 != SG_OK) return rc0;
+    unsigned char *b = (unsigned char *)base;
+    PushScratch s{};
+    s.tile_cnt = (uint32_t *)b;
+    s.tile_cur = s.tile_cnt + kNoAllocTiles;
+    s.tile_base = s.tile_cur + kNoAllocTiles;
+    s.total = (unsigned long long *)(b + kNoAllocTotalOff);
+    return push_run(row_ptr, col, weights, delays, n_neurons, active, n_active, step, ring, (cudaStream_t)stream, s,
+                    [&](unsigned long long total, PushScratch &sc) -> int {
+                      if (total > kNoAllocMaxEvents) {
+                        set_error("sg_push_spikes_noalloc: " + std::to_string(total) +
+                                  " synaptic events exceed the maximum " + std::to_string(kNoAllocMaxEvents) +
+                                  " per call; the ring was not modified");
+                        return SG_E_OVERFLOW;
+                      }
+                      sc.bkey = (uint32_t *)(b + kNoAllocBinsOff);
+                      sc.bw = (float *)(sc.bkey + kNoAllocMaxEvents);
+                      sc.bcell = (uint32_t *)(sc.bw + kNoAllocMaxEvents);
+                      return SG_OK;
+                    });
+  });
+}

@@ -73,6 +73,7 @@ SIGNATURES = {
     "sg_footprint": [vp, vp],
     "sg_stream": [vp, vp],
     "sg_push_spikes": [vp, vp, vp, vp, u32, vp, u32, u64, vp, vp],
+    "sg_push_spikes_noalloc": [vp, vp, vp, vp, u32, vp, u32, u64, vp, vp],
 }
 
 _lib = None

@@ -195,6 +195,23 @@ int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *we
                    const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
                    uint32_t n_active, uint64_t step, float *ring, void *stream);
 
+/* No counterpart in the reference.  sg_push_spikes without any device
+   allocation, for callers that cannot call cudaMalloc while they run (a host
+   loop that must stay allocation-free during CUDA-graph capture, a real-time
+   thread, an embedding with a fixed memory budget).  Same arguments and
+   results as sg_push_spikes.  Its scratch is one file-scope __device__ array
+   of about 12.1 MiB that every GPU loading this library holds until the
+   process exits.  Limits: n_neurons <= 8,388,608 and at most 1,048,576
+   synaptic events per call (the sum of the active rows' lengths); larger
+   inputs return SG_E_INVALID / SG_E_OVERFLOW before the ring is touched.
+   The first call on a device resolves the array's address on that device
+   (cudaGetSymbolAddress), so make that first call before any stream capture.
+   Every call shares the one array: calls that overlap on the GPU (other
+   streams, other host threads) race and must be serialised by the caller. */
+int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
+                           const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
+                           uint32_t n_active, uint64_t step, float *ring, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
