@@ -46,11 +46,10 @@ sys.path.insert(0, os.path.join(ROOT, "dioma-core_b200"))
 METRIC = "synaptic events/s"
 UNIT = "events/s"
 
-# algorithmic bytes: LIF neuron = v, refr read+write (16 B),
-# ring slot read + clear (8 B), spike bit (1/8 B); per event col 4 + weight 4
-# + delay 1 (expand) and ring read-modify-write 8 (apply); per spike the
-# active-list write+read and two row_ptr reads (16 B); per Poisson source
-# rate + seed reads (8 B).
+# algorithmic bytes: LIF neuron = v, refr read+write (16 B), ring slot read +
+# clear (8 B), spike bit (1/8 B); per event col 4 + weight 4 + delay 1 and
+# the ring read-modify-write 8; per spike the spike-list write+read and the
+# row start (16 B); per Poisson source rate + seed reads (8 B).
 B_NEURON = 24.125
 B_EVENT_EXPAND = 9.0
 B_EVENT_APPLY = 8.0
@@ -301,14 +300,12 @@ def run_ours(args):
     p_events = (net.events_total - ev0) / p_steps
     sp, _ = net.read_stats()
     p_spikes = float(sp[-p_steps:].mean()) if sp.size else 0.0
-    phases = ["neuron_kernel<LIF>", "expand_kernel", "stdp_ltp_kernel", "apply_kernel"]
+    phases = ["neuron_kernel<LIF>", "scatter_kernel"]
     n_src = spec["n"]
     alg = [spec["n"] * B_NEURON,
-           p_events * B_EVENT_EXPAND + p_spikes * B_SPIKE + n_src * B_SOURCE,
-           0.0,
-           p_events * B_EVENT_APPLY]
-    per_launch_ms = [ph_ms[i] / max(int(ph_launch[i]), 1) for i in range(4)]
-    dom = int(np.argmax(ph_ms))
+           p_events * (B_EVENT_EXPAND + B_EVENT_APPLY) + p_spikes * B_SPIKE + n_src * B_SOURCE]
+    per_launch_ms = [ph_ms[i] / max(int(ph_launch[i]), 1) for i in range(2)]
+    dom = int(np.argmax(ph_ms[:2]))
     peak, peak_kind = measured_peak()
     achieved = alg[dom] / (per_launch_ms[dom] / 1e3) / 1e9
     step_alg = sum(alg)
@@ -339,7 +336,7 @@ def run_ours(args):
                      "alg_bytes_per_launch": alg[dom], "launch_ms": per_launch_ms[dom],
                      "phases_ms_per_launch": dict(zip(phases, per_launch_ms))},
         "clocks": clk.summary(),
-        "gpu_launches": int(args.steps * S * 3),
+        "gpu_launches": int(args.steps * S * 2),
     }
     if not args.no_cpu_baseline and world == 1:
         cnet, cores, build_s = cpu_baseline(args, spec, args.cpu_seconds)

@@ -63,16 +63,32 @@ __device__ __forceinline__ float sg_expf(float x) {
   return (p * __int_as_float((k1 + 127) << 23)) * __int_as_float((k2 + 127) << 23);
 }
 
+// One neuron held in registers: state loaded/stored by the caller (128-bit
+// accesses of 4 neighbours), parameters uniform or loaded per neuron.
+template <int NS, int NP> struct RegNeuron {
+  mutable float s[NS];
+  float p[NP];
+  __device__ __forceinline__ float &st(int c) const { return s[c]; }
+  __device__ __forceinline__ float pr(int c) const { return p[c]; }
+};
+
+// One neuron's view of its population's SoA arrays.  Parameter columns that
+// hold one value for the whole population are passed as kernel arguments
+// (bit c of umask) instead of being read per neuron.
 struct Soa {
-  float *s;        // state [col][cap]
-  const float *p;  // params [col][cap]
+  float *s;            // state [col][cap]
+  const float *p;      // params [col][cap]
   uint32_t cap, i;
+  uint32_t umask;
+  const float *uval;
   __device__ __forceinline__ float &st(int c) const { return s[(size_t)c * cap + i]; }
-  __device__ __forceinline__ float pr(int c) const { return __ldg(&p[(size_t)c * cap + i]); }
+  __device__ __forceinline__ float pr(int c) const {
+    return ((umask >> c) & 1u) ? uval[c] : __ldg(&p[(size_t)c * cap + i]);
+  }
 };
 
 // P/zoo/neurons/lif.rs:47-78
-__device__ __forceinline__ bool lif_step(const Soa &c, float i_syn, float dt) {
+template <class A> __device__ __forceinline__ bool lif_step(const A &c, float i_syn, float dt) {
   float v = c.st(0), refr = c.st(1);
   const float inv_tau = c.pr(1), v_rest = c.pr(2), v_th = c.pr(3), v_reset = c.pr(4),
               tau_ref = c.pr(5);
@@ -89,7 +105,7 @@ __device__ __forceinline__ bool lif_step(const Soa &c, float i_syn, float dt) {
 
 // P/zoo/neurons/izhikevich.rs:71-125 (two 0.5*dt Euler half-steps on v,
 // du from the pre-integration v, refractory freezes v at c)
-__device__ __forceinline__ bool izh_step(const Soa &c, float i_syn, float dt) {
+template <class A> __device__ __forceinline__ bool izh_step(const A &c, float i_syn, float dt) {
   const float vs = c.st(0), u = c.st(1), refr = c.st(2);
   const float a = c.pr(1), b = c.pr(2), cc = c.pr(3), d = c.pr(4), tau_ref = c.pr(5),
               v_th = c.pr(6);
@@ -145,8 +161,8 @@ __device__ __forceinline__ float gp_tau2(float v, float t0, float t1, float th1,
 
 // ln(NAI/NAO) and ln(KO/KI) are constants; the host evaluates them once
 // with the reference's libm ln and passes them in (P/zoo/neurons/gpea.rs:273-278).
-__device__ __forceinline__ bool gpea_step(const Soa &c, float i_syn, float dt, float ln_na,
-                                          float ln_k) {
+template <class A>
+__device__ __forceinline__ bool gpea_step(const A &c, float i_syn, float dt, float ln_na, float ln_k) {
   using namespace gp;
   const float celsius = c.pr(1);
   const float rt = GAS_R * (273.0f + celsius - 9.5f) / CA_FARADAY * 1000.0f;
@@ -240,7 +256,7 @@ __device__ __forceinline__ void hh_deriv(const HHp &P, float v, float m, float h
   dh = ah * (1.0f - h) - bh * h;
   dn = an * (1.0f - n) - bn * n;
 }
-__device__ __forceinline__ bool hh_step(const Soa &c, float i_syn, float dt) {
+template <class A> __device__ __forceinline__ bool hh_step(const A &c, float i_syn, float dt) {
   const HHp P{c.pr(1), c.pr(2), c.pr(3), c.pr(4), c.pr(5), c.pr(6), c.pr(7), c.pr(8) + i_syn};
   const float v_th = c.pr(9);
   const float v = c.st(0), m = c.st(1), h = c.st(2), n = c.st(3);

@@ -75,6 +75,8 @@ template <typename T> struct DVec {
 struct HostPop {
   int model;
   uint32_t n, cap, dev_off, np, ns;
+  uint32_t umask = 0;   // uniform parameter columns
+  float uval[16] = {};
   std::vector<float> params, state;  // before build
   DBuf<float> d_params, d_state;     // after build
 };
@@ -116,20 +118,22 @@ struct sg_net {
 
   // device state
   DBuf<unsigned long long> d_step, d_ev_step, d_ev_total, d_clamp, d_stat_ev;
-  DBuf<uint32_t> d_n_active, d_active, d_last_bits, d_raster, d_done, d_stat_spk;
+  DBuf<uint32_t> d_blk_cnt, d_last_bits, d_raster, d_done, d_stat_spk;
+  DBuf<uint2> d_spk;
   DBuf<float> d_ring, d_kin_g;
   DBuf<uint32_t> d_row_ptr, d_col;
   DBuf<float> d_w;
   DBuf<uint8_t> d_code;
   uint64_t n_edges = 0;
-  DBuf<float> d_src_p, d_src_w;
-  DBuf<uint32_t> d_src_seed, d_src_ptr, d_src_post;
-  DBuf<uint8_t> d_src_code;
+  // per-row segment table [Nd][G+1] (u16, or u32 when a row is >= 65536 long)
+  DBuf<uint8_t> d_seg;
+  int seg32 = 0;
+  uint32_t G = 0, P = 0, pbits = 0;
+  // Poisson sources and their synapses grouped by scatter block
+  DBuf<float> d_src_p, d_se_w;
+  DBuf<uint32_t> d_src_seed, d_src_lo, d_se_src, d_se_post;
+  DBuf<uint8_t> d_se_code;
   uint64_t n_src_edges = 0;
-  DBuf<unsigned long long> d_bin_base;
-  DBuf<uint32_t> d_bin_cnt, d_bkey, d_bcell;
-  DBuf<float> d_bw;
-  uint32_t tshift = 11, n_tiles = 0, hbits = 13;
   DBuf<float> d_x_pre, d_x_post;
   DBuf<uint32_t> d_in_ptr, d_in_edge, d_in_pre;
   DBuf<double> d_drift;
@@ -140,13 +144,12 @@ struct sg_net {
   uint32_t stat_cap = 1u << 16;
   uint64_t stat_read_step = 0;
   uint64_t host_step = 0;  // steps issued
-  int apply_blocks = 0, expand_blocks = 0, src_blocks = 0;
-  size_t apply_smem = 0;
+  size_t scatter_smem = 0;
   // CUDA graph of `graph_steps` steps
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_steps = 0;
   std::vector<float> ln_consts{0, 0};
-  // per-phase CUDA-event timing (neuron, expand, stdp_ltp, apply)
+  // per-phase CUDA-event timing (0 neuron update, 1 scatter)
   bool profile = false;
   std::vector<cudaEvent_t> prof_ev;
   double prof_ms[4] = {0, 0, 0, 0};
@@ -200,8 +203,9 @@ void require_pop(const sg_net *net, uint32_t pop) {
 StepArgs make_args(sg_net *net) {
   StepArgs a{};
   a.step = net->d_step.p;
-  a.n_active = net->d_n_active.p;
-  a.active = net->d_active.p;
+  a.blk_cnt = net->d_blk_cnt.p;
+  a.spk = net->d_spk.p;
+  a.n_blk = net->Nd / kNeuronBlock;
   a.last_bits = net->d_last_bits.p;
   a.raster = net->raster_cap ? net->d_raster.p : nullptr;
   a.raster_cap = net->raster_cap ? net->raster_cap : 1;
@@ -226,21 +230,18 @@ StepArgs make_args(sg_net *net) {
   a.w = net->d_w.p;
   a.code = net->d_code.p;
   a.n_edges = (uint32_t)net->n_edges;
-  a.n_src = (uint32_t)net->srcs.size();
+  a.seg = net->d_seg.p;
+  a.seg32 = net->seg32;
+  a.G = net->G;
+  a.P = net->P;
+  a.pbits = net->pbits;
   a.src_p = net->d_src_p.p;
   a.src_seed = net->d_src_seed.p;
-  a.src_ptr = net->d_src_ptr.p;
-  a.src_post = net->d_src_post.p;
-  a.src_w = net->d_src_w.p;
-  a.src_code = net->d_src_code.p;
-  a.tshift = net->tshift;
-  a.n_tiles = net->n_tiles;
-  a.hbits = net->hbits;
-  a.bin_base = net->d_bin_base.p;
-  a.bin_cnt = net->d_bin_cnt.p;
-  a.bkey = net->d_bkey.p;
-  a.bw = net->d_bw.p;
-  a.bcell = net->d_bcell.p;
+  a.src_lo = net->d_src_lo.p;
+  a.se_src = net->d_se_src.p;
+  a.se_post = net->d_se_post.p;
+  a.se_w = net->d_se_w.p;
+  a.se_code = net->d_se_code.p;
   a.deterministic = net->deterministic;
   a.stdp = net->stdp_on ? 1 : 0;
   a.x_pre = net->d_x_pre.p;
@@ -285,6 +286,32 @@ float host_fast_exp(float x) {
 // ---------------------------------------------------------------------------
 // build kernels
 // ---------------------------------------------------------------------------
+__global__ void sort_key_kernel(const uint32_t *pre, const uint32_t *post, unsigned long long *key, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    key[i] = ((unsigned long long)pre[i] << 32) | post[i];
+}
+// Segment table: entry j of row `pre` = first position in the row whose post
+// is >= j*P (rows are sorted by post), entry G = row length.
+template <typename T>
+__global__ void seg_table_kernel(const uint32_t *row_ptr, const uint32_t *col, uint32_t Nd, uint32_t G, uint32_t P,
+                                 T *seg) {
+  for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x) {
+    const uint32_t beg = row_ptr[pre], end = row_ptr[pre + 1];
+    T *out = seg + (size_t)pre * (G + 1);
+    uint32_t lo = beg;
+    for (uint32_t j = 0; j < G; ++j) {
+      const uint32_t bound = j * P;
+      uint32_t hi = end;
+      while (lo < hi) {  // lower_bound of bound in [lo, end)
+        const uint32_t mid = (lo + hi) >> 1;
+        if (col[mid] < bound) lo = mid + 1;
+        else hi = mid;
+      }
+      out[j] = (T)(lo - beg);
+    }
+    out[G] = (T)(end - beg);
+  }
+}
 __global__ void iota_kernel(uint32_t *v, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     v[i] = (uint32_t)i;
@@ -446,9 +473,10 @@ void upload_staged_edges(sg_net *net, const uint32_t *pre, const uint32_t *post,
   net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
 }
 
-// Stable sort of the staged edges by pre (graph.rs:142-147; the reference
-// sort is unstable, this one keeps insertion order inside a row), then the
-// u32 row_ptr (graph.rs:149-180).
+// Sort of the staged edges by (pre, post), stable (graph.rs:142-147 sorts by
+// pre only, unstably, so the order inside a row is not part of the reference
+// contract).  Keeping repeated (pre, post) synapses in insertion order keeps
+// every ring cell's summation order.  Then the u32 row_ptr (graph.rs:149-180).
 void build_graph(sg_net *net) {
   cudaStream_t s = net->stream;
   const uint64_t E = net->e_pre.n;
@@ -462,27 +490,33 @@ void build_graph(sg_net *net) {
   cnt.alloc((size_t)Nd + 1);
   cnt.zero(s);
   if (E > 0) {
-    DBuf<uint32_t> keys_out, vals_in, vals_out;
+    DBuf<unsigned long long> keys_in, keys_out;
+    DBuf<uint32_t> vals_in, vals_out;
+    keys_in.alloc(E);
     keys_out.alloc(E);
     vals_in.alloc(E);
     vals_out.alloc(E);
+    launch_grid(E, [&](unsigned b) { sort_key_kernel<<<b, 256, 0, s>>>(net->e_pre.p, net->e_post.p, keys_in.p, E); });
     launch_grid(E, [&](unsigned b) { iota_kernel<<<b, 256, 0, s>>>(vals_in.p, E); });
-    int end_bit = 1;
-    while (end_bit < 32 && (1ull << end_bit) < (uint64_t)Nd) ++end_bit;
+    int nb = 1;
+    while (nb < 32 && (1ull << nb) < (uint64_t)Nd) ++nb;
+    const int end_bit = 32 + nb;
     size_t temp_bytes = 0;
-    SG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, net->e_pre.p, keys_out.p, vals_in.p,
-                                            vals_out.p, (int64_t)E, 0, end_bit, s));
+    SG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys_in.p, keys_out.p, vals_in.p, vals_out.p,
+                                            (int64_t)E, 0, end_bit, s));
     DBuf<uint8_t> temp;
     temp.alloc(std::max<size_t>(temp_bytes, 1));
-    SG_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, temp_bytes, net->e_pre.p, keys_out.p, vals_in.p,
-                                            vals_out.p, (int64_t)E, 0, end_bit, s));
+    SG_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, temp_bytes, keys_in.p, keys_out.p, vals_in.p, vals_out.p,
+                                            (int64_t)E, 0, end_bit, s));
     temp.release();
+    keys_in.release();
+    keys_out.release();
     vals_in.release();
     launch_grid(E, [&](unsigned b) {
       gather_edges_kernel<<<b, 256, 0, s>>>(vals_out.p, net->e_post.p, net->e_w.p, net->e_code.p,
                                             net->d_col.p, net->d_w.p, net->d_code.p, E);
     });
-    launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(keys_out.p, E, 0, cnt.p); });
+    launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->e_pre.p, E, 0, cnt.p); });
     SG_CUDA(cudaStreamSynchronize(s));
   }
   net->e_pre.release();
@@ -501,62 +535,70 @@ void build_graph(sg_net *net) {
   SG_CUDA(cudaStreamSynchronize(s));
 }
 
-// Bins: tile t holds at most (in-degree of its posts, neuron + source
-// synapses) events per step, since every synapse fires at most once per step.
-void build_bins(sg_net *net) {
+// Scatter geometry and the per-row segment table.
+void build_segments(sg_net *net) {
   cudaStream_t s = net->stream;
   const uint32_t Nd = net->Nd;
-  // tile size: 2^tshift posts (whole network when small)
-  uint32_t ts = 11;
-  while (ts > 5 && (1u << ts) > Nd * 2) --ts;
-  net->tshift = ts;
-  net->n_tiles = (Nd + (1u << ts) - 1) >> ts;
-  net->hbits = 13;
-  DBuf<unsigned long long> cnt;
-  cnt.alloc((size_t)net->n_tiles + 1);
-  cnt.zero(s);
-  if (net->n_edges)
-    launch_grid(net->n_edges, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->d_col.p, net->n_edges, ts, cnt.p); });
-  if (net->n_src_edges)
-    launch_grid(net->n_src_edges, [&](unsigned b) {
-      histogram_kernel<<<b, 256, 0, s>>>(net->d_src_post.p, net->n_src_edges, ts, cnt.p);
-    });
-  net->d_bin_base.alloc((size_t)net->n_tiles + 1);
-  size_t tb = 0;
-  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, net->d_bin_base.p, (int64_t)net->n_tiles + 1, s));
-  DBuf<uint8_t> temp;
-  temp.alloc(std::max<size_t>(tb, 1));
-  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, net->d_bin_base.p, (int64_t)net->n_tiles + 1, s));
-  const uint64_t tot = net->n_edges + net->n_src_edges;
-  net->d_bin_cnt.alloc(net->n_tiles);
-  net->d_bin_cnt.zero(s);
-  net->d_bkey.alloc(std::max<uint64_t>(tot, 1));
-  net->d_bw.alloc(std::max<uint64_t>(tot, 1));
-  net->d_bcell.alloc(std::max<uint64_t>(tot, 1));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+  uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)sms, Nd / 32));
+  uint32_t P = std::max<uint32_t>(32, (uint32_t)align_up((Nd + G - 1) / G, 32));
+  G = std::max<uint32_t>(1, (Nd + P - 1) / P);
+  net->G = G;
+  net->P = P;
+  uint32_t pb = 1;
+  while ((1u << pb) < P) ++pb;
+  net->pbits = pb;
+  SG_REQUIRE(((uint64_t)(4 * kSlots) << pb) < 0xFFFFFFFFull, SG_E_INVALID, "network too large for the cell encoding");
+  // longest row decides the table width
+  std::vector<uint32_t> rp((size_t)Nd + 1);
+  SG_CUDA(cudaMemcpyAsync(rp.data(), net->d_row_ptr.p, rp.size() * 4, cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  uint32_t longest = 0;
+  for (uint32_t i = 0; i < Nd; ++i) longest = std::max(longest, rp[i + 1] - rp[i]);
+  net->seg32 = longest >= 65536 ? 1 : 0;
+  const size_t esz = net->seg32 ? 4 : 2;
+  net->d_seg.alloc(std::max<size_t>((size_t)Nd * (G + 1) * esz, 1));
+  launch_grid(Nd, [&](unsigned b) {
+    if (net->seg32)
+      seg_table_kernel<uint32_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, Nd, G, P, (uint32_t *)net->d_seg.p);
+    else
+      seg_table_kernel<uint16_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, Nd, G, P, (uint16_t *)net->d_seg.p);
+  });
+  SG_CUDA(cudaGetLastError());
   SG_CUDA(cudaStreamSynchronize(s));
 }
 
+// Poisson sources: rate and seed per source; their synapses grouped by the
+// scatter block that owns the post, each group in (source, connect) order.
 void build_sources(sg_net *net) {
   const size_t S = net->srcs.size();
-  std::vector<float> p(S), w;
-  std::vector<uint32_t> seed(S), ptr(S + 1, 0), post;
-  std::vector<uint8_t> code;
+  const uint32_t G = net->G, P = net->P;
+  std::vector<float> p(S);
+  std::vector<uint32_t> seed(S);
+  std::vector<uint64_t> cnt((size_t)G + 1, 0);
   uint64_t tot = 0;
   for (size_t i = 0; i < S; ++i) {
     p[i] = net->srcs[i].p;
     seed[i] = net->srcs[i].seed;
-    ptr[i] = (uint32_t)tot;
+    for (uint32_t q : net->srcs[i].post) cnt[q / P]++;
     tot += net->srcs[i].post.size();
   }
   SG_REQUIRE(tot < 0xFFFFFFFFull, SG_E_OVERFLOW, "too many Poisson-source synapses");
-  ptr[S] = (uint32_t)tot;
-  post.reserve(tot);
-  w.reserve(tot);
-  code.reserve(tot);
-  for (auto &sr : net->srcs) {
-    post.insert(post.end(), sr.post.begin(), sr.post.end());
-    w.insert(w.end(), sr.w.begin(), sr.w.end());
-    code.insert(code.end(), sr.code.begin(), sr.code.end());
+  std::vector<uint32_t> lo((size_t)G + 1, 0);
+  for (uint32_t j = 0; j < G; ++j) lo[j + 1] = lo[j] + (uint32_t)cnt[j];
+  std::vector<uint32_t> cur(lo.begin(), lo.end() - 1), se_src(tot), se_post(tot);
+  std::vector<float> se_w(tot);
+  std::vector<uint8_t> se_code(tot);
+  for (size_t i = 0; i < S; ++i) {
+    const auto &sr = net->srcs[i];
+    for (size_t k = 0; k < sr.post.size(); ++k) {
+      const uint32_t pos = cur[sr.post[k] / P]++;
+      se_src[pos] = (uint32_t)i;
+      se_post[pos] = sr.post[k];
+      se_w[pos] = sr.w[k];
+      se_code[pos] = sr.code[k];
+    }
   }
   net->n_src_edges = tot;
   auto up = [&](auto &buf, const auto &vec) {
@@ -566,10 +608,11 @@ void build_sources(sg_net *net) {
   };
   up(net->d_src_p, p);
   up(net->d_src_seed, seed);
-  up(net->d_src_ptr, ptr);
-  up(net->d_src_post, post);
-  up(net->d_src_w, w);
-  up(net->d_src_code, code);
+  up(net->d_src_lo, lo);
+  up(net->d_se_src, se_src);
+  up(net->d_se_post, se_post);
+  up(net->d_se_w, se_w);
+  up(net->d_se_code, se_code);
   SG_CUDA(cudaStreamSynchronize(net->stream));
   for (auto &sr : net->srcs) {  // host copies are no longer needed
     std::vector<uint32_t>().swap(sr.post);
@@ -619,12 +662,26 @@ void build_stdp(sg_net *net) {
   net->ln_consts[3] = host_fast_exp(-net->stdp_dt / net->tau_post);
 }
 
+void compute_uniform(HostPop &p) {
+  p.umask = 0;
+  for (uint32_t c = 0; c < p.np && c < 16; ++c) {
+    const float *col = p.params.data() + (size_t)c * p.cap;
+    bool uni = p.n > 0;
+    for (uint32_t i = 1; i < p.n && uni; ++i) uni = std::memcmp(&col[i], &col[0], 4) == 0;
+    if (uni) {
+      p.umask |= 1u << c;
+      p.uval[c] = col[0];
+    }
+  }
+}
+
 void finish_build(sg_net *net) {
   cudaStream_t s = net->stream;
   const uint32_t Nd = net->Nd;
   SG_REQUIRE(net->kin.size() <= 3, SG_E_INVALID, "at most 3 kinetic profiles are supported on the device path");
   // populations -> device
   for (auto &p : net->pops) {
+    compute_uniform(p);
     p.d_params.alloc(std::max<size_t>(p.params.size(), 1));
     p.d_state.alloc(std::max<size_t>(p.state.size(), 1));
     if (!p.params.empty())
@@ -644,9 +701,9 @@ void finish_build(sg_net *net) {
   net->d_kin_g.zero(s);
   net->d_step.alloc(1);
   net->d_step.zero(s);
-  net->d_n_active.alloc(1);
-  net->d_n_active.zero(s);
-  net->d_active.alloc(std::max<uint32_t>(Nd, 1));
+  net->d_blk_cnt.alloc(std::max<uint32_t>(Nd / kNeuronBlock, 1));
+  net->d_blk_cnt.zero(s);
+  net->d_spk.alloc(std::max<uint32_t>(Nd, 1));
   net->d_last_bits.alloc(std::max<uint32_t>(Nd / 32, 1));
   net->d_last_bits.zero(s);
   net->d_done.alloc(1);
@@ -661,23 +718,28 @@ void finish_build(sg_net *net) {
   net->d_stat_spk.zero(s);
   net->d_stat_ev.alloc(net->stat_cap);
   net->d_stat_ev.zero(s);
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
-  net->apply_blocks = (int)std::min<uint32_t>(net->n_tiles, (uint32_t)sms * 4);
-  net->apply_smem = (size_t)4 << net->hbits;
-  SG_CUDA(cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)net->apply_smem));
-  net->src_blocks = (int)((net->srcs.size() + 255) / 256);
-  net->expand_blocks = sms * 8;
+  net->scatter_smem = sizeof(ScatterSmem);
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)net->scatter_smem));
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)net->scatter_smem));
   SG_CUDA(cudaStreamSynchronize(s));
   net->built = true;
 }
 
 template <int M> void launch_neuron(sg_net *net, const StepArgs &a, HostPop &p) {
-  PopArgs pa{p.d_state.p, p.d_params.p, p.n, p.cap, p.dev_off, net->ln_consts[0], net->ln_consts[1]};
-  const unsigned blocks = (p.cap + 255) / 256;
-  neuron_kernel<M><<<blocks, 256, 0, net->stream>>>(a, pa);
+  PopArgs pa{};
+  pa.state = p.d_state.p;
+  pa.params = p.d_params.p;
+  pa.n = p.n;
+  pa.cap = p.cap;
+  pa.dev_off = p.dev_off;
+  pa.umask = p.umask;
+  for (int c = 0; c < 16; ++c) pa.uval[c] = p.uval[c];
+  pa.ln_na = net->ln_consts[0];
+  pa.ln_k = net->ln_consts[1];
+  neuron_kernel<M><<<p.cap / kNeuronBlock, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, pa);
 }
 
+// Phases: 0 neuron update (all populations), 1 scatter.
 void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
   cudaStream_t s = net->stream;
   if (ev) SG_CUDA(cudaEventRecord(ev[0], s));
@@ -691,12 +753,9 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
     }
   }
   if (ev) SG_CUDA(cudaEventRecord(ev[1], s));
-  expand_kernel<<<net->src_blocks + net->expand_blocks, 256, 0, s>>>(a, (uint32_t)net->src_blocks);
+  if (net->seg32) scatter_kernel<true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+  else scatter_kernel<false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
   if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
-  if (net->stdp_on) stdp_ltp_kernel<<<net->expand_blocks, 256, 0, s>>>(a);
-  if (ev) SG_CUDA(cudaEventRecord(ev[3], s));
-  apply_kernel<<<net->apply_blocks, 512, net->apply_smem, s>>>(a);
-  if (ev) SG_CUDA(cudaEventRecord(ev[4], s));
 }
 
 // Profiled steps: eager launches with CUDA events between the phases, read
@@ -704,17 +763,19 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
 void do_steps_profiled(sg_net *net, uint32_t n) {
   const StepArgs a = make_args(net);
   if (net->prof_ev.empty()) {
-    net->prof_ev.resize(5);
+    net->prof_ev.resize(3);
     for (auto &e : net->prof_ev) SG_CUDA(cudaEventCreate(&e));
   }
+  size_t n_launch_pops = 0;
+  for (auto &p : net->pops) n_launch_pops += p.n ? 1 : 0;
   for (uint32_t k = 0; k < n; ++k) {
     enqueue_step(net, a, net->prof_ev.data());
-    SG_CUDA(cudaEventSynchronize(net->prof_ev[4]));
-    for (int ph = 0; ph < 4; ++ph) {
+    SG_CUDA(cudaEventSynchronize(net->prof_ev[2]));
+    for (int ph = 0; ph < 2; ++ph) {
       float ms = 0;
       SG_CUDA(cudaEventElapsedTime(&ms, net->prof_ev[ph], net->prof_ev[ph + 1]));
       net->prof_ms[ph] += ms;
-      if (ph != 2 || net->stdp_on) net->prof_launches[ph] += (ph == 0 ? net->pops.size() : 1);
+      net->prof_launches[ph] += ph == 0 ? n_launch_pops : 1;
     }
   }
   SG_CUDA(cudaGetLastError());
@@ -833,7 +894,7 @@ int sg_pop_add(sg_net *net, int model, uint32_t n, uint32_t *out_pop) {
     HostPop p;
     p.model = model;
     p.n = n;
-    p.cap = (uint32_t)align_up(n, 32);
+    p.cap = (uint32_t)align_up(n, kNeuronBlock);
     p.dev_off = net->Nd;
     p.np = n_params(model);
     p.ns = n_state(model);
@@ -874,8 +935,21 @@ static int pop_write(sg_net *net, uint32_t pop, uint32_t col, bool param, const 
       src = tmp.data();
     }
     float *dst = (param ? p.d_params.p : p.d_state.p) + (size_t)col * p.cap;
-    SG_CUDA(cudaMemcpyAsync(dst, src, (size_t)p.n * 4, cudaMemcpyHostToDevice, net->stream));
     SG_CUDA(cudaStreamSynchronize(net->stream));
+    SG_CUDA(cudaMemcpy(dst, src, (size_t)p.n * 4, cudaMemcpyHostToDevice));
+    if (param && col < 16) {
+      // keep the uniform-column summary in step with the device copy; the
+      // captured step graph bakes it in, so it is re-captured
+      bool uni = p.n > 0;
+      for (uint32_t i = 1; i < p.n && uni; ++i) uni = std::memcmp(&src[i], &src[0], 4) == 0;
+      if (uni) {
+        p.umask |= 1u << col;
+        p.uval[col] = src[0];
+      } else {
+        p.umask &= ~(1u << col);
+      }
+      drop_graph(net);
+    }
   });
 }
 
@@ -1117,8 +1191,8 @@ int sg_build(sg_net *net) {
     SG_REQUIRE(E + src_e < 0xFFFFFFFFull, SG_E_OVERFLOW,
                "SparseGraph: too many synapses for a u32 CSR row_ptr / event key");
     build_graph(net);
+    build_segments(net);
     build_sources(net);
-    build_bins(net);
     if (net->stdp_on) build_stdp(net);
     finish_build(net);
   });
@@ -1523,12 +1597,15 @@ int sg_clamp_hits(sg_net *net, uint64_t *out) {
 int sg_footprint(sg_net *net, uint64_t *out) {
   NET_CHECK(net);
   return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
     uint64_t b = 0;
     for (auto &p : net->pops) b += (p.d_params.n + p.d_state.n) * 4;
     b += net->d_ring.n * 4 + net->d_kin_g.n * 4 + net->d_row_ptr.n * 4 + net->d_col.n * 4 + net->d_w.n * 4 +
-         net->d_code.n + net->d_bkey.n * 4 + net->d_bw.n * 4 + net->d_bcell.n * 4 + net->d_active.n * 4 +
-         net->d_src_post.n * 4 + net->d_src_w.n * 4 + net->d_src_code.n + net->d_src_p.n * 4 +
-         net->d_src_seed.n * 4 + net->d_src_ptr.n * 4 + net->d_raster.n * 4 + net->d_in_edge.n * 8;
+         net->d_code.n + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
+         net->d_src_p.n * 4 + net->d_src_seed.n * 4 + net->d_src_lo.n * 4 + net->d_se_src.n * 4 +
+         net->d_se_post.n * 4 + net->d_se_w.n * 4 + net->d_se_code.n + net->d_raster.n * 4 +
+         (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
+         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4;
     *out = b;
   });
 }

@@ -1,31 +1,33 @@
 // step_kernels.cuh — the device side of one simulation step.
 //
-// One step of the reference (P/api/net/network/step.rs:18-189) runs as three
+// One step of the reference (P/api/net/network/step.rs:18-189) runs as two
 // kernels on the network's stream:
 //
-//   neuron_kernel<M>  one thread per neuron (one launch per population):
+//   neuron_kernel<M>  one thread per neuron, one launch per population:
 //                     read + clear the current ring slot (and the kinetic
 //                     rings), integrate the model, ballot the spikes into a
-//                     bitmask word per warp, append spiking neurons to the
-//                     active list, update STDP traces.
-//   expand_kernel     one warp per spiking neuron walks its outgoing CSR row
-//                     (coalesced), one thread per Poisson source rolls the
-//                     source; every synaptic event (edge id, weight, target
-//                     cell) is appended to the bin of its post tile.  Pair-STDP
-//                     depression of the walked edges is fused here.
-//   apply_kernel      one block per post tile applies the tile's events to
-//                     the ring in the reference's summation order.
+//                     bitmask word per warp, write the block's spiking
+//                     neurons in ascending order to its slot of the spike
+//                     list (no global atomics), update the STDP traces.
+//   scatter_kernel    one persistent block per SM; block j owns the posts
+//                     [j*P, (j+1)*P).  It walks the spike list in neuron
+//                     order, reads the segment of each spiking row that
+//                     targets its posts (rows are sorted by post; a per-row
+//                     table holds the segment bounds), rolls the Poisson
+//                     sources that target its posts, and applies every event
+//                     to the ring cells it owns.
 //
-// Determinism.  The reference adds the events of a step to each ring cell in
-// (spiking pre ascending, CSR row order) and then Poisson-source order
-// (push.rs:143-172, step.rs:166-185).  That order is exactly ascending CSR
-// edge id, with source edges numbered after all neuron edges; each event
-// carries that id as its key.  apply_kernel resolves cells touched by several
-// events in rounds: every pending event posts its key with atomicMin to a
-// shared-memory owner slot hashed from its cell, the owner of each slot adds
-// its weight, the rest retry.  Events sharing a cell always share a slot, so
-// each cell receives its adds in ascending key order: the reference's order,
-// with the same float rounding.
+// Determinism.  The reference adds the events of one step to each ring cell
+// in (spiking pre ascending, CSR row order) and then Poisson-source order
+// (push.rs:143-172, step.rs:166-185).  A block generates its events exactly
+// in that order (rows are stored sorted by post with a stable sort, which
+// keeps the relative order of repeated synapses to one post), in windows of
+// up to kWin events.  Inside a window, cells are entered in an exact
+// shared-memory hash table; ownership rounds (atomicMin on the window index)
+// link the events of each cell into a chain in window order; the chain head
+// loads the ring value once, adds the chain's weights in order and stores
+// it.  Windows are applied one after another.  Every cell therefore receives
+// its adds in the reference's order, with the reference's rounding.
 #pragma once
 #include <cstdint>
 
@@ -34,13 +36,32 @@
 
 namespace sg {
 
+constexpr uint32_t kNeuronBlock = 1024;  // neurons per neuron-kernel block (= spike-list slot)
+constexpr uint32_t kScatterThreads = 1024;
+constexpr uint32_t kWin = 8192;          // events per window
+constexpr uint32_t kBuckets = 8192;      // per-window event lists, by post (post % kBuckets)
+constexpr uint32_t kPreChunk = 4096;     // spiking rows per sub-chunk (4 per thread)
+constexpr uint32_t kBlkChunk = 1024;     // spike-list slots scanned per chunk
+constexpr uint32_t kNone16 = 0xFFFFu;
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr unsigned long long kEmpty64 = ~0ull;
+constexpr uint32_t kMaxPops = 16;
+
+// neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
+// GPEA/HH are compute heavy and keep one neuron per thread
+template <int M> struct NeuronCfg {
+  static constexpr int NPT = (M == kLIF || M == kIZH) ? 4 : 1;
+  static constexpr int THREADS = (int)kNeuronBlock / NPT;
+};
+
 struct StepArgs {
   // step bookkeeping
   unsigned long long *step;  // device step counter
-  uint32_t *n_active;
-  uint32_t *active;
-  uint32_t *last_bits;  // spike bitmask of the last step, [Nd/32]
-  uint32_t *raster;     // [raster_cap][Nd/32] or null
+  uint32_t *blk_cnt;         // [n_blk] spikes per neuron block
+  uint2 *spk;                // [Nd] (pre, row_start) per block slot, ascending
+  uint32_t n_blk;
+  uint32_t *last_bits;       // spike bitmask of the last step, [Nd/32]
+  uint32_t *raster;          // [raster_cap][Nd/32] or null
   uint32_t raster_cap;
   uint32_t words;
   uint32_t *done;
@@ -58,29 +79,26 @@ struct StepArgs {
   float kin_a[3];
   float kin_erev[3];
   float *kin_g;  // [n_kin][Nd]
-  // CSR (device neuron indices)
+  // CSR (device neuron indices), rows sorted by post
   const uint32_t *row_ptr;
   const uint32_t *col;
   float *w;
   const uint8_t *code;
   uint32_t n_edges;
-  // Poisson sources
-  uint32_t n_src;
+  // per-row segment table: [Nd][G+1] offsets inside the row (u16 or u32)
+  const void *seg;
+  int seg32;
+  uint32_t G;      // scatter blocks
+  uint32_t P;      // posts per scatter block (multiple of 32)
+  uint32_t pbits;  // bits of a local post index
+  // Poisson sources, per scatter block: entries [src_lo[j], src_lo[j+1])
   const float *src_p;
   const uint32_t *src_seed;
-  const uint32_t *src_ptr;
-  const uint32_t *src_post;
-  const float *src_w;
-  const uint8_t *src_code;
-  // bins
-  uint32_t tshift;
-  uint32_t n_tiles;
-  uint32_t hbits;
-  const unsigned long long *bin_base;
-  uint32_t *bin_cnt;
-  uint32_t *bkey;
-  float *bw;
-  uint32_t *bcell;
+  const uint32_t *src_lo;
+  const uint32_t *se_src;
+  const uint32_t *se_post;
+  const float *se_w;
+  const uint8_t *se_code;
   // scatter mode
   int deterministic;
   // pair STDP
@@ -98,7 +116,9 @@ struct PopArgs {
   float *state;
   const float *params;
   uint32_t n, cap, dev_off;
-  float ln_na, ln_k;  // GPEA constants
+  uint32_t umask;      // bit c: parameter column c is uniform
+  float uval[16];      // its value
+  float ln_na, ln_k;   // GPEA constants
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -106,183 +126,293 @@ __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 // ---------------------------------------------------------------------------
 // neuron phase
 // ---------------------------------------------------------------------------
+template <int NPT> struct VecF;
+template <> struct VecF<1> {
+  __device__ __forceinline__ static void load(const float *p, float *v) { v[0] = *p; }
+  __device__ __forceinline__ static void ldg(const float *p, float *v) { v[0] = __ldg(p); }
+  __device__ __forceinline__ static void store(float *p, const float *v) { *p = v[0]; }
+};
+template <> struct VecF<4> {
+  __device__ __forceinline__ static void load(const float *p, float *v) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  }
+  __device__ __forceinline__ static void ldg(const float *p, float *v) {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  }
+  __device__ __forceinline__ static void store(float *p, const float *v) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+
 template <int MODEL>
-__global__ void __launch_bounds__(256) neuron_kernel(StepArgs a, PopArgs p) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // < cap (multiple of 32)
-  if (i >= p.cap) return;                                    // whole warps only
+__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS) neuron_kernel(StepArgs a, PopArgs p) {
+  constexpr int NPT = NeuronCfg<MODEL>::NPT;
+  constexpr int NS = n_state(MODEL), NP = n_params(MODEL);
+  using V = VecF<NPT>;
+  __shared__ uint32_t warp_cnt[32];
+  __shared__ uint32_t warp_clamp[32];
+  const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
+  const uint32_t i0 = blockIdx.x * kNeuronBlock + tid * NPT;  // population index of my first neuron
+  const uint32_t gi0 = p.dev_off + i0;
   const unsigned long long step = *a.step;
   const uint32_t slot = (uint32_t)(step & 31ull);
-  const uint32_t gi = p.dev_off + i;
-  bool spike = false;
-  if (i < p.n) {
-    // 1-2. read the slot, clear it (step.rs:27-34)
-    float *rs = a.ring + (size_t)slot * a.Nd + gi;
-    float x = *rs;
-    *rs = 0.0f;
-    // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start
-    if (a.n_kin > 0) {
-      const float v0 = p.state[i];
-      for (int k = 0; k < a.n_kin; ++k) {
-        float *ks = a.ring + ((size_t)(k + 1) * kSlots + slot) * a.Nd + gi;
-        const float jump = *ks;
-        *ks = 0.0f;
-        float *g = a.kin_g + (size_t)k * a.Nd + gi;
-        const float gn = *g * a.kin_a[k] + jump;
-        *g = gn;
-        x += gn * (a.kin_erev[k] - v0);
+  // 1-2. read the slot, clear it (step.rs:27-34)
+  float x[NPT], zero[NPT];
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) zero[q] = 0.0f;
+  float *rs = a.ring + (size_t)slot * a.Nd + gi0;
+  V::load(rs, x);
+  V::store(rs, zero);
+  float sv[NS][NPT];
+#pragma unroll
+  for (int c = 0; c < NS; ++c) V::load(p.state + (size_t)c * p.cap + i0, sv[c]);
+  // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start
+  for (int k = 0; k < a.n_kin; ++k) {
+    float jump[NPT], g[NPT];
+    float *ks = a.ring + ((size_t)(k + 1) * kSlots + slot) * a.Nd + gi0;
+    V::load(ks, jump);
+    V::store(ks, zero);
+    float *gp = a.kin_g + (size_t)k * a.Nd + gi0;
+    V::load(gp, g);
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+      g[q] = g[q] * a.kin_a[k] + jump[q];
+      x[q] += g[q] * (a.kin_erev[k] - sv[0][q]);
+    }
+    V::store(gp, g);
+  }
+  float pv[NP][NPT];
+#pragma unroll
+  for (int c = 0; c < NP; ++c) {
+    if ((p.umask >> c) & 1u) {
+#pragma unroll
+      for (int q = 0; q < NPT; ++q) pv[c][q] = p.uval[c];
+    } else {
+      V::ldg(p.params + (size_t)c * p.cap + i0, pv[c]);
+    }
+  }
+  // dt = param column 0 of neuron 0, broadcast (population.rs:307,361)
+  const float dt = (p.umask & 1u) ? p.uval[0] : __ldg(p.params);
+  uint32_t nib = 0, nclamp = 0;
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) {
+    if (i0 + q < p.n) {
+      float xi = x[q];
+      if (clamps(MODEL)) {
+        const float xc = fminf(fmaxf(xi, -100.0f), 100.0f);
+        nclamp += xc != xi;
+        xi = xc;
       }
+      RegNeuron<NS, NP> r;
+#pragma unroll
+      for (int c = 0; c < NS; ++c) r.s[c] = sv[c][q];
+#pragma unroll
+      for (int c = 0; c < NP; ++c) r.p[c] = pv[c][q];
+      bool sp;
+      if (MODEL == kLIF) sp = lif_step(r, xi, dt);
+      else if (MODEL == kIZH) sp = izh_step(r, xi, dt);
+      else if (MODEL == kGPEA) sp = gpea_step(r, xi, dt, p.ln_na, p.ln_k);
+      else sp = hh_step(r, xi, dt);
+#pragma unroll
+      for (int c = 0; c < NS; ++c) sv[c][q] = r.s[c];
+      nib |= (sp ? 1u : 0u) << q;
     }
-    if (clamps(MODEL)) {
-      const float xc = fminf(fmaxf(x, -100.0f), 100.0f);
-      if (a.clamp_hits != nullptr && xc != x) atomicAdd(a.clamp_hits, 1ull);
-      x = xc;
+  }
+#pragma unroll
+  for (int c = 0; c < NS; ++c) V::store(p.state + (size_t)c * p.cap + i0, sv[c]);
+  // 4. compaction: bitmask words (32 neurons each) and the block's spike list
+  uint32_t word;
+  if (NPT == 4) {
+    word = nib << (4 * (lane & 7));
+    word |= __shfl_xor_sync(0xffffffffu, word, 1);
+    word |= __shfl_xor_sync(0xffffffffu, word, 2);
+    word |= __shfl_xor_sync(0xffffffffu, word, 4);
+    if ((lane & 7) == 0) {
+      a.last_bits[gi0 >> 5] = word;
+      if (a.raster != nullptr) a.raster[(size_t)(step % a.raster_cap) * a.words + (gi0 >> 5)] = word;
     }
-    // dt = param column 0 of neuron 0, broadcast (population.rs:307,361)
-    const float dt = __ldg(p.params);
-    const Soa c{p.state, p.params, p.cap, i};
-    if (MODEL == kLIF) spike = lif_step(c, x, dt);
-    else if (MODEL == kIZH) spike = izh_step(c, x, dt);
-    else if (MODEL == kGPEA) spike = gpea_step(c, x, dt, p.ln_na, p.ln_k);
-    else spike = hh_step(c, x, dt);
-  }
-  // 4. compaction: warp ballot -> bitmask word + active-list append
-  const uint32_t m = __ballot_sync(0xffffffffu, spike);
-  const uint32_t lane = lane_id();
-  uint32_t base = 0;
-  if (lane == 0) {
-    a.last_bits[gi >> 5] = m;
-    if (a.raster != nullptr) a.raster[(size_t)(step % a.raster_cap) * a.words + (gi >> 5)] = m;
-    if (m) base = atomicAdd(a.n_active, (uint32_t)__popc(m));
-  }
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (spike) a.active[base + __popc(m & ((1u << lane) - 1u))] = gi;
-  // pair-STDP traces: x = fma(x, d, s) (P/api/learn/brain.rs:212-222)
-  if (a.stdp && i < p.n) {
-    const float add = spike ? 1.0f : 0.0f;
-    a.x_pre[gi] = __fmaf_rn(a.x_pre[gi], a.d_pre, add);
-    a.x_post[gi] = __fmaf_rn(a.x_post[gi], a.d_post, add);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// expand phase
-// ---------------------------------------------------------------------------
-// Append one event to the bin of its post tile.  `mask` = lanes of the warp
-// executing this call together; reservation is warp-aggregated per tile.
-__device__ __forceinline__ void emit_event(const StepArgs &a, uint32_t mask, uint32_t key,
-                                           uint32_t post, float w, uint8_t code,
-                                           unsigned long long step) {
-  const uint32_t slot = (uint32_t)((step + max(code_delay(code), 1u)) & 31ull);
-  const uint32_t ringi = code_ring(code);
-  if (!a.deterministic) {
-    atomicAdd(a.ring + ((size_t)ringi * kSlots + slot) * a.Nd + post, w);
-    return;
-  }
-  const uint32_t tile = post >> a.tshift;
-  const uint32_t cell = ((ringi * kSlots + slot) << a.tshift) | (post & ((1u << a.tshift) - 1u));
-  const uint32_t peers = __match_any_sync(mask, tile);
-  const uint32_t lane = lane_id();
-  const uint32_t leader = __ffs(peers) - 1;
-  uint32_t off = 0;
-  if (lane == leader) off = atomicAdd(a.bin_cnt + tile, (uint32_t)__popc(peers));
-  off = __shfl_sync(peers, off, leader);
-  const unsigned long long pos = a.bin_base[tile] + off + __popc(peers & ((1u << lane) - 1u));
-  a.bkey[pos] = key;
-  a.bw[pos] = w;
-  a.bcell[pos] = cell;
-}
-
-__global__ void __launch_bounds__(256) expand_kernel(StepArgs a, uint32_t src_blocks) {
-  const unsigned long long step = *a.step;
-  const uint32_t lane = lane_id();
-  if (blockIdx.x >= src_blocks) {
-    // --- spiking neurons: one warp per active row (push.rs:143-172) ---
-    const uint32_t n_act = *a.n_active;
-    const uint32_t warps_per_block = blockDim.x >> 5;
-    const uint32_t gw = (blockIdx.x - src_blocks) * warps_per_block + (threadIdx.x >> 5);
-    const uint32_t nw = (gridDim.x - src_blocks) * warps_per_block;
-    unsigned long long ev = 0;
-    for (uint32_t r = gw; r < n_act; r += nw) {
-      const uint32_t pre = a.active[r];
-      const uint32_t beg = __ldg(a.row_ptr + pre), end = __ldg(a.row_ptr + pre + 1);
-      ev += end - beg;
-      for (uint32_t e0 = beg; e0 < end; e0 += 32) {
-        const uint32_t e = e0 + lane;
-        const bool ok = e < end;
-        const uint32_t mask = __ballot_sync(0xffffffffu, ok);
-        if (ok) {
-          const uint32_t post = __ldg(a.col + e);
-          const float w = a.w[e];
-          const uint8_t code = __ldg(a.code + e);
-          emit_event(a, mask, e, post, w, code, step);
-          if (a.stdp && code_stdp(code)) {
-            // depression at a pre spike, pushed weight is the pre-update one
-            const float w1 = fminf(fmaxf(w - a.a_minus * a.x_post[post], a.w_min), a.w_max);
-            a.w[e] = w1;
-            atomicAdd(a.drift, (double)w1 - (double)w);
-          }
-        }
-      }
-    }
-    if (lane == 0 && ev) atomicAdd(a.ev_step, ev);
   } else {
-    // --- Poisson sources: one thread per source (step.rs:166-185) ---
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    bool fired = false;
-    uint32_t beg = 0, end = 0;
-    if (s < a.n_src) {
-      const float p = a.src_p[s];
-      fired = p > 0.0f && poisson_spike(a.src_seed[s], 0, step, p);
-      if (fired) {
-        beg = a.src_ptr[s];
-        end = a.src_ptr[s + 1];
-      }
+    word = __ballot_sync(0xffffffffu, nib != 0);
+    if (lane == 0) {
+      a.last_bits[gi0 >> 5] = word;
+      if (a.raster != nullptr) a.raster[(size_t)(step % a.raster_cap) * a.words + (gi0 >> 5)] = word;
     }
-    uint32_t deg = end - beg;
-    uint32_t maxdeg = deg;
-    for (int o = 16; o > 0; o >>= 1) maxdeg = max(maxdeg, __shfl_xor_sync(0xffffffffu, maxdeg, o));
-    for (uint32_t k = 0; k < maxdeg; ++k) {
-      const bool ok = k < deg;
-      const uint32_t mask = __ballot_sync(0xffffffffu, ok);
-      if (ok) {
-        const uint32_t j = beg + k;
-        emit_event(a, mask, a.n_edges + j, a.src_post[j], a.src_w[j], a.src_code[j], step);
-      }
-    }
-    unsigned long long ev = deg;
-    for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
-    if (lane == 0 && ev) atomicAdd(a.ev_step, ev);
   }
-}
-
-// Pair-STDP potentiation: one warp per spiking post walks its plastic
-// in-edges (runs after expand_kernel, so it sees this step's depression).
-__global__ void __launch_bounds__(256) stdp_ltp_kernel(StepArgs a) {
-  const uint32_t n_act = *a.n_active;
-  const uint32_t lane = lane_id();
-  const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t r = gw; r < n_act; r += nw) {
-    const uint32_t post = a.active[r];
-    const uint32_t beg = a.in_ptr[post], end = a.in_ptr[post + 1];
-    for (uint32_t k = beg + lane; k < end; k += 32) {
-      const uint32_t e = a.in_edge[k];
-      const float w0 = a.w[e];
-      const float w1 = fminf(fmaxf(w0 + a.a_plus * a.x_pre[a.in_pre[k]], a.w_min), a.w_max);
-      a.w[e] = w1;
-      atomicAdd(a.drift, (double)w1 - (double)w0);
-    }
+  const uint32_t cnt = __popc(nib);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  uint32_t clw = nclamp;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) clw += __shfl_xor_sync(0xffffffffu, clw, o);
+  if (lane == 31) warp_cnt[wid] = incl;
+  if (lane == 0) warp_clamp[wid] = clw;
+  __syncthreads();
+  constexpr uint32_t NW = NeuronCfg<MODEL>::THREADS / 32;
+  uint32_t before = incl - cnt, total = 0, clamp_tot = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < NW; ++k) {
+    const uint32_t c = warp_cnt[k];
+    before += k < wid ? c : 0u;
+    total += c;
+    clamp_tot += warp_clamp[k];
+  }
+  const uint32_t gblk = gi0 / kNeuronBlock;
+  uint2 *out = a.spk + (size_t)gblk * kNeuronBlock + before;
+#pragma unroll
+  for (int q = 0; q < NPT; ++q)
+    if (nib & (1u << q)) *out++ = make_uint2(gi0 + q, __ldg(a.row_ptr + gi0 + q));
+  if (tid == 0) {
+    a.blk_cnt[gblk] = total;
+    if (a.clamp_hits != nullptr && clamp_tot) atomicAdd(a.clamp_hits, (unsigned long long)clamp_tot);
+  }
+  // pair-STDP traces: x = fma(x, d, s) (P/api/learn/brain.rs:212-222)
+  if (a.stdp) {
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (i0 + q < p.n) {
+        const uint32_t gi = gi0 + q;
+        const float add = (nib >> q) & 1u ? 1.0f : 0.0f;
+        a.x_pre[gi] = __fmaf_rn(a.x_pre[gi], a.d_pre, add);
+        a.x_post[gi] = __fmaf_rn(a.x_post[gi], a.d_post, add);
+      }
   }
 }
 
 // ---------------------------------------------------------------------------
-// apply phase
+// block-wide helpers (kScatterThreads threads)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t owner_slot(uint32_t cell, uint32_t hbits) {
-  return (cell * 2654435761u) >> (32 - hbits);
+// Exclusive scan of one value per thread; returns the prefix, *total = sum.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *wsum, uint32_t *total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  __syncthreads();  // wsum reuse
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t t = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= (uint32_t)o) t += y;
+    }
+    wsum[lane] = t;  // inclusive per warp
+  }
+  __syncthreads();
+  *total = wsum[31];
+  return (x - v) + (wid ? wsum[wid - 1] : 0u);
 }
 
-__device__ __forceinline__ void end_of_step(const StepArgs &a) {
+// largest i in [0, n) with pre[i] <= v (pre ascending, pre[0] = 0)
+__device__ __forceinline__ uint32_t upper_index(const uint32_t *pre, uint32_t n, uint32_t v) {
+  uint32_t lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct ScatterSmem {
+  uint32_t head[kBuckets];        // latest event of each post bucket in the window
+  uint32_t ecell[kWin];           // window events in reference order: cell,
+  float ew[kWin];                 //   weight,
+  uint16_t enext[kWin];           //   previous event of the same bucket
+  uint32_t plo[kPreChunk];        // absolute first edge of each row segment
+  uint32_t pseg[kPreChunk + 1];   // prefix of segment lengths
+  uint32_t boff[kBlkChunk + 1];   // prefix of spike-list slot counts
+  uint32_t wsum[32];
+  double drift;
+  unsigned long long events;
+};
+static_assert(sizeof(ScatterSmem) <= 232448, "scatter shared memory exceeds 227 KB");
+
+constexpr uint32_t kEPT = kWin / kScatterThreads;         // window events per thread (8)
+constexpr uint32_t kBPT = kBuckets / kScatterThreads;     // buckets per thread (8)
+constexpr uint32_t kPPT = kPreChunk / kScatterThreads;    // spiking rows per thread (4)
+
+__device__ __forceinline__ float *cell_addr(const StepArgs &a, uint32_t cell, uint32_t p0) {
+  return a.ring + (size_t)(cell >> a.pbits) * a.Nd + p0 + (cell & ((1u << a.pbits) - 1u));
+}
+
+__device__ __forceinline__ void clear_heads(ScatterSmem &S) {
+#pragma unroll
+  for (uint32_t r = 0; r < kBPT; ++r) S.head[threadIdx.x + r * kScatterThreads] = kEmpty;
+}
+
+// Prepend event k to the list of its post bucket (arrival order).
+__device__ __forceinline__ void link_event(const StepArgs &a, ScatterSmem &S, uint32_t k) {
+  const uint32_t b = S.ecell[k] & (kBuckets - 1u) & ((1u << a.pbits) - 1u);
+  const uint32_t prev = atomicExch(&S.head[b], k);
+  S.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
+}
+
+// Each thread owns buckets b = threadIdx.x + r * kScatterThreads and adds
+// their events to the ring in ascending window (= reference) order.  A
+// bucket holds one post's events (several posts only when a block owns more
+// than kBuckets posts), so every ring cell sees its adds in order.
+__device__ __forceinline__ void apply_buckets(const StepArgs &a, ScatterSmem &S, uint32_t p0) {
+  uint32_t hd[kBPT];
+  float v[kBPT];
+  uint32_t single = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < kBPT; ++r) {
+    hd[r] = S.head[threadIdx.x + r * kScatterThreads];
+    v[r] = 0.0f;
+    if (hd[r] != kEmpty && S.enext[hd[r]] == kNone16) {
+      single |= 1u << r;
+      v[r] = *cell_addr(a, S.ecell[hd[r]], p0);  // loads issued together
+    }
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < kBPT; ++r) {
+    if (hd[r] == kEmpty) continue;
+    if (single & (1u << r)) {
+      *cell_addr(a, S.ecell[hd[r]], p0) = v[r] + S.ew[hd[r]];
+      continue;
+    }
+    // several events: take them in ascending window order (selection over
+    // the short list), one read-modify-write each
+    uint32_t last = 0;
+    bool first = true;
+    while (true) {
+      uint32_t best = kEmpty;
+      for (uint32_t j = hd[r]; j != kNone16; j = S.enext[j])
+        if ((first || j > last) && j < best) best = j;
+      if (best == kEmpty) break;
+      float *p = cell_addr(a, S.ecell[best], p0);
+      *p = *p + S.ew[best];
+      last = best;
+      first = false;
+    }
+  }
+}
+
+// One event into the window (or straight into the ring in atomic mode).
+__device__ __forceinline__ void put_event(const StepArgs &a, ScatterSmem &S, uint32_t k, uint32_t post,
+                                          float w, uint8_t code, unsigned long long step, uint32_t p0) {
+  const uint32_t slot = (uint32_t)((step + max(code_delay(code), 1u)) & 31ull);
+  const uint32_t cell = ((code_ring(code) * kSlots + slot) << a.pbits) | (post - p0);
+  if (a.deterministic) {
+    S.ecell[k] = cell;
+    S.ew[k] = w;
+  } else {
+    atomicAdd(cell_addr(a, cell, p0), w);
+  }
+}
+
+__device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -290,15 +420,13 @@ __device__ __forceinline__ void end_of_step(const StepArgs &a) {
     if (t == gridDim.x - 1) {
       __threadfence();
       const unsigned long long step = *a.step;
-      const uint32_t n_act = *(volatile uint32_t *)a.n_active;
       const unsigned long long ev = *(volatile unsigned long long *)a.ev_step;
       if (a.stat_cap) {
-        a.stat_spk[step % a.stat_cap] = n_act;
+        a.stat_spk[step % a.stat_cap] = n_spikes;
         a.stat_ev[step % a.stat_cap] = ev;
       }
       *a.ev_total += ev;
       *a.ev_step = 0;
-      *a.n_active = 0;
       *a.done = 0;
       *a.step = step + 1;
       __threadfence();
@@ -306,64 +434,202 @@ __device__ __forceinline__ void end_of_step(const StepArgs &a) {
   }
 }
 
-constexpr uint32_t kDone = 0xFFFFFFFFu;
-
-__global__ void __launch_bounds__(512) apply_kernel(StepArgs a) {
-  extern __shared__ uint32_t owner[];
-  const uint32_t hbits = a.hbits;
-  const uint32_t tmask = (1u << a.tshift) - 1u;
-  if (a.deterministic) {
-    for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-      const uint32_t cnt = a.bin_cnt[tile];
-      if (cnt == 0) continue;  // uniform across the block
-      const unsigned long long base = a.bin_base[tile];
-      uint32_t *cellp = a.bcell + base;
-      const uint32_t *keyp = a.bkey + base;
-      const float *wp = a.bw + base;
-      for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) owner[owner_slot(cellp[k], hbits)] = kDone;
-      __syncthreads();
-      bool pending = true;
-      while (__syncthreads_or(pending)) {
-        // (a) post keys
-        pending = false;
-        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
-          const uint32_t c = cellp[k];
-          if (c != kDone) atomicMin(&owner[owner_slot(c, hbits)], keyp[k]);
-        }
-        __syncthreads();
-        // (b) the smallest key of each slot applies its add
-        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
-          const uint32_t c = cellp[k];
-          if (c == kDone) continue;
-          if (owner[owner_slot(c, hbits)] == keyp[k]) {
-            float *r = a.ring + (size_t)(c >> a.tshift) * a.Nd + ((size_t)tile << a.tshift) + (c & tmask);
-            *r = *r + wp[k];
-            cellp[k] = kDone;
+template <bool SEG32>
+__global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
+  const uint32_t tid = threadIdx.x;
+  const uint32_t j = blockIdx.x;
+  const uint32_t p0 = j * a.P;
+  const unsigned long long step = *a.step;
+  const uint32_t G1 = a.G + 1;
+  if (tid == 0) {
+    S.drift = 0.0;
+    S.events = 0;
+  }
+  uint32_t n_spikes = 0;
+  // ---- neuron events, in spiking-neuron order ----
+  for (uint32_t cb0 = 0; cb0 < a.n_blk; cb0 += kBlkChunk) {
+    const uint32_t c = (cb0 + tid < a.n_blk) ? a.blk_cnt[cb0 + tid] : 0u;
+    uint32_t spikes;
+    const uint32_t ex = block_excl_scan(c, S.wsum, &spikes);
+    S.boff[tid] = ex;
+    if (tid == 0) S.boff[kBlkChunk] = spikes;
+    n_spikes += spikes;
+    __syncthreads();
+    for (uint32_t s0 = 0; s0 < spikes; s0 += kPreChunk) {
+      const uint32_t pc = min(kPreChunk, spikes - s0);
+      // rows tid*kPPT .. +kPPT of this sub-chunk: segment of each for this block
+      uint32_t len[kPPT], mylen = 0;
+#pragma unroll
+      for (uint32_t q = 0; q < kPPT; ++q) {
+        const uint32_t i = tid * kPPT + q;
+        len[q] = 0;
+        if (i < pc) {
+          const uint32_t r = s0 + i;
+          const uint32_t b = upper_index(S.boff, kBlkChunk, r);
+          const uint2 e = a.spk[(size_t)(cb0 + b) * kNeuronBlock + (r - S.boff[b])];
+          uint32_t lo, hi;
+          if (SEG32) {
+            const uint32_t *t = (const uint32_t *)a.seg + (size_t)e.x * G1 + j;
+            lo = __ldg(t);
+            hi = __ldg(t + 1);
           } else {
-            pending = true;
+            const uint16_t *t = (const uint16_t *)a.seg + (size_t)e.x * G1 + j;
+            lo = __ldg(t);
+            hi = __ldg(t + 1);
+          }
+          S.plo[i] = e.y + lo;
+          len[q] = hi - lo;
+          mylen += len[q];
+        }
+      }
+      uint32_t M;
+      uint32_t ex2 = block_excl_scan(mylen, S.wsum, &M);
+#pragma unroll
+      for (uint32_t q = 0; q < kPPT; ++q) {
+        S.pseg[tid * kPPT + q] = ex2;
+        ex2 += len[q];
+      }
+      if (tid == 0) {
+        S.pseg[kPreChunk] = M;
+        S.events += M;
+      }
+      __syncthreads();
+      for (uint32_t w0 = 0; w0 < M; w0 += kWin) {
+        const uint32_t m = min(kWin, M - w0);
+        if (a.deterministic) clear_heads(S);
+        // each spiking row writes the edge ids of its window events (rows are
+        // short segments); then thread tid takes events k = tid + r*kScatterThreads
+#pragma unroll
+        for (uint32_t q = 0; q < kPPT; ++q) {
+          const uint32_t i = tid * kPPT + q;
+          if (i < pc) {
+            const uint32_t g0 = max(S.pseg[i], w0), g1 = min(S.pseg[i + 1], w0 + m);
+            const uint32_t d = S.plo[i] - S.pseg[i];
+            for (uint32_t g = g0; g < g1; ++g) S.ecell[g - w0] = d + g;
           }
         }
         __syncthreads();
-        // (c) free the slots still wanted
-        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
-          const uint32_t c = cellp[k];
-          if (c != kDone) owner[owner_slot(c, hbits)] = kDone;
+        uint32_t ev_e[kEPT];
+#pragma unroll
+        for (uint32_t r = 0; r < kEPT; ++r) {
+          const uint32_t k = tid + r * kScatterThreads;
+          ev_e[r] = k < m ? S.ecell[k] : 0u;
+        }
+        uint32_t ev_post[kEPT];
+        float ev_w[kEPT];
+        uint8_t ev_code[kEPT];
+#pragma unroll
+        for (uint32_t r = 0; r < kEPT; ++r) {
+          const uint32_t k = tid + r * kScatterThreads;
+          if (k < m) {
+            ev_post[r] = __ldg(a.col + ev_e[r]);
+            ev_w[r] = a.w[ev_e[r]];
+            ev_code[r] = __ldg(a.code + ev_e[r]);
+          }
+        }
+#pragma unroll
+        for (uint32_t r = 0; r < kEPT; ++r) {
+          const uint32_t k = tid + r * kScatterThreads;
+          if (k < m) {
+            put_event(a, S, k, ev_post[r], ev_w[r], ev_code[r], step, p0);
+            if (a.stdp && code_stdp(ev_code[r])) {
+              // depression at a pre spike; the pushed weight is the pre-update one
+              const float w1 = fminf(fmaxf(ev_w[r] - a.a_minus * a.x_post[ev_post[r]], a.w_min), a.w_max);
+              a.w[ev_e[r]] = w1;
+              atomicAdd(&S.drift, (double)w1 - (double)ev_w[r]);
+            }
+            if (a.deterministic) link_event(a, S, k);
+          }
+        }
+        __syncthreads();
+        if (a.deterministic) {
+          apply_buckets(a, S, p0);
+          __syncthreads();
         }
       }
-      if (threadIdx.x == 0) a.bin_cnt[tile] = 0;
-      __syncthreads();
     }
   }
-  end_of_step(a);
+  // ---- Poisson sources targeting this block's posts, in source order ----
+  const uint32_t lst0 = a.src_lo[j], lst1 = a.src_lo[j + 1];
+  for (uint32_t base = lst0; base < lst1; base += kWin) {
+    if (a.deterministic) clear_heads(S);
+    // thread tid owns entries [base + tid*kEPT, +kEPT): order-preserving compaction
+    uint32_t sp_src[kEPT], sp_post[kEPT];
+    float sp_w[kEPT];
+    uint8_t sp_code[kEPT];
+#pragma unroll
+    for (uint32_t r = 0; r < kEPT; ++r) {
+      const uint32_t e = base + tid * kEPT + r;
+      if (e < lst1) {
+        sp_src[r] = a.se_src[e];
+        sp_post[r] = a.se_post[e];
+        sp_w[r] = a.se_w[e];
+        sp_code[r] = a.se_code[e];
+      }
+    }
+    uint32_t fired = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < kEPT; ++r) {
+      const uint32_t e = base + tid * kEPT + r;
+      if (e < lst1) {
+        const float p = a.src_p[sp_src[r]];
+        if (p > 0.0f && poisson_spike(a.src_seed[sp_src[r]], 0, step, p)) fired |= 1u << r;
+      }
+    }
+    uint32_t m;
+    uint32_t pos = block_excl_scan(__popc(fired), S.wsum, &m);
+#pragma unroll
+    for (uint32_t r = 0; r < kEPT; ++r)
+      if (fired & (1u << r)) put_event(a, S, pos++, sp_post[r], sp_w[r], sp_code[r], step, p0);
+    if (tid == 0) S.events += m;
+    if (a.deterministic && m) {
+      __syncthreads();
+#pragma unroll
+      for (uint32_t r = 0; r < kEPT; ++r) {
+        const uint32_t k = tid + r * kScatterThreads;
+        if (k < m) link_event(a, S, k);
+      }
+      __syncthreads();
+      apply_buckets(a, S, p0);
+    }
+    __syncthreads();
+  }
+  // ---- pair-STDP potentiation on the plastic in-edges of spiking posts ----
+  if (a.stdp) {
+    __syncthreads();
+    const uint32_t p1 = min(p0 + a.P, a.Nd);
+    for (uint32_t wd = p0 / 32 + tid; wd < p1 / 32; wd += kScatterThreads) {
+      uint32_t bits = a.last_bits[wd];
+      while (bits) {
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const uint32_t q = wd * 32 + b;
+        for (uint32_t k = a.in_ptr[q]; k < a.in_ptr[q + 1]; ++k) {
+          const uint32_t e = a.in_edge[k];
+          const float w0 = a.w[e];
+          const float w1 = fminf(fmaxf(w0 + a.a_plus * a.x_pre[a.in_pre[k]], a.w_min), a.w_max);
+          a.w[e] = w1;
+          atomicAdd(&S.drift, (double)w1 - (double)w0);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (S.events) atomicAdd(a.ev_step, S.events);
+    if (a.stdp && S.drift != 0.0) atomicAdd(a.drift, S.drift);
+  }
+  end_of_step(a, n_spikes);
 }
 
 // ---------------------------------------------------------------------------
 // inject_current (build.rs:243-275): values land in the slot the next step
 // reads.  `sequential` = the index list has repeats, apply in list order.
 // ---------------------------------------------------------------------------
-__global__ void inject_kernel(float *ring, uint32_t Nd, const unsigned long long *step,
-                              const uint32_t *idx, const float *vals, uint64_t n, uint32_t dev_off,
-                              int sequential) {
+__global__ void inject_kernel(float *ring, uint32_t Nd, const unsigned long long *step, const uint32_t *idx,
+                              const float *vals, uint64_t n, uint32_t dev_off, int sequential) {
   const uint32_t slot = (uint32_t)(*step & 31ull);
   float *rs = ring + (size_t)slot * Nd + dev_off;
   if (sequential) {
@@ -371,8 +637,7 @@ __global__ void inject_kernel(float *ring, uint32_t Nd, const unsigned long long
       for (uint64_t k = 0; k < n; ++k) rs[idx[k]] = rs[idx[k]] + vals[k];
     return;
   }
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (uint64_t)gridDim.x * blockDim.x)
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
     rs[idx[k]] = rs[idx[k]] + vals[k];
 }
 

@@ -7,7 +7,8 @@ import re
 
 _PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_PKG_DIR)  # dioma-core_b200/
-library_path = os.path.join(_ROOT, "libsimuse_b200.so")
+# SIMUSE_B200_LIB overrides the library location (e.g. an installed copy)
+library_path = os.environ.get("SIMUSE_B200_LIB", os.path.join(_ROOT, "libsimuse_b200.so"))
 header_path = os.path.join(os.path.dirname(_ROOT), "include", "simuse_b200.h")
 
 
