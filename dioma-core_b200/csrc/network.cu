@@ -121,18 +121,24 @@ struct sg_net {
   DBuf<uint32_t> d_blk_cnt, d_last_bits, d_raster, d_done, d_stat_spk;
   DBuf<uint2> d_spk;
   DBuf<float> d_ring, d_kin_g;
-  DBuf<uint32_t> d_row_ptr, d_col;
-  DBuf<float> d_w;
-  DBuf<uint8_t> d_code;
+  DBuf<uint32_t> d_row_ptr;
+  // one 8-byte record per synapse: x = post (| code << 24 when packed), y = weight bits
+  DBuf<uint2> d_edge;
+  DBuf<uint8_t> d_code;  // code byte per synapse when it does not fit in x
+  int packed = 1;
   uint64_t n_edges = 0;
   // per-row segment table [Nd][G+1] (u16, or u32 when a row is >= 65536 long)
   DBuf<uint8_t> d_seg;
   int seg32 = 0;
   uint32_t G = 0, P = 0, pbits = 0;
   // Poisson sources and their synapses grouped by scatter block
-  DBuf<float> d_src_p, d_se_w;
-  DBuf<uint32_t> d_src_seed, d_src_lo, d_se_src, d_se_post;
-  DBuf<uint8_t> d_se_code;
+  // runs of source synapses where source id, post and seed advance by one and
+  // rate, weight and code are shared (the one-source-per-neuron drive is one
+  // run per scatter block)
+  DBuf<uint32_t> d_run_lo, d_run_src0, d_run_post0, d_run_len, d_run_seed0;
+  DBuf<float> d_run_w, d_run_p;
+  DBuf<uint8_t> d_run_code;
+  uint64_t n_runs = 0;
   uint64_t n_src_edges = 0;
   DBuf<float> d_x_pre, d_x_post;
   DBuf<uint32_t> d_in_ptr, d_in_edge, d_in_pre;
@@ -226,22 +232,23 @@ StepArgs make_args(sg_net *net) {
   }
   a.kin_g = net->d_kin_g.p;
   a.row_ptr = net->d_row_ptr.p;
-  a.col = net->d_col.p;
-  a.w = net->d_w.p;
-  a.code = net->d_code.p;
+  a.edge = net->d_edge.p;
+  a.code = net->packed ? nullptr : net->d_code.p;
+  a.post_mask = net->packed ? 0x00FFFFFFu : 0xFFFFFFFFu;
   a.n_edges = (uint32_t)net->n_edges;
   a.seg = net->d_seg.p;
   a.seg32 = net->seg32;
   a.G = net->G;
   a.P = net->P;
   a.pbits = net->pbits;
-  a.src_p = net->d_src_p.p;
-  a.src_seed = net->d_src_seed.p;
-  a.src_lo = net->d_src_lo.p;
-  a.se_src = net->d_se_src.p;
-  a.se_post = net->d_se_post.p;
-  a.se_w = net->d_se_w.p;
-  a.se_code = net->d_se_code.p;
+  a.run_lo = net->d_run_lo.p;
+  a.run_src0 = net->d_run_src0.p;
+  a.run_post0 = net->d_run_post0.p;
+  a.run_len = net->d_run_len.p;
+  a.run_seed0 = net->d_run_seed0.p;
+  a.run_w = net->d_run_w.p;
+  a.run_p = net->d_run_p.p;
+  a.run_code = net->d_run_code.p;
   a.deterministic = net->deterministic;
   a.stdp = net->stdp_on ? 1 : 0;
   a.x_pre = net->d_x_pre.p;
@@ -286,6 +293,10 @@ float host_fast_exp(float x) {
 // ---------------------------------------------------------------------------
 // build kernels
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t edge_post(uint2 e, int packed) { return packed ? (e.x & 0x00FFFFFFu) : e.x; }
+__device__ __forceinline__ uint8_t edge_code_of(uint2 e, const uint8_t *code, uint64_t i, int packed) {
+  return packed ? (uint8_t)(e.x >> 24) : code[i];
+}
 __global__ void sort_key_kernel(const uint32_t *pre, const uint32_t *post, unsigned long long *key, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     key[i] = ((unsigned long long)pre[i] << 32) | post[i];
@@ -293,8 +304,8 @@ __global__ void sort_key_kernel(const uint32_t *pre, const uint32_t *post, unsig
 // Segment table: entry j of row `pre` = first position in the row whose post
 // is >= j*P (rows are sorted by post), entry G = row length.
 template <typename T>
-__global__ void seg_table_kernel(const uint32_t *row_ptr, const uint32_t *col, uint32_t Nd, uint32_t G, uint32_t P,
-                                 T *seg) {
+__global__ void seg_table_kernel(const uint32_t *row_ptr, const uint2 *edge, int packed, uint32_t Nd, uint32_t G,
+                                 uint32_t P, T *seg) {
   for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x) {
     const uint32_t beg = row_ptr[pre], end = row_ptr[pre + 1];
     T *out = seg + (size_t)pre * (G + 1);
@@ -304,7 +315,7 @@ __global__ void seg_table_kernel(const uint32_t *row_ptr, const uint32_t *col, u
       uint32_t hi = end;
       while (lo < hi) {  // lower_bound of bound in [lo, end)
         const uint32_t mid = (lo + hi) >> 1;
-        if (col[mid] < bound) lo = mid + 1;
+        if (edge_post(edge[mid], packed) < bound) lo = mid + 1;
         else hi = mid;
       }
       out[j] = (T)(lo - beg);
@@ -317,13 +328,12 @@ __global__ void iota_kernel(uint32_t *v, uint64_t n) {
     v[i] = (uint32_t)i;
 }
 __global__ void gather_edges_kernel(const uint32_t *perm, const uint32_t *post_in, const float *w_in,
-                                    const uint8_t *code_in, uint32_t *col, float *w, uint8_t *code,
-                                    uint64_t n) {
+                                    const uint8_t *code_in, uint2 *edge, uint8_t *code, int packed, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t j = perm[i];
-    col[i] = post_in[j];
-    w[i] = w_in[j];
-    code[i] = code_in[j];
+    const uint8_t c = code_in[j];
+    edge[i] = make_uint2(packed ? (post_in[j] | ((uint32_t)c << 24)) : post_in[j], __float_as_uint(w_in[j]));
+    if (!packed) code[i] = c;
   }
 }
 __global__ void histogram_kernel(const uint32_t *keys, uint64_t n, uint32_t shift, unsigned long long *cnt) {
@@ -335,18 +345,18 @@ __global__ void to_u32_kernel(const unsigned long long *in, uint32_t *out, uint6
     out[i] = (uint32_t)in[i];
 }
 // Plastic in-edges grouped by post.
-__global__ void csc_count_kernel(const uint32_t *row_ptr, const uint32_t *col, const uint8_t *code,
+__global__ void csc_count_kernel(const uint32_t *row_ptr, const uint2 *edge, const uint8_t *code, int packed,
                                  uint32_t Nd, unsigned long long *cnt) {
   for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x)
     for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e)
-      if (code_stdp(code[e])) atomicAdd(cnt + col[e], 1ull);
+      if (code_stdp(edge_code_of(edge[e], code, e, packed))) atomicAdd(cnt + edge_post(edge[e], packed), 1ull);
 }
-__global__ void csc_fill_kernel(const uint32_t *row_ptr, const uint32_t *col, const uint8_t *code,
+__global__ void csc_fill_kernel(const uint32_t *row_ptr, const uint2 *edge, const uint8_t *code, int packed,
                                 uint32_t Nd, uint32_t *cursor, uint32_t *in_edge, uint32_t *in_pre) {
   for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x)
     for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e)
-      if (code_stdp(code[e])) {
-        const uint32_t k = atomicAdd(cursor + col[e], 1u);
+      if (code_stdp(edge_code_of(edge[e], code, e, packed))) {
+        const uint32_t k = atomicAdd(cursor + edge_post(edge[e], packed), 1u);
         in_edge[k] = e;
         in_pre[k] = pre;
       }
@@ -483,9 +493,9 @@ void build_graph(sg_net *net) {
   net->n_edges = E;
   const uint32_t Nd = net->Nd;
   net->d_row_ptr.alloc((size_t)Nd + 1);
-  net->d_col.alloc(std::max<uint64_t>(E, 1));
-  net->d_w.alloc(std::max<uint64_t>(E, 1));
-  net->d_code.alloc(std::max<uint64_t>(E, 1));
+  net->packed = Nd <= (1u << 24) ? 1 : 0;
+  net->d_edge.alloc(std::max<uint64_t>(E, 1));
+  net->d_code.alloc(net->packed ? 1 : std::max<uint64_t>(E, 1));
   DBuf<unsigned long long> cnt;
   cnt.alloc((size_t)Nd + 1);
   cnt.zero(s);
@@ -514,7 +524,7 @@ void build_graph(sg_net *net) {
     vals_in.release();
     launch_grid(E, [&](unsigned b) {
       gather_edges_kernel<<<b, 256, 0, s>>>(vals_out.p, net->e_post.p, net->e_w.p, net->e_code.p,
-                                            net->d_col.p, net->d_w.p, net->d_code.p, E);
+                                            net->d_edge.p, net->d_code.p, net->packed, E);
     });
     launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->e_pre.p, E, 0, cnt.p); });
     SG_CUDA(cudaStreamSynchronize(s));
@@ -561,9 +571,11 @@ void build_segments(sg_net *net) {
   net->d_seg.alloc(std::max<size_t>((size_t)Nd * (G + 1) * esz, 1));
   launch_grid(Nd, [&](unsigned b) {
     if (net->seg32)
-      seg_table_kernel<uint32_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, Nd, G, P, (uint32_t *)net->d_seg.p);
+      seg_table_kernel<uint32_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->packed, Nd, G, P,
+                                                   (uint32_t *)net->d_seg.p);
     else
-      seg_table_kernel<uint16_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, Nd, G, P, (uint16_t *)net->d_seg.p);
+      seg_table_kernel<uint16_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->packed, Nd, G, P,
+                                                   (uint16_t *)net->d_seg.p);
   });
   SG_CUDA(cudaGetLastError());
   SG_CUDA(cudaStreamSynchronize(s));
@@ -600,19 +612,48 @@ void build_sources(sg_net *net) {
       se_code[pos] = sr.code[k];
     }
   }
+  // run-length encoding per block (runs never cross blocks; <= 2^20 long)
+  std::vector<uint32_t> run_lo((size_t)G + 1, 0), r_src0, r_post0, r_len, r_seed0;
+  std::vector<float> r_w, r_p;
+  std::vector<uint8_t> r_code;
+  for (uint32_t jb = 0; jb < G; ++jb) {
+    run_lo[jb] = (uint32_t)r_len.size();
+    for (uint32_t e = lo[jb]; e < lo[jb + 1]; ++e) {
+      const uint32_t src = se_src[e];
+      const bool extend = e > lo[jb] && !r_len.empty() && r_len.back() < (1u << 20) &&
+                          src == r_src0.back() + r_len.back() && se_post[e] == r_post0.back() + r_len.back() &&
+                          seed[src] == r_seed0.back() + r_len.back() &&
+                          std::memcmp(&se_w[e], &r_w.back(), 4) == 0 && se_code[e] == r_code.back() &&
+                          std::memcmp(&p[src], &r_p.back(), 4) == 0;
+      if (extend) {
+        r_len.back()++;
+      } else {
+        r_src0.push_back(src);
+        r_post0.push_back(se_post[e]);
+        r_len.push_back(1);
+        r_seed0.push_back(seed[src]);
+        r_w.push_back(se_w[e]);
+        r_p.push_back(p[src]);
+        r_code.push_back(se_code[e]);
+      }
+    }
+  }
+  run_lo[G] = (uint32_t)r_len.size();
+  net->n_runs = r_len.size();
   net->n_src_edges = tot;
   auto up = [&](auto &buf, const auto &vec) {
     using T = typename std::decay_t<decltype(vec)>::value_type;
     buf.alloc(std::max<size_t>(vec.size(), 1));
     if (!vec.empty()) SG_CUDA(cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice, net->stream));
   };
-  up(net->d_src_p, p);
-  up(net->d_src_seed, seed);
-  up(net->d_src_lo, lo);
-  up(net->d_se_src, se_src);
-  up(net->d_se_post, se_post);
-  up(net->d_se_w, se_w);
-  up(net->d_se_code, se_code);
+  up(net->d_run_lo, run_lo);
+  up(net->d_run_src0, r_src0);
+  up(net->d_run_post0, r_post0);
+  up(net->d_run_len, r_len);
+  up(net->d_run_seed0, r_seed0);
+  up(net->d_run_w, r_w);
+  up(net->d_run_p, r_p);
+  up(net->d_run_code, r_code);
   SG_CUDA(cudaStreamSynchronize(net->stream));
   for (auto &sr : net->srcs) {  // host copies are no longer needed
     std::vector<uint32_t>().swap(sr.post);
@@ -634,7 +675,7 @@ void build_stdp(sg_net *net) {
   cnt.alloc((size_t)Nd + 1);
   cnt.zero(s);
   launch_grid(Nd, [&](unsigned b) {
-    csc_count_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, net->d_code.p, Nd, cnt.p);
+    csc_count_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_code.p, net->packed, Nd, cnt.p);
   });
   ip64.alloc((size_t)Nd + 1);
   size_t tb = 0;
@@ -653,7 +694,7 @@ void build_stdp(sg_net *net) {
   cursor.alloc((size_t)Nd + 1);
   SG_CUDA(cudaMemcpyAsync(cursor.p, net->d_in_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToDevice, s));
   launch_grid(Nd, [&](unsigned b) {
-    csc_fill_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_col.p, net->d_code.p, Nd, cursor.p,
+    csc_fill_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_code.p, net->packed, Nd, cursor.p,
                                       net->d_in_edge.p, net->d_in_pre.p);
   });
   SG_CUDA(cudaStreamSynchronize(s));
@@ -1491,15 +1532,17 @@ int sg_events_total(sg_net *net, uint64_t *out) {
 static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *d, bool only_w) {
   const uint32_t Nd = net->Nd;
   const uint64_t E = net->n_edges;
-  std::vector<uint32_t> rp(Nd + 1), c(E);
-  std::vector<uint8_t> code(E);
+  std::vector<uint32_t> rp(Nd + 1);
+  std::vector<uint2> ed(E);
+  std::vector<uint8_t> code(net->packed ? 0 : E);
   SG_CUDA(cudaMemcpyAsync(rp.data(), net->d_row_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToHost, net->stream));
   if (E) {
-    if (!only_w) SG_CUDA(cudaMemcpyAsync(c.data(), net->d_col.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
-    SG_CUDA(cudaMemcpyAsync(w, net->d_w.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
-    if (!only_w) SG_CUDA(cudaMemcpyAsync(code.data(), net->d_code.p, E, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(ed.data(), net->d_edge.p, E * 8, cudaMemcpyDeviceToHost, net->stream));
+    if (!net->packed && !only_w)
+      SG_CUDA(cudaMemcpyAsync(code.data(), net->d_code.p, E, cudaMemcpyDeviceToHost, net->stream));
   }
   SG_CUDA(cudaStreamSynchronize(net->stream));
+  for (uint64_t e = 0; e < E; ++e) std::memcpy(&w[e], &ed[e].y, 4);
   if (only_w) return;
   // device index -> global index
   std::vector<uint32_t> d2g(Nd, 0xFFFFFFFFu);
@@ -1510,8 +1553,10 @@ static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float
     for (uint32_t i = 0; i < net->pops[p].n; ++i) row_ptr[net->offsets[p] + i] = rp[net->pops[p].dev_off + i];
   row_ptr[net->total] = (uint32_t)E;
   for (uint64_t e = 0; e < E; ++e) {
-    col[e] = d2g[c[e]];
-    d[e] = (uint8_t)code_delay(code[e]);
+    const uint32_t post = net->packed ? (ed[e].x & 0x00FFFFFFu) : ed[e].x;
+    const uint8_t c = net->packed ? (uint8_t)(ed[e].x >> 24) : code[e];
+    col[e] = d2g[post];
+    d[e] = (uint8_t)code_delay(c);
   }
 }
 
@@ -1600,10 +1645,9 @@ int sg_footprint(sg_net *net, uint64_t *out) {
     SG_REQUIRE(out, SG_E_INVALID, "null output");
     uint64_t b = 0;
     for (auto &p : net->pops) b += (p.d_params.n + p.d_state.n) * 4;
-    b += net->d_ring.n * 4 + net->d_kin_g.n * 4 + net->d_row_ptr.n * 4 + net->d_col.n * 4 + net->d_w.n * 4 +
-         net->d_code.n + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
-         net->d_src_p.n * 4 + net->d_src_seed.n * 4 + net->d_src_lo.n * 4 + net->d_se_src.n * 4 +
-         net->d_se_post.n * 4 + net->d_se_w.n * 4 + net->d_se_code.n + net->d_raster.n * 4 +
+    b += net->d_ring.n * 4 + net->d_kin_g.n * 4 + net->d_row_ptr.n * 4 + net->d_edge.n * 8 +
+         (net->packed ? 0 : net->d_code.n) + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
+         net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
          (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4;
     *out = b;

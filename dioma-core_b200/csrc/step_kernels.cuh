@@ -79,11 +79,12 @@ struct StepArgs {
   float kin_a[3];
   float kin_erev[3];
   float *kin_g;  // [n_kin][Nd]
-  // CSR (device neuron indices), rows sorted by post
+  // CSR (device neuron indices), rows sorted by post; one 8-byte record per
+  // synapse: x = post | code << 24 (packed) or post (code in `code`), y = weight
   const uint32_t *row_ptr;
-  const uint32_t *col;
-  float *w;
-  const uint8_t *code;
+  uint2 *edge;
+  const uint8_t *code;  // null when packed
+  uint32_t post_mask;
   uint32_t n_edges;
   // per-row segment table: [Nd][G+1] offsets inside the row (u16 or u32)
   const void *seg;
@@ -91,14 +92,17 @@ struct StepArgs {
   uint32_t G;      // scatter blocks
   uint32_t P;      // posts per scatter block (multiple of 32)
   uint32_t pbits;  // bits of a local post index
-  // Poisson sources, per scatter block: entries [src_lo[j], src_lo[j+1])
-  const float *src_p;
-  const uint32_t *src_seed;
-  const uint32_t *src_lo;
-  const uint32_t *se_src;
-  const uint32_t *se_post;
-  const float *se_w;
-  const uint8_t *se_code;
+  // Poisson-source synapses of scatter block j: runs [run_lo[j], run_lo[j+1]);
+  // entry t of a run is source run_src0 + t -> post run_post0 + t, seed
+  // run_seed0 + t, with the run's rate, weight and code
+  const uint32_t *run_lo;
+  const uint32_t *run_src0;
+  const uint32_t *run_post0;
+  const uint32_t *run_len;
+  const uint32_t *run_seed0;
+  const float *run_w;
+  const float *run_p;
+  const uint8_t *run_code;
   // scatter mode
   int deterministic;
   // pair STDP
@@ -122,6 +126,50 @@ struct PopArgs {
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// L2 cache policies: the CSR of the spiking rows streams through once per
+// step (evict first); the delay ring is re-read every step (evict last) and
+// has to stay resident in L2 for the scatter's random read-modify-writes.
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long policy_evict_last() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t *p, unsigned long long pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_stream_f32(const float *p, unsigned long long pol) {
+  float v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_stream_u8(const uint8_t *p, unsigned long long pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u8 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint2 ld_stream_edge(const uint2 *p, unsigned long long pol) {
+  uint2 v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_ring(const float *p, unsigned long long pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_ring(float *p, float v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
 
 // ---------------------------------------------------------------------------
 // neuron phase
@@ -351,52 +399,83 @@ __device__ __forceinline__ void clear_heads(ScatterSmem &S) {
   for (uint32_t r = 0; r < kBPT; ++r) S.head[threadIdx.x + r * kScatterThreads] = kEmpty;
 }
 
-// Prepend event k to the list of its post bucket (arrival order).
-__device__ __forceinline__ void link_event(const StepArgs &a, ScatterSmem &S, uint32_t k) {
-  const uint32_t b = S.ecell[k] & (kBuckets - 1u) & ((1u << a.pbits) - 1u);
-  const uint32_t prev = atomicExch(&S.head[b], k);
+__device__ __forceinline__ uint32_t bucket_of(uint32_t cell) { return (cell * 2654435761u) >> (32 - 13); }
+static_assert(kBuckets == 8192, "bucket_of assumes 2^13 buckets");
+
+// Prepend event k to the list of its bucket (arrival order).
+__device__ __forceinline__ void link_event(ScatterSmem &S, uint32_t k) {
+  const uint32_t prev = atomicExch(&S.head[bucket_of(S.ecell[k])], k);
   S.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
 }
 
-// Each thread owns buckets b = threadIdx.x + r * kScatterThreads and adds
-// their events to the ring in ascending window (= reference) order.  A
-// bucket holds one post's events (several posts only when a block owns more
-// than kBuckets posts), so every ring cell sees its adds in order.
-__device__ __forceinline__ void apply_buckets(const StepArgs &a, ScatterSmem &S, uint32_t p0) {
-  uint32_t hd[kBPT];
-  float v[kBPT];
-  uint32_t single = 0;
+// Apply the window's m linked events to the ring in reference order.  Each
+// event finds, in its bucket's list, its rank among the earlier events of
+// the same cell, its predecessor, and whether a later one exists.  Rank-0
+// events load the ring value (all loads in flight together); partial sums
+// then advance one rank per level in shared memory (ew[k] becomes the cell's
+// running value after event k); the last event of each cell stores it.
+// Called by all threads after the linking barrier; ends with a barrier.
+__device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t p0) {
+  const unsigned long long pol = policy_evict_last();
+  uint32_t rk[kEPT], pv[kEPT], lastm = 0, maxrank = 0;
+  float w[kEPT];
 #pragma unroll
-  for (uint32_t r = 0; r < kBPT; ++r) {
-    hd[r] = S.head[threadIdx.x + r * kScatterThreads];
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t k = threadIdx.x + r * kScatterThreads;
+    rk[r] = 0;
+    pv[r] = kNone16;
+    w[r] = 0.0f;
+    if (k < m) {
+      const uint32_t c = S.ecell[k];
+      bool last = true;
+      for (uint32_t j = S.head[bucket_of(c)]; j != kNone16; j = S.enext[j]) {
+        if (j == k || S.ecell[j] != c) continue;
+        if (j < k) {
+          ++rk[r];
+          if (pv[r] == kNone16 || j > pv[r]) pv[r] = j;
+        } else {
+          last = false;
+        }
+      }
+      lastm |= (last ? 1u : 0u) << r;
+      maxrank = max(maxrank, rk[r]);
+      w[r] = S.ew[k];
+    }
+  }
+  // level 0: one ring load per cell
+  float v[kEPT];
+#pragma unroll
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t k = threadIdx.x + r * kScatterThreads;
     v[r] = 0.0f;
-    if (hd[r] != kEmpty && S.enext[hd[r]] == kNone16) {
-      single |= 1u << r;
-      v[r] = *cell_addr(a, S.ecell[hd[r]], p0);  // loads issued together
-    }
+    if (k < m && rk[r] == 0) v[r] = ld_ring(cell_addr(a, S.ecell[k], p0), pol);
   }
 #pragma unroll
-  for (uint32_t r = 0; r < kBPT; ++r) {
-    if (hd[r] == kEmpty) continue;
-    if (single & (1u << r)) {
-      *cell_addr(a, S.ecell[hd[r]], p0) = v[r] + S.ew[hd[r]];
-      continue;
-    }
-    // several events: take them in ascending window order (selection over
-    // the short list), one read-modify-write each
-    uint32_t last = 0;
-    bool first = true;
-    while (true) {
-      uint32_t best = kEmpty;
-      for (uint32_t j = hd[r]; j != kNone16; j = S.enext[j])
-        if ((first || j > last) && j < best) best = j;
-      if (best == kEmpty) break;
-      float *p = cell_addr(a, S.ecell[best], p0);
-      *p = *p + S.ew[best];
-      last = best;
-      first = false;
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t k = threadIdx.x + r * kScatterThreads;
+    if (k < m && rk[r] == 0) {
+      v[r] = v[r] + w[r];
+      S.ew[k] = v[r];
     }
   }
+  // later ranks: partial sums in order, one level per round
+  for (uint32_t lvl = 1; __syncthreads_or(maxrank >= lvl); ++lvl) {
+#pragma unroll
+    for (uint32_t r = 0; r < kEPT; ++r) {
+      const uint32_t k = threadIdx.x + r * kScatterThreads;
+      if (k < m && rk[r] == lvl) {
+        v[r] = S.ew[pv[r]] + w[r];
+        S.ew[k] = v[r];
+      }
+    }
+  }
+  // the last event of each cell stores the cell's value
+#pragma unroll
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t k = threadIdx.x + r * kScatterThreads;
+    if (k < m && (lastm & (1u << r))) st_ring(cell_addr(a, S.ecell[k], p0), v[r], pol);
+  }
+  __syncthreads();
 }
 
 // One event into the window (or straight into the ring in atomic mode).
@@ -520,13 +599,15 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
         uint32_t ev_post[kEPT];
         float ev_w[kEPT];
         uint8_t ev_code[kEPT];
+        const unsigned long long spol = policy_evict_first();
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
           if (k < m) {
-            ev_post[r] = __ldg(a.col + ev_e[r]);
-            ev_w[r] = a.w[ev_e[r]];
-            ev_code[r] = __ldg(a.code + ev_e[r]);
+            const uint2 rec = ld_stream_edge(a.edge + ev_e[r], spol);
+            ev_post[r] = rec.x & a.post_mask;
+            ev_w[r] = __uint_as_float(rec.y);
+            ev_code[r] = a.code ? (uint8_t)ld_stream_u8(a.code + ev_e[r], spol) : (uint8_t)(rec.x >> 24);
           }
         }
 #pragma unroll
@@ -537,62 +618,78 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
             if (a.stdp && code_stdp(ev_code[r])) {
               // depression at a pre spike; the pushed weight is the pre-update one
               const float w1 = fminf(fmaxf(ev_w[r] - a.a_minus * a.x_post[ev_post[r]], a.w_min), a.w_max);
-              a.w[ev_e[r]] = w1;
+              a.edge[ev_e[r]].y = __float_as_uint(w1);
               atomicAdd(&S.drift, (double)w1 - (double)ev_w[r]);
             }
-            if (a.deterministic) link_event(a, S, k);
+            if (a.deterministic) link_event(S, k);
           }
         }
         __syncthreads();
-        if (a.deterministic) {
-          apply_buckets(a, S, p0);
-          __syncthreads();
-        }
+        if (a.deterministic) apply_window(a, S, m, p0);
       }
     }
   }
   // ---- Poisson sources targeting this block's posts, in source order ----
-  const uint32_t lst0 = a.src_lo[j], lst1 = a.src_lo[j + 1];
-  for (uint32_t base = lst0; base < lst1; base += kWin) {
-    if (a.deterministic) clear_heads(S);
-    // thread tid owns entries [base + tid*kEPT, +kEPT): order-preserving compaction
-    uint32_t sp_src[kEPT], sp_post[kEPT];
-    float sp_w[kEPT];
-    uint8_t sp_code[kEPT];
+  const uint32_t rl0 = a.run_lo[j], rl1 = a.run_lo[j + 1];
+  for (uint32_t rc0 = rl0; rc0 < rl1; rc0 += kPreChunk) {
+    const uint32_t rc = min(kPreChunk, rl1 - rc0);
+    // runs tid*kPPT .. +kPPT of this chunk
+    uint32_t len[kPPT], mylen = 0;
 #pragma unroll
-    for (uint32_t r = 0; r < kEPT; ++r) {
-      const uint32_t e = base + tid * kEPT + r;
-      if (e < lst1) {
-        sp_src[r] = a.se_src[e];
-        sp_post[r] = a.se_post[e];
-        sp_w[r] = a.se_w[e];
-        sp_code[r] = a.se_code[e];
-      }
+    for (uint32_t q = 0; q < kPPT; ++q) {
+      const uint32_t i = tid * kPPT + q;
+      len[q] = i < rc ? a.run_len[rc0 + i] : 0u;
+      mylen += len[q];
     }
-    uint32_t fired = 0;
+    uint32_t T;
+    uint32_t ex = block_excl_scan(mylen, S.wsum, &T);
 #pragma unroll
-    for (uint32_t r = 0; r < kEPT; ++r) {
-      const uint32_t e = base + tid * kEPT + r;
-      if (e < lst1) {
-        const float p = a.src_p[sp_src[r]];
-        if (p > 0.0f && poisson_spike(a.src_seed[sp_src[r]], 0, step, p)) fired |= 1u << r;
-      }
+    for (uint32_t q = 0; q < kPPT; ++q) {
+      S.pseg[tid * kPPT + q] = ex;
+      ex += len[q];
     }
-    uint32_t m;
-    uint32_t pos = block_excl_scan(__popc(fired), S.wsum, &m);
-#pragma unroll
-    for (uint32_t r = 0; r < kEPT; ++r)
-      if (fired & (1u << r)) put_event(a, S, pos++, sp_post[r], sp_w[r], sp_code[r], step, p0);
-    if (tid == 0) S.events += m;
-    if (a.deterministic && m) {
+    if (tid == 0) S.pseg[kPreChunk] = T;
+    __syncthreads();
+    for (uint32_t w0 = 0; w0 < T; w0 += kWin) {
+      const uint32_t mt = min(kWin, T - w0);
+      if (a.deterministic) clear_heads(S);
       __syncthreads();
+      // thread tid owns entries [tid*kEPT, +kEPT) of the window: roll them,
+      // then an order-preserving compaction of the fired ones
+      uint32_t fired = 0, e_post[kEPT];
+      float e_w[kEPT];
+      uint8_t e_code[kEPT];
 #pragma unroll
       for (uint32_t r = 0; r < kEPT; ++r) {
-        const uint32_t k = tid + r * kScatterThreads;
-        if (k < m) link_event(a, S, k);
+        const uint32_t k = tid * kEPT + r;
+        if (k < mt) {
+          // runs are few and long: find the run by search (balanced)
+          const uint32_t g = w0 + k;
+          const uint32_t i = upper_index(S.pseg, rc, g);
+          const uint32_t ri = rc0 + i, t = g - S.pseg[i];
+          const float p = __ldg(a.run_p + ri);
+          e_post[r] = __ldg(a.run_post0 + ri) + t;
+          e_w[r] = __ldg(a.run_w + ri);
+          e_code[r] = __ldg(a.run_code + ri);
+          if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + ri) + t, 0, step, p)) fired |= 1u << r;
+        }
       }
+      uint32_t m;
+      uint32_t pos = block_excl_scan(__popc(fired), S.wsum, &m);  // all reads of the window are done
+#pragma unroll
+      for (uint32_t r = 0; r < kEPT; ++r)
+        if (fired & (1u << r)) put_event(a, S, pos++, e_post[r], e_w[r], e_code[r], step, p0);
+      if (tid == 0) S.events += m;
       __syncthreads();
-      apply_buckets(a, S, p0);
+      if (a.deterministic && m) {
+#pragma unroll
+        for (uint32_t r = 0; r < kEPT; ++r) {
+          const uint32_t k = tid + r * kScatterThreads;
+          if (k < m) link_event(S, k);
+        }
+        __syncthreads();
+        apply_window(a, S, m, p0);
+      }
     }
     __syncthreads();
   }
@@ -608,9 +705,9 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
         const uint32_t q = wd * 32 + b;
         for (uint32_t k = a.in_ptr[q]; k < a.in_ptr[q + 1]; ++k) {
           const uint32_t e = a.in_edge[k];
-          const float w0 = a.w[e];
+          const float w0 = __uint_as_float(a.edge[e].y);
           const float w1 = fminf(fmaxf(w0 + a.a_plus * a.x_pre[a.in_pre[k]], a.w_min), a.w_max);
-          a.w[e] = w1;
+          a.edge[e].y = __float_as_uint(w1);
           atomicAdd(&S.drift, (double)w1 - (double)w0);
         }
       }
