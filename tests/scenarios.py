@@ -156,3 +156,74 @@ def lif_small_balanced(make_net, n=2000, k_in=100, steps=300, device_generator=F
         net.step(1)
         raster.append(net.spikes(pop).copy())
     return net, pop, np.array(raster)
+
+
+def hh_network(make_net, n=240, k_out=12, steps=400, seed=11, stdp=True, precision_net=None):
+    """A downscaled HH network with conductance synapses and pair STDP: HH
+    neurons (squid axon, RK4, dt 0.01 ms), ExpOne E (0 mV) / I (-80 mV)
+    synapses tau 5 ms, lognormal out-degree, 80/20 E/I, bias N(10, 2),
+    weights U(0, 0.5) nS, STDP on E synapses (tau 20 ms, A+ 0.01, A- 0.0105,
+    clip [0, 1])."""
+    rng = np.random.default_rng(seed)
+    dt = 0.01
+    net = make_net()
+    n_e = n * 4 // 5
+    pe = net.add_population(HH, n_e)
+    pi = net.add_population(HH, n - n_e)
+    for p, cnt in ((pe, n_e), (pi, n - n_e)):
+        for col, v in enumerate([dt, 1.0, 120.0, 36.0, 0.3, 50.0, -77.0, -54.4, 0.0, 0.0]):
+            net.fill_param(p, col, v)
+        net.set_param(p, 8, rng.normal(10.0, 2.0, cnt).astype(np.float32))
+        v0 = rng.uniform(-70, -60, cnt).astype(np.float32)
+        net.set_state(p, 0, v0)
+        net.fill_state(p, 1, 0.0529)
+        net.fill_state(p, 2, 0.5961)
+        net.fill_state(p, 3, 0.3177)
+    ke = net.register_expone(5.0, 0.0, dt)
+    ki = net.register_expone(5.0, -80.0, dt)
+    net.stdp_config(dt, 20.0, 20.0, 0.01, 0.0105, 0.0, 1.0)
+    sigma = np.sqrt(np.log(1 + (0.4) ** 2))
+    for src_pop, cnt, st, plastic in ((pe, n_e, ke, stdp), (pi, n - n_e, ki, False)):
+        deg = np.clip(np.round(rng.lognormal(np.log(k_out) - sigma ** 2 / 2, sigma, cnt)), 1, None).astype(int)
+        pre = np.repeat(np.arange(cnt), deg).astype(np.uint32)
+        tot = pre.size
+        tgt = rng.integers(0, n, tot)
+        for dst_pop, lo, hi in ((pe, 0, n_e), (pi, n_e, n)):
+            sel = (tgt >= lo) & (tgt < hi)
+            k = int(sel.sum())
+            if k == 0:
+                continue
+            net.connect(src_pop, pre[sel], dst_pop, (tgt[sel] - lo).astype(np.uint32),
+                        rng.uniform(0, 0.5, k).astype(np.float32), rng.integers(1, 30, k).astype(np.uint8),
+                        syn_types=np.full(k, st, np.uint8), stdp=plastic)
+    net.build()
+    rast = []
+    for s in range(steps):
+        net.step(1)
+        rast.append(np.concatenate([net.spikes(pe), net.spikes(pi)]))
+    return net, (pe, pi), np.array(rast)
+
+
+def gpea_network(make_net, n=64, steps=300, seed=5):
+    """A small GPEA population with random synapses and a current step."""
+    rng = np.random.default_rng(seed)
+    net = make_net()
+    p = net.add_population(GPEA, n)
+    params = [0.025, 24.0, 1.0, 0.0, 2513.2742, 50.0, 10.0, 0.05, -60.0, 0.5, 1.0, 2.0, 3.355e-11, 0.1]
+    for col, v in enumerate(params):
+        net.fill_param(p, col, v)
+    net.set_state(p, 0, rng.uniform(-65, -55, n).astype(np.float32))
+    for col, v in ((1, 0.05), (2, 0.6), (3, 0.3), (4, 0.1), (5, 0.5), (6, 5e-5), (7, 0.0), (8, 1.0)):
+        net.fill_state(p, col, v)
+    k = n * 6
+    net.connect(p, rng.integers(0, n, k).astype(np.uint32), p, rng.integers(0, n, k).astype(np.uint32),
+                rng.uniform(0, 8, k).astype(np.float32), rng.integers(1, 8, k).astype(np.uint8))
+    net.build()
+    idx = np.arange(n, dtype=np.uint32)
+    rast, v = [], []
+    for s in range(steps):
+        if s > 20:
+            net.inject_current(p, idx, np.full(n, 12.0, np.float32))
+        net.step(1)
+        rast.append(net.spikes(p).copy())
+    return net, p, np.array(rast)
