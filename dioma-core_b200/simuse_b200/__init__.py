@@ -18,3 +18,4 @@ from .network import (  # noqa: F401
     W_FP8,
     Network,
 )
+from .kuramoto import KuramotoBatch  # noqa: F401,E402

@@ -75,6 +75,17 @@ SIGNATURES = {
     "sg_stream": [vp, vp],
     "sg_push_spikes": [vp, vp, vp, vp, u32, vp, u32, u64, vp, vp],
     "sg_push_spikes_noalloc": [vp, vp, vp, vp, u32, vp, u32, u64, vp, vp],
+    "sg_kuramoto_create": [vp, i32, u32, vp, vp, f32],
+    "sg_kuramoto_destroy": [vp],
+    "sg_kuramoto_total": [vp, vp],
+    "sg_kuramoto_set_state": [vp, vp, vp],
+    "sg_kuramoto_record": [vp, u64],
+    "sg_kuramoto_run": [vp, u32],
+    "sg_kuramoto_synchronize": [vp],
+    "sg_kuramoto_get_theta": [vp, vp],
+    "sg_kuramoto_get_r": [vp, vp, u64, vp],
+    "sg_kuramoto_get_r_mean": [vp, vp],
+    "sg_kuramoto_stream": [vp, vp],
 }
 
 _lib = None

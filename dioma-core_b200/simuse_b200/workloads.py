@@ -199,3 +199,26 @@ def build_lif(net, spec: dict, model_lif: int = 1, device_generator: bool = True
             s = net.add_poisson_source(spec["ext_rate_hz"], spec["dt"], i)
             net.connect_poisson_source(s, pop, np.array([i], np.uint32), ones_w, one_d)
     return pop
+
+
+# ---------------------------------------------------------------------------
+# Kuramoto sweep (the oscillator half of the batched uneven sweep)
+# ---------------------------------------------------------------------------
+def kuramoto_sweep(n_inst: int = 1024, n_min: int = 256, n_max: int = 65536, k_max: float = 4.0,
+                   gamma: float = 0.5, seed: int = 0) -> dict:
+    """``n_inst`` all-to-all Kuramoto populations: N log-uniform in
+    [n_min, n_max], coupling K linearly from 0 to k_max over the instances,
+    theta0 ~ U(-pi, pi), omega ~ Lorentzian(0, gamma) by the inverse CDF
+    gamma*tan(pi*(u - 1/2)) in FP64, rounded to FP32."""
+    i = np.arange(n_inst, dtype=np.uint64)
+    u = uniform01(seed, 1, i)
+    sizes = np.floor(np.exp(np.log(n_min) + u * (np.log(n_max + 1) - np.log(n_min)))).astype(np.int64)
+    sizes = np.clip(sizes, n_min, n_max).astype(np.uint32)
+    coupling = (np.linspace(0.0, k_max, n_inst) if n_inst > 1 else np.zeros(1)).astype(np.float32)
+    total = int(sizes.astype(np.int64).sum())
+    j = np.arange(total, dtype=np.uint64)
+    theta = ((uniform01(seed, 2, j) * 2.0 - 1.0) * np.pi).astype(np.float32)
+    uo = uniform01(seed, 3, j)
+    uo = np.clip(uo, 1e-12, 1.0 - 1e-12)
+    omega = (gamma * np.tan(np.pi * (uo - 0.5))).astype(np.float32)
+    return dict(sizes=sizes, coupling=coupling, theta=theta, omega=omega, dt=0.01, seed=seed)

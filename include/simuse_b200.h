@@ -212,6 +212,39 @@ int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *col, const f
                            const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
                            uint32_t n_active, uint64_t step, float *ring, void *stream);
 
+/* ---- batched Kuramoto populations ----------------------------------------- */
+/* A batch of independent all-to-all Kuramoto populations integrated by RK4:
+     dth_i/dt = omega_i + K/N sum_j sin(th_j - th_i)
+              = omega_i + K (S cos th_i - C sin th_i),  C + iS = mean e^{i th},
+   the exact mean-field identity of crates/SiMuse/crates/t3/src/oscillator.rs:
+   15-20,549, so each RK4 stage costs one O(N) reduction instead of the O(N^2)
+   dense sum of P/kernels/phase/sparse.rs:40-140.  After each step the phase
+   wraps to [-pi, pi] as P/kernels/phase/kuramoto.rs:42-68 does
+   (th - 2 pi round(th / 2 pi)).  Phases are FP32; the order parameter
+   r(t) = |mean e^{i th}| is recorded per step in FP32 and its time average is
+   accumulated in FP64 (t3/src/oscillator.rs:440-450).  Instance sizes are
+   1..65,536 oscillators; instance i's oscillators are [off_i, off_i + n_i)
+   with off_i the prefix sum of sizes. */
+typedef struct sg_kura sg_kura;
+int sg_kuramoto_create(sg_kura **out, int device, uint32_t n_instances, const uint32_t *sizes,
+                       const float *coupling, float dt);
+int sg_kuramoto_destroy(sg_kura *kb);
+/* Total oscillators over all instances (length of theta/omega arrays). */
+int sg_kuramoto_total(sg_kura *kb, uint64_t *out);
+/* Phases (radians) and natural frequencies, `total` each, instance-major. */
+int sg_kuramoto_set_state(sg_kura *kb, const float *theta, const float *omega);
+/* Keep r(t) of the next `max_steps` steps (0 turns recording off). */
+int sg_kuramoto_record(sg_kura *kb, uint64_t max_steps);
+/* Advance every instance by n_steps RK4 steps (asynchronous). */
+int sg_kuramoto_run(sg_kura *kb, uint32_t n_steps);
+int sg_kuramoto_synchronize(sg_kura *kb);
+int sg_kuramoto_get_theta(sg_kura *kb, float *theta);
+/* Recorded r(t), [n_instances][n_steps] row-major; cap = floats available. */
+int sg_kuramoto_get_r(sg_kura *kb, float *r, uint64_t cap, uint64_t *n_steps);
+/* Time average of r(t) over all steps run so far, FP64, per instance. */
+int sg_kuramoto_get_r_mean(sg_kura *kb, double *r_mean);
+int sg_kuramoto_stream(sg_kura *kb, void **out);
+
 #ifdef __cplusplus
 }
 #endif

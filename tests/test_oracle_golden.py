@@ -173,3 +173,32 @@ def test_hh_fp32_vs_fp64_close():
     assert np.array_equal(r32, r64)
     assert r32.sum() > 0
     assert np.max(np.abs(v32 - v64)) < 1e-2
+
+
+def test_kuramoto_oracle_mean_field_is_the_dense_sum():
+    """The oracle's mean-field coupling K*(S cos th_i - C sin th_i) equals the
+    dense K/N sum_j sin(th_j - th_i) of P/kernels/phase/sparse.rs:40-140, and
+    its RK4 + wrap (P/kernels/mod.rs:74-77) matches an independent FP64 RK4."""
+    rng = np.random.default_rng(12)
+    n, K, dt, steps = 48, 1.3, 0.05, 7
+    th0 = rng.uniform(-np.pi, np.pi, n).astype(np.float32)
+    om = rng.normal(0, 1, n).astype(np.float32)
+
+    Kd, hd = float(np.float32(K)), float(np.float32(dt))  # the C ABI takes K and dt as f32
+
+    def f(x):
+        return om.astype(np.float64) + Kd / n * np.sin(x[None, :] - x[:, None]).sum(axis=1)
+
+    x = th0.astype(np.float64)
+    r_ref = []
+    for _ in range(steps):
+        k1 = f(x)
+        k2 = f(x + hd / 2 * k1)
+        k3 = f(x + hd / 2 * k2)
+        k4 = f(x + hd * k3)
+        x = x + hd / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+        x = x - 2 * np.pi * np.round(x / (2 * np.pi))
+        r_ref.append(abs(np.exp(1j * x).mean()))
+    th, r = O.kuramoto_rk4(th0, om, K, dt, steps, precision=1)
+    assert np.abs(np.angle(np.exp(1j * (th - x)))).max() < 1e-6  # th is rounded to f32
+    assert np.abs(r - np.array(r_ref)).max() < 1e-12
