@@ -90,7 +90,8 @@ def config(args, name, spec):
         "sim_steps_per_bench_step": args.sim_steps,
         "external_drive": {"rate_hz": spec["ext_rate_hz"], "ring_weight": spec["ext_weight"]},
         "weights": "fp32", "scatter": "deterministic (reference summation order)",
-        "l2": "inputs larger than L2 (9 GB CSR streamed every step)",
+        "l2": "inputs larger than L2: 8 GB of synapse records and 128 MB of delay rings against a "
+              "126 MB L2; each step reads the spiking rows",
         "parallelism": f"replicas x{args.gpus}",
     }
 
@@ -189,13 +190,18 @@ def measured_peak():
 
 
 def profiled_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    """DRAM bytes (read + write) per launch of `kernel` on the bench workload,
+    from the committed ncu summary profiles/dram_traffic.txt (lines
+    `<kernel> dram_bytes_per_launch=<bytes>`)."""
+    import re
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        v = d.get(kernel)
-        return None if v is None else float(v["dram_bytes_per_launch"])
-    except Exception:
-        return None
+        for line in open(os.path.join(ROOT, "profiles", "dram_traffic.txt")):
+            m = re.match(r"\s*(\S+)\s+dram_bytes_per_launch=([0-9.eE+]+)", line)
+            if m and m.group(1) == kernel:
+                return float(m.group(2))
+    except OSError:
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------

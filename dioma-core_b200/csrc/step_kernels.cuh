@@ -22,12 +22,15 @@
 // (push.rs:143-172, step.rs:166-185).  A block generates its events exactly
 // in that order (rows are stored sorted by post with a stable sort, which
 // keeps the relative order of repeated synapses to one post), in windows of
-// up to kWin events.  Inside a window, cells are entered in an exact
-// shared-memory hash table; ownership rounds (atomicMin on the window index)
-// link the events of each cell into a chain in window order; the chain head
-// loads the ring value once, adds the chain's weights in order and stores
-// it.  Windows are applied one after another.  Every cell therefore receives
-// its adds in the reference's order, with the reference's rounding.
+// up to kWin events.  Inside a window every event is prepended to the list of
+// its cell's bucket (8192 buckets hashed from the cell); walking that list,
+// an event finds its rank among the window's earlier events of the same
+// cell, its predecessor, and whether a later one exists.  Rank-0 events load
+// the ring value (all loads in flight together), partial sums then advance
+// one rank per level in shared memory, and the last event of each cell
+// stores the cell's value.  Windows are applied one after another.  Every
+// cell therefore receives its adds in the reference's order, with the
+// reference's rounding.
 #pragma once
 #include <cstdint>
 
