@@ -105,6 +105,8 @@ struct sg_net {
   std::vector<uint32_t> offsets{0};  // reference global offsets
   uint64_t total = 0;                // reference neuron count
   uint32_t Nd = 0;                   // padded device neuron count
+  uint32_t max_delay = 0;            // largest synaptic delay added so far
+  uint32_t nslots = kSlots;          // ring slots in use (largest effective delay + 1)
   // staged edges (device)
   DVec<uint32_t> e_pre, e_post;
   DVec<float> e_w;
@@ -225,6 +227,7 @@ StepArgs make_args(sg_net *net) {
   a.clamp_hits = net->d_clamp.p;
   a.ring = net->d_ring.p;
   a.Nd = net->Nd;
+  a.nslots = net->nslots;
   a.n_kin = (int)net->kin.size();
   for (size_t k = 0; k < net->kin.size() && k < 3; ++k) {
     a.kin_a[k] = net->kin[k].a_decay;
@@ -551,7 +554,7 @@ void build_segments(sg_net *net) {
   const uint32_t Nd = net->Nd;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
-  uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)sms, Nd / 32));
+  uint32_t G = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)sms * kScatterBlocksPerSM, Nd / 32));
   uint32_t P = std::max<uint32_t>(32, (uint32_t)align_up((Nd + G - 1) / G, 32));
   G = std::max<uint32_t>(1, (Nd + P - 1) / P);
   net->G = G;
@@ -736,7 +739,10 @@ void finish_build(sg_net *net) {
     std::vector<float>().swap(p.state);
   }
   const size_t n_rings = 1 + net->kin.size();
-  net->d_ring.alloc(std::max<size_t>(n_rings * kSlots * Nd, 1));
+  // a step's events land at most max(delay, 1) steps ahead, so that many
+  // slots plus the one being read hold every pending arrival
+  net->nslots = std::max<uint32_t>(net->max_delay, 1u) + 1u;
+  net->d_ring.alloc(std::max<size_t>(n_rings * net->nslots * Nd, 1));
   net->d_ring.zero(s);
   net->d_kin_g.alloc(std::max<size_t>(net->kin.size() * Nd, 1));
   net->d_kin_g.zero(s);
@@ -1056,6 +1062,7 @@ int sg_connect_ex(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, c
       SG_REQUIRE(ti[i] < pt.n, SG_E_INVALID, "to index " + std::to_string(ti[i]) + " out of bounds");
       SG_REQUIRE(std::isfinite(w[i]), SG_E_INVALID, "Network::connect: weight " + std::to_string(i) + " must be finite");
       SG_REQUIRE(d[i] < kSlots, SG_E_INVALID, "delay " + std::to_string(d[i]) + " >= MAX_DELAY_SLOTS (32)");
+      net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
       const uint8_t s = st ? st[i] : 0;
       SG_REQUIRE(s <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
       pre[i] = pf.dev_off + fi[i];
@@ -1088,6 +1095,7 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
     SG_REQUIRE(pf.n > 0 || k_in == 0, SG_E_INVALID, "empty source population");
     const uint64_t n = (uint64_t)pt.n * k_in;
     if (n == 0) return;
+    net->max_delay = std::max<uint32_t>(net->max_delay, d_max);
     DevGuard g(net->device);
     const size_t n0 = net->e_pre.n;
     net->e_pre.reserve(n0 + n, net->stream);
@@ -1155,6 +1163,7 @@ int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *p
       SG_REQUIRE(posts[i] < pt.n, SG_E_INVALID, "post index out of bounds");
       SG_REQUIRE(std::isfinite(w[i]), SG_E_INVALID, "connect_poisson_source: weight must be finite");
       SG_REQUIRE(d[i] < kSlots, SG_E_INVALID, "connect_poisson_source: delay >= MAX_DELAY_SLOTS (32)");
+      net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
       const uint8_t t = st ? st[i] : 0;
       SG_REQUIRE(t <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
       s.post.push_back(pt.dev_off + posts[i]);
@@ -1173,6 +1182,7 @@ int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint3
     require_pop(net, to);
     SG_REQUIRE(std::isfinite(weight), SG_E_INVALID, "weight must be finite");
     SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
+    if (n) net->max_delay = std::max<uint32_t>(net->max_delay, delay);
     const auto &pt = net->pops[to];
     for (uint32_t i = 0; i < n; ++i) {
       const uint32_t q = posts ? posts[i] : i;
@@ -1260,6 +1270,7 @@ int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col,
         SG_REQUIRE(col[e] < N, SG_E_INVALID, "col index out of range");
         SG_REQUIRE(std::isfinite(w[e]), SG_E_INVALID, "weight must be finite");
         SG_REQUIRE(d[e] < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
+        net->max_delay = std::max<uint32_t>(net->max_delay, d[e]);
         pre[e] = g2d[i];
         post[e] = g2d[col[e]];
         code[e] = edge_code(d[e], 0, false);
@@ -1296,7 +1307,7 @@ int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals,
     SG_CUDA(cudaMemcpyAsync(net->d_inj_idx.p, idx, n * 4, cudaMemcpyHostToDevice, net->stream));
     SG_CUDA(cudaMemcpyAsync(net->d_inj_val.p, vals, n * 4, cudaMemcpyHostToDevice, net->stream));
     unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 8);
-    inject_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->d_step.p, net->d_inj_idx.p,
+    inject_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->nslots, net->d_step.p, net->d_inj_idx.p,
                                                    net->d_inj_val.p, n, p.dev_off, dup ? 1 : 0);
     SG_CUDA(cudaGetLastError());
     // the staging buffers are reused by the next call
@@ -1587,16 +1598,25 @@ int sg_ring_read(sg_net *net, uint32_t ring, float *out) {
     SG_REQUIRE(ring <= net->kin.size(), SG_E_INVALID, "ring out of range");
     SG_REQUIRE(out, SG_E_INVALID, "null output");
     DevGuard g(net->device);
-    const uint32_t Nd = net->Nd;
-    std::vector<float> r((size_t)kSlots * Nd);
-    SG_CUDA(cudaMemcpyAsync(r.data(), net->d_ring.p + (size_t)ring * kSlots * Nd, r.size() * 4,
+    const uint32_t Nd = net->Nd, M = net->nslots;
+    std::vector<float> r((size_t)M * Nd);
+    SG_CUDA(cudaMemcpyAsync(r.data(), net->d_ring.p + (size_t)ring * M * Nd, r.size() * 4,
                             cudaMemcpyDeviceToHost, net->stream));
+    unsigned long long step = 0;
+    SG_CUDA(cudaMemcpyAsync(&step, net->d_step.p, sizeof(step), cudaMemcpyDeviceToHost, net->stream));
     SG_CUDA(cudaStreamSynchronize(net->stream));
+    // reference slot s holds the arrivals of the step t in [step, step + 31]
+    // with t % 32 == s; the device keeps t in slot t % M while t - step < M,
+    // and no arrival lies further ahead
     const uint64_t N = net->total;
-    for (uint32_t s = 0; s < kSlots; ++s)
+    for (uint32_t s = 0; s < kSlots; ++s) {
+      const unsigned long long t = step + ((s + kSlots - (uint32_t)(step % kSlots)) % kSlots);
+      const bool held = t - step < M;
+      const uint32_t ds = (uint32_t)(t % M);
       for (size_t p = 0; p < net->pops.size(); ++p)
         for (uint32_t i = 0; i < net->pops[p].n; ++i)
-          out[(size_t)s * N + net->offsets[p] + i] = r[(size_t)s * Nd + net->pops[p].dev_off + i];
+          out[(size_t)s * N + net->offsets[p] + i] = held ? r[(size_t)ds * Nd + net->pops[p].dev_off + i] : 0.0f;
+    }
   });
 }
 

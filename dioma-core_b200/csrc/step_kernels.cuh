@@ -23,7 +23,7 @@
 // in that order (rows are stored sorted by post with a stable sort, which
 // keeps the relative order of repeated synapses to one post), in windows of
 // up to kWin events.  Inside a window every event is prepended to the list of
-// its cell's bucket (8192 buckets hashed from the cell); walking that list,
+// its cell's bucket (kBuckets buckets hashed from the cell); walking that list,
 // an event finds its rank among the window's earlier events of the same
 // cell, its predecessor, and whether a later one exists.  Rank-0 events load
 // the ring value (all loads in flight together), partial sums then advance
@@ -41,11 +41,12 @@ namespace sg {
 
 constexpr uint32_t kNeuronBlock = 1024;  // neurons per neuron-kernel block (= spike-list slot)
 constexpr uint32_t kScatterThreads = 1024;
+constexpr uint32_t kScatterBlocksPerSM = 1;
 constexpr uint32_t kWin = 8192;          // events per window
-constexpr uint32_t kBuckets = 8192;      // per-window event lists, by post (post % kBuckets)
-constexpr uint32_t kPreChunk = 4096;     // spiking rows per sub-chunk (4 per thread)
-constexpr uint32_t kBlkChunk = 1024;     // spike-list slots scanned per chunk
-constexpr uint32_t kNone16 = 0xFFFFu;
+constexpr uint32_t kBucketBits = 13;
+constexpr uint32_t kBuckets = 1u << kBucketBits;  // per-window event lists, by hashed cell
+constexpr uint32_t kPreChunk = 4 * kScatterThreads;  // spiking rows per sub-chunk (4 per thread)
+constexpr uint32_t kBlkChunk = kScatterThreads;      // spike-list slots scanned per chunk
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr unsigned long long kEmpty64 = ~0ull;
 constexpr uint32_t kMaxPops = 16;
@@ -74,9 +75,12 @@ struct StepArgs {
   unsigned long long *stat_ev;
   uint32_t stat_cap;
   unsigned long long *clamp_hits;
-  // rings: [n_rings][32][Nd]
+  // rings: [n_rings][nslots][Nd]; a step's arrivals go to slot step % nslots
+  // (nslots = the largest effective delay + 1, at most 32: the reference's
+  // 32-slot ring, P/api/net/delay.rs:30-101, without the slots no delay reaches)
   float *ring;
   uint32_t Nd;
+  uint32_t nslots;
   // kinetic ExpOne profiles (ring k+1)
   int n_kin;
   float kin_a[3];
@@ -165,9 +169,11 @@ __device__ __forceinline__ uint2 ld_stream_edge(const uint2 *p, unsigned long lo
                : "l"(p), "l"(pol));
   return v;
 }
+// Ring loads do not allocate in L1: a window issues kWin of them per SM at
+// once and the ring is re-read only in later steps.
 __device__ __forceinline__ float ld_ring(const float *p, unsigned long long pol) {
   float v;
-  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol) : "memory");
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_ring(float *p, float v, unsigned long long pol) {
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS) neuron_kernel(StepA
   const uint32_t i0 = blockIdx.x * kNeuronBlock + tid * NPT;  // population index of my first neuron
   const uint32_t gi0 = p.dev_off + i0;
   const unsigned long long step = *a.step;
-  const uint32_t slot = (uint32_t)(step & 31ull);
+  const uint32_t slot = (uint32_t)(step % a.nslots);
   // 1-2. read the slot, clear it (step.rs:27-34)
   float x[NPT], zero[NPT];
 #pragma unroll
@@ -222,7 +228,7 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS) neuron_kernel(StepA
   // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start
   for (int k = 0; k < a.n_kin; ++k) {
     float jump[NPT], g[NPT];
-    float *ks = a.ring + ((size_t)(k + 1) * kSlots + slot) * a.Nd + gi0;
+    float *ks = a.ring + ((size_t)(k + 1) * a.nslots + slot) * a.Nd + gi0;
     V::load(ks, jump);
     V::store(ks, zero);
     float *gp = a.kin_g + (size_t)k * a.Nd + gi0;
@@ -351,7 +357,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *wsum, 
   if (lane == 31) wsum[wid] = x;
   __syncthreads();
   if (wid == 0) {
-    uint32_t t = wsum[lane];
+    uint32_t t = lane < (blockDim.x >> 5) ? wsum[lane] : 0u;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
@@ -376,10 +382,11 @@ __device__ __forceinline__ uint32_t upper_index(const uint32_t *pre, uint32_t n,
 }
 
 struct ScatterSmem {
-  uint32_t head[kBuckets];        // latest event of each post bucket in the window
-  uint32_t ecell[kWin];           // window events in reference order: cell,
+  uint32_t head[kBuckets];        // latest-linked event of each bucket in the window
+  uint32_t ecell[kWin];           // window events in reference order: cell (the edge id
+                                  //   before the cell is known),
   float ew[kWin];                 //   weight,
-  uint16_t enext[kWin];           //   previous event of the same bucket
+  uint16_t enext[kWin];           //   next event of the same bucket
   uint32_t plo[kPreChunk];        // absolute first edge of each row segment
   uint32_t pseg[kPreChunk + 1];   // prefix of segment lengths
   uint32_t boff[kBlkChunk + 1];   // prefix of spike-list slot counts
@@ -402,10 +409,12 @@ __device__ __forceinline__ void clear_heads(ScatterSmem &S) {
   for (uint32_t r = 0; r < kBPT; ++r) S.head[threadIdx.x + r * kScatterThreads] = kEmpty;
 }
 
-__device__ __forceinline__ uint32_t bucket_of(uint32_t cell) { return (cell * 2654435761u) >> (32 - 13); }
-static_assert(kBuckets == 8192, "bucket_of assumes 2^13 buckets");
+// Knuth's multiplicative hash of the cell onto the buckets
+__device__ __forceinline__ uint32_t bucket_of(uint32_t cell) { return (cell * 2654435761u) >> (32 - kBucketBits); }
+constexpr uint32_t kNone16 = 0xFFFFu;
 
-// Prepend event k to the list of its bucket (arrival order).
+// Prepend event k to the list of its bucket (list order is arbitrary; the
+// walk below compares event indices).
 __device__ __forceinline__ void link_event(ScatterSmem &S, uint32_t k) {
   const uint32_t prev = atomicExch(&S.head[bucket_of(S.ecell[k])], k);
   S.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
@@ -413,12 +422,16 @@ __device__ __forceinline__ void link_event(ScatterSmem &S, uint32_t k) {
 
 // Apply the window's m linked events to the ring in reference order.  Each
 // event finds, in its bucket's list, its rank among the earlier events of
-// the same cell, its predecessor, and whether a later one exists.  Rank-0
-// events load the ring value (all loads in flight together); partial sums
-// then advance one rank per level in shared memory (ew[k] becomes the cell's
-// running value after event k); the last event of each cell stores it.
-// Called by all threads after the linking barrier; ends with a barrier.
-__device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t p0) {
+// the same cell, its predecessor, and whether a later one exists.  `pre`
+// holds the ring value of each of this thread's events (k = tid + r*threads),
+// loaded before linking so that the loads overlap the linking barrier and
+// the walk; rank-0 events add their weight to it, partial sums then advance
+// one rank per level in shared memory (ew[k] becomes the cell's running value
+// after event k; the values loaded for later ranks are not used), and the
+// last event of each cell stores it.  Called by all threads after the
+// linking barrier; ends with a barrier.
+__device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t p0,
+                                             const float (&pre)[kEPT]) {
   const unsigned long long pol = policy_evict_last();
   uint32_t rk[kEPT], pv[kEPT], lastm = 0, maxrank = 0;
   float w[kEPT];
@@ -431,7 +444,9 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     if (k < m) {
       const uint32_t c = S.ecell[k];
       bool last = true;
-      for (uint32_t j = S.head[bucket_of(c)]; j != kNone16; j = S.enext[j]) {
+      uint32_t j = S.head[bucket_of(c)];
+      if (j == kEmpty) j = kNone16;
+      for (; j != kNone16; j = S.enext[j]) {
         if (j == k || S.ecell[j] != c) continue;
         if (j < k) {
           ++rk[r];
@@ -445,14 +460,10 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
       w[r] = S.ew[k];
     }
   }
-  // level 0: one ring load per cell
+  // level 0: the first event of each cell adds to the loaded ring value
   float v[kEPT];
 #pragma unroll
-  for (uint32_t r = 0; r < kEPT; ++r) {
-    const uint32_t k = threadIdx.x + r * kScatterThreads;
-    v[r] = 0.0f;
-    if (k < m && rk[r] == 0) v[r] = ld_ring(cell_addr(a, S.ecell[k], p0), pol);
-  }
+  for (uint32_t r = 0; r < kEPT; ++r) v[r] = pre[r];
 #pragma unroll
   for (uint32_t r = 0; r < kEPT; ++r) {
     const uint32_t k = threadIdx.x + r * kScatterThreads;
@@ -482,16 +493,19 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
 }
 
 // One event into the window (or straight into the ring in atomic mode).
-__device__ __forceinline__ void put_event(const StepArgs &a, ScatterSmem &S, uint32_t k, uint32_t post,
-                                          float w, uint8_t code, unsigned long long step, uint32_t p0) {
-  const uint32_t slot = (uint32_t)((step + max(code_delay(code), 1u)) & 31ull);
-  const uint32_t cell = ((code_ring(code) * kSlots + slot) << a.pbits) | (post - p0);
+// `base` = step % nslots; the event lands in slot (step + max(delay, 1)) % nslots.
+__device__ __forceinline__ uint32_t put_event(const StepArgs &a, ScatterSmem &S, uint32_t k, uint32_t post,
+                                              float w, uint8_t code, uint32_t base, uint32_t p0) {
+  uint32_t slot = base + max(code_delay(code), 1u);
+  if (slot >= a.nslots) slot -= a.nslots;
+  const uint32_t cell = ((code_ring(code) * a.nslots + slot) << a.pbits) | (post - p0);
   if (a.deterministic) {
     S.ecell[k] = cell;
     S.ew[k] = w;
   } else {
     atomicAdd(cell_addr(a, cell, p0), w);
   }
+  return cell;
 }
 
 __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes) {
@@ -517,13 +531,14 @@ __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes
 }
 
 template <bool SEG32>
-__global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a) {
+__global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_kernel(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
   const uint32_t tid = threadIdx.x;
   const uint32_t j = blockIdx.x;
   const uint32_t p0 = j * a.P;
   const unsigned long long step = *a.step;
+  const uint32_t base = (uint32_t)(step % a.nslots);
   const uint32_t G1 = a.G + 1;
   if (tid == 0) {
     S.drift = 0.0;
@@ -613,11 +628,14 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
             ev_code[r] = a.code ? (uint8_t)ld_stream_u8(a.code + ev_e[r], spol) : (uint8_t)(rec.x >> 24);
           }
         }
+        float pre[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
+          pre[r] = 0.0f;
           if (k < m) {
-            put_event(a, S, k, ev_post[r], ev_w[r], ev_code[r], step, p0);
+            const uint32_t cell = put_event(a, S, k, ev_post[r], ev_w[r], ev_code[r], base, p0);
+            if (a.deterministic) pre[r] = ld_ring(cell_addr(a, cell, p0), policy_evict_last());
             if (a.stdp && code_stdp(ev_code[r])) {
               // depression at a pre spike; the pushed weight is the pre-update one
               const float w1 = fminf(fmaxf(ev_w[r] - a.a_minus * a.x_post[ev_post[r]], a.w_min), a.w_max);
@@ -628,7 +646,7 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
           }
         }
         __syncthreads();
-        if (a.deterministic) apply_window(a, S, m, p0);
+        if (a.deterministic) apply_window(a, S, m, p0, pre);
       }
     }
   }
@@ -681,17 +699,22 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
       uint32_t pos = block_excl_scan(__popc(fired), S.wsum, &m);  // all reads of the window are done
 #pragma unroll
       for (uint32_t r = 0; r < kEPT; ++r)
-        if (fired & (1u << r)) put_event(a, S, pos++, e_post[r], e_w[r], e_code[r], step, p0);
+        if (fired & (1u << r)) put_event(a, S, pos++, e_post[r], e_w[r], e_code[r], base, p0);
       if (tid == 0) S.events += m;
       __syncthreads();
       if (a.deterministic && m) {
+        float pre[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
-          if (k < m) link_event(S, k);
+          pre[r] = 0.0f;
+          if (k < m) {
+            pre[r] = ld_ring(cell_addr(a, S.ecell[k], p0), policy_evict_last());
+            link_event(S, k);
+          }
         }
         __syncthreads();
-        apply_window(a, S, m, p0);
+        apply_window(a, S, m, p0, pre);
       }
     }
     __syncthreads();
@@ -728,9 +751,9 @@ __global__ void __launch_bounds__(kScatterThreads, 1) scatter_kernel(StepArgs a)
 // inject_current (build.rs:243-275): values land in the slot the next step
 // reads.  `sequential` = the index list has repeats, apply in list order.
 // ---------------------------------------------------------------------------
-__global__ void inject_kernel(float *ring, uint32_t Nd, const unsigned long long *step, const uint32_t *idx,
-                              const float *vals, uint64_t n, uint32_t dev_off, int sequential) {
-  const uint32_t slot = (uint32_t)(*step & 31ull);
+__global__ void inject_kernel(float *ring, uint32_t Nd, uint32_t nslots, const unsigned long long *step,
+                              const uint32_t *idx, const float *vals, uint64_t n, uint32_t dev_off, int sequential) {
+  const uint32_t slot = (uint32_t)(*step % nslots);
   float *rs = ring + (size_t)slot * Nd + dev_off;
   if (sequential) {
     if (blockIdx.x == 0 && threadIdx.x == 0)
