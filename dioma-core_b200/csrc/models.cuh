@@ -295,4 +295,19 @@ __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
+// Counter-based uniform on [0, 1) with 53 random bits: two SplitMix64
+// rounds over (seed * golden ratio) ^ (stream << 40) ^ counter.
+__host__ __device__ __forceinline__ double hash_uniform01(uint64_t seed, uint32_t stream, uint64_t ctr) {
+  const uint64_t key = (seed * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)stream << 40) ^ ctr;
+  return (double)(splitmix64(splitmix64(key)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Standard normal by the Box-Muller transform in FP64 from the uniforms of
+// counters 2c and 2c + 1 (the first mapped to (0, 1]).
+__device__ __forceinline__ double hash_std_normal(uint64_t seed, uint32_t stream, uint64_t ctr) {
+  const double u1 = 1.0 - hash_uniform01(seed, stream, ctr * 2ull);
+  const double u2 = hash_uniform01(seed, stream, ctr * 2ull + 1ull);
+  return sqrt(-2.0 * log(u1)) * cos(2.0 * 3.141592653589793 * u2);
+}
+
 }  // namespace sg

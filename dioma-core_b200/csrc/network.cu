@@ -77,6 +77,11 @@ struct HostPop {
   uint32_t n, cap, dev_off, np, ns;
   uint32_t umask = 0;   // uniform parameter columns
   float uval[16] = {};
+  // Gaussian input noise (sg_pop_set_noise)
+  bool noise = false;
+  uint32_t noise_stream = 0, noise_split = 0;
+  uint64_t noise_seed = 0, noise_stride = 0, noise_step0 = 0;
+  double noise_sigma[2] = {0.0, 0.0};
   std::vector<float> params, state;  // before build
   DBuf<float> d_params, d_state;     // after build
 };
@@ -153,6 +158,14 @@ struct sg_net {
   uint64_t stat_read_step = 0;
   uint64_t host_step = 0;  // steps issued
   size_t scatter_smem = 0;
+  // neuron work table: per population its kernel arguments, per model the
+  // (population, block) pairs its launch covers
+  DBuf<PopArgs> d_pop_tab;
+  DBuf<uint2> d_blk_map;
+  std::vector<PopArgs> pop_tab;  // host copy
+  uint32_t model_blk_off[5] = {}, model_blk_cnt[5] = {};
+  int model_single[5] = {-1, -1, -1, -1, -1};  // the one population of a model, or -1
+  bool pop_tab_dirty = true;
   // CUDA graph of `graph_steps` steps
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_steps = 0;
@@ -380,6 +393,43 @@ __global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, u
     post[base + t] = to_off + j;
     w[base + t] = exc ? w_exc : w_inh;
     code[base + t] = edge_code((uint8_t)d, exc ? st_e : st_i, exc && (flags_e & SG_EDGE_STDP));
+  }
+}
+
+// Fixed out-degree with distinct targets (Floyd's sampling): source i draws
+// k distinct targets from the m = n_to (- 1 without self-loops) candidates;
+// draw q (j = m - k + q) takes t = floor(hi32(h) * (j + 1) / 2^32) in [0, j],
+// or j itself when t was already drawn, h = splitmix64(seed ^ ((i*k + q) *
+// 0x9E3779B97F4A7C15)); without self-loops t >= i maps to t + 1.  The weight
+// is w_exc (i < n_exc) or w_inh, times lo32(h) / 2^32 when random_w.  Edges
+// are written in (source, draw) order.
+constexpr uint32_t kMaxOutDegree = 1024;
+__global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, uint8_t *code, uint64_t base,
+                                       uint32_t n_from, uint32_t k, uint64_t seed, uint32_t from_off,
+                                       uint32_t to_off, uint32_t n_to, int no_self, uint32_t n_exc, float w_exc,
+                                       float w_inh, int random_w, uint8_t delay) {
+  const uint32_t m = n_to - (no_self ? 1u : 0u);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_from; i += gridDim.x * blockDim.x) {
+    uint32_t sel[kMaxOutDegree];
+    const bool exc = i < n_exc;
+    for (uint32_t q = 0; q < k; ++q) {
+      const uint32_t j = m - k + q;
+      const uint64_t h = splitmix64(seed ^ (((uint64_t)i * k + q) * 0x9E3779B97F4A7C15ull));
+      uint32_t t = (uint32_t)(((h >> 32) * (uint64_t)(j + 1)) >> 32);
+      for (uint32_t r = 0; r < q; ++r)
+        if (sel[r] == t) {
+          t = j;
+          break;
+        }
+      sel[q] = t;
+      const uint32_t tgt = (no_self && t >= i) ? t + 1 : t;
+      const float scale = exc ? w_exc : w_inh;
+      const uint64_t e = base + (uint64_t)i * k + q;
+      pre[e] = from_off + i;
+      post[e] = to_off + tgt;
+      w[e] = random_w ? scale * ((float)(uint32_t)(h & 0xffffffffull) * 2.3283064365386963e-10f) : scale;
+      code[e] = edge_code(delay, 0, false);
+    }
   }
 }
 
@@ -772,33 +822,78 @@ void finish_build(sg_net *net) {
   net->built = true;
 }
 
-template <int M> void launch_neuron(sg_net *net, const StepArgs &a, HostPop &p) {
-  PopArgs pa{};
-  pa.state = p.d_state.p;
-  pa.params = p.d_params.p;
-  pa.n = p.n;
-  pa.cap = p.cap;
-  pa.dev_off = p.dev_off;
-  pa.umask = p.umask;
-  for (int c = 0; c < 16; ++c) pa.uval[c] = p.uval[c];
-  pa.ln_na = net->ln_consts[0];
-  pa.ln_k = net->ln_consts[1];
-  neuron_kernel<M><<<p.cap / kNeuronBlock, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, pa);
+// Uploads the neuron work table (after build and after a parameter column
+// changed its uniform/non-uniform status), ordered on the network's stream.
+void upload_pop_table(sg_net *net) {
+  if (!net->pop_tab_dirty) return;
+  std::vector<PopArgs> tab(net->pops.size());
+  std::vector<uint2> map;
+  for (size_t i = 0; i < net->pops.size(); ++i) {
+    const HostPop &p = net->pops[i];
+    PopArgs &pa = tab[i];
+    pa.state = p.d_state.p;
+    pa.params = p.d_params.p;
+    pa.n = p.n;
+    pa.cap = p.cap;
+    pa.dev_off = p.dev_off;
+    pa.umask = p.umask;
+    for (int c = 0; c < 16; ++c) pa.uval[c] = p.uval[c];
+    pa.ln_na = net->ln_consts[0];
+    pa.ln_k = net->ln_consts[1];
+    pa.noise = p.noise ? 1 : 0;
+    pa.noise_stream = p.noise_stream;
+    pa.noise_split = p.noise_split;
+    pa.noise_seed = p.noise_seed;
+    pa.noise_stride = p.noise_stride;
+    pa.noise_step0 = p.noise_step0;
+    pa.noise_sigma[0] = p.noise_sigma[0];
+    pa.noise_sigma[1] = p.noise_sigma[1];
+  }
+  for (int m = 1; m <= 4; ++m) {
+    net->model_blk_off[m] = (uint32_t)map.size();
+    int n_pops = 0, last = -1;
+    for (size_t i = 0; i < net->pops.size(); ++i) {
+      const HostPop &p = net->pops[i];
+      if (p.model != m || p.n == 0) continue;
+      ++n_pops;
+      last = (int)i;
+      for (uint32_t b = 0; b < p.cap / kNeuronBlock; ++b) map.push_back(make_uint2((uint32_t)i, b));
+    }
+    net->model_blk_cnt[m] = (uint32_t)map.size() - net->model_blk_off[m];
+    net->model_single[m] = n_pops == 1 ? last : -1;
+  }
+  net->pop_tab = tab;
+  if (net->d_pop_tab.n < tab.size()) net->d_pop_tab.alloc(std::max<size_t>(tab.size(), 1));
+  if (net->d_blk_map.n < map.size()) net->d_blk_map.alloc(std::max<size_t>(map.size(), 1));
+  if (!tab.empty())
+    SG_CUDA(cudaMemcpyAsync(net->d_pop_tab.p, tab.data(), tab.size() * sizeof(PopArgs), cudaMemcpyHostToDevice,
+                            net->stream));
+  if (!map.empty())
+    SG_CUDA(cudaMemcpyAsync(net->d_blk_map.p, map.data(), map.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                            net->stream));
+  SG_CUDA(cudaStreamSynchronize(net->stream));
+  net->pop_tab_dirty = false;
+}
+
+template <int M> void launch_neuron(sg_net *net, const StepArgs &a) {
+  const uint32_t nb = net->model_blk_cnt[M];
+  if (nb == 0) return;
+  if (net->model_single[M] >= 0)
+    neuron_kernel<M><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, net->pop_tab[net->model_single[M]], nullptr,
+                                                                    nullptr);
+  else
+    neuron_kernel<M><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, PopArgs{}, net->d_pop_tab.p,
+                                                                    net->d_blk_map.p + net->model_blk_off[M]);
 }
 
 // Phases: 0 neuron update (all populations), 1 scatter.
 void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
   cudaStream_t s = net->stream;
   if (ev) SG_CUDA(cudaEventRecord(ev[0], s));
-  for (auto &p : net->pops) {
-    if (p.n == 0) continue;
-    switch (p.model) {
-      case kLIF: launch_neuron<kLIF>(net, a, p); break;
-      case kIZH: launch_neuron<kIZH>(net, a, p); break;
-      case kGPEA: launch_neuron<kGPEA>(net, a, p); break;
-      case kHH: launch_neuron<kHH>(net, a, p); break;
-    }
-  }
+  launch_neuron<kLIF>(net, a);
+  launch_neuron<kIZH>(net, a);
+  launch_neuron<kGPEA>(net, a);
+  launch_neuron<kHH>(net, a);
   if (ev) SG_CUDA(cudaEventRecord(ev[1], s));
   if (net->seg32) scatter_kernel<true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
   else scatter_kernel<false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
@@ -808,13 +903,14 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
 // Profiled steps: eager launches with CUDA events between the phases, read
 // back after every step (adds host synchronisation; for measurement only).
 void do_steps_profiled(sg_net *net, uint32_t n) {
+  upload_pop_table(net);
   const StepArgs a = make_args(net);
   if (net->prof_ev.empty()) {
     net->prof_ev.resize(3);
     for (auto &e : net->prof_ev) SG_CUDA(cudaEventCreate(&e));
   }
   size_t n_launch_pops = 0;
-  for (auto &p : net->pops) n_launch_pops += p.n ? 1 : 0;
+  for (int m = 1; m <= 4; ++m) n_launch_pops += net->model_blk_cnt[m] ? 1 : 0;
   for (uint32_t k = 0; k < n; ++k) {
     enqueue_step(net, a, net->prof_ev.data());
     SG_CUDA(cudaEventSynchronize(net->prof_ev[2]));
@@ -847,6 +943,7 @@ void do_steps(sg_net *net, uint32_t n) {
     net->host_step += n;
     return;
   }
+  upload_pop_table(net);
   const StepArgs a = make_args(net);
   const uint32_t G = 32;  // steps per graph launch
   uint32_t done = 0;
@@ -995,6 +1092,7 @@ static int pop_write(sg_net *net, uint32_t pop, uint32_t col, bool param, const 
       } else {
         p.umask &= ~(1u << col);
       }
+      net->pop_tab_dirty = true;
       drop_graph(net);
     }
   });
@@ -1107,6 +1205,39 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
                                                         pt.n, k_in, seed, pf.dev_off, pf.n, pt.dev_off, n_exc, w_exc,
                                                         w_inh, d_min, (uint32_t)(d_max - d_min + 1), st_e, st_i, flags_e);
     });
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
+  });
+}
+
+int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k, uint64_t seed, int no_self,
+                               uint32_t n_exc, float w_exc, float w_inh, int random_w, uint8_t delay) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+    require_pop(net, from);
+    require_pop(net, to);
+    SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
+    SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
+    SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
+    const auto &pf = net->pops[from];
+    const auto &pt = net->pops[to];
+    const uint32_t m = pt.n - (no_self && pt.n ? 1u : 0u);
+    SG_REQUIRE(k <= m && k <= kMaxOutDegree, SG_E_INVALID, "out-degree larger than the candidate targets or 1024");
+    const uint64_t n = (uint64_t)pf.n * k;
+    if (n == 0) return;
+    net->max_delay = std::max<uint32_t>(net->max_delay, delay);
+    DevGuard g(net->device);
+    const size_t n0 = net->e_pre.n;
+    net->e_pre.reserve(n0 + n, net->stream);
+    net->e_post.reserve(n0 + n, net->stream);
+    net->e_w.reserve(n0 + n, net->stream);
+    net->e_code.reserve(n0 + n, net->stream);
+    const unsigned blocks = (unsigned)std::min<uint64_t>((pf.n + 127) / 128, 148u * 16u);
+    synth_outdegree_kernel<<<blocks, 128, 0, net->stream>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p,
+                                                             n0, pf.n, k, seed, pf.dev_off, pt.dev_off, pt.n,
+                                                             no_self, n_exc, w_exc, w_inh, random_w, delay);
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaStreamSynchronize(net->stream));
     net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
@@ -1279,6 +1410,26 @@ int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col,
     if (E) upload_staged_edges(net, pre.data(), post.data(), w, code.data(), E);
   });
   return rc != SG_OK ? rc : sg_build(net);
+}
+
+int sg_pop_set_noise(sg_net *net, uint32_t pop, uint64_t seed, uint32_t stream, uint64_t stride, uint64_t step0,
+                     double sigma_lo, double sigma_hi, uint32_t split) {
+  NET_CHECK(net);
+  return run([&] {
+    require_pop(net, pop);
+    SG_REQUIRE(std::isfinite(sigma_lo) && std::isfinite(sigma_hi), SG_E_INVALID, "noise sigma must be finite");
+    HostPop &p = net->pops[pop];
+    p.noise = sigma_lo != 0.0 || sigma_hi != 0.0;
+    p.noise_seed = seed;
+    p.noise_stream = stream;
+    p.noise_stride = stride;
+    p.noise_step0 = step0;
+    p.noise_sigma[0] = sigma_lo;
+    p.noise_sigma[1] = sigma_hi;
+    p.noise_split = split;
+    net->pop_tab_dirty = true;
+    drop_graph(net);  // a captured step graph may hold the old arguments by value
+  });
 }
 
 int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals, uint64_t n) {

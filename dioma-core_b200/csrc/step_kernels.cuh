@@ -130,6 +130,14 @@ struct PopArgs {
   uint32_t umask;      // bit c: parameter column c is uniform
   float uval[16];      // its value
   float ln_na, ln_k;   // GPEA constants
+  // Gaussian input current added to every neuron's synaptic input each step
+  // (as an inject_current of that step would): sigma_i * N(0,1) from the
+  // counter i + (step - noise_step0) * noise_stride of the noise stream, with
+  // sigma_i = noise_sigma[0] for i < noise_split, noise_sigma[1] after
+  int noise;
+  uint32_t noise_stream, noise_split;
+  unsigned long long noise_seed, noise_stride, noise_step0;
+  double noise_sigma[2];
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -203,15 +211,16 @@ template <> struct VecF<4> {
   }
 };
 
+// The update of one 1024-neuron block `blk` of population p.
 template <int MODEL>
-__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS) neuron_kernel(StepArgs a, PopArgs p) {
+__device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p, uint32_t blk) {
   constexpr int NPT = NeuronCfg<MODEL>::NPT;
   constexpr int NS = n_state(MODEL), NP = n_params(MODEL);
   using V = VecF<NPT>;
   __shared__ uint32_t warp_cnt[32];
   __shared__ uint32_t warp_clamp[32];
   const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
-  const uint32_t i0 = blockIdx.x * kNeuronBlock + tid * NPT;  // population index of my first neuron
+  const uint32_t i0 = blk * kNeuronBlock + tid * NPT;  // population index of my first neuron
   const uint32_t gi0 = p.dev_off + i0;
   const unsigned long long step = *a.step;
   const uint32_t slot = (uint32_t)(step % a.nslots);
@@ -222,6 +231,16 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS) neuron_kernel(StepA
   float *rs = a.ring + (size_t)slot * a.Nd + gi0;
   V::load(rs, x);
   V::store(rs, zero);
+  if (p.noise) {
+    const unsigned long long t = step - p.noise_step0;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (i0 + q < p.n) {
+        const uint32_t i = i0 + q;
+        const double z = hash_std_normal(p.noise_seed, p.noise_stream, (unsigned long long)i + t * p.noise_stride);
+        x[q] = x[q] + (float)(p.noise_sigma[i < p.noise_split ? 0 : 1] * z);
+      }
+  }
   float sv[NS][NPT];
 #pragma unroll
   for (int c = 0; c < NS; ++c) V::load(p.state + (size_t)c * p.cap + i0, sv[c]);
@@ -339,6 +358,22 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS) neuron_kernel(StepA
         a.x_post[gi] = __fmaf_rn(a.x_post[gi], a.d_post, add);
       }
   }
+}
+
+// One launch per neuron model updates every population of that model: block
+// b takes entry map[b] = (population, block within it) of the work table, so
+// many small populations (a batch of networks) step in one launch.  A model
+// with a single population passes its arguments by value (map == null) and
+// block b is its block b.
+template <int MODEL>
+__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS)
+    neuron_kernel(StepArgs a, PopArgs p0, const PopArgs *__restrict__ pops, const uint2 *__restrict__ map) {
+  if (map == nullptr) {
+    neuron_block<MODEL>(a, p0, blockIdx.x);
+    return;
+  }
+  const uint2 bm = map[blockIdx.x];
+  neuron_block<MODEL>(a, pops[bm.x], bm.y);
 }
 
 // ---------------------------------------------------------------------------

@@ -42,6 +42,7 @@ SIGNATURES = {
     "sg_connect": [vp, u32, vp, u32, vp, vp, vp, u64],
     "sg_connect_ex": [vp, u32, vp, u32, vp, vp, vp, vp, u64, u32],
     "sg_connect_fixed_indegree": [vp, u32, u32, u32, u64, u32, f32, f32, u8, u8, u8, u8, u32],
+    "sg_connect_fixed_outdegree": [vp, u32, u32, u32, u64, i32, u32, f32, f32, i32, u8],
     "sg_register_expone": [vp, f32, f32, f32, vp],
     "sg_poisson_add": [vp, f32, f32, u32, vp],
     "sg_poisson_add_many": [vp, u32, f32, f32, vp, u32, vp],
@@ -52,6 +53,7 @@ SIGNATURES = {
     "sg_set_deterministic": [vp, i32],
     "sg_build": [vp],
     "sg_build_from_csr": [vp, vp, vp, vp, vp],
+    "sg_pop_set_noise": [vp, u32, u64, u32, u64, u64, f64, f64, u32],
     "sg_inject": [vp, u32, vp, vp, u64],
     "sg_step": [vp, u32],
     "sg_raster_enable": [vp, u32],

@@ -105,6 +105,12 @@ class Network:
                                               d_min, d_max, syn_type_exc, syn_type_inh,
                                               EDGE_STDP if stdp_exc else 0))
 
+    def connect_fixed_outdegree(self, frm, to, k, seed, no_self, n_exc, w_exc, w_inh, random_w=True, delay=1):
+        """k distinct targets per source, generated on the device
+        (sg_connect_fixed_outdegree); weights w_exc/w_inh times U(0,1)."""
+        check(lib().sg_connect_fixed_outdegree(self._h, frm, to, k, seed, 1 if no_self else 0, n_exc,
+                                               float(w_exc), float(w_inh), 1 if random_w else 0, delay))
+
     def register_expone(self, tau_decay: float, erev: float, dt: float) -> int:
         out = C.c_uint32()
         check(lib().sg_register_expone(self._h, tau_decay, erev, dt, C.byref(out)))
@@ -152,6 +158,16 @@ class Network:
         check(lib().sg_build_from_csr(self._h, _p(rp), _p(c), _p(w), _p(d)))
 
     # -- run (build.rs / step.rs) -----------------------------------------------
+    def set_noise(self, pop: int, seed: int, sigma_lo: float, sigma_hi: float | None = None,
+                  split: int | None = None, stream: int = 4, stride: int | None = None, step0: int = 0):
+        """Device Gaussian input: neuron i gets sigma_i * N(0,1) each step from
+        counter i + (step - step0) * stride (stride defaults to the population
+        size); sigma_i = sigma_lo below `split`, sigma_hi from there on."""
+        n = self._sizes[pop]
+        check(lib().sg_pop_set_noise(self._h, pop, int(seed), int(stream), int(n if stride is None else stride),
+                                     int(step0), float(sigma_lo), float(sigma_lo if sigma_hi is None else sigma_hi),
+                                     int(n if split is None else split)))
+
     def inject_current(self, pop, indices, values):
         i = np.ascontiguousarray(indices, np.uint32)
         v = np.ascontiguousarray(values, np.float32)

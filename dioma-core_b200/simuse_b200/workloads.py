@@ -106,6 +106,82 @@ def izhikevich_input(spec: dict, step: int) -> np.ndarray:
     return (scale * z).astype(np.float32)
 
 
+def fixed_outdegree_edges(n: int, k: int, seed: int, n_exc: int, w_exc: float, w_inh: float,
+                          no_self: bool = True, random_w: bool = True):
+    """NumPy twin of the device generator sg_connect_fixed_outdegree (same
+    hash, same Floyd draws, same (source, draw) edge order)."""
+    m = n - (1 if no_self else 0)
+    i = np.arange(n, dtype=np.uint64)
+    sel = np.empty((n, k), np.uint64)
+    w = np.empty((n, k), np.float32)
+    scale = np.where(np.arange(n) < n_exc, np.float32(w_exc), np.float32(w_inh)).astype(np.float32)
+    with np.errstate(over="ignore"):
+        for q in range(k):
+            j = np.uint64(m - k + q)
+            h = splitmix64(np.uint64(seed) ^ ((i * np.uint64(k) + np.uint64(q)) * PHI))
+            t = ((h >> np.uint64(32)) * (j + np.uint64(1))) >> np.uint64(32)
+            if q:
+                dup = (sel[:, :q] == t[:, None]).any(axis=1)
+                t = np.where(dup, j, t)
+            sel[:, q] = t
+            u = (h & np.uint64(0xFFFFFFFF)).astype(np.float32) * np.float32(2.3283064365386963e-10)
+            w[:, q] = scale * u if random_w else scale
+    tgt = sel.copy()
+    if no_self:
+        tgt = np.where(tgt >= i[:, None], tgt + np.uint64(1), tgt)
+    pre = np.repeat(np.arange(n, dtype=np.uint32), k)
+    return pre, tgt.astype(np.uint32).ravel(), w.ravel()
+
+
+def izhikevich_params(n: int, n_exc: int, seed: int):
+    """Per-neuron a, b, c, d of the pulse-network recipe (r ~ U(0,1) per neuron)."""
+    r = uniform01(seed, IZH_STREAM_R, np.arange(n, dtype=np.uint64))
+    exc = np.arange(n) < n_exc
+    a = np.where(exc, 0.02, 0.02 + 0.08 * r).astype(np.float32)
+    b = np.where(exc, 0.2, 0.25 - 0.05 * r).astype(np.float32)
+    c = np.where(exc, -65.0 + 15.0 * r * r, -65.0).astype(np.float32)
+    d = np.where(exc, 8.0 - 6.0 * r * r, 2.0).astype(np.float32)
+    return a, b, c, d
+
+
+def add_izhikevich_instance(net, n: int, seed: int, k_out: int = 100, device_edges: bool = True,
+                            device_noise: bool = True, model_izh: int = 2) -> int:
+    """One pulse-coupled Izhikevich network (the recipe of izhikevich_pulse,
+    with the fixed-out-degree generator for its 100 distinct targets) added
+    to `net` as its own population; several calls build a batch that steps
+    as one network.  Device noise draws the thalamic input of
+    izhikevich_input on the GPU (same hash, counter i + step * n)."""
+    n_exc = n * 4 // 5
+    a, b, c, d = izhikevich_params(n, n_exc, seed)
+    pop = net.add_population(model_izh, n)
+    net.fill_param(pop, 0, 1.0)
+    net.set_param(pop, 1, a)
+    net.set_param(pop, 2, b)
+    net.set_param(pop, 3, c)
+    net.set_param(pop, 4, d)
+    net.fill_param(pop, 5, 0.0)
+    net.fill_param(pop, 6, 30.0)
+    net.fill_state(pop, 0, -65.0)
+    net.set_state(pop, 1, (b * np.float32(-65.0)).astype(np.float32))
+    k = min(k_out, n - 1)
+    if device_edges:
+        net.connect_fixed_outdegree(pop, pop, k, seed, True, n_exc, 0.5, -1.0, True, 1)
+    else:
+        pre, post, w = fixed_outdegree_edges(n, k, seed, n_exc, 0.5, -1.0)
+        net.connect(pop, pre, pop, post, w, np.ones(pre.size, np.uint8))
+    if device_noise:
+        net.set_noise(pop, seed, 5.0, 2.0, split=n_exc, stream=IZH_STREAM_NOISE, stride=n)
+    return pop
+
+
+def thalamic_input(n: int, seed: int, step: int) -> np.ndarray:
+    """Host form of the device noise of add_izhikevich_instance (f32)."""
+    n_exc = n * 4 // 5
+    ctr = np.arange(n, dtype=np.uint64) + np.uint64(step) * np.uint64(n)
+    z = std_normal(seed, IZH_STREAM_NOISE, ctr)
+    return (np.where(np.arange(n) < n_exc, 5.0, 2.0) * z).astype(np.float32)
+
+
 def build_izhikevich(net, spec: dict, model_izh: int = 2) -> int:
     """Apply the spec through the reference builder API; returns the population."""
     n = spec["n"]

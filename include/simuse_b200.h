@@ -103,6 +103,19 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
                               uint8_t d_min, uint8_t d_max, uint8_t syn_type_exc,
                               uint8_t syn_type_inh, uint32_t flags_exc);
 
+/* Seeded synthetic projection generated on the device: every neuron i of
+   `from` gets exactly k distinct targets in `to` (no self-loop when no_self,
+   which needs from == to), drawn by Floyd's sampling: with m candidates,
+   draw q (j = m - k + q) takes t = hi32(h) * (j + 1) >> 32, or j when t was
+   drawn before, h = splitmix64(seed ^ (i*k + q)*0x9E3779B97F4A7C15); without
+   self-loops t >= i maps to t + 1.  Weight w_exc for i < n_exc else w_inh,
+   times lo32(h) / 2^32 when random_w; fixed delay.  Edges are appended in
+   (source, draw) order.  This is the generator of the Izhikevich pulse
+   network recipe (100 distinct targets, weights 0.5 U / -U, delay 1). */
+int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k, uint64_t seed,
+                               int no_self, uint32_t n_exc, float w_exc, float w_inh, int random_w,
+                               uint8_t delay);
+
 /* Network::register_kinetics(SynapseKinetics::ExpOne{tau_decay, erev}, dt)
    -> profile id (1-based), core.rs:564-584; step.rs:248-345 */
 int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id);
@@ -137,6 +150,20 @@ int sg_build(sg_net *net);
 /* SparseGraph::from_csr + build (graph.rs:217-275): all-static, not plastic */
 int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col,
                       const float *weights, const uint8_t *delays);
+
+/* Device-generated Gaussian input current, the device form of feeding a
+   population's noise through inject_current every step (how the reference's
+   Izhikevich examples drive the thalamic input, build.rs:243-275).  At device
+   step t, neuron i of the population receives sigma_i * z, z the FP64
+   Box-Muller normal of the SplitMix64 counters 2c and 2c+1 with
+   c = i + (t - step0) * stride (uniform = (splitmix64(splitmix64((seed *
+   0x9E3779B97F4A7C15) ^ (stream << 40) ^ counter)) >> 11) * 2^-53),
+   sigma_i = sigma_lo for i < split and sigma_hi after, rounded to f32 and
+   added to the slot value before kinetic currents and the clamp, i.e. after
+   any host injection of the same step.  sigma_lo = sigma_hi = 0 turns it
+   off.  Allowed before and after build. */
+int sg_pop_set_noise(sg_net *net, uint32_t pop, uint64_t seed, uint32_t stream, uint64_t stride,
+                     uint64_t step0, double sigma_lo, double sigma_hi, uint32_t split);
 
 /* ---- run -------------------------------------------------------------- */
 /* Network::inject_current(pop, idx, vals), build.rs:243-275: same-step slot */
