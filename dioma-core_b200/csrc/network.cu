@@ -403,33 +403,55 @@ __global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, u
 // 0x9E3779B97F4A7C15)); without self-loops t >= i maps to t + 1.  The weight
 // is w_exc (i < n_exc) or w_inh, times lo32(h) / 2^32 when random_w.  Edges
 // are written in (source, draw) order.
-constexpr uint32_t kMaxOutDegree = 1024;
+// With per-source degrees (deg != null) source i draws deg[i] targets into
+// the edges from base + off[i]; the hash counter is then off[i] + q.
+constexpr uint32_t kMaxOutDegree = 4096;
 __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, uint8_t *code, uint64_t base,
-                                       uint32_t n_from, uint32_t k, uint64_t seed, uint32_t from_off,
+                                       uint32_t n_from, uint32_t k_fixed, const uint32_t *deg,
+                                       const unsigned long long *off, uint64_t seed, uint32_t from_off,
                                        uint32_t to_off, uint32_t n_to, int no_self, uint32_t n_exc, float w_exc,
                                        float w_inh, int random_w, uint8_t delay) {
   const uint32_t m = n_to - (no_self ? 1u : 0u);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_from; i += gridDim.x * blockDim.x) {
-    uint32_t sel[kMaxOutDegree];
     const bool exc = i < n_exc;
+    const uint32_t k = deg ? deg[i] : k_fixed;
+    const uint64_t first = deg ? (uint64_t)off[i] : (uint64_t)i * k_fixed;
+    uint32_t *row = post + base + first;  // this source's targets so far (to_off + mapped draw)
     for (uint32_t q = 0; q < k; ++q) {
       const uint32_t j = m - k + q;
-      const uint64_t h = splitmix64(seed ^ (((uint64_t)i * k + q) * 0x9E3779B97F4A7C15ull));
+      const uint64_t h = splitmix64(seed ^ ((first + q) * 0x9E3779B97F4A7C15ull));
       uint32_t t = (uint32_t)(((h >> 32) * (uint64_t)(j + 1)) >> 32);
-      for (uint32_t r = 0; r < q; ++r)
-        if (sel[r] == t) {
+      for (uint32_t r = 0; r < q; ++r) {
+        uint32_t d = row[r] - to_off;  // undo the self-loop mapping: draws are compared raw
+        if (no_self && d > i) --d;
+        if (d == t) {
           t = j;
           break;
         }
-      sel[q] = t;
+      }
       const uint32_t tgt = (no_self && t >= i) ? t + 1 : t;
       const float scale = exc ? w_exc : w_inh;
-      const uint64_t e = base + (uint64_t)i * k + q;
+      const uint64_t e = base + first + q;
       pre[e] = from_off + i;
-      post[e] = to_off + tgt;
+      row[q] = to_off + tgt;
       w[e] = random_w ? scale * ((float)(uint32_t)(h & 0xffffffffull) * 2.3283064365386963e-10f) : scale;
       code[e] = edge_code(delay, 0, false);
     }
+  }
+}
+
+__global__ void widen_kernel(const uint32_t *in, unsigned long long *out, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
+    out[i] = i < n ? in[i] : 0ull;
+}
+
+// Lognormal out-degrees: deg[i] = round(exp(mu + sigma * z_i)) clipped to
+// [1, kmax], z_i the FP64 Box-Muller normal of counter i (stream 7).
+__global__ void lognormal_degree_kernel(uint32_t *deg, uint32_t n, uint64_t seed, double mu, double sigma,
+                                        uint32_t kmax) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double k = rint(exp(mu + sigma * hash_std_normal(seed, 7, i)));
+    deg[i] = (uint32_t)fmin(fmax(k, 1.0), (double)kmax);
   }
 }
 
@@ -1236,11 +1258,70 @@ int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t
     net->e_code.reserve(n0 + n, net->stream);
     const unsigned blocks = (unsigned)std::min<uint64_t>((pf.n + 127) / 128, 148u * 16u);
     synth_outdegree_kernel<<<blocks, 128, 0, net->stream>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p,
-                                                             n0, pf.n, k, seed, pf.dev_off, pt.dev_off, pt.n,
-                                                             no_self, n_exc, w_exc, w_inh, random_w, delay);
+                                                             n0, pf.n, k, nullptr, nullptr, seed, pf.dev_off,
+                                                             pt.dev_off, pt.n, no_self, n_exc, w_exc, w_inh,
+                                                             random_w, delay);
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaStreamSynchronize(net->stream));
     net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
+  });
+}
+
+int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, double mean, double sd,
+                                   uint64_t seed, int no_self, uint32_t n_exc, float w_exc, float w_inh,
+                                   int random_w, uint8_t delay) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+    require_pop(net, from);
+    require_pop(net, to);
+    SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
+    SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
+    SG_REQUIRE(std::isfinite(mean) && mean > 0 && std::isfinite(sd) && sd >= 0, SG_E_INVALID,
+               "lognormal degree needs mean > 0 and sd >= 0");
+    SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
+    const auto &pf = net->pops[from];
+    const auto &pt = net->pops[to];
+    const uint32_t m = pt.n - (no_self && pt.n ? 1u : 0u);
+    if (pf.n == 0) return;
+    SG_REQUIRE(m >= 1, SG_E_INVALID, "no candidate targets");
+    const double s2 = std::log(1.0 + (sd * sd) / (mean * mean));
+    const double mu = std::log(mean) - 0.5 * s2, sigma = std::sqrt(s2);
+    const uint32_t kmax = std::min<uint32_t>(m, kMaxOutDegree);
+    DevGuard g(net->device);
+    cudaStream_t s = net->stream;
+    DBuf<uint32_t> deg;
+    deg.alloc(pf.n);
+    DBuf<unsigned long long> off, deg64;
+    off.alloc((size_t)pf.n + 1);
+    deg64.alloc((size_t)pf.n + 1);
+    const unsigned blocks = (unsigned)std::min<uint64_t>((pf.n + 255) / 256, 148u * 16u);
+    lognormal_degree_kernel<<<blocks, 256, 0, s>>>(deg.p, pf.n, seed, mu, sigma, kmax);
+    SG_CUDA(cudaGetLastError());
+    widen_kernel<<<blocks, 256, 0, s>>>(deg.p, deg64.p, pf.n);
+    SG_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg64.p, off.p, (int64_t)pf.n + 1, s));
+    DBuf<uint8_t> temp;
+    temp.alloc(std::max<size_t>(tb, 1));
+    SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, deg64.p, off.p, (int64_t)pf.n + 1, s));
+    unsigned long long total = 0;
+    SG_CUDA(cudaMemcpyAsync(&total, off.p + pf.n, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    if (total == 0) return;
+    net->max_delay = std::max<uint32_t>(net->max_delay, delay);
+    const size_t n0 = net->e_pre.n;
+    net->e_pre.reserve(n0 + total, s);
+    net->e_post.reserve(n0 + total, s);
+    net->e_w.reserve(n0 + total, s);
+    net->e_code.reserve(n0 + total, s);
+    const unsigned b2 = (unsigned)std::min<uint64_t>((pf.n + 127) / 128, 148u * 16u);
+    synth_outdegree_kernel<<<b2, 128, 0, s>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p, n0, pf.n, 0,
+                                              deg.p, off.p, seed, pf.dev_off, pt.dev_off, pt.n, no_self, n_exc,
+                                              w_exc, w_inh, random_w, delay);
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaStreamSynchronize(s));
+    net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + total;
   });
 }
 

@@ -111,6 +111,14 @@ class Network:
         check(lib().sg_connect_fixed_outdegree(self._h, frm, to, k, seed, 1 if no_self else 0, n_exc,
                                                float(w_exc), float(w_inh), 1 if random_w else 0, delay))
 
+    def connect_lognormal_outdegree(self, frm, to, mean, sd, seed, no_self, n_exc, w_exc, w_inh,
+                                    random_w=True, delay=1):
+        """Lognormal out-degree per source, distinct targets, generated on the
+        device (sg_connect_lognormal_outdegree)."""
+        check(lib().sg_connect_lognormal_outdegree(self._h, frm, to, float(mean), float(sd), seed,
+                                                   1 if no_self else 0, n_exc, float(w_exc), float(w_inh),
+                                                   1 if random_w else 0, delay))
+
     def register_expone(self, tau_decay: float, erev: float, dt: float) -> int:
         out = C.c_uint32()
         check(lib().sg_register_expone(self._h, tau_decay, erev, dt, C.byref(out)))
@@ -201,10 +209,15 @@ class Network:
         n = C.c_uint64()
         if capacity is None:
             k = self.step_counter - getattr(self, "_raster_mark", 0)
-            capacity = max(1, k * self.total_neurons)
+            capacity = max(1, min(k * self.total_neurons, 1 << 20))
         st = np.empty(capacity, np.uint32)
         ix = np.empty(capacity, np.uint32)
-        check(lib().sg_raster_read_events(self._h, _p(st), _p(ix), capacity, C.byref(n)))
+        rc = lib().sg_raster_read_events(self._h, _p(st), _p(ix), capacity, C.byref(n))
+        if rc < 0 and n.value > capacity:  # too small: nothing was consumed, read again at the exact size
+            st = np.empty(n.value, np.uint32)
+            ix = np.empty(n.value, np.uint32)
+            rc = lib().sg_raster_read_events(self._h, _p(st), _p(ix), n.value, C.byref(n))
+        check(rc)
         self._raster_mark = self.step_counter
         return st[: n.value], ix[: n.value]
 

@@ -1,0 +1,295 @@
+"""A served stream of simulation requests on one GPU.
+
+Each request names a seeded network (LIF or Izhikevich, N neurons, lognormal
+out-degree) and a number of simulation steps, and gets back its spike events
+and per-neuron firing rates.  The server keeps every admitted network's state,
+synapses and delay rings resident in HBM until it finishes, and batches
+continuously: a request that arrives while others are running is admitted
+as soon as a resident slot and enough of the memory budget are free, and its
+steps then run beside theirs, each network on its own CUDA stream, so their
+kernels overlap on the device.  Admission is by resident footprint against
+the budget (an estimate at admission, replaced by the measured footprint of
+the built network).  Latency is measured per request from submission to
+completion.
+
+Networks do not interact, and each one's random streams (Poisson drive,
+input noise) are keyed by its own seed and its own step counter, so a
+request's result does not depend on what else is resident: the same bits
+alone and in any mix.
+
+The reference has no serving layer; this is the north-star request loop,
+written over the same builder/step API the reference's callers use
+(crates/SiMuse/crates/pillars/src/api/net/network/).
+"""
+from __future__ import annotations
+
+import dataclasses
+import queue
+import threading
+import time
+
+import numpy as np
+
+from . import workloads as W
+from .network import IZH, LIF, Network
+
+
+@dataclasses.dataclass
+class Request:
+    kind: str                 # "lif" or "izh"
+    n: int                    # neurons
+    seed: int
+    steps: int                # simulation steps to run
+    mean_degree: float = 100.0
+    sd_degree: float = 60.0
+    # filled by the server
+    id: int = -1
+    t_submit: float = 0.0
+    t_admit: float = 0.0
+    t_done: float = 0.0
+    footprint: int = 0
+    spike_steps: np.ndarray | None = None
+    spike_index: np.ndarray | None = None
+    rates_hz: np.ndarray | None = None
+    error: str | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+    @property
+    def dt_ms(self) -> float:
+        return 0.1 if self.kind == "lif" else 1.0
+
+
+def estimate_footprint(req: Request) -> int:
+    """Device bytes a request holds while it is built and resident: synapse
+    records, the per-row segment table, rings, state, spike lists and the
+    build-time sort buffers (the peak), rounded up generously."""
+    n = req.n
+    nd = -(-n // 1024) * 1024
+    e = int(n * req.mean_degree * 1.05)
+    per_neuron = 32 * 4 + 16 * 4 + 8 + 148 * 2 + 64   # rings (<= 32 slots), state+params, spike list, segments
+    build_peak = e * 45                                # staged edges + radix-sort double buffers + records
+    return int(nd * per_neuron + build_peak + (64 << 20))
+
+
+def build_request(req: Request, device: int = 0) -> Network:
+    """The request's network through the builder API (not yet built)."""
+    net = Network(device)
+    n, n_exc = req.n, req.n * 4 // 5
+    if req.kind == "lif":
+        pop = net.add_population(LIF, n)
+        for col, v in enumerate(W.LIF_PARAMS):
+            net.fill_param(pop, col, v)
+        u = W.uniform01(req.seed, W.LIF_STREAM_V0, np.arange(n, dtype=np.uint64))
+        net.set_state(pop, 0, (10.0 + 10.0 * u).astype(np.float32))
+        # ring weights J*tau/dt for J = 0.1 mV (g = 5), delay 2 steps
+        net.connect_lognormal_outdegree(pop, pop, req.mean_degree, req.sd_degree, req.seed, True, n_exc,
+                                        20.0, -100.0, random_w=False, delay=2)
+        first = net.add_poisson_sources(n, 4000.0, 0.1, seed0=req.seed * 7919)
+        net.connect_poisson_one_to_one(first, n, pop, 100.0, 1)
+    elif req.kind == "izh":
+        pop = net.add_population(IZH, n)
+        a, b, c, d = W.izhikevich_params(n, n_exc, req.seed)
+        net.fill_param(pop, 0, 1.0)
+        for col, v in ((1, a), (2, b), (3, c), (4, d)):
+            net.set_param(pop, col, v)
+        net.fill_param(pop, 5, 0.0)
+        net.fill_param(pop, 6, 30.0)
+        net.fill_state(pop, 0, -65.0)
+        net.set_state(pop, 1, (b * np.float32(-65.0)).astype(np.float32))
+        net.connect_lognormal_outdegree(pop, pop, req.mean_degree, req.sd_degree, req.seed, True, n_exc,
+                                        0.5, -1.0, random_w=True, delay=1)
+        net.set_noise(pop, req.seed, 5.0, 2.0, split=n_exc, stream=W.IZH_STREAM_NOISE, stride=n)
+    else:
+        raise ValueError(f"unknown request kind {req.kind!r}")
+    return net
+
+
+def run_alone(req: Request, device: int = 0, chunk: int = 256) -> Request:
+    """The plain path: build, run and read back one request by itself."""
+    req.t_submit = req.t_admit = time.perf_counter()
+    net = build_request(req, device)
+    net.build()
+    _run_to_end(net, req, chunk)
+    net.close()
+    req.t_done = time.perf_counter()
+    return req
+
+
+def _run_to_end(net: Network, req: Request, chunk: int):
+    net.enable_raster(chunk)
+    st, ix = [], []
+    done = 0
+    while done < req.steps:
+        k = min(chunk, req.steps - done)
+        net.step(k)
+        s, i = net.read_spike_events()
+        st.append(s)
+        ix.append(i)
+        done += k
+    _finish(req, st, ix)
+
+
+def _finish(req: Request, st, ix):
+    req.spike_steps = np.concatenate(st) if st else np.empty(0, np.uint32)
+    req.spike_index = np.concatenate(ix) if ix else np.empty(0, np.uint32)
+    counts = np.bincount(req.spike_index.astype(np.int64), minlength=req.n)
+    req.rates_hz = counts / (req.steps * req.dt_ms * 1e-3)
+
+
+class _Resident:
+    def __init__(self, req: Request, net: Network, chunk: int):
+        self.req, self.net, self.chunk = req, net, chunk
+        self.done = 0
+        self.k = 0
+        self.st: list[np.ndarray] = []
+        self.ix: list[np.ndarray] = []
+        net.enable_raster(chunk)
+
+
+class Server:
+    """Continuous-batching request loop on one GPU (see the module text).
+
+    budget_bytes: device memory the resident networks may hold together.
+    max_resident: resident networks at most (streams in flight).
+    chunk: steps a resident network advances per scheduling round.
+    """
+
+    def __init__(self, device: int = 0, budget_bytes: int = 160 * 10**9, max_resident: int = 32,
+                 chunk: int = 256):
+        self.device, self.budget, self.max_resident, self.chunk = device, int(budget_bytes), max_resident, chunk
+        self._pending: queue.Queue[Request] = queue.Queue()
+        self._built: queue.Queue[tuple[Request, Network | None]] = queue.Queue()
+        self._to_build: queue.Queue[Request | None] = queue.Queue()
+        self._lock = threading.Lock()
+        self._reserved = 0            # budget bytes held by building and resident networks
+        self._next_id = 0
+        self.completed: list[Request] = []
+        self._stop = threading.Event()
+        self._idle = threading.Event()
+        self._n_open = 0
+        self._builder = threading.Thread(target=self._build_loop, daemon=True)
+        self._stepper = threading.Thread(target=self._step_loop, daemon=True)
+        self._builder.start()
+        self._stepper.start()
+
+    # -- client side ----------------------------------------------------------
+    def submit(self, req: Request) -> Request:
+        req.t_submit = time.perf_counter()
+        with self._lock:
+            req.id = self._next_id
+            self._next_id += 1
+            self._n_open += 1
+            self._idle.clear()
+        if estimate_footprint(req) > self.budget:
+            req.error = "request larger than the device budget"
+            self._complete(req)
+            return req
+        self._pending.put(req)
+        return req
+
+    def wait_idle(self, timeout: float | None = None) -> bool:
+        return self._idle.wait(timeout)
+
+    def close(self):
+        self._stop.set()
+        self._to_build.put(None)
+        self._stepper.join()
+        self._builder.join()
+
+    def latency_percentiles(self) -> dict:
+        lat = np.array([r.latency for r in self.completed if r.error is None])
+        if lat.size == 0:
+            return {"p50_s": None, "p99_s": None, "n": 0}
+        return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)), "n": int(lat.size)}
+
+    # -- server side ------------------------------------------------------------
+    def _complete(self, req: Request):
+        req.t_done = time.perf_counter()
+        with self._lock:
+            self.completed.append(req)
+            self._n_open -= 1
+            if self._n_open == 0:
+                self._idle.set()
+
+    def _build_loop(self):
+        while True:
+            req = self._to_build.get()
+            if req is None:
+                return
+            try:
+                net = build_request(req, self.device)
+                net.build()
+                net.synchronize()
+                self._built.put((req, net))
+            except Exception as e:  # a failed build releases its reservation
+                req.error = str(e)
+                self._built.put((req, None))
+
+    def _step_loop(self):
+        resident: list[_Resident] = []
+        building = 0
+        waiting: list[Request] = []
+        while not self._stop.is_set() or resident or building:
+            # arrivals
+            while True:
+                try:
+                    waiting.append(self._pending.get_nowait())
+                except queue.Empty:
+                    break
+            # admission in arrival order, by footprint and slot
+            while waiting and len(resident) + building < self.max_resident:
+                req = waiting[0]
+                est = estimate_footprint(req)
+                with self._lock:
+                    if self._reserved + est > self.budget:
+                        break
+                    self._reserved += est
+                req.footprint = est
+                req.t_admit = time.perf_counter()
+                waiting.pop(0)
+                building += 1
+                self._to_build.put(req)
+            # networks that finished building join the running set
+            while True:
+                try:
+                    req, net = self._built.get_nowait()
+                except queue.Empty:
+                    break
+                building -= 1
+                if net is None:
+                    with self._lock:
+                        self._reserved -= req.footprint
+                    self._complete(req)
+                    continue
+                true_fp = net.footprint
+                with self._lock:                  # the measured footprint replaces the estimate
+                    self._reserved += true_fp - req.footprint
+                req.footprint = true_fp
+                resident.append(_Resident(req, net, self.chunk))
+            if not resident:
+                time.sleep(0.0005)
+                continue
+            # one round: every resident network advances one chunk on its own
+            # stream (launches are asynchronous, so the chunks overlap), then
+            # each chunk's spikes are read back
+            for r in resident:
+                r.k = min(r.chunk, r.req.steps - r.done)
+                r.net.step(r.k)
+            finished = []
+            for r in resident:
+                s, i = r.net.read_spike_events()
+                r.st.append(s)
+                r.ix.append(i)
+                r.done += r.k
+                if r.done >= r.req.steps:
+                    finished.append(r)
+            for r in finished:
+                resident.remove(r)
+                _finish(r.req, r.st, r.ix)
+                r.net.close()
+                with self._lock:
+                    self._reserved -= r.req.footprint
+                self._complete(r.req)

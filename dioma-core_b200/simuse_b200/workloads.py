@@ -133,6 +133,45 @@ def fixed_outdegree_edges(n: int, k: int, seed: int, n_exc: int, w_exc: float, w
     return pre, tgt.astype(np.uint32).ravel(), w.ravel()
 
 
+def lognormal_degrees(n: int, mean: float, sd: float, seed: int, kmax: int) -> np.ndarray:
+    """Per-source degrees of sg_connect_lognormal_outdegree (stream 7)."""
+    s2 = np.log(1.0 + (sd * sd) / (mean * mean))
+    mu, sigma = np.log(mean) - 0.5 * s2, np.sqrt(s2)
+    z = std_normal(seed, 7, np.arange(n, dtype=np.uint64))
+    return np.clip(np.rint(np.exp(mu + sigma * z)), 1, kmax).astype(np.int64)
+
+
+def lognormal_outdegree_edges(n: int, mean: float, sd: float, seed: int, n_exc: int, w_exc: float,
+                              w_inh: float, no_self: bool = True, random_w: bool = True):
+    """NumPy twin of sg_connect_lognormal_outdegree (small n: loops per source)."""
+    m = n - (1 if no_self else 0)
+    deg = lognormal_degrees(n, mean, sd, seed, min(m, 4096))
+    off = np.concatenate([[0], np.cumsum(deg)])
+    pre = np.repeat(np.arange(n, dtype=np.uint32), deg)
+    post = np.empty(off[-1], np.uint32)
+    w = np.empty(off[-1], np.float32)
+    with np.errstate(over="ignore"):
+        for i in range(n):
+            k = int(deg[i])
+            ctr = np.arange(off[i], off[i] + k, dtype=np.uint64)
+            h = splitmix64(np.uint64(seed) ^ (ctr * PHI))
+            sel = []
+            for q in range(k):
+                j = m - k + q
+                t = int((int(h[q]) >> 32) * (j + 1) >> 32)
+                if t in sel:
+                    t = j
+                sel.append(t)
+            tt = np.array(sel, np.int64)
+            if no_self:
+                tt = np.where(tt >= i, tt + 1, tt)
+            post[off[i]:off[i + 1]] = tt
+            scale = np.float32(w_exc if i < n_exc else w_inh)
+            u = (h & np.uint64(0xFFFFFFFF)).astype(np.float32) * np.float32(2.3283064365386963e-10)
+            w[off[i]:off[i + 1]] = scale * u if random_w else scale
+    return pre, post, w
+
+
 def izhikevich_params(n: int, n_exc: int, seed: int):
     """Per-neuron a, b, c, d of the pulse-network recipe (r ~ U(0,1) per neuron)."""
     r = uniform01(seed, IZH_STREAM_R, np.arange(n, dtype=np.uint64))

@@ -108,13 +108,23 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
    which needs from == to), drawn by Floyd's sampling: with m candidates,
    draw q (j = m - k + q) takes t = hi32(h) * (j + 1) >> 32, or j when t was
    drawn before, h = splitmix64(seed ^ (i*k + q)*0x9E3779B97F4A7C15); without
-   self-loops t >= i maps to t + 1.  Weight w_exc for i < n_exc else w_inh,
-   times lo32(h) / 2^32 when random_w; fixed delay.  Edges are appended in
+   self-loops t >= i maps to t + 1 (k <= 4096).  Weight w_exc for i < n_exc
+   else w_inh, times lo32(h) / 2^32 when random_w; fixed delay.  Edges are appended in
    (source, draw) order.  This is the generator of the Izhikevich pulse
    network recipe (100 distinct targets, weights 0.5 U / -U, delay 1). */
 int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k, uint64_t seed,
                                int no_self, uint32_t n_exc, float w_exc, float w_inh, int random_w,
                                uint8_t delay);
+
+/* As sg_connect_fixed_outdegree with a lognormal out-degree per source:
+   deg_i = round(exp(mu + sigma z_i)) clipped to [1, min(candidates, 4096)],
+   sigma^2 = ln(1 + sd^2/mean^2), mu = ln(mean) - sigma^2/2, z_i the FP64
+   Box-Muller normal of counter i (stream 7, the sg_pop_set_noise hash);
+   source i's draws use hash counters off_i + q (off = exclusive prefix sum
+   of the degrees). */
+int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, double mean, double sd,
+                                   uint64_t seed, int no_self, uint32_t n_exc, float w_exc, float w_inh,
+                                   int random_w, uint8_t delay);
 
 /* Network::register_kinetics(SynapseKinetics::ExpOne{tau_decay, erev}, dt)
    -> profile id (1-based), core.rs:564-584; step.rs:248-345 */

@@ -137,3 +137,22 @@ def test_noise_change_after_steps_takes_effect():
     assert np.array_equal(a.state(pa, 0), b.state(pb, 0))
     a.close()
     b.close()
+
+
+def test_lognormal_outdegree_generator_matches_numpy_twin():
+    n, seed = 1200, 8
+    net = sg.Network(0)
+    p = net.add_population(IZH, n)
+    net.connect_lognormal_outdegree(p, p, 100.0, 60.0, seed, True, 960, 0.5, -1.0)
+    net.build()
+    rp, col, w, d = net.graph()
+    pre, post, ww = W.lognormal_outdegree_edges(n, 100.0, 60.0, seed, 960, 0.5, -1.0)
+    order = np.lexsort((post, pre))
+    assert np.array_equal(col, post[order])
+    assert np.array_equal(w, ww[order])
+    deg = np.diff(rp)
+    assert abs(deg.mean() - 100.0) < 6.0 and abs(deg.std() - 60.0) < 8.0
+    for i in range(0, n, 97):                      # distinct targets, no self-loop
+        r = col[rp[i]:rp[i + 1]]
+        assert np.unique(r).size == r.size and not np.any(r == i)
+    net.close()
