@@ -25,6 +25,11 @@ Reported, one JSON line on rank 0:
           steps) against MEASURED_PEAKS.json's copy bandwidth.
   cpu_baseline  the CPU restatement of the reference step (oracle/) on this
           host's cores, on a bounded sample of the same network.
+  batched   (extra key) 64 uneven Izhikevich networks stepping as one batch
+          against the same instances one at a time.
+  serving   (extra key) a Poisson stream of LIF / Izhikevich requests through
+          the continuous-batching server: served sims/s, p50/p99 latency,
+          against the one-at-a-time loop.
 `--impl reference` times that CPU path alone as the reference arm.
 Multi-GPU (`--gpus N` under torchrun): each rank simulates its own replica
 (seed + rank); no data-path collective (weak scaling).
@@ -69,6 +74,10 @@ def parse():
     ap.add_argument("--k-in", type=int, default=1000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
     return ap.parse_args()
 
 
@@ -90,7 +99,8 @@ def config(args, name, spec):
         "sim_steps_per_bench_step": args.sim_steps,
         "external_drive": {"rate_hz": spec["ext_rate_hz"], "ring_weight": spec["ext_weight"]},
         "weights": "fp32", "scatter": "deterministic (reference summation order)",
-        "l2": "inputs larger than L2: 8 GB of synapse records and 128 MB of delay rings against a "
+        "l2": "inputs larger than L2: 8 GB of synapse records and "
+              f"{(21 * spec['n'] * 4) / 1e6:.0f} MB of delay rings (21 slots for delays up to 20) against a "
               "126 MB L2; each step reads the spiking rows",
         "parallelism": f"replicas x{args.gpus}",
     }
@@ -205,6 +215,103 @@ def profiled_traffic(kernel):
 
 
 # ---------------------------------------------------------------------------
+def run_batched(args, local):
+    """Many uneven Izhikevich networks (the pulse-network recipe, N log-uniform
+    in 500..200,000, device-generated synapses and thalamic noise) stepping as
+    one batch, against the same instances run one at a time."""
+    import numpy as np
+    import torch
+
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+    K, steps = args.batch_instances, 1000
+    u = W.uniform01(7, 1, np.arange(K, dtype=np.uint64))
+    sizes = np.floor(np.exp(np.log(500) + u * (np.log(200001) - np.log(500)))).astype(int)
+
+    def timed(net, n_steps):
+        st = torch.cuda.ExternalStream(net.stream, device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0 = net.events_total
+        e0.record(st)
+        net.step(n_steps)
+        e1.record(st)
+        net.synchronize()
+        return e0.elapsed_time(e1), net.events_total - ev0
+
+    net = sg.Network(local)
+    for i, n in enumerate(sizes):
+        W.add_izhikevich_instance(net, int(n), 1000 + i)
+    net.build()
+    net.step(64)
+    ms, ev = timed(net, steps)
+    fp = net.footprint
+    net.close()
+    solo_ms, solo_ev, n_solo = 0.0, 0, min(8, K)
+    for i in range(n_solo):
+        a = sg.Network(local)
+        W.add_izhikevich_instance(a, int(sizes[i]), 1000 + i)
+        a.build()
+        a.step(64)
+        m, e = timed(a, steps)
+        solo_ms, solo_ev = solo_ms + m, solo_ev + e
+        a.close()
+    ev_s, solo_s = ev / (ms / 1e3), solo_ev / (solo_ms / 1e3)
+    return {"workload": f"{K} Izhikevich pulse networks, N log-uniform 500..200000 ({int(sizes.sum())} neurons, "
+                        "100 distinct targets each, device thalamic noise), 1000 steps, one batch",
+            "events_per_s": ev_s, "neuron_updates_per_s": float(sizes.sum()) * steps / (ms / 1e3),
+            "ms_per_step": ms / steps, "footprint_gb": fp / 1e9, "weights": "fp32",
+            "one_at_a_time_events_per_s": solo_s, "one_at_a_time_sample": f"first {n_solo} instances",
+            "speedup_vs_one_at_a_time": ev_s / solo_s}
+
+
+def run_serving(args, local):
+    """A Poisson stream of seeded LIF / Izhikevich requests (N log-uniform in
+    10,000..2,000,000, lognormal out-degree mean 100 sd 60, 1 s simulated)
+    through the continuous-batching server, against the one-at-a-time loop."""
+    import numpy as np
+
+    from simuse_b200 import serve as S
+    from simuse_b200 import workloads as W
+    n_req, lam = args.serve_requests, args.serve_rate
+
+    def make():
+        idx = np.arange(n_req, dtype=np.uint64)
+        u = W.uniform01(77, 1, idx)
+        ns = np.floor(np.exp(np.log(1e4) + u * (np.log(2e6) - np.log(1e4)))).astype(int)
+        kinds = np.where(W.uniform01(77, 2, idx) < 0.5, "lif", "izh")
+        return [S.Request(str(k), int(n), 500 + i, 10000 if k == "lif" else 1000)
+                for i, (k, n) in enumerate(zip(kinds, ns))]
+
+    t0 = time.perf_counter()
+    solo = [S.run_alone(r, device=local, chunk=1000) for r in make()]
+    t_solo = time.perf_counter() - t0
+    reqs = make()
+    arrive = np.cumsum(-np.log(1.0 - W.uniform01(78, 1, np.arange(n_req, dtype=np.uint64))) / lam)
+    srv = S.Server(device=local, budget_bytes=160 * 10**9, max_resident=16, chunk=500)
+    t0 = time.perf_counter()
+    for r, ta in zip(reqs, arrive):
+        wait = t0 + ta - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        srv.submit(r)
+    srv.wait_idle(1800)
+    t_all = time.perf_counter() - t0
+    srv.close()
+    lat = srv.latency_percentiles()
+    same = all(np.array_equal(a.spike_steps, b.spike_steps) and np.array_equal(a.spike_index, b.spike_index)
+               for a, b in zip(solo, reqs))
+    solo_lat = np.array([r.latency for r in solo])
+    return {"workload": f"{n_req} requests, Poisson arrivals at {lam:g}/s, LIF (10000 steps) or Izhikevich "
+                        "(1000 steps), N log-uniform 1e4..2e6, lognormal out-degree (100, 60)",
+            "served_sims_per_s": n_req / t_all, "p50_latency_s": lat["p50_s"], "p99_latency_s": lat["p99_s"],
+            "one_at_a_time_sims_per_s": n_req / t_solo,
+            "one_at_a_time_p50_s": float(np.percentile(solo_lat, 50)),
+            "one_at_a_time_p99_s": float(np.percentile(solo_lat, 99)),
+            "speedup_vs_one_at_a_time": (n_req / t_all) / (n_req / t_solo),
+            "budget_gb": 160, "weights": "fp32", "results_same_as_alone": bool(same),
+            "errors": int(sum(r.error is not None for r in reqs))}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -317,8 +424,8 @@ def run_ours(args):
     step_alg = sum(alg)
     step_ms = ms / (args.steps * S)
 
+    net.close()  # the headline network leaves HBM before the extra measurements
     if dist is not None:
-        net.close()
         dist.destroy_process_group()
     if rank != 0:
         return
@@ -344,6 +451,9 @@ def run_ours(args):
         "clocks": clk.summary(),
         "gpu_launches": int(args.steps * S * 2),
     }
+    if not args.no_extras and world == 1:
+        out["batched"] = run_batched(args, local)
+        out["serving"] = run_serving(args, local)
     if not args.no_cpu_baseline and world == 1:
         cnet, cores, build_s = cpu_baseline(args, spec, args.cpu_seconds)
         ev, nsteps, el = run_cpu_sample(cnet, args.cpu_seconds)

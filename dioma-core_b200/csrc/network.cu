@@ -1051,6 +1051,21 @@ int sg_synchronize(sg_net *net) {
   });
 }
 
+int sg_query(sg_net *net, int *idle) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(idle, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    const cudaError_t e = cudaStreamQuery(net->stream);
+    if (e == cudaErrorNotReady) {
+      *idle = 0;
+      return;
+    }
+    SG_CUDA(e);
+    *idle = 1;
+  });
+}
+
 int sg_pop_add(sg_net *net, int model, uint32_t n, uint32_t *out_pop) {
   NET_CHECK(net);
   return run([&] {

@@ -187,6 +187,12 @@ class Network:
     def step(self, n_steps: int = 1):
         check(lib().sg_step(self._h, n_steps))
 
+    def idle(self) -> bool:
+        """True when every step queued so far has finished (non-blocking)."""
+        out = C.c_int()
+        check(lib().sg_query(self._h, C.byref(out)))
+        return bool(out.value)
+
     def synchronize(self):
         check(lib().sg_synchronize(self._h))
 

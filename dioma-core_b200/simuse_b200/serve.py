@@ -272,20 +272,28 @@ class Server:
             if not resident:
                 time.sleep(0.0005)
                 continue
-            # one round: every resident network advances one chunk on its own
-            # stream (launches are asynchronous, so the chunks overlap), then
-            # each chunk's spikes are read back
-            for r in resident:
-                r.k = min(r.chunk, r.req.steps - r.done)
-                r.net.step(r.k)
+            # every resident network advances independently: when its last
+            # chunk has finished (non-blocking query) its spikes are read back
+            # and its next chunk is queued on its own stream, so the chunks of
+            # different networks overlap on the device and a small network is
+            # never held back by a large one
+            progressed = False
             finished = []
             for r in resident:
-                s, i = r.net.read_spike_events()
-                r.st.append(s)
-                r.ix.append(i)
-                r.done += r.k
+                if r.k and not r.net.idle():
+                    continue
+                progressed = True
+                if r.k:
+                    s, i = r.net.read_spike_events()
+                    r.st.append(s)
+                    r.ix.append(i)
+                    r.done += r.k
+                    r.k = 0
                 if r.done >= r.req.steps:
                     finished.append(r)
+                    continue
+                r.k = min(r.chunk, r.req.steps - r.done)
+                r.net.step(r.k)
             for r in finished:
                 resident.remove(r)
                 _finish(r.req, r.st, r.ix)
@@ -293,3 +301,5 @@ class Server:
                 with self._lock:
                     self._reserved -= r.req.footprint
                 self._complete(r.req)
+            if not progressed:
+                time.sleep(0.0002)

@@ -69,6 +69,9 @@ int sg_device_count(int *out);
 int sg_net_create(sg_net **out, int device);    /* Network::new, core.rs:87-113 */
 int sg_net_destroy(sg_net *net);                /* Drop for Network */
 int sg_synchronize(sg_net *net);
+/* Non-blocking: *idle = 1 when all work queued on the handle's stream has
+   completed, 0 while some is still running (cudaStreamQuery). */
+int sg_query(sg_net *net, int *idle);
 
 /* ---- builder (before sg_build) ---------------------------------------- */
 /* Network::add_population::<M>(n) -> PopulationId, core.rs:149-155 */
