@@ -82,6 +82,7 @@ struct HostPop {
   uint32_t noise_stream = 0, noise_split = 0;
   uint64_t noise_seed = 0, noise_stride = 0, noise_step0 = 0;
   double noise_sigma[2] = {0.0, 0.0};
+  DBuf<float> d_bias;  // sg_pop_set_bias, [cap] (zero past n)
   std::vector<float> params, state;  // before build
   DBuf<float> d_params, d_state;     // after build
 };
@@ -870,6 +871,7 @@ void upload_pop_table(sg_net *net) {
     pa.noise_step0 = p.noise_step0;
     pa.noise_sigma[0] = p.noise_sigma[0];
     pa.noise_sigma[1] = p.noise_sigma[1];
+    pa.bias = p.d_bias.n ? p.d_bias.p : nullptr;
   }
   for (int m = 1; m <= 4; ++m) {
     net->model_blk_off[m] = (uint32_t)map.size();
@@ -1525,6 +1527,40 @@ int sg_pop_set_noise(sg_net *net, uint32_t pop, uint64_t seed, uint32_t stream, 
     p.noise_split = split;
     net->pop_tab_dirty = true;
     drop_graph(net);  // a captured step graph may hold the old arguments by value
+  });
+}
+
+int sg_pop_set_bias(sg_net *net, uint32_t pop, const float *vals, uint32_t n) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "set_bias needs a built network");
+    require_pop(net, pop);
+    HostPop &p = net->pops[pop];
+    SG_REQUIRE(n <= p.n, SG_E_INVALID, "more bias values than neurons");
+    DevGuard g(net->device);
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    if (n == 0) {
+      p.d_bias.release();
+    } else {
+      for (uint32_t i = 0; i < n; ++i) SG_REQUIRE(std::isfinite(vals[i]), SG_E_INVALID, "bias must be finite");
+      if (p.d_bias.n != p.cap) p.d_bias.alloc(p.cap);
+      std::vector<float> h(p.cap, 0.0f);
+      std::copy(vals, vals + n, h.begin());
+      SG_CUDA(cudaMemcpy(p.d_bias.p, h.data(), (size_t)p.cap * 4, cudaMemcpyHostToDevice));
+    }
+    net->pop_tab_dirty = true;
+    drop_graph(net);
+  });
+}
+
+int sg_ring_clear(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    DevGuard g(net->device);
+    net->d_ring.zero(net->stream);
+    net->d_kin_g.zero(net->stream);
+    SG_CUDA(cudaStreamSynchronize(net->stream));
   });
 }
 

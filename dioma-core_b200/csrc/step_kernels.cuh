@@ -138,6 +138,9 @@ struct PopArgs {
   uint32_t noise_stream, noise_split;
   unsigned long long noise_seed, noise_stride, noise_step0;
   double noise_sigma[2];
+  // constant per-neuron input current added every step (as an
+  // inject_current of the same values each step would), or null
+  const float *bias;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -231,6 +234,12 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   float *rs = a.ring + (size_t)slot * a.Nd + gi0;
   V::load(rs, x);
   V::store(rs, zero);
+  if (p.bias != nullptr) {
+    float bv[NPT];
+    V::ldg(p.bias + i0, bv);
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) x[q] = x[q] + bv[q];
+  }
   if (p.noise) {
     const unsigned long long t = step - p.noise_step0;
 #pragma unroll

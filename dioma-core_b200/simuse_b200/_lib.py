@@ -56,6 +56,8 @@ SIGNATURES = {
     "sg_build": [vp],
     "sg_build_from_csr": [vp, vp, vp, vp, vp],
     "sg_pop_set_noise": [vp, u32, u64, u32, u64, u64, f64, f64, u32],
+    "sg_pop_set_bias": [vp, u32, vp, u32],
+    "sg_ring_clear": [vp],
     "sg_inject": [vp, u32, vp, vp, u64],
     "sg_step": [vp, u32],
     "sg_raster_enable": [vp, u32],

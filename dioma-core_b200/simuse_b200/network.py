@@ -176,6 +176,15 @@ class Network:
                                      int(step0), float(sigma_lo), float(sigma_lo if sigma_hi is None else sigma_hi),
                                      int(n if split is None else split)))
 
+    def set_bias(self, pop: int, values):
+        """Constant input current per neuron, added every step (sg_pop_set_bias)."""
+        a = np.ascontiguousarray(values, np.float32)
+        check(lib().sg_pop_set_bias(self._h, pop, _p(a), a.size))
+
+    def clear_rings(self):
+        """Empty the delay rings (the state of a freshly built network)."""
+        check(lib().sg_ring_clear(self._h))
+
     def inject_current(self, pop, indices, values):
         i = np.ascontiguousarray(indices, np.uint32)
         v = np.ascontiguousarray(values, np.float32)

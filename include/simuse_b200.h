@@ -178,6 +178,17 @@ int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col,
 int sg_pop_set_noise(sg_net *net, uint32_t pop, uint64_t seed, uint32_t stream, uint64_t stride,
                      uint64_t step0, double sigma_lo, double sigma_hi, uint32_t split);
 
+/* Constant per-neuron input current added to the slot value every step, the
+   device form of calling inject_current with the same values before each
+   step (BrainRunner::run's external_I, pillars-connectome runner.rs:798-937;
+   the add is the same float operation, so results are identical).  Values
+   past n are 0; n = 0 removes it.  Needs a built network. */
+int sg_pop_set_bias(sg_net *net, uint32_t pop, const float *vals, uint32_t n);
+/* Empties every delay ring (and kinetic conductance): the state of a freshly
+   built Network, which BrainRunner::run starts from on every call
+   (runner.rs:1342-1440 rebuilds its Brain each run). */
+int sg_ring_clear(sg_net *net);
+
 /* ---- run -------------------------------------------------------------- */
 /* Network::inject_current(pop, idx, vals), build.rs:243-275: same-step slot */
 int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals, uint64_t n);
