@@ -62,7 +62,7 @@ B_SPIKE = 16.0
 B_SOURCE = 8.0
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -78,7 +78,11 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=200.0)
-    return ap.parse_args()
+    return ap.parse_args(argv)
+
+
+def parse_args_for_test(argv):
+    return parse(argv)
 
 
 def workload(args, rank=0):
@@ -215,6 +219,19 @@ def profiled_traffic(kernel):
 
 
 # ---------------------------------------------------------------------------
+def reduce_over_ranks(dist, device, t, events):
+    """Job time = the slowest rank's time, job work = the sum over ranks
+    (every rank takes these two collectives in the same order)."""
+    if dist is None:
+        return t, events
+    import torch
+    tt = torch.tensor([float(t)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    ee = torch.tensor([float(events)], device=device, dtype=torch.float64)
+    dist.all_reduce(ee, op=dist.ReduceOp.SUM)
+    return float(tt.item()), float(ee.item())
+
+
 def run_batched(args, local):
     """Many uneven Izhikevich networks (the pulse-network recipe, N log-uniform
     in 500..200,000, device-generated synapses and thalamic noise) stepping as
@@ -365,15 +382,7 @@ def run_ours(args):
     events = net.events_total - ev0
     spk, evs = net.read_stats()
     spk = spk[-args.steps * S:]
-    t_max = ms
-    ev_all = events
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        e = torch.tensor([float(events)], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        ev_all = float(e.item())
+    t_max, ev_all = reduce_over_ranks(dist, f"cuda:{local}", ms, events)
     value = ev_all / (t_max / 1e3)
 
     # ---- (B) end to end through the C ABI with host buffers --------------------
@@ -393,13 +402,7 @@ def run_ours(args):
         d2h += n_sp * 8
     t_e2e = time.perf_counter() - t0
     ev_e2e = net.events_total - ev0
-    if dist is not None:
-        t = torch.tensor([t_e2e], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-        e = torch.tensor([float(ev_e2e)], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        ev_e2e = float(e.item())
+    t_e2e, ev_e2e = reduce_over_ranks(dist, f"cuda:{local}", t_e2e, ev_e2e)
     net.enable_raster(0)
 
     # ---- (C) per-kernel timing: CUDA events around each phase --------------------
