@@ -75,6 +75,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--weights", default="fp32", choices=["fp32", "bf16"],
+                    help="synapse weight storage (bf16: 6 B per synapse, FP32 accumulation)")
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=200.0)
@@ -102,7 +104,7 @@ def config(args, name, spec):
         "dt_ms": spec["dt"],
         "sim_steps_per_bench_step": args.sim_steps,
         "external_drive": {"rate_hz": spec["ext_rate_hz"], "ring_weight": spec["ext_weight"]},
-        "weights": "fp32", "scatter": "deterministic (reference summation order)",
+        "weights": args.weights, "scatter": "deterministic (reference summation order)",
         "l2": "inputs larger than L2: 8 GB of synapse records and "
               f"{(21 * spec['n'] * 4) / 1e6:.0f} MB of delay rings (21 slots for delays up to 20) against a "
               "126 MB L2; each step reads the spiking rows",
@@ -350,6 +352,8 @@ def run_ours(args):
 
     spec, name = workload(args, rank)
     net = sg.Network(local)
+    if args.weights == "bf16":
+        net.set_weight_format(sg.W_BF16)   # 20, -100 and 100 are exact in bf16: same spikes as fp32
     W.build_lif(net, spec)
     net.build()
     net.synchronize()

@@ -132,6 +132,8 @@ struct sg_net {
   DBuf<uint32_t> d_row_ptr;
   // one 8-byte record per synapse: x = post (| code << 24 when packed), y = weight bits
   DBuf<uint2> d_edge;
+  DBuf<uint32_t> d_edge_x;  // BF16 form: the records' x words
+  DBuf<uint16_t> d_w16;     //   and their weights in bf16
   DBuf<uint8_t> d_code;  // code byte per synapse when it does not fit in x
   int packed = 1;
   uint64_t n_edges = 0;
@@ -250,6 +252,9 @@ StepArgs make_args(sg_net *net) {
   a.kin_g = net->d_kin_g.p;
   a.row_ptr = net->d_row_ptr.p;
   a.edge = net->d_edge.p;
+  a.wbf16 = net->weight_format == SG_W_BF16 ? 1 : 0;
+  a.edge_x = net->d_edge_x.p;
+  a.w16 = net->d_w16.p;
   a.code = net->packed ? nullptr : net->d_code.p;
   a.post_mask = net->packed ? 0x00FFFFFFu : 0xFFFFFFFFu;
   a.n_edges = (uint32_t)net->n_edges;
@@ -790,6 +795,33 @@ void compute_uniform(HostPop &p) {
       p.uval[c] = col[0];
     }
   }
+}
+
+// f32 -> bf16 by round to nearest even (finite inputs; weights are checked)
+__global__ void split_bf16_kernel(const uint2 *edge, uint32_t *ex, uint16_t *w16, uint64_t E) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 r = edge[e];
+    ex[e] = r.x;
+    w16[e] = (uint16_t)((r.y + 0x7FFFu + ((r.y >> 16) & 1u)) >> 16);
+  }
+}
+
+// BF16 weight storage: after the segment table is built from the records,
+// split them into x words and bf16 weights and free the 8-byte records.
+void split_bf16(sg_net *net) {
+  if (net->weight_format != SG_W_BF16) return;
+  SG_REQUIRE(!net->stdp_on, SG_E_INVALID, "BF16 weights are read-only: pair STDP needs FP32 weights");
+  const uint64_t E = net->n_edges;
+  cudaStream_t s = net->stream;
+  net->d_edge_x.alloc(std::max<uint64_t>(E, 1));
+  net->d_w16.alloc(std::max<uint64_t>(E, 1));
+  if (E) {
+    const unsigned b = (unsigned)std::min<uint64_t>((E + 255) / 256, 148u * 32u);
+    split_bf16_kernel<<<b, 256, 0, s>>>(net->d_edge.p, net->d_edge_x.p, net->d_w16.p, E);
+    SG_CUDA(cudaGetLastError());
+  }
+  SG_CUDA(cudaStreamSynchronize(s));
+  net->d_edge.release();
 }
 
 void finish_build(sg_net *net) {
@@ -1445,7 +1477,8 @@ int sg_set_weight_format(sg_net *net, int format) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "weight format must be set before build()");
-    SG_REQUIRE(format == SG_W_F32, SG_E_INVALID, "only FP32 weights are available in this build");
+    SG_REQUIRE(format == SG_W_F32 || format == SG_W_BF16, SG_E_INVALID,
+               "weight format: FP32 and BF16 are available (FP8 is not built)");
     net->weight_format = format;
   });
 }
@@ -1474,6 +1507,7 @@ int sg_build(sg_net *net) {
     build_segments(net);
     build_sources(net);
     if (net->stdp_on) build_stdp(net);
+    split_bf16(net);
     finish_build(net);
   });
 }
@@ -1830,7 +1864,16 @@ static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float
   std::vector<uint2> ed(E);
   std::vector<uint8_t> code(net->packed ? 0 : E);
   SG_CUDA(cudaMemcpyAsync(rp.data(), net->d_row_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToHost, net->stream));
-  if (E) {
+  if (E && net->weight_format == SG_W_BF16) {
+    std::vector<uint32_t> ex(E);
+    std::vector<uint16_t> w16(E);
+    SG_CUDA(cudaMemcpyAsync(ex.data(), net->d_edge_x.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(w16.data(), net->d_w16.p, E * 2, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (uint64_t e = 0; e < E; ++e) ed[e] = make_uint2(ex[e], (uint32_t)w16[e] << 16);
+    if (!net->packed && !only_w)
+      SG_CUDA(cudaMemcpyAsync(code.data(), net->d_code.p, E, cudaMemcpyDeviceToHost, net->stream));
+  } else if (E) {
     SG_CUDA(cudaMemcpyAsync(ed.data(), net->d_edge.p, E * 8, cudaMemcpyDeviceToHost, net->stream));
     if (!net->packed && !only_w)
       SG_CUDA(cudaMemcpyAsync(code.data(), net->d_code.p, E, cudaMemcpyDeviceToHost, net->stream));
@@ -1949,6 +1992,7 @@ int sg_footprint(sg_net *net, uint64_t *out) {
     uint64_t b = 0;
     for (auto &p : net->pops) b += (p.d_params.n + p.d_state.n) * 4;
     b += net->d_ring.n * 4 + net->d_kin_g.n * 4 + net->d_row_ptr.n * 4 + net->d_edge.n * 8 +
+         net->d_edge_x.n * 4 + net->d_w16.n * 2 +
          (net->packed ? 0 : net->d_code.n) + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
          net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +

@@ -91,6 +91,11 @@ struct StepArgs {
   const uint32_t *row_ptr;
   uint2 *edge;
   const uint8_t *code;  // null when packed
+  // BF16 weight storage: the record's x word and the bf16 weight in two
+  // arrays (6 B per synapse instead of 8); edge is null then
+  int wbf16;
+  const uint32_t *edge_x;
+  const uint16_t *w16;
   uint32_t post_mask;
   uint32_t n_edges;
   // per-row segment table: [Nd][G+1] offsets inside the row (u16 or u32)
@@ -182,6 +187,17 @@ __device__ __forceinline__ uint2 ld_stream_edge(const uint2 *p, unsigned long lo
 }
 // Ring loads do not allocate in L1: a window issues kWin of them per SM at
 // once and the ring is re-read only in later steps.
+__device__ __forceinline__ uint32_t ld_stream_u16(const uint16_t *p, unsigned long long pol) {
+  uint16_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
+  return v;
+}
+// One synapse record (x = post | code << 24, y = f32 weight bits); the bf16
+// form widens the stored weight to f32 (its upper 16 bits).
+__device__ __forceinline__ uint2 ld_record(const StepArgs &a, uint32_t e, unsigned long long pol) {
+  if (a.wbf16) return make_uint2(ld_stream_u32(a.edge_x + e, pol), ld_stream_u16(a.w16 + e, pol) << 16);
+  return ld_stream_edge(a.edge + e, pol);
+}
 __device__ __forceinline__ float ld_ring(const float *p, unsigned long long pol) {
   float v;
   asm volatile("ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol) : "memory");
@@ -666,7 +682,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
           if (k < m) {
-            const uint2 rec = ld_stream_edge(a.edge + ev_e[r], spol);
+            const uint2 rec = ld_record(a, ev_e[r], spol);
             ev_post[r] = rec.x & a.post_mask;
             ev_w[r] = __uint_as_float(rec.y);
             ev_code[r] = a.code ? (uint8_t)ld_stream_u8(a.code + ev_e[r], spol) : (uint8_t)(rec.x >> 24);
