@@ -132,6 +132,9 @@ struct sg_net {
   DBuf<uint32_t> d_row_ptr;
   // one 8-byte record per synapse: x = post (| code << 24 when packed), y = weight bits
   DBuf<uint2> d_edge;
+  DBuf<uint32_t> d_ns_count, d_ns_last;  // sg_neuron_stats_enable
+  DBuf<double> d_ns_s1, d_ns_s2;
+  unsigned long long ns_step0 = 0;
   DBuf<uint32_t> d_edge_x;  // BF16 form: the records' x words
   DBuf<uint16_t> d_w16;     //   and their weights in bf16
   DBuf<uint8_t> d_code;  // code byte per synapse when it does not fit in x
@@ -241,6 +244,11 @@ StepArgs make_args(sg_net *net) {
   a.stat_ev = net->d_stat_ev.p;
   a.stat_cap = net->stat_cap;
   a.clamp_hits = net->d_clamp.p;
+  a.ns_count = net->d_ns_count.n ? net->d_ns_count.p : nullptr;
+  a.ns_last = net->d_ns_last.p;
+  a.ns_s1 = net->d_ns_s1.p;
+  a.ns_s2 = net->d_ns_s2.p;
+  a.ns_step0 = net->ns_step0;
   a.ring = net->d_ring.p;
   a.Nd = net->Nd;
   a.nslots = net->nslots;
@@ -1943,6 +1951,67 @@ int sg_ring_read(sg_net *net, uint32_t ring, float *out) {
         for (uint32_t i = 0; i < net->pops[p].n; ++i)
           out[(size_t)s * N + net->offsets[p] + i] = held ? r[(size_t)ds * Nd + net->pops[p].dev_off + i] : 0.0f;
     }
+  });
+}
+
+int sg_neuron_stats_enable(sg_net *net, int on) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    DevGuard g(net->device);
+    cudaStream_t s = net->stream;
+    SG_CUDA(cudaStreamSynchronize(s));
+    drop_graph(net);
+    if (!on) {
+      net->d_ns_count.release();
+      net->d_ns_last.release();
+      net->d_ns_s1.release();
+      net->d_ns_s2.release();
+      return;
+    }
+    const uint32_t Nd = net->Nd;
+    net->d_ns_count.alloc(Nd);
+    net->d_ns_last.alloc(Nd);
+    net->d_ns_s1.alloc(Nd);
+    net->d_ns_s2.alloc(Nd);
+    net->d_ns_count.zero(s);
+    SG_CUDA(cudaMemsetAsync(net->d_ns_last.p, 0xFF, (size_t)Nd * 4, s));
+    net->d_ns_s1.zero(s);
+    net->d_ns_s2.zero(s);
+    SG_CUDA(cudaMemcpyAsync(&net->ns_step0, net->d_step.p, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int sg_neuron_stats_read(sg_net *net, uint32_t pop, uint32_t *counts, double *isi_mean, double *isi_cv,
+                         uint64_t *steps) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->d_ns_count.n, SG_E_STATE, "neuron statistics are not enabled");
+    require_pop(net, pop);
+    SG_REQUIRE(counts && isi_mean && isi_cv && steps, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    cudaStream_t s = net->stream;
+    const HostPop &p = net->pops[pop];
+    std::vector<uint32_t> c(p.n);
+    std::vector<double> s1(p.n), s2(p.n);
+    unsigned long long step = 0;
+    if (p.n) {
+      SG_CUDA(cudaMemcpyAsync(c.data(), net->d_ns_count.p + p.dev_off, (size_t)p.n * 4, cudaMemcpyDeviceToHost, s));
+      SG_CUDA(cudaMemcpyAsync(s1.data(), net->d_ns_s1.p + p.dev_off, (size_t)p.n * 8, cudaMemcpyDeviceToHost, s));
+      SG_CUDA(cudaMemcpyAsync(s2.data(), net->d_ns_s2.p + p.dev_off, (size_t)p.n * 8, cudaMemcpyDeviceToHost, s));
+    }
+    SG_CUDA(cudaMemcpyAsync(&step, net->d_step.p, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t i = 0; i < p.n; ++i) {
+      counts[i] = c[i];
+      const double k = c[i] ? (double)(c[i] - 1) : 0.0;  // intervals
+      isi_mean[i] = k > 0 ? s1[i] / k : 0.0;
+      // sample variance of the intervals (P/kernels/stats/isi.rs:30-66: >= 2 intervals)
+      const double var = k >= 2 ? (s2[i] - s1[i] * s1[i] / k) / (k - 1.0) : 0.0;
+      isi_cv[i] = (k >= 2 && isi_mean[i] > 0) ? std::sqrt(std::max(var, 0.0)) / isi_mean[i] : 0.0;
+    }
+    *steps = step - net->ns_step0;
   });
 }
 

@@ -75,6 +75,14 @@ struct StepArgs {
   unsigned long long *stat_ev;
   uint32_t stat_cap;
   unsigned long long *clamp_hits;
+  // per-neuron spike statistics (null when off): count, last spike step
+  // (steps since they were enabled, ~0u before the first), FP64 sums of the
+  // inter-spike intervals and of their squares (in steps: exact integers)
+  uint32_t *ns_count;
+  uint32_t *ns_last;
+  double *ns_s1;
+  double *ns_s2;
+  unsigned long long ns_step0;
   // rings: [n_rings][nslots][Nd]; a step's arrivals go to slot step % nslots
   // (nslots = the largest effective delay + 1, at most 32: the reference's
   // 32-slot ring, P/api/net/delay.rs:30-101, without the slots no delay reaches)
@@ -323,6 +331,22 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   }
 #pragma unroll
   for (int c = 0; c < NS; ++c) V::store(p.state + (size_t)c * p.cap + i0, sv[c]);
+  if (a.ns_count != nullptr && nib) {
+    const uint32_t t = (uint32_t)(step - a.ns_step0);
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (nib & (1u << q)) {
+        const uint32_t gi = gi0 + q;
+        const uint32_t last = a.ns_last[gi];
+        if (last != 0xFFFFFFFFu) {
+          const double isi = (double)(t - last);
+          a.ns_s1[gi] += isi;
+          a.ns_s2[gi] += isi * isi;
+        }
+        a.ns_last[gi] = t;
+        a.ns_count[gi] += 1u;
+      }
+  }
   // 4. compaction: bitmask words (32 neurons each) and the block's spike list
   uint32_t word;
   if (NPT == 4) {

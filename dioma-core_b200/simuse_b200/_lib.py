@@ -78,6 +78,8 @@ SIGNATURES = {
     "sg_stdp_traces": [vp, vp, vp],
     "sg_clamp_hits": [vp, vp],
     "sg_footprint": [vp, vp],
+    "sg_neuron_stats_enable": [vp, i32],
+    "sg_neuron_stats_read": [vp, u32, vp, vp, vp, vp],
     "sg_stream": [vp, vp],
     "sg_push_spikes": [vp, vp, vp, vp, u32, vp, u32, u64, vp, vp],
     "sg_push_spikes_noalloc": [vp, vp, vp, vp, u32, vp, u32, u64, vp, vp],

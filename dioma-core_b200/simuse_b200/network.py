@@ -262,6 +262,22 @@ class Network:
         return spk[: k.value], ev[: k.value]
 
     # -- readback -----------------------------------------------------------
+    def enable_neuron_stats(self, on: bool = True):
+        """Start (or stop) per-neuron spike statistics on the device."""
+        check(lib().sg_neuron_stats_enable(self._h, 1 if on else 0))
+
+    def neuron_stats(self, pop: int, dt_ms: float):
+        """(rates_hz, isi_cv, isi_mean_ms, steps) since the statistics were enabled."""
+        n = self._sizes[pop]
+        counts = np.empty(n, np.uint32)
+        mean = np.empty(n, np.float64)
+        cv = np.empty(n, np.float64)
+        steps = C.c_uint64()
+        check(lib().sg_neuron_stats_read(self._h, pop, _p(counts), _p(mean), _p(cv), C.byref(steps)))
+        dur_s = steps.value * dt_ms * 1e-3
+        rates = counts / dur_s if dur_s > 0 else np.zeros(n)
+        return rates, cv, mean * dt_ms, steps.value
+
     def spikes(self, pop: int) -> np.ndarray:
         out = np.empty(self._sizes[pop], np.int32)
         check(lib().sg_spikes(self._h, pop, _p(out), out.size))

@@ -229,6 +229,15 @@ int sg_stdp_traces(sg_net *net, float *x_pre, float *x_post);
 int sg_clamp_hits(sg_net *net, uint64_t *out); /* i_syn values that hit the +-100 clamp */
 /* Device bytes held by this network (state + CSR + rings + scratch). */
 int sg_footprint(sg_net *net, uint64_t *out);
+/* Per-neuron spike statistics accumulated on the device from the next step
+   on (P/kernels/stats/rates.rs:1-40, isi.rs:27-66): spike count, and the
+   mean and coefficient of variation of the inter-spike intervals (sample
+   variance, only for neurons with >= 2 intervals, else 0) from FP64 sums;
+   intervals in steps (the CV is unitless; rate = count / (steps * dt)).
+   Enabling (again) restarts them. */
+int sg_neuron_stats_enable(sg_net *net, int on);
+int sg_neuron_stats_read(sg_net *net, uint32_t pop, uint32_t *counts, double *isi_mean_steps,
+                         double *isi_cv, uint64_t *steps_observed);
 /* Device stream of the handle (cudaStream_t), for event timing. */
 int sg_stream(sg_net *net, void **out);
 

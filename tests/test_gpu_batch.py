@@ -156,3 +156,40 @@ def test_lognormal_outdegree_generator_matches_numpy_twin():
         r = col[rp[i]:rp[i + 1]]
         assert np.unique(r).size == r.size and not np.any(r == i)
     net.close()
+
+
+def _reference_cvs(raster, dt_s):
+    """P/kernels/stats/isi.rs:30-66 in float32 (two-pass, sample variance)."""
+    n_steps, n = raster.shape
+    out = np.zeros(n, np.float32)
+    for i in range(n):
+        t = np.nonzero(raster[:, i])[0]
+        isi = (np.diff(t).astype(np.float32) * np.float32(dt_s) * np.float32(1000.0)).astype(np.float32)
+        isi = isi[isi > 0]
+        if isi.size >= 2:
+            m = np.float32(isi.sum(dtype=np.float32) / np.float32(isi.size))
+            var = np.float32(((isi - m) ** 2).sum(dtype=np.float32) / np.float32(isi.size - 1))
+            out[i] = np.sqrt(var) / m
+    return out
+
+
+def test_device_rates_and_isi_cv_match_the_raster():
+    n, steps = 1000, 600
+    net = sg.Network(0)
+    p = W.add_izhikevich_instance(net, n, 17)
+    net.build()
+    net.step(20)
+    net.enable_neuron_stats()
+    net.enable_raster(steps)
+    net.step(steps)
+    raster = net.read_raster()
+    rates, cv, mean_ms, nst = net.neuron_stats(p, 1.0)
+    assert nst == steps
+    counts = raster.sum(axis=0)
+    assert np.array_equal(np.rint(rates * steps * 1e-3).astype(int), counts)
+    ref = _reference_cvs(raster, 1e-3)
+    has = ref > 0
+    assert has.sum() > 100
+    assert np.allclose(cv[has], ref[has], rtol=1e-4)
+    assert np.all(cv[~has] == 0)
+    net.close()
