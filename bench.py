@@ -75,6 +75,15 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--case", default="headline", choices=["headline", "kuramoto-sweep", "izh-batch", "hh-stdp"],
+                    help="headline: the JSON line above; the others time one workload alone (also the "
+                         "profiling entry points)")
+    ap.add_argument("--instances", type=int, default=1024)
+    ap.add_argument("--hh-wmax", type=float, default=0.01,
+                    help="hh-stdp weights U(0, w_max) (raw conductance per synapse): the stated 0.5 "
+                         "silences the network after its onset volley, 0.01 keeps it firing irregularly")
+    ap.add_argument("--hh-steps", type=int, default=200_000,
+                    help="hh-stdp simulation steps timed (200000 = the stated 2 s run at dt 0.01 ms)")
     ap.add_argument("--weights", default="fp32", choices=["fp32", "bf16"],
                     help="synapse weight storage (bf16: 6 B per synapse, FP32 accumulation)")
     ap.add_argument("--batch-instances", type=int, default=64)
@@ -499,9 +508,76 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_case(args):
+    """One workload alone, one JSON line (oscillator-steps/s or events/s)."""
+    import numpy as np
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if args.case == "izh-batch":
+        args.batch_instances = args.instances
+        print(json.dumps({"case": args.case, **run_batched(args, local)}), flush=True)
+        return
+    if args.case == "hh-stdp":
+        import simuse_b200 as sg
+        from simuse_b200 import workloads as W
+        n = args.n if args.n != 1_000_000 else 100_000
+        net = sg.Network(local)
+        pop = W.add_hh_stdp(net, n, w_max=args.hh_wmax)
+        net.build()
+        net.step(args.warmup * 100)
+        net.enable_neuron_stats()
+        net.synchronize()
+        S = args.hh_steps
+        st = torch.cuda.ExternalStream(net.stream, device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0, d0 = net.events_total, net.stdp_drift
+        e0.record(st)
+        net.step(S)
+        e1.record(st)
+        net.synchronize()
+        ms = e0.elapsed_time(e1)
+        ev = net.events_total - ev0
+        rates = net.neuron_stats(pop, 0.01)[0]
+        print(json.dumps({"case": args.case, "metric": "synaptic events/s", "value": ev / (ms / 1e3),
+                          "neuron_updates_per_s": n * S / (ms / 1e3), "neurons": n,
+                          "synapses": net.num_synapses, "steps": S, "simulated_s": S * 0.01e-3,
+                          "ms_per_step": ms / S, "events_per_step": ev / S,
+                          "stdp_drift": net.stdp_drift - d0, "w_max": args.hh_wmax,
+                          "rate_hz": float(rates.mean()),
+                          "workload": "HH (RK4, dt 0.01 ms) + ExpOne conductance synapses + pair STDP, lognormal "
+                                      "out-degree (200, 80), bias N(10, 2), weights U(0, w_max), per-neuron "
+                                      "spike counts on"}), flush=True)
+        net.close()
+        return
+    from simuse_b200 import KuramotoBatch
+    from simuse_b200 import workloads as W
+    sp = W.kuramoto_sweep(args.instances)
+    kb = KuramotoBatch(sp["sizes"], sp["coupling"], sp["dt"], device=local)
+    kb.set_state(sp["theta"], sp["omega"])
+    kb.run(args.warmup)
+    kb.synchronize()
+    st = torch.cuda.ExternalStream(kb.stream(), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    kb.run(args.sim_steps)
+    e1.record(st)
+    kb.synchronize()
+    ms = e0.elapsed_time(e1)
+    print(json.dumps({"case": args.case, "metric": "oscillator-steps/s",
+                      "value": kb.total * args.sim_steps / (ms / 1e3), "instances": args.instances,
+                      "oscillators": kb.total, "steps": args.sim_steps, "us_per_step": ms * 1e3 / args.sim_steps,
+                      "workload": "Kuramoto populations, N log-uniform 256..65536, K linear 0..4, omega "
+                                  "Lorentzian(0, 0.5), RK4 dt 0.01 (mean field)"}), flush=True)
+    kb.close()
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.case != "headline":
+        run_case(a)
     else:
         run_ours(a)

@@ -420,11 +420,23 @@ __global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, u
 // With per-source degrees (deg != null) source i draws deg[i] targets into
 // the edges from base + off[i]; the hash counter is then off[i] + q.
 constexpr uint32_t kMaxOutDegree = 4096;
+struct OutDegreeSpec {
+  uint64_t seed;
+  uint32_t from_off, to_off, n_to, n_exc;
+  int no_self, random_w;
+  float w_exc, w_inh;
+  uint32_t d_min, d_span;       // delay uniform in [d_min, d_min + d_span)
+  uint8_t st_exc, st_inh;       // synapse type (kinetic profile) by source class
+  uint32_t flags_exc;           // SG_EDGE_STDP for excitatory sources
+};
+
 __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, uint8_t *code, uint64_t base,
                                        uint32_t n_from, uint32_t k_fixed, const uint32_t *deg,
-                                       const unsigned long long *off, uint64_t seed, uint32_t from_off,
-                                       uint32_t to_off, uint32_t n_to, int no_self, uint32_t n_exc, float w_exc,
-                                       float w_inh, int random_w, uint8_t delay) {
+                                       const unsigned long long *off, OutDegreeSpec sp) {
+  const uint64_t seed = sp.seed;
+  const uint32_t from_off = sp.from_off, to_off = sp.to_off, n_to = sp.n_to, n_exc = sp.n_exc;
+  const int no_self = sp.no_self, random_w = sp.random_w;
+  const float w_exc = sp.w_exc, w_inh = sp.w_inh;
   const uint32_t m = n_to - (no_self ? 1u : 0u);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_from; i += gridDim.x * blockDim.x) {
     const bool exc = i < n_exc;
@@ -449,7 +461,8 @@ __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, 
       pre[e] = from_off + i;
       row[q] = to_off + tgt;
       w[e] = random_w ? scale * ((float)(uint32_t)(h & 0xffffffffull) * 2.3283064365386963e-10f) : scale;
-      code[e] = edge_code(delay, 0, false);
+      const uint32_t dly = sp.d_span > 1 ? sp.d_min + (uint32_t)(splitmix64(h) & 0xffffffffull) % sp.d_span : sp.d_min;
+      code[e] = edge_code((uint8_t)dly, exc ? sp.st_exc : sp.st_inh, exc && (sp.flags_exc & SG_EDGE_STDP));
     }
   }
 }
@@ -1290,23 +1303,49 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
   });
 }
 
+// Common checks and the generator parameters of the two out-degree builders.
+static OutDegreeSpec outdegree_spec(sg_net *net, uint32_t from, uint32_t to, uint64_t seed, int no_self,
+                                    uint32_t n_exc, float w_exc, float w_inh, int random_w, uint8_t d_min,
+                                    uint8_t d_max, uint8_t st_e, uint8_t st_i, uint32_t flags_e) {
+  SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
+  require_pop(net, from);
+  require_pop(net, to);
+  SG_REQUIRE(d_min <= d_max && d_max < kSlots, SG_E_INVALID, "delay range invalid (d_min <= d_max < 32)");
+  SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
+  SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
+  SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
+  OutDegreeSpec sp{};
+  sp.seed = seed;
+  sp.from_off = net->pops[from].dev_off;
+  sp.to_off = net->pops[to].dev_off;
+  sp.n_to = net->pops[to].n;
+  sp.n_exc = n_exc;
+  sp.no_self = no_self;
+  sp.random_w = random_w;
+  sp.w_exc = w_exc;
+  sp.w_inh = w_inh;
+  sp.d_min = d_min;
+  sp.d_span = (uint32_t)(d_max - d_min) + 1u;
+  sp.st_exc = st_e;
+  sp.st_inh = st_i;
+  sp.flags_exc = flags_e;
+  return sp;
+}
+
 int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k, uint64_t seed, int no_self,
-                               uint32_t n_exc, float w_exc, float w_inh, int random_w, uint8_t delay) {
+                               uint32_t n_exc, float w_exc, float w_inh, int random_w, uint8_t d_min, uint8_t d_max,
+                               uint8_t st_e, uint8_t st_i, uint32_t flags_e) {
   NET_CHECK(net);
   return run([&] {
-    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
-    require_pop(net, from);
-    require_pop(net, to);
-    SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
-    SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
-    SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
+    const OutDegreeSpec sp =
+        outdegree_spec(net, from, to, seed, no_self, n_exc, w_exc, w_inh, random_w, d_min, d_max, st_e, st_i, flags_e);
     const auto &pf = net->pops[from];
     const auto &pt = net->pops[to];
     const uint32_t m = pt.n - (no_self && pt.n ? 1u : 0u);
-    SG_REQUIRE(k <= m && k <= kMaxOutDegree, SG_E_INVALID, "out-degree larger than the candidate targets or 1024");
+    SG_REQUIRE(k <= m && k <= kMaxOutDegree, SG_E_INVALID, "out-degree larger than the candidate targets or 4096");
     const uint64_t n = (uint64_t)pf.n * k;
     if (n == 0) return;
-    net->max_delay = std::max<uint32_t>(net->max_delay, delay);
+    net->max_delay = std::max<uint32_t>(net->max_delay, d_max);
     DevGuard g(net->device);
     const size_t n0 = net->e_pre.n;
     net->e_pre.reserve(n0 + n, net->stream);
@@ -1315,9 +1354,7 @@ int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t
     net->e_code.reserve(n0 + n, net->stream);
     const unsigned blocks = (unsigned)std::min<uint64_t>((pf.n + 127) / 128, 148u * 16u);
     synth_outdegree_kernel<<<blocks, 128, 0, net->stream>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p,
-                                                             n0, pf.n, k, nullptr, nullptr, seed, pf.dev_off,
-                                                             pt.dev_off, pt.n, no_self, n_exc, w_exc, w_inh,
-                                                             random_w, delay);
+                                                             n0, pf.n, k, nullptr, nullptr, sp);
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaStreamSynchronize(net->stream));
     net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + n;
@@ -1326,17 +1363,14 @@ int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t
 
 int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, double mean, double sd,
                                    uint64_t seed, int no_self, uint32_t n_exc, float w_exc, float w_inh,
-                                   int random_w, uint8_t delay) {
+                                   int random_w, uint8_t d_min, uint8_t d_max, uint8_t st_e, uint8_t st_i,
+                                   uint32_t flags_e) {
   NET_CHECK(net);
   return run([&] {
-    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
-    require_pop(net, from);
-    require_pop(net, to);
-    SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
-    SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
     SG_REQUIRE(std::isfinite(mean) && mean > 0 && std::isfinite(sd) && sd >= 0, SG_E_INVALID,
                "lognormal degree needs mean > 0 and sd >= 0");
-    SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
+    const OutDegreeSpec sp =
+        outdegree_spec(net, from, to, seed, no_self, n_exc, w_exc, w_inh, random_w, d_min, d_max, st_e, st_i, flags_e);
     const auto &pf = net->pops[from];
     const auto &pt = net->pops[to];
     const uint32_t m = pt.n - (no_self && pt.n ? 1u : 0u);
@@ -1366,7 +1400,7 @@ int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, doub
     SG_CUDA(cudaMemcpyAsync(&total, off.p + pf.n, 8, cudaMemcpyDeviceToHost, s));
     SG_CUDA(cudaStreamSynchronize(s));
     if (total == 0) return;
-    net->max_delay = std::max<uint32_t>(net->max_delay, delay);
+    net->max_delay = std::max<uint32_t>(net->max_delay, d_max);
     const size_t n0 = net->e_pre.n;
     net->e_pre.reserve(n0 + total, s);
     net->e_post.reserve(n0 + total, s);
@@ -1374,8 +1408,7 @@ int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, doub
     net->e_code.reserve(n0 + total, s);
     const unsigned b2 = (unsigned)std::min<uint64_t>((pf.n + 127) / 128, 148u * 16u);
     synth_outdegree_kernel<<<b2, 128, 0, s>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p, n0, pf.n, 0,
-                                              deg.p, off.p, seed, pf.dev_off, pt.dev_off, pt.n, no_self, n_exc,
-                                              w_exc, w_inh, random_w, delay);
+                                              deg.p, off.p, sp);
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaStreamSynchronize(s));
     net->e_pre.n = net->e_post.n = net->e_w.n = net->e_code.n = n0 + total;

@@ -43,8 +43,8 @@ SIGNATURES = {
     "sg_connect": [vp, u32, vp, u32, vp, vp, vp, u64],
     "sg_connect_ex": [vp, u32, vp, u32, vp, vp, vp, vp, u64, u32],
     "sg_connect_fixed_indegree": [vp, u32, u32, u32, u64, u32, f32, f32, u8, u8, u8, u8, u32],
-    "sg_connect_fixed_outdegree": [vp, u32, u32, u32, u64, i32, u32, f32, f32, i32, u8],
-    "sg_connect_lognormal_outdegree": [vp, u32, u32, f64, f64, u64, i32, u32, f32, f32, i32, u8],
+    "sg_connect_fixed_outdegree": [vp, u32, u32, u32, u64, i32, u32, f32, f32, i32, u8, u8, u8, u8, u32],
+    "sg_connect_lognormal_outdegree": [vp, u32, u32, f64, f64, u64, i32, u32, f32, f32, i32, u8, u8, u8, u8, u32],
     "sg_register_expone": [vp, f32, f32, f32, vp],
     "sg_poisson_add": [vp, f32, f32, u32, vp],
     "sg_poisson_add_many": [vp, u32, f32, f32, vp, u32, vp],

@@ -105,19 +105,25 @@ class Network:
                                               d_min, d_max, syn_type_exc, syn_type_inh,
                                               EDGE_STDP if stdp_exc else 0))
 
-    def connect_fixed_outdegree(self, frm, to, k, seed, no_self, n_exc, w_exc, w_inh, random_w=True, delay=1):
+    def connect_fixed_outdegree(self, frm, to, k, seed, no_self, n_exc, w_exc, w_inh, random_w=True, delay=1,
+                                d_max=None, syn_type_exc=0, syn_type_inh=0, stdp_exc=False):
         """k distinct targets per source, generated on the device
-        (sg_connect_fixed_outdegree); weights w_exc/w_inh times U(0,1)."""
+        (sg_connect_fixed_outdegree); weights w_exc/w_inh times U(0,1);
+        delay uniform in [delay, d_max] (d_max defaults to delay)."""
         check(lib().sg_connect_fixed_outdegree(self._h, frm, to, k, seed, 1 if no_self else 0, n_exc,
-                                               float(w_exc), float(w_inh), 1 if random_w else 0, delay))
+                                               float(w_exc), float(w_inh), 1 if random_w else 0, delay,
+                                               delay if d_max is None else d_max, syn_type_exc, syn_type_inh,
+                                               EDGE_STDP if stdp_exc else 0))
 
     def connect_lognormal_outdegree(self, frm, to, mean, sd, seed, no_self, n_exc, w_exc, w_inh,
-                                    random_w=True, delay=1):
+                                    random_w=True, delay=1, d_max=None, syn_type_exc=0, syn_type_inh=0,
+                                    stdp_exc=False):
         """Lognormal out-degree per source, distinct targets, generated on the
         device (sg_connect_lognormal_outdegree)."""
         check(lib().sg_connect_lognormal_outdegree(self._h, frm, to, float(mean), float(sd), seed,
                                                    1 if no_self else 0, n_exc, float(w_exc), float(w_inh),
-                                                   1 if random_w else 0, delay))
+                                                   1 if random_w else 0, delay, delay if d_max is None else d_max,
+                                                   syn_type_exc, syn_type_inh, EDGE_STDP if stdp_exc else 0))
 
     def register_expone(self, tau_decay: float, erev: float, dt: float) -> int:
         out = C.c_uint32()

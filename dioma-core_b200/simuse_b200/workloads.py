@@ -106,6 +106,14 @@ def izhikevich_input(spec: dict, step: int) -> np.ndarray:
     return (scale * z).astype(np.float32)
 
 
+def outdegree_delays(h: np.ndarray, d_min: int, d_max: int) -> np.ndarray:
+    """Delays of the out-degree generators from each draw's hash h."""
+    span = d_max - d_min + 1
+    if span <= 1:
+        return np.full(h.shape, d_min, np.uint8)
+    return (d_min + (splitmix64(h) & np.uint64(0xFFFFFFFF)) % np.uint64(span)).astype(np.uint8)
+
+
 def fixed_outdegree_edges(n: int, k: int, seed: int, n_exc: int, w_exc: float, w_inh: float,
                           no_self: bool = True, random_w: bool = True):
     """NumPy twin of the device generator sg_connect_fixed_outdegree (same
@@ -131,6 +139,14 @@ def fixed_outdegree_edges(n: int, k: int, seed: int, n_exc: int, w_exc: float, w
         tgt = np.where(tgt >= i[:, None], tgt + np.uint64(1), tgt)
     pre = np.repeat(np.arange(n, dtype=np.uint32), k)
     return pre, tgt.astype(np.uint32).ravel(), w.ravel()
+
+
+def fixed_outdegree_delays(n: int, k: int, seed: int, d_min: int, d_max: int) -> np.ndarray:
+    """Delays the device generator draws for fixed_outdegree_edges' edges."""
+    ctr = np.arange(n * k, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        h = splitmix64(np.uint64(seed) ^ (ctr * PHI))
+    return outdegree_delays(h, d_min, d_max)
 
 
 def lognormal_degrees(n: int, mean: float, sd: float, seed: int, kmax: int) -> np.ndarray:
@@ -337,3 +353,44 @@ def kuramoto_sweep(n_inst: int = 1024, n_min: int = 256, n_max: int = 65536, k_m
     uo = np.clip(uo, 1e-12, 1.0 - 1e-12)
     omega = (gamma * np.tan(np.pi * (uo - 0.5))).astype(np.float32)
     return dict(sizes=sizes, coupling=coupling, theta=theta, omega=omega, dt=0.01, seed=seed)
+
+
+
+# ---------------------------------------------------------------------------
+# Hodgkin-Huxley network with conductance synapses and pair STDP
+# ---------------------------------------------------------------------------
+HH_STREAM_BIAS, HH_STREAM_V0 = 9, 10
+HH_PARAMS = (0.01, 1.0, 120.0, 36.0, 0.3, 50.0, -77.0, -54.4)  # dt c_m g_na g_k g_l e_na e_k e_l
+
+
+def add_hh_stdp(net, n: int = 100_000, seed: int = 3, mean_degree: float = 200.0, sd_degree: float = 80.0,
+                d_min: int = 1, d_max: int = 20, w_max: float = 0.5, model_hh: int = 4) -> int:
+    """The HH + pair-STDP network: n squid-axon HH neurons (RK4, dt 0.01 ms),
+    the first 80 % excitatory; conductance synapses with exponential decay
+    tau 5 ms (E_rev 0 mV excitatory, -80 mV inhibitory); lognormal out-degree
+    (mean 200, sd 80), distinct targets, weights U(0, w_max) (the stated
+    w_max = 0.5, taken as a raw conductance per synapse as the reference's
+    ExpOne ring does: the synchronous onset volley of 200 inputs leaves the
+    neurons shunted and silent from then on; at w_max = 0.04 they stay silent
+    for ~40 ms between population bursts; at w_max = 0.01 they fire
+    irregularly at ~60 Hz), delays uniform in d_min..d_max steps; pair STDP on excitatory synapses (tau+ = tau- =
+    20 ms, A+ 0.01, A- 0.0105, weights clipped to [0, 1]); bias current
+    N(10, 2) per neuron; v0 ~ U(-70, -60) and the gates at rest."""
+    n_exc = n * 4 // 5
+    pop = net.add_population(model_hh, n)
+    for col, v in enumerate(HH_PARAMS):
+        net.fill_param(pop, col, v)
+    idx = np.arange(n, dtype=np.uint64)
+    net.set_param(pop, 8, (10.0 + 2.0 * std_normal(seed, HH_STREAM_BIAS, idx)).astype(np.float32))
+    net.fill_param(pop, 9, 0.0)          # spike threshold (upward crossing)
+    net.set_state(pop, 0, (-70.0 + 10.0 * uniform01(seed, HH_STREAM_V0, idx)).astype(np.float32))
+    net.fill_state(pop, 1, 0.0529)
+    net.fill_state(pop, 2, 0.5961)
+    net.fill_state(pop, 3, 0.3177)
+    ke = net.register_expone(5.0, 0.0, 0.01)
+    ki = net.register_expone(5.0, -80.0, 0.01)
+    net.stdp_config(0.01, 20.0, 20.0, 0.01, 0.0105, 0.0, 1.0)
+    net.connect_lognormal_outdegree(pop, pop, mean_degree, sd_degree, seed, True, n_exc, w_max, w_max,
+                                    random_w=True, delay=d_min, d_max=d_max, syn_type_exc=ke,
+                                    syn_type_inh=ki, stdp_exc=True)
+    return pop

@@ -112,12 +112,15 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
    draw q (j = m - k + q) takes t = hi32(h) * (j + 1) >> 32, or j when t was
    drawn before, h = splitmix64(seed ^ (i*k + q)*0x9E3779B97F4A7C15); without
    self-loops t >= i maps to t + 1 (k <= 4096).  Weight w_exc for i < n_exc
-   else w_inh, times lo32(h) / 2^32 when random_w; fixed delay.  Edges are appended in
-   (source, draw) order.  This is the generator of the Izhikevich pulse
-   network recipe (100 distinct targets, weights 0.5 U / -U, delay 1). */
+   else w_inh, times lo32(h) / 2^32 when random_w; delay d_min +
+   lo32(splitmix64(h)) % (d_max - d_min + 1); synapse type st_exc / st_inh and,
+   for excitatory sources, flags_exc (SG_EDGE_STDP).  Edges are appended in
+   (source, draw) order.  The generator of the Izhikevich pulse network
+   recipe (100 distinct targets, weights 0.5 U / -U, delay 1). */
 int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t k, uint64_t seed,
                                int no_self, uint32_t n_exc, float w_exc, float w_inh, int random_w,
-                               uint8_t delay);
+                               uint8_t d_min, uint8_t d_max, uint8_t st_exc, uint8_t st_inh,
+                               uint32_t flags_exc);
 
 /* As sg_connect_fixed_outdegree with a lognormal out-degree per source:
    deg_i = round(exp(mu + sigma z_i)) clipped to [1, min(candidates, 4096)],
@@ -127,7 +130,8 @@ int sg_connect_fixed_outdegree(sg_net *net, uint32_t from, uint32_t to, uint32_t
    of the degrees). */
 int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, double mean, double sd,
                                    uint64_t seed, int no_self, uint32_t n_exc, float w_exc, float w_inh,
-                                   int random_w, uint8_t delay);
+                                   int random_w, uint8_t d_min, uint8_t d_max, uint8_t st_exc,
+                                   uint8_t st_inh, uint32_t flags_exc);
 
 /* Network::register_kinetics(SynapseKinetics::ExpOne{tau_decay, erev}, dt)
    -> profile id (1-based), core.rs:564-584; step.rs:248-345 */

@@ -193,3 +193,32 @@ def test_device_rates_and_isi_cv_match_the_raster():
     assert np.allclose(cv[has], ref[has], rtol=1e-4)
     assert np.all(cv[~has] == 0)
     net.close()
+
+
+def test_outdegree_generator_delays_types_and_stdp_flags():
+    n, k, seed = 800, 40, 5
+    net = sg.Network(0)
+    p = net.add_population(sg.HH, n)
+    ke = net.register_expone(5.0, 0.0, 0.01)
+    ki = net.register_expone(5.0, -80.0, 0.01)
+    net.stdp_config(0.01, 20.0, 20.0, 0.01, 0.0105, 0.0, 1.0)
+    net.connect_fixed_outdegree(p, p, k, seed, True, 640, 0.5, 0.5, True, 3, d_max=17,
+                                syn_type_exc=ke, syn_type_inh=ki, stdp_exc=True)
+    net.build()
+    rp, col, w, d = net.graph()
+    pre, post, _ = W.fixed_outdegree_edges(n, k, seed, 640, 0.5, 0.5)
+    dd = W.fixed_outdegree_delays(n, k, seed, 3, 17)
+    order = np.lexsort((post, pre))
+    assert np.array_equal(d, dd[order])
+    assert d.min() >= 3 and d.max() <= 17 and np.unique(d).size == 15
+    net.close()
+
+
+def test_hh_stdp_workload_builds_and_runs():
+    net = sg.Network(0)
+    W.add_hh_stdp(net, n=5000)
+    net.build()
+    net.step(500)
+    assert net.events_total > 0
+    assert net.stdp_drift != 0.0
+    net.close()
