@@ -164,6 +164,16 @@ struct sg_net {
   uint64_t stat_read_step = 0;
   uint64_t host_step = 0;  // steps issued
   size_t scatter_smem = 0;
+  // pending-event lists of the deterministic scatter (list_mode)
+  int list_mode = 0;
+  uint32_t nkeys = 0, lcap = 0;
+  uint64_t blk_src_max = 0;  // most Poisson-source synapses into one scatter block
+  std::vector<double> src_abs;  // per post, sum of |w| of its source synapses
+  int src_lo = 1 << 20;         //   smallest low-bit exponent of a source weight
+  bool src_bad = false;         //   a source weight is not finite
+  DBuf<uint16_t> d_lpost;
+  DBuf<float> d_lw;
+  DBuf<uint32_t> d_lcnt;
   // neuron work table: per population its kernel arguments, per model the
   // (population, block) pairs its launch covers
   DBuf<PopArgs> d_pop_tab;
@@ -280,6 +290,12 @@ StepArgs make_args(sg_net *net) {
   a.run_p = net->d_run_p.p;
   a.run_code = net->d_run_code.p;
   a.deterministic = net->deterministic;
+  a.list_mode = net->list_mode && net->deterministic ? 1 : 0;
+  a.nkeys = net->nkeys;
+  a.lcap = net->lcap;
+  a.lpost = net->d_lpost.p;
+  a.lw = net->d_lw.p;
+  a.lcnt = net->d_lcnt.p;
   a.stdp = net->stdp_on ? 1 : 0;
   a.x_pre = net->d_x_pre.p;
   a.x_post = net->d_x_post.p;
@@ -685,6 +701,20 @@ void build_segments(sg_net *net) {
 
 // Poisson sources: rate and seed per source; their synapses grouped by the
 // scatter block that owns the post, each group in (source, connect) order.
+// Exponent of the lowest set bit of a nonzero finite float (w = odd * 2^e).
+__host__ __device__ inline int low_exponent(uint32_t bits) {
+  int ex = (int)((bits >> 23) & 0xFFu);
+  uint32_t mant = bits & 0x7FFFFFu;
+  if (ex) mant |= 0x800000u;
+  else ex = 1;
+  int tz = 0;
+  while (!(mant & 1u)) {
+    mant >>= 1;
+    ++tz;
+  }
+  return ex - 150 + tz;
+}
+
 void build_sources(sg_net *net) {
   const size_t S = net->srcs.size();
   const uint32_t G = net->G, P = net->P;
@@ -692,15 +722,32 @@ void build_sources(sg_net *net) {
   std::vector<uint32_t> seed(S);
   std::vector<uint64_t> cnt((size_t)G + 1, 0);
   uint64_t tot = 0;
+  // the source weights' part of the exact-sum test (rings_exact)
+  net->src_abs.assign(net->Nd, 0.0);
+  net->src_lo = 1 << 20;
+  net->src_bad = false;
   for (size_t i = 0; i < S; ++i) {
     p[i] = net->srcs[i].p;
     seed[i] = net->srcs[i].seed;
     for (uint32_t q : net->srcs[i].post) cnt[q / P]++;
     tot += net->srcs[i].post.size();
+    for (size_t k = 0; k < net->srcs[i].post.size(); ++k) {
+      const float w = net->srcs[i].w[k];
+      uint32_t bits;
+      std::memcpy(&bits, &w, 4);
+      if (!std::isfinite(w)) {
+        net->src_bad = true;
+      } else if (bits & 0x7FFFFFFFu) {
+        net->src_lo = std::min(net->src_lo, low_exponent(bits));
+        net->src_abs[net->srcs[i].post[k]] += std::fabs((double)w);
+      }
+    }
   }
   SG_REQUIRE(tot < 0xFFFFFFFFull, SG_E_OVERFLOW, "too many Poisson-source synapses");
   std::vector<uint32_t> lo((size_t)G + 1, 0);
   for (uint32_t j = 0; j < G; ++j) lo[j + 1] = lo[j] + (uint32_t)cnt[j];
+  net->blk_src_max = 0;
+  for (uint32_t j = 0; j < G; ++j) net->blk_src_max = std::max<uint64_t>(net->blk_src_max, cnt[j]);
   std::vector<uint32_t> cur(lo.begin(), lo.end() - 1), se_src(tot), se_post(tot);
   std::vector<float> se_w(tot);
   std::vector<uint8_t> se_code(tot);
@@ -835,7 +882,7 @@ void split_bf16(sg_net *net) {
   const uint64_t E = net->n_edges;
   cudaStream_t s = net->stream;
   net->d_edge_x.alloc(std::max<uint64_t>(E, 1));
-  net->d_w16.alloc(std::max<uint64_t>(E, 1));
+  net->d_w16.alloc(std::max<uint64_t>(E + (E & 1), 2));  // even: the scatter reads aligned pairs
   if (E) {
     const unsigned b = (unsigned)std::min<uint64_t>((E + 255) / 256, 148u * 32u);
     split_bf16_kernel<<<b, 256, 0, s>>>(net->d_edge.p, net->d_edge_x.p, net->d_w16.p, E);
@@ -843,6 +890,138 @@ void split_bf16(sg_net *net) {
   }
   SG_CUDA(cudaStreamSynchronize(s));
   net->d_edge.release();
+}
+
+// Synapses into each scatter block's posts (the most events the block can
+// take from spiking rows in one step), summed over the segment table.
+template <class T>
+__global__ void block_indeg_kernel(const T *seg, uint32_t Nd, uint32_t G, unsigned long long *out) {
+  extern __shared__ unsigned long long hist[];
+  for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) hist[g] = 0;
+  __syncthreads();
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < Nd; i += (uint64_t)gridDim.x * blockDim.x) {
+    const T *t = seg + i * (G + 1);
+    for (uint32_t g = 0; g < G; ++g) {
+      const uint32_t l = (uint32_t)(t[g + 1] - t[g]);
+      if (l) atomicAdd(&hist[g], (unsigned long long)l);
+    }
+  }
+  __syncthreads();
+  for (uint32_t g = threadIdx.x; g < G; g += blockDim.x)
+    if (hist[g]) atomicAdd(&out[g], hist[g]);
+}
+
+// Weight scan for the exact-sum test: per post the sum of |w| over its
+// synapses (FP64), the smallest low-bit exponent of any weight, and whether
+// any weight is not finite.
+__global__ void weight_scan_kernel(const uint2 *edge, const uint32_t *edge_x, const uint16_t *w16, int bf16,
+                                   uint64_t E, uint32_t post_mask, double *sum, int *emin, int *bad) {
+  int lo = 1 << 20;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = bf16 ? edge_x[e] : edge[e].x;
+    const uint32_t bits = bf16 ? (uint32_t)w16[e] << 16 : edge[e].y;
+    const float w = __uint_as_float(bits);
+    if (!isfinite(w)) {
+      atomicOr(bad, 1);
+      continue;
+    }
+    if (bits & 0x7FFFFFFFu) {
+      lo = min(lo, low_exponent(bits));
+      atomicAdd(&sum[x & post_mask], fabs((double)w));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(emin, lo);
+}
+
+// Whether float addition on the rings is exact: every weight that reaches a
+// ring (synapses and Poisson sources) is a multiple of 2^e for the smallest
+// low-bit exponent e, and no post's weights sum in magnitude to 2^(23+e).
+// A ring cell is cleared to +0 and receives each of its post's synapses at
+// most once before it is read (a synapse reaches one slot per emission
+// step, and a slot is read before the same synapse can reach it again), so
+// every partial sum is a multiple of 2^e below 2^(23+e) in magnitude: exact.
+// Plastic synapses change their weights, so STDP rules it out.
+bool rings_exact(sg_net *net) {
+  if (net->stdp_on) return false;
+  cudaStream_t s = net->stream;
+  const uint32_t Nd = net->Nd;
+  if (net->src_bad) return false;
+  std::vector<double> psum(std::move(net->src_abs));  // recorded by build_sources
+  psum.resize(Nd, 0.0);
+  int lo = net->src_lo;
+  DBuf<double> sum;
+  sum.alloc(std::max<uint32_t>(Nd, 1));
+  SG_CUDA(cudaMemcpyAsync(sum.p, psum.data(), (size_t)Nd * 8, cudaMemcpyHostToDevice, s));
+  DBuf<int> flags;
+  flags.alloc(2);
+  const int init[2] = {1 << 20, 0};
+  SG_CUDA(cudaMemcpyAsync(flags.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  const uint64_t E = net->n_edges;
+  const int bf16 = net->weight_format == SG_W_BF16 ? 1 : 0;
+  if (E) {
+    const unsigned b = (unsigned)std::min<uint64_t>((E + 255) / 256, 148u * 16u);
+    weight_scan_kernel<<<b, 256, 0, s>>>(net->d_edge.p, net->d_edge_x.p, net->d_w16.p, bf16, E,
+                                         net->packed ? 0x00FFFFFFu : 0xFFFFFFFFu, sum.p, flags.p, flags.p + 1);
+    SG_CUDA(cudaGetLastError());
+  }
+  int h[2];
+  SG_CUDA(cudaMemcpyAsync(psum.data(), sum.p, (size_t)Nd * 8, cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaMemcpyAsync(h, flags.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  if (h[1]) return false;
+  lo = std::min(lo, h[0]);
+  double most = 0.0;
+  for (double v : psum) most = std::max(most, v);
+  if (most == 0.0) return true;
+  return most < std::ldexp(1.0, 23 + lo);
+}
+
+// Pending-event lists: used by the deterministic scatter when the ring sums
+// are exact (rings_exact), a block's posts fit its shared memory and the
+// (ring, slot) keys fit.  A list holds up to lcap events: at most 4 windows,
+// fewer when no block can take that many events in one step (every row
+// spiking, every source firing), so that a window always fits an emptied
+// list.
+void setup_lists(sg_net *net) {
+  cudaStream_t s = net->stream;
+  const size_t n_rings = 1 + net->kin.size();
+  net->nkeys = (uint32_t)(n_rings * net->nslots);
+  net->list_mode = (net->Nd > 0 && net->P <= kListPosts && net->nkeys <= kMaxKeys && net->G > 0) ? 1 : 0;
+  if (net->list_mode) net->list_mode = rings_exact(net) ? 1 : 0;
+  if (!net->list_mode) return;
+  DBuf<unsigned long long> indeg;
+  indeg.alloc(net->G);
+  indeg.zero(s);
+  const size_t hsm = (size_t)net->G * sizeof(unsigned long long);
+  const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(1184, (net->Nd + 255) / 256));
+  if (net->seg32)
+    block_indeg_kernel<uint32_t><<<blocks, 256, hsm, s>>>((const uint32_t *)net->d_seg.p, net->Nd, net->G, indeg.p);
+  else
+    block_indeg_kernel<uint16_t><<<blocks, 256, hsm, s>>>((const uint16_t *)net->d_seg.p, net->Nd, net->G, indeg.p);
+  SG_CUDA(cudaGetLastError());
+  std::vector<unsigned long long> h(net->G);
+  SG_CUDA(cudaMemcpyAsync(h.data(), indeg.p, h.size() * 8, cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  uint64_t most = 0;
+  for (auto v : h) most = std::max<uint64_t>(most, v);
+  most += net->blk_src_max;
+  net->lcap = (uint32_t)std::min<uint64_t>(4ull * kWin, std::max<uint64_t>(align_up(std::max<uint64_t>(most, 1), 256), 256));
+  const size_t n = (size_t)net->G * net->nkeys * net->lcap;
+  net->d_lpost.alloc(n);
+  net->d_lw.alloc(n);
+  net->d_lcnt.alloc((size_t)net->G * net->nkeys);
+  net->d_lcnt.zero(s);
+}
+
+// Adds every pending list to its ring cells (the rings then hold the
+// reference's ring contents exactly).
+void flush_lists(sg_net *net) {
+  if (!net->list_mode || !net->built) return;
+  StepArgs a = make_args(net);
+  a.list_mode = 1;
+  list_flush_all_kernel<<<net->G, kScatterThreads, net->scatter_smem, net->stream>>>(a);
+  SG_CUDA(cudaGetLastError());
 }
 
 void finish_build(sg_net *net) {
@@ -892,8 +1071,13 @@ void finish_build(sg_net *net) {
   net->d_stat_ev.alloc(net->stat_cap);
   net->d_stat_ev.zero(s);
   net->scatter_smem = sizeof(ScatterSmem);
-  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)net->scatter_smem));
-  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)net->scatter_smem));
+  const int sm = (int)net->scatter_smem;
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  SG_CUDA(cudaFuncSetAttribute(list_flush_all_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  setup_lists(net);
   SG_CUDA(cudaStreamSynchronize(s));
   net->built = true;
 }
@@ -972,8 +1156,13 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
   launch_neuron<kGPEA>(net, a);
   launch_neuron<kHH>(net, a);
   if (ev) SG_CUDA(cudaEventRecord(ev[1], s));
-  if (net->seg32) scatter_kernel<true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
-  else scatter_kernel<false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+  if (a.list_mode) {
+    if (net->seg32) scatter_kernel<true, true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+    else scatter_kernel<false, true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+  } else {
+    if (net->seg32) scatter_kernel<true, false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+    else scatter_kernel<false, false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+  }
   if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
 }
 
@@ -1524,9 +1713,22 @@ int sg_set_weight_format(sg_net *net, int format) {
   });
 }
 
+int sg_scatter_mode(sg_net *net, int *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = !net->deterministic ? SG_SCATTER_ATOMIC : net->list_mode ? SG_SCATTER_EXACT : SG_SCATTER_ORDERED;
+  });
+}
+
 int sg_set_deterministic(sg_net *net, int on) {
   NET_CHECK(net);
   return run([&] {
+    if (net->built && net->deterministic && !on) {  // atomic adds go straight to the ring cells
+      DevGuard g(net->device);
+      flush_lists(net);
+    }
     net->deterministic = on ? 1 : 0;
     drop_graph(net);
   });
@@ -1635,6 +1837,7 @@ int sg_ring_clear(sg_net *net) {
     DevGuard g(net->device);
     net->d_ring.zero(net->stream);
     net->d_kin_g.zero(net->stream);
+    if (net->list_mode) net->d_lcnt.zero(net->stream);
     SG_CUDA(cudaStreamSynchronize(net->stream));
   });
 }
@@ -1966,6 +2169,7 @@ int sg_ring_read(sg_net *net, uint32_t ring, float *out) {
     SG_REQUIRE(out, SG_E_INVALID, "null output");
     DevGuard g(net->device);
     const uint32_t Nd = net->Nd, M = net->nslots;
+    flush_lists(net);
     std::vector<float> r((size_t)M * Nd);
     SG_CUDA(cudaMemcpyAsync(r.data(), net->d_ring.p + (size_t)ring * M * Nd, r.size() * 4,
                             cudaMemcpyDeviceToHost, net->stream));
@@ -2098,7 +2302,7 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          (net->packed ? 0 : net->d_code.n) + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
          net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
-         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4;
+         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4;
     *out = b;
   });
 }

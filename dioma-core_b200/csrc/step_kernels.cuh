@@ -50,6 +50,11 @@ constexpr uint32_t kBlkChunk = kScatterThreads;      // spike-list slots scanned
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr unsigned long long kEmpty64 = ~0ull;
 constexpr uint32_t kMaxPops = 16;
+// pending-event lists (exact-sum mode): one per (scatter block, ring, slot);
+// a block owns at most kListPosts posts in this mode (a local post index
+// fits 16 bits)
+constexpr uint32_t kMaxKeys = 128;
+constexpr uint32_t kListPosts = 32768;
 
 // neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
 // GPEA/HH are compute heavy and keep one neuron per thread
@@ -125,6 +130,23 @@ struct StepArgs {
   const uint8_t *run_code;
   // scatter mode
   int deterministic;
+  // pending-event lists (exact-sum mode): when every weight that reaches a
+  // ring is a multiple of one power of two 2^e and no post's weights sum in
+  // magnitude to 2^(23+e), every partial sum of a ring cell is exact in
+  // FP32, so float addition on the rings is associative and any order of
+  // the adds gives the bits of the reference's order.  The scatter then
+  // appends each event to the list of (its scatter block, ring, arrival
+  // slot) = key ring * nslots + slot, and a list is added to its ring cells
+  // in shared memory before the slot is read (the block's lists of slot
+  // step + 1 at the end of every step), or earlier when it would overflow.
+  // List (j, key): lpost/lw[(j * nkeys + key) * lcap + i], local post index
+  // and weight; lcnt[j * nkeys + key] entries.
+  int list_mode;
+  uint32_t nkeys;
+  uint32_t lcap;
+  uint16_t *lpost;
+  float *lw;
+  uint32_t *lcnt;
   // pair STDP
   int stdp;
   float *x_pre;
@@ -200,6 +222,26 @@ __device__ __forceinline__ uint32_t ld_stream_u16(const uint16_t *p, unsigned lo
   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
   return v;
 }
+// Asynchronous global -> shared copies (no registers held while in flight,
+// so a thread can have all of its window's loads outstanding at once).
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, unsigned long long pol) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;" ::"r"(d), "l"(gmem), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, unsigned long long pol) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // One synapse record (x = post | code << 24, y = f32 weight bits); the bf16
 // form widens the stored weight to f32 (its upper 16 bits).
 __device__ __forceinline__ uint2 ld_record(const StepArgs &a, uint32_t e, unsigned long long pol) {
@@ -465,16 +507,35 @@ __device__ __forceinline__ uint32_t upper_index(const uint32_t *pre, uint32_t n,
   return lo;
 }
 
-struct ScatterSmem {
-  uint32_t head[kBuckets];        // latest-linked event of each bucket in the window
-  uint32_t ecell[kWin];           // window events in reference order: cell (the edge id
-                                  //   before the cell is known),
+struct WinSmem {                  // one window of events
+  uint32_t head[kBuckets];        // ring mode: latest-linked event of each bucket;
+                                  //   list mode: edge ids; spike rows while a
+                                  //   sub-chunk's segments are fetched
+  uint32_t ecell[kWin];           // window events in reference order: cell (ring mode) or
+                                  //   key << 16 | local post (list mode); the edge id
+                                  //   (ring mode) or record x word (list mode) before
   float ew[kWin];                 //   weight,
-  uint16_t enext[kWin];           //   next event of the same bucket
+  uint16_t enext[kWin];           //   ring mode: next event of the same bucket
+  uint32_t w16p[kWin];            // list mode, bf16 weights: the aligned pair holding
+                                  //   the event's weight
+};
+struct FlushSmem {                // one list being added to its ring cells
+  float acc[kListPosts];          // the block's ring cells of the list's (ring, slot)
+  uint16_t fpost[kWin];           // one window of the list: local posts
+  float fw[kWin];                 //   and weights
+};
+struct ScatterSmem {
+  union {
+    WinSmem w;
+    FlushSmem f;
+  } u;
   uint32_t plo[kPreChunk];        // absolute first edge of each row segment
   uint32_t pseg[kPreChunk + 1];   // prefix of segment lengths
   uint32_t boff[kBlkChunk + 1];   // prefix of spike-list slot counts
   uint32_t wsum[32];
+  uint32_t lcnt[kMaxKeys];        // list mode: entries in each of this block's lists
+  uint32_t wkey[kMaxKeys];        //   window events per key, then the placing cursor
+  uint32_t wstart[kMaxKeys];      //   first grouped window entry per key
   double drift;
   unsigned long long events;
 };
@@ -490,7 +551,7 @@ __device__ __forceinline__ float *cell_addr(const StepArgs &a, uint32_t cell, ui
 
 __device__ __forceinline__ void clear_heads(ScatterSmem &S) {
 #pragma unroll
-  for (uint32_t r = 0; r < kBPT; ++r) S.head[threadIdx.x + r * kScatterThreads] = kEmpty;
+  for (uint32_t r = 0; r < kBPT; ++r) S.u.w.head[threadIdx.x + r * kScatterThreads] = kEmpty;
 }
 
 // Knuth's multiplicative hash of the cell onto the buckets
@@ -500,8 +561,8 @@ constexpr uint32_t kNone16 = 0xFFFFu;
 // Prepend event k to the list of its bucket (list order is arbitrary; the
 // walk below compares event indices).
 __device__ __forceinline__ void link_event(ScatterSmem &S, uint32_t k) {
-  const uint32_t prev = atomicExch(&S.head[bucket_of(S.ecell[k])], k);
-  S.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
+  const uint32_t prev = atomicExch(&S.u.w.head[bucket_of(S.u.w.ecell[k])], k);
+  S.u.w.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
 }
 
 // Apply the window's m linked events to the ring in reference order.  Each
@@ -526,12 +587,12 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     pv[r] = kNone16;
     w[r] = 0.0f;
     if (k < m) {
-      const uint32_t c = S.ecell[k];
+      const uint32_t c = S.u.w.ecell[k];
       bool last = true;
-      uint32_t j = S.head[bucket_of(c)];
+      uint32_t j = S.u.w.head[bucket_of(c)];
       if (j == kEmpty) j = kNone16;
-      for (; j != kNone16; j = S.enext[j]) {
-        if (j == k || S.ecell[j] != c) continue;
+      for (; j != kNone16; j = S.u.w.enext[j]) {
+        if (j == k || S.u.w.ecell[j] != c) continue;
         if (j < k) {
           ++rk[r];
           if (pv[r] == kNone16 || j > pv[r]) pv[r] = j;
@@ -541,7 +602,7 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
       }
       lastm |= (last ? 1u : 0u) << r;
       maxrank = max(maxrank, rk[r]);
-      w[r] = S.ew[k];
+      w[r] = S.u.w.ew[k];
     }
   }
   // level 0: the first event of each cell adds to the loaded ring value
@@ -553,7 +614,7 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     const uint32_t k = threadIdx.x + r * kScatterThreads;
     if (k < m && rk[r] == 0) {
       v[r] = v[r] + w[r];
-      S.ew[k] = v[r];
+      S.u.w.ew[k] = v[r];
     }
   }
   // later ranks: partial sums in order, one level per round
@@ -562,8 +623,8 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     for (uint32_t r = 0; r < kEPT; ++r) {
       const uint32_t k = threadIdx.x + r * kScatterThreads;
       if (k < m && rk[r] == lvl) {
-        v[r] = S.ew[pv[r]] + w[r];
-        S.ew[k] = v[r];
+        v[r] = S.u.w.ew[pv[r]] + w[r];
+        S.u.w.ew[k] = v[r];
       }
     }
   }
@@ -571,25 +632,160 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
 #pragma unroll
   for (uint32_t r = 0; r < kEPT; ++r) {
     const uint32_t k = threadIdx.x + r * kScatterThreads;
-    if (k < m && (lastm & (1u << r))) st_ring(cell_addr(a, S.ecell[k], p0), v[r], pol);
+    if (k < m && (lastm & (1u << r))) st_ring(cell_addr(a, S.u.w.ecell[k], p0), v[r], pol);
   }
   __syncthreads();
 }
 
 // One event into the window (or straight into the ring in atomic mode).
 // `base` = step % nslots; the event lands in slot (step + max(delay, 1)) % nslots.
+template <bool LIST>
 __device__ __forceinline__ uint32_t put_event(const StepArgs &a, ScatterSmem &S, uint32_t k, uint32_t post,
                                               float w, uint8_t code, uint32_t base, uint32_t p0) {
   uint32_t slot = base + max(code_delay(code), 1u);
   if (slot >= a.nslots) slot -= a.nslots;
-  const uint32_t cell = ((code_ring(code) * a.nslots + slot) << a.pbits) | (post - p0);
+  const uint32_t key = code_ring(code) * a.nslots + slot;
+  if (LIST) {
+    S.u.w.ecell[k] = (key << 16) | (post - p0);
+    S.u.w.ew[k] = w;
+    return 0;
+  }
+  const uint32_t cell = (key << a.pbits) | (post - p0);
   if (a.deterministic) {
-    S.ecell[k] = cell;
-    S.ew[k] = w;
+    S.u.w.ecell[k] = cell;
+    S.u.w.ew[k] = w;
   } else {
     atomicAdd(cell_addr(a, cell, p0), w);
   }
   return cell;
+}
+
+// ---- pending-event lists (exact-sum mode) -----------------------------------
+// Append the window's m events (ecell/ew) to this block's lists.  The order
+// inside a list is free (the sums are exact), so the window is grouped by key
+// with shared-memory counters (count, offsets, place) into the idle head/w16p
+// arrays, and each key's run is then copied to the tail of its list with
+// coalesced stores.  Called by all threads after the barrier that publishes
+// ecell/ew; ends with a barrier.
+__device__ __forceinline__ void list_append(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t j) {
+  WinSmem &W = S.u.w;
+  const uint32_t tid = threadIdx.x, nk = a.nkeys;
+  if (tid < nk) S.wkey[tid] = 0;
+  __syncthreads();
+#pragma unroll
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t k = tid + r * kScatterThreads;
+    if (k < m) atomicAdd(&S.wkey[W.ecell[k] >> 16], 1u);
+  }
+  __syncthreads();
+  if (tid < 32) {  // window offsets of the keys (nk <= kMaxKeys = 4 * 32)
+    uint32_t c[kMaxKeys / 32], run = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kMaxKeys / 32; ++q) {
+      const uint32_t key = tid * (kMaxKeys / 32) + q;
+      c[q] = key < nk ? S.wkey[key] : 0u;
+      run += c[q];
+    }
+    uint32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (tid >= (uint32_t)o) x += y;
+    }
+    uint32_t st = x - run;
+#pragma unroll
+    for (uint32_t q = 0; q < kMaxKeys / 32; ++q) {
+      const uint32_t key = tid * (kMaxKeys / 32) + q;
+      if (key < nk) {
+        S.wstart[key] = st;
+        S.wkey[key] = st;  // the placing cursor
+      }
+      st += c[q];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t k = tid + r * kScatterThreads;
+    if (k < m) {
+      const uint32_t v = W.ecell[k];
+      const uint32_t i = atomicAdd(&S.wkey[v >> 16], 1u);
+      W.head[i] = v;
+      W.w16p[i] = __float_as_uint(W.ew[k]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t r = 0; r < kEPT; ++r) {
+    const uint32_t i = tid + r * kScatterThreads;
+    if (i < m) {
+      const uint32_t v = W.head[i], key = v >> 16;
+      const size_t off = ((size_t)j * nk + key) * a.lcap + S.lcnt[key] + (i - S.wstart[key]);
+      a.lpost[off] = (uint16_t)(v & 0xFFFFu);
+      a.lw[off] = __uint_as_float(W.w16p[i]);
+    }
+  }
+  __syncthreads();
+  if (tid < nk) S.lcnt[tid] += S.wkey[tid] - S.wstart[tid];
+  __syncthreads();
+}
+
+struct ListArgs {
+  float *ring;
+  const uint16_t *lpost;
+  const float *lw;
+  uint32_t Nd, nkeys, lcap;
+};
+__device__ __forceinline__ ListArgs list_args(const StepArgs &a) {
+  return ListArgs{a.ring, a.lpost, a.lw, a.Nd, a.nkeys, a.lcap};
+}
+
+// Add list (j, key) to its ring cells and empty it: the block's cells of the
+// key's (ring, slot) are copied to shared memory, the list is added to them
+// kWin events at a time with shared-memory atomics (exact sums: the order is
+// free), and the cells are written back.  Called by all threads with S.lcnt
+// stable; ends with a barrier.
+__device__ __noinline__ void list_flush(const ListArgs a, ScatterSmem &S, uint32_t key, uint32_t j, uint32_t p0,
+                                        uint32_t pj) {
+  FlushSmem &F = S.u.f;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t n = S.lcnt[key];
+  if (n == 0) return;
+  const unsigned long long keep = policy_evict_last(), once = policy_evict_first();
+  // the cells: pj is a multiple of 32 and the range starts 128-byte aligned
+  float *cells = a.ring + (size_t)key * a.Nd + p0;
+  for (uint32_t c = tid; c < pj / 4; c += kScatterThreads) cp_async16(&F.acc[c * 4], cells + c * 4, keep);
+  // a list starts at a multiple of 256 entries and its capacity is one, so
+  // the 16-byte copies rounded up past the last entry stay inside the list
+  const size_t lb = ((size_t)j * a.nkeys + key) * a.lcap;
+  for (uint32_t w0 = 0; w0 < n; w0 += kWin) {
+    const uint32_t fm = min(kWin, n - w0);
+    for (uint32_t c = tid; c < (fm + 7) / 8; c += kScatterThreads)
+      cp_async16(&F.fpost[c * 8], a.lpost + lb + w0 + c * 8, once);
+    for (uint32_t c = tid; c < (fm + 3) / 4; c += kScatterThreads)
+      cp_async16(&F.fw[c * 4], a.lw + lb + w0 + c * 4, once);
+    cp_async_wait_all();
+    __syncthreads();  // window (and cells) in shared memory
+#pragma unroll
+    for (uint32_t r = 0; r < kEPT; ++r) {
+      const uint32_t k = tid + r * kScatterThreads;
+      if (k < fm) atomicAdd(&F.acc[F.fpost[k]], F.fw[k]);
+    }
+    __syncthreads();  // window applied before the next one is copied in
+  }
+  for (uint32_t i = tid; i < pj; i += kScatterThreads) cells[i] = F.acc[i];
+  __syncthreads();
+  if (tid == 0) S.lcnt[key] = 0;
+  __syncthreads();
+}
+
+// Before a window of m events: flush every list that might not hold them.
+__device__ __forceinline__ void list_reserve(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t j, uint32_t p0,
+                                             uint32_t pj) {
+  const bool need = threadIdx.x < a.nkeys && S.lcnt[threadIdx.x] + m > a.lcap;
+  if (!__syncthreads_or(need)) return;
+  for (uint32_t key = 0; key < a.nkeys; ++key)
+    if (S.lcnt[key] + m > a.lcap) list_flush(list_args(a), S, key, j, p0, pj);
 }
 
 __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes) {
@@ -614,7 +810,7 @@ __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes
   }
 }
 
-template <bool SEG32>
+template <bool SEG32, bool LIST>
 __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_kernel(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
@@ -624,10 +820,13 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   const unsigned long long step = *a.step;
   const uint32_t base = (uint32_t)(step % a.nslots);
   const uint32_t G1 = a.G + 1;
+  const uint32_t pj = min(a.P, a.Nd - p0);
   if (tid == 0) {
     S.drift = 0.0;
     S.events = 0;
   }
+  if (LIST && tid < a.nkeys) S.lcnt[tid] = a.lcnt[j * a.nkeys + tid];
+  __syncthreads();
   uint32_t n_spikes = 0;
   // ---- neuron events, in spiking-neuron order ----
   for (uint32_t cb0 = 0; cb0 < a.n_blk; cb0 += kBlkChunk) {
@@ -640,25 +839,52 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     __syncthreads();
     for (uint32_t s0 = 0; s0 < spikes; s0 += kPreChunk) {
       const uint32_t pc = min(kPreChunk, spikes - s0);
-      // rows tid*kPPT .. +kPPT of this sub-chunk: segment of each for this block
+      // rows tid*kPPT .. +kPPT of this sub-chunk: their spike-list entries,
+      // then the bounds of each row's segment for this block, fetched with
+      // asynchronous copies into the (idle) window area
+      uint2 *srow = reinterpret_cast<uint2 *>(S.u.w.head);  // [kPreChunk] (pre, row start)
+      uint32_t *sseg = S.u.w.ecell;                         // [kPreChunk][2] words holding lo, hi
       uint32_t len[kPPT], mylen = 0;
+#pragma unroll
+      for (uint32_t q = 0; q < kPPT; ++q) {
+        const uint32_t i = tid * kPPT + q;
+        if (i < pc) {
+          const uint32_t r = s0 + i;
+          const uint32_t b = upper_index(S.boff, kBlkChunk, r);
+          cp_async8(&srow[i], a.spk + (size_t)(cb0 + b) * kNeuronBlock + (r - S.boff[b]));
+        }
+      }
+      cp_async_wait_all();
+#pragma unroll
+      for (uint32_t q = 0; q < kPPT; ++q) {
+        const uint32_t i = tid * kPPT + q;
+        if (i < pc) {
+          const size_t idx = (size_t)srow[i].x * G1 + j;
+          const uint32_t *words = (const uint32_t *)a.seg;
+          if (SEG32) {
+            cp_async4(&sseg[2 * i], words + idx);
+            cp_async4(&sseg[2 * i + 1], words + idx + 1);
+          } else {  // u16 entries idx, idx + 1 from the 32-bit words holding them
+            cp_async4(&sseg[2 * i], words + (idx >> 1));
+            cp_async4(&sseg[2 * i + 1], words + ((idx + 1) >> 1));
+          }
+        }
+      }
+      cp_async_wait_all();
 #pragma unroll
       for (uint32_t q = 0; q < kPPT; ++q) {
         const uint32_t i = tid * kPPT + q;
         len[q] = 0;
         if (i < pc) {
-          const uint32_t r = s0 + i;
-          const uint32_t b = upper_index(S.boff, kBlkChunk, r);
-          const uint2 e = a.spk[(size_t)(cb0 + b) * kNeuronBlock + (r - S.boff[b])];
+          const uint2 e = srow[i];
+          const size_t idx = (size_t)e.x * G1 + j;
           uint32_t lo, hi;
           if (SEG32) {
-            const uint32_t *t = (const uint32_t *)a.seg + (size_t)e.x * G1 + j;
-            lo = __ldg(t);
-            hi = __ldg(t + 1);
+            lo = sseg[2 * i];
+            hi = sseg[2 * i + 1];
           } else {
-            const uint16_t *t = (const uint16_t *)a.seg + (size_t)e.x * G1 + j;
-            lo = __ldg(t);
-            hi = __ldg(t + 1);
+            lo = (sseg[2 * i] >> ((uint32_t)(idx & 1) * 16)) & 0xFFFFu;
+            hi = (sseg[2 * i + 1] >> ((uint32_t)((idx + 1) & 1) * 16)) & 0xFFFFu;
           }
           S.plo[i] = e.y + lo;
           len[q] = hi - lo;
@@ -679,29 +905,73 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
       __syncthreads();
       for (uint32_t w0 = 0; w0 < M; w0 += kWin) {
         const uint32_t m = min(kWin, M - w0);
-        if (a.deterministic) clear_heads(S);
+        if (LIST) list_reserve(a, S, m, j, p0, pj);
+        else if (a.deterministic) clear_heads(S);
         // each spiking row writes the edge ids of its window events (rows are
         // short segments); then thread tid takes events k = tid + r*kScatterThreads
+        uint32_t *eid = LIST ? S.u.w.head : S.u.w.ecell;
 #pragma unroll
         for (uint32_t q = 0; q < kPPT; ++q) {
           const uint32_t i = tid * kPPT + q;
           if (i < pc) {
             const uint32_t g0 = max(S.pseg[i], w0), g1 = min(S.pseg[i + 1], w0 + m);
             const uint32_t d = S.plo[i] - S.pseg[i];
-            for (uint32_t g = g0; g < g1; ++g) S.ecell[g - w0] = d + g;
+            for (uint32_t g = g0; g < g1; ++g) eid[g - w0] = d + g;
           }
         }
         __syncthreads();
+        const unsigned long long spol = policy_evict_first();
+        if (LIST) {
+          // the window's records into shared memory (ecell <- x, ew <- weight;
+          // bf16: the aligned pair holding the weight into sw), all in flight
+          WinSmem &W = S.u.w;
+#pragma unroll
+          for (uint32_t r = 0; r < kEPT; ++r) {
+            const uint32_t k = tid + r * kScatterThreads;
+            if (k < m) {
+              const uint32_t e = W.head[k];
+              if (a.wbf16) {
+                cp_async4(&W.ecell[k], a.edge_x + e, spol);
+                cp_async4(&W.w16p[k], a.w16 + (e & ~1u), spol);
+              } else {
+                const uint32_t *rec = reinterpret_cast<const uint32_t *>(a.edge + e);
+                cp_async4(&W.ecell[k], rec, spol);
+                cp_async4(&W.ew[k], rec + 1, spol);
+              }
+            }
+          }
+          cp_async_wait_all();
+#pragma unroll
+          for (uint32_t r = 0; r < kEPT; ++r) {
+            const uint32_t k = tid + r * kScatterThreads;
+            if (k < m) {
+              const uint32_t e = W.head[k], x = W.ecell[k];
+              const uint32_t wb = a.wbf16 ? ((W.w16p[k] >> ((e & 1u) * 16)) & 0xFFFFu) << 16
+                                          : __float_as_uint(W.ew[k]);
+              const float w = __uint_as_float(wb);
+              const uint32_t post = x & a.post_mask;
+              const uint8_t code = a.code ? (uint8_t)ld_stream_u8(a.code + e, spol) : (uint8_t)(x >> 24);
+              put_event<true>(a, S, k, post, w, code, base, p0);
+              if (a.stdp && code_stdp(code)) {
+                // depression at a pre spike; the pushed weight is the pre-update one
+                const float w1 = fminf(fmaxf(w - a.a_minus * a.x_post[post], a.w_min), a.w_max);
+                a.edge[e].y = __float_as_uint(w1);
+                atomicAdd(&S.drift, (double)w1 - (double)w);
+              }
+            }
+          }
+          __syncthreads();
+          list_append(a, S, m, j);
+        } else {
         uint32_t ev_e[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
-          ev_e[r] = k < m ? S.ecell[k] : 0u;
+          ev_e[r] = k < m ? S.u.w.ecell[k] : 0u;
         }
         uint32_t ev_post[kEPT];
         float ev_w[kEPT];
         uint8_t ev_code[kEPT];
-        const unsigned long long spol = policy_evict_first();
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
@@ -718,7 +988,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
           const uint32_t k = tid + r * kScatterThreads;
           pre[r] = 0.0f;
           if (k < m) {
-            const uint32_t cell = put_event(a, S, k, ev_post[r], ev_w[r], ev_code[r], base, p0);
+            const uint32_t cell = put_event<false>(a, S, k, ev_post[r], ev_w[r], ev_code[r], base, p0);
             if (a.deterministic) pre[r] = ld_ring(cell_addr(a, cell, p0), policy_evict_last());
             if (a.stdp && code_stdp(ev_code[r])) {
               // depression at a pre spike; the pushed weight is the pre-update one
@@ -731,6 +1001,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
         }
         __syncthreads();
         if (a.deterministic) apply_window(a, S, m, p0, pre);
+        }
       }
     }
   }
@@ -757,43 +1028,58 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     __syncthreads();
     for (uint32_t w0 = 0; w0 < T; w0 += kWin) {
       const uint32_t mt = min(kWin, T - w0);
-      if (a.deterministic) clear_heads(S);
+      if (LIST) list_reserve(a, S, mt, j, p0, pj);
+      else if (a.deterministic) clear_heads(S);
       __syncthreads();
       // thread tid owns entries [tid*kEPT, +kEPT) of the window: roll them,
       // then an order-preserving compaction of the fired ones
       uint32_t fired = 0, e_post[kEPT];
       float e_w[kEPT];
       uint8_t e_code[kEPT];
+      // runs are few and long: find the run of the first entry by search,
+      // then walk forward, reading a run's parameters once
+      uint32_t ri = kEmpty, i = 0, post0 = 0, seed0 = 0;
+      float p = 0.0f, rw = 0.0f;
+      uint8_t rcode = 0;
+      if (tid * kEPT < mt) i = upper_index(S.pseg, rc, w0 + tid * kEPT);
 #pragma unroll
       for (uint32_t r = 0; r < kEPT; ++r) {
         const uint32_t k = tid * kEPT + r;
         if (k < mt) {
-          // runs are few and long: find the run by search (balanced)
           const uint32_t g = w0 + k;
-          const uint32_t i = upper_index(S.pseg, rc, g);
-          const uint32_t ri = rc0 + i, t = g - S.pseg[i];
-          const float p = __ldg(a.run_p + ri);
-          e_post[r] = __ldg(a.run_post0 + ri) + t;
-          e_w[r] = __ldg(a.run_w + ri);
-          e_code[r] = __ldg(a.run_code + ri);
-          if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + ri) + t, 0, step, p)) fired |= 1u << r;
+          while (g >= S.pseg[i + 1]) ++i;
+          if (rc0 + i != ri) {
+            ri = rc0 + i;
+            p = __ldg(a.run_p + ri);
+            post0 = __ldg(a.run_post0 + ri);
+            seed0 = __ldg(a.run_seed0 + ri);
+            rw = __ldg(a.run_w + ri);
+            rcode = __ldg(a.run_code + ri);
+          }
+          const uint32_t t = g - S.pseg[i];
+          e_post[r] = post0 + t;
+          e_w[r] = rw;
+          e_code[r] = rcode;
+          if (p > 0.0f && poisson_spike(seed0 + t, 0, step, p)) fired |= 1u << r;
         }
       }
       uint32_t m;
       uint32_t pos = block_excl_scan(__popc(fired), S.wsum, &m);  // all reads of the window are done
 #pragma unroll
       for (uint32_t r = 0; r < kEPT; ++r)
-        if (fired & (1u << r)) put_event(a, S, pos++, e_post[r], e_w[r], e_code[r], base, p0);
+        if (fired & (1u << r)) put_event<LIST>(a, S, pos++, e_post[r], e_w[r], e_code[r], base, p0);
       if (tid == 0) S.events += m;
       __syncthreads();
-      if (a.deterministic && m) {
+      if (LIST) {
+        if (m) list_append(a, S, m, j);
+      } else if (a.deterministic && m) {
         float pre[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
           pre[r] = 0.0f;
           if (k < m) {
-            pre[r] = ld_ring(cell_addr(a, S.ecell[k], p0), policy_evict_last());
+            pre[r] = ld_ring(cell_addr(a, S.u.w.ecell[k], p0), policy_evict_last());
             link_event(S, k);
           }
         }
@@ -824,11 +1110,30 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     }
   }
   __syncthreads();
+  if (LIST) {
+    // the next step reads slot step + 1: its lists go to the ring cells now
+    const uint32_t nxt = base + 1 == a.nslots ? 0u : base + 1;
+    for (uint32_t k = nxt; k < a.nkeys; k += a.nslots) list_flush(list_args(a), S, k, j, p0, pj);
+    if (tid < a.nkeys) a.lcnt[j * a.nkeys + tid] = S.lcnt[tid];
+  }
   if (tid == 0) {
     if (S.events) atomicAdd(a.ev_step, S.events);
     if (a.stdp && S.drift != 0.0) atomicAdd(a.drift, S.drift);
   }
   end_of_step(a, n_spikes);
+}
+
+// Every pending list of every block into its ring cells (before the rings
+// are read from the host, or the scatter mode changes).
+__global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) list_flush_all_kernel(StepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
+  const uint32_t j = blockIdx.x, p0 = j * a.P;
+  const uint32_t pj = min(a.P, a.Nd - p0);
+  if (threadIdx.x < a.nkeys) S.lcnt[threadIdx.x] = a.lcnt[j * a.nkeys + threadIdx.x];
+  __syncthreads();
+  for (uint32_t k = 0; k < a.nkeys; ++k) list_flush(list_args(a), S, k, j, p0, pj);
+  if (threadIdx.x < a.nkeys) a.lcnt[j * a.nkeys + threadIdx.x] = S.lcnt[threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------

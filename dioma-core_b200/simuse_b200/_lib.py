@@ -53,6 +53,7 @@ SIGNATURES = {
     "sg_stdp_config": [vp, f32, f32, f32, f32, f32, f32, f32],
     "sg_set_weight_format": [vp, i32],
     "sg_set_deterministic": [vp, i32],
+    "sg_scatter_mode": [vp, vp],
     "sg_build": [vp],
     "sg_build_from_csr": [vp, vp, vp, vp, vp],
     "sg_pop_set_noise": [vp, u32, u64, u32, u64, u64, f64, f64, u32],

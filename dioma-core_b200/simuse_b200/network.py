@@ -158,6 +158,13 @@ class Network:
     def set_weight_format(self, fmt: int):
         check(lib().sg_set_weight_format(self._h, fmt))
 
+    @property
+    def scatter_mode(self) -> str:
+        """"ordered", "exact" or "atomic": the scatter path of the built network."""
+        m = C.c_int()
+        check(lib().sg_scatter_mode(self._h, C.byref(m)))
+        return ("ordered", "exact", "atomic")[m.value]
+
     def set_deterministic(self, on: bool):
         check(lib().sg_set_deterministic(self._h, 1 if on else 0))
 

@@ -71,7 +71,15 @@ def estimate_footprint(req: Request) -> int:
     e = int(n * req.mean_degree * 1.05)
     per_neuron = 32 * 4 + 16 * 4 + 8 + 148 * 2 + 64   # rings (<= 32 slots), state+params, spike list, segments
     build_peak = e * 45                                # staged edges + radix-sort double buffers + records
-    return int(nd * per_neuron + build_peak + (64 << 20))
+    # pending-event lists of the scatter: per block and ring slot, room for
+    # the block's heaviest step (bounded generously) up to 4 windows of 8192
+    g = max(1, min(148, nd // 32))
+    p = -(-(-(-nd // g)) // 32) * 32
+    g = -(-nd // p)
+    slots = 3 if req.kind == "lif" else 2
+    lcap = min(4 * 8192, -(-int(p * req.mean_degree * 4 + p) // 256) * 256)
+    lists = g * slots * (lcap * 6 + 4)
+    return int(nd * per_neuron + build_peak + lists + (64 << 20))
 
 
 def build_request(req: Request, device: int = 0) -> Network:

@@ -161,6 +161,19 @@ int sg_set_weight_format(sg_net *net, int format);
 /* Scatter mode: 1 = deterministic (reference summation order, default),
    0 = atomic accumulation (tolerance mode, order not fixed). */
 int sg_set_deterministic(sg_net *net, int on);
+/* The scatter path a built network uses (no reference counterpart; the
+   reference has one sequential push, P/api/net/push.rs:143-172):
+   SG_SCATTER_ORDERED  ring cells updated in the reference's order;
+   SG_SCATTER_EXACT    the ring sums are exact in FP32 (every weight a
+                       multiple of one power of two 2^e, every post's weights
+                       summing in magnitude below 2^(23+e), no STDP), so the
+                       events go through per-slot lists and are added in any
+                       order: the same bits;
+   SG_SCATTER_ATOMIC   atomic adds in any order (sg_set_deterministic(0)). */
+#define SG_SCATTER_ORDERED 0
+#define SG_SCATTER_EXACT 1
+#define SG_SCATTER_ATOMIC 2
+int sg_scatter_mode(sg_net *net, int *out);
 
 /* Network::build(), build.rs:18-109 (a second call is SG_E_STATE) */
 int sg_build(sg_net *net);
