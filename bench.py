@@ -105,7 +105,16 @@ def workload(args, rank=0):
     return spec, name
 
 
-def config(args, name, spec):
+SCATTER_TEXT = {
+    "exact": "exact-sum lists: the ring weights (20, -100, Poisson 100) are integers and no post's weights sum past "
+             "2^23, so every FP32 partial sum is exact; the per-slot event lists are added in any order and give "
+             "the reference's bits",
+    "ordered": "ordered ring cells (reference summation order)",
+    "atomic": "atomic adds (order not fixed)",
+}
+
+
+def config(args, name, spec, scatter_path="ordered"):
     return {
         "workload": name,
         "neurons": spec["n"],
@@ -113,7 +122,8 @@ def config(args, name, spec):
         "dt_ms": spec["dt"],
         "sim_steps_per_bench_step": args.sim_steps,
         "external_drive": {"rate_hz": spec["ext_rate_hz"], "ring_weight": spec["ext_weight"]},
-        "weights": args.weights, "scatter": "deterministic (reference summation order)",
+        "weights": args.weights,
+        "scatter": SCATTER_TEXT[scatter_path],
         "l2": "inputs larger than L2: 8 GB of synapse records and "
               f"{(21 * spec['n'] * 4) / 1e6:.0f} MB of delay rings (21 slots for delays up to 20) against a "
               "126 MB L2; each step reads the spiking rows",
@@ -366,6 +376,7 @@ def run_ours(args):
     W.build_lif(net, spec)
     net.build()
     net.synchronize()
+    scatter_path = net.scatter_mode
     stream = torch.cuda.ExternalStream(net.stream, device=local)
 
     def barrier():
@@ -451,7 +462,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": config(args, name, spec),
+        "config": config(args, name, spec, scatter_path),
         "sim": {"ms_per_sim_step": step_ms, "events_per_sim_step": events / (args.steps * S),
                 "spikes_per_sim_step": mean_spk, "rate_hz": mean_spk / spec["n"] / (spec["dt"] * 1e-3),
                 "neuron_updates_per_s": spec["n"] * args.steps * S / (ms / 1e3) * world,
