@@ -828,6 +828,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   if (LIST && tid < a.nkeys) S.lcnt[tid] = a.lcnt[j * a.nkeys + tid];
   __syncthreads();
   uint32_t n_spikes = 0;
+  double drift = 0.0;  // this thread's part of the step's STDP weight change
   // ---- neuron events, in spiking-neuron order ----
   for (uint32_t cb0 = 0; cb0 < a.n_blk; cb0 += kBlkChunk) {
     const uint32_t c = (cb0 + tid < a.n_blk) ? a.blk_cnt[cb0 + tid] : 0u;
@@ -956,7 +957,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
                 // depression at a pre spike; the pushed weight is the pre-update one
                 const float w1 = fminf(fmaxf(w - a.a_minus * a.x_post[post], a.w_min), a.w_max);
                 a.edge[e].y = __float_as_uint(w1);
-                atomicAdd(&S.drift, (double)w1 - (double)w);
+                drift += (double)w1 - (double)w;
               }
             }
           }
@@ -994,7 +995,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
               // depression at a pre spike; the pushed weight is the pre-update one
               const float w1 = fminf(fmaxf(ev_w[r] - a.a_minus * a.x_post[ev_post[r]], a.w_min), a.w_max);
               a.edge[ev_e[r]].y = __float_as_uint(w1);
-              atomicAdd(&S.drift, (double)w1 - (double)ev_w[r]);
+              drift += (double)w1 - (double)ev_w[r];
             }
             if (a.deterministic) link_event(S, k);
           }
@@ -1090,24 +1091,29 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     __syncthreads();
   }
   // ---- pair-STDP potentiation on the plastic in-edges of spiking posts ----
+  // warp w takes the spiking posts of the block's words w, w + 32, ...; its
+  // lanes share each post's in-edges (every edge belongs to one post, so the
+  // updates are independent)
   if (a.stdp) {
     __syncthreads();
-    const uint32_t p1 = min(p0 + a.P, a.Nd);
-    for (uint32_t wd = p0 / 32 + tid; wd < p1 / 32; wd += kScatterThreads) {
+    const uint32_t p1 = min(p0 + a.P, a.Nd), lane = lane_id();
+    for (uint32_t wd = p0 / 32 + (tid >> 5); wd < p1 / 32; wd += kScatterThreads / 32) {
       uint32_t bits = a.last_bits[wd];
       while (bits) {
         const uint32_t b = __ffs(bits) - 1;
         bits &= bits - 1;
         const uint32_t q = wd * 32 + b;
-        for (uint32_t k = a.in_ptr[q]; k < a.in_ptr[q + 1]; ++k) {
+        for (uint32_t k = a.in_ptr[q] + lane; k < a.in_ptr[q + 1]; k += 32) {
           const uint32_t e = a.in_edge[k];
           const float w0 = __uint_as_float(a.edge[e].y);
           const float w1 = fminf(fmaxf(w0 + a.a_plus * a.x_pre[a.in_pre[k]], a.w_min), a.w_max);
           a.edge[e].y = __float_as_uint(w1);
-          atomicAdd(&S.drift, (double)w1 - (double)w0);
+          drift += (double)w1 - (double)w0;
         }
       }
     }
+    for (int o = 16; o > 0; o >>= 1) drift += __shfl_xor_sync(0xffffffffu, drift, o);
+    if (lane == 0 && drift != 0.0) atomicAdd(&S.drift, drift);
   }
   __syncthreads();
   if (LIST) {
