@@ -24,6 +24,7 @@
 // tree over the warps), so results are reproducible run to run and an
 // instance gives the same bits alone or in any batch.  Instances are binned
 // by CTA shape, one launch per bin, on the handle's stream.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -361,8 +362,13 @@ int sg_kuramoto_create(sg_kura **out, int device, uint32_t n_inst, const uint32_
     kb->n_inst = n_inst;
     kb->total = total;
     kb->dt = dt;
+    // largest instances first in each bin: the CTAs are handed to the SMs
+    // in block order, so the long ones start at once and the short ones
+    // fill the SMs as they free up (longest-processing-time-first)
     std::vector<uint32_t> order;
     for (int b = 0; b < kKBins; ++b) {
+      std::stable_sort(bins[b].begin(), bins[b].end(),
+                       [&](uint32_t x, uint32_t y) { return sizes[x] > sizes[y]; });
       kb->bin_off[b] = (uint32_t)order.size();
       kb->bin_count[b] = (uint32_t)bins[b].size();
       order.insert(order.end(), bins[b].begin(), bins[b].end());
