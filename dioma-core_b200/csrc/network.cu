@@ -47,6 +47,12 @@ template <typename T> struct DBuf {
   void zero(cudaStream_t s) {
     if (p) SG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
   }
+  // at least `count` elements, keeping the buffer when it is large enough
+  // (grown by a quarter beyond the request when it is not)
+  void ensure(size_t count) {
+    if (count <= n) return;
+    alloc(count + count / 4);
+  }
 };
 
 // growable device array for staged edges
@@ -174,6 +180,10 @@ struct sg_net {
   DBuf<uint16_t> d_lpost;
   DBuf<float> d_lw;
   DBuf<uint32_t> d_lcnt;
+  // raster readback work buffers, kept from call to call (grow only)
+  DBuf<unsigned long long> rr_cnt, rr_off;
+  DBuf<uint8_t> rr_temp;
+  DBuf<uint32_t> rr_step, rr_idx, rr_pd, rr_pg;
   // neuron work table: per population its kernel arguments, per model the
   // (population, block) pairs its launch covers
   DBuf<PopArgs> d_pop_tab;
@@ -1977,16 +1987,19 @@ int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t 
       net->raster_read_step = net->host_step;
       return;
     }
-    DBuf<unsigned long long> cnt, off;
-    cnt.alloc(nb + 1);
-    off.alloc(nb + 1);
-    cnt.zero(s);
+    // work buffers live in the network and only grow: no allocation in a
+    // steady read loop
+    auto &cnt = net->rr_cnt;
+    auto &off = net->rr_off;
+    cnt.ensure(nb + 1);
+    off.ensure(nb + 1);
+    SG_CUDA(cudaMemsetAsync(cnt.p, 0, (nb + 1) * sizeof(unsigned long long), s));
     raster_count_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, net->raster_read_step, nw,
                                                      cnt.p);
     size_t tb = 0;
     SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, off.p, (int64_t)nb + 1, s));
-    DBuf<uint8_t> temp;
-    temp.alloc(std::max<size_t>(tb, 1));
+    auto &temp = net->rr_temp;
+    temp.ensure(std::max<size_t>(tb, 1));
     SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, off.p, (int64_t)nb + 1, s));
     unsigned long long total = 0;
     SG_CUDA(cudaMemcpyAsync(&total, off.p + nb, 8, cudaMemcpyDeviceToHost, s));
@@ -2002,13 +2015,16 @@ int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t 
       pd.push_back(net->pops[p].dev_off);
       pgl.push_back(net->offsets[p]);
     }
-    DBuf<uint32_t> d_pd, d_pg, o_step, o_idx;
-    d_pd.alloc(pd.size());
-    d_pg.alloc(pgl.size());
+    auto &d_pd = net->rr_pd;
+    auto &d_pg = net->rr_pg;
+    auto &o_step = net->rr_step;
+    auto &o_idx = net->rr_idx;
+    d_pd.ensure(pd.size());
+    d_pg.ensure(pgl.size());
     SG_CUDA(cudaMemcpyAsync(d_pd.p, pd.data(), pd.size() * 4, cudaMemcpyHostToDevice, s));
     SG_CUDA(cudaMemcpyAsync(d_pg.p, pgl.data(), pgl.size() * 4, cudaMemcpyHostToDevice, s));
-    o_step.alloc(total);
-    o_idx.alloc(total);
+    o_step.ensure(total);
+    o_idx.ensure(total);
     raster_write_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, net->raster_read_step, nw,
                                                      off.p, d_pd.p, d_pg.p, (int)pd.size(), o_step.p, o_idx.p);
     SG_CUDA(cudaGetLastError());
@@ -2302,7 +2318,8 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          (net->packed ? 0 : net->d_code.n) + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
          net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
-         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4;
+         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4 +
+         (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4;
     *out = b;
   });
 }
