@@ -369,8 +369,8 @@ __global__ void seg_table_kernel(const uint32_t *row_ptr, const uint2 *edge, int
     for (uint32_t j = 0; j < G; ++j) {
       const uint32_t bound = j * P;
       uint32_t hi = end;
-      while (lo < hi) {  // lower_bound of bound in [lo, end)
-        const uint32_t mid = (lo + hi) >> 1;
+      while (lo < hi) {  // lower_bound of bound in [lo, end); no overflow past 2^31 edges
+        const uint32_t mid = lo + ((hi - lo) >> 1);
         if (edge_post(edge[mid], packed) < bound) lo = mid + 1;
         else hi = mid;
       }
@@ -383,14 +383,20 @@ __global__ void iota_kernel(uint32_t *v, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     v[i] = (uint32_t)i;
 }
+// Records in CSR order: edge i is staged edge perm[i] (perm null: edge i).
 __global__ void gather_edges_kernel(const uint32_t *perm, const uint32_t *post_in, const float *w_in,
                                     const uint8_t *code_in, uint2 *edge, uint8_t *code, int packed, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t j = perm[i];
+    const uint64_t j = perm ? perm[i] : i;
     const uint8_t c = code_in[j];
     edge[i] = make_uint2(packed ? (post_in[j] | ((uint32_t)c << 24)) : post_in[j], __float_as_uint(w_in[j]));
     if (!packed) code[i] = c;
   }
+}
+// Whether the staged edges are already in CSR order, (pre, post) ascending.
+__global__ void sorted_check_kernel(const uint32_t *pre, const uint32_t *post, uint64_t n, int *unsorted) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (pre[i] > pre[i + 1] || (pre[i] == pre[i + 1] && post[i] > post[i + 1])) *unsorted = 1;
 }
 __global__ void histogram_kernel(const uint32_t *keys, uint64_t n, uint32_t shift, unsigned long long *cnt) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -489,6 +495,27 @@ __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, 
       w[e] = random_w ? scale * ((float)(uint32_t)(h & 0xffffffffull) * 2.3283064365386963e-10f) : scale;
       const uint32_t dly = sp.d_span > 1 ? sp.d_min + (uint32_t)(splitmix64(h) & 0xffffffffull) % sp.d_span : sp.d_min;
       code[e] = edge_code((uint8_t)dly, exc ? sp.st_exc : sp.st_inh, exc && (sp.flags_exc & SG_EDGE_STDP));
+    }
+    // the row sorted by target (shell sort; the targets are distinct), so
+    // that generated edges arrive in CSR order and the build needs no sort
+    float *rw = w + base + first;
+    uint8_t *rc = code + base + first;
+    const uint32_t gaps[] = {701, 301, 132, 57, 23, 10, 4, 1};
+    for (uint32_t gap : gaps) {
+      for (uint32_t a = gap; a < k; ++a) {
+        const uint32_t tp = row[a];
+        const float tw = rw[a];
+        const uint8_t tc = rc[a];
+        uint32_t b = a;
+        for (; b >= gap && row[b - gap] > tp; b -= gap) {
+          row[b] = row[b - gap];
+          rw[b] = rw[b - gap];
+          rc[b] = rc[b - gap];
+        }
+        row[b] = tp;
+        rw[b] = tw;
+        rc[b] = tc;
+      }
     }
   }
 }
@@ -627,7 +654,23 @@ void build_graph(sg_net *net) {
   DBuf<unsigned long long> cnt;
   cnt.alloc((size_t)Nd + 1);
   cnt.zero(s);
-  if (E > 0) {
+  int unsorted = 1;
+  if (E > 0) {  // edges staged in CSR order already (device generators, sources in order) need no sort
+    DBuf<int> flag;
+    flag.alloc(1);
+    flag.zero(s);
+    launch_grid(E, [&](unsigned b) { sorted_check_kernel<<<b, 256, 0, s>>>(net->e_pre.p, net->e_post.p, E, flag.p); });
+    SG_CUDA(cudaMemcpyAsync(&unsorted, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+  }
+  if (E > 0 && !unsorted) {
+    launch_grid(E, [&](unsigned b) {
+      gather_edges_kernel<<<b, 256, 0, s>>>(nullptr, net->e_post.p, net->e_w.p, net->e_code.p, net->d_edge.p,
+                                            net->d_code.p, net->packed, E);
+    });
+    launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->e_pre.p, E, 0, cnt.p); });
+    SG_CUDA(cudaStreamSynchronize(s));
+  } else if (E > 0) {
     DBuf<unsigned long long> keys_in, keys_out;
     DBuf<uint32_t> vals_in, vals_out;
     keys_in.alloc(E);
