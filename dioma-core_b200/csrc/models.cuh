@@ -288,6 +288,40 @@ __device__ __forceinline__ bool poisson_spike(uint32_t seed, uint32_t stream, ui
   return u < p;
 }
 
+// ---- Tsodyks-Markram short-term plasticity (P/api/net/push.rs:25-102) ----
+// f32 powi as the reference's Rust lowers it for a run-time exponent (the
+// compiler runtime's square-and-multiply from the exponent's lowest bit,
+// product starting at 1), so that the recovery factors round identically.
+__host__ __device__ __forceinline__ float tm_powi(float a, int b) {
+  const bool recip = b < 0;
+  unsigned e = recip ? 0u - (unsigned)b : (unsigned)b;
+  float r = 1.0f;
+  while (true) {
+    if (e & 1u) r *= a;
+    e >>= 1;
+    if (e == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0f / r : r;
+}
+// One spike on one synapse (tm_spike, push.rs:50-81): R and U relax over the
+// steps since the last spike, the delivered weight is w * R * U with the
+// pre-spike values, then R is depleted and U facilitated.
+__host__ __device__ __forceinline__ float tm_spike(float u0, float a_rec, float a_fac, bool fac, float &r,
+                                                   float &u, uint32_t &last, float w, unsigned long long step) {
+  const unsigned long long el = step > last ? step - last : 0ull;
+  const int n = (int)(el < 1000000ull ? el : 1000000ull);
+  if (n > 0) {
+    r = 1.0f + (r - 1.0f) * tm_powi(a_rec, n);
+    if (fac) u = u0 + (u - u0) * tm_powi(a_fac, n);
+  }
+  last = (uint32_t)step;
+  const float scale = r * u;
+  r *= 1.0f - u;
+  if (fac) u += u0 * (1.0f - u);
+  return w * scale;
+}
+
 __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ull;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;

@@ -105,6 +105,12 @@ struct Kin {
   float a_decay, erev;
 };
 
+// Tsodyks-Markram profile constants for the network's dt (push.rs:25-35)
+struct TmHost {
+  float u0, a_rec, a_fac;
+  bool fac;
+};
+
 }  // namespace sg
 
 using namespace sg;
@@ -180,6 +186,15 @@ struct sg_net {
   DBuf<uint16_t> d_lpost;
   DBuf<float> d_lw;
   DBuf<uint32_t> d_lcnt;
+  // short-term plasticity: profiles, staged per-edge ids (kept only once an
+  // edge has a profile; zero-filled for the edges staged without one), and
+  // after build the ids and R, U, last-spike state in CSR order
+  std::vector<TmHost> tm_prof;
+  DVec<uint8_t> e_pt;
+  bool tm_edges = false;
+  DBuf<uint8_t> d_pt;
+  DBuf<float> d_tm_r, d_tm_u;
+  DBuf<uint32_t> d_tm_last;
   // raster readback work buffers, kept from call to call (grow only)
   DBuf<unsigned long long> rr_cnt, rr_off;
   DBuf<uint8_t> rr_temp;
@@ -306,6 +321,18 @@ StepArgs make_args(sg_net *net) {
   a.lpost = net->d_lpost.p;
   a.lw = net->d_lw.p;
   a.lcnt = net->d_lcnt.p;
+  a.tm = net->tm_edges ? 1 : 0;
+  a.tm_pt = net->d_pt.p;
+  a.tm_r = net->d_tm_r.p;
+  a.tm_u = net->d_tm_u.p;
+  a.tm_last = net->d_tm_last.p;
+  a.tm_fac = 0;
+  for (size_t k = 0; k < net->tm_prof.size() && k < kMaxTm; ++k) {
+    a.tm_u0[k] = net->tm_prof[k].u0;
+    a.tm_arec[k] = net->tm_prof[k].a_rec;
+    a.tm_afac[k] = net->tm_prof[k].a_fac;
+    if (net->tm_prof[k].fac) a.tm_fac |= 1u << k;
+  }
   a.stdp = net->stdp_on ? 1 : 0;
   a.x_pre = net->d_x_pre.p;
   a.x_post = net->d_x_post.p;
@@ -392,6 +419,10 @@ __global__ void gather_edges_kernel(const uint32_t *perm, const uint32_t *post_i
     edge[i] = make_uint2(packed ? (post_in[j] | ((uint32_t)c << 24)) : post_in[j], __float_as_uint(w_in[j]));
     if (!packed) code[i] = c;
   }
+}
+__global__ void gather_u8_kernel(const uint32_t *perm, const uint8_t *in, uint8_t *out, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[perm ? perm[i] : i];
 }
 // Whether the staged edges are already in CSR order, (pre, post) ascending.
 __global__ void sorted_check_kernel(const uint32_t *pre, const uint32_t *post, uint64_t n, int *unsorted) {
@@ -623,9 +654,25 @@ template <typename F> void launch_grid(uint64_t n, F f) {
   f((unsigned)blocks);
 }
 
+// Profile ids of the staged edges up to `upto` (zero for the edges staged
+// without one), once any edge carries a profile.
+void fill_staged_pt(sg_net *net, uint64_t upto) {
+  if (!net->tm_edges || net->e_pt.n >= upto) return;
+  net->e_pt.reserve(upto, net->stream);
+  SG_CUDA(cudaMemsetAsync(net->e_pt.p + net->e_pt.n, 0, upto - net->e_pt.n, net->stream));
+  net->e_pt.n = upto;
+}
+
 void upload_staged_edges(sg_net *net, const uint32_t *pre, const uint32_t *post, const float *w,
-                         const uint8_t *code, uint64_t n) {
+                         const uint8_t *code, uint64_t n, const uint8_t *pt = nullptr) {
   const size_t n0 = net->e_pre.n;
+  if (pt) {
+    net->tm_edges = true;
+    fill_staged_pt(net, n0);
+    net->e_pt.reserve(n0 + n, net->stream);
+    SG_CUDA(cudaMemcpyAsync(net->e_pt.p + n0, pt, n, cudaMemcpyHostToDevice, net->stream));
+    net->e_pt.n = n0 + n;
+  }
   net->e_pre.reserve(n0 + n, net->stream);
   net->e_post.reserve(n0 + n, net->stream);
   net->e_w.reserve(n0 + n, net->stream);
@@ -663,11 +710,17 @@ void build_graph(sg_net *net) {
     SG_CUDA(cudaMemcpyAsync(&unsorted, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SG_CUDA(cudaStreamSynchronize(s));
   }
+  if (net->tm_edges) {
+    fill_staged_pt(net, E);
+    net->d_pt.alloc(std::max<uint64_t>(E, 1));
+  }
   if (E > 0 && !unsorted) {
     launch_grid(E, [&](unsigned b) {
       gather_edges_kernel<<<b, 256, 0, s>>>(nullptr, net->e_post.p, net->e_w.p, net->e_code.p, net->d_edge.p,
                                             net->d_code.p, net->packed, E);
     });
+    if (net->tm_edges)
+      launch_grid(E, [&](unsigned b) { gather_u8_kernel<<<b, 256, 0, s>>>(nullptr, net->e_pt.p, net->d_pt.p, E); });
     launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->e_pre.p, E, 0, cnt.p); });
     SG_CUDA(cudaStreamSynchronize(s));
   } else if (E > 0) {
@@ -697,6 +750,8 @@ void build_graph(sg_net *net) {
       gather_edges_kernel<<<b, 256, 0, s>>>(vals_out.p, net->e_post.p, net->e_w.p, net->e_code.p,
                                             net->d_edge.p, net->d_code.p, net->packed, E);
     });
+    if (net->tm_edges)
+      launch_grid(E, [&](unsigned b) { gather_u8_kernel<<<b, 256, 0, s>>>(vals_out.p, net->e_pt.p, net->d_pt.p, E); });
     launch_grid(E, [&](unsigned b) { histogram_kernel<<<b, 256, 0, s>>>(net->e_pre.p, E, 0, cnt.p); });
     SG_CUDA(cudaStreamSynchronize(s));
   }
@@ -704,6 +759,7 @@ void build_graph(sg_net *net) {
   net->e_post.release();
   net->e_w.release();
   net->e_code.release();
+  net->e_pt.release();
   // exclusive scan in u64 -> u32 row_ptr
   DBuf<unsigned long long> rp64;
   rp64.alloc((size_t)Nd + 1);
@@ -945,6 +1001,13 @@ void split_bf16(sg_net *net) {
   net->d_edge.release();
 }
 
+__global__ void tm_init_kernel(const uint8_t *pt, const float *u0, float *r, float *u, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    r[i] = 1.0f;
+    u[i] = pt[i] ? u0[pt[i] - 1] : 0.0f;
+  }
+}
+
 // Synapses into each scatter block's posts (the most events the block can
 // take from spiking rows in one step), summed over the segment table.
 template <class T>
@@ -996,7 +1059,7 @@ __global__ void weight_scan_kernel(const uint2 *edge, const uint32_t *edge_x, co
 // every partial sum is a multiple of 2^e below 2^(23+e) in magnitude: exact.
 // Plastic synapses change their weights, so STDP rules it out.
 bool rings_exact(sg_net *net) {
-  if (net->stdp_on) return false;
+  if (net->stdp_on || net->tm_edges) return false;  // weights change, or are scaled by R*U
   cudaStream_t s = net->stream;
   const uint32_t Nd = net->Nd;
   if (net->src_bad) return false;
@@ -1131,6 +1194,21 @@ void finish_build(sg_net *net) {
   SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   SG_CUDA(cudaFuncSetAttribute(list_flush_all_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   setup_lists(net);
+  if (net->tm_edges) {  // build.rs:69-84: R = 1, U = U0 of the edge's profile, last = 0
+    const uint64_t E = std::max<uint64_t>(net->n_edges, 1);
+    net->d_tm_r.alloc(E);
+    net->d_tm_u.alloc(E);
+    net->d_tm_last.alloc(E);
+    net->d_tm_last.zero(s);
+    float u0[kMaxTm] = {};
+    for (size_t k = 0; k < net->tm_prof.size(); ++k) u0[k] = net->tm_prof[k].u0;
+    DBuf<float> d_u0;
+    d_u0.alloc(kMaxTm);
+    SG_CUDA(cudaMemcpyAsync(d_u0.p, u0, sizeof(u0), cudaMemcpyHostToDevice, s));
+    launch_grid(E, [&](unsigned b) { tm_init_kernel<<<b, 256, 0, s>>>(net->d_pt.p, d_u0.p, net->d_tm_r.p, net->d_tm_u.p, E); });
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaStreamSynchronize(s));
+  }
   SG_CUDA(cudaStreamSynchronize(s));
   net->built = true;
 }
@@ -1476,8 +1554,9 @@ int sg_pop_get_param(sg_net *net, uint32_t pop, uint32_t col, float *out, uint32
   return pop_read(net, pop, col, true, out, n);
 }
 
-int sg_connect_ex(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, const uint32_t *ti,
-                  const float *w, const uint8_t *d, const uint8_t *st, uint64_t n, uint32_t flags) {
+static int connect_impl(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, const uint32_t *ti,
+                        const float *w, const uint8_t *d, const uint8_t *st, const uint8_t *ptype, uint64_t n,
+                        uint32_t flags) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
@@ -1497,12 +1576,44 @@ int sg_connect_ex(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, c
       net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
       const uint8_t s = st ? st[i] : 0;
       SG_REQUIRE(s <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
+      if (ptype)
+        SG_REQUIRE(ptype[i] <= net->tm_prof.size(), SG_E_INVALID,
+                   "Network::build: plast_type " + std::to_string(ptype[i]) + " exceeds registered plasticity profiles");
       pre[i] = pf.dev_off + fi[i];
       post[i] = pt.dev_off + ti[i];
       code[i] = edge_code(d[i], s, (flags & SG_EDGE_STDP) != 0);
     }
     DevGuard g(net->device);
-    upload_staged_edges(net, pre.data(), post.data(), w, code.data(), n);
+    upload_staged_edges(net, pre.data(), post.data(), w, code.data(), n, ptype);
+  });
+}
+
+int sg_connect_ex(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, const uint32_t *ti,
+                  const float *w, const uint8_t *d, const uint8_t *st, uint64_t n, uint32_t flags) {
+  return connect_impl(net, from, fi, to, ti, w, d, st, nullptr, n, flags);
+}
+
+int sg_connect_plastic(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t to, const uint32_t *ti,
+                       const float *w, const uint8_t *d, const uint8_t *st, const uint8_t *pt, uint64_t n,
+                       uint32_t flags) {
+  return connect_impl(net, from, fi, to, ti, w, d, st, pt, n, flags);
+}
+
+int sg_register_plasticity(sg_net *net, float u0, float tau_rec, int facilitation, float tau_fac, float dt,
+                           uint32_t *out_id) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "register_plasticity must be called before build()");
+    SG_REQUIRE(std::isfinite(dt) && dt > 0, SG_E_INVALID, "register_plasticity: dt must be finite and > 0");
+    SG_REQUIRE(std::isfinite(u0) && u0 > 0.0f && u0 <= 1.0f, SG_E_INVALID, "init_release_prob must be in (0, 1]");
+    SG_REQUIRE(std::isfinite(tau_rec) && tau_rec > 0.0f, SG_E_INVALID, "tau_rec must be finite and > 0");
+    SG_REQUIRE(!facilitation || (std::isfinite(tau_fac) && tau_fac > 0.0f), SG_E_INVALID,
+               "tau_fac must be finite and > 0");
+    SG_REQUIRE(net->tm_prof.size() < kMaxTm, SG_E_INVALID,
+               "at most " + std::to_string(kMaxTm) + " plasticity profiles are supported on the device path");
+    net->tm_prof.push_back(TmHost{u0, std::exp(-dt / tau_rec), facilitation ? std::exp(-dt / tau_fac) : 0.0f,
+                                  facilitation != 0});
+    if (out_id) *out_id = (uint32_t)net->tm_prof.size();
   });
 }
 
@@ -2362,7 +2473,8 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
          (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4 +
-         (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4;
+         (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4 +
+         net->d_pt.n + (net->d_tm_r.n + net->d_tm_u.n + net->d_tm_last.n) * 4;
     *out = b;
   });
 }

@@ -54,6 +54,7 @@ constexpr uint32_t kMaxPops = 16;
 // a block owns at most kListPosts posts in this mode (a local post index
 // fits 16 bits)
 constexpr uint32_t kMaxKeys = 128;
+constexpr uint32_t kMaxTm = 8;  // short-term plasticity profiles on the device
 constexpr uint32_t kListPosts = 32768;
 
 // neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
@@ -147,6 +148,15 @@ struct StepArgs {
   uint16_t *lpost;
   float *lw;
   uint32_t *lcnt;
+  // Tsodyks-Markram short-term plasticity: per-edge profile id (0 = none)
+  // and state R, U, last spike step (CSR order), the profiles' constants
+  int tm;
+  const uint8_t *tm_pt;
+  float *tm_r;
+  float *tm_u;
+  uint32_t *tm_last;
+  float tm_u0[kMaxTm], tm_arec[kMaxTm], tm_afac[kMaxTm];
+  uint32_t tm_fac;  // bit k: profile k + 1 facilitates
   // pair STDP
   int stdp;
   float *x_pre;
@@ -983,13 +993,29 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
             ev_code[r] = a.code ? (uint8_t)ld_stream_u8(a.code + ev_e[r], spol) : (uint8_t)(rec.x >> 24);
           }
         }
+        // short-term plasticity: the delivered weight is w * R * U (each
+        // edge belongs to one post and so to this block alone)
+        float ev_wd[kEPT];
+#pragma unroll
+        for (uint32_t r = 0; r < kEPT; ++r) {
+          const uint32_t k = tid + r * kScatterThreads;
+          ev_wd[r] = ev_w[r];
+          if (a.tm && k < m) {
+            const uint32_t e = ev_e[r], pt = a.tm_pt[e];
+            if (pt) {
+              const uint32_t q = pt - 1;
+              ev_wd[r] = tm_spike(a.tm_u0[q], a.tm_arec[q], a.tm_afac[q], (a.tm_fac >> q) & 1u, a.tm_r[e],
+                                  a.tm_u[e], a.tm_last[e], ev_w[r], step);
+            }
+          }
+        }
         float pre[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
           pre[r] = 0.0f;
           if (k < m) {
-            const uint32_t cell = put_event<false>(a, S, k, ev_post[r], ev_w[r], ev_code[r], base, p0);
+            const uint32_t cell = put_event<false>(a, S, k, ev_post[r], ev_wd[r], ev_code[r], base, p0);
             if (a.deterministic) pre[r] = ld_ring(cell_addr(a, cell, p0), policy_evict_last());
             if (a.stdp && code_stdp(ev_code[r])) {
               // depression at a pre spike; the pushed weight is the pre-update one

@@ -54,6 +54,8 @@ SIGNATURES = {
     "sg_set_weight_format": [vp, i32],
     "sg_set_deterministic": [vp, i32],
     "sg_scatter_mode": [vp, vp],
+    "sg_register_plasticity": [vp, f32, f32, i32, f32, f32, vp],
+    "sg_connect_plastic": [vp, u32, vp, u32, vp, vp, vp, vp, vp, u64, u32],
     "sg_build": [vp],
     "sg_build_from_csr": [vp, vp, vp, vp, vp],
     "sg_pop_set_noise": [vp, u32, u64, u32, u64, u64, f64, f64, u32],

@@ -87,17 +87,34 @@ class Network:
         check(lib().sg_pop_get_param(self._h, pop, col, _p(out), out.size))
         return out
 
-    def connect(self, frm, from_idx, to, to_idx, weights, delays, syn_types=None, stdp=False):
+    def connect(self, frm, from_idx, to, to_idx, weights, delays, syn_types=None, stdp=False, plast_types=None):
+        """Edges from[from_idx[i]] -> to[to_idx[i]]; optional per-edge kinetic
+        synapse types, pair STDP, and short-term plasticity profile ids
+        (register_plasticity; 0 = none)."""
         fi = np.ascontiguousarray(from_idx, np.uint32)
         ti = np.ascontiguousarray(to_idx, np.uint32)
         w = np.ascontiguousarray(weights, np.float32)
         d = np.ascontiguousarray(delays, np.uint8)
         st = None if syn_types is None else np.ascontiguousarray(syn_types, np.uint8)
-        if not (fi.size == ti.size == w.size == d.size) or (st is not None and st.size != fi.size):
+        pt = None if plast_types is None else np.ascontiguousarray(plast_types, np.uint8)
+        if not (fi.size == ti.size == w.size == d.size) or (st is not None and st.size != fi.size) \
+                or (pt is not None and pt.size != fi.size):
             from ._lib import SimuseError
             raise SimuseError(-1, "connect: slice length mismatch")
-        check(lib().sg_connect_ex(self._h, frm, _p(fi), to, _p(ti), _p(w), _p(d), _p(st), fi.size,
-                                  EDGE_STDP if stdp else 0))
+        if pt is None:
+            check(lib().sg_connect_ex(self._h, frm, _p(fi), to, _p(ti), _p(w), _p(d), _p(st), fi.size,
+                                      EDGE_STDP if stdp else 0))
+        else:
+            check(lib().sg_connect_plastic(self._h, frm, _p(fi), to, _p(ti), _p(w), _p(d), _p(st), _p(pt),
+                                           fi.size, EDGE_STDP if stdp else 0))
+
+    def register_plasticity(self, u0: float, tau_rec: float, dt: float, tau_fac: float | None = None) -> int:
+        """Tsodyks-Markram profile (depression; with facilitation when tau_fac
+        is given) for steps of dt ms; returns its 1-based id."""
+        out = C.c_uint32()
+        check(lib().sg_register_plasticity(self._h, u0, tau_rec, 0 if tau_fac is None else 1,
+                                           0.0 if tau_fac is None else tau_fac, dt, C.byref(out)))
+        return out.value
 
     def connect_fixed_indegree(self, frm, to, k_in, seed, n_exc, w_exc, w_inh, d_min, d_max,
                                syn_type_exc=0, syn_type_inh=0, stdp_exc=False):

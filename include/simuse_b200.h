@@ -133,6 +133,19 @@ int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, doub
                                    int random_w, uint8_t d_min, uint8_t d_max, uint8_t st_exc,
                                    uint8_t st_inh, uint32_t flags_exc);
 
+/* Network::register_plasticity(PlasticityProfile, dt) -> profile id (1-based),
+   core.rs:586-623; synapse.rs:220-292 (Tsodyks-Markram: U0 = u0 in (0, 1],
+   recovery tau_rec, facilitation tau_fac when `facilitation` is set; the
+   device holds at most 8 profiles).  A spike on a synapse with a profile
+   delivers weight * R * U, push.rs:25-102. */
+int sg_register_plasticity(sg_net *net, float u0, float tau_rec, int facilitation, float tau_fac, float dt,
+                           uint32_t *out_id);
+/* connect_edges with Edge::with_synapse_plasticity, core.rs:254-279: as
+   sg_connect_ex plus a per-edge plasticity profile id (0 = none; may be
+   NULL). */
+int sg_connect_plastic(sg_net *net, uint32_t from, const uint32_t *from_idx, uint32_t to,
+                       const uint32_t *to_idx, const float *weights, const uint8_t *delays,
+                       const uint8_t *syn_types, const uint8_t *plast_types, uint64_t n, uint32_t flags);
 /* Network::register_kinetics(SynapseKinetics::ExpOne{tau_decay, erev}, dt)
    -> profile id (1-based), core.rs:564-584; step.rs:248-345 */
 int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id);

@@ -57,7 +57,9 @@ def lib():
             "or_pop_get_state": (i32, [vp, i32, i32, vp, u32]),
             "or_pop_get_state_f64": (i32, [vp, i32, i32, vp, u32]),
             "or_pop_get_param": (i32, [vp, i32, i32, vp, u32]),
-            "or_connect": (i32, [vp, i32, vp, i32, vp, vp, vp, vp, u64, u32]),
+            "or_connect": (i32, [vp, i32, vp, i32, vp, vp, vp, vp, vp, u64, u32]),
+            "or_register_plasticity": (i32, [vp, f32, f32, i32, f32, f32]),
+            "or_tm_sequence": (i32, [f32, f32, f32, i32, f32, vp, u32, vp]),
             "or_register_expone": (i32, [vp, f32, f32, f32]),
             "or_poisson_add": (i32, [vp, f32, f32, u32]),
             "or_poisson_connect": (i32, [vp, i32, i32, vp, vp, vp, vp, u64]),
@@ -157,15 +159,24 @@ class Network:
         _chk(lib().or_pop_get_param(self._h, pop, col, _p(out), out.size))
         return out
 
-    def connect(self, frm, from_idx, to, to_idx, weights, delays, syn_types=None, stdp=False):
+    def connect(self, frm, from_idx, to, to_idx, weights, delays, syn_types=None, stdp=False, plast_types=None):
         fi = np.ascontiguousarray(from_idx, np.uint32)
         ti = np.ascontiguousarray(to_idx, np.uint32)
         w = np.ascontiguousarray(weights, np.float32)
         d = np.ascontiguousarray(delays, np.uint8)
         st = None if syn_types is None else np.ascontiguousarray(syn_types, np.uint8)
-        if not (fi.size == ti.size == w.size == d.size) or (st is not None and st.size != fi.size):
+        pt = None if plast_types is None else np.ascontiguousarray(plast_types, np.uint8)
+        if not (fi.size == ti.size == w.size == d.size) or (st is not None and st.size != fi.size) \
+                or (pt is not None and pt.size != fi.size):
             raise OracleError("connect: slice length mismatch")
-        _chk(lib().or_connect(self._h, frm, _p(fi), to, _p(ti), _p(w), _p(d), _p(st), fi.size, 1 if stdp else 0))
+        _chk(lib().or_connect(self._h, frm, _p(fi), to, _p(ti), _p(w), _p(d), _p(st), _p(pt), fi.size,
+                              1 if stdp else 0))
+
+    def register_plasticity(self, u0, tau_rec, dt, tau_fac=None) -> int:
+        """Tsodyks-Markram profile (depression, or depression + facilitation
+        when tau_fac is given); returns its 1-based id."""
+        return _chk(lib().or_register_plasticity(self._h, u0, tau_rec, 0 if tau_fac is None else 1,
+                                                 0.0 if tau_fac is None else tau_fac, dt))
 
     def register_expone(self, tau_decay, erev, dt) -> int:
         return _chk(lib().or_register_expone(self._h, tau_decay, erev, dt))
@@ -278,6 +289,14 @@ class Network:
         b = np.empty(self.total_neurons, np.float32)
         _chk(lib().or_traces_read(self._h, _p(a), _p(b)))
         return a, b
+
+
+def tm_sequence(u0, a_rec, a_fac, facilitation, steps, w=1.0) -> np.ndarray:
+    """Delivered weights of one Tsodyks-Markram synapse spiking at `steps`."""
+    st = np.ascontiguousarray(steps, np.uint64)
+    out = np.zeros(st.size, np.float32)
+    _chk(lib().or_tm_sequence(u0, a_rec, a_fac, 1 if facilitation else 0, w, _p(st), st.size, _p(out)))
+    return out
 
 
 def fast_exp(x: float) -> float:

@@ -366,8 +366,51 @@ template <typename T> struct Pop {
 struct EdgeIn {
   uint32_t pre, post;
   float w;
-  uint8_t d, st, flags;
+  uint8_t d, st, flags, pt;  // pt: short-term plasticity profile id (0 = none)
 };
+
+// P/api/net/push.rs:25-35 PlastRtProfile: Tsodyks-Markram constants for one dt
+struct TmProf {
+  float u0, a_rec, a_fac;
+  bool fac;
+};
+
+// f32 powi as Rust lowers it for a run-time exponent (the compiler runtime's
+// __powisf2): square-and-multiply from the exponent's lowest bit, the
+// product starting at 1, reciprocal for a negative exponent.
+static float powi_f32(float a, int b) {
+  const bool recip = b < 0;
+  unsigned e = recip ? 0u - (unsigned)b : (unsigned)b;
+  float r = 1.0f;
+  while (true) {
+    if (e & 1u) r *= a;
+    e >>= 1;
+    if (e == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0f / r : r;
+}
+
+// P/api/net/push.rs:50-81 tm_spike: lazy exponential recovery over the steps
+// since the last spike, deliver weight * R * U with the pre-spike R and U,
+// then deplete R and facilitate U.
+static float tm_spike(const TmProf &p, float &r, float &u, uint32_t &last, float w, uint64_t step) {
+  const uint64_t el = step > last ? step - last : 0;
+  const int n = (int)std::min<uint64_t>(el, 1000000);
+  if (n > 0) {
+    const float ar = powi_f32(p.a_rec, n);
+    r = 1.0f + (r - 1.0f) * ar;
+    if (p.fac) {
+      const float af = powi_f32(p.a_fac, n);
+      u = p.u0 + (u - p.u0) * af;
+    }
+  }
+  last = (uint32_t)step;
+  const float scale = r * u;
+  r *= 1.0f - u;
+  if (p.fac) u += p.u0 * (1.0f - u);
+  return w * scale;
+}
 
 struct Kin {
   float a_decay, erev;  // P/api/net/network/step.rs:248-302 (ExpOne)
@@ -398,7 +441,10 @@ template <typename T> struct Net : NetBase {
   std::vector<EdgeIn> edges;
   std::vector<uint32_t> row_ptr, col;
   std::vector<T> w;
-  std::vector<uint8_t> d, st, plastic;
+  std::vector<uint8_t> d, st, plastic, pt;
+  std::vector<TmProf> tm;           // short-term plasticity profiles (id - 1)
+  std::vector<float> tm_r, tm_u;    // per edge (CSR order): R, U
+  std::vector<uint32_t> tm_last;    //   and the step of its last spike
   std::vector<Kin> kin;
   std::vector<T> g;     // [nk][N] kinetic conductances
   std::vector<T> ring;  // [1 + nk][32][N]
@@ -437,6 +483,7 @@ template <typename T> int build_csr(Net<T> &net) {
   net.d.assign(E, 0);
   net.st.assign(E, 0);
   net.plastic.assign(E, 0);
+  net.pt.assign(E, 0);
   std::vector<uint64_t> cursor(net.row_ptr.begin(), net.row_ptr.end() - 1);
   for (auto &e : net.edges) {
     uint64_t pos = cursor[e.pre]++;
@@ -445,6 +492,7 @@ template <typename T> int build_csr(Net<T> &net) {
     net.d[pos] = e.d;
     net.st[pos] = e.st;
     net.plastic[pos] = e.flags & 1;
+    net.pt[pos] = e.pt;
   }
   net.edges.clear();
   net.edges.shrink_to_fit();
@@ -453,6 +501,15 @@ template <typename T> int build_csr(Net<T> &net) {
 
 template <typename T> void alloc_runtime(Net<T> &net) {
   const size_t N = net.total;
+  // P/api/net/network/build.rs:69-84: R = 1, U = U0 of the edge's profile, last = 0
+  if (!net.tm.empty()) {
+    const size_t E = net.col.size();
+    net.tm_r.assign(E, 1.0f);
+    net.tm_u.assign(E, 0.0f);
+    net.tm_last.assign(E, 0);
+    for (size_t e = 0; e < E; ++e)
+      if (net.pt[e]) net.tm_u[e] = net.tm[net.pt[e] - 1].u0;
+  }
   net.ring.assign((1 + net.kin.size()) * kSlots * N, (T)0);
   net.g.assign(net.kin.size() * N, (T)0);
   net.i_in.assign(N, (T)0);
@@ -558,6 +615,13 @@ template <typename T> void net_step(Net<T> &net) {
     uint32_t ts = (uint32_t)((s + std::max<uint32_t>(dl, 1)) % kSlots);
     net.ring_slot(st, ts)[post] += wv;
   };
+  // the delivered weight of edge e: its weight, scaled by R*U for a
+  // short-term-plastic edge (P/api/net/push.rs:83-102; each edge fires at most
+  // once per step, so the push threads update disjoint edge states)
+  auto tm_weight = [&](uint64_t e) -> T {
+    if (net.tm.empty() || net.pt[e] == 0) return net.w[e];
+    return (T)tm_spike(net.tm[net.pt[e] - 1], net.tm_r[e], net.tm_u[e], net.tm_last[e], (float)net.w[e], s);
+  };
   if (g_threads > 1 && net.active.size() > 64) {
     struct Tri {
       uint32_t post;
@@ -574,7 +638,7 @@ template <typename T> void net_step(Net<T> &net) {
       for (size_t a = a0; a < a1; ++a) {
         uint32_t pre = net.active[a];
         for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e)
-          out.push_back(Tri{net.col[e], net.d[e], net.st[e], net.w[e]});
+          out.push_back(Tri{net.col[e], net.d[e], net.st[e], tm_weight(e)});
       }
     };
     std::vector<std::thread> pool;
@@ -586,7 +650,7 @@ template <typename T> void net_step(Net<T> &net) {
   } else {
     for (uint32_t pre : net.active)
       for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e)
-        deliver(net.col[e], net.d[e], net.st[e], net.w[e]);
+        deliver(net.col[e], net.d[e], net.st[e], tm_weight(e));
   }
   for (uint32_t pre : net.active) net.events += net.row_ptr[pre + 1] - net.row_ptr[pre];
   // 5b. Poisson sources (step.rs:163-185)
@@ -821,7 +885,7 @@ int or_pop_get_param(or_net *h, int pop, int col, float *out, uint32_t n) {
 
 // P/api/net/network/core.rs:166-249 connect / connect_inner
 int or_connect(or_net *h, int from, const uint32_t *fi, int to, const uint32_t *ti, const float *w,
-               const uint8_t *dl, const uint8_t *st, uint64_t n, uint32_t flags) {
+               const uint8_t *dl, const uint8_t *st, const uint8_t *pt, uint64_t n, uint32_t flags) {
   DISPATCH(h, {
     if (net.built) return fail("Cannot connect after build()");
     if (from < 0 || (size_t)from >= net.pops.size()) return fail("from population out of range");
@@ -834,9 +898,41 @@ int or_connect(or_net *h, int from, const uint32_t *fi, int to, const uint32_t *
       if (!std::isfinite(w[i])) return fail("Network::connect: weight must be finite");
       if (dl[i] >= kSlots) return fail("delay >= MAX_DELAY_SLOTS");
       uint8_t s = st ? st[i] : 0;
-      net.edges.push_back(EdgeIn{fo + fi[i], tof + ti[i], w[i], dl[i], s, (uint8_t)(flags & 1)});
+      const uint8_t p = pt ? pt[i] : 0;
+      if (p > net.tm.size()) return fail("Network::build: plast_type exceeds registered plasticity profiles");
+      net.edges.push_back(EdgeIn{fo + fi[i], tof + ti[i], w[i], dl[i], s, (uint8_t)(flags & 1), p});
     }
   });
+  return 0;
+}
+
+// P/api/net/network/core.rs:586-623 register_plasticity, validation of
+// P/api/net/synapse.rs:268-292; a_rec = exp(-dt/tau_rec) in f32 on the host
+int or_register_plasticity(or_net *h, float u0, float tau_rec, int facilitation, float tau_fac, float dt) {
+  int id = -1;
+  if (!(dt > 0) || !std::isfinite(dt)) return fail("register_plasticity: dt must be finite and > 0");
+  if (!std::isfinite(u0) || u0 <= 0.0f || u0 > 1.0f) return fail("init_release_prob must be in (0, 1]");
+  if (!std::isfinite(tau_rec) || tau_rec <= 0.0f) return fail("tau_rec must be finite and > 0");
+  if (facilitation && (!std::isfinite(tau_fac) || tau_fac <= 0.0f)) return fail("tau_fac must be finite and > 0");
+  DISPATCH(h, {
+    if (net.built) return fail("register_plasticity must be called before build()");
+    if (net.tm.size() >= 255) return fail("profile id overflow");
+    net.tm.push_back(TmProf{u0, std::exp(-dt / tau_rec), facilitation ? std::exp(-dt / tau_fac) : 0.0f,
+                            facilitation != 0});
+    id = (int)net.tm.size();
+  });
+  return id;
+}
+
+// tm_spike on one synapse over a spike sequence (the reference's NEURON
+// goldens, P/api/net/push.rs:646-695): out[k] = delivered weight of a spike
+// of weight w at steps[k]
+int or_tm_sequence(float u0, float a_rec, float a_fac, int facilitation, float w, const uint64_t *steps,
+                   uint32_t n, float *out) {
+  TmProf p{u0, a_rec, a_fac, facilitation != 0};
+  float r = 1.0f, u = u0;
+  uint32_t last = 0;
+  for (uint32_t k = 0; k < n; ++k) out[k] = tm_spike(p, r, u, last, w, steps[k]);
   return 0;
 }
 

@@ -44,7 +44,11 @@ int or_pop_get_param(or_net *net, int pop, int col, float *out, uint32_t n);
 /* flags bit 0: the edges take part in pair STDP */
 int or_connect(or_net *net, int from, const uint32_t *from_idx, int to,
                const uint32_t *to_idx, const float *w, const uint8_t *delay,
-               const uint8_t *syn_type, uint64_t n, uint32_t flags);
+               const uint8_t *syn_type, const uint8_t *plast_type, uint64_t n, uint32_t flags);
+/* Tsodyks-Markram profile; returns its id (1-based) or a negative status */
+int or_register_plasticity(or_net *net, float u0, float tau_rec, int facilitation, float tau_fac, float dt);
+int or_tm_sequence(float u0, float a_rec, float a_fac, int facilitation, float w, const uint64_t *steps,
+                   uint32_t n, float *out);
 int or_register_expone(or_net *net, float tau_decay, float erev, float dt);
 int or_poisson_add(or_net *net, float rate_hz, float dt_ms, uint32_t seed);
 int or_poisson_add_many(or_net *net, uint32_t n, float rate_hz, float dt_ms, uint32_t seed0);

@@ -166,6 +166,30 @@ def main(root):
         require(txt, needle, rel)
     pins["poisson"] = {"cite": f"{rel}:5-14"}
 
+    # Tsodyks-Markram delivered weights against NEURON:
+    # src/api/net/push.rs:646-695 (test_tm_matches_neuron_delivered_weights)
+    rel = f"{P}/src/api/net/push.rs"
+    txt = read(root, rel)
+    start = txt.index("fn test_tm_matches_neuron_delivered_weights")
+    body = txt[start:start + 4000]
+
+    def f32_array(name):
+        m = re.search(name + r": \[f32; (\d+)\] = \[([^\]]*)\]", body)
+        if not m:
+            raise SystemExit(f"pin not found: {name} in {rel}")
+        vals = [float(x) for x in m.group(2).replace("\n", " ").split(",") if x.strip()]
+        assert len(vals) == int(m.group(1))
+        return vals
+    for needle in ["u0: 0.5,", "a_rec: (-0.5f32 / 100.0).exp(),", "u0: 0.1,", "a_rec: (-0.5f32 / 1e6).exp(),",
+                   "a_fac: (-0.5f32 / 50.0).exp(),", "let step = 20 + 40 * k;", "(w - ref_w).abs() < 1e-4"]:
+        require(body, needle, rel)
+    pins["tm_neuron"] = {
+        "cite": f"{rel}:646-695",
+        "dt": 0.5, "steps": [20 + 40 * k for k in range(12)], "tol": 1e-4,
+        "depression": {"u0": 0.5, "tau_rec": 100.0, "ref": f32_array("REF_DEP")},
+        "facilitation": {"u0": 0.1, "tau_rec": 1e6, "tau_fac": 50.0, "ref": f32_array("REF_FAC")},
+    }
+
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_pins.json")
     with open(out, "w") as f:
         json.dump(pins, f, indent=1)

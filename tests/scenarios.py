@@ -227,3 +227,27 @@ def gpea_network(make_net, n=64, steps=300, seed=5):
         net.step(1)
         rast.append(net.spikes(p).copy())
     return net, p, np.array(rast)
+
+
+def tm_drive(make_net, steps=500):
+    """P/api/net/network/tests.rs:530-575 (plastic_synapse_depresses_repeated_drive):
+    three LIF neurons with the test's parameters, a fast-refractory pre
+    driven by 100 every step, pre -> post 1 static (weight 100, delay 0) and
+    pre -> post 2 through a depressing Tsodyks-Markram synapse (U0 0.5,
+    tau_rec 10 ms, dt 0.5).  Returns (spikes of post 1, of post 2)."""
+    net = make_net()
+    p = net.add_population(LIF, 3)
+    for col, v in enumerate([0.5, 0.1, -70.0, -65.0, -70.0, 1.0]):  # v_thresh -65, tau_ref 1
+        net.fill_param(p, col, v)
+    net.fill_state(p, 0, -70.0)
+    plast = net.register_plasticity(0.5, 10.0, 0.5)
+    assert plast == 1
+    net.connect(p, np.array([0, 0], np.uint32), p, np.array([1, 2], np.uint32), np.array([100.0, 100.0], np.float32),
+                np.zeros(2, np.uint8), plast_types=np.array([0, plast], np.uint8))
+    net.build()
+    fired = np.zeros(3, np.int64)
+    for _ in range(steps):
+        net.inject_current(p, np.array([0], np.uint32), np.array([100.0], np.float32))
+        net.step(1)
+        fired += net.spikes(p)
+    return net, int(fired[1]), int(fired[2])

@@ -202,3 +202,35 @@ def test_kuramoto_oracle_mean_field_is_the_dense_sum():
     th, r = O.kuramoto_rk4(th0, om, K, dt, steps, precision=1)
     assert np.abs(np.angle(np.exp(1j * (th - x)))).max() < 1e-6  # th is rounded to f32
     assert np.abs(r - np.array(r_ref)).max() < 1e-12
+
+
+def test_tm_matches_neuron_delivered_weights():
+    """P/api/net/push.rs:646-695: delivered weights of a depressing and a
+    facilitating Tsodyks-Markram synapse against NEURON, spikes at steps
+    20 + 40k, dt 0.5 ms, within the reference's 1e-4."""
+    pin = PINS["tm_neuron"]
+    dt = np.float32(pin["dt"])
+    dep, fac = pin["depression"], pin["facilitation"]
+    a_dep = float(np.exp(np.float32(-dt / np.float32(dep["tau_rec"]))))
+    got = O.tm_sequence(dep["u0"], a_dep, 0.0, False, pin["steps"])
+    assert np.max(np.abs(got - np.array(dep["ref"], np.float32))) < pin["tol"]
+    a_rec = float(np.exp(np.float32(-dt / np.float32(fac["tau_rec"]))))
+    a_fac = float(np.exp(np.float32(-dt / np.float32(fac["tau_fac"]))))
+    got = O.tm_sequence(fac["u0"], a_rec, a_fac, True, pin["steps"])
+    assert np.max(np.abs(got - np.array(fac["ref"], np.float32))) < pin["tol"]
+
+
+def test_tm_depressing_synapse_silences_its_post():
+    """P/api/net/network/tests.rs:530-575: the static edge keeps driving its
+    post, the depressed edge leaves its post silent."""
+    _, static, plastic = S.tm_drive(lambda: O.Network(0))
+    assert static > 20
+    assert plastic == 0
+
+
+def test_register_plasticity_rejects_invalid_profile():
+    """P/api/net/network/tests.rs:577-593."""
+    net = O.Network(0)
+    for u0, tau in ((0.0, 1.0), (1.5, 1.0), (0.5, 0.0), (0.5, float("nan"))):
+        with pytest.raises(O.OracleError):
+            net.register_plasticity(u0, tau, 0.5)
