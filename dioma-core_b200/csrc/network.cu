@@ -101,8 +101,14 @@ struct HostSrc {
   std::vector<uint8_t> code;
 };
 
+// A kinetic synapse profile's per-step constants (P/api/net/network/step.rs:
+// 206-298): kind 0 ExpOne {a_decay}, 1 ExpTwo {a_rise, a_decay, norm},
+// 2 Alpha {r, e*(dt/tau)*r}, 3 ExpThree {a_rise, a_decay1, a_decay2, wf1,
+// wf2, k_a, gbase1, gbase2}
 struct Kin {
-  float a_decay, erev;
+  int kind;
+  float erev;
+  float c[8];
 };
 
 // Tsodyks-Markram profile constants for the network's dt (push.rs:25-35)
@@ -289,7 +295,8 @@ StepArgs make_args(sg_net *net) {
   a.nslots = net->nslots;
   a.n_kin = (int)net->kin.size();
   for (size_t k = 0; k < net->kin.size() && k < 3; ++k) {
-    a.kin_a[k] = net->kin[k].a_decay;
+    a.kin_kind[k] = net->kin[k].kind;
+    for (int q = 0; q < 8; ++q) a.kin_c[k][q] = net->kin[k].c[q];
     a.kin_erev[k] = net->kin[k].erev;
   }
   a.kin_g = net->d_kin_g.p;
@@ -1165,7 +1172,7 @@ void finish_build(sg_net *net) {
   net->nslots = std::max<uint32_t>(net->max_delay, 1u) + 1u;
   net->d_ring.alloc(std::max<size_t>(n_rings * net->nslots * Nd, 1));
   net->d_ring.zero(s);
-  net->d_kin_g.alloc(std::max<size_t>(net->kin.size() * Nd, 1));
+  net->d_kin_g.alloc(std::max<size_t>(net->kin.size() * 3 * Nd, 1));  // up to 3 state arrays per profile
   net->d_kin_g.zero(s);
   net->d_step.alloc(1);
   net->d_step.zero(s);
@@ -1768,17 +1775,65 @@ int sg_connect_lognormal_outdegree(sg_net *net, uint32_t from, uint32_t to, doub
   });
 }
 
-int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id) {
+// P/api/net/synapse.rs:296-305 exp_waveform_factor (NeuroML waveformFactor), f32
+static float waveform_factor(float tr, float td) {
+  const float t_peak = (tr * td) / (td - tr) * std::log(td / tr);
+  const float h = std::exp(-t_peak / td) - std::exp(-t_peak / tr);
+  return 1.0f / h;
+}
+
+int sg_register_kinetics(sg_net *net, int kind, const float *p, float erev, float dt, uint32_t *out_id) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "register_kinetics must be called before build()");
-    SG_REQUIRE(std::isfinite(dt) && dt > 0, SG_E_INVALID, "register_kinetics: dt must be finite and > 0");
-    SG_REQUIRE(std::isfinite(tau_decay) && tau_decay > 0, SG_E_INVALID, "tau_decay must be finite and > 0");
+    SG_REQUIRE(p, SG_E_INVALID, "null parameters");
     SG_REQUIRE(std::isfinite(erev), SG_E_INVALID, "erev must be finite");
+    SG_REQUIRE(std::isfinite(dt) && dt > 0, SG_E_INVALID, "register_kinetics: dt must be finite and > 0");
     SG_REQUIRE(net->kin.size() < 3, SG_E_INVALID, "at most 3 kinetic profiles are supported on the device path");
-    net->kin.push_back(Kin{std::exp(-dt / tau_decay), erev});  // step.rs:252-254 (f32 exp)
+    auto pos = [](float x) { return std::isfinite(x) && x > 0.0f; };
+    Kin k{kind, erev, {}};
+    if (kind == SG_KIN_EXPONE) {  // synapse.rs:102-106 validation; step.rs:251-253
+      SG_REQUIRE(pos(p[0]), SG_E_INVALID, "tau_decay must be finite and > 0");
+      k.c[0] = std::exp(-dt / p[0]);
+    } else if (kind == SG_KIN_EXPTWO) {  // synapse.rs:107-122; step.rs:254-262
+      SG_REQUIRE(pos(p[1]), SG_E_INVALID, "tau_decay must be finite and > 0");
+      SG_REQUIRE(pos(p[0]), SG_E_INVALID, "tau_rise must be finite and > 0");
+      SG_REQUIRE(p[0] < p[1], SG_E_INVALID, "tau_rise must be < tau_decay");
+      k.c[0] = std::exp(-dt / p[0]);
+      k.c[1] = std::exp(-dt / p[1]);
+      k.c[2] = waveform_factor(p[0], p[1]);
+    } else if (kind == SG_KIN_ALPHA) {  // synapse.rs:123-127; step.rs:263-269
+      SG_REQUIRE(pos(p[0]), SG_E_INVALID, "tau must be finite and > 0");
+      const float r = std::exp(-dt / p[0]);
+      k.c[0] = r;
+      k.c[1] = 2.7182817f * (dt / p[0]) * r;  // std::f32::consts::E
+    } else if (kind == SG_KIN_EXPTHREE) {  // synapse.rs:128-156; step.rs:270-291
+      const float tr = p[0], td1 = p[1], td2 = p[2], g1 = p[3], g2 = p[4];
+      SG_REQUIRE(pos(tr), SG_E_INVALID, "tau_rise must be finite and > 0");
+      SG_REQUIRE(std::isfinite(td1) && td1 > tr, SG_E_INVALID, "tau_decay1 must be finite and > tau_rise");
+      SG_REQUIRE(std::isfinite(td2) && td2 > tr, SG_E_INVALID, "tau_decay2 must be finite and > tau_rise");
+      SG_REQUIRE(std::isfinite(g1) && g1 >= 0.0f && std::isfinite(g2) && g2 >= 0.0f, SG_E_INVALID,
+                 "gbase1 and gbase2 must be finite and >= 0");
+      SG_REQUIRE(g1 + g2 > 0.0f, SG_E_INVALID, "gbase1 + gbase2 must be > 0");
+      const float wf1 = waveform_factor(tr, td1), wf2 = waveform_factor(tr, td2);
+      k.c[0] = std::exp(-dt / tr);
+      k.c[1] = std::exp(-dt / td1);
+      k.c[2] = std::exp(-dt / td2);
+      k.c[3] = wf1;
+      k.c[4] = wf2;
+      k.c[5] = (g1 * wf1 + g2 * wf2) / (g1 + g2);
+      k.c[6] = g1;
+      k.c[7] = g2;
+    } else {
+      SG_REQUIRE(false, SG_E_INVALID, "unknown kinetics kind " + std::to_string(kind));
+    }
+    net->kin.push_back(k);
     if (out_id) *out_id = (uint32_t)net->kin.size();
   });
+}
+
+int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id) {
+  return sg_register_kinetics(net, SG_KIN_EXPONE, &tau_decay, erev, dt, out_id);
 }
 
 int sg_poisson_add_many(sg_net *net, uint32_t n, float rate_hz, float dt_ms, const uint32_t *seeds, uint32_t seed0,

@@ -95,11 +95,14 @@ struct StepArgs {
   float *ring;
   uint32_t Nd;
   uint32_t nslots;
-  // kinetic ExpOne profiles (ring k+1)
+  // kinetic synapse profiles (ring k+1): kind (0 ExpOne, 1 ExpTwo, 2 Alpha,
+  // 3 ExpThree), per-step constants (P/api/net/network/step.rs:206-298),
+  // reversal potential; state [n_kin][3][Nd]
   int n_kin;
-  float kin_a[3];
+  int kin_kind[3];
+  float kin_c[3][8];
   float kin_erev[3];
-  float *kin_g;  // [n_kin][Nd]
+  float *kin_g;
   // CSR (device neuron indices), rows sorted by post; one 8-byte record per
   // synapse: x = post | code << 24 (packed) or post (code in `code`), y = weight
   const uint32_t *row_ptr;
@@ -331,18 +334,43 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   for (int c = 0; c < NS; ++c) V::load(p.state + (size_t)c * p.cap + i0, sv[c]);
   // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start
   for (int k = 0; k < a.n_kin; ++k) {
-    float jump[NPT], g[NPT];
+    float jump[NPT], s0[NPT], s1[NPT], s2[NPT];
     float *ks = a.ring + ((size_t)(k + 1) * a.nslots + slot) * a.Nd + gi0;
     V::load(ks, jump);
     V::store(ks, zero);
-    float *gp = a.kin_g + (size_t)k * a.Nd + gi0;
-    V::load(gp, g);
+    const int kind = a.kin_kind[k];
+    const float *c = a.kin_c[k];
+    float *g0 = a.kin_g + ((size_t)k * 3 + 0) * a.Nd + gi0;
+    float *g1 = a.kin_g + ((size_t)k * 3 + 1) * a.Nd + gi0;
+    float *g2 = a.kin_g + ((size_t)k * 3 + 2) * a.Nd + gi0;
+    V::load(g0, s0);
+    if (kind != 0) V::load(g1, s1);
+    if (kind == 3) V::load(g2, s2);
 #pragma unroll
-    for (int q = 0; q < NPT; ++q) {
-      g[q] = g[q] * a.kin_a[k] + jump[q];
-      x[q] += g[q] * (a.kin_erev[k] - sv[0][q]);
+    for (int q = 0; q < NPT; ++q) {  // step.rs:336-398
+      const float j = jump[q], dv = a.kin_erev[k] - sv[0][q];
+      if (kind == 0) {  // ExpOne: g
+        s0[q] = s0[q] * c[0] + j;
+        x[q] += s0[q] * dv;
+      } else if (kind == 1) {  // ExpTwo: g (decay), x (rise)
+        s0[q] = s0[q] * c[1] + j;
+        s1[q] = s1[q] * c[0] + j;
+        x[q] += c[2] * (s0[q] - s1[q]) * dv;
+      } else if (kind == 2) {  // Alpha: g, a
+        const float a_old = s1[q];
+        s1[q] = a_old * c[0] + j;
+        s0[q] = s0[q] * c[0] + c[1] * a_old;
+        x[q] += s0[q] * dv;
+      } else {  // ExpThree: a (rise), b, c (decays)
+        s0[q] = s0[q] * c[0] + j * c[5];
+        s1[q] = s1[q] * c[1] + j * c[3];
+        s2[q] = s2[q] * c[2] + j * c[4];
+        x[q] += (c[6] * (s1[q] - s0[q]) + c[7] * (s2[q] - s0[q])) * dv;
+      }
     }
-    V::store(gp, g);
+    V::store(g0, s0);
+    if (kind != 0) V::store(g1, s1);
+    if (kind == 3) V::store(g2, s2);
   }
   float pv[NP][NPT];
 #pragma unroll

@@ -55,6 +55,7 @@ SIGNATURES = {
     "sg_set_deterministic": [vp, i32],
     "sg_scatter_mode": [vp, vp],
     "sg_register_plasticity": [vp, f32, f32, i32, f32, f32, vp],
+    "sg_register_kinetics": [vp, i32, vp, f32, f32, vp],
     "sg_connect_plastic": [vp, u32, vp, u32, vp, vp, vp, vp, vp, u64, u32],
     "sg_build": [vp],
     "sg_build_from_csr": [vp, vp, vp, vp, vp],

@@ -147,6 +147,16 @@ class Network:
         check(lib().sg_register_expone(self._h, tau_decay, erev, dt, C.byref(out)))
         return out.value
 
+    def register_kinetics(self, kind: int, params, erev: float, dt: float) -> int:
+        """Kinetic synapse profile: kind 0 ExpOne {tau_decay}, 1 ExpTwo
+        {tau_rise, tau_decay}, 2 Alpha {tau}, 3 ExpThree {tau_rise, tau_decay1,
+        tau_decay2, gbase1, gbase2}; returns its 1-based id (the syn_type)."""
+        p = np.zeros(5, np.float32)
+        p[:len(params)] = params
+        out = C.c_uint32()
+        check(lib().sg_register_kinetics(self._h, int(kind), _p(p), erev, dt, C.byref(out)))
+        return out.value
+
     def add_poisson_source(self, rate_hz: float, dt_ms: float, seed: int) -> int:
         out = C.c_uint32()
         check(lib().sg_poisson_add(self._h, rate_hz, dt_ms, seed, C.byref(out)))

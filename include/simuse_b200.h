@@ -149,6 +149,16 @@ int sg_connect_plastic(sg_net *net, uint32_t from, const uint32_t *from_idx, uin
 /* Network::register_kinetics(SynapseKinetics::ExpOne{tau_decay, erev}, dt)
    -> profile id (1-based), core.rs:564-584; step.rs:248-345 */
 int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint32_t *out_id);
+/* Network::register_kinetics(SynapseKinetics, dt) for every waveform kind,
+   core.rs:564-584; synapse.rs:36-158 (parameters and validation);
+   step.rs:206-398 (exact per-step update).  params: ExpOne {tau_decay},
+   ExpTwo {tau_rise, tau_decay}, Alpha {tau}, ExpThree {tau_rise, tau_decay1,
+   tau_decay2, gbase1, gbase2}.  At most 3 profiles on the device. */
+#define SG_KIN_EXPONE 0
+#define SG_KIN_EXPTWO 1
+#define SG_KIN_ALPHA 2
+#define SG_KIN_EXPTHREE 3
+int sg_register_kinetics(sg_net *net, int kind, const float *params, float erev, float dt, uint32_t *out_id);
 
 /* Network::add_poisson_source(rate_hz, dt_ms, seed) -> id, core.rs:288-312 */
 int sg_poisson_add(sg_net *net, float rate_hz, float dt_ms, uint32_t seed, uint32_t *out_id);

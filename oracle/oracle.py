@@ -61,6 +61,7 @@ def lib():
             "or_register_plasticity": (i32, [vp, f32, f32, i32, f32, f32]),
             "or_tm_sequence": (i32, [f32, f32, f32, i32, f32, vp, u32, vp]),
             "or_register_expone": (i32, [vp, f32, f32, f32]),
+            "or_register_kinetics": (i32, [vp, i32, vp, f32, f32]),
             "or_poisson_add": (i32, [vp, f32, f32, u32]),
             "or_poisson_connect": (i32, [vp, i32, i32, vp, vp, vp, vp, u64]),
             "or_poisson_add_many": (i32, [vp, u32, f32, f32, u32]),
@@ -180,6 +181,12 @@ class Network:
 
     def register_expone(self, tau_decay, erev, dt) -> int:
         return _chk(lib().or_register_expone(self._h, tau_decay, erev, dt))
+
+    def register_kinetics(self, kind, params, erev, dt) -> int:
+        """kind 0 ExpOne, 1 ExpTwo, 2 Alpha, 3 ExpThree (params as in the C API)."""
+        p = np.zeros(5, np.float32)
+        p[:len(params)] = params
+        return _chk(lib().or_register_kinetics(self._h, int(kind), _p(p), erev, dt))
 
     def add_poisson_source(self, rate_hz, dt_ms, seed) -> int:
         return _chk(lib().or_poisson_add(self._h, rate_hz, dt_ms, seed))

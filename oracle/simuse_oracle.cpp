@@ -412,9 +412,22 @@ static float tm_spike(const TmProf &p, float &r, float &u, uint32_t &last, float
   return w * scale;
 }
 
+// P/api/net/network/step.rs:206-298 KinKind: a kinetic synapse's per-step
+// constants (f32, from the host libm).  kind 0 ExpOne {a_decay}, 1 ExpTwo
+// {a_rise, a_decay, norm}, 2 Alpha {r, e*(dt/tau)*r}, 3 ExpThree {a_rise,
+// a_decay1, a_decay2, wf1, wf2, k_a, gbase1, gbase2}
 struct Kin {
-  float a_decay, erev;  // P/api/net/network/step.rs:248-302 (ExpOne)
+  int kind;
+  float erev;
+  float c[8];
 };
+
+// P/api/net/synapse.rs:296-305 exp_waveform_factor (NeuroML waveformFactor)
+static float waveform_factor(float tr, float td) {
+  const float t_peak = (tr * td) / (td - tr) * std::log(td / tr);
+  const float h = std::exp(-t_peak / td) - std::exp(-t_peak / tr);
+  return 1.0f / h;
+}
 
 template <typename T> struct Src {
   float p;
@@ -511,7 +524,7 @@ template <typename T> void alloc_runtime(Net<T> &net) {
       if (net.pt[e]) net.tm_u[e] = net.tm[net.pt[e] - 1].u0;
   }
   net.ring.assign((1 + net.kin.size()) * kSlots * N, (T)0);
-  net.g.assign(net.kin.size() * N, (T)0);
+  net.g.assign(net.kin.size() * 3 * N, (T)0);  // up to three state arrays per profile
   net.i_in.assign(N, (T)0);
   net.v_scr.assign(N, (T)0);
   net.scratch.assign(N, (T)0);
@@ -572,12 +585,40 @@ template <typename T> void net_step(Net<T> &net) {
       T *ks = net.ring_slot((uint32_t)k + 1, slot);
       std::memcpy(net.scratch.data(), ks, N * sizeof(T));
       std::memset(ks, 0, N * sizeof(T));
-      const T a = (T)net.kin[k].a_decay, erev = (T)net.kin[k].erev;
-      T *g = &net.g[k * N];
-      for (size_t i = 0; i < N; ++i) {
-        T gn = g[i] * a + net.scratch[i];
-        g[i] = gn;
-        net.i_in[i] += gn * (erev - net.v_scr[i]);
+      const Kin &K = net.kin[k];
+      const T erev = (T)K.erev;
+      T c[8];
+      for (int q = 0; q < 8; ++q) c[q] = (T)K.c[q];
+      T *s0 = &net.g[(k * 3 + 0) * N], *s1 = &net.g[(k * 3 + 1) * N], *s2 = &net.g[(k * 3 + 2) * N];
+      for (size_t i = 0; i < N; ++i) {  // step.rs:336-398
+        const T j = net.scratch[i], dv = erev - net.v_scr[i];
+        if (K.kind == 0) {  // ExpOne: g
+          const T gn = s0[i] * c[0] + j;
+          s0[i] = gn;
+          net.i_in[i] += gn * dv;
+        } else if (K.kind == 1) {  // ExpTwo: g (decay), x (rise)
+          const T gn = s0[i] * c[1] + j;
+          const T xn = s1[i] * c[0] + j;
+          s0[i] = gn;
+          s1[i] = xn;
+          net.i_in[i] += c[2] * (gn - xn) * dv;
+        } else if (K.kind == 2) {  // Alpha: g, a
+          const T a_old = s1[i];
+          const T an = a_old * c[0] + j;
+          const T gn = s0[i] * c[0] + c[1] * a_old;
+          s0[i] = gn;
+          s1[i] = an;
+          net.i_in[i] += gn * dv;
+        } else {  // ExpThree: a (rise), b, c (decays)
+          const T an = s0[i] * c[0] + j * c[5];
+          const T bn = s1[i] * c[1] + j * c[3];
+          const T cn = s2[i] * c[2] + j * c[4];
+          s0[i] = an;
+          s1[i] = bn;
+          s2[i] = cn;
+          const T cur = c[6] * (bn - an) + c[7] * (cn - an);
+          net.i_in[i] += cur * dv;
+        }
       }
     }
   }
@@ -936,6 +977,59 @@ int or_tm_sequence(float u0, float a_rec, float a_fac, int facilitation, float w
   return 0;
 }
 
+// P/api/net/network/core.rs:564-584 register_kinetics for every waveform
+// kind, validation of P/api/net/synapse.rs:95-158, constants of
+// step.rs:249-297.  p: ExpOne {tau_decay}, ExpTwo {tau_rise, tau_decay},
+// Alpha {tau}, ExpThree {tau_rise, tau_decay1, tau_decay2, gbase1, gbase2}.
+int or_register_kinetics(or_net *h, int kind, const float *p, float erev, float dt) {
+  int id = -1;
+  auto pos = [](float x) { return std::isfinite(x) && x > 0.0f; };
+  if (!std::isfinite(erev)) return fail("erev must be finite");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail("register_kinetics: dt must be finite and > 0");
+  Kin k{kind, erev, {}};
+  if (kind == 0) {
+    if (!pos(p[0])) return fail("tau_decay must be finite and > 0");
+    k.c[0] = std::exp(-dt / p[0]);
+  } else if (kind == 1) {
+    if (!pos(p[1])) return fail("tau_decay must be finite and > 0");
+    if (!pos(p[0])) return fail("tau_rise must be finite and > 0");
+    if (p[0] >= p[1]) return fail("tau_rise must be < tau_decay");
+    k.c[0] = std::exp(-dt / p[0]);
+    k.c[1] = std::exp(-dt / p[1]);
+    k.c[2] = waveform_factor(p[0], p[1]);
+  } else if (kind == 2) {
+    if (!pos(p[0])) return fail("tau must be finite and > 0");
+    const float r = std::exp(-dt / p[0]);
+    k.c[0] = r;
+    k.c[1] = 2.7182817f * (dt / p[0]) * r;  // std::f32::consts::E
+  } else if (kind == 3) {
+    const float tr = p[0], td1 = p[1], td2 = p[2], g1 = p[3], g2 = p[4];
+    if (!pos(tr)) return fail("tau_rise must be finite and > 0");
+    if (!std::isfinite(td1) || td1 <= tr) return fail("tau_decay1 must be finite and > tau_rise");
+    if (!std::isfinite(td2) || td2 <= tr) return fail("tau_decay2 must be finite and > tau_rise");
+    if (!std::isfinite(g1) || g1 < 0.0f || !std::isfinite(g2) || g2 < 0.0f) return fail("gbase must be finite and >= 0");
+    if (g1 + g2 <= 0.0f) return fail("gbase1 + gbase2 must be > 0");
+    const float wf1 = waveform_factor(tr, td1), wf2 = waveform_factor(tr, td2);
+    k.c[0] = std::exp(-dt / tr);
+    k.c[1] = std::exp(-dt / td1);
+    k.c[2] = std::exp(-dt / td2);
+    k.c[3] = wf1;
+    k.c[4] = wf2;
+    k.c[5] = (g1 * wf1 + g2 * wf2) / (g1 + g2);
+    k.c[6] = g1;
+    k.c[7] = g2;
+  } else {
+    return fail("unknown kinetics kind");
+  }
+  DISPATCH(h, {
+    if (net.built) return fail("register_kinetics must be called before build()");
+    if (net.kin.size() >= 255) return fail("profile id overflow");
+    net.kin.push_back(k);
+    id = (int)net.kin.size();
+  });
+  return id;
+}
+
 // P/api/net/network/core.rs:564-584 register_kinetics (ExpOne profile,
 // a_decay = exp(-dt/tau) in f32, step.rs:252-254)
 int or_register_expone(or_net *h, float tau_decay, float erev, float dt) {
@@ -945,7 +1039,8 @@ int or_register_expone(or_net *h, float tau_decay, float erev, float dt) {
   DISPATCH(h, {
     if (net.built) return fail("register_kinetics must be called before build()");
     if (net.kin.size() >= 255) return fail("profile id overflow");
-    net.kin.push_back(Kin{std::exp(-dt / tau_decay), erev});
+    Kin k{0, erev, {std::exp(-dt / tau_decay)}};
+    net.kin.push_back(k);
     id = (int)net.kin.size();
   });
   return id;

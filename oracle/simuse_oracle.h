@@ -50,6 +50,9 @@ int or_register_plasticity(or_net *net, float u0, float tau_rec, int facilitatio
 int or_tm_sequence(float u0, float a_rec, float a_fac, int facilitation, float w, const uint64_t *steps,
                    uint32_t n, float *out);
 int or_register_expone(or_net *net, float tau_decay, float erev, float dt);
+/* kind 0 ExpOne {tau_decay}, 1 ExpTwo {tau_rise, tau_decay}, 2 Alpha {tau},
+   3 ExpThree {tau_rise, tau_decay1, tau_decay2, gbase1, gbase2} */
+int or_register_kinetics(or_net *net, int kind, const float *params, float erev, float dt);
 int or_poisson_add(or_net *net, float rate_hz, float dt_ms, uint32_t seed);
 int or_poisson_add_many(or_net *net, uint32_t n, float rate_hz, float dt_ms, uint32_t seed0);
 int or_poisson_connect_one_to_one(or_net *net, int first, uint32_t n, int to, float w, uint8_t delay);
