@@ -201,6 +201,17 @@ struct sg_net {
   DBuf<uint8_t> d_pt;
   DBuf<float> d_tm_r, d_tm_u;
   DBuf<uint32_t> d_tm_last;
+  // dopamine-modulated eligibility learning (sg_learn_enable): per-neuron
+  // traces, per-synapse eligibility and sync step (relative to l_t0, the
+  // step counter when learning began), in-edges of every neuron, motor counts
+  bool learn_on = false;
+  float l_dt = 0, l_tau_pre = 0, l_tau_post = 0, l_tau_e = 0, l_a_ltp = 0, l_a_ltd = 0, l_lr = 0, l_w_min = 0,
+        l_w_max = 0;
+  float l_dpre = 0, l_dpost = 0, l_de = 0;
+  unsigned long long l_t0 = 0;
+  uint32_t l_motor[4] = {0, 0, 0, 0};
+  DBuf<float> d_l_tp, d_l_tq, d_l_elig, d_l_baked;
+  DBuf<uint32_t> d_l_last, d_l_in_ptr, d_l_in_edge, d_l_in_pre, d_l_motor;
   // raster readback work buffers, kept from call to call (grow only)
   DBuf<unsigned long long> rr_cnt, rr_off;
   DBuf<uint8_t> rr_temp;
@@ -355,6 +366,13 @@ StepArgs make_args(sg_net *net) {
   a.in_edge = net->d_in_edge.p;
   a.in_pre = net->d_in_pre.p;
   a.drift = net->d_drift.p;
+  a.learn = net->learn_on ? 1 : 0;
+  a.l_tp = net->d_l_tp.p;
+  a.l_tq = net->d_l_tq.p;
+  a.l_dpre = net->l_dpre;
+  a.l_dpost = net->l_dpost;
+  for (int k = 0; k < 4; ++k) a.l_motor[k] = net->l_motor[k];
+  a.l_motor_acc = net->d_l_motor.p;
   return a;
 }
 
@@ -445,17 +463,18 @@ __global__ void to_u32_kernel(const unsigned long long *in, uint32_t *out, uint6
     out[i] = (uint32_t)in[i];
 }
 // Plastic in-edges grouped by post.
+// in-edges per post of the plastic synapses (all = 0) or of every synapse
 __global__ void csc_count_kernel(const uint32_t *row_ptr, const uint2 *edge, const uint8_t *code, int packed,
-                                 uint32_t Nd, unsigned long long *cnt) {
+                                 uint32_t Nd, unsigned long long *cnt, int all) {
   for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x)
     for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e)
-      if (code_stdp(edge_code_of(edge[e], code, e, packed))) atomicAdd(cnt + edge_post(edge[e], packed), 1ull);
+      if (all || code_stdp(edge_code_of(edge[e], code, e, packed))) atomicAdd(cnt + edge_post(edge[e], packed), 1ull);
 }
 __global__ void csc_fill_kernel(const uint32_t *row_ptr, const uint2 *edge, const uint8_t *code, int packed,
-                                uint32_t Nd, uint32_t *cursor, uint32_t *in_edge, uint32_t *in_pre) {
+                                uint32_t Nd, uint32_t *cursor, uint32_t *in_edge, uint32_t *in_pre, int all) {
   for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x)
     for (uint32_t e = row_ptr[pre]; e < row_ptr[pre + 1]; ++e)
-      if (code_stdp(edge_code_of(edge[e], code, e, packed))) {
+      if (all || code_stdp(edge_code_of(edge[e], code, e, packed))) {
         const uint32_t k = atomicAdd(cursor + edge_post(edge[e], packed), 1u);
         in_edge[k] = e;
         in_pre[k] = pre;
@@ -927,6 +946,40 @@ void build_sources(sg_net *net) {
   }
 }
 
+// In-edges per post (CSC over the CSR records): in_ptr [Nd+1], and per
+// in-edge its record index and pre; `all` = every synapse, else the plastic ones.
+void build_in_edges(sg_net *net, int all, DBuf<uint32_t> &in_ptr, DBuf<uint32_t> &in_edge, DBuf<uint32_t> &in_pre) {
+  cudaStream_t s = net->stream;
+  const uint32_t Nd = net->Nd;
+  DBuf<unsigned long long> cnt, ip64;
+  cnt.alloc((size_t)Nd + 1);
+  cnt.zero(s);
+  launch_grid(Nd, [&](unsigned b) {
+    csc_count_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_code.p, net->packed, Nd, cnt.p, all);
+  });
+  ip64.alloc((size_t)Nd + 1);
+  size_t tb = 0;
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, ip64.p, (int64_t)Nd + 1, s));
+  DBuf<uint8_t> temp;
+  temp.alloc(std::max<size_t>(tb, 1));
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, ip64.p, (int64_t)Nd + 1, s));
+  in_ptr.alloc((size_t)Nd + 1);
+  launch_grid((uint64_t)Nd + 1, [&](unsigned b) { to_u32_kernel<<<b, 256, 0, s>>>(ip64.p, in_ptr.p, (uint64_t)Nd + 1); });
+  unsigned long long n_in = 0;
+  SG_CUDA(cudaMemcpyAsync(&n_in, ip64.p + Nd, 8, cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  in_edge.alloc(std::max<unsigned long long>(n_in, 1));
+  in_pre.alloc(std::max<unsigned long long>(n_in, 1));
+  DBuf<uint32_t> cursor;
+  cursor.alloc((size_t)Nd + 1);
+  SG_CUDA(cudaMemcpyAsync(cursor.p, in_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToDevice, s));
+  launch_grid(Nd, [&](unsigned b) {
+    csc_fill_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_code.p, net->packed, Nd, cursor.p,
+                                      in_edge.p, in_pre.p, all);
+  });
+  SG_CUDA(cudaStreamSynchronize(s));
+}
+
 void build_stdp(sg_net *net) {
   cudaStream_t s = net->stream;
   const uint32_t Nd = net->Nd;
@@ -936,33 +989,7 @@ void build_stdp(sg_net *net) {
   net->d_x_post.zero(s);
   net->d_drift.alloc(1);
   net->d_drift.zero(s);
-  DBuf<unsigned long long> cnt, ip64;
-  cnt.alloc((size_t)Nd + 1);
-  cnt.zero(s);
-  launch_grid(Nd, [&](unsigned b) {
-    csc_count_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_code.p, net->packed, Nd, cnt.p);
-  });
-  ip64.alloc((size_t)Nd + 1);
-  size_t tb = 0;
-  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, ip64.p, (int64_t)Nd + 1, s));
-  DBuf<uint8_t> temp;
-  temp.alloc(std::max<size_t>(tb, 1));
-  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, ip64.p, (int64_t)Nd + 1, s));
-  net->d_in_ptr.alloc((size_t)Nd + 1);
-  launch_grid((uint64_t)Nd + 1, [&](unsigned b) { to_u32_kernel<<<b, 256, 0, s>>>(ip64.p, net->d_in_ptr.p, (uint64_t)Nd + 1); });
-  unsigned long long n_in = 0;
-  SG_CUDA(cudaMemcpyAsync(&n_in, ip64.p + Nd, 8, cudaMemcpyDeviceToHost, s));
-  SG_CUDA(cudaStreamSynchronize(s));
-  net->d_in_edge.alloc(std::max<unsigned long long>(n_in, 1));
-  net->d_in_pre.alloc(std::max<unsigned long long>(n_in, 1));
-  DBuf<uint32_t> cursor;
-  cursor.alloc((size_t)Nd + 1);
-  SG_CUDA(cudaMemcpyAsync(cursor.p, net->d_in_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToDevice, s));
-  launch_grid(Nd, [&](unsigned b) {
-    csc_fill_kernel<<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_code.p, net->packed, Nd, cursor.p,
-                                      net->d_in_edge.p, net->d_in_pre.p);
-  });
-  SG_CUDA(cudaStreamSynchronize(s));
+  build_in_edges(net, 0, net->d_in_ptr, net->d_in_edge, net->d_in_pre);
   net->ln_consts.resize(4);
   net->ln_consts[2] = host_fast_exp(-net->stdp_dt / net->tau_pre);
   net->ln_consts[3] = host_fast_exp(-net->stdp_dt / net->tau_post);
@@ -1301,6 +1328,28 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
     if (net->seg32) scatter_kernel<true, false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
     else scatter_kernel<false, false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
   }
+  if (net->learn_on && net->n_edges) {
+    LearnArgs L{};
+    L.bits = net->d_last_bits.p;
+    L.row_ptr = net->d_row_ptr.p;
+    L.edge = net->d_edge.p;
+    L.packed = net->packed;
+    L.in_ptr = net->d_l_in_ptr.p;
+    L.in_edge = net->d_l_in_edge.p;
+    L.in_pre = net->d_l_in_pre.p;
+    L.tp = net->d_l_tp.p;
+    L.tq = net->d_l_tq.p;
+    L.elig = net->d_l_elig.p;
+    L.last = net->d_l_last.p;
+    L.step = net->d_step.p;
+    L.t0 = net->l_t0;
+    L.words = net->Nd / 32;
+    L.d_e = net->l_de;
+    L.a_ltp = net->l_a_ltp;
+    L.a_ltd = net->l_a_ltd;
+    const unsigned blocks = (unsigned)std::max<uint32_t>(1, std::min<uint32_t>((L.words + 7) / 8, 148u * 8u));
+    learn_elig_kernel<<<blocks, 256, 0, s>>>(L);
+  }
   if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
 }
 
@@ -1308,6 +1357,7 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
 // back after every step (adds host synchronisation; for measurement only).
 void do_steps_profiled(sg_net *net, uint32_t n) {
   upload_pop_table(net);
+  if (net->learn_on) net->d_l_motor.zero(net->stream);  // motor counts are per step call
   const StepArgs a = make_args(net);
   if (net->prof_ev.empty()) {
     net->prof_ev.resize(3);
@@ -1348,6 +1398,7 @@ void do_steps(sg_net *net, uint32_t n) {
     return;
   }
   upload_pop_table(net);
+  if (net->learn_on) net->d_l_motor.zero(net->stream);  // motor counts are per step call
   const StepArgs a = make_args(net);
   const uint32_t G = 32;  // steps per graph launch
   uint32_t done = 0;
@@ -2516,6 +2567,214 @@ int sg_clamp_hits(sg_net *net, uint64_t *out) {
   });
 }
 
+// ---------------------------------------------------------------------------
+// Dopamine-modulated eligibility learning over the built network's synapses
+// (P/api/learn/brain.rs Brain, bound to the network as
+// pillars-wgpu/src/network.rs:902-1336 step_many_learn / reward do).  The
+// synapse index is the CSR record index, the order sg_graph_read reports.
+// ---------------------------------------------------------------------------
+static void require_learn(const sg_net *net) {
+  SG_REQUIRE(net->built && net->learn_on, SG_E_STATE, "learning is not enabled");
+}
+
+static unsigned learn_blocks(uint64_t E) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((E + 255) / 256, 148u * 16u));
+}
+
+int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float tau_e, float a_ltp, float a_ltd,
+                    float lr, float w_min, float w_max) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "learning needs a built network");
+    SG_REQUIRE(!net->learn_on, SG_E_STATE, "learning is already enabled");
+    SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID, "BF16 weights are read-only: learning needs FP32 weights");
+    const float v[9] = {dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max};
+    for (float x : v) SG_REQUIRE(std::isfinite(x), SG_E_INVALID, "learning config: values must be finite");
+    SG_REQUIRE(dt > 0 && tau_pre > 0 && tau_post > 0 && tau_e > 0 && w_min <= w_max, SG_E_INVALID,
+               "learning config: dt and time constants must be positive and w_min <= w_max");
+    DevGuard g(net->device);
+    cudaStream_t s = net->stream;
+    // rewards change weights, so the exact-sum condition of the rings no
+    // longer holds: pending lists go to the rings, the ordered path takes over
+    flush_lists(net);
+    net->list_mode = 0;
+    drop_graph(net);
+    const uint32_t Nd = net->Nd;
+    const uint64_t E = net->n_edges;
+    net->l_dt = dt, net->l_tau_pre = tau_pre, net->l_tau_post = tau_post, net->l_tau_e = tau_e;
+    net->l_a_ltp = a_ltp, net->l_a_ltd = a_ltd, net->l_lr = lr, net->l_w_min = w_min, net->l_w_max = w_max;
+    // the per-step factors (brain.rs:206-208)
+    net->l_dpre = host_fast_exp(-dt / tau_pre);
+    net->l_dpost = host_fast_exp(-dt / tau_post);
+    net->l_de = host_fast_exp(-dt / tau_e);
+    net->d_l_tp.alloc(std::max<uint32_t>(Nd, 1));
+    net->d_l_tp.zero(s);
+    net->d_l_tq.alloc(std::max<uint32_t>(Nd, 1));
+    net->d_l_tq.zero(s);
+    net->d_l_elig.alloc(std::max<uint64_t>(E, 1));
+    net->d_l_elig.zero(s);
+    net->d_l_last.alloc(std::max<uint64_t>(E, 1));
+    net->d_l_last.zero(s);
+    net->d_l_motor.alloc(2);
+    net->d_l_motor.zero(s);
+    for (auto &m : net->l_motor) m = 0;
+    if (Nd) build_in_edges(net, 1, net->d_l_in_ptr, net->d_l_in_edge, net->d_l_in_pre);
+    SG_CUDA(cudaMemcpyAsync(&net->l_t0, net->d_step.p, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    net->learn_on = true;
+  });
+}
+
+int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    const float w_max = std::isfinite(w_cap) ? w_cap : net->l_w_max;
+    SG_REQUIRE(net->l_w_min <= w_max, SG_E_INVALID, "reward: weight ceiling below the floor");
+    DevGuard g(net->device);
+    // reward_gated: dopamine * gate.clamp(0, 1) (brain.rs:405-409), then lr * dopamine
+    const float gc = gate < 0.0f ? 0.0f : (gate > 1.0f ? 1.0f : gate);
+    const float dop = dopamine * gc;
+    const float lr_dopa = net->l_lr * dop;
+    const uint64_t E = net->n_edges;
+    if (E)
+      learn_reward_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p, net->d_l_elig.p, net->d_l_last.p,
+                                                                     net->d_step.p, net->l_t0, E, net->l_de, lr_dopa,
+                                                                     net->l_w_min, w_max);
+    SG_CUDA(cudaGetLastError());
+  });
+}
+
+int sg_learn_clear(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    DevGuard g(net->device);
+    const uint64_t E = net->n_edges;
+    if (E)
+      learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_elig.p, net->d_l_last.p, nullptr,
+                                                                    net->d_step.p, net->l_t0, E);
+    SG_CUDA(cudaGetLastError());
+  });
+}
+
+int sg_learn_restrict(sg_net *net, const uint8_t *keep, uint64_t n) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    const uint64_t E = net->n_edges;
+    SG_REQUIRE(n == E, SG_E_INVALID, "restrict: mask length differs from the synapse count");
+    SG_REQUIRE(keep || E == 0, SG_E_INVALID, "null mask");
+    if (!E) return;
+    DevGuard g(net->device);
+    DBuf<uint8_t> k;
+    k.alloc(E);
+    SG_CUDA(cudaMemcpyAsync(k.p, keep, E, cudaMemcpyHostToDevice, net->stream));
+    learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_elig.p, net->d_l_last.p, k.p,
+                                                                  net->d_step.p, net->l_t0, E);
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+int sg_learn_set_eligibility(sg_net *net, const float *elig, uint64_t n) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    const uint64_t E = net->n_edges;
+    SG_REQUIRE(n == E, SG_E_INVALID, "set_eligibility: length differs from the synapse count");
+    SG_REQUIRE(elig || E == 0, SG_E_INVALID, "null input");
+    if (!E) return;
+    DevGuard g(net->device);
+    SG_CUDA(cudaMemcpyAsync(net->d_l_elig.p, elig, E * 4, cudaMemcpyHostToDevice, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+// a global neuron index -> the device index of the first neuron at or after
+// it (padding neurons never fire, so ranges map exactly)
+static uint32_t dev_bound(const sg_net *net, uint64_t x) {
+  for (size_t p = 0; p < net->pops.size(); ++p)
+    if (x < (uint64_t)net->offsets[p] + net->pops[p].n) {
+      const uint64_t r = x > net->offsets[p] ? x - net->offsets[p] : 0;
+      return net->pops[p].dev_off + (uint32_t)r;
+    }
+  return net->Nd;
+}
+
+int sg_learn_motor(sg_net *net, uint64_t lo0, uint64_t hi0, uint64_t lo1, uint64_t hi1) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    net->l_motor[0] = dev_bound(net, lo0);
+    net->l_motor[1] = dev_bound(net, hi0);
+    net->l_motor[2] = dev_bound(net, lo1);
+    net->l_motor[3] = dev_bound(net, hi1);
+    drop_graph(net);
+  });
+}
+
+int sg_learn_motor_read(sg_net *net, uint32_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    SG_CUDA(cudaMemcpyAsync(out, net->d_l_motor.p, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+int sg_learn_snapshot(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    const uint64_t E = net->n_edges;
+    if (!E) return;
+    DevGuard g(net->device);
+    net->d_l_baked.alloc(E);
+    learn_baked_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p, net->d_l_baked.p, E, 0, 0.0f);
+    SG_CUDA(cudaGetLastError());
+  });
+}
+
+int sg_learn_recall(sg_net *net, float alpha) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    const uint64_t E = net->n_edges;
+    if (!E || !net->d_l_baked.n) return;  // no snapshot: nothing to pull toward (brain.rs:350-356)
+    DevGuard g(net->device);
+    learn_baked_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p, net->d_l_baked.p, E, 1, alpha);
+    SG_CUDA(cudaGetLastError());
+  });
+}
+
+int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post, uint64_t *t) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    DevGuard g(net->device);
+    cudaStream_t s = net->stream;
+    const uint64_t E = net->n_edges;
+    if (elig && E) SG_CUDA(cudaMemcpyAsync(elig, net->d_l_elig.p, E * 4, cudaMemcpyDeviceToHost, s));
+    std::vector<float> a(net->Nd), b(net->Nd);
+    if (net->Nd) {
+      SG_CUDA(cudaMemcpyAsync(a.data(), net->d_l_tp.p, a.size() * 4, cudaMemcpyDeviceToHost, s));
+      SG_CUDA(cudaMemcpyAsync(b.data(), net->d_l_tq.p, b.size() * 4, cudaMemcpyDeviceToHost, s));
+    }
+    unsigned long long step = 0;
+    SG_CUDA(cudaMemcpyAsync(&step, net->d_step.p, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      for (uint32_t i = 0; i < net->pops[p].n; ++i) {
+        if (trace_pre) trace_pre[net->offsets[p] + i] = a[net->pops[p].dev_off + i];
+        if (trace_post) trace_post[net->offsets[p] + i] = b[net->pops[p].dev_off + i];
+      }
+    if (t) *t = step - net->l_t0;
+  });
+}
+
 int sg_footprint(sg_net *net, uint64_t *out) {
   NET_CHECK(net);
   return run([&] {
@@ -2529,7 +2788,9 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
          (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4 +
          (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4 +
-         net->d_pt.n + (net->d_tm_r.n + net->d_tm_u.n + net->d_tm_last.n) * 4;
+         net->d_pt.n + (net->d_tm_r.n + net->d_tm_u.n + net->d_tm_last.n) * 4 +
+         (net->d_l_tp.n + net->d_l_tq.n + net->d_l_elig.n + net->d_l_baked.n + net->d_l_last.n + net->d_l_in_ptr.n +
+          net->d_l_in_edge.n + net->d_l_in_pre.n + net->d_l_motor.n) * 4;
     *out = b;
   });
 }

@@ -169,6 +169,14 @@ struct StepArgs {
   const uint32_t *in_edge;
   const uint32_t *in_pre;
   double *drift;
+  // dopamine-modulated eligibility learning: per-neuron traces decayed by
+  // fma with this step's spike, and spikes of two device index ranges
+  // [l_motor[0], l_motor[1]) and [l_motor[2], l_motor[3]) counted
+  int learn;
+  float *l_tp, *l_tq;
+  float l_dpre, l_dpost;
+  uint32_t l_motor[4];
+  uint32_t *l_motor_acc;
 };
 
 struct PopArgs {
@@ -486,6 +494,24 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
         a.x_pre[gi] = __fmaf_rn(a.x_pre[gi], a.d_pre, add);
         a.x_post[gi] = __fmaf_rn(a.x_post[gi], a.d_post, add);
       }
+  }
+  // learning traces (P/api/learn/brain.rs:211-222) and motor counts
+  // (pillars-wgpu/shaders/dopamine.wgsl:126-136)
+  if (a.learn) {
+    uint32_t m0 = 0, m1 = 0;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (i0 + q < p.n) {
+        const uint32_t gi = gi0 + q;
+        const bool fired = (nib >> q) & 1u;
+        const float add = fired ? 1.0f : 0.0f;
+        a.l_tp[gi] = __fmaf_rn(a.l_tp[gi], a.l_dpre, add);
+        a.l_tq[gi] = __fmaf_rn(a.l_tq[gi], a.l_dpost, add);
+        m0 += fired && gi >= a.l_motor[0] && gi < a.l_motor[1] ? 1u : 0u;
+        m1 += fired && gi >= a.l_motor[2] && gi < a.l_motor[3] ? 1u : 0u;
+      }
+    if (m0) atomicAdd(a.l_motor_acc, m0);
+    if (m1) atomicAdd(a.l_motor_acc + 1, m1);
   }
 }
 
@@ -1194,6 +1220,128 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) list_flu
   __syncthreads();
   for (uint32_t k = 0; k < a.nkeys; ++k) list_flush(list_args(a), S, k, j, p0, pj);
   if (threadIdx.x < a.nkeys) a.lcnt[j * a.nkeys + threadIdx.x] = S.lcnt[threadIdx.x];
+}
+
+// ---------------------------------------------------------------------------
+// Dopamine-modulated eligibility over the network's synapses, lazy form
+// (P/api/learn/brain.rs:199-286).  A synapse's eligibility is stored as of
+// its last sync step; each step touches only the synapses of spiking
+// neurons: the gap since the last sync decays by repeated multiplication
+// with d_e (one rounding per elapsed step, as the per-step dense update
+// does), this step's terms are added in the order the reference stages them
+// (neurons ascending, a neuron's in-edges before its out-edges), then one
+// trailing multiplication by d_e.  A synapse whose post spiked is handled
+// with its post's in-edges (with its LTD term too when its pre also
+// spiked), one whose only the pre spiked with the pre's out-edges: every
+// synapse has one owner per step, so the updates need no atomics.
+// ---------------------------------------------------------------------------
+struct LearnArgs {
+  const uint32_t *bits;     // this step's spike bitmask [Nd/32]
+  const uint32_t *row_ptr;  // out-edges (CSR, synapse index = record index)
+  const uint2 *edge;
+  int packed;
+  const uint32_t *in_ptr, *in_edge, *in_pre;  // in-edges of every neuron
+  const float *tp, *tq;                        // traces after this step's spikes
+  float *elig;
+  uint32_t *last;                              // sync step, relative to t0
+  const unsigned long long *step;
+  unsigned long long t0;
+  uint32_t words;
+  float d_e, a_ltp, a_ltd;
+};
+
+__device__ __forceinline__ bool bit_set(const uint32_t *bits, uint32_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
+
+// e decayed over n steps, one rounding per step; 0 stays 0 (of either sign)
+__device__ __forceinline__ float decay_steps(float e, uint32_t n, float d) {
+  for (uint32_t k = 0; k < n && e != 0.0f; ++k) e = __fmul_rn(e, d);
+  return e;
+}
+
+__global__ void __launch_bounds__(256) learn_elig_kernel(LearnArgs L) {
+  const uint32_t t = (uint32_t)(*L.step - L.t0);  // the step counter has advanced past this step
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t wd = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wd < L.words; wd += nw) {
+    uint32_t bits = L.bits[wd];
+    while (bits) {
+      const uint32_t n = wd * 32 + (__ffs(bits) - 1);
+      bits &= bits - 1;
+      const float ltd_n = __fmul_rn(L.a_ltd, L.tq[n]);
+      // n as post: LTP on every in-edge, LTD too where the pre fired
+      for (uint32_t k = L.in_ptr[n] + lane; k < L.in_ptr[n + 1]; k += 32) {
+        const uint32_t i = L.in_edge[k], p = L.in_pre[k];
+        const float ltp = __fmul_rn(L.a_ltp, L.tp[p]);
+        const uint32_t s = L.last[i];
+        float e = decay_steps(L.elig[i], s < t ? t - s - 1 : 0u, L.d_e);
+        if (bit_set(L.bits, p))
+          e = p < n ? __fadd_rn(__fsub_rn(e, ltd_n), ltp) : __fsub_rn(__fadd_rn(e, ltp), ltd_n);
+        else
+          e = __fadd_rn(e, ltp);
+        L.elig[i] = __fmul_rn(e, L.d_e);
+        L.last[i] = t;
+      }
+      // n as pre: LTD on out-edges whose post did not fire
+      for (uint32_t i = L.row_ptr[n] + lane; i < L.row_ptr[n + 1]; i += 32) {
+        const uint2 r = L.edge[i];
+        const uint32_t q = L.packed ? (r.x & 0x00FFFFFFu) : r.x;
+        if (bit_set(L.bits, q)) continue;
+        const uint32_t s = L.last[i];
+        float e = decay_steps(L.elig[i], s < t ? t - s - 1 : 0u, L.d_e);
+        e = __fsub_rn(e, __fmul_rn(L.a_ltd, L.tq[q]));
+        L.elig[i] = __fmul_rn(e, L.d_e);
+        L.last[i] = t;
+      }
+    }
+  }
+}
+
+// Reward (brain.rs:254-309): every eligibility brought to now, then
+// w += lr*dopamine*e clamped to [w_min, w_max]; a zero delta leaves w as it is.
+__global__ void learn_reward_kernel(uint2 *edge, float *elig, uint32_t *last, const unsigned long long *step,
+                                    unsigned long long t0, uint64_t E, float d_e, float lr_dopa, float w_min,
+                                    float w_max) {
+  const uint32_t t = (uint32_t)(*step - t0);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = last[i];
+    float e = elig[i];
+    if (s < t) {
+      if (e != 0.0f) {
+        e = decay_steps(e, t - s, d_e);
+        elig[i] = e;
+      }
+      last[i] = t;
+    }
+    const float delta = __fmul_rn(lr_dopa, e);
+    if (delta == 0.0f) continue;
+    float w = __fadd_rn(__uint_as_float(edge[i].y), delta);
+    w = w < w_min ? w_min : (w > w_max ? w_max : w);
+    edge[i].y = __float_as_uint(w);
+  }
+}
+
+// clear (brain.rs:271-275): zero and synced to now; or keep[i] == 0 zeroes
+// synapse i (restrict, brain.rs:278-285)
+__global__ void learn_clear_kernel(float *elig, uint32_t *last, const uint8_t *keep, const unsigned long long *step,
+                                   unsigned long long t0, uint64_t E) {
+  const uint32_t t = (uint32_t)(*step - t0);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (keep == nullptr) {
+      elig[i] = 0.0f;
+      last[i] = t;
+    } else if (!keep[i]) {
+      elig[i] = 0.0f;
+    }
+  }
+}
+
+// snapshot (mode 0) and recall w += alpha * (snapshot - w) (brain.rs:343-356)
+__global__ void learn_baked_kernel(uint2 *edge, float *baked, uint64_t E, int recall, float alpha) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float w = __uint_as_float(edge[i].y);
+    if (!recall) baked[i] = w;
+    else edge[i].y = __float_as_uint(__fadd_rn(w, __fmul_rn(alpha, __fsub_rn(baked[i], w))));
+  }
 }
 
 // ---------------------------------------------------------------------------

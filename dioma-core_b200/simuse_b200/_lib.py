@@ -81,6 +81,16 @@ SIGNATURES = {
     "sg_stdp_drift": [vp, vp],
     "sg_stdp_traces": [vp, vp, vp],
     "sg_clamp_hits": [vp, vp],
+    "sg_learn_enable": [vp, f32, f32, f32, f32, f32, f32, f32, f32, f32],
+    "sg_learn_reward": [vp, f32, f32, f32],
+    "sg_learn_clear": [vp],
+    "sg_learn_restrict": [vp, vp, u64],
+    "sg_learn_set_eligibility": [vp, vp, u64],
+    "sg_learn_motor": [vp, u64, u64, u64, u64],
+    "sg_learn_motor_read": [vp, vp],
+    "sg_learn_snapshot": [vp],
+    "sg_learn_recall": [vp, f32],
+    "sg_learn_read": [vp, vp, vp, vp, vp],
     "sg_footprint": [vp, vp],
     "sg_neuron_stats_enable": [vp, i32],
     "sg_neuron_stats_read": [vp, u32, vp, vp, vp, vp],

@@ -383,6 +383,54 @@ class Network:
         check(lib().sg_stdp_traces(self._h, _p(a), _p(b)))
         return a, b
 
+    # -- dopamine-modulated eligibility learning (P/api/learn/brain.rs) --------
+    def enable_learning(self, dt=0.5, tau_pre=20.0, tau_post=20.0, tau_e=1000.0, a_ltp=0.1, a_ltd=0.12, lr=1.0,
+                        w_min=0.0, w_max=1.0):
+        """Learn on the built network's synapses from this step on (StdpConfig
+        defaults, brain.rs:46-60).  Needs FP32 weights."""
+        check(lib().sg_learn_enable(self._h, dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max))
+
+    def reward(self, dopamine, gate=1.0, w_cap=None):
+        """reward / reward_gated / reward_capped (brain.rs:400-416)."""
+        check(lib().sg_learn_reward(self._h, dopamine, gate, float("nan") if w_cap is None else w_cap))
+
+    def clear_eligibility(self):
+        check(lib().sg_learn_clear(self._h))
+
+    def restrict_eligibility(self, keep):
+        k = np.ascontiguousarray(keep, dtype=np.uint8)
+        check(lib().sg_learn_restrict(self._h, _p(k), k.size))
+
+    def set_eligibility(self, elig):
+        e = np.ascontiguousarray(elig, dtype=np.float32)
+        check(lib().sg_learn_set_eligibility(self._h, _p(e), e.size))
+
+    def set_motor(self, left, right):
+        """Count the spikes of neurons [left[0], left[1]) and [right[0],
+        right[1]) over each step() call."""
+        check(lib().sg_learn_motor(self._h, left[0], left[1], right[0], right[1]))
+
+    def motor_counts(self):
+        out = np.zeros(2, np.uint32)
+        check(lib().sg_learn_motor_read(self._h, _p(out)))
+        return int(out[0]), int(out[1])
+
+    def snapshot(self):
+        check(lib().sg_learn_snapshot(self._h))
+
+    def recall(self, alpha):
+        check(lib().sg_learn_recall(self._h, alpha))
+
+    def learning_state(self):
+        """(eligibility [synapses, CSR order], pre traces, post traces, t)."""
+        E, N = self.num_synapses, self.total_neurons
+        e = np.zeros(max(E, 1), np.float32)
+        tp = np.zeros(max(N, 1), np.float32)
+        tq = np.zeros(max(N, 1), np.float32)
+        t = C.c_uint64()
+        check(lib().sg_learn_read(self._h, _p(e), _p(tp), _p(tq), C.byref(t)))
+        return e[:E], tp[:N], tq[:N], t.value
+
     @property
     def stream(self) -> int:
         out = C.c_void_p()

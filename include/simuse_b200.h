@@ -267,6 +267,37 @@ int sg_ring_read(sg_net *net, uint32_t ring, float *out);
 int sg_stdp_drift(sg_net *net, double *out);
 int sg_stdp_traces(sg_net *net, float *x_pre, float *x_post);
 int sg_clamp_hits(sg_net *net, uint64_t *out); /* i_syn values that hit the +-100 clamp */
+
+/* ---- dopamine-modulated eligibility learning ----------------------------
+   The reference's Brain (P/api/learn/brain.rs:62-418: StdpConfig, step,
+   fold_eligibility, reward_dopamine, LearnToken::reward / reward_gated /
+   reward_capped, clear/restrict/set_eligibility, snapshot/recall), bound to
+   the built network's own synapses and spikes the way
+   pillars-wgpu/src/network.rs:902-1336 (step_many_learn, reward,
+   download_motor_sums) binds it: after every step's spikes the per-neuron
+   traces decay and take the spike (fma), and the eligibility of every synapse
+   of a spiking neuron takes +a_ltp * trace_pre[pre] (as post) and
+   -a_ltd * trace_post[post] (as pre), lazily decayed by repeated
+   multiplication with exp(-dt/tau_e).  Synapse i is CSR record i (the order
+   sg_graph_read reports).  Needs FP32 weights; drops the exact-sum scatter
+   path (rewards change weights).  Learning begins at the step it is enabled. */
+int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float tau_e, float a_ltp, float a_ltd,
+                    float lr, float w_min, float w_max);
+/* w += lr * dopamine * clamp(gate, 0, 1) * e, clamped to [w_min, cap] where
+   cap = w_cap when finite (reward_capped) else w_max; zero deltas skip. */
+int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap);
+int sg_learn_clear(sg_net *net);                                       /* brain.rs:271-275 */
+int sg_learn_restrict(sg_net *net, const uint8_t *keep, uint64_t n);   /* brain.rs:278-285 */
+int sg_learn_set_eligibility(sg_net *net, const float *elig, uint64_t n); /* brain.rs:160-170 */
+/* spikes of neurons [lo0, hi0) and [lo1, hi1) counted over each sg_step call
+   (network.rs:902-955 motor sums; shaders/dopamine.wgsl:126-136) */
+int sg_learn_motor(sg_net *net, uint64_t lo0, uint64_t hi0, uint64_t lo1, uint64_t hi1);
+int sg_learn_motor_read(sg_net *net, uint32_t *out /* [2] */);
+int sg_learn_snapshot(sg_net *net);                                    /* brain.rs:343-347 */
+int sg_learn_recall(sg_net *net, float alpha);                         /* brain.rs:349-356 */
+/* eligibility [synapses] as of each synapse's last sync (Brain::eligibility),
+   traces [total_neurons], steps since learning began (Brain::t); any may be null */
+int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post, uint64_t *t);
 /* Device bytes held by this network (state + CSR + rings + scratch). */
 int sg_footprint(sg_net *net, uint64_t *out);
 /* Per-neuron spike statistics accumulated on the device from the next step

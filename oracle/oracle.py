@@ -62,6 +62,16 @@ def lib():
             "or_tm_sequence": (i32, [f32, f32, f32, i32, f32, vp, u32, vp]),
             "or_register_expone": (i32, [vp, f32, f32, f32]),
             "or_register_kinetics": (i32, [vp, i32, vp, f32, f32]),
+            "or_learn_enable": (i32, [vp, f32, f32, f32, f32, f32, f32, f32, f32, f32]),
+            "or_learn_reward": (i32, [vp, f32, f32, f32]),
+            "or_learn_clear": (i32, [vp]),
+            "or_learn_restrict": (i32, [vp, vp, u64]),
+            "or_learn_set_eligibility": (i32, [vp, vp, u64]),
+            "or_learn_motor": (i32, [vp, u64, u64, u64, u64]),
+            "or_learn_motor_read": (i32, [vp, vp]),
+            "or_learn_snapshot": (i32, [vp]),
+            "or_learn_recall": (i32, [vp, f32]),
+            "or_learn_read": (i32, [vp, vp, vp, vp, vp]),
             "or_poisson_add": (i32, [vp, f32, f32, u32]),
             "or_poisson_connect": (i32, [vp, i32, i32, vp, vp, vp, vp, u64]),
             "or_poisson_add_many": (i32, [vp, u32, f32, f32, u32]),
@@ -181,6 +191,48 @@ class Network:
 
     def register_expone(self, tau_decay, erev, dt) -> int:
         return _chk(lib().or_register_expone(self._h, tau_decay, erev, dt))
+
+    def enable_learning(self, dt=0.5, tau_pre=20.0, tau_post=20.0, tau_e=1000.0, a_ltp=0.1, a_ltd=0.12, lr=1.0,
+                        w_min=0.0, w_max=1.0):
+        _chk(lib().or_learn_enable(self._h, dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max))
+
+    def reward(self, dopamine, gate=1.0, w_cap=None):
+        _chk(lib().or_learn_reward(self._h, dopamine, gate, float("nan") if w_cap is None else w_cap))
+
+    def clear_eligibility(self):
+        _chk(lib().or_learn_clear(self._h))
+
+    def restrict_eligibility(self, keep):
+        k = np.ascontiguousarray(keep, dtype=np.uint8)
+        _chk(lib().or_learn_restrict(self._h, _p(k), k.size))
+
+    def set_eligibility(self, elig):
+        e = np.ascontiguousarray(elig, dtype=np.float32)
+        _chk(lib().or_learn_set_eligibility(self._h, _p(e), e.size))
+
+    def set_motor(self, left, right):
+        _chk(lib().or_learn_motor(self._h, left[0], left[1], right[0], right[1]))
+
+    def motor_counts(self):
+        out = np.zeros(2, np.uint32)
+        _chk(lib().or_learn_motor_read(self._h, _p(out)))
+        return int(out[0]), int(out[1])
+
+    def snapshot(self):
+        _chk(lib().or_learn_snapshot(self._h))
+
+    def recall(self, alpha):
+        _chk(lib().or_learn_recall(self._h, alpha))
+
+    def learning_state(self):
+        """(eligibility [CSR order], pre traces, post traces, t)."""
+        E, N = self.num_synapses, self.total_neurons
+        e = np.zeros(max(E, 1), np.float32)
+        tp = np.zeros(max(N, 1), np.float32)
+        tq = np.zeros(max(N, 1), np.float32)
+        t = C.c_uint64()
+        _chk(lib().or_learn_read(self._h, _p(e), _p(tp), _p(tq), C.byref(t)))
+        return e[:E], tp[:N], tq[:N], t.value
 
     def register_kinetics(self, kind, params, erev, dt) -> int:
         """kind 0 ExpOne, 1 ExpTwo, 2 Alpha, 3 ExpThree (params as in the C API)."""

@@ -442,6 +442,23 @@ struct Stdp {
   float dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max;
 };
 
+// P/api/learn/brain.rs:17-141 StdpConfig + Brain state (dopamine-modulated
+// eligibility learning over the network's own synapses, CSR order)
+struct Learn {
+  bool on = false;
+  float dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max;
+  uint64_t t = 0;
+  std::vector<float> tp, tq, elig;
+  std::vector<uint64_t> last, stamp;
+  std::vector<uint32_t> in_ptr, in_edge, pre_of;
+  std::vector<std::pair<uint32_t, float>> events;
+  std::vector<float> baked;  // snapshot of the weights (brain.rs:344-347)
+  // spikes of [lo0, hi0) and [lo1, hi1) counted since the step call began
+  // (pillars-wgpu/src/network.rs:902-955 motor sums)
+  uint64_t motor_lo[2] = {0, 0}, motor_hi[2] = {0, 0};
+  uint32_t motor[2] = {0, 0};
+};
+
 struct NetBase {
   virtual ~NetBase() {}
 };
@@ -470,13 +487,16 @@ template <typename T> struct Net : NetBase {
   std::vector<T> x_pre, x_post;
   std::vector<uint32_t> in_ptr, in_edge, in_pre;  // CSC of plastic edges
   double drift = 0.0;
+  Learn learn;
 
   T *ring_slot(uint32_t r, uint32_t slot) { return &ring[((size_t)r * kSlots + slot) * total]; }
 };
 
-// P/api/net/graph.rs:104-206 from_triplets_with_types: validate, sort by pre
-// (the reference's sort is unstable; this one is stable so that edges of one
-// row keep insertion order), count, prefix-sum a u32 row_ptr, place.
+// P/api/net/graph.rs:104-206 from_triplets_with_types: validate, sort by pre,
+// count, prefix-sum a u32 row_ptr, place.  The reference sorts by pre with an
+// unstable sort, so the order inside a row is not part of its contract; here
+// a row is ordered by post, stably (repeated (pre, post) synapses keep
+// insertion order, and with it every ring cell's summation order).
 template <typename T> int build_csr(Net<T> &net) {
   const uint64_t E = net.edges.size();
   const uint64_t N = net.total;
@@ -509,6 +529,28 @@ template <typename T> int build_csr(Net<T> &net) {
   }
   net.edges.clear();
   net.edges.shrink_to_fit();
+  std::vector<uint64_t> idx;
+  for (uint64_t i = 0; i < N; ++i) {
+    const uint64_t a = net.row_ptr[i], b = net.row_ptr[i + 1];
+    bool sorted = true;
+    for (uint64_t e = a + 1; e < b && sorted; ++e) sorted = net.col[e - 1] <= net.col[e];
+    if (sorted) continue;
+    idx.resize(b - a);
+    for (uint64_t k = 0; k < b - a; ++k) idx[k] = a + k;
+    std::stable_sort(idx.begin(), idx.end(), [&](uint64_t x, uint64_t y) { return net.col[x] < net.col[y]; });
+    auto permute = [&](auto &v) {
+      using V = typename std::decay_t<decltype(v)>::value_type;
+      std::vector<V> tmp(b - a);
+      for (uint64_t k = 0; k < b - a; ++k) tmp[k] = v[idx[k]];
+      std::copy(tmp.begin(), tmp.end(), v.begin() + a);
+    };
+    permute(net.col);
+    permute(net.w);
+    permute(net.d);
+    permute(net.st);
+    permute(net.plastic);
+    permute(net.pt);
+  }
   return 0;
 }
 
@@ -734,7 +776,54 @@ template <typename T> void net_step(Net<T> &net) {
         net.drift += (double)w1 - (double)w0;
       }
   }
+  if (net.learn.on) learn_step(net);
   net.step++;
+}
+
+// P/api/learn/brain.rs:204-286 Brain::step: traces decay and take this
+// step's spikes (fused mul_add); every spike stages an event for each of its
+// neuron's in-edges (+a_ltp * pre trace) then out-edges (-a_ltd * post
+// trace), neurons ascending; phase A brings each touched synapse's
+// eligibility from its last sync by repeated multiplication with d_e and adds
+// the events in order, phase B applies one trailing decay per touched synapse.
+template <typename T> void learn_step(Net<T> &net) {
+  Learn &L = net.learn;
+  const size_t N = net.total;
+  L.t += 1;
+  const uint64_t t = L.t;
+  const float d_pre = fast_exp_f(-L.dt / L.tau_pre), d_post = fast_exp_f(-L.dt / L.tau_post);
+  const float d_e = fast_exp_f(-L.dt / L.tau_e);
+  for (size_t n = 0; n < N; ++n) {
+    const float add = net.spikes[n] > 0 ? 1.0f : 0.0f;
+    L.tp[n] = std::fma(L.tp[n], d_pre, add);
+    L.tq[n] = std::fma(L.tq[n], d_post, add);
+    if (net.spikes[n] != 0)
+      for (int m = 0; m < 2; ++m) L.motor[m] += (n >= L.motor_lo[m] && n < L.motor_hi[m]) ? 1u : 0u;
+  }
+  L.events.clear();
+  for (size_t n = 0; n < N; ++n) {
+    if (net.spikes[n] == 0) continue;
+    for (uint32_t k = L.in_ptr[n]; k < L.in_ptr[n + 1]; ++k) {
+      const uint32_t i = L.in_edge[k];
+      L.events.push_back({i, L.a_ltp * L.tp[L.pre_of[i]]});
+    }
+    for (uint64_t e = net.row_ptr[n]; e < net.row_ptr[n + 1]; ++e)
+      L.events.push_back({(uint32_t)e, -L.a_ltd * L.tq[net.col[e]]});
+  }
+  for (auto &ev : L.events) {
+    float &e = L.elig[ev.first];
+    const uint64_t s0 = L.last[ev.first];
+    if (s0 < t) {
+      for (uint64_t k = 1; k < t - s0; ++k) e *= d_e;
+      L.last[ev.first] = t;
+    }
+    e += ev.second;
+  }
+  for (auto &ev : L.events)
+    if (L.stamp[ev.first] != t) {
+      L.stamp[ev.first] = t;
+      L.elig[ev.first] *= d_e;
+    }
 }
 
 struct Handle {
@@ -974,6 +1063,157 @@ int or_tm_sequence(float u0, float a_rec, float a_fac, int facilitation, float w
   float r = 1.0f, u = u0;
   uint32_t last = 0;
   for (uint32_t k = 0; k < n; ++k) out[k] = tm_spike(p, r, u, last, w, steps[k]);
+  return 0;
+}
+
+// Learning over the built network's synapses (Brain::new, brain.rs:106-141):
+// in-edges per post in CSR index order, traces and eligibility zero.
+int or_learn_enable(or_net *h, float dt, float tau_pre, float tau_post, float tau_e, float a_ltp, float a_ltd,
+                    float lr, float w_min, float w_max) {
+  DISPATCH(h, {
+    if (!net.built) return fail("learning needs a built network");
+    Learn &L = net.learn;
+    L = Learn{};
+    L.on = true;
+    L.dt = dt, L.tau_pre = tau_pre, L.tau_post = tau_post, L.tau_e = tau_e;
+    L.a_ltp = a_ltp, L.a_ltd = a_ltd, L.lr = lr, L.w_min = w_min, L.w_max = w_max;
+    const size_t N = net.total, E = net.col.size();
+    L.tp.assign(N, 0.0f);
+    L.tq.assign(N, 0.0f);
+    L.elig.assign(E, 0.0f);
+    L.last.assign(E, 0);
+    L.stamp.assign(E, 0);
+    L.pre_of.assign(E, 0);
+    std::vector<uint64_t> cnt(N + 1, 0);
+    for (uint64_t pre = 0; pre < N; ++pre)
+      for (uint64_t e = net.row_ptr[pre]; e < net.row_ptr[pre + 1]; ++e) {
+        L.pre_of[e] = (uint32_t)pre;
+        cnt[net.col[e]]++;
+      }
+    L.in_ptr.assign(N + 1, 0);
+    for (size_t i = 0; i < N; ++i) L.in_ptr[i + 1] = L.in_ptr[i] + (uint32_t)cnt[i];
+    L.in_edge.assign(E, 0);
+    std::vector<uint32_t> cur(L.in_ptr.begin(), L.in_ptr.end() - 1);
+    for (uint64_t e = 0; e < E; ++e) L.in_edge[cur[net.col[e]]++] = (uint32_t)e;
+  });
+  return 0;
+}
+
+// brain.rs:288-341 fold_eligibility + reward_dopamine: every eligibility is
+// brought to now by repeated multiplication, then w += lr*dopamine*e clamped to
+// [w_min, cap] (cap: w_max unless w_cap is finite); zero deltas leave w alone.
+int or_learn_reward(or_net *h, float dopamine, float gate, float w_cap) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    const float w_max = std::isfinite(w_cap) ? w_cap : L.w_max;
+    if (!(L.w_min <= w_max)) return fail("weight ceiling below the floor");
+    // reward_gated: dopamine * gate.clamp(0, 1) (brain.rs:405-409)
+    const float g = gate < 0.0f ? 0.0f : (gate > 1.0f ? 1.0f : gate);
+    const float dop = dopamine * g;
+    const float d_e = fast_exp_f(-L.dt / L.tau_e);
+    for (size_t i = 0; i < L.elig.size(); ++i) {
+      const uint64_t s0 = L.last[i];
+      if (s0 < L.t && L.elig[i] != 0.0f) {
+        for (uint64_t k = 0; k < L.t - s0; ++k) L.elig[i] *= d_e;
+        L.last[i] = L.t;
+      } else if (s0 < L.t) {
+        L.last[i] = L.t;
+      }
+    }
+    const float lr_dopa = L.lr * dop;
+    for (size_t i = 0; i < net.w.size(); ++i) {
+      const float delta = lr_dopa * L.elig[i];
+      if (delta == 0.0f) continue;
+      const float w = (float)net.w[i] + delta;
+      net.w[i] = (std::decay_t<decltype(net.w[i])>)(w < L.w_min ? L.w_min : (w > w_max ? w_max : w));
+    }
+  });
+  return 0;
+}
+
+// brain.rs:271-280 clear_eligibility: zero, synced to now
+int or_learn_clear(or_net *h) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    std::fill(L.elig.begin(), L.elig.end(), 0.0f);
+    std::fill(L.last.begin(), L.last.end(), L.t);
+  });
+  return 0;
+}
+
+// brain.rs:282-289 restrict_eligibility: keep[i] == 0 zeroes synapse i
+int or_learn_restrict(or_net *h, const uint8_t *keep, uint64_t n) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    for (uint64_t i = 0; i < n && i < L.elig.size(); ++i)
+      if (!keep[i]) L.elig[i] = 0.0f;
+  });
+  return 0;
+}
+
+// brain.rs:160-170 set_eligibility: values replaced, sync steps kept
+int or_learn_set_eligibility(or_net *h, const float *elig, uint64_t n) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    if (n != L.elig.size()) return fail("eligibility length differs from the synapse count");
+    std::copy(elig, elig + n, L.elig.begin());
+  });
+  return 0;
+}
+
+int or_learn_motor(or_net *h, uint64_t lo0, uint64_t hi0, uint64_t lo1, uint64_t hi1) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    L.motor_lo[0] = lo0, L.motor_hi[0] = hi0, L.motor_lo[1] = lo1, L.motor_hi[1] = hi1;
+  });
+  return 0;
+}
+
+int or_learn_motor_read(or_net *h, uint32_t *out) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    out[0] = L.motor[0], out[1] = L.motor[1];
+  });
+  return 0;
+}
+
+// brain.rs:343-356 snapshot / recall: w += alpha * (snapshot - w)
+int or_learn_snapshot(or_net *h) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    L.baked.assign(net.w.begin(), net.w.end());
+  });
+  return 0;
+}
+
+int or_learn_recall(or_net *h, float alpha) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    for (size_t i = 0; i < L.baked.size() && i < net.w.size(); ++i) {
+      const float w = (float)net.w[i];
+      net.w[i] = (std::decay_t<decltype(net.w[i])>)(w + alpha * (L.baked[i] - w));
+    }
+  });
+  return 0;
+}
+
+int or_learn_read(or_net *h, float *elig, float *tp, float *tq, uint64_t *t) {
+  DISPATCH(h, {
+    Learn &L = net.learn;
+    if (!L.on) return fail("learning is not enabled");
+    if (elig) std::copy(L.elig.begin(), L.elig.end(), elig);
+    if (tp) std::copy(L.tp.begin(), L.tp.end(), tp);
+    if (tq) std::copy(L.tq.begin(), L.tq.end(), tq);
+    if (t) *t = L.t;
+  });
   return 0;
 }
 
@@ -1270,6 +1510,7 @@ int or_inject(or_net *h, int pop, const uint32_t *idx, const float *v, uint64_t 
 int or_step(or_net *h, uint32_t n_steps, uint8_t *raster) {
   DISPATCH(h, {
     if (!net.built) return fail("Network::step() called before build()");
+    net.learn.motor[0] = net.learn.motor[1] = 0;
     for (uint32_t k = 0; k < n_steps; ++k) {
       net_step(net);
       if (raster)

@@ -53,6 +53,19 @@ int or_register_expone(or_net *net, float tau_decay, float erev, float dt);
 /* kind 0 ExpOne {tau_decay}, 1 ExpTwo {tau_rise, tau_decay}, 2 Alpha {tau},
    3 ExpThree {tau_rise, tau_decay1, tau_decay2, gbase1, gbase2} */
 int or_register_kinetics(or_net *net, int kind, const float *params, float erev, float dt);
+/* dopamine-modulated eligibility learning (P/api/learn/brain.rs) over the
+   built network's synapses; reward w_cap: non-finite = the config's w_max */
+int or_learn_enable(or_net *net, float dt, float tau_pre, float tau_post, float tau_e, float a_ltp,
+                    float a_ltd, float lr, float w_min, float w_max);
+int or_learn_reward(or_net *net, float dopamine, float gate, float w_cap);
+int or_learn_clear(or_net *net);
+int or_learn_restrict(or_net *net, const uint8_t *keep, uint64_t n);
+int or_learn_set_eligibility(or_net *net, const float *elig, uint64_t n);
+int or_learn_motor(or_net *net, uint64_t lo0, uint64_t hi0, uint64_t lo1, uint64_t hi1);
+int or_learn_motor_read(or_net *net, uint32_t *out);
+int or_learn_snapshot(or_net *net);
+int or_learn_recall(or_net *net, float alpha);
+int or_learn_read(or_net *net, float *elig, float *trace_pre, float *trace_post, uint64_t *t);
 int or_poisson_add(or_net *net, float rate_hz, float dt_ms, uint32_t seed);
 int or_poisson_add_many(or_net *net, uint32_t n, float rate_hz, float dt_ms, uint32_t seed0);
 int or_poisson_connect_one_to_one(or_net *net, int first, uint32_t n, int to, float w, uint8_t delay);

@@ -251,3 +251,58 @@ def tm_drive(make_net, steps=500):
         net.step(1)
         fired += net.spikes(p)
     return net, int(fired[1]), int(fired[2])
+
+
+def lcg_net(seed, n, max_out=5, max_in=10):
+    """The reference's Brain test connectome (P/api/learn/brain.rs:428-453):
+    an LCG (Knuth's MMIX constants, >> 33) gives each source 0-4 synapses to
+    random targets with weights in [0, 1); in-degree is capped at `max_in` so
+    that a scripted network's synaptic input stays below threshold."""
+    state = [seed]
+
+    def nxt():
+        state[0] = (state[0] * 6364136223846793005 + 1442695040888963407) & (2**64 - 1)
+        return state[0] >> 33
+
+    pre, post, w, indeg = [], [], [], np.zeros(n, np.int64)
+    for src in range(n):
+        for _ in range(nxt() % max_out):
+            dst = nxt() % n
+            wt = (nxt() % 1_000_000) / 1_000_000.0
+            if indeg[dst] < max_in:
+                indeg[dst] += 1
+                pre.append(src)
+                post.append(dst)
+                w.append(wt)
+    return np.array(pre, np.uint32), np.array(post, np.uint32), np.array(w, np.float32)
+
+
+def learn_scripted(make_net, n, pre, post, w, spikes, cfg, actions=None, motor=None):
+    """A network whose spikes are scripted: LIF neurons with dt = 1/tau = 1
+    (v = v_rest + input each step, no refractory time) at rest 0, threshold
+    50; a neuron fires when it is given 100 (the input clamp) through
+    inject_current, and the synaptic input alone (in-degree <= 10, weights
+    <= 4) stays below threshold.  Learning runs on the network's synapses;
+    `actions[t]` (a list of (verb, args)) is applied after step t."""
+    net = make_net()
+    p = net.add_population(LIF, n)
+    for col, v in enumerate([1.0, 1.0, 0.0, 50.0, 0.0, 0.0]):
+        net.fill_param(p, col, v)
+    net.connect(p, pre, p, post, w, np.ones(pre.size, np.uint8))
+    net.build()
+    net.enable_learning(**cfg)
+    if motor is not None:
+        net.set_motor(*motor)
+    out = []
+    for t, row in enumerate(spikes):
+        idx = np.nonzero(row)[0].astype(np.uint32)
+        if idx.size:
+            net.inject_current(p, idx, np.full(idx.size, 100.0, np.float32))
+        net.step(1)
+        got = np.asarray(net.spikes(p))
+        assert np.array_equal(got != 0, np.asarray(row) != 0), f"scripted spikes broke at step {t}"
+        for verb, args in (actions or {}).get(t, []):
+            r = getattr(net, verb)(*args)
+            if r is not None:
+                out.append((t, verb, r))
+    return net, out
