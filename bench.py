@@ -75,7 +75,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
-    ap.add_argument("--case", default="headline", choices=["headline", "kuramoto-sweep", "izh-batch", "hh-stdp"],
+    ap.add_argument("--case", default="headline", choices=["headline", "kuramoto-sweep", "izh-batch", "hh-stdp",
+                                                           "lif-learn"],
                     help="headline: the JSON line above; the others time one workload alone (also the "
                          "profiling entry points)")
     ap.add_argument("--instances", type=int, default=1024)
@@ -562,6 +563,9 @@ def run_case(args):
                                       "spike counts on"}), flush=True)
         net.close()
         return
+    if args.case == "lif-learn":
+        run_lif_learn(args, local)
+        return
     from simuse_b200 import KuramotoBatch
     from simuse_b200 import workloads as W
     sp = W.kuramoto_sweep(args.instances)
@@ -582,6 +586,62 @@ def run_case(args):
                       "workload": "Kuramoto populations, N log-uniform 256..65536, K linear 0..4, omega "
                                   "Lorentzian(0, 0.5), RK4 dt 0.01 (mean field)"}), flush=True)
     kb.close()
+
+
+def run_lif_learn(args, local):
+    """The headline LIF network with dopamine-modulated eligibility learning
+    on its synapses: the same sim steps timed without learning (exact-sum
+    rings) and with it (ordered rings + the eligibility kernel after every
+    step), then full-network rewards (every eligibility folded to now, every
+    weight updated)."""
+    import torch
+
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+    spec, name = workload(args, 0)
+    net = sg.Network(local)
+    W.build_lif(net, spec)
+    net.build()
+    net.synchronize()
+    st = torch.cuda.ExternalStream(net.stream, device=local)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    S = args.sim_steps
+    net.step(S * args.warmup)
+    mode0 = net.scatter_mode
+    ev0 = net.events_total
+    ms0 = timed(lambda: net.step(S * args.steps))
+    ev_a = net.events_total - ev0
+    net.enable_learning(dt=spec["dt"], tau_pre=20.0, tau_post=20.0, tau_e=1000.0, a_ltp=0.1, a_ltd=0.12, lr=0.01,
+                        w_min=-200.0, w_max=200.0)
+    net.step(S * args.warmup)
+    ev1 = net.events_total
+    ms1 = timed(lambda: net.step(S * args.steps))
+    ev_b = net.events_total - ev1
+    rew = [timed(lambda: net.reward(1.0)) for _ in range(max(args.steps, 3))]
+    E = net.num_synapses
+    steps = S * args.steps
+    peak, kind = measured_peak()
+    # reward: per synapse read sync step, eligibility and weight, write all three
+    r_ms = sorted(rew)[len(rew) // 2]
+    r_gbs = 24.0 * E / (r_ms / 1e3) / 1e9
+    print(json.dumps({
+        "case": args.case, "workload": name, "neurons": spec["n"], "synapses": E, "sim_steps": steps,
+        "no_learning": {"scatter": mode0, "ms_per_step": ms0 / steps, "events_per_s": ev_a / (ms0 / 1e3)},
+        "learning": {"scatter": net.scatter_mode, "ms_per_step": ms1 / steps, "events_per_s": ev_b / (ms1 / 1e3),
+                     "events_per_step": ev_b / steps},
+        "reward": {"first_ms_with_fold": rew[0], "ms": r_ms, "algorithmic_bytes_per_synapse": 24, "achieved_gbs": r_gbs, "peak_gbs": peak,
+                   "frac": r_gbs / peak, "peak_kind": kind},
+        "learn_config": "dt 0.1, tau_pre = tau_post 20, tau_e 1000, a_ltp 0.1, a_ltd 0.12, lr 0.01, w in [-200, 200]",
+    }), flush=True)
+    net.close()
 
 
 if __name__ == "__main__":

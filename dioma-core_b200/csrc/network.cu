@@ -210,8 +210,12 @@ struct sg_net {
   float l_dpre = 0, l_dpost = 0, l_de = 0;
   unsigned long long l_t0 = 0;
   uint32_t l_motor[4] = {0, 0, 0, 0};
-  DBuf<float> d_l_tp, d_l_tq, d_l_elig, d_l_baked;
-  DBuf<uint32_t> d_l_last, d_l_in_ptr, d_l_in_edge, d_l_in_pre, d_l_motor;
+  DBuf<float> d_l_tp, d_l_tq, d_l_baked, d_l_qb;
+  DBuf<uint2> d_l_st;  // per synapse {eligibility bits, sync step}
+  DBuf<uint4> d_l_qa;  // deferred long-gap synapses, kLearnBuckets x l_qcap
+  DBuf<uint32_t> d_l_in_ptr, d_l_in_edge, d_l_in_pre, d_l_motor, d_l_flat;
+  DBuf<uint32_t> d_l_ctr;  // [0] spiking neurons this step, [1] next to take, [2..] queued per bucket
+  uint32_t l_qcap = 0;
   // raster readback work buffers, kept from call to call (grow only)
   DBuf<unsigned long long> rr_cnt, rr_off;
   DBuf<uint8_t> rr_temp;
@@ -373,6 +377,8 @@ StepArgs make_args(sg_net *net) {
   a.l_dpost = net->l_dpost;
   for (int k = 0; k < 4; ++k) a.l_motor[k] = net->l_motor[k];
   a.l_motor_acc = net->d_l_motor.p;
+  a.l_flat = net->d_l_flat.p;
+  a.l_flat_cnt = net->d_l_ctr.p;
   return a;
 }
 
@@ -1316,6 +1322,7 @@ template <int M> void launch_neuron(sg_net *net, const StepArgs &a) {
 void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
   cudaStream_t s = net->stream;
   if (ev) SG_CUDA(cudaEventRecord(ev[0], s));
+  if (net->learn_on) SG_CUDA(cudaMemsetAsync(net->d_l_ctr.p, 0, net->d_l_ctr.n * 4, s));
   launch_neuron<kLIF>(net, a);
   launch_neuron<kIZH>(net, a);
   launch_neuron<kGPEA>(net, a);
@@ -1331,6 +1338,9 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
   if (net->learn_on && net->n_edges) {
     LearnArgs L{};
     L.bits = net->d_last_bits.p;
+    L.flat = net->d_l_flat.p;
+    L.flat_cnt = net->d_l_ctr.p;
+    L.grab = net->d_l_ctr.p + 1;
     L.row_ptr = net->d_row_ptr.p;
     L.edge = net->d_edge.p;
     L.packed = net->packed;
@@ -1339,16 +1349,19 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
     L.in_pre = net->d_l_in_pre.p;
     L.tp = net->d_l_tp.p;
     L.tq = net->d_l_tq.p;
-    L.elig = net->d_l_elig.p;
-    L.last = net->d_l_last.p;
+    L.st = net->d_l_st.p;
+    L.qa = net->d_l_qa.p;
+    L.qb = net->d_l_qb.p;
+    L.qcnt = net->d_l_ctr.p + 2;
+    L.qcap = net->l_qcap;
     L.step = net->d_step.p;
     L.t0 = net->l_t0;
-    L.words = net->Nd / 32;
     L.d_e = net->l_de;
     L.a_ltp = net->l_a_ltp;
     L.a_ltd = net->l_a_ltd;
-    const unsigned blocks = (unsigned)std::max<uint32_t>(1, std::min<uint32_t>((L.words + 7) / 8, 148u * 8u));
-    learn_elig_kernel<<<blocks, 256, 0, s>>>(L);
+    const unsigned blocks = 148u * (2048u / kLearnThreads);
+    learn_elig_kernel<<<blocks, kLearnThreads, 0, s>>>(L);
+    learn_decay_kernel<<<blocks, kLearnThreads, 0, s>>>(L);
   }
   if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
 }
@@ -2611,10 +2624,16 @@ int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float 
     net->d_l_tp.zero(s);
     net->d_l_tq.alloc(std::max<uint32_t>(Nd, 1));
     net->d_l_tq.zero(s);
-    net->d_l_elig.alloc(std::max<uint64_t>(E, 1));
-    net->d_l_elig.zero(s);
-    net->d_l_last.alloc(std::max<uint64_t>(E, 1));
-    net->d_l_last.zero(s);
+    net->d_l_st.alloc(std::max<uint64_t>(E, 1));
+    net->d_l_st.zero(s);
+    net->d_l_flat.alloc(std::max<uint32_t>(Nd, 1));
+    net->d_l_ctr.alloc(2 + kLearnBuckets);
+    net->d_l_ctr.zero(s);
+    // long-gap queue: per bucket room for 1/64 of the synapses (4M at most,
+    // 64K at least); a synapse that finds its bucket full decays in place
+    net->l_qcap = (uint32_t)std::min<uint64_t>(1u << 22, std::max<uint64_t>(E / 64, 1u << 16));
+    net->d_l_qa.alloc((size_t)kLearnBuckets * net->l_qcap);
+    net->d_l_qb.alloc((size_t)kLearnBuckets * net->l_qcap);
     net->d_l_motor.alloc(2);
     net->d_l_motor.zero(s);
     for (auto &m : net->l_motor) m = 0;
@@ -2638,9 +2657,9 @@ int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap) {
     const float lr_dopa = net->l_lr * dop;
     const uint64_t E = net->n_edges;
     if (E)
-      learn_reward_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p, net->d_l_elig.p, net->d_l_last.p,
-                                                                     net->d_step.p, net->l_t0, E, net->l_de, lr_dopa,
-                                                                     net->l_w_min, w_max);
+      learn_reward_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p, net->d_l_st.p, net->d_step.p,
+                                                                     net->l_t0, E, net->l_de, lr_dopa, net->l_w_min,
+                                                                     w_max);
     SG_CUDA(cudaGetLastError());
   });
 }
@@ -2652,8 +2671,8 @@ int sg_learn_clear(sg_net *net) {
     DevGuard g(net->device);
     const uint64_t E = net->n_edges;
     if (E)
-      learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_elig.p, net->d_l_last.p, nullptr,
-                                                                    net->d_step.p, net->l_t0, E);
+      learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_st.p, nullptr, net->d_step.p, net->l_t0,
+                                                                    E);
     SG_CUDA(cudaGetLastError());
   });
 }
@@ -2670,8 +2689,7 @@ int sg_learn_restrict(sg_net *net, const uint8_t *keep, uint64_t n) {
     DBuf<uint8_t> k;
     k.alloc(E);
     SG_CUDA(cudaMemcpyAsync(k.p, keep, E, cudaMemcpyHostToDevice, net->stream));
-    learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_elig.p, net->d_l_last.p, k.p,
-                                                                  net->d_step.p, net->l_t0, E);
+    learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_st.p, k.p, net->d_step.p, net->l_t0, E);
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaStreamSynchronize(net->stream));
   });
@@ -2686,7 +2704,8 @@ int sg_learn_set_eligibility(sg_net *net, const float *elig, uint64_t n) {
     SG_REQUIRE(elig || E == 0, SG_E_INVALID, "null input");
     if (!E) return;
     DevGuard g(net->device);
-    SG_CUDA(cudaMemcpyAsync(net->d_l_elig.p, elig, E * 4, cudaMemcpyHostToDevice, net->stream));
+    // eligibility into the x words of the state records; sync steps kept
+    SG_CUDA(cudaMemcpy2DAsync(net->d_l_st.p, 8, elig, 4, 4, E, cudaMemcpyHostToDevice, net->stream));
     SG_CUDA(cudaStreamSynchronize(net->stream));
   });
 }
@@ -2757,7 +2776,7 @@ int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post,
     DevGuard g(net->device);
     cudaStream_t s = net->stream;
     const uint64_t E = net->n_edges;
-    if (elig && E) SG_CUDA(cudaMemcpyAsync(elig, net->d_l_elig.p, E * 4, cudaMemcpyDeviceToHost, s));
+    if (elig && E) SG_CUDA(cudaMemcpy2DAsync(elig, 4, net->d_l_st.p, 8, 4, E, cudaMemcpyDeviceToHost, s));
     std::vector<float> a(net->Nd), b(net->Nd);
     if (net->Nd) {
       SG_CUDA(cudaMemcpyAsync(a.data(), net->d_l_tp.p, a.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -2789,8 +2808,9 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4 +
          (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4 +
          net->d_pt.n + (net->d_tm_r.n + net->d_tm_u.n + net->d_tm_last.n) * 4 +
-         (net->d_l_tp.n + net->d_l_tq.n + net->d_l_elig.n + net->d_l_baked.n + net->d_l_last.n + net->d_l_in_ptr.n +
-          net->d_l_in_edge.n + net->d_l_in_pre.n + net->d_l_motor.n) * 4;
+         (net->d_l_tp.n + net->d_l_tq.n + net->d_l_baked.n + net->d_l_qb.n + net->d_l_in_ptr.n + net->d_l_in_edge.n +
+          net->d_l_in_pre.n + net->d_l_motor.n + net->d_l_flat.n + net->d_l_ctr.n) * 4 +
+         net->d_l_st.n * 8 + net->d_l_qa.n * 16;
     *out = b;
   });
 }

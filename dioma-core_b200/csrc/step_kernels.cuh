@@ -177,6 +177,7 @@ struct StepArgs {
   float l_dpre, l_dpost;
   uint32_t l_motor[4];
   uint32_t *l_motor_acc;
+  uint32_t *l_flat, *l_flat_cnt;  // this step's spiking neurons, in any order
 };
 
 struct PopArgs {
@@ -512,6 +513,13 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
       }
     if (m0) atomicAdd(a.l_motor_acc, m0);
     if (m1) atomicAdd(a.l_motor_acc + 1, m1);
+    __shared__ uint32_t flat_base;
+    if (tid == 0) flat_base = total ? atomicAdd(a.l_flat_cnt, total) : 0u;
+    __syncthreads();
+    uint32_t pos = flat_base + before;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (nib & (1u << q)) a.l_flat[pos++] = gi0 + q;
   }
 }
 
@@ -1235,82 +1243,153 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) list_flu
 // spiked), one whose only the pre spiked with the pre's out-edges: every
 // synapse has one owner per step, so the updates need no atomics.
 // ---------------------------------------------------------------------------
+// Per synapse the state is one 8-byte record: x = eligibility (f32 bits),
+// y = the step of its last sync.
+constexpr uint32_t kLearnInline = 32;   // gaps up to this many steps decay in the gather kernel
+constexpr uint32_t kLearnBuckets = 12;  // longer ones by floor(log2(gap)) - 5, the last open-ended
+constexpr uint32_t kLearnThreads = 256;
+
 struct LearnArgs {
   const uint32_t *bits;     // this step's spike bitmask [Nd/32]
+  const uint32_t *flat;     // this step's spiking neurons
+  const uint32_t *flat_cnt;
+  uint32_t *grab;           // next entry of `flat` to take
   const uint32_t *row_ptr;  // out-edges (CSR, synapse index = record index)
   const uint2 *edge;
   int packed;
   const uint32_t *in_ptr, *in_edge, *in_pre;  // in-edges of every neuron
   const float *tp, *tq;                        // traces after this step's spikes
-  float *elig;
-  uint32_t *last;                              // sync step, relative to t0
+  uint2 *st;
+  uint4 *qa;      // deferred synapses per bucket: {synapse, e, gap | two << 31, s1}
+  float *qb;      //   and s2
+  uint32_t *qcnt;  // [kLearnBuckets]
+  uint32_t qcap;   // entries per bucket
   const unsigned long long *step;
   unsigned long long t0;
-  uint32_t words;
   float d_e, a_ltp, a_ltd;
 };
 
 __device__ __forceinline__ bool bit_set(const uint32_t *bits, uint32_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 
-// e decayed over n steps, one rounding per step; 0 stays 0 (of either sign)
-__device__ __forceinline__ float decay_steps(float e, uint32_t n, float d) {
-  for (uint32_t k = 0; k < n && e != 0.0f; ++k) e = __fmul_rn(e, d);
-  return e;
+// A synapse's update after its gap has decayed: this step's terms in the
+// reference's order (e - ltd is computed as e + (-ltd), the same IEEE result),
+// then the trailing decay.
+__device__ __forceinline__ uint2 learn_finish(float e, float s1, float s2, bool two, float d_e, uint32_t t) {
+  e = __fadd_rn(e, s1);
+  if (two) e = __fadd_rn(e, s2);
+  return make_uint2(__float_as_uint(__fmul_rn(e, d_e)), t);
 }
 
-__global__ void __launch_bounds__(256) learn_elig_kernel(LearnArgs L) {
+// Gather: CTAs take this step's spiking neurons one at a time; the threads of
+// a CTA share the neuron's synapses (in-edges, then out-edges), read each
+// one's state and terms, finish short gaps in place and queue long ones by
+// gap length for learn_decay_kernel, so that a warp there runs gaps of
+// similar length.  A synapse whose post spiked is handled with its post's
+// in-edges, one whose only the pre spiked with the pre's out-edges: every
+// synapse has one owner per step.
+__global__ void __launch_bounds__(kLearnThreads) learn_elig_kernel(LearnArgs L) {
+  __shared__ uint32_t s_n;
+  __shared__ uint32_t s_qbase[kLearnThreads / 32][kLearnBuckets];
   const uint32_t t = (uint32_t)(*L.step - L.t0);  // the step counter has advanced past this step
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t wd = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wd < L.words; wd += nw) {
-    uint32_t bits = L.bits[wd];
-    while (bits) {
-      const uint32_t n = wd * 32 + (__ffs(bits) - 1);
-      bits &= bits - 1;
-      const float ltd_n = __fmul_rn(L.a_ltd, L.tq[n]);
-      // n as post: LTP on every in-edge, LTD too where the pre fired
-      for (uint32_t k = L.in_ptr[n] + lane; k < L.in_ptr[n + 1]; k += 32) {
-        const uint32_t i = L.in_edge[k], p = L.in_pre[k];
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  const uint32_t n_spk = *L.flat_cnt;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t j = atomicAdd(L.grab, 1u);
+      s_n = j < n_spk ? L.flat[j] : 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    const uint32_t n = s_n;
+    __syncthreads();
+    if (n == 0xFFFFFFFFu) break;
+    const uint32_t k0 = L.in_ptr[n], n_in = L.in_ptr[n + 1] - k0, r0 = L.row_ptr[n];
+    const uint32_t K = n_in + (L.row_ptr[n + 1] - r0);
+    const float ltd_n = __fmul_rn(L.a_ltd, L.tq[n]);
+    for (uint32_t b0 = 0; b0 < K; b0 += kLearnThreads) {
+      const uint32_t x = b0 + threadIdx.x;
+      bool work = x < K, two = false;
+      uint32_t i = 0;
+      float s1 = 0.0f, s2 = 0.0f;
+      if (work && x < n_in) {  // n as post: LTP, and LTD where the pre fired too
+        const uint32_t k = k0 + x, p = L.in_pre[k];
+        i = L.in_edge[k];
         const float ltp = __fmul_rn(L.a_ltp, L.tp[p]);
-        const uint32_t s = L.last[i];
-        float e = decay_steps(L.elig[i], s < t ? t - s - 1 : 0u, L.d_e);
-        if (bit_set(L.bits, p))
-          e = p < n ? __fadd_rn(__fsub_rn(e, ltd_n), ltp) : __fsub_rn(__fadd_rn(e, ltp), ltd_n);
-        else
-          e = __fadd_rn(e, ltp);
-        L.elig[i] = __fmul_rn(e, L.d_e);
-        L.last[i] = t;
-      }
-      // n as pre: LTD on out-edges whose post did not fire
-      for (uint32_t i = L.row_ptr[n] + lane; i < L.row_ptr[n + 1]; i += 32) {
+        two = bit_set(L.bits, p);
+        s1 = two && p < n ? -ltd_n : ltp;
+        s2 = two && p < n ? ltp : -ltd_n;
+      } else if (work) {  // n as pre: LTD where the post did not fire
+        i = r0 + (x - n_in);
         const uint2 r = L.edge[i];
         const uint32_t q = L.packed ? (r.x & 0x00FFFFFFu) : r.x;
-        if (bit_set(L.bits, q)) continue;
-        const uint32_t s = L.last[i];
-        float e = decay_steps(L.elig[i], s < t ? t - s - 1 : 0u, L.d_e);
-        e = __fsub_rn(e, __fmul_rn(L.a_ltd, L.tq[q]));
-        L.elig[i] = __fmul_rn(e, L.d_e);
-        L.last[i] = t;
+        work = !bit_set(L.bits, q);
+        if (work) s1 = -__fmul_rn(L.a_ltd, L.tq[q]);
       }
+      float e = 0.0f;
+      uint32_t gap = 0;
+      if (work) {
+        const uint2 st = L.st[i];
+        e = __uint_as_float(st.x);
+        gap = st.y < t && e != 0.0f ? t - st.y - 1u : 0u;  // a zero stays zero under decay
+      }
+      uint32_t bk = 0xFFu;
+      if (work && gap > kLearnInline) bk = min(31u - (uint32_t)__clz(gap), 5u + kLearnBuckets - 1u) - 5u;
+      // queue long gaps, one atomic per bucket and warp
+      const uint32_t peers = __match_any_sync(0xffffffffu, bk);
+      bool queued = false;
+      if (bk != 0xFFu) {
+        const uint32_t leader = __ffs(peers) - 1;
+        if (lane == leader) s_qbase[wid][bk] = atomicAdd(L.qcnt + bk, (uint32_t)__popc(peers));
+      }
+      __syncwarp();
+      if (bk != 0xFFu) {
+        const uint32_t slot = s_qbase[wid][bk] + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+        if (slot < L.qcap) {
+          const size_t o = (size_t)bk * L.qcap + slot;
+          L.qa[o] = make_uint4(i, __float_as_uint(e), gap | (two ? 0x80000000u : 0u), __float_as_uint(s1));
+          L.qb[o] = s2;
+          queued = true;
+        }
+      }
+      __syncwarp();
+      if (work && !queued) {  // short gap (or a full queue)
+        for (uint32_t u = 0; u < gap && e != 0.0f; ++u) e = __fmul_rn(e, L.d_e);
+        L.st[i] = learn_finish(e, s1, s2, two, L.d_e, t);
+      }
+    }
+  }
+}
+
+// The queued synapses: each thread one synapse, buckets in turn.
+__global__ void __launch_bounds__(kLearnThreads) learn_decay_kernel(LearnArgs L) {
+  const uint32_t t = (uint32_t)(*L.step - L.t0);
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x, G = gridDim.x * blockDim.x;
+  for (uint32_t b = 0; b < kLearnBuckets; ++b) {
+    const uint32_t nb = min(L.qcnt[b], L.qcap);
+    for (uint32_t k = g; k < nb; k += G) {
+      const size_t o = (size_t)b * L.qcap + k;
+      const uint4 q = L.qa[o];
+      const float s2 = L.qb[o];
+      float e = __uint_as_float(q.y);
+      const uint32_t gap = q.z & 0x7FFFFFFFu;
+      for (uint32_t u = 0; u < gap && e != 0.0f; ++u) e = __fmul_rn(e, L.d_e);
+      L.st[q.x] = learn_finish(e, __uint_as_float(q.w), s2, (q.z >> 31) != 0u, L.d_e, t);
     }
   }
 }
 
 // Reward (brain.rs:254-309): every eligibility brought to now, then
 // w += lr*dopamine*e clamped to [w_min, w_max]; a zero delta leaves w as it is.
-__global__ void learn_reward_kernel(uint2 *edge, float *elig, uint32_t *last, const unsigned long long *step,
-                                    unsigned long long t0, uint64_t E, float d_e, float lr_dopa, float w_min,
-                                    float w_max) {
+__global__ void __launch_bounds__(256) learn_reward_kernel(uint2 *edge, uint2 *st, const unsigned long long *step,
+                                                           unsigned long long t0, uint64_t E, float d_e,
+                                                           float lr_dopa, float w_min, float w_max) {
   const uint32_t t = (uint32_t)(*step - t0);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t s = last[i];
-    float e = elig[i];
-    if (s < t) {
-      if (e != 0.0f) {
-        e = decay_steps(e, t - s, d_e);
-        elig[i] = e;
-      }
-      last[i] = t;
+    const uint2 s = st[i];
+    float e = __uint_as_float(s.x);
+    if (s.y < t) {
+      if (e != 0.0f)
+        for (uint32_t u = 0; u < t - s.y && e != 0.0f; ++u) e = __fmul_rn(e, d_e);
+      st[i] = make_uint2(__float_as_uint(e), t);
     }
     const float delta = __fmul_rn(lr_dopa, e);
     if (delta == 0.0f) continue;
@@ -1322,16 +1401,12 @@ __global__ void learn_reward_kernel(uint2 *edge, float *elig, uint32_t *last, co
 
 // clear (brain.rs:271-275): zero and synced to now; or keep[i] == 0 zeroes
 // synapse i (restrict, brain.rs:278-285)
-__global__ void learn_clear_kernel(float *elig, uint32_t *last, const uint8_t *keep, const unsigned long long *step,
+__global__ void learn_clear_kernel(uint2 *st, const uint8_t *keep, const unsigned long long *step,
                                    unsigned long long t0, uint64_t E) {
   const uint32_t t = (uint32_t)(*step - t0);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
-    if (keep == nullptr) {
-      elig[i] = 0.0f;
-      last[i] = t;
-    } else if (!keep[i]) {
-      elig[i] = 0.0f;
-    }
+    if (keep == nullptr) st[i] = make_uint2(0u, t);
+    else if (!keep[i]) st[i].x = 0u;
   }
 }
 
