@@ -10,6 +10,7 @@
 // its CUDA stream; it is movable, not copyable.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -39,6 +40,12 @@ inline void check(int rc) {
 
 enum class Model { Lif = SG_LIF, Izhikevich = SG_IZH, Gpea = SG_GPEA, HodgkinHuxley = SG_HH };
 using PopulationId = uint32_t;
+
+// P/api/learn/brain.rs:24-60 StdpConfig (its defaults)
+struct LearnConfig {
+  float dt = 0.5f, tau_pre = 20.0f, tau_post = 20.0f, tau_e = 1000.0f, a_ltp = 0.1f, a_ltd = 0.12f, lr = 1.0f,
+        w_min = 0.0f, w_max = 1.0f;
+};
 
 class Network {
  public:
@@ -119,6 +126,30 @@ class Network {
     uint64_t n = 0;
     check(sg_total_neurons(h_, &n));
     return n;
+  }
+  uint64_t num_synapses() const {
+    uint64_t n = 0;
+    check(sg_num_synapses(h_, &n));
+    return n;
+  }
+  std::vector<float> weights() const {
+    std::vector<float> w(num_synapses());
+    check(sg_weights_read(h_, w.data()));
+    return w;
+  }
+
+  // -- dopamine learning on the network's synapses (brain.rs Brain / LearnToken) --
+  void enable_learning(const LearnConfig &c = {}) {
+    check(sg_learn_enable(h_, c.dt, c.tau_pre, c.tau_post, c.tau_e, c.a_ltp, c.a_ltd, c.lr, c.w_min, c.w_max));
+  }
+  void reward(float dopamine) { check(sg_learn_reward(h_, dopamine, 1.0f, std::nanf(""))); }
+  void reward_gated(float dopamine, float gate) { check(sg_learn_reward(h_, dopamine, gate, std::nanf(""))); }
+  void reward_capped(float dopamine, float w_cap) { check(sg_learn_reward(h_, dopamine, 1.0f, w_cap)); }
+  void clear_eligibility() { check(sg_learn_clear(h_)); }
+  std::vector<float> eligibility() const {
+    std::vector<float> e(num_synapses());
+    check(sg_learn_read(h_, e.data(), nullptr, nullptr, nullptr));
+    return e;
   }
   sg_net *handle() const { return h_; }
 
