@@ -10,6 +10,7 @@
 // floats (P/api/net/delay.rs:26-35), ring 0 static, ring k the k-th kinetic
 // profile.  The CSR keeps the reference's u32 row_ptr/col (graph.rs:67-80),
 // f32 weights, and one code byte per edge (delay | syn_type | STDP flag).
+#include "taas.h"
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -2390,7 +2391,8 @@ int sg_events_total(sg_net *net, uint64_t *out) {
   });
 }
 
-static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *d, bool only_w) {
+static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *d, bool only_w,
+                            uint8_t *syn = nullptr) {
   const uint32_t Nd = net->Nd;
   const uint64_t E = net->n_edges;
   std::vector<uint32_t> rp(Nd + 1);
@@ -2427,6 +2429,7 @@ static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float
     const uint8_t c = net->packed ? (uint8_t)(ed[e].x >> 24) : code[e];
     col[e] = d2g[post];
     d[e] = (uint8_t)code_delay(c);
+    if (syn) syn[e] = (uint8_t)code_ring(c);
   }
 }
 
@@ -2791,6 +2794,212 @@ int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post,
         if (trace_post) trace_post[net->offsets[p] + i] = b[net->pops[p].dev_off + i];
       }
     if (t) *t = step - net->l_t0;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// .taas v2 snapshots (crates/SiMuse/crates/taas-format; the connectome
+// sections of src/python/python/taas_format.rs:16-31)
+// ---------------------------------------------------------------------------
+static void write_file(const char *path, const std::vector<uint8_t> &b) {
+  std::FILE *f = std::fopen(path, "wb");
+  if (!f) throw std::runtime_error(std::string("write ") + path + ": cannot open");
+  const size_t w = b.empty() ? 0 : std::fwrite(b.data(), 1, b.size(), f);
+  const int c = std::fclose(f);
+  if (w != b.size() || c != 0) throw std::runtime_error(std::string("write ") + path + ": short write");
+}
+
+int sg_taas_write(const char *path, const char *created, const char *game, uint32_t n, const char *const *names,
+                  const char *const *kinds, const uint64_t *counts, const void *const *data, const uint64_t *bytes,
+                  uint32_t n_meta, const char *const *keys, const char *const *values, int zstd_level) {
+  return run([&] {
+    SG_REQUIRE(path, SG_E_INVALID, "null path");
+    SG_REQUIRE(n == 0 || (names && kinds && counts && data && bytes), SG_E_INVALID, "null section arrays");
+    SG_REQUIRE(n_meta == 0 || (keys && values), SG_E_INVALID, "null metadata arrays");
+    SG_REQUIRE(zstd_level >= 0 && zstd_level <= 22, SG_E_INVALID, "zstd level: 0 (none) or 1..22");
+    taas::Writer w;
+    w.m.created = created ? created : taas::created_now();
+    if (game) {
+      w.m.has_game = true;
+      w.m.game = game;
+    }
+    for (uint32_t k = 0; k < n_meta; ++k) w.m.metadata[keys[k]] = values[k];
+    w.level = zstd_level;
+    for (uint32_t k = 0; k < n; ++k) {
+      const std::string kind = kinds[k];
+      const size_t es = taas::kind_size(kind);
+      SG_REQUIRE(es || kind == "str" || kind == "json" || kind == "blob", SG_E_INVALID, "unknown section kind " + kind);
+      SG_REQUIRE(es ? bytes[k] == counts[k] * es : bytes[k] == counts[k], SG_E_INVALID,
+                 std::string("section '") + names[k] + "': byte length does not match its count");
+      SG_REQUIRE(data[k] || bytes[k] == 0, SG_E_INVALID, "null section data");
+      w.push(names[k], kind, counts[k], data[k], bytes[k]);
+    }
+    write_file(path, w.to_bytes());
+  });
+}
+
+int sg_taas_read(const char *path, const char *name, const char *kind, void *out, uint64_t cap, uint64_t *bytes) {
+  return run([&] {
+    SG_REQUIRE(path && name && kind, SG_E_INVALID, "null argument");
+    taas::Reader r;
+    r.open(path);
+    const std::vector<uint8_t> b = r.get(name, kind);
+    if (bytes) *bytes = b.size();
+    if (out) {
+      SG_REQUIRE(cap >= b.size(), SG_E_INVALID, "output buffer too small");
+      if (!b.empty()) std::memcpy(out, b.data(), b.size());
+    }
+  });
+}
+
+int sg_taas_validate(const char *path) {
+  return run([&] {
+    SG_REQUIRE(path, SG_E_INVALID, "null path");
+    taas::Reader r;
+    r.open(path);
+    for (const auto &sct : r.m.sections) r.get(sct.name, sct.kind);
+  });
+}
+
+int sg_taas_inspect(const char *path, char *buf, uint64_t len, uint64_t *needed) {
+  return run([&] {
+    SG_REQUIRE(path, SG_E_INVALID, "null path");
+    taas::Reader r;
+    r.open(path);
+    const std::string o = std::string(".taas archive: ") + path + "\n" + r.inspect();
+    if (needed) *needed = o.size() + 1;
+    if (buf && len) {
+      const size_t k = std::min<size_t>(o.size(), (size_t)len - 1);
+      std::memcpy(buf, o.data(), k);
+      buf[k] = 0;
+    }
+  });
+}
+
+// The built network as a snapshot: row_ptr, col_indices, values (the
+// connectome sections), delays, syn_types and, while learning, eligibility.
+int sg_taas_save(sg_net *net, const char *path, const char *created, int zstd_level) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(path, SG_E_INVALID, "null path");
+    SG_REQUIRE(zstd_level >= 0 && zstd_level <= 22, SG_E_INVALID, "zstd level: 0 (none) or 1..22");
+    const uint64_t N = net->total, E = net->n_edges;
+    SG_REQUIRE(N < 0x7FFFFFFFull && E <= 0x7FFFFFFFull, SG_E_OVERFLOW,
+               "the .taas connectome sections are i32: at most 2^31 - 1 synapses and neurons");
+    DevGuard g(net->device);
+    flush_lists(net);
+    std::vector<uint32_t> rp(N + 1), col(E);
+    std::vector<float> w(E);
+    std::vector<uint8_t> d(E), st(E);
+    read_csr_global(net, rp.data(), col.data(), w.data(), d.data(), false, st.data());
+    unsigned long long step = 0;
+    SG_CUDA(cudaMemcpyAsync(&step, net->d_step.p, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    taas::Writer wr;
+    wr.m.created = created ? created : taas::created_now();
+    wr.m.has_game = true;
+    wr.m.game = "dioma";
+    wr.m.metadata["type"] = "Network";
+    wr.m.metadata["n_neurons"] = std::to_string(N);
+    wr.m.metadata["n_synapses"] = std::to_string(E);
+    wr.m.metadata["step"] = std::to_string(step);
+    wr.level = zstd_level;
+    wr.push("row_ptr", "i32", N + 1, rp.data(), (N + 1) * 4);
+    wr.push("col_indices", "i32", E, col.data(), E * 4);
+    wr.push("values", "f32", E, w.data(), E * 4);
+    wr.push("delays", "u8", E, d.data(), E);
+    wr.push("syn_types", "u8", E, st.data(), E);
+    if (net->learn_on) {
+      std::vector<float> el(E);
+      if (E)
+        SG_CUDA(cudaMemcpy2DAsync(el.data(), 4, net->d_l_st.p, 8, 4, E, cudaMemcpyDeviceToHost, net->stream));
+      SG_CUDA(cudaStreamSynchronize(net->stream));
+      wr.push("eligibility", "f32", E, el.data(), E * 4);
+    }
+    write_file(path, wr.to_bytes());
+  });
+}
+
+// Resume: the snapshot's weights into the built network, whose synapses
+// (row_ptr, col_indices) must be the snapshot's.  The exact-sum scatter path
+// is left for the ordered one (the new weights are not checked for it).
+int sg_taas_load_weights(sg_net *net, const char *path) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(path, SG_E_INVALID, "null path");
+    SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID, "BF16 weights are read-only: loading needs FP32 weights");
+    taas::Reader r;
+    r.open(path);
+    const uint64_t N = net->total, E = net->n_edges;
+    const std::vector<uint8_t> rp = r.get("row_ptr", "i32"), col = r.get("col_indices", "i32"),
+                               vals = r.get("values", "f32");
+    SG_REQUIRE(rp.size() == (N + 1) * 4 && col.size() == E * 4 && vals.size() == E * 4, SG_E_INVALID,
+               "snapshot size differs from the network (neurons or synapses)");
+    DevGuard g(net->device);
+    std::vector<uint32_t> nrp(N + 1), ncol(E);
+    std::vector<float> w(E);
+    std::vector<uint8_t> d(E);
+    read_csr_global(net, nrp.data(), ncol.data(), w.data(), d.data(), false);
+    SG_REQUIRE(std::memcmp(rp.data(), nrp.data(), rp.size()) == 0 &&
+                   (E == 0 || std::memcmp(col.data(), ncol.data(), col.size()) == 0),
+               SG_E_INVALID, "snapshot synapses (row_ptr, col_indices) differ from the network's");
+    flush_lists(net);
+    net->list_mode = 0;
+    drop_graph(net);
+    if (E)
+      SG_CUDA(cudaMemcpy2DAsync((char *)net->d_edge.p + 4, 8, vals.data(), 4, 4, E, cudaMemcpyHostToDevice,
+                                net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
+// Synapses from a .taas CSR (a saved network or the reference's connectome
+// sections): row i of the file is neuron i of population `from`, column j
+// neuron j of `to`; delays and syn_types sections when present, else
+// `default_delay` and type 0.
+int sg_connect_taas(sg_net *net, uint32_t from, uint32_t to, const char *path, uint8_t default_delay) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(path, SG_E_INVALID, "null path");
+    require_pop(net, from);
+    require_pop(net, to);
+    taas::Reader r;
+    r.open(path);
+    const std::vector<uint8_t> rpb = r.get("row_ptr", "i32"), colb = r.get("col_indices", "i32"),
+                               wb = r.get("values", "f32");
+    const size_t rows = rpb.size() / 4, E = colb.size() / 4;
+    SG_REQUIRE(rows == (size_t)net->pops[from].n + 1, SG_E_INVALID,
+               "row_ptr length " + std::to_string(rows) + " != source population size + 1");
+    SG_REQUIRE(wb.size() / 4 == E, SG_E_INVALID, "values and col_indices differ in length");
+    std::vector<int32_t> rp(rows), col(E);
+    std::memcpy(rp.data(), rpb.data(), rpb.size());
+    if (E) std::memcpy(col.data(), colb.data(), colb.size());
+    SG_REQUIRE(rp[0] == 0 && (uint64_t)rp[rows - 1] == E, SG_E_INVALID, "row_ptr does not span col_indices");
+    std::vector<uint32_t> pre(E), post(E);
+    for (size_t i = 0; i + 1 < rows; ++i) {
+      SG_REQUIRE(rp[i] <= rp[i + 1], SG_E_INVALID, "row_ptr is not monotone");
+      for (int32_t e = rp[i]; e < rp[i + 1]; ++e) pre[e] = (uint32_t)i;
+    }
+    for (size_t e = 0; e < E; ++e) {
+      SG_REQUIRE(col[e] >= 0, SG_E_INVALID, "negative column index");
+      post[e] = (uint32_t)col[e];
+    }
+    std::vector<uint8_t> d(E, default_delay), st;
+    if (r.find("delays")) {
+      d = r.get("delays", "u8");
+      SG_REQUIRE(d.size() == E, SG_E_INVALID, "delays and col_indices differ in length");
+    }
+    if (r.find("syn_types")) {
+      st = r.get("syn_types", "u8");
+      SG_REQUIRE(st.size() == E, SG_E_INVALID, "syn_types and col_indices differ in length");
+    }
+    std::vector<float> w(E);
+    if (E) std::memcpy(w.data(), wb.data(), wb.size());
+    const int rc = connect_impl(net, from, pre.data(), to, post.data(), w.data(), d.data(),
+                                st.empty() ? nullptr : st.data(), nullptr, E, 0);
+    if (rc != SG_OK) throw Fail{rc};
   });
 }
 

@@ -19,3 +19,4 @@ from .network import (  # noqa: F401
     Network,
 )
 from .kuramoto import KuramotoBatch  # noqa: F401,E402
+from . import taas  # noqa: F401,E402

@@ -91,6 +91,13 @@ SIGNATURES = {
     "sg_learn_snapshot": [vp],
     "sg_learn_recall": [vp, f32],
     "sg_learn_read": [vp, vp, vp, vp, vp],
+    "sg_taas_write": [vp, vp, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32],
+    "sg_taas_read": [vp, vp, vp, vp, u64, vp],
+    "sg_taas_validate": [vp],
+    "sg_taas_inspect": [vp, vp, u64, vp],
+    "sg_taas_save": [vp, vp, vp, i32],
+    "sg_taas_load_weights": [vp, vp],
+    "sg_connect_taas": [vp, u32, u32, vp, u8],
     "sg_footprint": [vp, vp],
     "sg_neuron_stats_enable": [vp, i32],
     "sg_neuron_stats_read": [vp, u32, vp, vp, vp, vp],

@@ -431,6 +431,20 @@ class Network:
         check(lib().sg_learn_read(self._h, _p(e), _p(tp), _p(tq), C.byref(t)))
         return e[:E], tp[:N], tq[:N], t.value
 
+    # -- .taas v2 snapshots ------------------------------------------------------
+    def save_taas(self, path, created=None, zstd_level=0):
+        """Checkpoint: CSR synapses and weights (and eligibility while learning)."""
+        check(lib().sg_taas_save(self._h, str(path).encode(), created.encode() if created is not None else None,
+                                 int(zstd_level)))
+
+    def load_weights_taas(self, path):
+        """Resume: a snapshot's weights into this built network (same synapses)."""
+        check(lib().sg_taas_load_weights(self._h, str(path).encode()))
+
+    def connect_taas(self, from_pop, to_pop, path, default_delay=1):
+        """Synapses from a .taas CSR (row i = neuron i of from_pop)."""
+        check(lib().sg_connect_taas(self._h, from_pop, to_pop, str(path).encode(), int(default_delay)))
+
     @property
     def stream(self) -> int:
         out = C.c_void_p()

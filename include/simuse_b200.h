@@ -298,6 +298,35 @@ int sg_learn_recall(sg_net *net, float alpha);                         /* brain.
 /* eligibility [synapses] as of each synapse's last sync (Brain::eligibility),
    traces [total_neurons], steps since learning began (Brain::t); any may be null */
 int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post, uint64_t *t);
+
+/* ---- .taas v2 snapshots --------------------------------------------------
+   The reference's container (crates/SiMuse/crates/taas-format:
+   TaasWriter::push/to_bytes writer.rs:75-147, TaasReader::get_* /
+   validate reader.rs:161-281, inspect_taas inspect.rs:5-53): magic "TAAS2",
+   u64 LE manifest length, compact JSON manifest, section payloads, CRC32 per
+   section over its uncompressed bytes, optional zstd (level 1..22; 0 = none;
+   libzstd.so.1 loaded at run time).  The same sections and `created` give
+   the same bytes as the reference's writer (uncompressed).  No GPU needed. */
+int sg_taas_write(const char *path, const char *created /* null: clock */, const char *game /* null: none */,
+                  uint32_t n_sections, const char *const *names, const char *const *kinds /* f32 i32 i64 u64
+                  u8 str json blob */, const uint64_t *counts, const void *const *data, const uint64_t *bytes,
+                  uint32_t n_meta, const char *const *keys, const char *const *values, int zstd_level);
+/* uncompressed, CRC-checked bytes of a section of that kind; out may be null
+   (size query via *bytes) */
+int sg_taas_read(const char *path, const char *name, const char *kind, void *out, uint64_t cap, uint64_t *bytes);
+int sg_taas_validate(const char *path);                             /* every section's CRC */
+int sg_taas_inspect(const char *path, char *buf, uint64_t len, uint64_t *needed);
+/* The built network as a snapshot (checkpoint): sections row_ptr, col_indices,
+   values (the connectome sections of src/python/python/taas_format.rs:16-31),
+   delays, syn_types, and eligibility while learning; metadata type, n_neurons,
+   n_synapses, step; game "dioma". */
+int sg_taas_save(sg_net *net, const char *path, const char *created, int zstd_level);
+/* Resume: the snapshot's values as the built network's weights (its row_ptr
+   and col_indices must be the network's; FP32 weights; ordered scatter path). */
+int sg_taas_load_weights(sg_net *net, const char *path);
+/* Builder: synapses from a .taas CSR, row i = neuron i of `from`, column j =
+   neuron j of `to`; delays / syn_types sections when present. */
+int sg_connect_taas(sg_net *net, uint32_t from, uint32_t to, const char *path, uint8_t default_delay);
 /* Device bytes held by this network (state + CSR + rings + scratch). */
 int sg_footprint(sg_net *net, uint64_t *out);
 /* Per-neuron spike statistics accumulated on the device from the next step

@@ -90,6 +90,7 @@ def lib():
             "or_ring_read": (i32, [vp, i32, vp]),
             "or_graph_read": (i32, [vp, vp, vp, vp, vp]),
             "or_weights_read": (i32, [vp, vp]),
+            "or_weights_write": (i32, [vp, vp, u64]),
             "or_stdp_drift": (f64, [vp]),
             "or_traces_read": (i32, [vp, vp, vp]),
             "or_fast_exp": (f32, [f32]),
@@ -338,6 +339,10 @@ class Network:
         w = np.empty(self.num_synapses, np.float32)
         _chk(lib().or_weights_read(self._h, _p(w)))
         return w
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _chk(lib().or_weights_write(self._h, _p(w), w.size))
 
     @property
     def stdp_drift(self) -> float:

@@ -1585,6 +1585,16 @@ int or_weights_read(or_net *h, float *w) {
   return 0;
 }
 
+// Restore CSR weights (a checkpoint's values section) into the built network.
+int or_weights_write(or_net *h, const float *w, uint64_t n) {
+  DISPATCH(h, {
+    if (!net.built) return fail("not built");
+    if (n != net.w.size()) return fail("weight count differs from the synapse count");
+    for (size_t i = 0; i < net.w.size(); ++i) net.w[i] = (std::decay_t<decltype(net.w[i])>)w[i];
+  });
+  return 0;
+}
+
 double or_stdp_drift(const or_net *h) {
   double r = 0;
   DISPATCH(h, { r = net.drift; });

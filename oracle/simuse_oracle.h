@@ -95,6 +95,7 @@ uint64_t or_events(const or_net *net); /* synaptic events pushed so far */
 int or_ring_read(or_net *net, int ring, float *out); /* ring 0 static, k = kinetic k */
 int or_graph_read(or_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *delay);
 int or_weights_read(or_net *net, float *w); /* current CSR weights (STDP) */
+int or_weights_write(or_net *net, const float *w, uint64_t n);
 double or_stdp_drift(const or_net *net);
 int or_traces_read(or_net *net, float *x_pre, float *x_post);
 int or_set_threads(int n);
