@@ -76,7 +76,7 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--case", default="headline", choices=["headline", "kuramoto-sweep", "izh-batch", "hh-stdp",
-                                                           "lif-learn"],
+                                                           "lif-learn", "taas"],
                     help="headline: the JSON line above; the others time one workload alone (also the "
                          "profiling entry points)")
     ap.add_argument("--instances", type=int, default=1024)
@@ -566,6 +566,9 @@ def run_case(args):
     if args.case == "lif-learn":
         run_lif_learn(args, local)
         return
+    if args.case == "taas":
+        run_taas(args, local)
+        return
     from simuse_b200 import KuramotoBatch
     from simuse_b200 import workloads as W
     sp = W.kuramoto_sweep(args.instances)
@@ -641,6 +644,45 @@ def run_lif_learn(args, local):
                    "frac": r_gbs / peak, "peak_kind": kind},
         "learn_config": "dt 0.1, tau_pre = tau_post 20, tau_e 1000, a_ltp 0.1, a_ltd 0.12, lr 0.01, w in [-200, 200]",
     }), flush=True)
+    net.close()
+
+
+def run_taas(args, local):
+    """Checkpoint and resume of the LIF network through .taas v2 files:
+    sg_taas_save (device CSR to host, CRC32, file), validate (every CRC),
+    sg_taas_load_weights (file, CRC32, synapse check, weights to the device);
+    wall-clock, best of --steps runs."""
+    import tempfile
+    import time
+
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+    spec, name = workload(args, 0)
+    net = sg.Network(local)
+    W.build_lif(net, spec)
+    net.build()
+    net.synchronize()
+    out = {"case": args.case, "workload": name, "synapses": net.num_synapses}
+    with tempfile.TemporaryDirectory() as td:
+        for level in (0, 3):
+            path = os.path.join(td, f"net{level}.taas")
+            ts, tv, tl = [], [], []
+            for _ in range(max(args.steps, 1)):
+                t0 = time.perf_counter()
+                net.save_taas(path, zstd_level=level)
+                t1 = time.perf_counter()
+                sg.taas.validate(path)
+                t2 = time.perf_counter()
+                net.load_weights_taas(path)
+                net.synchronize()
+                t3 = time.perf_counter()
+                ts.append(t1 - t0)
+                tv.append(t2 - t1)
+                tl.append(t3 - t2)
+            size = os.path.getsize(path)
+            out[f"zstd{level}"] = {"file_bytes": size, "save_s": min(ts), "validate_s": min(tv), "load_s": min(tl),
+                                   "save_gbs": size / min(ts) / 1e9, "load_gbs": size / min(tl) / 1e9}
+    print(json.dumps(out), flush=True)
     net.close()
 
 
