@@ -2801,14 +2801,6 @@ int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post,
 // .taas v2 snapshots (crates/SiMuse/crates/taas-format; the connectome
 // sections of src/python/python/taas_format.rs:16-31)
 // ---------------------------------------------------------------------------
-static void write_file(const char *path, const std::vector<uint8_t> &b) {
-  std::FILE *f = std::fopen(path, "wb");
-  if (!f) throw std::runtime_error(std::string("write ") + path + ": cannot open");
-  const size_t w = b.empty() ? 0 : std::fwrite(b.data(), 1, b.size(), f);
-  const int c = std::fclose(f);
-  if (w != b.size() || c != 0) throw std::runtime_error(std::string("write ") + path + ": short write");
-}
-
 int sg_taas_write(const char *path, const char *created, const char *game, uint32_t n, const char *const *names,
                   const char *const *kinds, const uint64_t *counts, const void *const *data, const uint64_t *bytes,
                   uint32_t n_meta, const char *const *keys, const char *const *values, int zstd_level) {
@@ -2834,7 +2826,7 @@ int sg_taas_write(const char *path, const char *created, const char *game, uint3
       SG_REQUIRE(data[k] || bytes[k] == 0, SG_E_INVALID, "null section data");
       w.push(names[k], kind, counts[k], data[k], bytes[k]);
     }
-    write_file(path, w.to_bytes());
+    w.write(path);
   });
 }
 
@@ -2917,7 +2909,7 @@ int sg_taas_save(sg_net *net, const char *path, const char *created, int zstd_le
       SG_CUDA(cudaStreamSynchronize(net->stream));
       wr.push("eligibility", "f32", E, el.data(), E * 4);
     }
-    write_file(path, wr.to_bytes());
+    wr.write(path);
   });
 }
 

@@ -7,7 +7,6 @@
 #include <cstdio>
 #include <cstring>
 #include <ctime>
-#include <fstream>
 #include <stdexcept>
 
 namespace sg {
@@ -407,25 +406,49 @@ void Writer::push(const std::string &name, const std::string &kind, uint64_t cou
   m.sections.push_back(s);
 }
 
-std::vector<uint8_t> Writer::to_bytes() const {
+std::vector<uint8_t> Writer::head() const {
   const std::string h = manifest_json(m);
   std::vector<uint8_t> out;
-  out.reserve(13 + h.size() + payload.size());
+  out.reserve(13 + h.size());
   out.insert(out.end(), {'T', 'A', 'A', 'S', '2'});
   const uint64_t n = h.size();
   for (int k = 0; k < 8; ++k) out.push_back((uint8_t)(n >> (8 * k)));
   out.insert(out.end(), h.begin(), h.end());
+  return out;
+}
+
+std::vector<uint8_t> Writer::to_bytes() const {
+  std::vector<uint8_t> out = head();
   out.insert(out.end(), payload.begin(), payload.end());
   return out;
+}
+
+void Writer::write(const std::string &path) const {
+  const std::vector<uint8_t> h = head();
+  std::FILE *f = std::fopen(path.c_str(), "wb");
+  if (!f) throw std::runtime_error("write " + path + ": cannot open");
+  bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
+  ok = ok && (payload.empty() || std::fwrite(payload.data(), 1, payload.size(), f) == payload.size());
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) throw std::runtime_error("write " + path + ": short write");
 }
 
 // ---------------------------------------------------------------------------
 // reader (reader.rs:32-281)
 // ---------------------------------------------------------------------------
 void Reader::open(const std::string &path) {
-  std::ifstream f(path, std::ios::binary);
+  std::FILE *f = std::fopen(path.c_str(), "rb");
   if (!f) throw std::runtime_error("Cannot open file: " + path);
-  std::vector<uint8_t> b((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  std::vector<uint8_t> b;
+  bool ok = std::fseek(f, 0, SEEK_END) == 0;
+  const long n = ok ? std::ftell(f) : -1;
+  ok = ok && n >= 0 && std::fseek(f, 0, SEEK_SET) == 0;
+  if (ok) {
+    b.resize((size_t)n);
+    ok = n == 0 || std::fread(b.data(), 1, (size_t)n, f) == (size_t)n;
+  }
+  std::fclose(f);
+  if (!ok) throw std::runtime_error("Cannot read file: " + path);
   parse(std::move(b));
 }
 

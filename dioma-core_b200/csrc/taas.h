@@ -46,7 +46,9 @@ class Writer {
   std::vector<uint8_t> payload;
   int level = 0;  // zstd level for the next sections, 0 = none
   void push(const std::string &name, const std::string &kind, uint64_t count, const void *data, size_t bytes);
-  std::vector<uint8_t> to_bytes() const;
+  std::vector<uint8_t> head() const;      // magic, length, manifest
+  std::vector<uint8_t> to_bytes() const;  // head + payload
+  void write(const std::string &path) const;
 };
 
 class Reader {
