@@ -1271,6 +1271,18 @@ struct LearnArgs {
 
 __device__ __forceinline__ bool bit_set(const uint32_t *bits, uint32_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
 
+// e multiplied by d, g times, one rounding each (the reference's gap loop);
+// zero stays zero (of its sign), so the chain may stop there.  Chunks of 16
+// keep the loop overhead off the dependent multiplications.
+__device__ __forceinline__ float decay_by(float e, uint32_t g, float d) {
+  for (; g >= 16u && e != 0.0f; g -= 16u) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) e = __fmul_rn(e, d);
+  }
+  for (; g && e != 0.0f; --g) e = __fmul_rn(e, d);
+  return e;
+}
+
 // A synapse's update after its gap has decayed: this step's terms in the
 // reference's order (e - ltd is computed as e + (-ltd), the same IEEE result),
 // then the trailing decay.
@@ -1352,7 +1364,7 @@ __global__ void __launch_bounds__(kLearnThreads) learn_elig_kernel(LearnArgs L) 
       }
       __syncwarp();
       if (work && !queued) {  // short gap (or a full queue)
-        for (uint32_t u = 0; u < gap && e != 0.0f; ++u) e = __fmul_rn(e, L.d_e);
+        e = decay_by(e, gap, L.d_e);
         L.st[i] = learn_finish(e, s1, s2, two, L.d_e, t);
       }
     }
@@ -1369,9 +1381,7 @@ __global__ void __launch_bounds__(kLearnThreads) learn_decay_kernel(LearnArgs L)
       const size_t o = (size_t)b * L.qcap + k;
       const uint4 q = L.qa[o];
       const float s2 = L.qb[o];
-      float e = __uint_as_float(q.y);
-      const uint32_t gap = q.z & 0x7FFFFFFFu;
-      for (uint32_t u = 0; u < gap && e != 0.0f; ++u) e = __fmul_rn(e, L.d_e);
+      const float e = decay_by(__uint_as_float(q.y), q.z & 0x7FFFFFFFu, L.d_e);
       L.st[q.x] = learn_finish(e, __uint_as_float(q.w), s2, (q.z >> 31) != 0u, L.d_e, t);
     }
   }
@@ -1387,8 +1397,7 @@ __global__ void __launch_bounds__(256) learn_reward_kernel(uint2 *edge, uint2 *s
     const uint2 s = st[i];
     float e = __uint_as_float(s.x);
     if (s.y < t) {
-      if (e != 0.0f)
-        for (uint32_t u = 0; u < t - s.y && e != 0.0f; ++u) e = __fmul_rn(e, d_e);
+      e = decay_by(e, t - s.y, d_e);
       st[i] = make_uint2(__float_as_uint(e), t);
     }
     const float delta = __fmul_rn(lr_dopa, e);
