@@ -2835,12 +2835,8 @@ int sg_taas_read(const char *path, const char *name, const char *kind, void *out
     SG_REQUIRE(path && name && kind, SG_E_INVALID, "null argument");
     taas::Reader r;
     r.open(path);
-    const std::vector<uint8_t> b = r.get(name, kind);
-    if (bytes) *bytes = b.size();
-    if (out) {
-      SG_REQUIRE(cap >= b.size(), SG_E_INVALID, "output buffer too small");
-      if (!b.empty()) std::memcpy(out, b.data(), b.size());
-    }
+    const uint64_t n = r.get_into(name, kind, out, cap);  // out null: size only
+    if (bytes) *bytes = n;
   });
 }
 
@@ -2849,7 +2845,11 @@ int sg_taas_validate(const char *path) {
     SG_REQUIRE(path, SG_E_INVALID, "null path");
     taas::Reader r;
     r.open(path);
-    for (const auto &sct : r.m.sections) r.get(sct.name, sct.kind);
+    std::vector<uint8_t> buf;
+    for (const auto &sct : r.m.sections) {
+      buf.resize((size_t)r.get_into(sct.name, sct.kind, nullptr, 0));
+      r.get_into(sct.name, sct.kind, buf.data(), buf.size());
+    }
   });
 }
 
@@ -2902,8 +2902,9 @@ int sg_taas_save(sg_net *net, const char *path, const char *created, int zstd_le
     wr.push("values", "f32", E, w.data(), E * 4);
     wr.push("delays", "u8", E, d.data(), E);
     wr.push("syn_types", "u8", E, st.data(), E);
+    std::vector<float> el;  // sections are borrowed until the file is written
     if (net->learn_on) {
-      std::vector<float> el(E);
+      el.resize(E);
       if (E)
         SG_CUDA(cudaMemcpy2DAsync(el.data(), 4, net->d_l_st.p, 8, 4, E, cudaMemcpyDeviceToHost, net->stream));
       SG_CUDA(cudaStreamSynchronize(net->stream));

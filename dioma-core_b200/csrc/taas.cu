@@ -7,7 +7,9 @@
 #include <cstdio>
 #include <cstring>
 #include <ctime>
+#include <algorithm>
 #include <stdexcept>
+#include <thread>
 
 namespace sg {
 namespace taas {
@@ -18,7 +20,7 @@ namespace taas {
 // per table round (slicing-by-8: table k advances a byte's remainder through
 // k further zero bytes)
 // ---------------------------------------------------------------------------
-uint32_t crc32(const uint8_t *p, size_t n) {
+static uint32_t crc32_serial(const uint8_t *p, size_t n) {
   static const auto T = [] {
     std::vector<uint32_t> t(8 * 256);
     for (uint32_t i = 0; i < 256; ++i) {
@@ -43,6 +45,49 @@ uint32_t crc32(const uint8_t *p, size_t n) {
   }
   for (; n; ++p, --n) c = t[(c ^ *p) & 0xFFu] ^ (c >> 8);
   return c ^ 0xFFFFFFFFu;
+}
+
+// Polynomials over GF(2) modulo the CRC polynomial, in the reflected bit
+// order of the remainder (bit 31 = x^0): a*b mod P.
+static uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
+  uint32_t prod = 0;
+  for (uint32_t m = 1u << 31; m; m >>= 1) {
+    if (a & m) prod ^= b;
+    b = (b & 1u) ? (b >> 1) ^ 0xEDB88320u : b >> 1;  // b *= x
+  }
+  return prod;
+}
+
+// CRC of A||B from crc(A), crc(B) and |B|: crc(A) times x^(8|B|) mod P, plus
+// crc(B) (the pre and post conditioning cancel between the two).
+static uint32_t crc32_combine(uint32_t ca, uint32_t cb, uint64_t nb) {
+  uint32_t xp = 1u << 31;  // x^0
+  uint32_t sq = 1u << 30;  // x^1, squared below to x^(2^k)
+  for (uint64_t e = nb * 8; e; e >>= 1) {
+    if (e & 1u) xp = gf2_mulmod(xp, sq);
+    sq = gf2_mulmod(sq, sq);
+  }
+  return gf2_mulmod(ca, xp) ^ cb;
+}
+
+uint32_t crc32(const uint8_t *p, size_t n) {
+  const size_t min_chunk = 4u << 20;
+  unsigned T = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  T = (unsigned)std::min<size_t>(T, n / min_chunk);
+  if (T <= 1) return crc32_serial(p, n);
+  std::vector<uint32_t> c(T);
+  std::vector<size_t> len(T);
+  std::vector<std::thread> th;
+  const size_t chunk = n / T;
+  for (unsigned k = 0; k < T; ++k) {
+    const size_t a = k * chunk;
+    len[k] = k + 1 == T ? n - a : chunk;
+    th.emplace_back([&, k, a] { c[k] = crc32_serial(p + a, len[k]); });
+  }
+  for (auto &x : th) x.join();
+  uint32_t r = c[0];
+  for (unsigned k = 1; k < T; ++k) r = crc32_combine(r, c[k], len[k]);
+  return r;
 }
 
 // types.rs:58-67
@@ -383,26 +428,31 @@ void Writer::push(const std::string &name, const std::string &kind, uint64_t cou
   s.name = name;
   s.kind = kind;
   s.count = count;
-  s.offset = payload.size();
+  s.offset = offset_;
   s.has_crc = true;
   s.crc = crc32((const uint8_t *)data, bytes);
   const Zstd *z = level > 0 ? zstd() : nullptr;
   if (level > 0 && !z) throw std::runtime_error("zstd compression requested but libzstd.so.1 is not available");
+  Part part;
+  part.p = (const uint8_t *)data;
+  part.n = bytes;
+  s.size = bytes;
   if (z) {
     std::vector<uint8_t> c(z->bound(bytes));
     const size_t r = z->compress(c.data(), c.size(), data, bytes, level);
-    if (!z->is_error(r)) {
+    if (!z->is_error(r)) {  // the reference stores a section as is when compression fails
+      c.resize(r);
+      part.own = std::move(c);
+      part.p = nullptr;
+      part.n = r;
       s.size = r;
       s.compression = "zstd";
       s.has_usize = true;
       s.usize = bytes;
-      payload.insert(payload.end(), c.begin(), c.begin() + (ptrdiff_t)r);
-      m.sections.push_back(s);
-      return;
     }
   }
-  s.size = bytes;
-  payload.insert(payload.end(), (const uint8_t *)data, (const uint8_t *)data + bytes);
+  offset_ += s.size;
+  parts_.push_back(std::move(part));
   m.sections.push_back(s);
 }
 
@@ -419,7 +469,10 @@ std::vector<uint8_t> Writer::head() const {
 
 std::vector<uint8_t> Writer::to_bytes() const {
   std::vector<uint8_t> out = head();
-  out.insert(out.end(), payload.begin(), payload.end());
+  for (const Part &p : parts_) {
+    const uint8_t *d = p.own.empty() ? p.p : p.own.data();
+    if (p.n) out.insert(out.end(), d, d + p.n);
+  }
   return out;
 }
 
@@ -428,7 +481,10 @@ void Writer::write(const std::string &path) const {
   std::FILE *f = std::fopen(path.c_str(), "wb");
   if (!f) throw std::runtime_error("write " + path + ": cannot open");
   bool ok = std::fwrite(h.data(), 1, h.size(), f) == h.size();
-  ok = ok && (payload.empty() || std::fwrite(payload.data(), 1, payload.size(), f) == payload.size());
+  for (const Part &p : parts_) {
+    const uint8_t *d = p.own.empty() ? p.p : p.own.data();
+    ok = ok && (p.n == 0 || std::fwrite(d, 1, p.n, f) == p.n);
+  }
   ok = (std::fclose(f) == 0) && ok;
   if (!ok) throw std::runtime_error("write " + path + ": short write");
 }
@@ -436,34 +492,38 @@ void Writer::write(const std::string &path) const {
 // ---------------------------------------------------------------------------
 // reader (reader.rs:32-281)
 // ---------------------------------------------------------------------------
-void Reader::open(const std::string &path) {
+void Reader::read_at(uint64_t off, void *dst, uint64_t n) const {
+  if (n == 0) return;
   std::FILE *f = std::fopen(path.c_str(), "rb");
   if (!f) throw std::runtime_error("Cannot open file: " + path);
-  std::vector<uint8_t> b;
-  bool ok = std::fseek(f, 0, SEEK_END) == 0;
-  const long n = ok ? std::ftell(f) : -1;
-  ok = ok && n >= 0 && std::fseek(f, 0, SEEK_SET) == 0;
-  if (ok) {
-    b.resize((size_t)n);
-    ok = n == 0 || std::fread(b.data(), 1, (size_t)n, f) == (size_t)n;
-  }
+  const bool ok = std::fseek(f, (long)off, SEEK_SET) == 0 && std::fread(dst, 1, (size_t)n, f) == (size_t)n;
   std::fclose(f);
   if (!ok) throw std::runtime_error("Cannot read file: " + path);
-  parse(std::move(b));
 }
 
-void Reader::parse(std::vector<uint8_t> b) {
-  bytes = std::move(b);
-  if (bytes.size() < 13) throw std::runtime_error("File too short");
-  if (std::memcmp(bytes.data(), "TAAS2", 5) != 0) {
-    if (std::memcmp(bytes.data(), "TAAS1", 5) == 0)
+void Reader::open(const std::string &p) {
+  path = p;
+  std::FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) throw std::runtime_error("Cannot open file: " + path);
+  bool ok = std::fseek(f, 0, SEEK_END) == 0;
+  const long sz = ok ? std::ftell(f) : -1;
+  std::fclose(f);
+  if (!ok || sz < 0) throw std::runtime_error("Cannot read file: " + path);
+  file_size = (uint64_t)sz;
+  if (file_size < 13) throw std::runtime_error("File too short");
+  uint8_t pre[13];
+  read_at(0, pre, 13);
+  if (std::memcmp(pre, "TAAS2", 5) != 0) {
+    if (std::memcmp(pre, "TAAS1", 5) == 0)
       throw std::runtime_error("TAAS1 (the pre-v2 format) is not read here: migrate it to TAAS2 first");
     throw std::runtime_error("Invalid magic: expected TAAS2");
   }
   uint64_t hl = 0;
-  for (int k = 0; k < 8; ++k) hl |= (uint64_t)bytes[5 + k] << (8 * k);
-  if (hl > bytes.size() - 13) throw std::runtime_error("Header truncated");
-  JParser jp{(const char *)bytes.data() + 13, (const char *)bytes.data() + 13 + hl};
+  for (int k = 0; k < 8; ++k) hl |= (uint64_t)pre[5 + k] << (8 * k);
+  if (hl > file_size - 13) throw std::runtime_error("Header truncated");
+  std::vector<char> hb((size_t)hl);
+  read_at(13, hb.data(), hl);
+  JParser jp{hb.data(), hb.data() + hb.size()};
   const JVal root = jp.val();
   jp.ws();
   if (jp.p != jp.e) throw std::runtime_error("Invalid manifest JSON: trailing characters");
@@ -505,8 +565,8 @@ void Reader::parse(std::vector<uint8_t> b) {
   const JVal *md = root.get("metadata");
   if (md && md->t == JVal::Obj)
     for (auto &kv : md->o) m.metadata[kv.first] = jstr(&kv.second, "metadata value");
-  data_offset = 13 + (size_t)hl;
-  const uint64_t avail = bytes.size() - data_offset;
+  data_offset = 13 + hl;
+  const uint64_t avail = file_size - data_offset;
   for (const Section &s : m.sections)
     if (s.offset > avail || s.size > avail - s.offset)
       throw std::runtime_error("Section '" + s.name + "' (offset=" + std::to_string(s.offset) + ", size=" +
@@ -519,39 +579,56 @@ const Section *Reader::find(const std::string &name) const {
   return nullptr;
 }
 
-std::vector<uint8_t> Reader::get(const std::string &name, const std::string &kind) const {
+uint64_t Reader::plain_size(const Section &s) const {
+  if (s.compression.empty()) return s.size;
+  if (s.has_usize) return s.usize;
+  const Zstd *z = zstd();
+  if (!z) throw std::runtime_error("Section '" + s.name + "' zstd decompression failed: libzstd.so.1 is not available");
+  std::vector<uint8_t> head((size_t)std::min<uint64_t>(s.size, 18));
+  read_at(data_offset + s.offset, head.data(), head.size());
+  const unsigned long long n = z->content_size(head.data(), head.size());
+  if (n >= (1ull << 62)) throw std::runtime_error("Section '" + s.name + "' zstd decompression failed: unknown size");
+  return n;
+}
+
+uint64_t Reader::get_into(const std::string &name, const std::string &kind, void *dst, uint64_t cap) const {
   const Section *s = find(name);
   if (!s) throw std::runtime_error("Section '" + name + "' not found in manifest");
   if (s->kind != kind) throw std::runtime_error("Section '" + name + "' is not " + kind + ", got " + s->kind);
-  const uint8_t *src = bytes.data() + data_offset + s->offset;
-  std::vector<uint8_t> out;
-  if (s->compression == "zstd") {
+  if (!kind_known(kind)) throw std::runtime_error("Section '" + name + "' has unknown kind " + kind);
+  if (!s->compression.empty() && s->compression != "zstd")
+    throw std::runtime_error("Section '" + name + "' uses unknown compression " + s->compression);
+  const uint64_t n = plain_size(*s);
+  const size_t es = kind_size(kind);
+  if (es && n != s->count * es)
+    throw std::runtime_error("Section '" + name + "' " + kind + ": data len " + std::to_string(n) + " != count " +
+                             std::to_string(s->count) + " * " + std::to_string(es));
+  if (!dst) return n;
+  if (cap < n) throw std::runtime_error("Section '" + name + "': output buffer too small");
+  if (s->compression.empty()) {
+    read_at(data_offset + s->offset, dst, n);
+  } else {
     const Zstd *z = zstd();
     if (!z) throw std::runtime_error("Section '" + name + "' zstd decompression failed: libzstd.so.1 is not available");
-    unsigned long long n = s->has_usize ? s->usize : z->content_size(src, s->size);
-    if (n >= (1ull << 62)) throw std::runtime_error("Section '" + name + "' zstd decompression failed: unknown size");
-    out.resize((size_t)n);
-    const size_t r = z->decompress(out.data(), out.size(), src, s->size);
-    if (z->is_error(r) || r != n)
-      throw std::runtime_error("Section '" + name + "' zstd decompression failed");
-  } else if (!s->compression.empty()) {
-    throw std::runtime_error("Section '" + name + "' uses unknown compression " + s->compression);
-  } else {
-    out.assign(src, src + s->size);
+    std::vector<uint8_t> src((size_t)s->size);
+    read_at(data_offset + s->offset, src.data(), s->size);
+    const size_t r = z->decompress(dst, (size_t)n, src.data(), src.size());
+    if (z->is_error(r) || r != n) throw std::runtime_error("Section '" + name + "' zstd decompression failed");
   }
   if (s->has_crc) {
-    const uint32_t c = crc32(out.data(), out.size());
+    const uint32_t c = crc32((const uint8_t *)dst, (size_t)n);
     if (c != s->crc) {
       char msg[160];
       std::snprintf(msg, sizeof msg, "CRC32 mismatch: expected %08x, got %08x", s->crc, c);
       throw std::runtime_error("Section '" + name + "' " + msg);
     }
   }
-  const size_t es = kind_size(kind);
-  if (es && out.size() != s->count * es)
-    throw std::runtime_error("Section '" + name + "' " + kind + ": data len " + std::to_string(out.size()) +
-                             " != count " + std::to_string(s->count) + " * " + std::to_string(es));
-  if (!kind_known(kind)) throw std::runtime_error("Section '" + name + "' has unknown kind " + kind);
+  return n;
+}
+
+std::vector<uint8_t> Reader::get(const std::string &name, const std::string &kind) const {
+  std::vector<uint8_t> out((size_t)get_into(name, kind, nullptr, 0));
+  get_into(name, kind, out.data(), out.size());
   return out;
 }
 
@@ -590,7 +667,7 @@ std::string Reader::inspect() const {
       o += buf + kv.second + "\n";
     }
   }
-  o += "\n   Total size: " + human_size(bytes.size());
+  o += "\n   Total size: " + human_size(file_size);
   return o;
 }
 

@@ -36,33 +36,49 @@ struct Manifest {
   std::map<std::string, std::string> metadata;
 };
 
-uint32_t crc32(const uint8_t *p, size_t n);
-size_t kind_size(const std::string &kind);  // element bytes of a numeric kind, 0 for str/json/blob
+uint32_t crc32(const uint8_t *p, size_t n);  // threads over large buffers
+size_t kind_size(const std::string &kind);    // element bytes of a numeric kind, 0 for str/json/blob
 bool zstd_available();
 
 class Writer {
  public:
   Manifest m;
-  std::vector<uint8_t> payload;
   int level = 0;  // zstd level for the next sections, 0 = none
+  // An uncompressed section's bytes are borrowed and must stay valid until
+  // write(); a compressed section's bytes are kept here.
   void push(const std::string &name, const std::string &kind, uint64_t count, const void *data, size_t bytes);
   std::vector<uint8_t> head() const;      // magic, length, manifest
   std::vector<uint8_t> to_bytes() const;  // head + payload
   void write(const std::string &path) const;
+
+ private:
+  struct Part {
+    const uint8_t *p = nullptr;
+    size_t n = 0;
+    std::vector<uint8_t> own;
+  };
+  std::vector<Part> parts_;
+  uint64_t offset_ = 0;
 };
 
 class Reader {
  public:
   Manifest m;
-  std::vector<uint8_t> bytes;
-  size_t data_offset = 0;
-  // throws std::runtime_error with the reference's kind of message
+  std::string path;
+  uint64_t data_offset = 0, file_size = 0;
+  // reads the magic, length and manifest only; throws std::runtime_error
+  // with the reference's kind of message
   void open(const std::string &path);
-  void parse(std::vector<uint8_t> b);
   const Section *find(const std::string &name) const;
-  // uncompressed bytes of a section of the given kind (CRC checked)
+  // uncompressed bytes of a section of the given kind (kind, CRC and length
+  // checked), read straight into dst (cap bytes); dst null: size only
+  uint64_t get_into(const std::string &name, const std::string &kind, void *dst, uint64_t cap) const;
   std::vector<uint8_t> get(const std::string &name, const std::string &kind) const;
   std::string inspect() const;
+
+ private:
+  void read_at(uint64_t off, void *dst, uint64_t n) const;
+  uint64_t plain_size(const Section &s) const;
 };
 
 std::string created_now();  // lib.rs:68-78 fallback timestamp

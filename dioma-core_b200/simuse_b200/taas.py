@@ -16,15 +16,13 @@ _NP = {"f32": np.float32, "i32": np.int32, "i64": np.int64, "u64": np.uint64, "u
 
 
 def _payload(kind, value):
+    """(count, object holding the bytes, its address, byte length) without copying numeric arrays."""
     if kind in _NP:
         a = np.ascontiguousarray(value, dtype=_NP[kind])
-        return a.size, a.tobytes()
-    if kind in ("str", "json"):
+        return a.size, a, a.ctypes.data, a.nbytes
+    if kind in ("str", "json", "blob"):
         b = value.encode() if isinstance(value, str) else bytes(value)
-        return len(b), b
-    if kind == "blob":
-        b = bytes(value)
-        return len(b), b
+        return len(b), b, C.cast(C.c_char_p(b), C.c_void_p).value, len(b)
     raise ValueError(f"unknown section kind {kind!r}")
 
 
@@ -33,32 +31,33 @@ def write(path, sections, metadata=None, game=None, created=None, zstd_level=0):
     (str/json) or bytes (blob)."""
     n = len(sections)
     enc = [(nm.encode(), kd.encode()) + _payload(kd, v) for nm, kd, v in sections]
-    bufs = [C.create_string_buffer(p, max(len(p), 1)) for *_, p in enc]
     names = (C.c_char_p * max(n, 1))(*[e[0] for e in enc])
     kinds = (C.c_char_p * max(n, 1))(*[e[1] for e in enc])
     counts = (C.c_uint64 * max(n, 1))(*[e[2] for e in enc])
-    sizes = (C.c_uint64 * max(n, 1))(*[len(e[3]) for e in enc])
-    data = (C.c_void_p * max(n, 1))(*[C.cast(b, C.c_void_p) for b in bufs])
+    data = (C.c_void_p * max(n, 1))(*[e[4] for e in enc])
+    sizes = (C.c_uint64 * max(n, 1))(*[e[5] for e in enc])
     md = sorted((metadata or {}).items())
     keys = (C.c_char_p * max(len(md), 1))(*[k.encode() for k, _ in md])
     vals = (C.c_char_p * max(len(md), 1))(*[v.encode() for _, v in md])
     check(lib().sg_taas_write(str(path).encode(), created.encode() if created is not None else None,
                               game.encode() if game is not None else None, n, names, kinds, counts, data, sizes,
                               len(md), keys, vals, int(zstd_level)))
+    del enc  # the section buffers were borrowed until here
 
 
 def read(path, name, kind):
     """A section's values: numpy array (numeric kinds), str (str/json) or bytes."""
     size = C.c_uint64()
     check(lib().sg_taas_read(str(path).encode(), name.encode(), kind.encode(), None, 0, C.byref(size)))
-    buf = C.create_string_buffer(max(size.value, 1))
-    check(lib().sg_taas_read(str(path).encode(), name.encode(), kind.encode(), buf, size.value, C.byref(size)))
-    raw = buf.raw[:size.value]
+    buf = np.empty(max(size.value, 1), np.uint8)
+    check(lib().sg_taas_read(str(path).encode(), name.encode(), kind.encode(), buf.ctypes.data, size.value,
+                             C.byref(size)))
+    raw = buf[:size.value]
     if kind in _NP:
-        return np.frombuffer(raw, dtype=_NP[kind]).copy()
+        return raw.view(_NP[kind])
     if kind in ("str", "json"):
-        return raw.decode()
-    return raw
+        return raw.tobytes().decode()
+    return raw.tobytes()
 
 
 def validate(path):

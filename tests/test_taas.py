@@ -149,3 +149,20 @@ def test_reads_files_of_the_reference_layout(tmp_path):
     taas.validate(p)
     assert np.array_equal(taas.read(p, "row_ptr", "i32"), rp)
     assert taas.read(p, "groups", "json") == '[{"name":"a","indices":[0,1]}]'
+
+
+def test_large_sections_use_the_threaded_crc(tmp_path):
+    """Sections above a few MB are checksummed in chunks on several threads
+    and the chunk CRCs combined; the result must be the single-pass CRC32
+    (the oracle's zlib.crc32), and a flipped byte must still be caught."""
+    big = np.random.default_rng(5).random(12_000_003).astype(np.float32)   # 48 MB, odd length
+    secs = [("small", "u8", np.arange(7, dtype=np.uint8)), ("big", "f32", big)]
+    p = tmp_path / "big.taas"
+    taas.write(p, secs, created=CREATED)
+    assert p.read_bytes() == T.to_bytes(secs, created=CREATED)
+    assert np.array_equal(taas.read(p, "big", "f32"), big)
+    b = bytearray(p.read_bytes())
+    b[len(b) // 2] ^= 0x01
+    p.write_bytes(bytes(b))
+    with pytest.raises(sg.SimuseError, match="CRC32 mismatch"):
+        taas.read(p, "big", "f32")
