@@ -2647,10 +2647,16 @@ int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float 
   });
 }
 
-int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap) {
+// Reward of the synapses [lo, hi) only: in a pool of independent networks
+// (populations without synapses between them, e.g. creatures of one arena)
+// a network's synapses are one CSR range, and this is its own Brain's reward
+// (the per-block reward the reference's one-scalar shader lacks,
+// dioma-engine/src/brain/dynamics/gpu_pool.rs:12-16).
+int sg_learn_reward_range(sg_net *net, uint64_t lo, uint64_t hi, float dopamine, float gate, float w_cap) {
   NET_CHECK(net);
   return run([&] {
     require_learn(net);
+    SG_REQUIRE(lo <= hi && hi <= net->n_edges, SG_E_INVALID, "synapse range out of bounds");
     const float w_max = std::isfinite(w_cap) ? w_cap : net->l_w_max;
     SG_REQUIRE(net->l_w_min <= w_max, SG_E_INVALID, "reward: weight ceiling below the floor");
     DevGuard g(net->device);
@@ -2658,25 +2664,54 @@ int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap) {
     const float gc = gate < 0.0f ? 0.0f : (gate > 1.0f ? 1.0f : gate);
     const float dop = dopamine * gc;
     const float lr_dopa = net->l_lr * dop;
-    const uint64_t E = net->n_edges;
+    const uint64_t E = hi - lo;
     if (E)
-      learn_reward_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p, net->d_l_st.p, net->d_step.p,
-                                                                     net->l_t0, E, net->l_de, lr_dopa, net->l_w_min,
-                                                                     w_max);
+      learn_reward_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_edge.p + lo, net->d_l_st.p + lo,
+                                                                     net->d_step.p, net->l_t0, E, net->l_de, lr_dopa,
+                                                                     net->l_w_min, w_max);
+    SG_CUDA(cudaGetLastError());
+  });
+}
+
+int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap) {
+  NET_CHECK(net);
+  return sg_learn_reward_range(net, 0, net->n_edges, dopamine, gate, w_cap);
+}
+
+int sg_learn_clear_range(sg_net *net, uint64_t lo, uint64_t hi) {
+  NET_CHECK(net);
+  return run([&] {
+    require_learn(net);
+    SG_REQUIRE(lo <= hi && hi <= net->n_edges, SG_E_INVALID, "synapse range out of bounds");
+    DevGuard g(net->device);
+    const uint64_t E = hi - lo;
+    if (E)
+      learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_st.p + lo, nullptr, net->d_step.p,
+                                                                    net->l_t0, E);
     SG_CUDA(cudaGetLastError());
   });
 }
 
 int sg_learn_clear(sg_net *net) {
   NET_CHECK(net);
+  return sg_learn_clear_range(net, 0, net->n_edges);
+}
+
+// the CSR synapse range [lo, hi) of a population's rows
+int sg_pop_synapse_range(sg_net *net, uint32_t pop, uint64_t *lo, uint64_t *hi) {
+  NET_CHECK(net);
   return run([&] {
-    require_learn(net);
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    require_pop(net, pop);
+    SG_REQUIRE(lo && hi, SG_E_INVALID, "null output");
     DevGuard g(net->device);
-    const uint64_t E = net->n_edges;
-    if (E)
-      learn_clear_kernel<<<learn_blocks(E), 256, 0, net->stream>>>(net->d_l_st.p, nullptr, net->d_step.p, net->l_t0,
-                                                                    E);
-    SG_CUDA(cudaGetLastError());
+    uint32_t r[2] = {0, 0};
+    const uint32_t d0 = net->pops[pop].dev_off;
+    SG_CUDA(cudaMemcpyAsync(&r[0], net->d_row_ptr.p + d0, 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(&r[1], net->d_row_ptr.p + d0 + net->pops[pop].n, 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    *lo = r[0];
+    *hi = r[1];
   });
 }
 

@@ -84,6 +84,9 @@ SIGNATURES = {
     "sg_learn_enable": [vp, f32, f32, f32, f32, f32, f32, f32, f32, f32],
     "sg_learn_reward": [vp, f32, f32, f32],
     "sg_learn_clear": [vp],
+    "sg_learn_reward_range": [vp, u64, u64, f32, f32, f32],
+    "sg_learn_clear_range": [vp, u64, u64],
+    "sg_pop_synapse_range": [vp, u32, vp, vp],
     "sg_learn_restrict": [vp, vp, u64],
     "sg_learn_set_eligibility": [vp, vp, u64],
     "sg_learn_motor": [vp, u64, u64, u64, u64],

@@ -390,12 +390,26 @@ class Network:
         defaults, brain.rs:46-60).  Needs FP32 weights."""
         check(lib().sg_learn_enable(self._h, dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max))
 
-    def reward(self, dopamine, gate=1.0, w_cap=None):
-        """reward / reward_gated / reward_capped (brain.rs:400-416)."""
-        check(lib().sg_learn_reward(self._h, dopamine, gate, float("nan") if w_cap is None else w_cap))
+    def reward(self, dopamine, gate=1.0, w_cap=None, synapses=None):
+        """reward / reward_gated / reward_capped (brain.rs:400-416); `synapses`
+        = (lo, hi) rewards only that CSR range (one network of a pool)."""
+        cap = float("nan") if w_cap is None else w_cap
+        if synapses is None:
+            check(lib().sg_learn_reward(self._h, dopamine, gate, cap))
+        else:
+            check(lib().sg_learn_reward_range(self._h, synapses[0], synapses[1], dopamine, gate, cap))
 
-    def clear_eligibility(self):
-        check(lib().sg_learn_clear(self._h))
+    def clear_eligibility(self, synapses=None):
+        if synapses is None:
+            check(lib().sg_learn_clear(self._h))
+        else:
+            check(lib().sg_learn_clear_range(self._h, synapses[0], synapses[1]))
+
+    def population_synapses(self, pop):
+        """CSR range (lo, hi) of the synapses whose pre is in `pop`."""
+        lo, hi = C.c_uint64(), C.c_uint64()
+        check(lib().sg_pop_synapse_range(self._h, pop, C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value
 
     def restrict_eligibility(self, keep):
         k = np.ascontiguousarray(keep, dtype=np.uint8)

@@ -287,6 +287,13 @@ int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float 
    cap = w_cap when finite (reward_capped) else w_max; zero deltas skip. */
 int sg_learn_reward(sg_net *net, float dopamine, float gate, float w_cap);
 int sg_learn_clear(sg_net *net);                                       /* brain.rs:271-275 */
+/* Per-network reward and clear in a pool of independent networks (populations
+   without synapses between them): only synapses [lo, hi), e.g. the range
+   sg_pop_synapse_range gives for one network's population; the others keep
+   their eligibility (the per-block reward of dioma-engine gpu_pool.rs:12-16). */
+int sg_learn_reward_range(sg_net *net, uint64_t lo, uint64_t hi, float dopamine, float gate, float w_cap);
+int sg_learn_clear_range(sg_net *net, uint64_t lo, uint64_t hi);
+int sg_pop_synapse_range(sg_net *net, uint32_t pop, uint64_t *lo, uint64_t *hi); /* CSR range of its rows */
 int sg_learn_restrict(sg_net *net, const uint8_t *keep, uint64_t n);   /* brain.rs:278-285 */
 int sg_learn_set_eligibility(sg_net *net, const float *elig, uint64_t n); /* brain.rs:160-170 */
 /* spikes of neurons [lo0, hi0) and [lo1, hi1) counted over each sg_step call

@@ -65,6 +65,9 @@ def lib():
             "or_learn_enable": (i32, [vp, f32, f32, f32, f32, f32, f32, f32, f32, f32]),
             "or_learn_reward": (i32, [vp, f32, f32, f32]),
             "or_learn_clear": (i32, [vp]),
+            "or_learn_reward_range": (i32, [vp, u64, u64, f32, f32, f32]),
+            "or_learn_clear_range": (i32, [vp, u64, u64]),
+            "or_pop_synapse_range": (i32, [vp, i32, vp, vp]),
             "or_learn_restrict": (i32, [vp, vp, u64]),
             "or_learn_set_eligibility": (i32, [vp, vp, u64]),
             "or_learn_motor": (i32, [vp, u64, u64, u64, u64]),
@@ -197,11 +200,23 @@ class Network:
                         w_min=0.0, w_max=1.0):
         _chk(lib().or_learn_enable(self._h, dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max))
 
-    def reward(self, dopamine, gate=1.0, w_cap=None):
-        _chk(lib().or_learn_reward(self._h, dopamine, gate, float("nan") if w_cap is None else w_cap))
+    def reward(self, dopamine, gate=1.0, w_cap=None, synapses=None):
+        cap = float("nan") if w_cap is None else w_cap
+        if synapses is None:
+            _chk(lib().or_learn_reward(self._h, dopamine, gate, cap))
+        else:
+            _chk(lib().or_learn_reward_range(self._h, synapses[0], synapses[1], dopamine, gate, cap))
 
-    def clear_eligibility(self):
-        _chk(lib().or_learn_clear(self._h))
+    def clear_eligibility(self, synapses=None):
+        if synapses is None:
+            _chk(lib().or_learn_clear(self._h))
+        else:
+            _chk(lib().or_learn_clear_range(self._h, synapses[0], synapses[1]))
+
+    def population_synapses(self, pop):
+        lo, hi = C.c_uint64(), C.c_uint64()
+        _chk(lib().or_pop_synapse_range(self._h, pop, C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value
 
     def restrict_eligibility(self, keep):
         k = np.ascontiguousarray(keep, dtype=np.uint8)

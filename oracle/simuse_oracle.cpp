@@ -1102,17 +1102,21 @@ int or_learn_enable(or_net *h, float dt, float tau_pre, float tau_post, float ta
 // brain.rs:288-341 fold_eligibility + reward_dopamine: every eligibility is
 // brought to now by repeated multiplication, then w += lr*dopamine*e clamped to
 // [w_min, cap] (cap: w_max unless w_cap is finite); zero deltas leave w alone.
-int or_learn_reward(or_net *h, float dopamine, float gate, float w_cap) {
+// Reward of the synapses [lo, hi) only: in a pool of independent networks
+// (populations without synapses between them) one network's synapses are
+// one CSR range, and its reward is then exactly its own Brain's.
+int or_learn_reward_range(or_net *h, uint64_t lo, uint64_t hi, float dopamine, float gate, float w_cap) {
   DISPATCH(h, {
     Learn &L = net.learn;
     if (!L.on) return fail("learning is not enabled");
+    if (lo > hi || hi > L.elig.size()) return fail("synapse range out of bounds");
     const float w_max = std::isfinite(w_cap) ? w_cap : L.w_max;
     if (!(L.w_min <= w_max)) return fail("weight ceiling below the floor");
     // reward_gated: dopamine * gate.clamp(0, 1) (brain.rs:405-409)
     const float g = gate < 0.0f ? 0.0f : (gate > 1.0f ? 1.0f : gate);
     const float dop = dopamine * g;
     const float d_e = fast_exp_f(-L.dt / L.tau_e);
-    for (size_t i = 0; i < L.elig.size(); ++i) {
+    for (size_t i = lo; i < hi; ++i) {
       const uint64_t s0 = L.last[i];
       if (s0 < L.t && L.elig[i] != 0.0f) {
         for (uint64_t k = 0; k < L.t - s0; ++k) L.elig[i] *= d_e;
@@ -1122,7 +1126,7 @@ int or_learn_reward(or_net *h, float dopamine, float gate, float w_cap) {
       }
     }
     const float lr_dopa = L.lr * dop;
-    for (size_t i = 0; i < net.w.size(); ++i) {
+    for (size_t i = lo; i < hi; ++i) {
       const float delta = lr_dopa * L.elig[i];
       if (delta == 0.0f) continue;
       const float w = (float)net.w[i] + delta;
@@ -1132,13 +1136,37 @@ int or_learn_reward(or_net *h, float dopamine, float gate, float w_cap) {
   return 0;
 }
 
-// brain.rs:271-280 clear_eligibility: zero, synced to now
-int or_learn_clear(or_net *h) {
+int or_learn_reward(or_net *h, float dopamine, float gate, float w_cap) {
+  uint64_t E = 0;
+  DISPATCH(h, { E = net.learn.elig.size(); });
+  return or_learn_reward_range(h, 0, E, dopamine, gate, w_cap);
+}
+
+// brain.rs:271-280 clear_eligibility: zero, synced to now (of [lo, hi))
+int or_learn_clear_range(or_net *h, uint64_t lo, uint64_t hi) {
   DISPATCH(h, {
     Learn &L = net.learn;
     if (!L.on) return fail("learning is not enabled");
-    std::fill(L.elig.begin(), L.elig.end(), 0.0f);
-    std::fill(L.last.begin(), L.last.end(), L.t);
+    if (lo > hi || hi > L.elig.size()) return fail("synapse range out of bounds");
+    std::fill(L.elig.begin() + lo, L.elig.begin() + hi, 0.0f);
+    std::fill(L.last.begin() + lo, L.last.begin() + hi, L.t);
+  });
+  return 0;
+}
+
+int or_learn_clear(or_net *h) {
+  uint64_t E = 0;
+  DISPATCH(h, { E = net.learn.elig.size(); });
+  return or_learn_clear_range(h, 0, E);
+}
+
+// the CSR synapse range of a population's rows
+int or_pop_synapse_range(or_net *h, int pop, uint64_t *lo, uint64_t *hi) {
+  DISPATCH(h, {
+    if (!net.built) return fail("not built");
+    if (pop < 0 || (size_t)pop >= net.pops.size()) return fail("population out of range");
+    *lo = net.row_ptr[net.offsets[pop]];
+    *hi = net.row_ptr[net.offsets[pop + 1]];
   });
   return 0;
 }

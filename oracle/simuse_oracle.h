@@ -59,6 +59,9 @@ int or_learn_enable(or_net *net, float dt, float tau_pre, float tau_post, float 
                     float a_ltd, float lr, float w_min, float w_max);
 int or_learn_reward(or_net *net, float dopamine, float gate, float w_cap);
 int or_learn_clear(or_net *net);
+int or_learn_reward_range(or_net *net, uint64_t lo, uint64_t hi, float dopamine, float gate, float w_cap);
+int or_learn_clear_range(or_net *net, uint64_t lo, uint64_t hi);
+int or_pop_synapse_range(or_net *net, int pop, uint64_t *lo, uint64_t *hi);
 int or_learn_restrict(or_net *net, const uint8_t *keep, uint64_t n);
 int or_learn_set_eligibility(or_net *net, const float *elig, uint64_t n);
 int or_learn_motor(or_net *net, uint64_t lo0, uint64_t hi0, uint64_t lo1, uint64_t hi1);

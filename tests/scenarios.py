@@ -306,3 +306,42 @@ def learn_scripted(make_net, n, pre, post, w, spikes, cfg, actions=None, motor=N
             if r is not None:
                 out.append((t, verb, r))
     return net, out
+
+
+def learn_pool(make_net, creatures, cfg, steps):
+    """Several scripted networks (creatures) as populations of one network,
+    no synapses between them, learning on; creature k gets its own rewards
+    (`acts[t]` = [(dopamine, gate)]) on its own CSR synapse range."""
+    net = make_net()
+    pops = []
+    for n, pre, post, w, _, _ in creatures:
+        p = net.add_population(LIF, n)
+        for col, v in enumerate([1.0, 1.0, 0.0, 50.0, 0.0, 0.0]):
+            net.fill_param(p, col, v)
+        net.connect(p, pre, p, post, w, np.ones(pre.size, np.uint8))
+        pops.append(p)
+    net.build()
+    net.enable_learning(**cfg)
+    ranges = [net.population_synapses(p) for p in pops]
+    for t in range(steps):
+        for (n, _, _, _, spikes, _), p in zip(creatures, pops):
+            idx = np.nonzero(spikes[t])[0].astype(np.uint32)
+            if idx.size:
+                net.inject_current(p, idx, np.full(idx.size, 100.0, np.float32))
+        net.step(1)
+        for k, ((n, _, _, _, spikes, acts), p) in enumerate(zip(creatures, pops)):
+            assert np.array_equal(np.asarray(net.spikes(p)) != 0, spikes[t] != 0)
+            for dop, gate in acts.get(t, []):
+                net.reward(dop, gate, synapses=ranges[k])
+    return net, pops, ranges
+
+
+def pool_creatures(steps=300):
+    out = []
+    for seed, n, rate, every, phase, dop, gate in ((1, 24, 0.18, 10, 3, 1.0, 1.0), (2, 20, 0.25, 7, 2, -0.8, 0.5),
+                                                   (3, 16, 0.12, 13, 5, 2.0, 0.75)):
+        pre, post, w = lcg_net(seed, n)
+        spikes = (np.random.default_rng(seed + 10).random((steps, n)) < rate).astype(np.int32)
+        acts = {t: [(dop, gate)] for t in range(steps) if t % every == phase}
+        out.append((n, pre, post, w, spikes, acts))
+    return out

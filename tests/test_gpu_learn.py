@@ -141,3 +141,20 @@ def test_learning_errors():
     with pytest.raises(sg.SimuseError):     # BF16 weights are read-only
         b.enable_learning()
     b.close()
+
+
+def test_per_network_reward_in_a_pool_bit_identical_to_the_oracle():
+    """Three networks pooled as populations of one device network, each
+    rewarded on its own synapse range (the oracle's pooled reward equals
+    each network alone, tests/test_oracle_learn.py)."""
+    steps = 300
+    cr = S.pool_creatures(steps)
+    g, _, gr = S.learn_pool(lambda: sg.Network(0), cr, CFG, steps)
+    c, _, cr_ = S.learn_pool(lambda: O.Network(0), cr, CFG, steps)
+    assert gr == cr_
+    assert _same(g.weights(), c.weights())
+    for a, b in zip(g.learning_state()[:3], c.learning_state()[:3]):
+        assert _same(a, b)
+    with pytest.raises(sg.SimuseError):
+        g.reward(1.0, synapses=(0, g.num_synapses + 1))
+    g.close()

@@ -186,3 +186,23 @@ def test_learning_is_deterministic():
     a, _ = S.learn_scripted(lambda: O.Network(0), n, pre, post, w, spikes, CFG, acts)
     b, _ = S.learn_scripted(lambda: O.Network(0), n, pre, post, w, spikes, CFG, acts)
     assert np.array_equal(a.weights(), b.weights())
+
+
+def test_per_network_reward_in_a_pool_equals_separate_networks():
+    """Three scripted networks as populations of one network, each rewarded on
+    its own synapse range at its own times, end with the weights and
+    eligibility each would have alone: the per-block reward the reference's
+    pool lacks (dioma-engine/src/brain/dynamics/gpu_pool.rs:12-16)."""
+    steps = 300
+    cr = S.pool_creatures(steps)
+    pool, pops, ranges = S.learn_pool(lambda: O.Network(0), cr, CFG, steps)
+    w0 = S.learn_pool(lambda: O.Network(0), cr, CFG, 0)[0].weights()   # as built
+    wp = pool.weights()
+    ep = pool.learning_state()[0]
+    for (n, pre, post, w, spikes, acts), (lo, hi) in zip(cr, ranges):
+        a = {t: [("reward", x) for x in v] for t, v in acts.items()}
+        alone, _ = S.learn_scripted(lambda: O.Network(0), n, pre, post, w, spikes, CFG, a)
+        assert hi - lo == pre.size
+        assert np.array_equal(wp[lo:hi], alone.weights())
+        assert np.array_equal(ep[lo:hi], alone.learning_state()[0])
+        assert np.count_nonzero(wp[lo:hi] != w0[lo:hi]) > 0        # each network learned
