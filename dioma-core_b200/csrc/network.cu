@@ -90,6 +90,10 @@ struct HostPop {
   uint64_t noise_seed = 0, noise_stride = 0, noise_step0 = 0;
   double noise_sigma[2] = {0.0, 0.0};
   DBuf<float> d_bias;  // sg_pop_set_bias, [cap] (zero past n)
+  // external population (sg_pop_add_external): simulated elsewhere, its spike
+  // words of each step read from `ext_src` (population-local words)
+  bool external = false;
+  const uint32_t *ext_src = nullptr;
   std::vector<float> params, state;  // before build
   DBuf<float> d_params, d_state;     // after build
 };
@@ -282,6 +286,19 @@ void require_pop(const sg_net *net, uint32_t pop) {
   SG_REQUIRE(pop < net->pops.size(), SG_E_INVALID,
              "population " + std::to_string(pop) + " out of range (have " +
                  std::to_string(net->pops.size()) + ")");
+}
+
+// synapses, Poisson drive and input target neurons simulated here
+void require_local(const sg_net *net, uint32_t pop) {
+  require_pop(net, pop);
+  SG_REQUIRE(!net->pops[pop].external, SG_E_INVALID,
+             "population " + std::to_string(pop) + " is external: its synapses and input belong to the GPU that simulates it");
+}
+
+bool has_external(const sg_net *net) {
+  for (const auto &p : net->pops)
+    if (p.external) return true;
+  return false;
 }
 
 StepArgs make_args(sg_net *net) {
@@ -1319,16 +1336,35 @@ template <int M> void launch_neuron(sg_net *net, const StepArgs &a) {
                                                                     net->d_blk_map.p + net->model_blk_off[M]);
 }
 
-// Phases: 0 neuron update (all populations), 1 scatter.
-void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
+// The first half of a step: the neuron update of every population simulated here.
+void enqueue_neurons(sg_net *net, const StepArgs &a) {
   cudaStream_t s = net->stream;
-  if (ev) SG_CUDA(cudaEventRecord(ev[0], s));
   if (net->learn_on) SG_CUDA(cudaMemsetAsync(net->d_l_ctr.p, 0, net->d_l_ctr.n * 4, s));
   launch_neuron<kLIF>(net, a);
   launch_neuron<kIZH>(net, a);
   launch_neuron<kGPEA>(net, a);
   launch_neuron<kHH>(net, a);
+}
+
+void enqueue_rest(sg_net *net, const StepArgs &a);
+
+// Phases: 0 neuron update (all populations), 1 scatter.
+void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
+  cudaStream_t s = net->stream;
+  if (ev) SG_CUDA(cudaEventRecord(ev[0], s));
+  enqueue_neurons(net, a);
   if (ev) SG_CUDA(cudaEventRecord(ev[1], s));
+  enqueue_rest(net, a);
+  if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
+}
+
+// The second half: external populations' spikes (when the network is split
+// across GPUs), the scatter, the eligibility update.
+void enqueue_rest(sg_net *net, const StepArgs &a) {
+  cudaStream_t s = net->stream;
+  for (const auto &p : net->pops)
+    if (p.external && p.n)
+      ext_spikes_kernel<<<p.cap / kNeuronBlock, kNeuronBlock, 0, s>>>(a, p.dev_off, p.n, p.ext_src);
   if (a.list_mode) {
     if (net->seg32) scatter_kernel<true, true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
     else scatter_kernel<false, true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
@@ -1364,7 +1400,6 @@ void enqueue_step(sg_net *net, const StepArgs &a, cudaEvent_t *ev = nullptr) {
     learn_elig_kernel<<<blocks, kLearnThreads, 0, s>>>(L);
     learn_decay_kernel<<<blocks, kLearnThreads, 0, s>>>(L);
   }
-  if (ev) SG_CUDA(cudaEventRecord(ev[2], s));
 }
 
 // Profiled steps: eager launches with CUDA events between the phases, read
@@ -1537,6 +1572,32 @@ int sg_pop_add(sg_net *net, int model, uint32_t n, uint32_t *out_pop) {
   });
 }
 
+// A population simulated on another GPU (a network split across GPUs): it
+// holds no state, no parameters and no incoming synapses here; its neurons
+// are pre-synaptic neurons whose spikes arrive each step through the
+// exchange (sg_pop_set_external_source), at the same device indices, so the
+// scatter walks spiking neurons in the same order as the whole network.
+int sg_pop_add_external(sg_net *net, uint32_t n, uint32_t *out_pop) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "Cannot add populations after build()");
+    SG_REQUIRE(net->total + n <= 0xFFFFFFFFull, SG_E_INVALID, "Network: total neuron count exceeds u32::MAX");
+    HostPop p;
+    p.model = 0;
+    p.external = true;
+    p.n = n;
+    p.cap = (uint32_t)align_up(n, kNeuronBlock);
+    p.dev_off = net->Nd;
+    p.np = p.ns = 0;
+    SG_REQUIRE((uint64_t)net->Nd + p.cap <= 0xFFFFFFFFull, SG_E_INVALID, "device neuron count exceeds u32");
+    net->Nd += p.cap;
+    net->pops.push_back(std::move(p));
+    net->total += n;
+    net->offsets.push_back((uint32_t)net->total);
+    if (out_pop) *out_pop = (uint32_t)net->pops.size() - 1;
+  });
+}
+
 static int pop_col(sg_net *net, uint32_t pop, uint32_t col, bool param) {
   require_pop(net, pop);
   const auto &p = net->pops[pop];
@@ -1633,7 +1694,7 @@ static int connect_impl(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
     require_pop(net, from);
-    require_pop(net, to);
+    require_local(net, to);
     if (n == 0) return;
     SG_REQUIRE(fi && ti && w && d, SG_E_INVALID, "null slice");
     const auto &pf = net->pops[from];
@@ -1701,7 +1762,7 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
     require_pop(net, from);
-    require_pop(net, to);
+    require_local(net, to);
     SG_REQUIRE(d_min <= d_max && d_max < kSlots, SG_E_INVALID, "delay range invalid");
     SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
     SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
@@ -1734,7 +1795,7 @@ static OutDegreeSpec outdegree_spec(sg_net *net, uint32_t from, uint32_t to, uin
                                     uint8_t d_max, uint8_t st_e, uint8_t st_i, uint32_t flags_e) {
   SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
   require_pop(net, from);
-  require_pop(net, to);
+  require_local(net, to);
   SG_REQUIRE(d_min <= d_max && d_max < kSlots, SG_E_INVALID, "delay range invalid (d_min <= d_max < 32)");
   SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
   SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
@@ -1931,7 +1992,7 @@ int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *p
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
     SG_REQUIRE(src < net->srcs.size(), SG_E_INVALID, "poisson source out of range");
-    require_pop(net, to);
+    require_local(net, to);
     const auto &pt = net->pops[to];
     auto &s = net->srcs[src];
     for (uint64_t i = 0; i < n; ++i) {
@@ -1954,7 +2015,7 @@ int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint3
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
     SG_REQUIRE((uint64_t)first + n <= net->srcs.size(), SG_E_INVALID, "poisson source out of range");
-    require_pop(net, to);
+    require_local(net, to);
     SG_REQUIRE(std::isfinite(weight), SG_E_INVALID, "weight must be finite");
     SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
     if (n) net->max_delay = std::max<uint32_t>(net->max_delay, delay);
@@ -2130,7 +2191,7 @@ int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals,
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "inject_current() called before build()");
-    require_pop(net, pop);
+    require_local(net, pop);
     if (n == 0) return;
     SG_REQUIRE(idx && vals, SG_E_INVALID, "null slice");
     const auto &p = net->pops[pop];
@@ -2164,9 +2225,65 @@ int sg_step(sg_net *net, uint32_t n_steps) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "Network::step() called before build()");
+    SG_REQUIRE(!has_external(net), SG_E_STATE,
+               "a network with external populations steps with sg_step_begin / sg_step_end around its spike exchange");
     DevGuard g(net->device);
     if (net->profile && net->total > 0) do_steps_profiled(net, n_steps);
     else do_steps(net, n_steps);
+  });
+}
+
+// Where an external population's spike words of each step are read (device
+// memory, the population's words in the owner's bitmask order: bit i of word
+// k is neuron 32k + i); read by every sg_step_end.
+int sg_pop_set_external_source(sg_net *net, uint32_t pop, const uint32_t *dev_words) {
+  NET_CHECK(net);
+  return run([&] {
+    require_pop(net, pop);
+    SG_REQUIRE(net->pops[pop].external, SG_E_INVALID, "not an external population");
+    net->pops[pop].ext_src = dev_words;
+    drop_graph(net);
+  });
+}
+
+// This step's spike words of a population (device memory; valid after
+// sg_step_begin until the next sg_step_begin)
+int sg_spike_words(sg_net *net, uint32_t pop, const uint32_t **dev_words) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    require_pop(net, pop);
+    SG_REQUIRE(dev_words, SG_E_INVALID, "null output");
+    *dev_words = net->d_last_bits.p + net->pops[pop].dev_off / 32;
+  });
+}
+
+// One step in two halves around a spike exchange: sg_step_begin updates the
+// populations simulated here; sg_step_end publishes the external
+// populations' spikes (from their sources), scatters and learns.  Both are
+// asynchronous on the network's stream.
+int sg_step_begin(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "Network::step() called before build()");
+    DevGuard g(net->device);
+    upload_pop_table(net);
+    if (net->learn_on) net->d_l_motor.zero(net->stream);
+    enqueue_neurons(net, make_args(net));
+    SG_CUDA(cudaGetLastError());
+  });
+}
+
+int sg_step_end(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "Network::step() called before build()");
+    for (const auto &p : net->pops)
+      SG_REQUIRE(!p.external || p.ext_src || p.n == 0, SG_E_STATE, "an external population has no spike source");
+    DevGuard g(net->device);
+    enqueue_rest(net, make_args(net));
+    SG_CUDA(cudaGetLastError());
+    net->host_step += 1;
   });
 }
 
@@ -2992,7 +3109,7 @@ int sg_connect_taas(sg_net *net, uint32_t from, uint32_t to, const char *path, u
   return run([&] {
     SG_REQUIRE(path, SG_E_INVALID, "null path");
     require_pop(net, from);
-    require_pop(net, to);
+    require_local(net, to);
     taas::Reader r;
     r.open(path);
     const std::vector<uint8_t> rpb = r.get("row_ptr", "i32"), colb = r.get("col_indices", "i32"),

@@ -1429,6 +1429,52 @@ __global__ void learn_baked_kernel(uint2 *edge, float *baked, uint64_t E, int re
 }
 
 // ---------------------------------------------------------------------------
+// External populations: the neurons of a network split across GPUs that
+// other GPUs simulate.  Their spikes of this step arrive as bitmask words
+// (`src`, population-local, from the spike exchange); this kernel publishes
+// them as the neuron kernel publishes its own: bitmask words, raster words,
+// the block's ascending spike list, STDP and learning traces, the learning
+// spike list.  One 1024-thread block per 1024-neuron block, a neuron per thread.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kNeuronBlock) ext_spikes_kernel(StepArgs a, uint32_t dev_off, uint32_t n,
+                                                                  const uint32_t *__restrict__ src) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t flat_base;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  const uint32_t i = blockIdx.x * kNeuronBlock + tid, gi = dev_off + i;
+  const bool sp = i < n && ((__ldg(src + (i >> 5)) >> (i & 31u)) & 1u);
+  const uint32_t word = __ballot_sync(0xffffffffu, sp);
+  const unsigned long long step = *a.step;
+  if (lane == 0) {
+    a.last_bits[gi >> 5] = word;
+    if (a.raster != nullptr) a.raster[(size_t)(step % a.raster_cap) * a.words + (gi >> 5)] = word;
+  }
+  uint32_t total;
+  const uint32_t before = block_excl_scan(sp ? 1u : 0u, wsum, &total);
+  const uint32_t gblk = gi / kNeuronBlock;
+  if (sp) a.spk[(size_t)gblk * kNeuronBlock + before] = make_uint2(gi, __ldg(a.row_ptr + gi));
+  if (tid == 0) a.blk_cnt[gblk] = total;
+  if (i < n) {
+    const float add = sp ? 1.0f : 0.0f;
+    if (a.stdp) {
+      a.x_pre[gi] = __fmaf_rn(a.x_pre[gi], a.d_pre, add);
+      a.x_post[gi] = __fmaf_rn(a.x_post[gi], a.d_post, add);
+    }
+    if (a.learn) {
+      a.l_tp[gi] = __fmaf_rn(a.l_tp[gi], a.l_dpre, add);
+      a.l_tq[gi] = __fmaf_rn(a.l_tq[gi], a.l_dpost, add);
+      if (sp && gi >= a.l_motor[0] && gi < a.l_motor[1]) atomicAdd(a.l_motor_acc, 1u);
+      if (sp && gi >= a.l_motor[2] && gi < a.l_motor[3]) atomicAdd(a.l_motor_acc + 1, 1u);
+    }
+  }
+  if (a.learn) {
+    if (tid == 0) flat_base = total ? atomicAdd(a.l_flat_cnt, total) : 0u;
+    __syncthreads();
+    if (sp) a.l_flat[flat_base + before] = gi;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // inject_current (build.rs:243-275): values land in the slot the next step
 // reads.  `sequential` = the index list has repeats, apply in list order.
 // ---------------------------------------------------------------------------

@@ -94,6 +94,11 @@ SIGNATURES = {
     "sg_learn_snapshot": [vp],
     "sg_learn_recall": [vp, f32],
     "sg_learn_read": [vp, vp, vp, vp, vp],
+    "sg_pop_add_external": [vp, u32, vp],
+    "sg_pop_set_external_source": [vp, u32, vp],
+    "sg_spike_words": [vp, u32, vp],
+    "sg_step_begin": [vp],
+    "sg_step_end": [vp],
     "sg_taas_write": [vp, vp, vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, i32],
     "sg_taas_read": [vp, vp, vp, vp, u64, vp],
     "sg_taas_validate": [vp],

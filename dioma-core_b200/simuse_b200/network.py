@@ -445,6 +445,30 @@ class Network:
         check(lib().sg_learn_read(self._h, _p(e), _p(tp), _p(tq), C.byref(t)))
         return e[:E], tp[:N], tq[:N], t.value
 
+    # -- one network split across GPUs -------------------------------------------
+    def add_external_population(self, n: int) -> int:
+        """Neurons simulated on another GPU: pre-synaptic only here, their
+        spikes read each step from a source set by set_external_source."""
+        out = C.c_uint32()
+        check(lib().sg_pop_add_external(self._h, n, C.byref(out)))
+        self._sizes.append(n)
+        return out.value
+
+    def set_external_source(self, pop: int, dev_words: int):
+        check(lib().sg_pop_set_external_source(self._h, pop, C.c_void_p(dev_words)))
+
+    def spike_words_ptr(self, pop: int) -> int:
+        """Device address of this step's spike words of `pop`."""
+        out = C.c_void_p()
+        check(lib().sg_spike_words(self._h, pop, C.byref(out)))
+        return out.value or 0
+
+    def step_begin(self):
+        check(lib().sg_step_begin(self._h))
+
+    def step_end(self):
+        check(lib().sg_step_end(self._h))
+
     # -- .taas v2 snapshots ------------------------------------------------------
     def save_taas(self, path, created=None, zstd_level=0):
         """Checkpoint: CSR synapses and weights (and eligibility while learning)."""

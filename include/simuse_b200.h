@@ -306,6 +306,21 @@ int sg_learn_recall(sg_net *net, float alpha);                         /* brain.
    traces [total_neurons], steps since learning began (Brain::t); any may be null */
 int sg_learn_read(sg_net *net, float *elig, float *trace_pre, float *trace_post, uint64_t *t);
 
+/* ---- one network split across GPUs ---------------------------------------
+   Each GPU simulates a contiguous slice of the neurons and holds the synapses
+   onto them; the other GPUs' neurons are external populations here (same
+   device indices on every GPU, so the scatter walks spiking neurons in the
+   whole network's order and every ring cell gets the whole network's adds in
+   the same order).  Per step: sg_step_begin (local neuron update), an
+   exchange of this step's spike words (e.g. an NCCL all-gather of the
+   sg_spike_words of every GPU), sg_step_end (external spikes, scatter,
+   learning).  sg_step is refused on a network with external populations. */
+int sg_pop_add_external(sg_net *net, uint32_t n, uint32_t *out_pop);
+int sg_pop_set_external_source(sg_net *net, uint32_t pop, const uint32_t *dev_words);
+int sg_spike_words(sg_net *net, uint32_t pop, const uint32_t **dev_words);
+int sg_step_begin(sg_net *net);
+int sg_step_end(sg_net *net);
+
 /* ---- .taas v2 snapshots --------------------------------------------------
    The reference's container (crates/SiMuse/crates/taas-format:
    TaasWriter::push/to_bytes writer.rs:75-147, TaasReader::get_* /
