@@ -2973,7 +2973,7 @@ int sg_taas_write(const char *path, const char *created, const char *game, uint3
       const std::string kind = kinds[k];
       const size_t es = taas::kind_size(kind);
       SG_REQUIRE(es || kind == "str" || kind == "json" || kind == "blob", SG_E_INVALID, "unknown section kind " + kind);
-      SG_REQUIRE(es ? bytes[k] == counts[k] * es : bytes[k] == counts[k], SG_E_INVALID,
+      SG_REQUIRE(es ? (counts[k] <= UINT64_MAX / es && bytes[k] == counts[k] * es) : bytes[k] == counts[k], SG_E_INVALID,
                  std::string("section '") + names[k] + "': byte length does not match its count");
       SG_REQUIRE(data[k] || bytes[k] == 0, SG_E_INVALID, "null section data");
       w.push(names[k], kind, counts[k], data[k], bytes[k]);

@@ -4,6 +4,7 @@
 
 #include <dlfcn.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
@@ -600,7 +601,7 @@ uint64_t Reader::get_into(const std::string &name, const std::string &kind, void
     throw std::runtime_error("Section '" + name + "' uses unknown compression " + s->compression);
   const uint64_t n = plain_size(*s);
   const size_t es = kind_size(kind);
-  if (es && n != s->count * es)
+  if (es && (s->count > UINT64_MAX / es || n != s->count * es))
     throw std::runtime_error("Section '" + name + "' " + kind + ": data len " + std::to_string(n) + " != count " +
                              std::to_string(s->count) + " * " + std::to_string(es));
   if (!dst) return n;

@@ -166,3 +166,34 @@ def test_large_sections_use_the_threaded_crc(tmp_path):
     p.write_bytes(bytes(b))
     with pytest.raises(sg.SimuseError, match="CRC32 mismatch"):
         taas.read(p, "big", "f32")
+
+
+def test_untrusted_manifests_are_refused(tmp_path):
+    """A manifest whose count times element size wraps, whose section runs
+    past the file, or whose JSON is malformed is refused, not followed."""
+    import json
+    import struct
+    good = T.to_bytes([("x", "f32", np.ones(4, np.float32))], created=CREATED)
+    (hl,) = struct.unpack("<Q", good[5:13])
+    man = json.loads(good[13:13 + hl])
+    payload = good[13 + hl:]
+
+    def write(m, body=payload):
+        h = json.dumps(m, separators=(",", ":")).encode()
+        p = tmp_path / "m.taas"
+        p.write_bytes(b"TAAS2" + struct.pack("<Q", len(h)) + h + body)
+        return p
+
+    bad = json.loads(json.dumps(man))
+    bad["sections"][0]["count"] = 2 ** 62 + 4          # 4 * count wraps to 16
+    with pytest.raises(sg.SimuseError, match="data len"):
+        taas.read(write(bad), "x", "f32")
+    bad = json.loads(json.dumps(man))
+    bad["sections"][0]["offset"] = 2 ** 64 - 8         # offset + size wraps
+    with pytest.raises(sg.SimuseError, match="exceeds data"):
+        taas.validate(write(bad))
+    p = tmp_path / "j.taas"
+    for h in (b'{"version":"2.0.0"', b'{"version":2}', b'[1,2]', b'{"version":"2.0.0","created":"x","sections":[{}]}'):
+        p.write_bytes(b"TAAS2" + struct.pack("<Q", len(h)) + h)
+        with pytest.raises(sg.SimuseError, match="manifest"):
+            taas.validate(p)
