@@ -151,6 +151,32 @@ class Network {
     check(sg_learn_read(h_, e.data(), nullptr, nullptr, nullptr));
     return e;
   }
+  // -- .taas v2 snapshots (taas-format) --------------------------------------------
+  void save_taas(const std::string &path, int zstd_level = 0) {
+    check(sg_taas_save(h_, path.c_str(), nullptr, zstd_level));
+  }
+  void load_weights_taas(const std::string &path) { check(sg_taas_load_weights(h_, path.c_str())); }
+  void connect_taas(PopulationId from, PopulationId to, const std::string &path, uint8_t default_delay = 1) {
+    check(sg_connect_taas(h_, from, to, path.c_str(), default_delay));
+  }
+
+  // -- one network split across GPUs ------------------------------------------------
+  PopulationId add_external_population(uint32_t n) {
+    uint32_t id = 0;
+    check(sg_pop_add_external(h_, n, &id));
+    sizes_.push_back(n);
+    return id;
+  }
+  void set_external_source(PopulationId p, const uint32_t *dev_words) {
+    check(sg_pop_set_external_source(h_, p, dev_words));
+  }
+  const uint32_t *spike_words(PopulationId p) const {
+    const uint32_t *w = nullptr;
+    check(sg_spike_words(h_, p, &w));
+    return w;
+  }
+  void step_begin() { check(sg_step_begin(h_)); }
+  void step_end() { check(sg_step_end(h_)); }
   sg_net *handle() const { return h_; }
 
  private:
