@@ -62,6 +62,10 @@ def lib():
             "or_tm_sequence": (i32, [f32, f32, f32, i32, f32, vp, u32, vp]),
             "or_register_expone": (i32, [vp, f32, f32, f32]),
             "or_register_kinetics": (i32, [vp, i32, vp, f32, f32]),
+            "or_pop_add_external": (i32, [vp, u32]),
+            "or_step_begin": (i32, [vp]),
+            "or_set_external_spikes": (i32, [vp, i32, vp, u32]),
+            "or_step_end": (i32, [vp]),
             "or_learn_enable": (i32, [vp, f32, f32, f32, f32, f32, f32, f32, f32, f32]),
             "or_learn_reward": (i32, [vp, f32, f32, f32]),
             "or_learn_clear": (i32, [vp]),
@@ -195,6 +199,21 @@ class Network:
 
     def register_expone(self, tau_decay, erev, dt) -> int:
         return _chk(lib().or_register_expone(self._h, tau_decay, erev, dt))
+
+    def add_external_population(self, n):
+        pid = _chk(lib().or_pop_add_external(self._h, n))
+        self._sizes.append(n)
+        return pid
+
+    def step_begin(self):
+        _chk(lib().or_step_begin(self._h))
+
+    def set_external_spikes(self, pop, spikes):
+        s = np.ascontiguousarray(spikes, dtype=np.int32)
+        _chk(lib().or_set_external_spikes(self._h, pop, _p(s), s.size))
+
+    def step_end(self):
+        _chk(lib().or_step_end(self._h))
 
     def enable_learning(self, dt=0.5, tau_pre=20.0, tau_post=20.0, tau_e=1000.0, a_ltp=0.1, a_ltd=0.12, lr=1.0,
                         w_min=0.0, w_max=1.0):

@@ -606,12 +606,14 @@ int g_threads = 1;
 
 // P/api/net/network/step.rs:18-189 Network::step, then (when configured) the
 // pair-STDP update of the plastic weights.
-template <typename T> void net_step(Net<T> &net) {
+// A step in two halves, so that a network split across processes can
+// exchange the spikes of its external populations (neurons simulated by
+// another rank) between them: the first half reads the ring slot and
+// updates the populations simulated here; the second compacts every spike
+// (local and external), pushes, rolls the sources and learns.
+template <typename T> void net_step_begin(Net<T> &net) {
   const size_t N = net.total;
-  if (N == 0) {
-    net.step++;
-    return;
-  }
+  if (N == 0) return;
   const uint32_t slot = (uint32_t)(net.step % kSlots);
   // 1-2. read the current slot into i_in, clear it (step.rs:27-34)
   T *rs = net.ring_slot(0, slot);
@@ -668,7 +670,7 @@ template <typename T> void net_step(Net<T> &net) {
   // of neuron 0, broadcast to the population (:307,:361).
   for (size_t p = 0; p < net.pops.size(); ++p) {
     auto &pop = net.pops[p];
-    if (pop.n == 0) continue;
+    if (pop.n == 0 || pop.model == 0) continue;  // model 0: external, spikes set by the exchange
     const T dt = pop.params[0];
     const bool clamp = clamps_input(pop.model);
     const uint32_t off = net.offsets[p];
@@ -685,6 +687,14 @@ template <typename T> void net_step(Net<T> &net) {
       }
       net.spikes[off + i] = s ? 1 : 0;
     }
+  }
+}
+
+template <typename T> void net_step_end(Net<T> &net) {
+  const size_t N = net.total;
+  if (N == 0) {
+    net.step++;
+    return;
   }
   // 4. compaction, ascending (P/api/net/compact.rs:30-61)
   net.active.clear();
@@ -778,6 +788,11 @@ template <typename T> void net_step(Net<T> &net) {
   }
   if (net.learn.on) learn_step(net);
   net.step++;
+}
+
+template <typename T> void net_step(Net<T> &net) {
+  net_step_begin(net);
+  net_step_end(net);
 }
 
 // P/api/learn/brain.rs:204-286 Brain::step: traces decay and take this
@@ -951,6 +966,27 @@ int or_pop_add(or_net *h, int model, uint32_t n) {
   return id;
 }
 
+// A population simulated by another rank of a split network: no state or
+// parameters here, its spikes of each step set by or_set_external_spikes
+// between or_step_begin and or_step_end.
+int or_pop_add_external(or_net *h, uint32_t n) {
+  int id = -1;
+  DISPATCH(h, {
+    if (net.built) return fail("Cannot add populations after build()");
+    if (net.total + n > 0xFFFFFFFFull) return fail("Network: total neuron count exceeds u32::MAX");
+    Pop<std::remove_reference_t<decltype(net.w[0])>> p;
+    p.model = 0;
+    p.n = n;
+    p.cap = (n + 7) / 8 * 8;
+    p.np = p.ns = 0;
+    net.pops.push_back(std::move(p));
+    net.total += n;
+    net.offsets.push_back((uint32_t)net.total);
+    id = (int)net.pops.size() - 1;
+  });
+  return id;
+}
+
 int or_pop_fill_param(or_net *h, int pop, int col, double v) {
   DISPATCH(h, {
     if (pop_check(net, pop, col, true)) return -1;
@@ -1020,6 +1056,7 @@ int or_connect(or_net *h, int from, const uint32_t *fi, int to, const uint32_t *
     if (net.built) return fail("Cannot connect after build()");
     if (from < 0 || (size_t)from >= net.pops.size()) return fail("from population out of range");
     if (to < 0 || (size_t)to >= net.pops.size()) return fail("to population out of range");
+    if (net.pops[to].model == 0) return fail("no synapses onto an external population");
     const uint32_t fo = net.offsets[from], fc = net.offsets[from + 1] - fo;
     const uint32_t tof = net.offsets[to], tc = net.offsets[to + 1] - tof;
     for (uint64_t i = 0; i < n; ++i) {
@@ -1349,6 +1386,7 @@ int or_poisson_connect(or_net *h, int src, int to, const uint32_t *posts, const 
     if (net.built) return fail("Cannot connect after build()");
     if (src < 0 || (size_t)src >= net.srcs.size()) return fail("poisson source out of range");
     if (to < 0 || (size_t)to >= net.pops.size()) return fail("to population out of range");
+    if (net.pops[to].model == 0) return fail("no synapses onto an external population");
     const uint32_t tof = net.offsets[to], tc = net.offsets[to + 1] - tof;
     auto &s = net.srcs[src];
     for (uint64_t i = 0; i < n; ++i) {
@@ -1524,6 +1562,7 @@ int or_inject(or_net *h, int pop, const uint32_t *idx, const float *v, uint64_t 
   DISPATCH(h, {
     if (!net.built) return fail("inject_current() called before build()");
     if (pop < 0 || (size_t)pop >= net.pops.size()) return fail("inject_current: population out of range");
+    if (net.pops[pop].model == 0) return fail("inject_current: external population");
     const uint32_t start = net.offsets[pop], count = net.offsets[pop + 1] - start;
     for (uint64_t i = 0; i < n; ++i) {
       if (idx[i] >= count) return fail("inject_current: neuron index out of bounds");
@@ -1544,6 +1583,33 @@ int or_step(or_net *h, uint32_t n_steps, uint8_t *raster) {
       if (raster)
         for (uint64_t i = 0; i < net.total; ++i) raster[(size_t)k * net.total + i] = (uint8_t)net.spikes[i];
     }
+  });
+  return 0;
+}
+
+int or_step_begin(or_net *h) {
+  DISPATCH(h, {
+    if (!net.built) return fail("Network::step() called before build()");
+    net.learn.motor[0] = net.learn.motor[1] = 0;
+    net_step_begin(net);
+  });
+  return 0;
+}
+
+int or_set_external_spikes(or_net *h, int pop, const int32_t *s, uint32_t n) {
+  DISPATCH(h, {
+    if (pop < 0 || (size_t)pop >= net.pops.size()) return fail("population out of range");
+    if (net.pops[pop].model != 0) return fail("not an external population");
+    if (n != net.pops[pop].n) return fail("length mismatch");
+    for (uint32_t i = 0; i < n; ++i) net.spikes[net.offsets[pop] + i] = s[i] != 0 ? 1 : 0;
+  });
+  return 0;
+}
+
+int or_step_end(or_net *h) {
+  DISPATCH(h, {
+    if (!net.built) return fail("Network::step() called before build()");
+    net_step_end(net);
   });
   return 0;
 }

@@ -55,6 +55,12 @@ int or_register_expone(or_net *net, float tau_decay, float erev, float dt);
 int or_register_kinetics(or_net *net, int kind, const float *params, float erev, float dt);
 /* dopamine-modulated eligibility learning (P/api/learn/brain.rs) over the
    built network's synapses; reward w_cap: non-finite = the config's w_max */
+/* a network split across processes: external populations (simulated by
+   another rank), the step in two halves around the spike exchange */
+int or_pop_add_external(or_net *net, uint32_t n);
+int or_step_begin(or_net *net);
+int or_set_external_spikes(or_net *net, int pop, const int32_t *spikes, uint32_t n);
+int or_step_end(or_net *net);
 int or_learn_enable(or_net *net, float dt, float tau_pre, float tau_post, float tau_e, float a_ltp,
                     float a_ltd, float lr, float w_min, float w_max);
 int or_learn_reward(or_net *net, float dopamine, float gate, float w_cap);
