@@ -17,8 +17,8 @@ input noise) are keyed by its own seed and its own step counter, so a
 request's result does not depend on what else is resident: the same bits
 alone and in any mix.
 
-The reference has no serving layer; this is the north-star request loop,
-written over the same builder/step API the reference's callers use
+The reference has no serving layer; this is a request loop over many
+simulations, written over the same builder/step API the reference's callers use
 (crates/SiMuse/crates/pillars/src/api/net/network/).
 """
 from __future__ import annotations
