@@ -197,3 +197,16 @@ def test_untrusted_manifests_are_refused(tmp_path):
         p.write_bytes(b"TAAS2" + struct.pack("<Q", len(h)) + h)
         with pytest.raises(sg.SimuseError, match="manifest"):
             taas.validate(p)
+
+
+def test_empty_sections(tmp_path):
+    """Zero-length sections (a network without synapses) round-trip and keep
+    the reference writer's bytes."""
+    secs = [("row_ptr", "i32", np.zeros(1, np.int32)), ("col_indices", "i32", np.zeros(0, np.int32)),
+            ("values", "f32", np.zeros(0, np.float32)), ("name", "str", ""), ("raw", "blob", b"")]
+    p = tmp_path / "e.taas"
+    taas.write(p, secs, created=CREATED)
+    assert p.read_bytes() == T.to_bytes(secs, created=CREATED)
+    assert taas.read(p, "values", "f32").size == 0
+    assert taas.read(p, "name", "str") == "" and taas.read(p, "raw", "blob") == b""
+    taas.validate(p)
