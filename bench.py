@@ -52,14 +52,15 @@ METRIC = "synaptic events/s"
 UNIT = "events/s"
 
 # algorithmic bytes: LIF neuron = v, refr read+write (16 B), ring slot read +
-# clear (8 B), spike bit (1/8 B); per event col 4 + weight 4 + delay 1 and
-# the ring read-modify-write 8; per spike the spike-list write+read and the
-# row start (16 B); per Poisson source rate + seed reads (8 B).
+# clear (8 B), spike bit (1/8 B); per recurrent event col 4 + weight 4 +
+# delay 1 and the ring read-modify-write 8; per spike the spike-list
+# write+read and the row bounds (16 B).  The one-to-one Poisson drive is rolled
+# in the neuron kernel from the neuron index (seed) and one rate: no bytes.
 B_NEURON = 24.125
 B_EVENT_EXPAND = 9.0
 B_EVENT_APPLY = 8.0
 B_SPIKE = 16.0
-B_SOURCE = 8.0
+PARITY_STEPS = 200  # first simulation steps compared bit for bit with the oracle
 
 
 def parse(argv=None):
@@ -152,6 +153,15 @@ def cpu_baseline(args, spec, seconds):
                              spec["w_inh"], spec["d_min"], spec["d_max"])
     build_s = time.time() - t0
     return net, cores, build_s
+
+
+def run_cpu_parity(net, steps):
+    """The oracle's first `steps` steps from the initial state, timed, with
+    the raster recorded: (raster, events, seconds)."""
+    ev0 = net.events
+    t0 = time.perf_counter()
+    rc = net.step(steps, record=True)
+    return rc, net.events - ev0, time.perf_counter() - t0
 
 
 def run_cpu_sample(net, seconds, min_steps=5, chunk=5):
@@ -387,6 +397,13 @@ def run_ours(args):
         net.synchronize()
 
     S = args.sim_steps
+    # the first steps' raster, for the bit-for-bit comparison with the oracle
+    first_raster = None
+    if not args.no_cpu_baseline and world == 1:
+        net.enable_raster(PARITY_STEPS)
+        net.step(PARITY_STEPS)
+        first_raster = net.read_raster()
+        net.enable_raster(0)
     for _ in range(args.warmup):
         net.step(S)
     barrier()
@@ -433,18 +450,18 @@ def run_ours(args):
     # ---- (C) per-kernel timing: CUDA events around each phase --------------------
     net.profile(True)
     p_steps = min(S, 1000)
-    sp_before = net.step_counter
-    ev0 = net.events_total
+    ev0, src0 = net.events_total, net.source_events_total
     net.step(p_steps)
     ph_ms, ph_launch = net.profile_read()
     net.profile(False)
     p_events = (net.events_total - ev0) / p_steps
+    p_src = (net.source_events_total - src0) / p_steps
+    p_rec = p_events - p_src
     sp, _ = net.read_stats()
     p_spikes = float(sp[-p_steps:].mean()) if sp.size else 0.0
-    phases = ["neuron_kernel<LIF>", "scatter_kernel"]
-    n_src = spec["n"]
+    phases = ["neuron_kernel<LIF>", "scatter_red_kernel" if scatter_path != "ordered" else "scatter_kernel"]
     alg = [spec["n"] * B_NEURON,
-           p_events * (B_EVENT_EXPAND + B_EVENT_APPLY) + p_spikes * B_SPIKE + n_src * B_SOURCE]
+           p_rec * (B_EVENT_EXPAND + B_EVENT_APPLY) + p_spikes * B_SPIKE]
     per_launch_ms = [ph_ms[i] / max(int(ph_launch[i]), 1) for i in range(2)]
     dom = int(np.argmax(ph_ms[:2]))
     peak, peak_kind = measured_peak()
@@ -465,17 +482,22 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": config(args, name, spec, scatter_path),
         "sim": {"ms_per_sim_step": step_ms, "events_per_sim_step": events / (args.steps * S),
+                "recurrent_events_per_sim_step": p_rec, "source_events_per_sim_step": p_src,
                 "spikes_per_sim_step": mean_spk, "rate_hz": mean_spk / spec["n"] / (spec["dt"] * 1e-3),
                 "neuron_updates_per_s": spec["n"] * args.steps * S / (ms / 1e3) * world,
                 "step_roofline_frac": step_alg / (step_ms / 1e3) / 1e9 / peak},
         "e2e": {"value": ev_e2e / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(d2h / args.steps),
-                "path": "sg_step + sg_raster_read_events into pinned host buffers, wall clock"},
+                "path": "sg_step + sg_raster_read_events into pinned host buffers, wall clock",
+                "inputs": "none per step by design: the external drive is the network's own Poisson sources, "
+                          "rolled on the device; the per-step host output is the spike raster"},
         "roofline": {"bound": "hbm", "kernel": phases[dom], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": profiled_traffic(phases[dom]),
                      "alg_bytes_per_launch": alg[dom], "launch_ms": per_launch_ms[dom],
-                     "phases_ms_per_launch": dict(zip(phases, per_launch_ms))},
+                     "phases_ms_per_launch": dict(zip(phases, per_launch_ms)),
+                     "phases_frac": {ph: alg[i] / (per_launch_ms[i] / 1e3) / 1e9 / peak
+                                     for i, ph in enumerate(phases)}},
         "clocks": clk.summary(),
         "gpu_launches": int(args.steps * S * 2),
     }
@@ -484,10 +506,16 @@ def run_ours(args):
         out["serving"] = run_serving(args, local)
     if not args.no_cpu_baseline and world == 1:
         cnet, cores, build_s = cpu_baseline(args, spec, args.cpu_seconds)
-        ev, nsteps, el = run_cpu_sample(cnet, args.cpu_seconds)
+        rc, ev, el = run_cpu_parity(cnet, PARITY_STEPS)
         out["cpu_baseline"] = {"value": ev / el, "unit": UNIT, "cores": cores, "kind": "port",
-                               "sample": f"first {nsteps} steps of the same network from its initial state "
+                               "sample": f"first {PARITY_STEPS} steps of the same network from its initial state "
                                          f"({el:.1f} s; oracle/ C++ restatement, push collected on {cores} threads)"}
+        diff = np.nonzero((first_raster != rc).any(axis=1))[0]
+        out["parity"] = {"steps": PARITY_STEPS, "identical": bool(diff.size == 0),
+                         "first_divergent_step": int(diff[0]) if diff.size else None,
+                         "spikes": int(rc.sum()),
+                         "what": "spike raster of the first steps from the initial state, GPU against the oracle, "
+                                 "bit for bit"}
     print(json.dumps(out), flush=True)
 
 

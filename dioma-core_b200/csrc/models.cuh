@@ -23,6 +23,69 @@ __host__ __device__ constexpr int n_state(int m) {
 // (P/zoo/neurons/gpea.rs:210) and the HH conductance model has no clamp.
 __host__ __device__ constexpr bool clamps(int m) { return m == kLIF || m == kIZH; }
 
+// Natural log for the GPEA calcium Nernst potential, correctly rounded to
+// FP32 and compiled identically for the host and the device (so host-built
+// constants, the kernels and a host restatement agree bit for bit).  Method:
+// x = m * 2^k with m in [sqrt(1/2), sqrt(2)); ln m = 2 atanh(s),
+// s = (m - 1)/(m + 1), by the series 2s (1 + s^2/3 + s^4/5 + ... + s^24/25)
+// (Abramowitz & Stegun 4.1.27) evaluated in FP64 (|s| <= 0.1716, so the
+// truncation error is below 2^-70), plus k ln 2 with ln 2 split in a short
+// high part and a low correction, rounded once to FP32.  Every FP64 step is
+// an IEEE add, multiply or divide (no contraction), so the result is the same
+// on any IEEE machine.  Checked correctly rounded over every float in
+// [1e-12, 1e6].
+__host__ __device__ inline float sg_logf(float x) {
+#ifdef __CUDA_ARCH__
+  uint32_t b = __float_as_uint(x);
+#else
+  uint32_t b;
+  __builtin_memcpy(&b, &x, 4);
+#endif
+  if (!(x > 0.0f)) return x == 0.0f ? -__builtin_huge_valf() : __builtin_nanf("");
+  if (b >= 0x7f800000u) return x;  // +inf
+  int k = 0;
+  if (b < 0x00800000u) {  // subnormal: scale into the normal range
+    x = x * 16777216.0f;
+#ifdef __CUDA_ARCH__
+    b = __float_as_uint(x);
+#else
+    __builtin_memcpy(&b, &x, 4);
+#endif
+    k = -24;
+  }
+  k += (int)(b >> 23) - 127;
+  const uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
+  float mf;
+#ifdef __CUDA_ARCH__
+  mf = __uint_as_float(mb);
+#else
+  __builtin_memcpy(&mf, &mb, 4);
+#endif
+  double m = (double)mf;
+  if (m > 1.4142135623730951) {
+    m = m * 0.5;
+    k += 1;
+  }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 25.0;
+  p = p * z + 1.0 / 23.0;
+  p = p * z + 1.0 / 21.0;
+  p = p * z + 1.0 / 19.0;
+  p = p * z + 1.0 / 17.0;
+  p = p * z + 1.0 / 15.0;
+  p = p * z + 1.0 / 13.0;
+  p = p * z + 1.0 / 11.0;
+  p = p * z + 1.0 / 9.0;
+  p = p * z + 1.0 / 7.0;
+  p = p * z + 1.0 / 5.0;
+  p = p * z + 1.0 / 3.0;
+  p = p * z + 1.0;
+  const double lm = (2.0 * s) * p;
+  const double ln2_hi = 6.93147180369123816490e-01, ln2_lo = 1.90821492927058770002e-10;
+  return (float)((double)k * ln2_hi + ((double)k * ln2_lo + lm));
+}
+
 // P/math/fast_exp.rs:23-68 — the project's polynomial exp (fused flavour).
 __device__ __forceinline__ float fast_exp(float x) {
   const float log2e = 1.44269504088896340736f;
@@ -160,7 +223,7 @@ __device__ __forceinline__ float gp_tau2(float v, float t0, float t1, float th1,
 }
 
 // ln(NAI/NAO) and ln(KO/KI) are constants; the host evaluates them once
-// with the reference's libm ln and passes them in (P/zoo/neurons/gpea.rs:273-278).
+// with sg_logf and passes them in (P/zoo/neurons/gpea.rs:273-278).
 template <class A>
 __device__ __forceinline__ bool gpea_step(const A &c, float i_syn, float dt, float ln_na, float ln_k) {
   using namespace gp;
@@ -196,14 +259,14 @@ __device__ __forceinline__ bool gpea_step(const A &c, float i_syn, float dt, flo
   const float r_inf = gp_sigmoid(cai, AHP_TH_R, 1.0f / AHP_K_R);
   const float r_new = gp_exp_euler(r, r_inf, AHP_TAU_R, dt);
 
-  const float eca_old = -rt * logf(cai / CA_CAO) / 2.0f;
+  const float eca_old = -rt * sg_logf(cai / CA_CAO) / 2.0f;
   const float gcat_old = gcatbar * p * p * q;
   const float ica_old = gcat_old * (v - eca_old);
   const float j = -ica_old * area * 1e-14f / (2.0f * CA_FARADAY * vol);
   const float k_ca = caGain * kca;
   const float cai_decay = fast_exp(-dt * k_ca);
   const float cai_new = cai + (1.0f - cai_decay) * (caGain * j / k_ca - cai);
-  const float eca = -rt * logf(cai_new / CA_CAO) / 2.0f;
+  const float eca = -rt * sg_logf(cai_new / CA_CAO) / 2.0f;
 
   const float g_na = gnabar * (m_new * m_new * m_new) * h_new;
   const float n2 = n_new * n_new;

@@ -90,6 +90,11 @@ struct HostPop {
   uint64_t noise_seed = 0, noise_stride = 0, noise_step0 = 0;
   double noise_sigma[2] = {0.0, 0.0};
   DBuf<float> d_bias;  // sg_pop_set_bias, [cap] (zero past n)
+  // deferred drive (found by build_sources): one Poisson source per neuron,
+  // seed drv_seed0 + i, rate drv_p, weight drv_w, delay <= 1, ring 0
+  bool drv = false;
+  uint32_t drv_seed0 = 0;
+  float drv_p = 0.0f, drv_w = 0.0f;
   // external population (sg_pop_add_external): simulated elsewhere, its spike
   // words of each step read from `ext_src` (population-local words)
   bool external = false;
@@ -148,7 +153,7 @@ struct sg_net {
   int weight_format = SG_W_F32;
 
   // device state
-  DBuf<unsigned long long> d_step, d_ev_step, d_ev_total, d_clamp, d_stat_ev;
+  DBuf<unsigned long long> d_step, d_ev_step, d_ev_total, d_clamp, d_stat_ev, d_ev_src;  // d_ev_src: [step, total]
   DBuf<uint32_t> d_blk_cnt, d_last_bits, d_raster, d_done, d_stat_spk;
   DBuf<uint2> d_spk;
   DBuf<float> d_ring, d_kin_g;
@@ -160,6 +165,8 @@ struct sg_net {
   unsigned long long ns_step0 = 0;
   DBuf<uint32_t> d_edge_x;  // BF16 form: the records' x words
   DBuf<uint16_t> d_w16;     //   and their weights in bf16
+  DBuf<uint8_t> d_w8;       // FP8 form: E4M3 weights (x words in d_edge_x)
+  DBuf<float> d_row_scale;  //   and one scale per row
   DBuf<uint8_t> d_code;  // code byte per synapse when it does not fit in x
   int packed = 1;
   uint64_t n_edges = 0;
@@ -187,16 +194,20 @@ struct sg_net {
   uint64_t stat_read_step = 0;
   uint64_t host_step = 0;  // steps issued
   size_t scatter_smem = 0;
-  // pending-event lists of the deterministic scatter (list_mode)
-  int list_mode = 0;
-  uint32_t nkeys = 0, lcap = 0;
-  uint64_t blk_src_max = 0;  // most Poisson-source synapses into one scatter block
+  // the Poisson-source weights' part of the exact-sum test (rings_exact)
   std::vector<double> src_abs;  // per post, sum of |w| of its source synapses
   int src_lo = 1 << 20;         //   smallest low-bit exponent of a source weight
   bool src_bad = false;         //   a source weight is not finite
-  DBuf<uint16_t> d_lpost;
-  DBuf<float> d_lw;
-  DBuf<uint32_t> d_lcnt;
+  // pre-centric scatter (exact ring sums, or the atomic mode): flat list of
+  // the step's spiking neurons and its count; run offsets of the Poisson
+  // synapses it rolls
+  int red = 0;
+  bool exact = false;  // rings_exact at build (cleared when weights start changing)
+  DBuf<uint32_t> d_red_flat, d_red_cnt, d_run_off;
+  // deferred drive: device record of the last folded step, and its host copy
+  DBuf<unsigned long long> d_drv_fold;
+  unsigned long long drv_folded = ~0ull;
+  bool any_drv = false;
   // short-term plasticity: profiles, staged per-edge ids (kept only once an
   // edge has a profile; zero-filled for the edges staged without one), and
   // after build the ids and R, U, last-spike state in CSR order
@@ -314,6 +325,8 @@ StepArgs make_args(sg_net *net) {
   a.done = net->d_done.p;
   a.ev_step = net->d_ev_step.p;
   a.ev_total = net->d_ev_total.p;
+  a.ev_src_step = net->d_ev_src.p;
+  a.ev_src_total = net->d_ev_src.p + 1;
   a.stat_spk = net->d_stat_spk.p;
   a.stat_ev = net->d_stat_ev.p;
   a.stat_cap = net->stat_cap;
@@ -336,6 +349,9 @@ StepArgs make_args(sg_net *net) {
   a.row_ptr = net->d_row_ptr.p;
   a.edge = net->d_edge.p;
   a.wbf16 = net->weight_format == SG_W_BF16 ? 1 : 0;
+  a.wfp8 = net->weight_format == SG_W_FP8 ? 1 : 0;
+  a.w8 = net->d_w8.p;
+  a.row_scale = net->d_row_scale.p;
   a.edge_x = net->d_edge_x.p;
   a.w16 = net->d_w16.p;
   a.code = net->packed ? nullptr : net->d_code.p;
@@ -355,12 +371,13 @@ StepArgs make_args(sg_net *net) {
   a.run_p = net->d_run_p.p;
   a.run_code = net->d_run_code.p;
   a.deterministic = net->deterministic;
-  a.list_mode = net->list_mode && net->deterministic ? 1 : 0;
-  a.nkeys = net->nkeys;
-  a.lcap = net->lcap;
-  a.lpost = net->d_lpost.p;
-  a.lw = net->d_lw.p;
-  a.lcnt = net->d_lcnt.p;
+  a.red = net->red;
+  a.red_flat = net->d_red_flat.p;
+  a.red_cnt = net->d_red_cnt.p;
+  a.run_off = net->d_run_off.p;
+  a.n_runs = (uint32_t)net->n_runs;
+  a.n_src_syn = (uint32_t)net->n_src_edges;
+  a.drv_fold = net->d_drv_fold.p;
   a.tm = net->tm_edges ? 1 : 0;
   a.tm_pt = net->d_pt.p;
   a.tm_r = net->d_tm_r.p;
@@ -874,6 +891,40 @@ __host__ __device__ inline int low_exponent(uint32_t bits) {
   return ex - 150 + tz;
 }
 
+// A population whose only source synapses are one per neuron, from source
+// seed0 + i onto neuron i, with one rate, one weight, delay <= 1 and ring 0,
+// takes that drive in the neuron kernel (deferred drive, PopArgs::drv); its
+// synapses leave the scatter.  `post_cnt` etc. are per device neuron: number
+// of source synapses onto it, and the source, weight and code of the last one.
+void find_deferred_drive(sg_net *net, const std::vector<uint32_t> &post_cnt, const std::vector<uint32_t> &post_src,
+                         const std::vector<float> &post_w, const std::vector<uint8_t> &post_code,
+                         std::vector<uint8_t> &deferred) {
+  net->any_drv = false;
+  for (auto &pop : net->pops) {
+    pop.drv = false;
+    if (pop.external || pop.n == 0) continue;
+    const uint32_t q0 = pop.dev_off;
+    if (post_cnt[q0] != 1) continue;
+    const HostSrc &s0 = net->srcs[post_src[q0]];
+    const float w0 = post_w[q0];
+    bool ok = true;
+    for (uint32_t i = 0; i < pop.n && ok; ++i) {
+      const uint32_t q = q0 + i;
+      const uint8_t c = post_code[q];
+      const HostSrc &sr = net->srcs[post_src[q]];
+      ok = post_cnt[q] == 1 && code_delay(c) <= 1 && code_ring(c) == 0 && !code_stdp(c) &&
+           std::memcmp(&post_w[q], &w0, 4) == 0 && std::memcmp(&sr.p, &s0.p, 4) == 0 && sr.seed == s0.seed + i;
+    }
+    if (!ok) continue;
+    pop.drv = true;
+    pop.drv_seed0 = s0.seed;
+    pop.drv_p = s0.p;
+    pop.drv_w = w0;
+    net->any_drv = true;
+    std::fill(deferred.begin() + q0, deferred.begin() + q0 + pop.n, (uint8_t)1);
+  }
+}
+
 void build_sources(sg_net *net) {
   const size_t S = net->srcs.size();
   const uint32_t G = net->G, P = net->P;
@@ -885,12 +936,30 @@ void build_sources(sg_net *net) {
   net->src_abs.assign(net->Nd, 0.0);
   net->src_lo = 1 << 20;
   net->src_bad = false;
+  std::vector<uint8_t> deferred;
+  if (S) {
+    std::vector<uint32_t> post_cnt(net->Nd, 0), post_src(net->Nd, 0);
+    std::vector<float> post_w(net->Nd, 0.0f);
+    std::vector<uint8_t> post_code(net->Nd, 0);
+    for (size_t i = 0; i < S; ++i)
+      for (size_t k = 0; k < net->srcs[i].post.size(); ++k) {
+        const uint32_t q = net->srcs[i].post[k];
+        post_cnt[q]++;
+        post_src[q] = (uint32_t)i;
+        post_w[q] = net->srcs[i].w[k];
+        post_code[q] = net->srcs[i].code[k];
+      }
+    deferred.assign(net->Nd, 0);
+    find_deferred_drive(net, post_cnt, post_src, post_w, post_code, deferred);
+  } else {
+    net->any_drv = false;
+    for (auto &pop : net->pops) pop.drv = false;
+  }
   for (size_t i = 0; i < S; ++i) {
     p[i] = net->srcs[i].p;
     seed[i] = net->srcs[i].seed;
-    for (uint32_t q : net->srcs[i].post) cnt[q / P]++;
-    tot += net->srcs[i].post.size();
     for (size_t k = 0; k < net->srcs[i].post.size(); ++k) {
+      const uint32_t q = net->srcs[i].post[k];
       const float w = net->srcs[i].w[k];
       uint32_t bits;
       std::memcpy(&bits, &w, 4);
@@ -898,21 +967,23 @@ void build_sources(sg_net *net) {
         net->src_bad = true;
       } else if (bits & 0x7FFFFFFFu) {
         net->src_lo = std::min(net->src_lo, low_exponent(bits));
-        net->src_abs[net->srcs[i].post[k]] += std::fabs((double)w);
+        net->src_abs[q] += std::fabs((double)w);
       }
+      if (deferred[q]) continue;  // taken by the neuron kernel
+      cnt[q / P]++;
+      tot++;
     }
   }
   SG_REQUIRE(tot < 0xFFFFFFFFull, SG_E_OVERFLOW, "too many Poisson-source synapses");
   std::vector<uint32_t> lo((size_t)G + 1, 0);
   for (uint32_t j = 0; j < G; ++j) lo[j + 1] = lo[j] + (uint32_t)cnt[j];
-  net->blk_src_max = 0;
-  for (uint32_t j = 0; j < G; ++j) net->blk_src_max = std::max<uint64_t>(net->blk_src_max, cnt[j]);
   std::vector<uint32_t> cur(lo.begin(), lo.end() - 1), se_src(tot), se_post(tot);
   std::vector<float> se_w(tot);
   std::vector<uint8_t> se_code(tot);
   for (size_t i = 0; i < S; ++i) {
     const auto &sr = net->srcs[i];
     for (size_t k = 0; k < sr.post.size(); ++k) {
+      if (deferred[sr.post[k]]) continue;
       const uint32_t pos = cur[sr.post[k] / P]++;
       se_src[pos] = (uint32_t)i;
       se_post[pos] = sr.post[k];
@@ -949,6 +1020,8 @@ void build_sources(sg_net *net) {
   run_lo[G] = (uint32_t)r_len.size();
   net->n_runs = r_len.size();
   net->n_src_edges = tot;
+  std::vector<uint32_t> r_off(r_len.size() + 1, 0);  // the pre-centric scatter's run offsets
+  for (size_t r = 0; r < r_len.size(); ++r) r_off[r + 1] = r_off[r] + r_len[r];
   auto up = [&](auto &buf, const auto &vec) {
     using T = typename std::decay_t<decltype(vec)>::value_type;
     buf.alloc(std::max<size_t>(vec.size(), 1));
@@ -962,6 +1035,7 @@ void build_sources(sg_net *net) {
   up(net->d_run_w, r_w);
   up(net->d_run_p, r_p);
   up(net->d_run_code, r_code);
+  up(net->d_run_off, r_off);
   SG_CUDA(cudaStreamSynchronize(net->stream));
   for (auto &sr : net->srcs) {  // host copies are no longer needed
     std::vector<uint32_t>().swap(sr.post);
@@ -1059,6 +1133,61 @@ void split_bf16(sg_net *net) {
   net->d_edge.release();
 }
 
+// FP8 E4M3 weight storage, one warp per row: scale = max|w| of the row times
+// 2^-8 (a power-of-two factor, so the row's largest weight is 256 * scale
+// exactly), each weight rounded to the nearest E4M3 value of w / scale (ties
+// to even, saturating at 448).  The records' weights become the decoded
+// values (E4M3 value * scale in FP32), which the exact-sum test then scans
+// before the 8-byte records are freed.
+__global__ void split_fp8_kernel(const uint32_t *row_ptr, uint2 *edge, uint32_t *ex, uint8_t *w8, float *scale,
+                                 uint32_t Nd) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < Nd; r += (gridDim.x * blockDim.x) >> 5) {
+    const uint32_t b = row_ptr[r], e = row_ptr[r + 1];
+    float mx = 0.0f;
+    for (uint32_t k = b + lane; k < e; k += 32) mx = fmaxf(mx, fabsf(__uint_as_float(edge[k].y)));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float sc = mx * 0.00390625f;  // 2^-8
+    if (lane == 0) scale[r] = sc;
+    for (uint32_t k = b + lane; k < e; k += 32) {
+      const uint2 rec = edge[k];
+      const float w = __uint_as_float(rec.y);
+      const __nv_fp8_e4m3 q(sc > 0.0f ? w / sc : 0.0f);
+      const float dq = sc > 0.0f ? (float)q * sc : 0.0f;
+      ex[k] = rec.x;
+      w8[k] = (uint8_t)q.__x;
+      edge[k].y = __float_as_uint(dq);
+    }
+  }
+}
+
+void split_fp8(sg_net *net) {
+  if (net->weight_format != SG_W_FP8) return;
+  SG_REQUIRE(!net->stdp_on, SG_E_INVALID, "FP8 weights are read-only: pair STDP needs FP32 weights");
+  const uint64_t E = net->n_edges;
+  cudaStream_t s = net->stream;
+  net->d_edge_x.alloc(std::max<uint64_t>(E, 1));
+  net->d_w8.alloc(std::max<uint64_t>(E, 1));
+  net->d_row_scale.alloc(std::max<uint32_t>(net->Nd, 1));
+  if (E) {
+    split_fp8_kernel<<<148u * 8u, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_edge_x.p, net->d_w8.p,
+                                               net->d_row_scale.p, net->Nd);
+    SG_CUDA(cudaGetLastError());
+  }
+  SG_CUDA(cudaStreamSynchronize(s));
+}
+
+// E4M3 byte -> FP32 on the host (sign, 4-bit exponent with bias 7, 3-bit
+// mantissa; exponent 0 subnormal; S.1111.111 NaN).
+float host_e4m3(uint8_t b) {
+  const int ex = (b >> 3) & 15, m = b & 7;
+  float v;
+  if (ex == 15 && m == 7) v = NAN;
+  else if (ex == 0) v = std::ldexp((float)m, -9);
+  else v = std::ldexp(1.0f + (float)m / 8.0f, ex - 7);
+  return (b & 0x80) ? -v : v;
+}
+
 __global__ void tm_init_kernel(const uint8_t *pt, const float *u0, float *r, float *u, uint64_t n) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     r[i] = 1.0f;
@@ -1151,51 +1280,62 @@ bool rings_exact(sg_net *net) {
   return most < std::ldexp(1.0, 23 + lo);
 }
 
-// Pending-event lists: used by the deterministic scatter when the ring sums
-// are exact (rings_exact), a block's posts fit its shared memory and the
-// (ring, slot) keys fit.  A list holds up to lcap events: at most 4 windows,
-// fewer when no block can take that many events in one step (every row
-// spiking, every source firing), so that a window always fits an emptied
-// list.
-void setup_lists(sg_net *net) {
-  cudaStream_t s = net->stream;
-  const size_t n_rings = 1 + net->kin.size();
-  net->nkeys = (uint32_t)(n_rings * net->nslots);
-  net->list_mode = (net->Nd > 0 && net->P <= kListPosts && net->nkeys <= kMaxKeys && net->G > 0) ? 1 : 0;
-  if (net->list_mode) net->list_mode = rings_exact(net) ? 1 : 0;
-  if (!net->list_mode) return;
-  DBuf<unsigned long long> indeg;
-  indeg.alloc(net->G);
-  indeg.zero(s);
-  const size_t hsm = (size_t)net->G * sizeof(unsigned long long);
-  const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(1184, (net->Nd + 255) / 256));
-  if (net->seg32)
-    block_indeg_kernel<uint32_t><<<blocks, 256, hsm, s>>>((const uint32_t *)net->d_seg.p, net->Nd, net->G, indeg.p);
-  else
-    block_indeg_kernel<uint16_t><<<blocks, 256, hsm, s>>>((const uint16_t *)net->d_seg.p, net->Nd, net->G, indeg.p);
-  SG_CUDA(cudaGetLastError());
-  std::vector<unsigned long long> h(net->G);
-  SG_CUDA(cudaMemcpyAsync(h.data(), indeg.p, h.size() * 8, cudaMemcpyDeviceToHost, s));
-  SG_CUDA(cudaStreamSynchronize(s));
-  uint64_t most = 0;
-  for (auto v : h) most = std::max<uint64_t>(most, v);
-  most += net->blk_src_max;
-  net->lcap = (uint32_t)std::min<uint64_t>(4ull * kWin, std::max<uint64_t>(align_up(std::max<uint64_t>(most, 1), 256), 256));
-  const size_t n = (size_t)net->G * net->nkeys * net->lcap;
-  net->d_lpost.alloc(n);
-  net->d_lw.alloc(n);
-  net->d_lcnt.alloc((size_t)net->G * net->nkeys);
-  net->d_lcnt.zero(s);
+void drop_graph(sg_net *net);
+
+// The scatter path: the pre-centric scatter (scatter_red_kernel) when the
+// ring sums are exact (any order of the adds gives the reference's bits) or
+// the order is not fixed (sg_set_deterministic(0)); the ordered owner-computes
+// scatter otherwise.
+void update_path(sg_net *net) {
+  const int red = (!net->deterministic || net->exact) ? 1 : 0;
+  if (red != net->red) drop_graph(net);
+  net->red = red;
 }
 
-// Adds every pending list to its ring cells (the rings then hold the
-// reference's ring contents exactly).
-void flush_lists(sg_net *net) {
-  if (!net->list_mode || !net->built) return;
-  StepArgs a = make_args(net);
-  a.list_mode = 1;
-  list_flush_all_kernel<<<net->G, kScatterThreads, net->scatter_smem, net->stream>>>(a);
+void setup_scatter(sg_net *net) {
+  cudaStream_t s = net->stream;
+  net->exact = net->Nd > 0 && rings_exact(net);
+  net->d_red_flat.alloc(std::max<uint32_t>(net->Nd, 1));
+  net->d_red_cnt.alloc(1);
+  net->d_red_cnt.zero(s);
+  net->d_drv_fold.alloc(1);
+  const unsigned long long none = ~0ull;
+  SG_CUDA(cudaMemcpyAsync(net->d_drv_fold.p, &none, sizeof(none), cudaMemcpyHostToDevice, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  net->drv_folded = none;
+  update_path(net);
+}
+
+// Before anything reads or adds to the ring between steps (inject_current,
+// a ring readback): the deferred drive of the last step goes to the ring,
+// where the reference holds it, and the next neuron kernel leaves it out.
+void fold_drive(sg_net *net) {
+  if (!net->any_drv || !net->built) return;
+  const unsigned long long t = net->host_step;
+  if (t == 0 || net->drv_folded == t - 1) return;
+  for (const auto &p : net->pops) {
+    if (!p.drv || p.n == 0) continue;
+    PopArgs pa{};
+    pa.n = p.n;
+    pa.dev_off = p.dev_off;
+    pa.drv = 1;
+    pa.drv_seed0 = p.drv_seed0;
+    pa.drv_p = p.drv_p;
+    pa.drv_w = p.drv_w;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((p.n + 255) / 256, 148u * 8u);
+    drive_fold_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->nslots, t, pa, net->d_drv_fold.p);
+  }
   SG_CUDA(cudaGetLastError());
+  net->drv_folded = t - 1;
+}
+
+// Emptying the rings also drops the deferred drive of the last step.
+void drop_drive(sg_net *net) {
+  if (!net->any_drv || !net->built || net->host_step == 0) return;
+  const unsigned long long v = net->host_step - 1;
+  SG_CUDA(cudaMemcpyAsync(net->d_drv_fold.p, &v, sizeof(v), cudaMemcpyHostToDevice, net->stream));
+  SG_CUDA(cudaStreamSynchronize(net->stream));
+  net->drv_folded = v;
 }
 
 void finish_build(sg_net *net) {
@@ -1238,6 +1378,8 @@ void finish_build(sg_net *net) {
   net->d_ev_step.zero(s);
   net->d_ev_total.alloc(1);
   net->d_ev_total.zero(s);
+  net->d_ev_src.alloc(2);
+  net->d_ev_src.zero(s);
   net->d_clamp.alloc(1);
   net->d_clamp.zero(s);
   net->d_stat_spk.alloc(net->stat_cap);
@@ -1246,12 +1388,10 @@ void finish_build(sg_net *net) {
   net->d_stat_ev.zero(s);
   net->scatter_smem = sizeof(ScatterSmem);
   const int sm = (int)net->scatter_smem;
-  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  SG_CUDA(cudaFuncSetAttribute(list_flush_all_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-  setup_lists(net);
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  setup_scatter(net);
+  if (net->weight_format == SG_W_FP8) net->d_edge.release();  // scanned by the exact-sum test; x + E4M3 + scale from here
   if (net->tm_edges) {  // build.rs:69-84: R = 1, U = U0 of the edge's profile, last = 0
     const uint64_t E = std::max<uint64_t>(net->n_edges, 1);
     net->d_tm_r.alloc(E);
@@ -1298,6 +1438,10 @@ void upload_pop_table(sg_net *net) {
     pa.noise_sigma[0] = p.noise_sigma[0];
     pa.noise_sigma[1] = p.noise_sigma[1];
     pa.bias = p.d_bias.n ? p.d_bias.p : nullptr;
+    pa.drv = p.drv ? 1 : 0;
+    pa.drv_seed0 = p.drv_seed0;
+    pa.drv_p = p.drv_p;
+    pa.drv_w = p.drv_w;
   }
   for (int m = 1; m <= 4; ++m) {
     net->model_blk_off[m] = (uint32_t)map.size();
@@ -1365,12 +1509,13 @@ void enqueue_rest(sg_net *net, const StepArgs &a) {
   for (const auto &p : net->pops)
     if (p.external && p.n)
       ext_spikes_kernel<<<p.cap / kNeuronBlock, kNeuronBlock, 0, s>>>(a, p.dev_off, p.n, p.ext_src);
-  if (a.list_mode) {
-    if (net->seg32) scatter_kernel<true, true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
-    else scatter_kernel<false, true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+  if (a.red) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
+    scatter_red_kernel<<<(unsigned)sms * kRedBlocksPerSM, kRedThreads, 0, s>>>(a);
   } else {
-    if (net->seg32) scatter_kernel<true, false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
-    else scatter_kernel<false, false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+    if (net->seg32) scatter_kernel<true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+    else scatter_kernel<false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
   }
   if (net->learn_on && net->n_edges) {
     LearnArgs L{};
@@ -2052,8 +2197,8 @@ int sg_set_weight_format(sg_net *net, int format) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "weight format must be set before build()");
-    SG_REQUIRE(format == SG_W_F32 || format == SG_W_BF16, SG_E_INVALID,
-               "weight format: FP32 and BF16 are available (FP8 is not built)");
+    SG_REQUIRE(format == SG_W_F32 || format == SG_W_BF16 || format == SG_W_FP8, SG_E_INVALID,
+               "weight format: SG_W_F32, SG_W_BF16 or SG_W_FP8");
     net->weight_format = format;
   });
 }
@@ -2063,19 +2208,16 @@ int sg_scatter_mode(sg_net *net, int *out) {
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "not built");
     SG_REQUIRE(out, SG_E_INVALID, "null output");
-    *out = !net->deterministic ? SG_SCATTER_ATOMIC : net->list_mode ? SG_SCATTER_EXACT : SG_SCATTER_ORDERED;
+    *out = !net->deterministic ? SG_SCATTER_ATOMIC : net->red ? SG_SCATTER_EXACT : SG_SCATTER_ORDERED;
   });
 }
 
 int sg_set_deterministic(sg_net *net, int on) {
   NET_CHECK(net);
   return run([&] {
-    if (net->built && net->deterministic && !on) {  // atomic adds go straight to the ring cells
-      DevGuard g(net->device);
-      flush_lists(net);
-    }
     net->deterministic = on ? 1 : 0;
     drop_graph(net);
+    if (net->built) update_path(net);
   });
 }
 
@@ -2084,8 +2226,8 @@ int sg_build(sg_net *net) {
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Network::build() called twice — the graph is already built");
     DevGuard g(net->device);
-    // GPEA Nernst constants with the host libm ln (gpea.rs:277-278)
-    net->ln_consts = {std::log(10.0f / 140.0f), std::log(5.0f / 140.0f)};
+    // GPEA Nernst constants (gpea.rs:277-278), with the ln the kernels use
+    net->ln_consts = {sg_logf(10.0f / 140.0f), sg_logf(5.0f / 140.0f)};
     const uint64_t E = net->e_pre.n;
     uint64_t src_e = 0;
     for (auto &s : net->srcs) src_e += s.post.size();
@@ -2096,6 +2238,7 @@ int sg_build(sg_net *net) {
     build_sources(net);
     if (net->stdp_on) build_stdp(net);
     split_bf16(net);
+    split_fp8(net);
     finish_build(net);
   });
 }
@@ -2182,7 +2325,7 @@ int sg_ring_clear(sg_net *net) {
     DevGuard g(net->device);
     net->d_ring.zero(net->stream);
     net->d_kin_g.zero(net->stream);
-    if (net->list_mode) net->d_lcnt.zero(net->stream);
+    drop_drive(net);
     SG_CUDA(cudaStreamSynchronize(net->stream));
   });
 }
@@ -2212,6 +2355,7 @@ int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals,
     }
     SG_CUDA(cudaMemcpyAsync(net->d_inj_idx.p, idx, n * 4, cudaMemcpyHostToDevice, net->stream));
     SG_CUDA(cudaMemcpyAsync(net->d_inj_val.p, vals, n * 4, cudaMemcpyHostToDevice, net->stream));
+    fold_drive(net);  // the last step's deferred drive precedes this input in the slot
     unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 8);
     inject_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->nslots, net->d_step.p, net->d_inj_idx.p,
                                                    net->d_inj_val.p, n, p.dev_off, dup ? 1 : 0);
@@ -2508,15 +2652,48 @@ int sg_events_total(sg_net *net, uint64_t *out) {
   });
 }
 
+int sg_source_events_total(sg_net *net, uint64_t *out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    if (!net->built) {
+      *out = 0;
+      return;
+    }
+    DevGuard g(net->device);
+    unsigned long long v = 0;
+    SG_CUDA(cudaMemcpyAsync(&v, net->d_ev_src.p + 1, 8, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    *out = v;
+  });
+}
+
 static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8_t *d, bool only_w,
-                            uint8_t *syn = nullptr) {
+                            uint8_t *syn = nullptr, uint8_t *plastic = nullptr) {
   const uint32_t Nd = net->Nd;
   const uint64_t E = net->n_edges;
   std::vector<uint32_t> rp(Nd + 1);
   std::vector<uint2> ed(E);
   std::vector<uint8_t> code(net->packed ? 0 : E);
   SG_CUDA(cudaMemcpyAsync(rp.data(), net->d_row_ptr.p, ((size_t)Nd + 1) * 4, cudaMemcpyDeviceToHost, net->stream));
-  if (E && net->weight_format == SG_W_BF16) {
+  if (E && net->weight_format == SG_W_FP8) {
+    std::vector<uint32_t> ex(E);
+    std::vector<uint8_t> w8(E);
+    std::vector<float> sc(Nd);
+    SG_CUDA(cudaMemcpyAsync(ex.data(), net->d_edge_x.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(w8.data(), net->d_w8.p, E, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaMemcpyAsync(sc.data(), net->d_row_scale.p, (size_t)Nd * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (uint32_t r = 0; r < Nd; ++r)
+      for (uint64_t e = rp[r]; e < rp[r + 1]; ++e) {
+        const float v = host_e4m3(w8[e]) * sc[r];
+        uint32_t bits;
+        std::memcpy(&bits, &v, 4);
+        ed[e] = make_uint2(ex[e], bits);
+      }
+    if (!net->packed && !only_w)
+      SG_CUDA(cudaMemcpyAsync(code.data(), net->d_code.p, E, cudaMemcpyDeviceToHost, net->stream));
+  } else if (E && net->weight_format == SG_W_BF16) {
     std::vector<uint32_t> ex(E);
     std::vector<uint16_t> w16(E);
     SG_CUDA(cudaMemcpyAsync(ex.data(), net->d_edge_x.p, E * 4, cudaMemcpyDeviceToHost, net->stream));
@@ -2547,6 +2724,7 @@ static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float
     col[e] = d2g[post];
     d[e] = (uint8_t)code_delay(c);
     if (syn) syn[e] = (uint8_t)code_ring(c);
+    if (plastic) plastic[e] = code_stdp(c) ? 1 : 0;
   }
 }
 
@@ -2557,6 +2735,19 @@ int sg_graph_read(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *w, uint8
     SG_REQUIRE(row_ptr && col && w && d, SG_E_INVALID, "null output");
     DevGuard g(net->device);
     read_csr_global(net, row_ptr, col, w, d, false);
+  });
+}
+
+int sg_graph_read_types(sg_net *net, uint8_t *syn_types, uint8_t *stdp) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "not built");
+    SG_REQUIRE(syn_types && stdp, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    std::vector<uint32_t> rp(net->total + 1), col(net->n_edges);
+    std::vector<float> w(net->n_edges);
+    std::vector<uint8_t> d(net->n_edges);
+    read_csr_global(net, rp.data(), col.data(), w.data(), d.data(), false, syn_types, stdp);
   });
 }
 
@@ -2578,7 +2769,7 @@ int sg_ring_read(sg_net *net, uint32_t ring, float *out) {
     SG_REQUIRE(out, SG_E_INVALID, "null output");
     DevGuard g(net->device);
     const uint32_t Nd = net->Nd, M = net->nslots;
-    flush_lists(net);
+    fold_drive(net);
     std::vector<float> r((size_t)M * Nd);
     SG_CUDA(cudaMemcpyAsync(r.data(), net->d_ring.p + (size_t)ring * M * Nd, r.size() * 4,
                             cudaMemcpyDeviceToHost, net->stream));
@@ -2720,7 +2911,8 @@ int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float 
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "learning needs a built network");
     SG_REQUIRE(!net->learn_on, SG_E_STATE, "learning is already enabled");
-    SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID, "BF16 weights are read-only: learning needs FP32 weights");
+    SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID,
+               "BF16 and FP8 weights are read-only: learning needs FP32 weights");
     const float v[9] = {dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max};
     for (float x : v) SG_REQUIRE(std::isfinite(x), SG_E_INVALID, "learning config: values must be finite");
     SG_REQUIRE(dt > 0 && tau_pre > 0 && tau_post > 0 && tau_e > 0 && w_min <= w_max, SG_E_INVALID,
@@ -2728,9 +2920,9 @@ int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float 
     DevGuard g(net->device);
     cudaStream_t s = net->stream;
     // rewards change weights, so the exact-sum condition of the rings no
-    // longer holds: pending lists go to the rings, the ordered path takes over
-    flush_lists(net);
-    net->list_mode = 0;
+    // longer holds: the ordered path takes over
+    net->exact = false;
+    update_path(net);
     drop_graph(net);
     const uint32_t Nd = net->Nd;
     const uint64_t E = net->n_edges;
@@ -3032,7 +3224,6 @@ int sg_taas_save(sg_net *net, const char *path, const char *created, int zstd_le
     SG_REQUIRE(N < 0x7FFFFFFFull && E <= 0x7FFFFFFFull, SG_E_OVERFLOW,
                "the .taas connectome sections are i32: at most 2^31 - 1 synapses and neurons");
     DevGuard g(net->device);
-    flush_lists(net);
     std::vector<uint32_t> rp(N + 1), col(E);
     std::vector<float> w(E);
     std::vector<uint8_t> d(E), st(E);
@@ -3074,7 +3265,8 @@ int sg_taas_load_weights(sg_net *net, const char *path) {
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "not built");
     SG_REQUIRE(path, SG_E_INVALID, "null path");
-    SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID, "BF16 weights are read-only: loading needs FP32 weights");
+    SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID,
+               "BF16 and FP8 weights are read-only: loading needs FP32 weights");
     taas::Reader r;
     r.open(path);
     const uint64_t N = net->total, E = net->n_edges;
@@ -3090,8 +3282,8 @@ int sg_taas_load_weights(sg_net *net, const char *path) {
     SG_REQUIRE(std::memcmp(rp.data(), nrp.data(), rp.size()) == 0 &&
                    (E == 0 || std::memcmp(col.data(), ncol.data(), col.size()) == 0),
                SG_E_INVALID, "snapshot synapses (row_ptr, col_indices) differ from the network's");
-    flush_lists(net);
-    net->list_mode = 0;
+    net->exact = false;  // weights from the file: the exact-sum test no longer covers them
+    update_path(net);
     drop_graph(net);
     if (E)
       SG_CUDA(cudaMemcpy2DAsync((char *)net->d_edge.p + 4, 8, vals.data(), 4, 4, E, cudaMemcpyHostToDevice,
@@ -3159,7 +3351,7 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          (net->packed ? 0 : net->d_code.n) + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
          net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
-         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_lpost.n * 2 + net->d_lw.n * 4 + net->d_lcnt.n * 4 +
+         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_red_flat.n * 4 + net->d_run_off.n * 4 + net->d_w8.n + net->d_row_scale.n * 4 +
          (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4 +
          net->d_pt.n + (net->d_tm_r.n + net->d_tm_u.n + net->d_tm_last.n) * 4 +
          (net->d_l_tp.n + net->d_l_tq.n + net->d_l_baked.n + net->d_l_qb.n + net->d_l_in_ptr.n + net->d_l_in_edge.n +

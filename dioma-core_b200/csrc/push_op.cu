@@ -26,26 +26,42 @@ struct PushScratch {
   uint32_t *tile_cur;   // [n_tiles]   fill cursors
   uint32_t *tile_base;  // [n_tiles+1] exclusive prefix of tile_cnt
   unsigned long long *total;  // [1]   events of this call
+  uint32_t *bad;        // [1]   bit 0: an active entry >= n_neurons; bit 1: a col entry >= n_neurons
   uint32_t *bkey;       // [events]
   float *bw;            // [events]
   uint32_t *bcell;      // [events]
 };
 
+// Counts the events per post tile.  Entries outside [0, n_neurons) in
+// `active` or `col` are not followed: they set a bit of s.bad, which the host
+// reads with the total and turns into an error before anything is written.
 __global__ void push_count_kernel(const uint32_t *row_ptr, const uint32_t *col, const uint32_t *active,
-                                  uint32_t n_active, PushScratch s) {
+                                  uint32_t n_active, uint32_t n_neurons, PushScratch s) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t r = gw; r < n_active; r += nw) {
     const uint32_t pre = active[r];
+    if (pre >= n_neurons) {
+      if (lane == 0) atomicOr(s.bad, 1u);
+      continue;
+    }
     const uint32_t beg = row_ptr[pre], end = row_ptr[pre + 1];
     if (lane == 0 && end > beg) atomicAdd(s.total, (unsigned long long)(end - beg));
     for (uint32_t e0 = beg; e0 < end; e0 += 32) {
       const uint32_t e = e0 + lane;
-      const bool ok = e < end;
+      bool ok = e < end;
+      uint32_t post = 0;
+      if (ok) {
+        post = col[e];
+        if (post >= n_neurons) {
+          atomicOr(s.bad, 2u);
+          ok = false;
+        }
+      }
       const uint32_t mask = __ballot_sync(0xffffffffu, ok);
       if (ok) {
-        const uint32_t tile = col[e] >> kPushTileShift;
+        const uint32_t tile = post >> kPushTileShift;
         const uint32_t peers = __match_any_sync(mask, tile);
         if (lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(s.tile_cnt + tile, (uint32_t)__popc(peers));
       }
@@ -183,12 +199,17 @@ int push_run(const uint32_t *row_ptr, const uint32_t *col, const float *w, const
   SG_CUDA(cudaMemsetAsync(s.tile_cnt, 0, (size_t)n_tiles * 4, st));
   SG_CUDA(cudaMemsetAsync(s.tile_cur, 0, (size_t)n_tiles * 4, st));
   SG_CUDA(cudaMemsetAsync(s.total, 0, 8, st));
+  SG_CUDA(cudaMemsetAsync(s.bad, 0, 4, st));
   if (n_active == 0) return SG_OK;
-  push_count_kernel<<<push_grid(n_active), 256, 0, st>>>(row_ptr, col, active, n_active, s);
+  push_count_kernel<<<push_grid(n_active), 256, 0, st>>>(row_ptr, col, active, n_active, n_neurons, s);
   SG_CUDA(cudaGetLastError());
   unsigned long long total = 0;
+  uint32_t bad = 0;
   SG_CUDA(cudaMemcpyAsync(&total, s.total, 8, cudaMemcpyDeviceToHost, st));
+  SG_CUDA(cudaMemcpyAsync(&bad, s.bad, 4, cudaMemcpyDeviceToHost, st));
   SG_CUDA(cudaStreamSynchronize(st));
+  SG_REQUIRE(!(bad & 1u), SG_E_INVALID, "push_spikes: an active neuron index is >= n_neurons; the ring was not modified");
+  SG_REQUIRE(!(bad & 2u), SG_E_INVALID, "push_spikes: a col entry of an active row is >= n_neurons; the ring was not modified");
   if (total == 0) return SG_OK;
   const int rc = alloc_bins(total, s);
   if (rc != SG_OK) return rc;
@@ -202,11 +223,10 @@ int push_run(const uint32_t *row_ptr, const uint32_t *col, const float *w, const
 
 int push_check_args(const uint32_t *row_ptr, const uint32_t *col, const float *w, const uint8_t *delay,
                     uint32_t n_neurons, const uint32_t *active, uint32_t n_active, float *ring) {
-  SG_REQUIRE(row_ptr && ring && (n_active == 0 || active), SG_E_INVALID, "push_spikes: null device pointer");
+  SG_REQUIRE(row_ptr && ring, SG_E_INVALID, "push_spikes: null device pointer (row_ptr or ring)");
+  SG_REQUIRE(n_active == 0 || (active && col && w && delay), SG_E_INVALID,
+             "push_spikes: null device pointer (active, col, weights or delays)");
   SG_REQUIRE(n_neurons > 0, SG_E_INVALID, "push_spikes: n_neurons must be > 0");
-  (void)col;
-  (void)w;
-  (void)delay;
   return SG_OK;
 }
 
@@ -236,11 +256,12 @@ extern "C" int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, cons
     const uint32_t n_tiles = push_tiles(n_neurons);
     PushScratch s{};
     void *small = nullptr;
-    SG_CUDA(cudaMalloc(&small, (size_t)n_tiles * 12 + 4 + 16));
+    SG_CUDA(cudaMalloc(&small, (size_t)n_tiles * 12 + 32));
     s.tile_cnt = (uint32_t *)small;
     s.tile_cur = s.tile_cnt + n_tiles;
     s.tile_base = s.tile_cur + n_tiles;
     s.total = (unsigned long long *)(((uintptr_t)(s.tile_base + n_tiles + 1) + 7) & ~(uintptr_t)7);
+    s.bad = (uint32_t *)(s.total + 1);
     void *bins = nullptr;
     int rc = SG_OK;
     try {
@@ -269,10 +290,14 @@ extern "C" int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, cons
 
 // ---------------------------------------------------------------------------
 // sg_push_spikes_noalloc: the same operator for callers that cannot allocate
-// device memory while they run (a host inside a CUDA-graph capture that must
-// stay allocation-free, a real-time loop that forbids cudaMalloc, an embedding
-// with a fixed memory budget).  Its scratch is one file-scope __device__
-// array of fixed size that every GPU loading this library keeps until exit.
+// device memory while they run: a real-time loop whose timing budget has no
+// room for cudaMalloc/cudaFree (they can block on the driver and synchronise
+// the device), or an embedding that is handed a fixed device-memory budget up
+// front and owns every allocation itself.  Its scratch is one file-scope
+// __device__ array of fixed size that every GPU loading this library keeps
+// until the process exits.  Like sg_push_spikes, a call waits on its stream
+// once (it reads the event count back to the host) and returns after the
+// ring is updated.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -280,7 +305,7 @@ constexpr uint32_t kNoAllocMaxEvents = 1u << 20;   // synaptic events per call
 constexpr uint32_t kNoAllocMaxNeurons = 1u << 23;  // 8,388,608 neurons
 constexpr uint32_t kNoAllocTiles = kNoAllocMaxNeurons >> kPushTileShift;  // 4096
 constexpr size_t kNoAllocCounterBytes = ((size_t)kNoAllocTiles * 3 + 1) * 4;
-constexpr size_t kNoAllocTotalOff = (kNoAllocCounterBytes + 255) & ~(size_t)255;
+constexpr size_t kNoAllocTotalOff = (kNoAllocCounterBytes + 255) & ~(size_t)255;  // total (8 B), then the bad flag
 constexpr size_t kNoAllocBinsOff = kNoAllocTotalOff + 256;
 constexpr size_t kNoAllocBytes = kNoAllocBinsOff + (size_t)kNoAllocMaxEvents * 12;  // ~12.1 MiB
 
@@ -293,7 +318,9 @@ std::mutex g_noalloc_mu;
 void *g_noalloc_addr[kMaxDevices] = {};
 
 // Resolve the scratch array's device address on the current device (first
-// call per device only).
+// call per device only).  The address is kept for the life of the process: a
+// cudaDeviceReset on that device (which unloads this module) leaves it stale,
+// so do not call this entry point again after resetting its device.
 int noalloc_scratch(void **out) {
   int dev = 0;
   SG_CUDA(cudaGetDevice(&dev));
@@ -331,6 +358,7 @@ extern "C" int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *c
     s.tile_cur = s.tile_cnt + kNoAllocTiles;
     s.tile_base = s.tile_cur + kNoAllocTiles;
     s.total = (unsigned long long *)(b + kNoAllocTotalOff);
+    s.bad = (uint32_t *)(s.total + 1);
     return push_run(row_ptr, col, weights, delays, n_neurons, active, n_active, step, ring, (cudaStream_t)stream, s,
                     [&](unsigned long long total, PushScratch &sc) -> int {
                       if (total > kNoAllocMaxEvents) {

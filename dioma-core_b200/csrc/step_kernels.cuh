@@ -9,15 +9,23 @@
 //                     bitmask word per warp, write the block's spiking
 //                     neurons in ascending order to its slot of the spike
 //                     list (no global atomics), update the STDP traces.
-//   scatter_kernel    one persistent block per SM; block j owns the posts
-//                     [j*P, (j+1)*P).  It walks the spike list in neuron
-//                     order, reads the segment of each spiking row that
-//                     targets its posts (rows are sorted by post; a per-row
-//                     table holds the segment bounds), rolls the Poisson
-//                     sources that target its posts, and applies every event
-//                     to the ring cells it owns.
+//   scatter_red_kernel  (networks whose ring sums are exact in FP32, and the
+//                     atomic mode) warps take the step's spiking rows, read
+//                     each row once, whole and coalesced, and add every event
+//                     to its ring cell in L2 with red.global.add: any order of
+//                     the adds gives the reference's bits when every partial
+//                     sum is exact.
+//   scatter_kernel    (every other network) one persistent block per SM;
+//                     block j owns the posts [j*P, (j+1)*P).  It walks the
+//                     spike list in neuron order, reads the segment of each
+//                     spiking row that targets its posts (rows are sorted by
+//                     post; a per-row table holds the segment bounds), rolls
+//                     the Poisson sources that target its posts, and applies
+//                     every event to the ring cells it owns, in order.
+// A population driven one-to-one by delay-1 Poisson sources takes that drive
+// in the neuron kernel of the next step (PopArgs::drv).
 //
-// Determinism.  The reference adds the events of one step to each ring cell
+// Determinism of the ordered scatter.  The reference adds the events of one step to each ring cell
 // in (spiking pre ascending, CSR row order) and then Poisson-source order
 // (push.rs:143-172, step.rs:166-185).  A block generates its events exactly
 // in that order (rows are stored sorted by post with a stable sort, which
@@ -32,6 +40,8 @@
 // cell therefore receives its adds in the reference's order, with the
 // reference's rounding.
 #pragma once
+#include <cuda_fp8.h>
+
 #include <cstdint>
 
 #include "common.cuh"
@@ -50,12 +60,7 @@ constexpr uint32_t kBlkChunk = kScatterThreads;      // spike-list slots scanned
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr unsigned long long kEmpty64 = ~0ull;
 constexpr uint32_t kMaxPops = 16;
-// pending-event lists (exact-sum mode): one per (scatter block, ring, slot);
-// a block owns at most kListPosts posts in this mode (a local post index
-// fits 16 bits)
-constexpr uint32_t kMaxKeys = 128;
 constexpr uint32_t kMaxTm = 8;  // short-term plasticity profiles on the device
-constexpr uint32_t kListPosts = 32768;
 
 // neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
 // GPEA/HH are compute heavy and keep one neuron per thread
@@ -77,6 +82,8 @@ struct StepArgs {
   uint32_t *done;
   unsigned long long *ev_step;
   unsigned long long *ev_total;
+  unsigned long long *ev_src_step;   // of which Poisson-source events (this step)
+  unsigned long long *ev_src_total;
   uint32_t *stat_spk;
   unsigned long long *stat_ev;
   uint32_t stat_cap;
@@ -113,6 +120,11 @@ struct StepArgs {
   int wbf16;
   const uint32_t *edge_x;
   const uint16_t *w16;
+  // FP8 E4M3 weight storage: x words in edge_x, one E4M3 byte per synapse and
+  // one FP32 scale per row (weight = e4m3 value * row scale, 5 B per synapse)
+  int wfp8;
+  const uint8_t *w8;
+  const float *row_scale;
   uint32_t post_mask;
   uint32_t n_edges;
   // per-row segment table: [Nd][G+1] offsets inside the row (u16 or u32)
@@ -134,23 +146,22 @@ struct StepArgs {
   const uint8_t *run_code;
   // scatter mode
   int deterministic;
-  // pending-event lists (exact-sum mode): when every weight that reaches a
-  // ring is a multiple of one power of two 2^e and no post's weights sum in
-  // magnitude to 2^(23+e), every partial sum of a ring cell is exact in
-  // FP32, so float addition on the rings is associative and any order of
-  // the adds gives the bits of the reference's order.  The scatter then
-  // appends each event to the list of (its scatter block, ring, arrival
-  // slot) = key ring * nslots + slot, and a list is added to its ring cells
-  // in shared memory before the slot is read (the block's lists of slot
-  // step + 1 at the end of every step), or earlier when it would overflow.
-  // List (j, key): lpost/lw[(j * nkeys + key) * lcap + i], local post index
-  // and weight; lcnt[j * nkeys + key] entries.
-  int list_mode;
-  uint32_t nkeys;
-  uint32_t lcap;
-  uint16_t *lpost;
-  float *lw;
-  uint32_t *lcnt;
+  // pre-centric scatter (networks whose ring sums are exact, and the atomic
+  // mode): this step's spiking neurons in any order (red_flat, red_cnt
+  // entries; the neuron kernel appends, the scatter's last block resets the
+  // count), every event added to its ring cell in L2 with red.global.add
+  int red;
+  uint32_t *red_flat;
+  uint32_t *red_cnt;
+  // Poisson-source synapses of the pre-centric scatter: run r covers source
+  // synapses [run_off[r], run_off[r + 1]) of the n_src_syn in runs
+  const uint32_t *run_off;
+  uint32_t n_runs;
+  uint32_t n_src_syn;
+  // deferred drive: the step whose deferred Poisson events were already
+  // added to the ring (by drive_fold_kernel before an inject or a ring
+  // readback), or ~0
+  const unsigned long long *drv_fold;
   // Tsodyks-Markram short-term plasticity: per-edge profile id (0 = none)
   // and state R, U, last spike step (CSR order), the profiles' constants
   int tm;
@@ -198,6 +209,16 @@ struct PopArgs {
   // constant per-neuron input current added every step (as an
   // inject_current of the same values each step would), or null
   const float *bias;
+  // deferred drive: neuron i has one Poisson source (seed drv_seed0 + i,
+  // rate p = drv_p) with one synapse of weight drv_w and delay <= 1 onto it,
+  // and no other source synapse.  Its event of step t arrives in slot t + 1
+  // as the last add before that slot is read (later steps' events land in
+  // later slots; an inject_current in between first folds it into the ring),
+  // so the neuron kernel of step t + 1 rolls it and adds it to the slot
+  // value it read: the same float sums as the ring, without the event.
+  int drv;
+  uint32_t drv_seed0;
+  float drv_p, drv_w;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -264,10 +285,22 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, unsigne
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// E4M3 byte -> FP32 (exact).
+__device__ __forceinline__ float e4m3_to_f32(uint32_t b) {
+  __nv_fp8_e4m3 v;
+  v.__x = (__nv_fp8_storage_t)b;
+  return (float)v;
+}
+
 // One synapse record (x = post | code << 24, y = f32 weight bits); the bf16
-// form widens the stored weight to f32 (its upper 16 bits).
-__device__ __forceinline__ uint2 ld_record(const StepArgs &a, uint32_t e, unsigned long long pol) {
+// form widens the stored weight to f32 (its upper 16 bits), the fp8 form
+// multiplies the E4M3 value by its row's scale.
+__device__ __forceinline__ uint2 ld_record(const StepArgs &a, uint32_t e, unsigned long long pol,
+                                           float scale = 1.0f) {
   if (a.wbf16) return make_uint2(ld_stream_u32(a.edge_x + e, pol), ld_stream_u16(a.w16 + e, pol) << 16);
+  if (a.wfp8)
+    return make_uint2(ld_stream_u32(a.edge_x + e, pol),
+                      __float_as_uint(e4m3_to_f32(ld_stream_u8(a.w8 + e, pol)) * scale));
   return ld_stream_edge(a.edge + e, pol);
 }
 __device__ __forceinline__ float ld_ring(const float *p, unsigned long long pol) {
@@ -310,6 +343,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   using V = VecF<NPT>;
   __shared__ uint32_t warp_cnt[32];
   __shared__ uint32_t warp_clamp[32];
+  __shared__ uint32_t warp_fire[32];
   const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
   const uint32_t i0 = blk * kNeuronBlock + tid * NPT;  // population index of my first neuron
   const uint32_t gi0 = p.dev_off + i0;
@@ -322,6 +356,17 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   float *rs = a.ring + (size_t)slot * a.Nd + gi0;
   V::load(rs, x);
   V::store(rs, zero);
+  uint32_t nfire = 0;  // this step's deferred-drive events (counted now, applied next step)
+  if (p.drv) {
+    const bool take = step >= 1 && *a.drv_fold != step - 1;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (i0 + q < p.n) {
+        const uint32_t seed = p.drv_seed0 + i0 + q;
+        if (take && poisson_spike(seed, 0, step - 1, p.drv_p)) x[q] = x[q] + p.drv_w;
+        nfire += poisson_spike(seed, 0, step, p.drv_p) ? 1u : 0u;
+      }
+  }
   if (p.bias != nullptr) {
     float bv[NPT];
     V::ldg(p.bias + i0, bv);
@@ -335,14 +380,18 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
       if (i0 + q < p.n) {
         const uint32_t i = i0 + q;
         const double z = hash_std_normal(p.noise_seed, p.noise_stream, (unsigned long long)i + t * p.noise_stride);
-        x[q] = x[q] + (float)(p.noise_sigma[i < p.noise_split ? 0 : 1] * z);
+        x[q] = x[q] + (float)((i < p.noise_split ? p.noise_sigma[0] : p.noise_sigma[1]) * z);
       }
   }
   float sv[NS][NPT];
 #pragma unroll
   for (int c = 0; c < NS; ++c) V::load(p.state + (size_t)c * p.cap + i0, sv[c]);
-  // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start
-  for (int k = 0; k < a.n_kin; ++k) {
+  // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start.
+  // Unrolled over the (at most 3) profiles so that the profile constants are
+  // indexed at compile time and stay in the kernel parameter space.
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (k >= a.n_kin) break;
     float jump[NPT], s0[NPT], s1[NPT], s2[NPT];
     float *ks = a.ring + ((size_t)(k + 1) * a.nslots + slot) * a.Nd + gi0;
     V::load(ks, jump);
@@ -461,29 +510,51 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= (uint32_t)o) incl += y;
   }
-  uint32_t clw = nclamp;
+  uint32_t clw = nclamp, fw = nfire;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) clw += __shfl_xor_sync(0xffffffffu, clw, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    clw += __shfl_xor_sync(0xffffffffu, clw, o);
+    fw += __shfl_xor_sync(0xffffffffu, fw, o);
+  }
   if (lane == 31) warp_cnt[wid] = incl;
-  if (lane == 0) warp_clamp[wid] = clw;
+  if (lane == 0) {
+    warp_clamp[wid] = clw;
+    warp_fire[wid] = fw;
+  }
   __syncthreads();
   constexpr uint32_t NW = NeuronCfg<MODEL>::THREADS / 32;
-  uint32_t before = incl - cnt, total = 0, clamp_tot = 0;
+  uint32_t before = incl - cnt, total = 0, clamp_tot = 0, fire_tot = 0;
 #pragma unroll
   for (uint32_t k = 0; k < NW; ++k) {
     const uint32_t c = warp_cnt[k];
     before += k < wid ? c : 0u;
     total += c;
     clamp_tot += warp_clamp[k];
+    fire_tot += warp_fire[k];
   }
   const uint32_t gblk = gi0 / kNeuronBlock;
-  uint2 *out = a.spk + (size_t)gblk * kNeuronBlock + before;
+  if (a.red) {
+    // pre-centric scatter: the block's spiking neurons at one place of the flat list
+    __shared__ uint32_t red_base;
+    if (tid == 0) red_base = total ? atomicAdd(a.red_cnt, total) : 0u;
+    __syncthreads();
+    uint32_t pos = red_base + before;
 #pragma unroll
-  for (int q = 0; q < NPT; ++q)
-    if (nib & (1u << q)) *out++ = make_uint2(gi0 + q, __ldg(a.row_ptr + gi0 + q));
+    for (int q = 0; q < NPT; ++q)
+      if (nib & (1u << q)) a.red_flat[pos++] = gi0 + q;
+  } else {
+    uint2 *out = a.spk + (size_t)gblk * kNeuronBlock + before;
+#pragma unroll
+    for (int q = 0; q < NPT; ++q)
+      if (nib & (1u << q)) *out++ = make_uint2(gi0 + q, __ldg(a.row_ptr + gi0 + q));
+  }
   if (tid == 0) {
-    a.blk_cnt[gblk] = total;
+    if (!a.red) a.blk_cnt[gblk] = total;
     if (a.clamp_hits != nullptr && clamp_tot) atomicAdd(a.clamp_hits, (unsigned long long)clamp_tot);
+    if (fire_tot) {
+      atomicAdd(a.ev_step, (unsigned long long)fire_tot);
+      atomicAdd(a.ev_src_step, (unsigned long long)fire_tot);
+    }
   }
   // pair-STDP traces: x = fma(x, d, s) (P/api/learn/brain.rs:212-222)
   if (a.stdp) {
@@ -580,36 +651,23 @@ __device__ __forceinline__ uint32_t upper_index(const uint32_t *pre, uint32_t n,
 }
 
 struct WinSmem {                  // one window of events
-  uint32_t head[kBuckets];        // ring mode: latest-linked event of each bucket;
-                                  //   list mode: edge ids; spike rows while a
-                                  //   sub-chunk's segments are fetched
-  uint32_t ecell[kWin];           // window events in reference order: cell (ring mode) or
-                                  //   key << 16 | local post (list mode); the edge id
-                                  //   (ring mode) or record x word (list mode) before
+  uint32_t head[kBuckets];        // latest-linked event of each bucket; spike rows
+                                  //   while a sub-chunk's segments are fetched
+  uint32_t ecell[kWin];           // window events in reference order: cell, or the
+                                  //   edge id before the records are read
   float ew[kWin];                 //   weight,
-  uint16_t enext[kWin];           //   ring mode: next event of the same bucket
-  uint32_t w16p[kWin];            // list mode, bf16 weights: the aligned pair holding
-                                  //   the event's weight
-};
-struct FlushSmem {                // one list being added to its ring cells
-  float acc[kListPosts];          // the block's ring cells of the list's (ring, slot)
-  uint16_t fpost[kWin];           // one window of the list: local posts
-  float fw[kWin];                 //   and weights
+  uint16_t enext[kWin];           //   next event of the same bucket
 };
 struct ScatterSmem {
-  union {
-    WinSmem w;
-    FlushSmem f;
-  } u;
+  WinSmem w;
   uint32_t plo[kPreChunk];        // absolute first edge of each row segment
+  float pscale[kPreChunk];        // FP8 weights: the row's scale
   uint32_t pseg[kPreChunk + 1];   // prefix of segment lengths
   uint32_t boff[kBlkChunk + 1];   // prefix of spike-list slot counts
   uint32_t wsum[32];
-  uint32_t lcnt[kMaxKeys];        // list mode: entries in each of this block's lists
-  uint32_t wkey[kMaxKeys];        //   window events per key, then the placing cursor
-  uint32_t wstart[kMaxKeys];      //   first grouped window entry per key
   double drift;
   unsigned long long events;
+  unsigned long long src_events;
 };
 static_assert(sizeof(ScatterSmem) <= 232448, "scatter shared memory exceeds 227 KB");
 
@@ -623,7 +681,7 @@ __device__ __forceinline__ float *cell_addr(const StepArgs &a, uint32_t cell, ui
 
 __device__ __forceinline__ void clear_heads(ScatterSmem &S) {
 #pragma unroll
-  for (uint32_t r = 0; r < kBPT; ++r) S.u.w.head[threadIdx.x + r * kScatterThreads] = kEmpty;
+  for (uint32_t r = 0; r < kBPT; ++r) S.w.head[threadIdx.x + r * kScatterThreads] = kEmpty;
 }
 
 // Knuth's multiplicative hash of the cell onto the buckets
@@ -633,8 +691,8 @@ constexpr uint32_t kNone16 = 0xFFFFu;
 // Prepend event k to the list of its bucket (list order is arbitrary; the
 // walk below compares event indices).
 __device__ __forceinline__ void link_event(ScatterSmem &S, uint32_t k) {
-  const uint32_t prev = atomicExch(&S.u.w.head[bucket_of(S.u.w.ecell[k])], k);
-  S.u.w.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
+  const uint32_t prev = atomicExch(&S.w.head[bucket_of(S.w.ecell[k])], k);
+  S.w.enext[k] = (uint16_t)(prev == kEmpty ? kNone16 : prev);
 }
 
 // Apply the window's m linked events to the ring in reference order.  Each
@@ -659,12 +717,12 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     pv[r] = kNone16;
     w[r] = 0.0f;
     if (k < m) {
-      const uint32_t c = S.u.w.ecell[k];
+      const uint32_t c = S.w.ecell[k];
       bool last = true;
-      uint32_t j = S.u.w.head[bucket_of(c)];
+      uint32_t j = S.w.head[bucket_of(c)];
       if (j == kEmpty) j = kNone16;
-      for (; j != kNone16; j = S.u.w.enext[j]) {
-        if (j == k || S.u.w.ecell[j] != c) continue;
+      for (; j != kNone16; j = S.w.enext[j]) {
+        if (j == k || S.w.ecell[j] != c) continue;
         if (j < k) {
           ++rk[r];
           if (pv[r] == kNone16 || j > pv[r]) pv[r] = j;
@@ -674,7 +732,7 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
       }
       lastm |= (last ? 1u : 0u) << r;
       maxrank = max(maxrank, rk[r]);
-      w[r] = S.u.w.ew[k];
+      w[r] = S.w.ew[k];
     }
   }
   // level 0: the first event of each cell adds to the loaded ring value
@@ -686,7 +744,7 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     const uint32_t k = threadIdx.x + r * kScatterThreads;
     if (k < m && rk[r] == 0) {
       v[r] = v[r] + w[r];
-      S.u.w.ew[k] = v[r];
+      S.w.ew[k] = v[r];
     }
   }
   // later ranks: partial sums in order, one level per round
@@ -695,8 +753,8 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
     for (uint32_t r = 0; r < kEPT; ++r) {
       const uint32_t k = threadIdx.x + r * kScatterThreads;
       if (k < m && rk[r] == lvl) {
-        v[r] = S.u.w.ew[pv[r]] + w[r];
-        S.u.w.ew[k] = v[r];
+        v[r] = S.w.ew[pv[r]] + w[r];
+        S.w.ew[k] = v[r];
       }
     }
   }
@@ -704,160 +762,22 @@ __device__ __forceinline__ void apply_window(const StepArgs &a, ScatterSmem &S, 
 #pragma unroll
   for (uint32_t r = 0; r < kEPT; ++r) {
     const uint32_t k = threadIdx.x + r * kScatterThreads;
-    if (k < m && (lastm & (1u << r))) st_ring(cell_addr(a, S.u.w.ecell[k], p0), v[r], pol);
+    if (k < m && (lastm & (1u << r))) st_ring(cell_addr(a, S.w.ecell[k], p0), v[r], pol);
   }
   __syncthreads();
 }
 
-// One event into the window (or straight into the ring in atomic mode).
-// `base` = step % nslots; the event lands in slot (step + max(delay, 1)) % nslots.
-template <bool LIST>
+// One event into the window.  `base` = step % nslots; the event lands in
+// slot (step + max(delay, 1)) % nslots.
 __device__ __forceinline__ uint32_t put_event(const StepArgs &a, ScatterSmem &S, uint32_t k, uint32_t post,
                                               float w, uint8_t code, uint32_t base, uint32_t p0) {
   uint32_t slot = base + max(code_delay(code), 1u);
   if (slot >= a.nslots) slot -= a.nslots;
   const uint32_t key = code_ring(code) * a.nslots + slot;
-  if (LIST) {
-    S.u.w.ecell[k] = (key << 16) | (post - p0);
-    S.u.w.ew[k] = w;
-    return 0;
-  }
   const uint32_t cell = (key << a.pbits) | (post - p0);
-  if (a.deterministic) {
-    S.u.w.ecell[k] = cell;
-    S.u.w.ew[k] = w;
-  } else {
-    atomicAdd(cell_addr(a, cell, p0), w);
-  }
+  S.w.ecell[k] = cell;
+  S.w.ew[k] = w;
   return cell;
-}
-
-// ---- pending-event lists (exact-sum mode) -----------------------------------
-// Append the window's m events (ecell/ew) to this block's lists.  The order
-// inside a list is free (the sums are exact), so the window is grouped by key
-// with shared-memory counters (count, offsets, place) into the idle head/w16p
-// arrays, and each key's run is then copied to the tail of its list with
-// coalesced stores.  Called by all threads after the barrier that publishes
-// ecell/ew; ends with a barrier.
-__device__ __forceinline__ void list_append(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t j) {
-  WinSmem &W = S.u.w;
-  const uint32_t tid = threadIdx.x, nk = a.nkeys;
-  if (tid < nk) S.wkey[tid] = 0;
-  __syncthreads();
-#pragma unroll
-  for (uint32_t r = 0; r < kEPT; ++r) {
-    const uint32_t k = tid + r * kScatterThreads;
-    if (k < m) atomicAdd(&S.wkey[W.ecell[k] >> 16], 1u);
-  }
-  __syncthreads();
-  if (tid < 32) {  // window offsets of the keys (nk <= kMaxKeys = 4 * 32)
-    uint32_t c[kMaxKeys / 32], run = 0;
-#pragma unroll
-    for (uint32_t q = 0; q < kMaxKeys / 32; ++q) {
-      const uint32_t key = tid * (kMaxKeys / 32) + q;
-      c[q] = key < nk ? S.wkey[key] : 0u;
-      run += c[q];
-    }
-    uint32_t x = run;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (tid >= (uint32_t)o) x += y;
-    }
-    uint32_t st = x - run;
-#pragma unroll
-    for (uint32_t q = 0; q < kMaxKeys / 32; ++q) {
-      const uint32_t key = tid * (kMaxKeys / 32) + q;
-      if (key < nk) {
-        S.wstart[key] = st;
-        S.wkey[key] = st;  // the placing cursor
-      }
-      st += c[q];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (uint32_t r = 0; r < kEPT; ++r) {
-    const uint32_t k = tid + r * kScatterThreads;
-    if (k < m) {
-      const uint32_t v = W.ecell[k];
-      const uint32_t i = atomicAdd(&S.wkey[v >> 16], 1u);
-      W.head[i] = v;
-      W.w16p[i] = __float_as_uint(W.ew[k]);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (uint32_t r = 0; r < kEPT; ++r) {
-    const uint32_t i = tid + r * kScatterThreads;
-    if (i < m) {
-      const uint32_t v = W.head[i], key = v >> 16;
-      const size_t off = ((size_t)j * nk + key) * a.lcap + S.lcnt[key] + (i - S.wstart[key]);
-      a.lpost[off] = (uint16_t)(v & 0xFFFFu);
-      a.lw[off] = __uint_as_float(W.w16p[i]);
-    }
-  }
-  __syncthreads();
-  if (tid < nk) S.lcnt[tid] += S.wkey[tid] - S.wstart[tid];
-  __syncthreads();
-}
-
-struct ListArgs {
-  float *ring;
-  const uint16_t *lpost;
-  const float *lw;
-  uint32_t Nd, nkeys, lcap;
-};
-__device__ __forceinline__ ListArgs list_args(const StepArgs &a) {
-  return ListArgs{a.ring, a.lpost, a.lw, a.Nd, a.nkeys, a.lcap};
-}
-
-// Add list (j, key) to its ring cells and empty it: the block's cells of the
-// key's (ring, slot) are copied to shared memory, the list is added to them
-// kWin events at a time with shared-memory atomics (exact sums: the order is
-// free), and the cells are written back.  Called by all threads with S.lcnt
-// stable; ends with a barrier.
-__device__ __noinline__ void list_flush(const ListArgs a, ScatterSmem &S, uint32_t key, uint32_t j, uint32_t p0,
-                                        uint32_t pj) {
-  FlushSmem &F = S.u.f;
-  const uint32_t tid = threadIdx.x;
-  const uint32_t n = S.lcnt[key];
-  if (n == 0) return;
-  const unsigned long long keep = policy_evict_last(), once = policy_evict_first();
-  // the cells: pj is a multiple of 32 and the range starts 128-byte aligned
-  float *cells = a.ring + (size_t)key * a.Nd + p0;
-  for (uint32_t c = tid; c < pj / 4; c += kScatterThreads) cp_async16(&F.acc[c * 4], cells + c * 4, keep);
-  // a list starts at a multiple of 256 entries and its capacity is one, so
-  // the 16-byte copies rounded up past the last entry stay inside the list
-  const size_t lb = ((size_t)j * a.nkeys + key) * a.lcap;
-  for (uint32_t w0 = 0; w0 < n; w0 += kWin) {
-    const uint32_t fm = min(kWin, n - w0);
-    for (uint32_t c = tid; c < (fm + 7) / 8; c += kScatterThreads)
-      cp_async16(&F.fpost[c * 8], a.lpost + lb + w0 + c * 8, once);
-    for (uint32_t c = tid; c < (fm + 3) / 4; c += kScatterThreads)
-      cp_async16(&F.fw[c * 4], a.lw + lb + w0 + c * 4, once);
-    cp_async_wait_all();
-    __syncthreads();  // window (and cells) in shared memory
-#pragma unroll
-    for (uint32_t r = 0; r < kEPT; ++r) {
-      const uint32_t k = tid + r * kScatterThreads;
-      if (k < fm) atomicAdd(&F.acc[F.fpost[k]], F.fw[k]);
-    }
-    __syncthreads();  // window applied before the next one is copied in
-  }
-  for (uint32_t i = tid; i < pj; i += kScatterThreads) cells[i] = F.acc[i];
-  __syncthreads();
-  if (tid == 0) S.lcnt[key] = 0;
-  __syncthreads();
-}
-
-// Before a window of m events: flush every list that might not hold them.
-__device__ __forceinline__ void list_reserve(const StepArgs &a, ScatterSmem &S, uint32_t m, uint32_t j, uint32_t p0,
-                                             uint32_t pj) {
-  const bool need = threadIdx.x < a.nkeys && S.lcnt[threadIdx.x] + m > a.lcap;
-  if (!__syncthreads_or(need)) return;
-  for (uint32_t key = 0; key < a.nkeys; ++key)
-    if (S.lcnt[key] + m > a.lcap) list_flush(list_args(a), S, key, j, p0, pj);
 }
 
 __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes) {
@@ -875,14 +795,17 @@ __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes
       }
       *a.ev_total += ev;
       *a.ev_step = 0;
+      *a.ev_src_total += *(volatile unsigned long long *)a.ev_src_step;
+      *a.ev_src_step = 0;
       *a.done = 0;
+      if (a.red) *a.red_cnt = 0;  // the next step's neuron kernel appends from 0
       *a.step = step + 1;
       __threadfence();
     }
   }
 }
 
-template <bool SEG32, bool LIST>
+template <bool SEG32>
 __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_kernel(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
@@ -896,8 +819,8 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   if (tid == 0) {
     S.drift = 0.0;
     S.events = 0;
+    S.src_events = 0;
   }
-  if (LIST && tid < a.nkeys) S.lcnt[tid] = a.lcnt[j * a.nkeys + tid];
   __syncthreads();
   uint32_t n_spikes = 0;
   double drift = 0.0;  // this thread's part of the step's STDP weight change
@@ -915,8 +838,8 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
       // rows tid*kPPT .. +kPPT of this sub-chunk: their spike-list entries,
       // then the bounds of each row's segment for this block, fetched with
       // asynchronous copies into the (idle) window area
-      uint2 *srow = reinterpret_cast<uint2 *>(S.u.w.head);  // [kPreChunk] (pre, row start)
-      uint32_t *sseg = S.u.w.ecell;                         // [kPreChunk][2] words holding lo, hi
+      uint2 *srow = reinterpret_cast<uint2 *>(S.w.head);  // [kPreChunk] (pre, row start)
+      uint32_t *sseg = S.w.ecell;                         // [kPreChunk][2] words holding lo, hi
       uint32_t len[kPPT], mylen = 0;
 #pragma unroll
       for (uint32_t q = 0; q < kPPT; ++q) {
@@ -960,6 +883,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
             hi = (sseg[2 * i + 1] >> ((uint32_t)((idx + 1) & 1) * 16)) & 0xFFFFu;
           }
           S.plo[i] = e.y + lo;
+          if (a.wfp8) S.pscale[i] = __ldg(a.row_scale + e.x);
           len[q] = hi - lo;
           mylen += len[q];
         }
@@ -978,11 +902,10 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
       __syncthreads();
       for (uint32_t w0 = 0; w0 < M; w0 += kWin) {
         const uint32_t m = min(kWin, M - w0);
-        if (LIST) list_reserve(a, S, m, j, p0, pj);
-        else if (a.deterministic) clear_heads(S);
+        clear_heads(S);
         // each spiking row writes the edge ids of its window events (rows are
         // short segments); then thread tid takes events k = tid + r*kScatterThreads
-        uint32_t *eid = LIST ? S.u.w.head : S.u.w.ecell;
+        uint32_t *eid = S.w.ecell;
 #pragma unroll
         for (uint32_t q = 0; q < kPPT; ++q) {
           const uint32_t i = tid * kPPT + q;
@@ -990,57 +913,18 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
             const uint32_t g0 = max(S.pseg[i], w0), g1 = min(S.pseg[i + 1], w0 + m);
             const uint32_t d = S.plo[i] - S.pseg[i];
             for (uint32_t g = g0; g < g1; ++g) eid[g - w0] = d + g;
+            if (a.wfp8)  // the row's scale beside each event until the records are read
+              for (uint32_t g = g0; g < g1; ++g) S.w.ew[g - w0] = S.pscale[i];
           }
         }
         __syncthreads();
         const unsigned long long spol = policy_evict_first();
-        if (LIST) {
-          // the window's records into shared memory (ecell <- x, ew <- weight;
-          // bf16: the aligned pair holding the weight into sw), all in flight
-          WinSmem &W = S.u.w;
-#pragma unroll
-          for (uint32_t r = 0; r < kEPT; ++r) {
-            const uint32_t k = tid + r * kScatterThreads;
-            if (k < m) {
-              const uint32_t e = W.head[k];
-              if (a.wbf16) {
-                cp_async4(&W.ecell[k], a.edge_x + e, spol);
-                cp_async4(&W.w16p[k], a.w16 + (e & ~1u), spol);
-              } else {
-                const uint32_t *rec = reinterpret_cast<const uint32_t *>(a.edge + e);
-                cp_async4(&W.ecell[k], rec, spol);
-                cp_async4(&W.ew[k], rec + 1, spol);
-              }
-            }
-          }
-          cp_async_wait_all();
-#pragma unroll
-          for (uint32_t r = 0; r < kEPT; ++r) {
-            const uint32_t k = tid + r * kScatterThreads;
-            if (k < m) {
-              const uint32_t e = W.head[k], x = W.ecell[k];
-              const uint32_t wb = a.wbf16 ? ((W.w16p[k] >> ((e & 1u) * 16)) & 0xFFFFu) << 16
-                                          : __float_as_uint(W.ew[k]);
-              const float w = __uint_as_float(wb);
-              const uint32_t post = x & a.post_mask;
-              const uint8_t code = a.code ? (uint8_t)ld_stream_u8(a.code + e, spol) : (uint8_t)(x >> 24);
-              put_event<true>(a, S, k, post, w, code, base, p0);
-              if (a.stdp && code_stdp(code)) {
-                // depression at a pre spike; the pushed weight is the pre-update one
-                const float w1 = fminf(fmaxf(w - a.a_minus * a.x_post[post], a.w_min), a.w_max);
-                a.edge[e].y = __float_as_uint(w1);
-                drift += (double)w1 - (double)w;
-              }
-            }
-          }
-          __syncthreads();
-          list_append(a, S, m, j);
-        } else {
+        {
         uint32_t ev_e[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
-          ev_e[r] = k < m ? S.u.w.ecell[k] : 0u;
+          ev_e[r] = k < m ? S.w.ecell[k] : 0u;
         }
         uint32_t ev_post[kEPT];
         float ev_w[kEPT];
@@ -1049,7 +933,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
           if (k < m) {
-            const uint2 rec = ld_record(a, ev_e[r], spol);
+            const uint2 rec = ld_record(a, ev_e[r], spol, a.wfp8 ? S.w.ew[k] : 1.0f);
             ev_post[r] = rec.x & a.post_mask;
             ev_w[r] = __uint_as_float(rec.y);
             ev_code[r] = a.code ? (uint8_t)ld_stream_u8(a.code + ev_e[r], spol) : (uint8_t)(rec.x >> 24);
@@ -1077,19 +961,19 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
           const uint32_t k = tid + r * kScatterThreads;
           pre[r] = 0.0f;
           if (k < m) {
-            const uint32_t cell = put_event<false>(a, S, k, ev_post[r], ev_wd[r], ev_code[r], base, p0);
-            if (a.deterministic) pre[r] = ld_ring(cell_addr(a, cell, p0), policy_evict_last());
+            const uint32_t cell = put_event(a, S, k, ev_post[r], ev_wd[r], ev_code[r], base, p0);
+            pre[r] = ld_ring(cell_addr(a, cell, p0), policy_evict_last());
             if (a.stdp && code_stdp(ev_code[r])) {
               // depression at a pre spike; the pushed weight is the pre-update one
               const float w1 = fminf(fmaxf(ev_w[r] - a.a_minus * a.x_post[ev_post[r]], a.w_min), a.w_max);
               a.edge[ev_e[r]].y = __float_as_uint(w1);
               drift += (double)w1 - (double)ev_w[r];
             }
-            if (a.deterministic) link_event(S, k);
+            link_event(S, k);
           }
         }
         __syncthreads();
-        if (a.deterministic) apply_window(a, S, m, p0, pre);
+        apply_window(a, S, m, p0, pre);
         }
       }
     }
@@ -1117,8 +1001,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     __syncthreads();
     for (uint32_t w0 = 0; w0 < T; w0 += kWin) {
       const uint32_t mt = min(kWin, T - w0);
-      if (LIST) list_reserve(a, S, mt, j, p0, pj);
-      else if (a.deterministic) clear_heads(S);
+      clear_heads(S);
       __syncthreads();
       // thread tid owns entries [tid*kEPT, +kEPT) of the window: roll them,
       // then an order-preserving compaction of the fired ones
@@ -1156,19 +1039,20 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
       uint32_t pos = block_excl_scan(__popc(fired), S.wsum, &m);  // all reads of the window are done
 #pragma unroll
       for (uint32_t r = 0; r < kEPT; ++r)
-        if (fired & (1u << r)) put_event<LIST>(a, S, pos++, e_post[r], e_w[r], e_code[r], base, p0);
-      if (tid == 0) S.events += m;
+        if (fired & (1u << r)) put_event(a, S, pos++, e_post[r], e_w[r], e_code[r], base, p0);
+      if (tid == 0) {
+        S.events += m;
+        S.src_events += m;
+      }
       __syncthreads();
-      if (LIST) {
-        if (m) list_append(a, S, m, j);
-      } else if (a.deterministic && m) {
+      if (m) {
         float pre[kEPT];
 #pragma unroll
         for (uint32_t r = 0; r < kEPT; ++r) {
           const uint32_t k = tid + r * kScatterThreads;
           pre[r] = 0.0f;
           if (k < m) {
-            pre[r] = ld_ring(cell_addr(a, S.u.w.ecell[k], p0), policy_evict_last());
+            pre[r] = ld_ring(cell_addr(a, S.w.ecell[k], p0), policy_evict_last());
             link_event(S, k);
           }
         }
@@ -1204,30 +1088,149 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     if (lane == 0 && drift != 0.0) atomicAdd(&S.drift, drift);
   }
   __syncthreads();
-  if (LIST) {
-    // the next step reads slot step + 1: its lists go to the ring cells now
-    const uint32_t nxt = base + 1 == a.nslots ? 0u : base + 1;
-    for (uint32_t k = nxt; k < a.nkeys; k += a.nslots) list_flush(list_args(a), S, k, j, p0, pj);
-    if (tid < a.nkeys) a.lcnt[j * a.nkeys + tid] = S.lcnt[tid];
-  }
   if (tid == 0) {
     if (S.events) atomicAdd(a.ev_step, S.events);
+    if (S.src_events) atomicAdd(a.ev_src_step, S.src_events);
     if (a.stdp && S.drift != 0.0) atomicAdd(a.drift, S.drift);
   }
   end_of_step(a, n_spikes);
 }
 
-// Every pending list of every block into its ring cells (before the rings
-// are read from the host, or the scatter mode changes).
-__global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) list_flush_all_kernel(StepArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ScatterSmem &S = *reinterpret_cast<ScatterSmem *>(smem_raw);
-  const uint32_t j = blockIdx.x, p0 = j * a.P;
-  const uint32_t pj = min(a.P, a.Nd - p0);
-  if (threadIdx.x < a.nkeys) S.lcnt[threadIdx.x] = a.lcnt[j * a.nkeys + threadIdx.x];
+// ---------------------------------------------------------------------------
+// Pre-centric scatter (rings_exact networks, and the atomic mode).  When every
+// partial sum of a ring cell is exact, the order of the adds does not change
+// a cell's bits, so each spiking row is read once, whole and coalesced, and
+// every event goes to its ring cell with a fire-and-forget red.global.add in
+// L2 (the rings stay L2-resident: the synapse records stream through with
+// evict_first, the ring cells are updated with evict_last).  Warps take the
+// step's spiking neurons round robin; rows longer than kRedLong synapses are
+// shared by the threads of the whole block that found them.  Poisson-source
+// synapses that the neuron kernel does not take (deferred drive) follow, one
+// per thread.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRedThreads = 256;
+constexpr uint32_t kRedBlocksPerSM = 4;
+constexpr uint32_t kRedLong = 2048;
+constexpr uint32_t kRedLongMax = 32;  // long rows one block keeps for itself
+constexpr uint32_t kRedUnroll = 8;
+
+__device__ __forceinline__ void red_add(float *p, float v, unsigned long long pol) {
+  asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
+
+// Events [e, end) of one row, this thread taking every `stride`-th one
+// (`scale`: the row's FP8 weight scale).
+__device__ __forceinline__ void red_range(const StepArgs &a, uint32_t e, uint32_t end, uint32_t stride,
+                                          uint32_t base, unsigned long long pf, unsigned long long pl,
+                                          float scale) {
+  for (; e < end; e += stride * kRedUnroll) {
+    uint2 rec[kRedUnroll];
+    uint32_t cd[kRedUnroll];
+#pragma unroll
+    for (uint32_t u = 0; u < kRedUnroll; ++u) {
+      const uint32_t k = e + u * stride;
+      if (k < end) {
+        rec[u] = ld_record(a, k, pf, scale);
+        cd[u] = a.code ? ld_stream_u8(a.code + k, pf) : (rec[u].x >> 24);
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kRedUnroll; ++u) {
+      const uint32_t k = e + u * stride;
+      if (k < end) {
+        const uint32_t post = rec[u].x & a.post_mask;
+        const uint8_t code = (uint8_t)cd[u];
+        uint32_t slot = base + max(code_delay(code), 1u);
+        if (slot >= a.nslots) slot -= a.nslots;
+        float *cell = a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + post;
+        red_add(cell, __uint_as_float(rec[u].y), pl);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) scatter_red_kernel(StepArgs a) {
+  __shared__ uint4 s_long[kRedLongMax];  // begin, end, scale bits
+  __shared__ uint32_t s_long_n;
+  __shared__ unsigned long long s_events, s_src_events;
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const uint32_t gw = (blockIdx.x * kRedThreads + tid) >> 5, W = (gridDim.x * kRedThreads) >> 5;
+  if (tid == 0) {
+    s_long_n = 0;
+    s_events = 0;
+    s_src_events = 0;
+  }
   __syncthreads();
-  for (uint32_t k = 0; k < a.nkeys; ++k) list_flush(list_args(a), S, k, j, p0, pj);
-  if (threadIdx.x < a.nkeys) a.lcnt[j * a.nkeys + threadIdx.x] = S.lcnt[threadIdx.x];
+  const unsigned long long step = *a.step;
+  const uint32_t base = (uint32_t)(step % a.nslots);
+  const uint32_t n = *a.red_cnt;
+  const unsigned long long pf = policy_evict_first(), pl = policy_evict_last();
+  unsigned long long ev = 0, src_ev = 0;
+  for (uint32_t r = gw; r < n; r += W) {
+    const uint32_t gi = a.red_flat[r];
+    const uint32_t beg = __ldg(a.row_ptr + gi), end = __ldg(a.row_ptr + gi + 1);
+    const float scale = a.wfp8 ? __ldg(a.row_scale + gi) : 1.0f;
+    if (end - beg > kRedLong) {
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&s_long_n, 1u);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      if (k < kRedLongMax) {
+        if (lane == 0) s_long[k] = make_uint4(beg, end, __float_as_uint(scale), 0u);
+        continue;
+      }
+    }
+    red_range(a, beg + lane, end, 32, base, pf, pl, scale);
+    if (lane == 0) ev += end - beg;
+  }
+  __syncthreads();
+  const uint32_t nl = min(s_long_n, kRedLongMax);
+  for (uint32_t k = 0; k < nl; ++k) {
+    const uint4 rr = s_long[k];
+    red_range(a, rr.x + tid, rr.y, kRedThreads, base, pf, pl, __uint_as_float(rr.z));
+    if (tid == 0) ev += rr.y - rr.x;
+  }
+  // Poisson-source synapses in runs, source order free (exact sums)
+  for (uint32_t t = blockIdx.x * kRedThreads + tid; t < a.n_src_syn; t += gridDim.x * kRedThreads) {
+    uint32_t lo = 0, hi = a.n_runs - 1;  // largest run with run_off[run] <= t
+    while (lo < hi) {
+      const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+      if (__ldg(a.run_off + mid) <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t off = t - __ldg(a.run_off + lo);
+    const float p = __ldg(a.run_p + lo);
+    if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + lo) + off, 0, step, p)) {
+      const uint8_t code = __ldg(a.run_code + lo);
+      uint32_t slot = base + max(code_delay(code), 1u);
+      if (slot >= a.nslots) slot -= a.nslots;
+      red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + __ldg(a.run_post0 + lo) + off,
+              __ldg(a.run_w + lo), pl);
+      ++src_ev;
+    }
+  }
+  ev += src_ev;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_xor_sync(0xffffffffu, ev, o);
+    src_ev += __shfl_xor_sync(0xffffffffu, src_ev, o);
+  }
+  if (lane == 0 && ev) atomicAdd(&s_events, ev);
+  if (lane == 0 && src_ev) atomicAdd(&s_src_events, src_ev);
+  __syncthreads();
+  if (tid == 0 && s_events) atomicAdd(a.ev_step, s_events);
+  if (tid == 0 && s_src_events) atomicAdd(a.ev_src_step, s_src_events);
+  end_of_step(a, n);
+}
+
+// Adds the deferred drive of step t - 1 (t >= 1) of one population into
+// slot t, where the ring would hold it, and records that it was added (the
+// neuron kernel of step t then leaves it out).
+__global__ void drive_fold_kernel(float *ring, uint32_t Nd, uint32_t nslots, unsigned long long t, PopArgs p,
+                                  unsigned long long *fold) {
+  float *rs = ring + (size_t)(t % nslots) * Nd + p.dev_off;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += gridDim.x * blockDim.x)
+    if (poisson_spike(p.drv_seed0 + i, 0, t - 1, p.drv_p)) rs[i] = rs[i] + p.drv_w;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *fold = t - 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -1452,8 +1455,15 @@ __global__ void __launch_bounds__(kNeuronBlock) ext_spikes_kernel(StepArgs a, ui
   uint32_t total;
   const uint32_t before = block_excl_scan(sp ? 1u : 0u, wsum, &total);
   const uint32_t gblk = gi / kNeuronBlock;
-  if (sp) a.spk[(size_t)gblk * kNeuronBlock + before] = make_uint2(gi, __ldg(a.row_ptr + gi));
-  if (tid == 0) a.blk_cnt[gblk] = total;
+  if (a.red) {
+    __shared__ uint32_t red_base;
+    if (tid == 0) red_base = total ? atomicAdd(a.red_cnt, total) : 0u;
+    __syncthreads();
+    if (sp) a.red_flat[red_base + before] = gi;
+  } else {
+    if (sp) a.spk[(size_t)gblk * kNeuronBlock + before] = make_uint2(gi, __ldg(a.row_ptr + gi));
+    if (tid == 0) a.blk_cnt[gblk] = total;
+  }
   if (i < n) {
     const float add = sp ? 1.0f : 0.0f;
     if (a.stdp) {

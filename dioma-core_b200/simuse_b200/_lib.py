@@ -75,7 +75,9 @@ SIGNATURES = {
     "sg_total_neurons": [vp, vp],
     "sg_num_synapses": [vp, vp],
     "sg_events_total": [vp, vp],
+    "sg_source_events_total": [vp, vp],
     "sg_graph_read": [vp, vp, vp, vp, vp],
+    "sg_graph_read_types": [vp, vp, vp],
     "sg_weights_read": [vp, vp],
     "sg_ring_read": [vp, u32, vp],
     "sg_stdp_drift": [vp, vp],

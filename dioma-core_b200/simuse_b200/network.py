@@ -345,6 +345,11 @@ class Network:
         return self._u64(lib().sg_events_total)
 
     @property
+    def source_events_total(self) -> int:
+        """Events of Poisson-source synapses among events_total."""
+        return self._u64(lib().sg_source_events_total)
+
+    @property
     def clamp_hits(self) -> int:
         return self._u64(lib().sg_clamp_hits)
 
@@ -360,6 +365,14 @@ class Network:
         d = np.empty(e, np.uint8)
         check(lib().sg_graph_read(self._h, _p(rp), _p(c), _p(w), _p(d)))
         return rp, c, w, d
+
+    def graph_types(self):
+        """Per synapse (graph order): synapse type and pair-STDP flag."""
+        e = self.num_synapses
+        st = np.empty(e, np.uint8)
+        pl = np.empty(e, np.uint8)
+        check(lib().sg_graph_read_types(self._h, _p(st), _p(pl)))
+        return st, pl
 
     def weights(self) -> np.ndarray:
         w = np.empty(self.num_synapses, np.float32)

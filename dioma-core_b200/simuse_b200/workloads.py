@@ -364,7 +364,7 @@ HH_PARAMS = (0.01, 1.0, 120.0, 36.0, 0.3, 50.0, -77.0, -54.4)  # dt c_m g_na g_k
 
 
 def add_hh_stdp(net, n: int = 100_000, seed: int = 3, mean_degree: float = 200.0, sd_degree: float = 80.0,
-                d_min: int = 1, d_max: int = 20, w_max: float = 0.5, model_hh: int = 4) -> int:
+                d_min: int = 1, d_max: int = 20, w_max: float = 0.5, model_hh: int = 4, edges=None) -> int:
     """The HH + pair-STDP network: n squid-axon HH neurons (RK4, dt 0.01 ms),
     the first 80 % excitatory; conductance synapses with exponential decay
     tau 5 ms (E_rev 0 mV excitatory, -80 mV inhibitory); lognormal out-degree
@@ -390,7 +390,16 @@ def add_hh_stdp(net, n: int = 100_000, seed: int = 3, mean_degree: float = 200.0
     ke = net.register_expone(5.0, 0.0, 0.01)
     ki = net.register_expone(5.0, -80.0, 0.01)
     net.stdp_config(0.01, 20.0, 20.0, 0.01, 0.0105, 0.0, 1.0)
-    net.connect_lognormal_outdegree(pop, pop, mean_degree, sd_degree, seed, True, n_exc, w_max, w_max,
-                                    random_w=True, delay=d_min, d_max=d_max, syn_type_exc=ke,
-                                    syn_type_inh=ki, stdp_exc=True)
+    if edges is None:
+        net.connect_lognormal_outdegree(pop, pop, mean_degree, sd_degree, seed, True, n_exc, w_max, w_max,
+                                        random_w=True, delay=d_min, d_max=d_max, syn_type_exc=ke,
+                                        syn_type_inh=ki, stdp_exc=True)
+    else:
+        # the same synapses as an explicit CSR (row_ptr, col, w, delay, syn type, STDP flag), e.g. a
+        # device-generated network read back with graph() / graph_types()
+        rp, col, w, d, st, pl = edges
+        pre = np.repeat(np.arange(n, dtype=np.uint32), np.diff(rp.astype(np.int64)))
+        for flag in (1, 0):
+            sel = pl == flag
+            net.connect(pop, pre[sel], pop, col[sel], w[sel], d[sel], syn_types=st[sel], stdp=bool(flag))
     return pop

@@ -259,8 +259,14 @@ int sg_step_counter(sg_net *net, uint64_t *out);                    /* build.rs:
 int sg_total_neurons(sg_net *net, uint64_t *out);                   /* build.rs:130-134 */
 int sg_num_synapses(sg_net *net, uint64_t *out);                    /* graph.rs:285-287 */
 int sg_events_total(sg_net *net, uint64_t *out);
+/* Of those, the events of Poisson-source synapses (sources.rs:5-14). */
+int sg_source_events_total(sg_net *net, uint64_t *out);
 /* Network::graph() -> SparseGraph CSR arrays, build.rs:186-188 */
 int sg_graph_read(sg_net *net, uint32_t *row_ptr, uint32_t *col, float *weights, uint8_t *delays);
+/* Per synapse, in sg_graph_read's order: the synapse type (0 static, 1..3 a
+   kinetic profile; SparseGraph::syn_types, P/api/net/graph.rs:67-80) and
+   whether pair STDP updates it (1) or not (0). */
+int sg_graph_read_types(sg_net *net, uint8_t *syn_types, uint8_t *stdp);
 int sg_weights_read(sg_net *net, float *weights); /* current CSR weights (STDP) */
 /* DelayBuffer contents [32][total_neurons] of ring 0 (static) or kinetic k */
 int sg_ring_read(sg_net *net, uint32_t ring, float *out);
@@ -372,24 +378,31 @@ int sg_stream(sg_net *net, void **out);
    (row_ptr[n_neurons+1], col/weights/delays[row_ptr[n_neurons]]) and the
    ring [32][n_neurons] floats.  `stream` is a cudaStream_t (NULL: legacy
    default stream).  Scratch is allocated per call (cudaMalloc/cudaFree);
-   the call returns after the ring is updated. */
+   the call returns after the ring is updated.  Active or col entries
+   >= n_neurons return SG_E_INVALID with the ring untouched. */
 int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
                    const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
                    uint32_t n_active, uint64_t step, float *ring, void *stream);
 
 /* No counterpart in the reference.  sg_push_spikes without any device
-   allocation, for callers that cannot call cudaMalloc while they run (a host
-   loop that must stay allocation-free during CUDA-graph capture, a real-time
-   thread, an embedding with a fixed memory budget).  Same arguments and
-   results as sg_push_spikes.  Its scratch is one file-scope __device__ array
-   of about 12.1 MiB that every GPU loading this library holds until the
-   process exits.  Limits: n_neurons <= 8,388,608 and at most 1,048,576
-   synaptic events per call (the sum of the active rows' lengths); larger
-   inputs return SG_E_INVALID / SG_E_OVERFLOW before the ring is touched.
-   The first call on a device resolves the array's address on that device
-   (cudaGetSymbolAddress), so make that first call before any stream capture.
-   Every call shares the one array: calls that overlap on the GPU (other
-   streams, other host threads) race and must be serialised by the caller. */
+   allocation, for callers that cannot call cudaMalloc while they run: a
+   real-time loop with no room in its timing budget for cudaMalloc/cudaFree
+   (they can block in the driver and synchronise the device), or an
+   embedding that is handed a fixed device-memory budget up front and owns
+   every allocation itself.  Same arguments and results as sg_push_spikes;
+   like it, the call waits on `stream` once (it reads the event count back)
+   and returns after the ring is updated.  Its scratch is one file-scope
+   __device__ array of about 12.1 MiB that every GPU loading this library
+   holds until the process exits.  Limits: n_neurons <= 8,388,608 and at most
+   1,048,576 synaptic events per call (the sum of the active rows' lengths);
+   larger inputs return SG_E_INVALID / SG_E_OVERFLOW before the ring is
+   touched, as do active or col entries >= n_neurons.  The first call on a
+   device resolves the array's address on that device
+   (cudaGetSymbolAddress), so make that first call before any stream capture;
+   the address is kept until the process exits (do not call this again after
+   a cudaDeviceReset of that device).  Every call shares the one array: calls
+   that overlap on the GPU (other streams, other host threads) race and must
+   be serialised by the caller. */
 int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
                            const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
                            uint32_t n_active, uint64_t step, float *ring, void *stream);

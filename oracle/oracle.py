@@ -102,6 +102,7 @@ def lib():
             "or_traces_read": (i32, [vp, vp, vp]),
             "or_fast_exp": (f32, [f32]),
             "or_sg_expf": (f32, [f32]),
+            "or_sg_logf": (f32, [f32]),
             "or_poisson_spike": (i32, [u32, u32, u64, f32]),
             "or_compact": (u64, [vp, u64, vp]),
             "or_push_spikes": (i32, [vp, vp, vp, vp, u32, vp, u32, u64, vp]),
@@ -403,6 +404,10 @@ def fast_exp(x: float) -> float:
 
 def sg_expf(x: float) -> float:
     return float(lib().or_sg_expf(float(x)))
+
+
+def sg_logf(x: float) -> float:
+    return float(lib().or_sg_logf(float(x)))
 
 
 def poisson_spike(seed, stream, step, p) -> bool:

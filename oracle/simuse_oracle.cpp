@@ -124,11 +124,51 @@ float sg_expf(float x) {
   return (p * s1) * s2;
 }
 
+// Natural log used by the GPEA calcium Nernst potential in FP32, the same
+// definition as the CUDA kernel's: x = m * 2^k, m in [sqrt(1/2), sqrt(2)),
+// ln m = 2 atanh((m - 1)/(m + 1)) by its series to s^25 (Abramowitz & Stegun
+// 4.1.27) in FP64, plus k ln 2 (split in a high and a low part), rounded once
+// to FP32: correctly rounded over every float in [1e-12, 1e6].  The
+// reference's f32::ln is the platform libm logf, which (glibc) differs from
+// the correctly rounded value by one unit in the last place on about 0.07% of
+// those floats; this restatement takes the correctly rounded value so that
+// the device can reproduce it.
+float sg_logf(float x) {
+  uint32_t b;
+  std::memcpy(&b, &x, 4);
+  if (!(x > 0.0f)) return x == 0.0f ? -INFINITY : NAN;
+  if (b >= 0x7f800000u) return x;
+  int k = 0;
+  if (b < 0x00800000u) {
+    x = x * 16777216.0f;
+    std::memcpy(&b, &x, 4);
+    k = -24;
+  }
+  k += (int)(b >> 23) - 127;
+  const uint32_t mb = (b & 0x7fffffu) | 0x3f800000u;
+  float mf;
+  std::memcpy(&mf, &mb, 4);
+  double m = (double)mf;
+  if (m > 1.4142135623730951) {
+    m = m * 0.5;
+    k += 1;
+  }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 25.0;
+  const double inv[12] = {1.0 / 23.0, 1.0 / 21.0, 1.0 / 19.0, 1.0 / 17.0, 1.0 / 15.0, 1.0 / 13.0,
+                          1.0 / 11.0, 1.0 / 9.0,  1.0 / 7.0,  1.0 / 5.0,  1.0 / 3.0,  1.0};
+  for (double c : inv) p = p * z + c;
+  const double lm = (2.0 * s) * p;
+  const double ln2_hi = 6.93147180369123816490e-01, ln2_lo = 1.90821492927058770002e-10;
+  return (float)((double)k * ln2_hi + ((double)k * ln2_lo + lm));
+}
+
 template <typename T> struct M;
 template <> struct M<float> {
   static float fexp(float x) { return fast_exp_f(x); }  // GPEA, STDP decay
   static float hexp(float x) { return sg_expf(x); }     // HH rates
-  static float ln(float x) { return std::log(x); }
+  static float ln(float x) { return sg_logf(x); }      // GPEA Nernst
   static float fma(float a, float b, float c) { return std::fma(a, b, c); }
 };
 template <> struct M<double> {
@@ -1708,6 +1748,7 @@ int or_traces_read(or_net *h, float *x_pre, float *x_post) {
 
 float or_fast_exp(float x) { return fast_exp_f(x); }
 float or_sg_expf(float x) { return sg_expf(x); }
+float or_sg_logf(float x) { return sg_logf(x); }
 int or_poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p) {
   return poisson_spike(seed, stream, step, p) ? 1 : 0;
 }

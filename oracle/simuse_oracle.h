@@ -112,6 +112,7 @@ int or_set_threads(int n);
 /* ---- stand-alone reference pieces, for golden checks ---- */
 float or_fast_exp(float x);
 float or_sg_expf(float x);
+float or_sg_logf(float x);
 int or_poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p);
 uint64_t or_compact(const int32_t *spikes, uint64_t n, uint32_t *out);
 int or_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *w,

@@ -85,6 +85,4 @@ def test_bf16_refuses_stdp():
                 np.full(100, 0.5, np.float32), np.ones(100, np.uint8), stdp=True)
     with pytest.raises(sg.SimuseError, match="STDP"):
         net.build()
-    with pytest.raises(sg.SimuseError):
-        sg.Network(0).set_weight_format(sg.W_FP8)
     net.close()

@@ -4,10 +4,11 @@ When every weight that reaches a ring is a multiple of one power of two and
 no post's weights can sum past 24 bits of mantissa at that scale, every
 partial sum of a ring cell is exact in FP32: float addition on the rings is
 associative and the order of the adds cannot change a bit.  The network then
-routes its events through per-slot lists added in any order; everything else
+takes the pre-centric scatter (each spiking row read once, every event added
+to its ring cell in L2 with red.global.add, in any order); everything else
 keeps the reference's order.  These tests check which networks take the path
-and that it gives the oracle's bits, including when lists overflow inside a
-step and when the rings are read back between steps.
+and that it gives the oracle's bits, on a network where every neuron fires
+every step and when the rings are read back between steps.
 """
 import numpy as np
 import pytest
@@ -62,9 +63,8 @@ def test_stdp_keeps_the_ordered_path():
 
 def _dense(net, n=4096, k=512, steps=30):
     """Every neuron fires every step (dt * inv_tau = 1 puts v at rest + input,
-    rest above threshold, no refractory time): each scatter block takes
-    16384 events a step over two delays, so its lists overflow and are
-    flushed inside the step."""
+    rest above threshold, no refractory time): 2M events a step over two
+    delays, many of them onto the same ring cells within a step."""
     p = net.add_population(LIF, n)
     for col, v in enumerate([1.0, 1.0, 25.0, 20.0, 10.0, 0.0]):
         net.fill_param(p, col, v)
@@ -84,7 +84,7 @@ def _dense(net, n=4096, k=512, steps=30):
     return net, p, np.array(raster)
 
 
-def test_exact_lists_overflowing_within_a_step_match_the_oracle():
+def test_exact_dense_firing_matches_the_oracle():
     g, gp, rg = _dense(sg.Network(0))
     assert g.scatter_mode == "exact"
     c, cp, rc = _dense(O.Network(0))
@@ -96,8 +96,9 @@ def test_exact_lists_overflowing_within_a_step_match_the_oracle():
 
 
 def test_exact_ring_readback_between_steps():
-    """Reading the rings adds every pending list to them; stepping on from
-    there gives the same bits as never having read them."""
+    """Reading the rings between steps (which first adds the deferred drive
+    of the last step to them) and stepping on from there gives the same bits
+    as never having read them."""
     g = sg.Network(0)
     gp = _balanced(g)
     g.build()

@@ -94,7 +94,7 @@ def _driven(make_net, steps=600, reward_every=50):
 
 def test_driven_network_learning_bit_identical_to_the_oracle():
     g, gp, rg, sg_, w0 = _driven(lambda: sg.Network(0))
-    assert g.scatter_mode == "ordered"      # rewards change weights: no exact-sum lists
+    assert g.scatter_mode == "ordered"      # rewards change weights: the ordered path
     c, cp, rc, sc, _ = _driven(lambda: O.Network(0))
     assert rg.sum() > 1000
     assert np.array_equal(rg, rc)

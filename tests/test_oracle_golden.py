@@ -234,3 +234,23 @@ def test_register_plasticity_rejects_invalid_profile():
     for u0, tau in ((0.0, 1.0), (1.5, 1.0), (0.5, 0.0), (0.5, float("nan"))):
         with pytest.raises(O.OracleError):
             net.register_plasticity(u0, tau, 0.5)
+
+
+def test_sg_logf_is_correctly_rounded():
+    """The GPEA log (shared by the kernels and the oracle) equals the
+    correctly rounded FP32 log on a strided sample of every float in
+    [1e-12, 1e6] (the whole range was checked exhaustively once), and the
+    usual special values."""
+    import math
+    lo = np.array([1e-12], np.float32).view(np.uint32)[0]
+    hi = np.array([1e6], np.float32).view(np.uint32)[0]
+    bits = np.arange(lo, hi, 2003, dtype=np.uint64).astype(np.uint32)
+    xs = bits.view(np.float32)
+    want = np.log(xs.astype(np.float64)).astype(np.float32)
+    got = np.array([O.sg_logf(float(x)) for x in xs], np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert O.sg_logf(1.0) == 0.0
+    assert O.sg_logf(0.0) == -math.inf
+    assert math.isnan(O.sg_logf(-1.0))
+    assert O.sg_logf(math.inf) == math.inf
+    assert O.sg_logf(1e-40) == float(np.float32(math.log(np.float32(1e-40))))
