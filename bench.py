@@ -73,6 +73,7 @@ def parse(argv=None):
     ap.add_argument("--sim-steps", type=int, default=1000)
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--k-in", type=int, default=1000)
+    ap.add_argument("--d-max", type=int, default=20, help="largest synaptic delay (steps) of the LIF network")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
@@ -102,7 +103,7 @@ def workload(args, rank=0):
     from simuse_b200 import workloads as W
     kw = (dict(ext_rate_hz=4000.0, ext_weight=100.0) if args.variant == "driven"
           else dict(ext_rate_hz=2000.0, ext_weight=20.0))
-    spec = W.lif_balanced(n=args.n, k_in=args.k_in, seed=1 + rank, **kw)
+    spec = W.lif_balanced(n=args.n, k_in=args.k_in, seed=1 + rank, d_max=args.d_max, **kw)
     name = f"lif_balanced_{args.n // 1000}k_in{args.k_in}_{args.variant}"
     return spec, name
 
@@ -361,6 +362,132 @@ def run_serving(args, local):
             "errors": int(sum(r.error is not None for r in reqs))}
 
 
+def _timed_steps(net, local, n_steps):
+    """Device time (ms) of n_steps simulation steps on the network's stream."""
+    import torch
+    st = torch.cuda.ExternalStream(net.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    net.step(n_steps)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_precision_paths(args, local):
+    """The headline network with other weight storage and on the ordered
+    path: BF16 and FP8 weights (20, -100 and 100 stay exact: same spikes,
+    fewer scatter bytes), and J = 20.1 (not a dyadic multiple: every ring cell
+    takes its adds in the reference's order through the owner-computes
+    scatter).  Per case: events/s, scatter path, scatter kernel ms per launch
+    and its fraction of the HBM roofline."""
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+    peak, _ = measured_peak()
+    out = {}
+    S = 500
+    for name, fmt, w_exc in (("bf16", sg.W_BF16, 20.0), ("fp8", sg.W_FP8, 20.0), ("ordered_j20.1", None, 20.1)):
+        spec = W.lif_balanced(n=args.n, k_in=args.k_in, seed=1, ext_rate_hz=4000.0, ext_weight=100.0, w_exc=w_exc)
+        net = sg.Network(local)
+        if fmt is not None:
+            net.set_weight_format(fmt)
+        W.build_lif(net, spec)
+        net.build()
+        net.step(S)  # settle
+        ev0, src0 = net.events_total, net.source_events_total
+        ms = _timed_steps(net, local, S)
+        ev = net.events_total - ev0
+        rec = (ev - (net.source_events_total - src0)) / S
+        net.profile(True)
+        net.step(200)
+        ph_ms, ph_n = net.profile_read()
+        net.profile(False)
+        sp, _ = net.read_stats()
+        spikes = float(sp[-200:].mean())
+        scat_ms = ph_ms[1] / max(int(ph_n[1]), 1)
+        b_ev = {"bf16": 6.0, "fp8": 5.0}.get(name, 8.0) + 1.0 + B_EVENT_APPLY  # x word/record + delay + ring RMW
+        alg = rec * b_ev + spikes * B_SPIKE
+        out[name] = {"events_per_s": ev / (ms / 1e3), "ms_per_sim_step": ms / S, "scatter": net.scatter_mode,
+                     "scatter_ms_per_launch": scat_ms, "scatter_alg_bytes": alg,
+                     "scatter_frac": alg / (scat_ms / 1e3) / 1e9 / peak,
+                     "weights": name if fmt is not None else "fp32"}
+        net.close()
+    return out
+
+
+def run_hh_prefix(args, local):
+    """The HH + pair-STDP network at its stated size (100,000 neurons, RK4 at
+    dt 0.01 ms, lognormal out-degree (200, 80), conductance synapses, STDP on
+    excitatory synapses, weights U(0, 0.01)): 2,000 steps (20 ms) timed after
+    500 warm-up steps."""
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+    net = sg.Network(local)
+    W.add_hh_stdp(net, 100_000, w_max=0.01)
+    net.build()
+    net.step(500)
+    ev0, d0 = net.events_total, net.stdp_drift
+    ms = _timed_steps(net, local, 2000)
+    ev = net.events_total - ev0
+    out = {"events_per_s": ev / (ms / 1e3), "neuron_updates_per_s": 100_000 * 2000 / (ms / 1e3),
+           "us_per_sim_step": ms * 1e3 / 2000, "synapses": net.num_synapses, "steps": 2000,
+           "stdp_drift": net.stdp_drift - d0, "scatter": net.scatter_mode}
+    net.close()
+    return out
+
+
+def run_kuramoto(args, local):
+    """1024 all-to-all Kuramoto populations, N log-uniform 256..65,536, RK4 at
+    dt 0.01 with the mean-field identity: 500 steps timed."""
+    import torch
+
+    from simuse_b200 import KuramotoBatch
+    from simuse_b200 import workloads as W
+    sp = W.kuramoto_sweep(1024)
+    kb = KuramotoBatch(sp["sizes"], sp["coupling"], sp["dt"], device=local)
+    kb.set_state(sp["theta"], sp["omega"])
+    kb.run(20)
+    kb.synchronize()
+    st = torch.cuda.ExternalStream(kb.stream(), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    kb.run(500)
+    e1.record(st)
+    kb.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"oscillator_steps_per_s": kb.total * 500 / (ms / 1e3), "oscillators": kb.total,
+           "us_per_step": ms * 1e3 / 500}
+    kb.close()
+    return out
+
+
+def run_learn_short(args, local):
+    """The headline network with dopamine learning on its 1e9 synapses: 200
+    steps timed with learning after 300 learning steps, and one reward."""
+    import simuse_b200 as sg
+    from simuse_b200 import workloads as W
+    spec, _ = workload(args, 0)
+    net = sg.Network(local)
+    W.build_lif(net, spec)
+    net.build()
+    net.step(200)
+    net.enable_learning(dt=spec["dt"], tau_pre=20.0, tau_post=20.0, tau_e=1000.0, a_ltp=0.1, a_ltd=0.12, lr=0.01,
+                        w_min=-200.0, w_max=200.0)
+    net.step(300)
+    ms = _timed_steps(net, local, 200)
+    import torch
+    st = torch.cuda.ExternalStream(net.stream, device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    net.reward(1.0)
+    e1.record(st)
+    e1.synchronize()
+    out = {"ms_per_sim_step_learning": ms / 200, "reward_ms": e0.elapsed_time(e1), "scatter": net.scatter_mode,
+           "synapses": net.num_synapses}
+    net.close()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -502,8 +629,13 @@ def run_ours(args):
         "gpu_launches": int(args.steps * S * 2),
     }
     if not args.no_extras and world == 1:
-        out["batched"] = run_batched(args, local)
-        out["serving"] = run_serving(args, local)
+        for key, fn in (("precision_paths", run_precision_paths), ("hh_stdp_100k", run_hh_prefix),
+                        ("kuramoto_sweep", run_kuramoto), ("lif_learn", run_learn_short),
+                        ("batched", run_batched), ("serving", run_serving)):
+            try:
+                out[key] = fn(args, local)
+            except Exception as e:  # an extra measurement never takes the headline line down
+                out[key] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_cpu_baseline and world == 1:
         cnet, cores, build_s = cpu_baseline(args, spec, args.cpu_seconds)
         rc, ev, el = run_cpu_parity(cnet, PARITY_STEPS)

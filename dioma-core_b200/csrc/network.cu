@@ -206,6 +206,8 @@ struct sg_net {
   DBuf<uint32_t> d_red_flat, d_red_cnt, d_run_off;
   // deferred drive: device record of the last folded step, and its host copy
   DBuf<unsigned long long> d_drv_fold;
+  DBuf<uint32_t> d_err;        // device error word (scatter pipeline waits)
+  uint32_t debug_stall = 0;    // test hook: the scatter's producer stalls
   unsigned long long drv_folded = ~0ull;
   bool any_drv = false;
   // short-term plasticity: profiles, staged per-edge ids (kept only once an
@@ -378,6 +380,8 @@ StepArgs make_args(sg_net *net) {
   a.n_runs = (uint32_t)net->n_runs;
   a.n_src_syn = (uint32_t)net->n_src_edges;
   a.drv_fold = net->d_drv_fold.p;
+  a.err = net->d_err.p;
+  a.debug_stall = net->debug_stall;
   a.tm = net->tm_edges ? 1 : 0;
   a.tm_pt = net->d_pt.p;
   a.tm_r = net->d_tm_r.p;
@@ -763,8 +767,9 @@ void build_graph(sg_net *net) {
   const uint32_t Nd = net->Nd;
   net->d_row_ptr.alloc((size_t)Nd + 1);
   net->packed = Nd <= (1u << 24) ? 1 : 0;
-  net->d_edge.alloc(std::max<uint64_t>(E, 1));
-  net->d_code.alloc(net->packed ? 1 : std::max<uint64_t>(E, 1));
+  // padded: the scatter's bulk copies widen a row to 16-byte boundaries
+  net->d_edge.alloc(E + 2);
+  net->d_code.alloc(net->packed ? 1 : E + 16);
   DBuf<unsigned long long> cnt;
   cnt.alloc((size_t)Nd + 1);
   cnt.zero(s);
@@ -1122,8 +1127,8 @@ void split_bf16(sg_net *net) {
   SG_REQUIRE(!net->stdp_on, SG_E_INVALID, "BF16 weights are read-only: pair STDP needs FP32 weights");
   const uint64_t E = net->n_edges;
   cudaStream_t s = net->stream;
-  net->d_edge_x.alloc(std::max<uint64_t>(E, 1));
-  net->d_w16.alloc(std::max<uint64_t>(E + (E & 1), 2));  // even: the scatter reads aligned pairs
+  net->d_edge_x.alloc(E + 4);  // padded for the scatter's 16-byte bulk copies
+  net->d_w16.alloc(E + 8);
   if (E) {
     const unsigned b = (unsigned)std::min<uint64_t>((E + 255) / 256, 148u * 32u);
     split_bf16_kernel<<<b, 256, 0, s>>>(net->d_edge.p, net->d_edge_x.p, net->d_w16.p, E);
@@ -1166,8 +1171,8 @@ void split_fp8(sg_net *net) {
   SG_REQUIRE(!net->stdp_on, SG_E_INVALID, "FP8 weights are read-only: pair STDP needs FP32 weights");
   const uint64_t E = net->n_edges;
   cudaStream_t s = net->stream;
-  net->d_edge_x.alloc(std::max<uint64_t>(E, 1));
-  net->d_w8.alloc(std::max<uint64_t>(E, 1));
+  net->d_edge_x.alloc(E + 4);  // padded for the scatter's 16-byte bulk copies
+  net->d_w8.alloc(E + 16);
   net->d_row_scale.alloc(std::max<uint32_t>(net->Nd, 1));
   if (E) {
     split_fp8_kernel<<<148u * 8u, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->d_edge_x.p, net->d_w8.p,
@@ -1299,6 +1304,8 @@ void setup_scatter(sg_net *net) {
   net->d_red_cnt.alloc(1);
   net->d_red_cnt.zero(s);
   net->d_drv_fold.alloc(1);
+  net->d_err.alloc(1);
+  net->d_err.zero(s);
   const unsigned long long none = ~0ull;
   SG_CUDA(cudaMemcpyAsync(net->d_drv_fold.p, &none, sizeof(none), cudaMemcpyHostToDevice, s));
   SG_CUDA(cudaStreamSynchronize(s));
@@ -1469,15 +1476,29 @@ void upload_pop_table(sg_net *net) {
   net->pop_tab_dirty = false;
 }
 
+template <int M, bool FULL> void launch_neuron_form(sg_net *net, const StepArgs &a, uint32_t nb) {
+  if (net->model_single[M] >= 0)
+    neuron_kernel<M, FULL><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, net->pop_tab[net->model_single[M]],
+                                                                          nullptr, nullptr);
+  else
+    neuron_kernel<M, FULL><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, PopArgs{}, net->d_pop_tab.p,
+                                                                          net->d_blk_map.p + net->model_blk_off[M]);
+}
+
+// The lean neuron kernel serves steps without kinetic synapses, input
+// noise, neuron statistics, pair STDP or learning.
+bool needs_full_neuron_kernel(const sg_net *net, const StepArgs &a) {
+  if (a.n_kin || a.ns_count != nullptr || a.stdp || a.learn) return true;
+  for (const auto &p : net->pops)
+    if (p.noise) return true;
+  return false;
+}
+
 template <int M> void launch_neuron(sg_net *net, const StepArgs &a) {
   const uint32_t nb = net->model_blk_cnt[M];
   if (nb == 0) return;
-  if (net->model_single[M] >= 0)
-    neuron_kernel<M><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, net->pop_tab[net->model_single[M]], nullptr,
-                                                                    nullptr);
-  else
-    neuron_kernel<M><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, PopArgs{}, net->d_pop_tab.p,
-                                                                    net->d_blk_map.p + net->model_blk_off[M]);
+  if (needs_full_neuron_kernel(net, a)) launch_neuron_form<M, true>(net, a, nb);
+  else launch_neuron_form<M, false>(net, a, nb);
 }
 
 // The first half of a step: the neuron update of every population simulated here.
@@ -1512,7 +1533,7 @@ void enqueue_rest(sg_net *net, const StepArgs &a) {
   if (a.red) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
-    scatter_red_kernel<<<(unsigned)sms * kRedBlocksPerSM, kRedThreads, 0, s>>>(a);
+    scatter_red_kernel<<<(unsigned)sms * kRedBlocksPerSM, kRedThreads, sizeof(RedSmem), s>>>(a);
   } else {
     if (net->seg32) scatter_kernel<true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
     else scatter_kernel<false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
@@ -1670,11 +1691,34 @@ int sg_net_destroy(sg_net *net) {
   return SG_OK;
 }
 
+// The device error word: a wait of the scatter pipeline that ran out of time
+// (the step it belongs to is incomplete).  Read and cleared.
+void check_device_error(sg_net *net) {
+  if (!net->built || !net->d_err.p) return;
+  uint32_t e = 0;
+  SG_CUDA(cudaMemcpyAsync(&e, net->d_err.p, 4, cudaMemcpyDeviceToHost, net->stream));
+  SG_CUDA(cudaStreamSynchronize(net->stream));
+  if (e) {
+    SG_CUDA(cudaMemsetAsync(net->d_err.p, 0, 4, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    SG_REQUIRE(false, SG_E_CUDA, "scatter: a pipeline wait timed out on the device (the step's events are incomplete)");
+  }
+}
+
 int sg_synchronize(sg_net *net) {
   NET_CHECK(net);
   return run([&] {
     DevGuard g(net->device);
     SG_CUDA(cudaStreamSynchronize(net->stream));
+    check_device_error(net);
+  });
+}
+
+int sg_debug_stall_scatter(sg_net *net, int on) {
+  NET_CHECK(net);
+  return run([&] {
+    net->debug_stall = on ? 1u : 0u;
+    drop_graph(net);
   });
 }
 

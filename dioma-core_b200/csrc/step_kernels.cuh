@@ -64,9 +64,13 @@ constexpr uint32_t kMaxTm = 8;  // short-term plasticity profiles on the device
 
 // neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
 // GPEA/HH are compute heavy and keep one neuron per thread
+#ifndef SG_NEURON_MIN_BLOCKS
+#define SG_NEURON_MIN_BLOCKS 4  // resident 256-thread blocks per SM asked of the lean LIF/Izhikevich kernel
+#endif
 template <int M> struct NeuronCfg {
   static constexpr int NPT = (M == kLIF || M == kIZH) ? 4 : 1;
   static constexpr int THREADS = (int)kNeuronBlock / NPT;
+  static constexpr int MIN_BLOCKS = (M == kLIF || M == kIZH) ? SG_NEURON_MIN_BLOCKS : 1;
 };
 
 struct StepArgs {
@@ -158,6 +162,11 @@ struct StepArgs {
   const uint32_t *run_off;
   uint32_t n_runs;
   uint32_t n_src_syn;
+  // device error word: bit 0 a pipeline wait of the scatter ran out of time
+  // (read and cleared by sg_synchronize); the debug word stalls the
+  // scatter's producer (test hook: its consumers' waits then run out)
+  uint32_t *err;
+  uint32_t debug_stall;
   // deferred drive: the step whose deferred Poisson events were already
   // added to the ring (by drive_fold_kernel before an inject or a ring
   // readback), or ~0
@@ -336,7 +345,10 @@ template <> struct VecF<4> {
 };
 
 // The update of one 1024-neuron block `blk` of population p.
-template <int MODEL>
+// FULL = false: the lean form for steps without kinetic synapses, input
+// noise, neuron statistics, pair STDP or learning (fewer registers: all blocks
+// of a large population resident at once).
+template <int MODEL, bool FULL>
 __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p, uint32_t blk) {
   constexpr int NPT = NeuronCfg<MODEL>::NPT;
   constexpr int NS = n_state(MODEL), NP = n_params(MODEL);
@@ -373,7 +385,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
 #pragma unroll
     for (int q = 0; q < NPT; ++q) x[q] = x[q] + bv[q];
   }
-  if (p.noise) {
+  if (FULL && p.noise) {
     const unsigned long long t = step - p.noise_step0;
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
@@ -390,7 +402,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   // Unrolled over the (at most 3) profiles so that the profile constants are
   // indexed at compile time and stay in the kernel parameter space.
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < (FULL ? 3 : 0); ++k) {
     if (k >= a.n_kin) break;
     float jump[NPT], s0[NPT], s1[NPT], s2[NPT];
     float *ks = a.ring + ((size_t)(k + 1) * a.nslots + slot) * a.Nd + gi0;
@@ -469,7 +481,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   }
 #pragma unroll
   for (int c = 0; c < NS; ++c) V::store(p.state + (size_t)c * p.cap + i0, sv[c]);
-  if (a.ns_count != nullptr && nib) {
+  if (FULL && a.ns_count != nullptr && nib) {
     const uint32_t t = (uint32_t)(step - a.ns_step0);
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
@@ -557,7 +569,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     }
   }
   // pair-STDP traces: x = fma(x, d, s) (P/api/learn/brain.rs:212-222)
-  if (a.stdp) {
+  if (FULL && a.stdp) {
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
       if (i0 + q < p.n) {
@@ -569,7 +581,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   }
   // learning traces (P/api/learn/brain.rs:211-222) and motor counts
   // (pillars-wgpu/shaders/dopamine.wgsl:126-136)
-  if (a.learn) {
+  if (FULL && a.learn) {
     uint32_t m0 = 0, m1 = 0;
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
@@ -599,15 +611,15 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
 // many small populations (a batch of networks) step in one launch.  A model
 // with a single population passes its arguments by value (map == null) and
 // block b is its block b.
-template <int MODEL>
-__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS)
+template <int MODEL, bool FULL>
+__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCfg<MODEL>::MIN_BLOCKS)
     neuron_kernel(StepArgs a, PopArgs p0, const PopArgs *__restrict__ pops, const uint2 *__restrict__ map) {
   if (map == nullptr) {
-    neuron_block<MODEL>(a, p0, blockIdx.x);
+    neuron_block<MODEL, FULL>(a, p0, blockIdx.x);
     return;
   }
   const uint2 bm = map[blockIdx.x];
-  neuron_block<MODEL>(a, pops[bm.x], bm.y);
+  neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -1096,99 +1108,258 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   end_of_step(a, n_spikes);
 }
 
-// ---------------------------------------------------------------------------
-// Pre-centric scatter (rings_exact networks, and the atomic mode).  When every
-// partial sum of a ring cell is exact, the order of the adds does not change
-// a cell's bits, so each spiking row is read once, whole and coalesced, and
-// every event goes to its ring cell with a fire-and-forget red.global.add in
-// L2 (the rings stay L2-resident: the synapse records stream through with
-// evict_first, the ring cells are updated with evict_last).  Warps take the
-// step's spiking neurons round robin; rows longer than kRedLong synapses are
-// shared by the threads of the whole block that found them.  Poisson-source
-// synapses that the neuron kernel does not take (deferred drive) follow, one
-// per thread.
-// ---------------------------------------------------------------------------
-constexpr uint32_t kRedThreads = 256;
-constexpr uint32_t kRedBlocksPerSM = 4;
-constexpr uint32_t kRedLong = 2048;
-constexpr uint32_t kRedLongMax = 32;  // long rows one block keeps for itself
-constexpr uint32_t kRedUnroll = 8;
+constexpr uint32_t kRedThreads = 256;        // warp 0: producer; warps 1-7: consumers
+constexpr uint32_t kRedConsumers = kRedThreads - 32;
+#ifndef SG_RED_BLOCKS_PER_SM
+#define SG_RED_BLOCKS_PER_SM 2
+#endif
+#ifndef SG_RED_UNROLL
+#define SG_RED_UNROLL 1
+#endif
+constexpr uint32_t kRedBlocksPerSM = SG_RED_BLOCKS_PER_SM;
+constexpr int kRedUnroll = SG_RED_UNROLL;  // consumer loop unroll
+constexpr uint32_t kRedStages = 4;
+constexpr uint32_t kRedChunk = 1024;         // synapses per stage
+// a stage holds kRedChunk FP32 records widened to 16-byte boundaries (+16 B)
+// and, for networks whose code bytes are a separate array, their code bytes
+// (+32 B); x words + bf16/fp8 weights + code bytes take less
+constexpr uint32_t kRedStageBytes = 10240;
+static_assert(8 * (kRedChunk + 2) + 16 + (kRedChunk + 32) <= kRedStageBytes, "scatter stage too small");
+constexpr unsigned long long kWaitNs = 1000000000ull;     // every pipeline wait gives up after ~1 s
 
 __device__ __forceinline__ void red_add(float *p, float v, unsigned long long pol) {
   asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
 }
 
-// Events [e, end) of one row, this thread taking every `stride`-th one
-// (`scale`: the row's FP8 weight scale).
-__device__ __forceinline__ void red_range(const StepArgs &a, uint32_t e, uint32_t end, uint32_t stride,
-                                          uint32_t base, unsigned long long pf, unsigned long long pl,
-                                          float scale) {
-  for (; e < end; e += stride * kRedUnroll) {
-    uint2 rec[kRedUnroll];
-    uint32_t cd[kRedUnroll];
-#pragma unroll
-    for (uint32_t u = 0; u < kRedUnroll; ++u) {
-      const uint32_t k = e + u * stride;
-      if (k < end) {
-        rec[u] = ld_record(a, k, pf, scale);
-        cd[u] = a.code ? ld_stream_u8(a.code + k, pf) : (rec[u].x >> 24);
-      }
-    }
-#pragma unroll
-    for (uint32_t u = 0; u < kRedUnroll; ++u) {
-      const uint32_t k = e + u * stride;
-      if (k < end) {
-        const uint32_t post = rec[u].x & a.post_mask;
-        const uint8_t code = (uint8_t)cd[u];
-        uint32_t slot = base + max(code_delay(code), 1u);
-        if (slot >= a.nslots) slot -= a.nslots;
-        float *cell = a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + post;
-        red_add(cell, __uint_as_float(rec[u].y), pl);
-      }
-    }
+// ---- mbarrier / 1-D bulk copy helpers (this CTA's shared memory only) ----
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase of `parity` to complete, at most ~kWaitNs; false when
+// the time ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 63u) == 0 && global_ns() - t0 > kWaitNs) return false;
   }
 }
+// Bulk copy of `bytes` (a multiple of 16) from global `src` (16-byte aligned)
+// to shared `dst` (16-byte aligned), completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
 
-__global__ void __launch_bounds__(kRedThreads) scatter_red_kernel(StepArgs a) {
-  __shared__ uint4 s_long[kRedLongMax];  // begin, end, scale bits
-  __shared__ uint32_t s_long_n;
-  __shared__ unsigned long long s_events, s_src_events;
-  const uint32_t tid = threadIdx.x, lane = lane_id();
-  const uint32_t gw = (blockIdx.x * kRedThreads + tid) >> 5, W = (gridDim.x * kRedThreads) >> 5;
+// One stage: up to kRedChunk synapses of one row.
+struct RedStage {
+  uint32_t n;        // synapses in the stage, or kEmpty: the producer is done
+  uint32_t x_off;    // first synapse within the x / record buffer (elements)
+  uint32_t w_off;    // first weight within the weight buffer (split formats)
+  uint32_t c_off;    // first code byte within the code buffer (unpacked x words)
+  uint32_t w_base;   // byte offset of the weight buffer in the stage
+  uint32_t c_base;   // byte offset of the code buffer in the stage
+  float scale;       // FP8 row scale
+};
+struct RedSmem {
+  alignas(16) unsigned char buf[kRedStages][kRedStageBytes];
+  RedStage meta[kRedStages];
+  uint64_t full[kRedStages];
+  uint64_t empty[kRedStages];
+  unsigned long long events, src_events;
+};
+
+// Copies elements [b, e) of an array of `esz`-byte elements to `dst`: the
+// range is widened to 16-byte boundaries (the arrays are padded so that the
+// widened end stays inside them).  Returns the bytes copied; *off = index of
+// element b in the copy.
+__device__ __forceinline__ uint32_t bulk_elems(unsigned char *dst, const void *arr, uint32_t esz, uint32_t b,
+                                               uint32_t e, uint64_t *bar, uint32_t *off) {
+  const uint32_t per = 16u / esz;
+  const uint32_t b0 = b - b % per, e1 = (e + per - 1) / per * per;
+  *off = b - b0;
+  const uint32_t bytes = (e1 - b0) * esz;
+  bulk_g2s(dst, (const unsigned char *)arr + (size_t)b0 * esz, bytes, bar);
+  return bytes;
+}
+
+// ---------------------------------------------------------------------------
+// Pre-centric scatter (rings_exact networks, and the atomic mode).  When every
+// partial sum of a ring cell is exact, the order of the adds does not change
+// a cell's bits, so each spiking row is read once, whole, and every event goes
+// to its ring cell with a fire-and-forget red.global.add in L2 (the rings stay
+// L2-resident: the synapse records stream through, the ring cells are updated
+// with evict_last).  Block b takes the step's spiking rows b, b + G, ...
+// Warp 0 is the producer: its lanes look up 32 rows at a time (flat list,
+// row bounds) and lane 0 copies each row, kRedChunk synapses per stage, into
+// a kRedStages-deep shared-memory ring with 1-D bulk copies (cp.async.bulk,
+// this GPU's memory, no multicast) that complete on the stage's mbarrier.
+// Warps 1-7 consume: per stage they read the synapses from shared memory and
+// issue the reds, then release the stage.  Every wait gives up after ~1 s,
+// records the failure in *err and leaves the kernel (with the copies it
+// issued completed).  Poisson-source synapses that the neuron kernel does not
+// take (deferred drive) follow, one per thread.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM) scatter_red_kernel(StepArgs a) {
+  extern __shared__ __align__(128) unsigned char red_smem[];
+  RedSmem &S = *reinterpret_cast<RedSmem *>(red_smem);
+  const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   if (tid == 0) {
-    s_long_n = 0;
-    s_events = 0;
-    s_src_events = 0;
+    for (uint32_t k = 0; k < kRedStages; ++k) {
+      mbar_init(&S.full[k], 1);
+      mbar_init(&S.empty[k], kRedConsumers / 32);
+    }
+    S.events = 0;
+    S.src_events = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
   const unsigned long long step = *a.step;
   const uint32_t base = (uint32_t)(step % a.nslots);
   const uint32_t n = *a.red_cnt;
-  const unsigned long long pf = policy_evict_first(), pl = policy_evict_last();
+  const unsigned long long pl = policy_evict_last();
   unsigned long long ev = 0, src_ev = 0;
-  for (uint32_t r = gw; r < n; r += W) {
-    const uint32_t gi = a.red_flat[r];
-    const uint32_t beg = __ldg(a.row_ptr + gi), end = __ldg(a.row_ptr + gi + 1);
-    const float scale = a.wfp8 ? __ldg(a.row_scale + gi) : 1.0f;
-    if (end - beg > kRedLong) {
-      uint32_t k = 0;
-      if (lane == 0) k = atomicAdd(&s_long_n, 1u);
-      k = __shfl_sync(0xffffffffu, k, 0);
-      if (k < kRedLongMax) {
-        if (lane == 0) s_long[k] = make_uint4(beg, end, __float_as_uint(scale), 0u);
-        continue;
+  bool failed = false;
+  const uint32_t xsz = a.wbf16 || a.wfp8 ? 4u : 8u;  // bytes per x word or record
+  if (warp == 0) {
+    // ---- producer ----
+    uint32_t stage = 0, eph = 1;  // the first round of empty waits passes at once
+    uint32_t filled = 0, fill_par = 0;  // lane 0: per stage (bit), filled at least once, parity of the fills
+    for (uint32_t r0 = blockIdx.x; r0 < n && !failed; r0 += 32 * gridDim.x) {
+      const uint32_t r = r0 + lane * gridDim.x;
+      uint32_t beg = 0, end = 0;
+      float scale = 1.0f;
+      if (r < n) {
+        const uint32_t gi = a.red_flat[r];
+        beg = __ldg(a.row_ptr + gi);
+        end = __ldg(a.row_ptr + gi + 1);
+        if (a.wfp8) scale = __ldg(a.row_scale + gi);
+      }
+      for (uint32_t k = 0; k < 32 && !failed; ++k) {
+        const uint32_t b = __shfl_sync(0xffffffffu, beg, k), e = __shfl_sync(0xffffffffu, end, k);
+        const float sc = __shfl_sync(0xffffffffu, scale, k);
+        if (lane == 0) {
+          ev += e - b;
+          for (uint32_t c = b; c < e; c += kRedChunk) {
+            const uint32_t ce = min(e, c + kRedChunk);
+            if (a.debug_stall || !mbar_wait(&S.empty[stage], eph)) {
+              failed = true;
+              break;
+            }
+            // byte counts of the widened copies (as bulk_elems computes them)
+            const uint32_t per_x = 16u / xsz;
+            const uint32_t xb = ((ce + per_x - 1) / per_x * per_x - (c - c % per_x)) * xsz;
+            const uint32_t wb = a.wbf16 ? ((ce + 7u) / 8u * 8u - (c - c % 8u)) * 2u
+                                : a.wfp8 ? (ce + 15u) / 16u * 16u - (c - c % 16u)
+                                         : 0u;
+            const uint32_t cb = a.code ? (ce + 15u) / 16u * 16u - (c - c % 16u) : 0u;
+            RedStage &m = S.meta[stage];
+            m.n = ce - c;
+            m.scale = sc;
+            m.w_base = (xb + 15u) & ~15u;
+            m.c_base = (m.w_base + wb + 15u) & ~15u;
+            m.x_off = c % per_x;
+            m.w_off = a.wbf16 ? c % 8u : c % 16u;
+            m.c_off = c % 16u;
+            // the stage's description is written before the arrival that
+            // (with the copies' bytes) completes its phase
+            mbar_arrive_tx(&S.full[stage], xb + wb + cb);
+            unsigned char *dst = S.buf[stage];
+            uint32_t off;
+            if (xsz == 8) bulk_elems(dst, a.edge, 8, c, ce, &S.full[stage], &off);
+            else bulk_elems(dst, a.edge_x, 4, c, ce, &S.full[stage], &off);
+            if (a.wbf16) bulk_elems(dst + m.w_base, a.w16, 2, c, ce, &S.full[stage], &off);
+            if (a.wfp8) bulk_elems(dst + m.w_base, a.w8, 1, c, ce, &S.full[stage], &off);
+            if (a.code) bulk_elems(dst + m.c_base, a.code, 1, c, ce, &S.full[stage], &off);
+            filled |= 1u << stage;
+            fill_par ^= 1u << stage;
+            if (++stage == kRedStages) {
+              stage = 0;
+              eph ^= 1u;
+            }
+          }
+        }
+        failed = __shfl_sync(0xffffffffu, failed ? 1u : 0u, 0) != 0;
       }
     }
-    red_range(a, beg + lane, end, 32, base, pf, pl, scale);
-    if (lane == 0) ev += end - beg;
+    if (lane == 0) {
+      // end marker: the consumers leave when they reach it
+      if (!failed && !a.debug_stall && mbar_wait(&S.empty[stage], eph)) {
+        S.meta[stage].n = kEmpty;
+        mbar_arrive(&S.full[stage]);
+      } else {
+        atomicOr(a.err, 1u);
+        // the copies issued into each stage land before the block ends
+        for (uint32_t k = 0; k < kRedStages; ++k)  // the last fill's phase has parity (fills - 1) & 1
+          if ((filled >> k) & 1u) (void)mbar_wait(&S.full[k], ((fill_par >> k) & 1u) ^ 1u);
+      }
+    }
+  } else {
+    // ---- consumers ----
+    const uint32_t ct = tid - 32;
+    uint32_t stage = 0, fph = 0;
+    for (;;) {
+      if (!mbar_wait(&S.full[stage], fph)) {
+        if (ct == 0) atomicOr(a.err, 1u);
+        break;
+      }
+      const RedStage m = S.meta[stage];
+      if (m.n == kEmpty) break;
+      const unsigned char *src = S.buf[stage];
+#pragma unroll kRedUnroll
+      for (uint32_t k = ct; k < m.n; k += kRedConsumers) {
+        uint32_t x, wbits;
+        if (xsz == 8) {
+          const uint2 rec = reinterpret_cast<const uint2 *>(src)[m.x_off + k];
+          x = rec.x;
+          wbits = rec.y;
+        } else {
+          x = reinterpret_cast<const uint32_t *>(src)[m.x_off + k];
+          if (a.wbf16) wbits = (uint32_t)reinterpret_cast<const uint16_t *>(src + m.w_base)[m.w_off + k] << 16;
+          else wbits = __float_as_uint(e4m3_to_f32(src[m.w_base + m.w_off + k]) * m.scale);
+        }
+        const uint8_t code = a.code ? src[m.c_base + m.c_off + k] : (uint8_t)(x >> 24);
+        uint32_t slot = base + max(code_delay(code), 1u);
+        if (slot >= a.nslots) slot -= a.nslots;
+        red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + (x & a.post_mask),
+                __uint_as_float(wbits), pl);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&S.empty[stage]);
+      if (++stage == kRedStages) {
+        stage = 0;
+        fph ^= 1u;
+      }
+    }
   }
   __syncthreads();
-  const uint32_t nl = min(s_long_n, kRedLongMax);
-  for (uint32_t k = 0; k < nl; ++k) {
-    const uint4 rr = s_long[k];
-    red_range(a, rr.x + tid, rr.y, kRedThreads, base, pf, pl, __uint_as_float(rr.z));
-    if (tid == 0) ev += rr.y - rr.x;
-  }
   // Poisson-source synapses in runs, source order free (exact sums)
   for (uint32_t t = blockIdx.x * kRedThreads + tid; t < a.n_src_syn; t += gridDim.x * kRedThreads) {
     uint32_t lo = 0, hi = a.n_runs - 1;  // largest run with run_off[run] <= t
@@ -1214,11 +1385,11 @@ __global__ void __launch_bounds__(kRedThreads) scatter_red_kernel(StepArgs a) {
     ev += __shfl_xor_sync(0xffffffffu, ev, o);
     src_ev += __shfl_xor_sync(0xffffffffu, src_ev, o);
   }
-  if (lane == 0 && ev) atomicAdd(&s_events, ev);
-  if (lane == 0 && src_ev) atomicAdd(&s_src_events, src_ev);
+  if (lane == 0 && ev) atomicAdd(&S.events, ev);
+  if (lane == 0 && src_ev) atomicAdd(&S.src_events, src_ev);
   __syncthreads();
-  if (tid == 0 && s_events) atomicAdd(a.ev_step, s_events);
-  if (tid == 0 && s_src_events) atomicAdd(a.ev_src_step, s_src_events);
+  if (tid == 0 && S.events) atomicAdd(a.ev_step, S.events);
+  if (tid == 0 && S.src_events) atomicAdd(a.ev_src_step, S.src_events);
   end_of_step(a, n);
 }
 

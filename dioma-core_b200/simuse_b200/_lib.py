@@ -32,6 +32,7 @@ SIGNATURES = {
     "sg_net_create": [vp, i32],
     "sg_net_destroy": [vp],
     "sg_synchronize": [vp],
+    "sg_debug_stall_scatter": [vp, i32],
     "sg_query": [vp, vp],
     "sg_pop_add": [vp, i32, u32, vp],
     "sg_pop_fill_param": [vp, u32, u32, f32],

@@ -245,6 +245,11 @@ class Network:
     def synchronize(self):
         check(lib().sg_synchronize(self._h))
 
+    def debug_stall_scatter(self, on: bool):
+        """Test hook: the pre-centric scatter's producer stops feeding its
+        consumers, whose bounded waits run out and report an error."""
+        check(lib().sg_debug_stall_scatter(self._h, 1 if on else 0))
+
     def enable_raster(self, capacity_steps: int):
         check(lib().sg_raster_enable(self._h, capacity_steps))
         self._raster_mark = self.step_counter

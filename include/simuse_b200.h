@@ -68,7 +68,14 @@ int sg_device_count(int *out);
 /* ---- Network lifecycle ------------------------------------------------ */
 int sg_net_create(sg_net **out, int device);    /* Network::new, core.rs:87-113 */
 int sg_net_destroy(sg_net *net);                /* Drop for Network */
+/* Waits for the handle's stream.  Returns SG_E_CUDA if a step's scatter
+   pipeline gave up a wait on the device (its events are then incomplete);
+   the condition is reported once. */
 int sg_synchronize(sg_net *net);
+/* Test hook (no reference counterpart): on != 0 makes the pre-centric
+   scatter's producer stop feeding its consumers, whose waits then run out
+   (~1 s per step) and set the device error that sg_synchronize reports. */
+int sg_debug_stall_scatter(sg_net *net, int on);
 /* Non-blocking: *idle = 1 when all work queued on the handle's stream has
    completed, 0 while some is still running (cudaStreamQuery). */
 int sg_query(sg_net *net, int *idle);
