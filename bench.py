@@ -27,9 +27,13 @@ Reported, one JSON line on rank 0:
           host's cores, on a bounded sample of the same network.
   batched   (extra key) 64 uneven Izhikevich networks stepping as one batch
           against the same instances one at a time.
-  serving   (extra key) a Poisson stream of LIF / Izhikevich requests through
-          the continuous-batching server: served sims/s, p50/p99 latency,
-          against the one-at-a-time loop.
+  serving   (extra key) Poisson streams of LIF / Izhikevich requests at
+          5..200 requests/s through the continuous-batching server (pooled
+          steps): served sims/s, p50/p99 latency, against the one-at-a-time
+          loop on the same arrivals.
+  precision_paths, hh_stdp_100k, kuramoto_sweep, lif_learn  (extra keys)
+          BF16 / FP8 / ordered-path runs of the headline network, the 100k HH
+          + STDP network, the Kuramoto sweep and learning.
 `--impl reference` times that CPU path alone as the reference arm.
 Multi-GPU (`--gpus N` under torchrun): each rank simulates its own replica
 (seed + rank); no data-path collective (weak scaling).
@@ -90,8 +94,7 @@ def parse(argv=None):
     ap.add_argument("--weights", default="fp32", choices=["fp32", "bf16"],
                     help="synapse weight storage (bf16: 6 B per synapse, FP32 accumulation)")
     ap.add_argument("--batch-instances", type=int, default=64)
-    ap.add_argument("--serve-requests", type=int, default=24)
-    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-requests", type=int, default=100)
     return ap.parse_args(argv)
 
 
@@ -316,13 +319,19 @@ def run_batched(args, local):
 
 def run_serving(args, local):
     """A Poisson stream of seeded LIF / Izhikevich requests (N log-uniform in
-    10,000..2,000,000, lognormal out-degree mean 100 sd 60, 1 s simulated)
-    through the continuous-batching server, against the one-at-a-time loop."""
+    10,000..2,000,000, lognormal out-degree mean 100 sd 60, BF16 weights, 1 s
+    simulated: LIF 10,000 steps of 0.1 ms, Izhikevich 1,000 of 1 ms) through
+    the continuous-batching server (pooled steps), at arrival rates
+    lambda = 5, 20, 50, 100, 200 per s with the same requests.  Against the
+    one-at-a-time loop: each request run alone once (build, run, readback:
+    its service time), and the loop's latencies for each arrival stream from
+    those service times in arrival order (a single FIFO server, queueing
+    included)."""
     import numpy as np
 
     from simuse_b200 import serve as S
     from simuse_b200 import workloads as W
-    n_req, lam = args.serve_requests, args.serve_rate
+    n_req = args.serve_requests
 
     def make():
         idx = np.arange(n_req, dtype=np.uint64)
@@ -332,34 +341,42 @@ def run_serving(args, local):
         return [S.Request(str(k), int(n), 500 + i, 10000 if k == "lif" else 1000)
                 for i, (k, n) in enumerate(zip(kinds, ns))]
 
-    t0 = time.perf_counter()
     solo = [S.run_alone(r, device=local, chunk=1000) for r in make()]
-    t_solo = time.perf_counter() - t0
-    reqs = make()
-    arrive = np.cumsum(-np.log(1.0 - W.uniform01(78, 1, np.arange(n_req, dtype=np.uint64))) / lam)
-    srv = S.Server(device=local, budget_bytes=160 * 10**9, max_resident=16, chunk=500)
-    t0 = time.perf_counter()
-    for r, ta in zip(reqs, arrive):
-        wait = t0 + ta - time.perf_counter()
-        if wait > 0:
-            time.sleep(wait)
-        srv.submit(r)
-    srv.wait_idle(1800)
-    t_all = time.perf_counter() - t0
-    srv.close()
-    lat = srv.latency_percentiles()
-    same = all(np.array_equal(a.spike_steps, b.spike_steps) and np.array_equal(a.spike_index, b.spike_index)
-               for a, b in zip(solo, reqs))
-    solo_lat = np.array([r.latency for r in solo])
-    return {"workload": f"{n_req} requests, Poisson arrivals at {lam:g}/s, LIF (10000 steps) or Izhikevich "
-                        "(1000 steps), N log-uniform 1e4..2e6, lognormal out-degree (100, 60)",
+    service = np.array([r.latency for r in solo])
+    out = {"workload": f"{n_req} requests, LIF (10000 steps) or Izhikevich (1000 steps), N log-uniform 1e4..2e6, "
+                       "lognormal out-degree (100, 60), BF16 weights, Poisson arrivals",
+           "one_at_a_time_service_s_mean": float(service.mean()), "budget_gb": 160, "weights": "bf16",
+           "by_rate": {}}
+    for lam in (5.0, 20.0, 50.0, 100.0, 200.0):
+        arrive = np.cumsum(-np.log(1.0 - W.uniform01(78, int(lam), np.arange(n_req, dtype=np.uint64))) / lam)
+        reqs = make()
+        srv = S.Server(device=local, budget_bytes=160 * 10**9, max_resident=32, chunk=250)
+        t0 = time.perf_counter()
+        for r, ta in zip(reqs, arrive):
+            wait = t0 + ta - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            srv.submit(r)
+        srv.wait_idle(3600)
+        t_all = max(r.t_done for r in reqs) - t0
+        srv.close()
+        lat = srv.latency_percentiles()
+        same = all(a.spike_steps is not None and b.spike_steps is not None and
+                   np.array_equal(a.spike_steps, b.spike_steps) and np.array_equal(a.spike_index, b.spike_index)
+                   for a, b in zip(solo, reqs))
+        fin, q_lat = 0.0, []
+        for ta, sv in zip(arrive, service):  # the one-at-a-time loop on the same arrivals
+            fin = max(fin, ta) + sv
+            q_lat.append(fin - ta)
+        q_lat = np.array(q_lat)
+        out["by_rate"][f"{lam:g}"] = {
             "served_sims_per_s": n_req / t_all, "p50_latency_s": lat["p50_s"], "p99_latency_s": lat["p99_s"],
-            "one_at_a_time_sims_per_s": n_req / t_solo,
-            "one_at_a_time_p50_s": float(np.percentile(solo_lat, 50)),
-            "one_at_a_time_p99_s": float(np.percentile(solo_lat, 99)),
-            "speedup_vs_one_at_a_time": (n_req / t_all) / (n_req / t_solo),
-            "budget_gb": 160, "weights": "fp32", "results_same_as_alone": bool(same),
-            "errors": int(sum(r.error is not None for r in reqs))}
+            "one_at_a_time_sims_per_s": n_req / fin,
+            "one_at_a_time_p50_latency_s": float(np.percentile(q_lat, 50)),
+            "one_at_a_time_p99_latency_s": float(np.percentile(q_lat, 99)),
+            "speedup_vs_one_at_a_time": (n_req / t_all) / (n_req / fin), "pool_ticks": srv.ticks,
+            "results_same_as_alone": bool(same), "errors": int(sum(r.error is not None for r in reqs))}
+    return out
 
 
 def _timed_steps(net, local, n_steps):

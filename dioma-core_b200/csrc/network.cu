@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -109,6 +110,7 @@ struct HostSrc {
   std::vector<uint32_t> post;  // device indices
   std::vector<float> w;
   std::vector<uint8_t> code;
+  std::vector<uint8_t> pt;     // Tsodyks-Markram profile per synapse (0 none)
 };
 
 // A kinetic synapse profile's per-step constants (P/api/net/network/step.rs:
@@ -130,6 +132,8 @@ struct TmHost {
 }  // namespace sg
 
 using namespace sg;
+
+struct sg_pool;
 
 struct sg_net {
   int device = 0;
@@ -181,6 +185,10 @@ struct sg_net {
   DBuf<uint32_t> d_run_lo, d_run_src0, d_run_post0, d_run_len, d_run_seed0;
   DBuf<float> d_run_w, d_run_p;
   DBuf<uint8_t> d_run_code;
+  DBuf<uint8_t> d_run_pt;                 // TM profile per run (source synapses)
+  DBuf<float> d_src_tm_r, d_src_tm_u;     // TM state per source synapse (run order)
+  DBuf<uint32_t> d_src_tm_last;
+  bool src_tm = false;                    // a source synapse has a TM profile
   uint64_t n_runs = 0;
   uint64_t n_src_edges = 0;
   DBuf<float> d_x_pre, d_x_post;
@@ -208,6 +216,12 @@ struct sg_net {
   DBuf<unsigned long long> d_drv_fold;
   DBuf<uint32_t> d_err;        // device error word (scatter pipeline waits)
   uint32_t debug_stall = 0;    // test hook: the scatter's producer stalls
+  // the step arguments in device memory (the pre-centric scatter reads a
+  // table of networks' arguments; a network alone is a table of one)
+  DBuf<StepArgs> d_args;
+  StepArgs h_args{};
+  bool args_uploaded = false;
+  sg_pool *pool = nullptr;     // the pool this network steps in, if any
   unsigned long long drv_folded = ~0ull;
   bool any_drv = false;
   // short-term plasticity: profiles, staged per-edge ids (kept only once an
@@ -257,6 +271,27 @@ struct sg_net {
   uint64_t prof_launches[4] = {0, 0, 0, 0};
 
   uint32_t dev_index(uint32_t pop, uint32_t i) const { return pops[pop].dev_off + i; }
+};
+
+// A pool of built networks stepped together: per step one neuron launch per
+// model over every member's populations and one pre-centric scatter launch
+// over every member (continuous batching of resident networks).
+struct sg_pool {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<sg_net *> members;
+  std::vector<StepArgs> h_nets;
+  std::vector<PopArgs> h_pops;
+  std::vector<uint4> h_map;  // (member, population of h_pops, block), grouped by model
+  uint32_t model_off[5] = {}, model_cnt[5] = {};
+  bool full = false;
+  DBuf<StepArgs> d_nets;
+  DBuf<PopArgs> d_pops;
+  DBuf<uint4> d_map;
+  DBuf<uint32_t> d_done, d_err;
+  cudaGraphExec_t graph = nullptr;
+  uint32_t graph_steps = 0;
 };
 
 namespace {
@@ -380,8 +415,11 @@ StepArgs make_args(sg_net *net) {
   a.n_runs = (uint32_t)net->n_runs;
   a.n_src_syn = (uint32_t)net->n_src_edges;
   a.drv_fold = net->d_drv_fold.p;
-  a.err = net->d_err.p;
-  a.debug_stall = net->debug_stall;
+  a.src_tm = net->src_tm ? 1 : 0;
+  a.run_pt = net->d_run_pt.p;
+  a.src_tm_r = net->d_src_tm_r.p;
+  a.src_tm_u = net->d_src_tm_u.p;
+  a.src_tm_last = net->d_src_tm_last.p;
   a.tm = net->tm_edges ? 1 : 0;
   a.tm_pt = net->d_pt.p;
   a.tm_r = net->d_tm_r.p;
@@ -594,7 +632,11 @@ __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, 
       const uint64_t e = base + first + q;
       pre[e] = from_off + i;
       row[q] = to_off + tgt;
-      w[e] = random_w ? scale * ((float)(uint32_t)(h & 0xffffffffull) * 2.3283064365386963e-10f) : scale;
+      const uint32_t lo = (uint32_t)(h & 0xffffffffull);
+      // random_w 1: U = lo / 2^32; random_w = b >= 2: U on the 2^-b grid (the top b bits of lo)
+      const float u = random_w >= 2 ? (float)(lo >> (32 - random_w)) * __int_as_float((127 - random_w) << 23)
+                                    : (float)lo * 2.3283064365386963e-10f;
+      w[e] = random_w ? scale * u : scale;
       const uint32_t dly = sp.d_span > 1 ? sp.d_min + (uint32_t)(splitmix64(h) & 0xffffffffull) % sp.d_span : sp.d_min;
       code[e] = edge_code((uint8_t)dly, exc ? sp.st_exc : sp.st_inh, exc && (sp.flags_exc & SG_EDGE_STDP));
     }
@@ -903,7 +945,7 @@ __host__ __device__ inline int low_exponent(uint32_t bits) {
 // of source synapses onto it, and the source, weight and code of the last one.
 void find_deferred_drive(sg_net *net, const std::vector<uint32_t> &post_cnt, const std::vector<uint32_t> &post_src,
                          const std::vector<float> &post_w, const std::vector<uint8_t> &post_code,
-                         std::vector<uint8_t> &deferred) {
+                         const std::vector<uint8_t> &post_pt, std::vector<uint8_t> &deferred) {
   net->any_drv = false;
   for (auto &pop : net->pops) {
     pop.drv = false;
@@ -917,7 +959,7 @@ void find_deferred_drive(sg_net *net, const std::vector<uint32_t> &post_cnt, con
       const uint32_t q = q0 + i;
       const uint8_t c = post_code[q];
       const HostSrc &sr = net->srcs[post_src[q]];
-      ok = post_cnt[q] == 1 && code_delay(c) <= 1 && code_ring(c) == 0 && !code_stdp(c) &&
+      ok = post_cnt[q] == 1 && code_delay(c) <= 1 && code_ring(c) == 0 && !code_stdp(c) && post_pt[q] == 0 &&
            std::memcmp(&post_w[q], &w0, 4) == 0 && std::memcmp(&sr.p, &s0.p, 4) == 0 && sr.seed == s0.seed + i;
     }
     if (!ok) continue;
@@ -945,7 +987,7 @@ void build_sources(sg_net *net) {
   if (S) {
     std::vector<uint32_t> post_cnt(net->Nd, 0), post_src(net->Nd, 0);
     std::vector<float> post_w(net->Nd, 0.0f);
-    std::vector<uint8_t> post_code(net->Nd, 0);
+    std::vector<uint8_t> post_code(net->Nd, 0), post_pt(net->Nd, 0);
     for (size_t i = 0; i < S; ++i)
       for (size_t k = 0; k < net->srcs[i].post.size(); ++k) {
         const uint32_t q = net->srcs[i].post[k];
@@ -953,9 +995,10 @@ void build_sources(sg_net *net) {
         post_src[q] = (uint32_t)i;
         post_w[q] = net->srcs[i].w[k];
         post_code[q] = net->srcs[i].code[k];
+        post_pt[q] = net->srcs[i].pt[k];
       }
     deferred.assign(net->Nd, 0);
-    find_deferred_drive(net, post_cnt, post_src, post_w, post_code, deferred);
+    find_deferred_drive(net, post_cnt, post_src, post_w, post_code, post_pt, deferred);
   } else {
     net->any_drv = false;
     for (auto &pop : net->pops) pop.drv = false;
@@ -984,7 +1027,7 @@ void build_sources(sg_net *net) {
   for (uint32_t j = 0; j < G; ++j) lo[j + 1] = lo[j] + (uint32_t)cnt[j];
   std::vector<uint32_t> cur(lo.begin(), lo.end() - 1), se_src(tot), se_post(tot);
   std::vector<float> se_w(tot);
-  std::vector<uint8_t> se_code(tot);
+  std::vector<uint8_t> se_code(tot), se_pt(tot, 0);
   for (size_t i = 0; i < S; ++i) {
     const auto &sr = net->srcs[i];
     for (size_t k = 0; k < sr.post.size(); ++k) {
@@ -994,12 +1037,13 @@ void build_sources(sg_net *net) {
       se_post[pos] = sr.post[k];
       se_w[pos] = sr.w[k];
       se_code[pos] = sr.code[k];
+      se_pt[pos] = sr.pt[k];
     }
   }
   // run-length encoding per block (runs never cross blocks; <= 2^20 long)
   std::vector<uint32_t> run_lo((size_t)G + 1, 0), r_src0, r_post0, r_len, r_seed0;
   std::vector<float> r_w, r_p;
-  std::vector<uint8_t> r_code;
+  std::vector<uint8_t> r_code, r_pt;
   for (uint32_t jb = 0; jb < G; ++jb) {
     run_lo[jb] = (uint32_t)r_len.size();
     for (uint32_t e = lo[jb]; e < lo[jb + 1]; ++e) {
@@ -1008,7 +1052,7 @@ void build_sources(sg_net *net) {
                           src == r_src0.back() + r_len.back() && se_post[e] == r_post0.back() + r_len.back() &&
                           seed[src] == r_seed0.back() + r_len.back() &&
                           std::memcmp(&se_w[e], &r_w.back(), 4) == 0 && se_code[e] == r_code.back() &&
-                          std::memcmp(&p[src], &r_p.back(), 4) == 0;
+                          se_pt[e] == r_pt.back() && std::memcmp(&p[src], &r_p.back(), 4) == 0;
       if (extend) {
         r_len.back()++;
       } else {
@@ -1019,6 +1063,7 @@ void build_sources(sg_net *net) {
         r_w.push_back(se_w[e]);
         r_p.push_back(p[src]);
         r_code.push_back(se_code[e]);
+        r_pt.push_back(se_pt[e]);
       }
     }
   }
@@ -1041,11 +1086,25 @@ void build_sources(sg_net *net) {
   up(net->d_run_p, r_p);
   up(net->d_run_code, r_code);
   up(net->d_run_off, r_off);
+  // Tsodyks-Markram on source synapses (core.rs:372-378): R = 1, U = U0 of
+  // the profile, last = 0, per source synapse in run order
+  net->src_tm = std::any_of(se_pt.begin(), se_pt.end(), [](uint8_t v) { return v != 0; });
+  if (net->src_tm) {
+    std::vector<float> r0(tot, 1.0f), u0(tot, 0.0f);
+    for (size_t e = 0; e < tot; ++e)
+      if (se_pt[e]) u0[e] = net->tm_prof[se_pt[e] - 1].u0;
+    up(net->d_run_pt, r_pt);
+    up(net->d_src_tm_r, r0);
+    up(net->d_src_tm_u, u0);
+    net->d_src_tm_last.alloc(std::max<uint64_t>(tot, 1));
+    net->d_src_tm_last.zero(net->stream);
+  }
   SG_CUDA(cudaStreamSynchronize(net->stream));
   for (auto &sr : net->srcs) {  // host copies are no longer needed
     std::vector<uint32_t>().swap(sr.post);
     std::vector<float>().swap(sr.w);
     std::vector<uint8_t>().swap(sr.code);
+    std::vector<uint8_t>().swap(sr.pt);
   }
 }
 
@@ -1251,7 +1310,7 @@ __global__ void weight_scan_kernel(const uint2 *edge, const uint32_t *edge_x, co
 // every partial sum is a multiple of 2^e below 2^(23+e) in magnitude: exact.
 // Plastic synapses change their weights, so STDP rules it out.
 bool rings_exact(sg_net *net) {
-  if (net->stdp_on || net->tm_edges) return false;  // weights change, or are scaled by R*U
+  if (net->stdp_on || net->tm_edges || net->src_tm) return false;  // weights change, or are scaled by R*U
   cudaStream_t s = net->stream;
   const uint32_t Nd = net->Nd;
   if (net->src_bad) return false;
@@ -1291,8 +1350,33 @@ void drop_graph(sg_net *net);
 // ring sums are exact (any order of the adds gives the reference's bits) or
 // the order is not fixed (sg_set_deterministic(0)); the ordered owner-computes
 // scatter otherwise.
+// The device copy of the step arguments, refreshed when they change (before
+// a graph is captured: the launches read it through a stable pointer).
+void upload_args(sg_net *net, const StepArgs &a) {
+  if (net->args_uploaded && std::memcmp(&a, &net->h_args, sizeof(StepArgs)) == 0) return;
+  if (!net->d_args.n) net->d_args.alloc(1);
+  net->h_args = a;
+  SG_CUDA(cudaMemcpyAsync(net->d_args.p, &net->h_args, sizeof(StepArgs), cudaMemcpyHostToDevice, net->stream));
+  net->args_uploaded = true;
+}
+
+// The pre-centric scatter's shared memory (stage ring) exceeds the 48 KB
+// default: allowed once per device before its first launch.
+void allow_red_smem() {
+  SG_CUDA(cudaFuncSetAttribute(scatter_red_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RedSmem)));
+}
+
+unsigned red_grid(int device) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return (unsigned)sms * kRedBlocksPerSM;
+}
+
 void update_path(sg_net *net) {
-  const int red = (!net->deterministic || net->exact) ? 1 : 0;
+  // the pre-centric scatter applies neither pair STDP nor short-term
+  // plasticity: those networks keep the owner-computes scatter in any mode
+  const bool plain = !net->stdp_on && !net->tm_edges && !net->src_tm;
+  const int red = plain && (!net->deterministic || net->exact) ? 1 : 0;
   if (red != net->red) drop_graph(net);
   net->red = red;
 }
@@ -1397,6 +1481,7 @@ void finish_build(sg_net *net) {
   const int sm = (int)net->scatter_smem;
   SG_CUDA(cudaFuncSetAttribute(scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   SG_CUDA(cudaFuncSetAttribute(scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  allow_red_smem();
   setup_scatter(net);
   if (net->weight_format == SG_W_FP8) net->d_edge.release();  // scanned by the exact-sum test; x + E4M3 + scale from here
   if (net->tm_edges) {  // build.rs:69-84: R = 1, U = U0 of the edge's profile, last = 0
@@ -1476,13 +1561,37 @@ void upload_pop_table(sg_net *net) {
   net->pop_tab_dirty = false;
 }
 
+// Launches a step kernel with programmatic stream serialization: it may
+// start while the stream's previous kernel drains (the kernels call
+// pdl_wait() before touching what earlier kernels wrote).  Off when
+// SG_NO_PDL is set in the environment (the plain launch order).
+bool use_pdl() {
+  static const bool on = std::getenv("SG_NO_PDL") == nullptr;
+  return on;
+}
+template <typename... KArgs, typename... Args>
+void launch_step_kernel(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                        Args &&...args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = use_pdl() ? 1 : 0;
+  SG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
+
 template <int M, bool FULL> void launch_neuron_form(sg_net *net, const StepArgs &a, uint32_t nb) {
   if (net->model_single[M] >= 0)
-    neuron_kernel<M, FULL><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, net->pop_tab[net->model_single[M]],
-                                                                          nullptr, nullptr);
+    launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M>::THREADS, 0, net->stream, a,
+                       net->pop_tab[net->model_single[M]], (const PopArgs *)nullptr, (const uint2 *)nullptr);
   else
-    neuron_kernel<M, FULL><<<nb, NeuronCfg<M>::THREADS, 0, net->stream>>>(a, PopArgs{}, net->d_pop_tab.p,
-                                                                          net->d_blk_map.p + net->model_blk_off[M]);
+    launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M>::THREADS, 0, net->stream, a, PopArgs{},
+                       (const PopArgs *)net->d_pop_tab.p, (const uint2 *)(net->d_blk_map.p + net->model_blk_off[M]));
 }
 
 // The lean neuron kernel serves steps without kinetic synapses, input
@@ -1531,12 +1640,11 @@ void enqueue_rest(sg_net *net, const StepArgs &a) {
     if (p.external && p.n)
       ext_spikes_kernel<<<p.cap / kNeuronBlock, kNeuronBlock, 0, s>>>(a, p.dev_off, p.n, p.ext_src);
   if (a.red) {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
-    scatter_red_kernel<<<(unsigned)sms * kRedBlocksPerSM, kRedThreads, sizeof(RedSmem), s>>>(a);
+    launch_step_kernel(scatter_red_kernel, red_grid(net->device), kRedThreads, sizeof(RedSmem), s,
+                       (const StepArgs *)net->d_args.p, 1u, net->d_done.p, net->d_err.p, net->debug_stall);
   } else {
-    if (net->seg32) scatter_kernel<true><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
-    else scatter_kernel<false><<<net->G, kScatterThreads, net->scatter_smem, s>>>(a);
+    if (net->seg32) launch_step_kernel(scatter_kernel<true>, net->G, kScatterThreads, net->scatter_smem, s, a);
+    else launch_step_kernel(scatter_kernel<false>, net->G, kScatterThreads, net->scatter_smem, s, a);
   }
   if (net->learn_on && net->n_edges) {
     LearnArgs L{};
@@ -1574,6 +1682,7 @@ void do_steps_profiled(sg_net *net, uint32_t n) {
   upload_pop_table(net);
   if (net->learn_on) net->d_l_motor.zero(net->stream);  // motor counts are per step call
   const StepArgs a = make_args(net);
+  upload_args(net, a);
   if (net->prof_ev.empty()) {
     net->prof_ev.resize(3);
     for (auto &e : net->prof_ev) SG_CUDA(cudaEventCreate(&e));
@@ -1615,6 +1724,7 @@ void do_steps(sg_net *net, uint32_t n) {
   upload_pop_table(net);
   if (net->learn_on) net->d_l_motor.zero(net->stream);  // motor counts are per step call
   const StepArgs a = make_args(net);
+  upload_args(net, a);
   const uint32_t G = 32;  // steps per graph launch
   uint32_t done = 0;
   if (n >= G) {
@@ -1677,8 +1787,11 @@ int sg_net_create(sg_net **out, int device) {
   });
 }
 
+int sg_pool_remove(sg_pool *pool, sg_net *net);
+
 int sg_net_destroy(sg_net *net) {
   if (!net) return SG_OK;
+  if (net->pool) sg_pool_remove(net->pool, net);  // a destroyed network leaves its pool first
   {
     DevGuard g(net->device);
     cudaStreamSynchronize(net->stream);
@@ -1989,6 +2102,7 @@ static OutDegreeSpec outdegree_spec(sg_net *net, uint32_t from, uint32_t to, uin
   SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
   SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
   SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
+  SG_REQUIRE(random_w >= 0 && random_w <= 24, SG_E_INVALID, "random_w: 0, 1, or a grid of 2..24 bits");
   OutDegreeSpec sp{};
   sp.seed = seed;
   sp.from_off = net->pops[from].dev_off;
@@ -2175,27 +2289,39 @@ int sg_poisson_add(sg_net *net, float rate_hz, float dt_ms, uint32_t seed, uint3
   return sg_poisson_add_many(net, 1, rate_hz, dt_ms, nullptr, seed, out_id);
 }
 
-int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts, const float *w,
-                       const uint8_t *d, const uint8_t *st, uint64_t n) {
+int sg_poisson_connect_plastic(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts, const float *w,
+                               const uint8_t *d, const uint8_t *st, const uint8_t *plast, uint64_t n) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Cannot connect after build()");
     SG_REQUIRE(src < net->srcs.size(), SG_E_INVALID, "poisson source out of range");
     require_local(net, to);
+    SG_REQUIRE(n == 0 || (posts && w && d), SG_E_INVALID, "null slice");
     const auto &pt = net->pops[to];
     auto &s = net->srcs[src];
     for (uint64_t i = 0; i < n; ++i) {
       SG_REQUIRE(posts[i] < pt.n, SG_E_INVALID, "post index out of bounds");
       SG_REQUIRE(std::isfinite(w[i]), SG_E_INVALID, "connect_poisson_source: weight must be finite");
       SG_REQUIRE(d[i] < kSlots, SG_E_INVALID, "connect_poisson_source: delay >= MAX_DELAY_SLOTS (32)");
-      net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
       const uint8_t t = st ? st[i] : 0;
       SG_REQUIRE(t <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
+      const uint8_t q = plast ? plast[i] : 0;
+      SG_REQUIRE(q <= net->tm_prof.size(), SG_E_INVALID,
+                 "plasticity profile " + std::to_string(q) + " is not registered");
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+      net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
       s.post.push_back(pt.dev_off + posts[i]);
       s.w.push_back(w[i]);
-      s.code.push_back(edge_code(d[i], t, false));
+      s.code.push_back(edge_code(d[i], st ? st[i] : 0, false));
+      s.pt.push_back(plast ? plast[i] : 0);
     }
   });
+}
+
+int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts, const float *w,
+                       const uint8_t *d, const uint8_t *st, uint64_t n) {
+  return sg_poisson_connect_plastic(net, src, to, posts, w, d, st, nullptr, n);
 }
 
 int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint32_t to, const uint32_t *posts,
@@ -2216,6 +2342,7 @@ int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint3
       s.post.push_back(pt.dev_off + q);
       s.w.push_back(weight);
       s.code.push_back(edge_code(delay, 0, false));
+      s.pt.push_back(0);
     }
   });
 }
@@ -2469,7 +2596,9 @@ int sg_step_end(sg_net *net) {
     for (const auto &p : net->pops)
       SG_REQUIRE(!p.external || p.ext_src || p.n == 0, SG_E_STATE, "an external population has no spike source");
     DevGuard g(net->device);
-    enqueue_rest(net, make_args(net));
+    const StepArgs a = make_args(net);
+    upload_args(net, a);
+    enqueue_rest(net, a);
     SG_CUDA(cudaGetLastError());
     net->host_step += 1;
   });
@@ -3409,6 +3538,228 @@ int sg_stream(sg_net *net, void **out) {
   NET_CHECK(net);
   if (!out) return SG_E_INVALID;
   *out = (void *)net->stream;
+  return SG_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// pools of resident networks (continuous batching)
+// ===========================================================================
+namespace {
+
+void pool_drop_graph(sg_pool *pool) {
+  if (pool->graph) cudaGraphExecDestroy(pool->graph);
+  pool->graph = nullptr;
+  pool->graph_steps = 0;
+}
+
+// The members' arguments, populations and block map; uploaded (and the
+// captured graph dropped) when they change.
+void pool_prepare(sg_pool *pool) {
+  std::vector<StepArgs> nets;
+  std::vector<PopArgs> pops;
+  std::vector<uint4> map;
+  bool full = false;
+  for (size_t i = 0; i < pool->members.size(); ++i) {
+    sg_net *net = pool->members[i];
+    upload_pop_table(net);
+    const StepArgs a = make_args(net);
+    SG_REQUIRE(a.red, SG_E_STATE,
+               "pool: every member takes the pre-centric scatter (exact ring sums, or the atomic mode)");
+    SG_REQUIRE(!net->learn_on && !has_external(net), SG_E_STATE,
+               "pool: learning networks and networks split across GPUs step on their own");
+    full = full || needs_full_neuron_kernel(net, a);
+    nets.push_back(a);
+  }
+  for (int m = 1; m <= 4; ++m) {
+    pool->model_off[m] = (uint32_t)map.size();
+    for (size_t i = 0; i < pool->members.size(); ++i) {
+      sg_net *net = pool->members[i];
+      for (size_t q = 0; q < net->pops.size(); ++q) {
+        const HostPop &hp = net->pops[q];
+        if (hp.model != m || hp.n == 0 || hp.external) continue;
+        const uint32_t pi = (uint32_t)pops.size();
+        pops.push_back(net->pop_tab[q]);
+        for (uint32_t b = 0; b < hp.cap / kNeuronBlock; ++b) map.push_back(make_uint4((uint32_t)i, pi, b, 0u));
+      }
+    }
+    pool->model_cnt[m] = (uint32_t)map.size() - pool->model_off[m];
+  }
+  const bool same = nets.size() == pool->h_nets.size() && pops.size() == pool->h_pops.size() &&
+                    map.size() == pool->h_map.size() && full == pool->full &&
+                    std::memcmp(nets.data(), pool->h_nets.data(), nets.size() * sizeof(StepArgs)) == 0 &&
+                    std::memcmp(pops.data(), pool->h_pops.data(), pops.size() * sizeof(PopArgs)) == 0 &&
+                    std::memcmp(map.data(), pool->h_map.data(), map.size() * sizeof(uint4)) == 0;
+  if (same) return;
+  pool_drop_graph(pool);
+  SG_CUDA(cudaStreamSynchronize(pool->stream));  // no step in flight reads the old tables
+  pool->h_nets = std::move(nets);
+  pool->h_pops = std::move(pops);
+  pool->h_map = std::move(map);
+  pool->full = full;
+  if (pool->d_nets.n < pool->h_nets.size()) pool->d_nets.alloc(pool->h_nets.size());
+  if (pool->d_pops.n < std::max<size_t>(pool->h_pops.size(), 1)) pool->d_pops.alloc(std::max<size_t>(pool->h_pops.size(), 1));
+  if (pool->d_map.n < std::max<size_t>(pool->h_map.size(), 1)) pool->d_map.alloc(std::max<size_t>(pool->h_map.size(), 1));
+  SG_CUDA(cudaMemcpyAsync(pool->d_nets.p, pool->h_nets.data(), pool->h_nets.size() * sizeof(StepArgs),
+                          cudaMemcpyHostToDevice, pool->stream));
+  if (!pool->h_pops.empty())
+    SG_CUDA(cudaMemcpyAsync(pool->d_pops.p, pool->h_pops.data(), pool->h_pops.size() * sizeof(PopArgs),
+                            cudaMemcpyHostToDevice, pool->stream));
+  if (!pool->h_map.empty())
+    SG_CUDA(cudaMemcpyAsync(pool->d_map.p, pool->h_map.data(), pool->h_map.size() * sizeof(uint4),
+                            cudaMemcpyHostToDevice, pool->stream));
+  SG_CUDA(cudaStreamSynchronize(pool->stream));
+}
+
+template <int M> void pool_launch_neuron(sg_pool *pool) {
+  const uint32_t nb = pool->model_cnt[M];
+  if (nb == 0) return;
+  const uint4 *map = pool->d_map.p + pool->model_off[M];
+  if (pool->full)
+    launch_step_kernel(neuron_pool_kernel<M, true>, nb, NeuronCfg<M>::THREADS, 0, pool->stream,
+                       (const StepArgs *)pool->d_nets.p, (const PopArgs *)pool->d_pops.p, map);
+  else
+    launch_step_kernel(neuron_pool_kernel<M, false>, nb, NeuronCfg<M>::THREADS, 0, pool->stream,
+                       (const StepArgs *)pool->d_nets.p, (const PopArgs *)pool->d_pops.p, map);
+}
+
+void pool_enqueue_step(sg_pool *pool) {
+  pool_launch_neuron<kLIF>(pool);
+  pool_launch_neuron<kIZH>(pool);
+  pool_launch_neuron<kGPEA>(pool);
+  pool_launch_neuron<kHH>(pool);
+  launch_step_kernel(scatter_red_kernel, red_grid(pool->device), kRedThreads, sizeof(RedSmem), pool->stream,
+                     (const StepArgs *)pool->d_nets.p, (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u);
+}
+
+}  // namespace
+
+extern "C" {
+
+int sg_pool_create(sg_pool **out, int device) {
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = nullptr;
+    int n = 0;
+    SG_CUDA(cudaGetDeviceCount(&n));
+    SG_REQUIRE(device >= 0 && device < n, SG_E_INVALID, "device ordinal out of range");
+    DevGuard g(device);
+    auto *pool = new sg_pool();
+    pool->device = device;
+    if (cudaStreamCreateWithFlags(&pool->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&pool->ev, cudaEventDisableTiming) != cudaSuccess) {
+      if (pool->stream) cudaStreamDestroy(pool->stream);
+      delete pool;
+      SG_REQUIRE(false, SG_E_CUDA, "pool: stream or event creation failed");
+    }
+    pool->d_done.alloc(1);
+    pool->d_done.zero(pool->stream);
+    pool->d_err.alloc(1);
+    pool->d_err.zero(pool->stream);
+    allow_red_smem();
+    SG_CUDA(cudaStreamSynchronize(pool->stream));
+    *out = pool;
+  });
+}
+
+int sg_pool_add(sg_pool *pool, sg_net *net) {
+  return run([&] {
+    SG_REQUIRE(pool && net, SG_E_INVALID, "null pool or network");
+    SG_REQUIRE(net->built, SG_E_STATE, "pool: the network is not built");
+    SG_REQUIRE(net->device == pool->device, SG_E_INVALID, "pool: the network lives on another device");
+    SG_REQUIRE(net->pool == nullptr, SG_E_STATE, "pool: the network is already in a pool");
+    SG_REQUIRE(pool->members.size() < kPoolMax, SG_E_INVALID,
+               "pool: at most " + std::to_string(kPoolMax) + " networks");
+    SG_REQUIRE(net->red, SG_E_STATE,
+               "pool: only networks on the pre-centric scatter (exact ring sums, or the atomic mode) join a pool");
+    pool->members.push_back(net);
+    net->pool = pool;
+  });
+}
+
+int sg_pool_remove(sg_pool *pool, sg_net *net) {
+  return run([&] {
+    SG_REQUIRE(pool && net, SG_E_INVALID, "null pool or network");
+    auto it = std::find(pool->members.begin(), pool->members.end(), net);
+    SG_REQUIRE(it != pool->members.end(), SG_E_INVALID, "pool: the network is not a member");
+    DevGuard g(pool->device);
+    SG_CUDA(cudaStreamSynchronize(pool->stream));
+    pool->members.erase(it);
+    net->pool = nullptr;
+    pool_drop_graph(pool);
+  });
+}
+
+int sg_pool_size(sg_pool *pool, uint32_t *out) {
+  return run([&] {
+    SG_REQUIRE(pool && out, SG_E_INVALID, "null pool or output");
+    *out = (uint32_t)pool->members.size();
+  });
+}
+
+int sg_pool_step(sg_pool *pool, uint32_t n_steps) {
+  return run([&] {
+    SG_REQUIRE(pool, SG_E_INVALID, "null pool");
+    if (pool->members.empty() || n_steps == 0) return;
+    DevGuard g(pool->device);
+    for (sg_net *net : pool->members) SG_REQUIRE(net->total > 0, SG_E_STATE, "pool: an empty network");
+    pool_prepare(pool);
+    // the pool's steps follow everything queued on the members' streams
+    for (sg_net *net : pool->members) {
+      SG_CUDA(cudaEventRecord(pool->ev, net->stream));
+      SG_CUDA(cudaStreamWaitEvent(pool->stream, pool->ev, 0));
+    }
+    const uint32_t G = 32;
+    uint32_t done = 0;
+    if (n_steps >= G) {
+      if (!pool->graph || pool->graph_steps != G) {
+        pool_drop_graph(pool);
+        cudaGraph_t gr;
+        SG_CUDA(cudaStreamBeginCapture(pool->stream, cudaStreamCaptureModeThreadLocal));
+        for (uint32_t k = 0; k < G; ++k) pool_enqueue_step(pool);
+        SG_CUDA(cudaStreamEndCapture(pool->stream, &gr));
+        SG_CUDA(cudaGraphInstantiate(&pool->graph, gr, 0));
+        cudaGraphDestroy(gr);
+        pool->graph_steps = G;
+      }
+      for (; done + G <= n_steps; done += G) SG_CUDA(cudaGraphLaunch(pool->graph, pool->stream));
+    }
+    for (; done < n_steps; ++done) pool_enqueue_step(pool);
+    SG_CUDA(cudaGetLastError());
+    // and everything queued on a member's stream later follows them
+    SG_CUDA(cudaEventRecord(pool->ev, pool->stream));
+    for (sg_net *net : pool->members) {
+      SG_CUDA(cudaStreamWaitEvent(net->stream, pool->ev, 0));
+      net->host_step += n_steps;
+    }
+  });
+}
+
+int sg_pool_synchronize(sg_pool *pool) {
+  return run([&] {
+    SG_REQUIRE(pool, SG_E_INVALID, "null pool");
+    DevGuard g(pool->device);
+    SG_CUDA(cudaStreamSynchronize(pool->stream));
+    uint32_t e = 0;
+    SG_CUDA(cudaMemcpy(&e, pool->d_err.p, 4, cudaMemcpyDeviceToHost));
+    if (e) {
+      SG_CUDA(cudaMemset(pool->d_err.p, 0, 4));
+      SG_REQUIRE(false, SG_E_CUDA, "pool scatter: a pipeline wait timed out on the device");
+    }
+  });
+}
+
+int sg_pool_destroy(sg_pool *pool) {
+  if (!pool) return SG_OK;
+  DevGuard g(pool->device);
+  cudaStreamSynchronize(pool->stream);
+  for (sg_net *net : pool->members) net->pool = nullptr;
+  pool_drop_graph(pool);
+  cudaEventDestroy(pool->ev);
+  cudaStream_t s = pool->stream;
+  delete pool;
+  cudaStreamDestroy(s);
   return SG_OK;
 }
 

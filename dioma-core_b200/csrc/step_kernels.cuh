@@ -162,11 +162,14 @@ struct StepArgs {
   const uint32_t *run_off;
   uint32_t n_runs;
   uint32_t n_src_syn;
-  // device error word: bit 0 a pipeline wait of the scatter ran out of time
-  // (read and cleared by sg_synchronize); the debug word stalls the
-  // scatter's producer (test hook: its consumers' waits then run out)
-  uint32_t *err;
-  uint32_t debug_stall;
+  // Tsodyks-Markram on Poisson-source synapses: profile per run (0 none) and
+  // per source synapse (index run_off[run] + offset) its R, U and last spike
+  // step (P/api/net/network/step.rs:166-180)
+  int src_tm;
+  const uint8_t *run_pt;
+  float *src_tm_r;
+  float *src_tm_u;
+  uint32_t *src_tm_last;
   // deferred drive: the step whose deferred Poisson events were already
   // added to the ring (by drive_fold_kernel before an inject or a ring
   // readback), or ~0
@@ -231,6 +234,16 @@ struct PopArgs {
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Programmatic dependent launch: the step kernels are launched so that the
+// next kernel of the stream may start while this one drains.  pdl_wait()
+// returns once the previous kernel of the stream has completed and its memory
+// is visible (a no-op for a kernel launched without the attribute); every
+// kernel calls it before it touches data an earlier kernel of the step wrote.
+// pdl_release() lets the next kernel launch (its blocks then run up to their
+// own pdl_wait()).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // L2 cache policies: the CSR of the spiking rows streams through once per
 // step (evict first); the delay ring is re-read every step (evict last) and
@@ -614,6 +627,8 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
 template <int MODEL, bool FULL>
 __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCfg<MODEL>::MIN_BLOCKS)
     neuron_kernel(StepArgs a, PopArgs p0, const PopArgs *__restrict__ pops, const uint2 *__restrict__ map) {
+  pdl_wait();
+  pdl_release();
   if (map == nullptr) {
     neuron_block<MODEL, FULL>(a, p0, blockIdx.x);
     return;
@@ -792,6 +807,23 @@ __device__ __forceinline__ uint32_t put_event(const StepArgs &a, ScatterSmem &S,
   return cell;
 }
 
+// The last block of a step's scatter: per-step statistics, event totals,
+// the step counter (and the pre-centric scatter's spike count).
+__device__ __forceinline__ void end_of_step_last(const StepArgs &a, uint32_t n_spikes) {
+  const unsigned long long step = *a.step;
+  const unsigned long long ev = *(volatile unsigned long long *)a.ev_step;
+  if (a.stat_cap) {
+    a.stat_spk[step % a.stat_cap] = n_spikes;
+    a.stat_ev[step % a.stat_cap] = ev;
+  }
+  *a.ev_total += ev;
+  *a.ev_step = 0;
+  *a.ev_src_total += *(volatile unsigned long long *)a.ev_src_step;
+  *a.ev_src_step = 0;
+  if (a.red) *a.red_cnt = 0;  // the next step's neuron kernel appends from 0
+  *a.step = step + 1;
+}
+
 __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -799,19 +831,8 @@ __device__ __forceinline__ void end_of_step(const StepArgs &a, uint32_t n_spikes
     const uint32_t t = atomicAdd(a.done, 1u);
     if (t == gridDim.x - 1) {
       __threadfence();
-      const unsigned long long step = *a.step;
-      const unsigned long long ev = *(volatile unsigned long long *)a.ev_step;
-      if (a.stat_cap) {
-        a.stat_spk[step % a.stat_cap] = n_spikes;
-        a.stat_ev[step % a.stat_cap] = ev;
-      }
-      *a.ev_total += ev;
-      *a.ev_step = 0;
-      *a.ev_src_total += *(volatile unsigned long long *)a.ev_src_step;
-      *a.ev_src_step = 0;
+      end_of_step_last(a, n_spikes);
       *a.done = 0;
-      if (a.red) *a.red_cnt = 0;  // the next step's neuron kernel appends from 0
-      *a.step = step + 1;
       __threadfence();
     }
   }
@@ -824,6 +845,8 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   const uint32_t tid = threadIdx.x;
   const uint32_t j = blockIdx.x;
   const uint32_t p0 = j * a.P;
+  pdl_wait();
+  pdl_release();
   const unsigned long long step = *a.step;
   const uint32_t base = (uint32_t)(step % a.nslots);
   const uint32_t G1 = a.G + 1;
@@ -1022,9 +1045,9 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
       uint8_t e_code[kEPT];
       // runs are few and long: find the run of the first entry by search,
       // then walk forward, reading a run's parameters once
-      uint32_t ri = kEmpty, i = 0, post0 = 0, seed0 = 0;
+      uint32_t ri = kEmpty, i = 0, post0 = 0, seed0 = 0, roff = 0;
       float p = 0.0f, rw = 0.0f;
-      uint8_t rcode = 0;
+      uint8_t rcode = 0, rpt = 0;
       if (tid * kEPT < mt) i = upper_index(S.pseg, rc, w0 + tid * kEPT);
 #pragma unroll
       for (uint32_t r = 0; r < kEPT; ++r) {
@@ -1039,12 +1062,23 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
             seed0 = __ldg(a.run_seed0 + ri);
             rw = __ldg(a.run_w + ri);
             rcode = __ldg(a.run_code + ri);
+            if (a.src_tm) {
+              rpt = __ldg(a.run_pt + ri);
+              roff = __ldg(a.run_off + ri);
+            }
           }
           const uint32_t t = g - S.pseg[i];
           e_post[r] = post0 + t;
           e_w[r] = rw;
           e_code[r] = rcode;
-          if (p > 0.0f && poisson_spike(seed0 + t, 0, step, p)) fired |= 1u << r;
+          if (p > 0.0f && poisson_spike(seed0 + t, 0, step, p)) {
+            fired |= 1u << r;
+            if (rpt) {  // the synapse's short-term plasticity scales the delivered weight
+              const uint32_t q = rpt - 1u, e = roff + t;  // each source synapse belongs to one block
+              e_w[r] = tm_spike(a.tm_u0[q], a.tm_arec[q], a.tm_afac[q], (a.tm_fac >> q) & 1u, a.src_tm_r[e],
+                                a.src_tm_u[e], a.src_tm_last[e], rw, step);
+            }
+          }
         }
       }
       uint32_t m;
@@ -1120,11 +1154,14 @@ constexpr uint32_t kRedBlocksPerSM = SG_RED_BLOCKS_PER_SM;
 constexpr int kRedUnroll = SG_RED_UNROLL;  // consumer loop unroll
 constexpr uint32_t kRedStages = 4;
 constexpr uint32_t kRedChunk = 1024;         // synapses per stage
-// a stage holds kRedChunk FP32 records widened to 16-byte boundaries (+16 B)
-// and, for networks whose code bytes are a separate array, their code bytes
-// (+32 B); x words + bf16/fp8 weights + code bytes take less
-constexpr uint32_t kRedStageBytes = 10240;
-static_assert(8 * (kRedChunk + 2) + 16 + (kRedChunk + 32) <= kRedStageBytes, "scatter stage too small");
+constexpr uint32_t kRedSegs = 16;            // row pieces per stage (short rows share a stage)
+// Stage regions: x words or FP32 records, weights (split formats), code
+// bytes (networks whose code bytes are a separate array).  Each row piece is
+// widened to 16-byte boundaries: at most 32 extra bytes per piece and region.
+constexpr uint32_t kRedXBytes = kRedChunk * 8 + kRedSegs * 32;
+constexpr uint32_t kRedWBytes = kRedChunk * 2 + kRedSegs * 32;
+constexpr uint32_t kRedCBytes = kRedChunk + kRedSegs * 32;
+constexpr uint32_t kRedStageBytes = kRedXBytes + kRedWBytes + kRedCBytes;
 constexpr unsigned long long kWaitNs = 1000000000ull;     // every pipeline wait gives up after ~1 s
 
 __device__ __forceinline__ void red_add(float *p, float v, unsigned long long pol) {
@@ -1168,45 +1205,69 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     if ((i & 63u) == 0 && global_ns() - t0 > kWaitNs) return false;
   }
 }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
 // Bulk copy of `bytes` (a multiple of 16) from global `src` (16-byte aligned)
-// to shared `dst` (16-byte aligned), completing on `bar`.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+// to shared `dst` (16-byte aligned), completing on `bar`; L2 policy `pol`
+// (the synapse stream is evict_first, so that it does not push the delay
+// rings out of L2).
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                         unsigned long long pol) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
       : "memory");
 }
 
-// One stage: up to kRedChunk synapses of one row.
+constexpr uint32_t kPoolMax = 64;  // networks in one pooled step
+// The consumers' view of one network of the launch.
+struct RedNet {
+  float *ring;
+  const uint8_t *code;  // separate code bytes, or null
+  uint32_t Nd, nslots, base, post_mask;
+  int fmt;              // 0 FP32 records, 1 BF16, 2 FP8
+};
+// One piece of a row in a stage.
+struct RedSeg {
+  uint32_t first;   // index of its first synapse among the stage's synapses
+  uint32_t x;       // element index of its first synapse in the stage's x region
+  uint32_t w;       // element index of its first weight in the weight region
+  uint32_t c;       // index of its first code byte in the code region
+  uint32_t net;     // the network it belongs to
+  float scale;      // FP8 row scale
+};
+// One stage: up to kRedChunk synapses from up to kRedSegs row pieces.
 struct RedStage {
-  uint32_t n;        // synapses in the stage, or kEmpty: the producer is done
-  uint32_t x_off;    // first synapse within the x / record buffer (elements)
-  uint32_t w_off;    // first weight within the weight buffer (split formats)
-  uint32_t c_off;    // first code byte within the code buffer (unpacked x words)
-  uint32_t w_base;   // byte offset of the weight buffer in the stage
-  uint32_t c_base;   // byte offset of the code buffer in the stage
-  float scale;       // FP8 row scale
+  uint32_t n;       // synapses in the stage, or kEmpty: the producer is done
+  uint32_t n_seg;
+  RedSeg seg[kRedSegs];
 };
 struct RedSmem {
   alignas(16) unsigned char buf[kRedStages][kRedStageBytes];
   RedStage meta[kRedStages];
   uint64_t full[kRedStages];
   uint64_t empty[kRedStages];
-  unsigned long long events, src_events;
+  RedNet nets[kPoolMax];
+  unsigned long long ev[kPoolMax], src_ev[kPoolMax];  // this block's events per network
 };
 
-// Copies elements [b, e) of an array of `esz`-byte elements to `dst`: the
-// range is widened to 16-byte boundaries (the arrays are padded so that the
-// widened end stays inside them).  Returns the bytes copied; *off = index of
-// element b in the copy.
-__device__ __forceinline__ uint32_t bulk_elems(unsigned char *dst, const void *arr, uint32_t esz, uint32_t b,
-                                               uint32_t e, uint64_t *bar, uint32_t *off) {
+// Copies elements [b, e) of an array of `esz`-byte elements to shared memory
+// at byte offset *cursor of `region`, widened to 16-byte boundaries (the
+// arrays are padded so that the widened end stays inside them), announcing
+// the bytes on `bar` first.  Returns the element index of b in the region
+// and advances *cursor.
+__device__ __forceinline__ uint32_t bulk_elems(unsigned char *region, uint32_t *cursor, const void *arr, uint32_t esz,
+                                               uint32_t b, uint32_t e, uint64_t *bar, unsigned long long pol) {
   const uint32_t per = 16u / esz;
   const uint32_t b0 = b - b % per, e1 = (e + per - 1) / per * per;
-  *off = b - b0;
   const uint32_t bytes = (e1 - b0) * esz;
-  bulk_g2s(dst, (const unsigned char *)arr + (size_t)b0 * esz, bytes, bar);
-  return bytes;
+  const uint32_t at = *cursor;
+  mbar_expect_tx(bar, bytes);
+  bulk_g2s(region + at, (const unsigned char *)arr + (size_t)b0 * esz, bytes, bar, pol);
+  *cursor = at + bytes;
+  return at / esz + (b - b0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1215,8 +1276,10 @@ __device__ __forceinline__ uint32_t bulk_elems(unsigned char *dst, const void *a
 // a cell's bits, so each spiking row is read once, whole, and every event goes
 // to its ring cell with a fire-and-forget red.global.add in L2 (the rings stay
 // L2-resident: the synapse records stream through, the ring cells are updated
-// with evict_last).  Block b takes the step's spiking rows b, b + G, ...
-// Warp 0 is the producer: its lanes look up 32 rows at a time (flat list,
+// with evict_last).  One launch serves a table of networks (a single network,
+// or every network of a pool): block b takes spiking rows b, b + G, ... of
+// each network in turn.  Warp 0 is the producer: its lanes look up 32 rows
+// at a time (flat list,
 // row bounds) and lane 0 copies each row, kRedChunk synapses per stage, into
 // a kRedStages-deep shared-memory ring with 1-D bulk copies (cp.async.bulk,
 // this GPU's memory, no multicast) that complete on the stage's mbarrier.
@@ -1224,9 +1287,12 @@ __device__ __forceinline__ uint32_t bulk_elems(unsigned char *dst, const void *a
 // issue the reds, then release the stage.  Every wait gives up after ~1 s,
 // records the failure in *err and leaves the kernel (with the copies it
 // issued completed).  Poisson-source synapses that the neuron kernel does not
-// take (deferred drive) follow, one per thread.
+// take (deferred drive) follow, one per thread.  The last block to finish
+// closes the step of every network of the table.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM) scatter_red_kernel(StepArgs a) {
+__global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
+    scatter_red_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done, uint32_t *err,
+                       uint32_t stall) {
   extern __shared__ __align__(128) unsigned char red_smem[];
   RedSmem &S = *reinterpret_cast<RedSmem *>(red_smem);
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
@@ -1235,89 +1301,117 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM) scatter_red_kern
       mbar_init(&S.full[k], 1);
       mbar_init(&S.empty[k], kRedConsumers / 32);
     }
-    S.events = 0;
-    S.src_events = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  pdl_wait();
+  pdl_release();
+  for (uint32_t i = tid; i < n_nets; i += kRedThreads) {
+    const StepArgs &a = nets[i];
+    RedNet r;
+    r.ring = a.ring;
+    r.code = a.code;
+    r.Nd = a.Nd;
+    r.nslots = a.nslots;
+    r.base = (uint32_t)(*a.step % a.nslots);
+    r.post_mask = a.post_mask;
+    r.fmt = a.wbf16 ? 1 : a.wfp8 ? 2 : 0;
+    S.nets[i] = r;
+    S.ev[i] = 0;
+    S.src_ev[i] = 0;
+  }
   __syncthreads();
-  const unsigned long long step = *a.step;
-  const uint32_t base = (uint32_t)(step % a.nslots);
-  const uint32_t n = *a.red_cnt;
   const unsigned long long pl = policy_evict_last();
-  unsigned long long ev = 0, src_ev = 0;
   bool failed = false;
-  const uint32_t xsz = a.wbf16 || a.wfp8 ? 4u : 8u;  // bytes per x word or record
   if (warp == 0) {
     // ---- producer ----
-    uint32_t stage = 0, eph = 1;  // the first round of empty waits passes at once
-    uint32_t filled = 0, fill_par = 0;  // lane 0: per stage (bit), filled at least once, parity of the fills
-    for (uint32_t r0 = blockIdx.x; r0 < n && !failed; r0 += 32 * gridDim.x) {
-      const uint32_t r = r0 + lane * gridDim.x;
-      uint32_t beg = 0, end = 0;
-      float scale = 1.0f;
-      if (r < n) {
-        const uint32_t gi = a.red_flat[r];
-        beg = __ldg(a.row_ptr + gi);
-        end = __ldg(a.row_ptr + gi + 1);
-        if (a.wfp8) scale = __ldg(a.row_scale + gi);
+    const unsigned long long pf = policy_evict_first();
+    uint32_t stage = 0, eph = 1;        // the first round of empty waits passes at once
+    uint32_t filled = 0, fill_par = 0;  // lane 0: per stage (bit), closed at least once, parity of the closes
+    bool open = false;                  // lane 0: a stage is being filled
+    uint32_t cnt = 0, nseg = 0, xc = 0, wc = 0, cc = 0;
+    // lane 0 only: start filling the next stage once the consumers released it
+    auto open_stage = [&]() -> bool {
+      if (stall || !mbar_wait(&S.empty[stage], eph)) return false;
+      open = true;
+      cnt = nseg = xc = wc = cc = 0;
+      return true;
+    };
+    // lane 0 only: the stage's description, then the arrival that (with the
+    // copies' bytes) completes its phase
+    auto close_stage = [&]() {
+      S.meta[stage].n = cnt;
+      S.meta[stage].n_seg = nseg;
+      mbar_arrive(&S.full[stage]);
+      filled |= 1u << stage;
+      fill_par ^= 1u << stage;
+      open = false;
+      if (++stage == kRedStages) {
+        stage = 0;
+        eph ^= 1u;
       }
-      for (uint32_t k = 0; k < 32 && !failed; ++k) {
-        const uint32_t b = __shfl_sync(0xffffffffu, beg, k), e = __shfl_sync(0xffffffffu, end, k);
-        const float sc = __shfl_sync(0xffffffffu, scale, k);
-        if (lane == 0) {
-          ev += e - b;
-          for (uint32_t c = b; c < e; c += kRedChunk) {
-            const uint32_t ce = min(e, c + kRedChunk);
-            if (a.debug_stall || !mbar_wait(&S.empty[stage], eph)) {
-              failed = true;
-              break;
-            }
-            // byte counts of the widened copies (as bulk_elems computes them)
-            const uint32_t per_x = 16u / xsz;
-            const uint32_t xb = ((ce + per_x - 1) / per_x * per_x - (c - c % per_x)) * xsz;
-            const uint32_t wb = a.wbf16 ? ((ce + 7u) / 8u * 8u - (c - c % 8u)) * 2u
-                                : a.wfp8 ? (ce + 15u) / 16u * 16u - (c - c % 16u)
-                                         : 0u;
-            const uint32_t cb = a.code ? (ce + 15u) / 16u * 16u - (c - c % 16u) : 0u;
-            RedStage &m = S.meta[stage];
-            m.n = ce - c;
-            m.scale = sc;
-            m.w_base = (xb + 15u) & ~15u;
-            m.c_base = (m.w_base + wb + 15u) & ~15u;
-            m.x_off = c % per_x;
-            m.w_off = a.wbf16 ? c % 8u : c % 16u;
-            m.c_off = c % 16u;
-            // the stage's description is written before the arrival that
-            // (with the copies' bytes) completes its phase
-            mbar_arrive_tx(&S.full[stage], xb + wb + cb);
-            unsigned char *dst = S.buf[stage];
-            uint32_t off;
-            if (xsz == 8) bulk_elems(dst, a.edge, 8, c, ce, &S.full[stage], &off);
-            else bulk_elems(dst, a.edge_x, 4, c, ce, &S.full[stage], &off);
-            if (a.wbf16) bulk_elems(dst + m.w_base, a.w16, 2, c, ce, &S.full[stage], &off);
-            if (a.wfp8) bulk_elems(dst + m.w_base, a.w8, 1, c, ce, &S.full[stage], &off);
-            if (a.code) bulk_elems(dst + m.c_base, a.code, 1, c, ce, &S.full[stage], &off);
-            filled |= 1u << stage;
-            fill_par ^= 1u << stage;
-            if (++stage == kRedStages) {
-              stage = 0;
-              eph ^= 1u;
+    };
+    for (uint32_t i = 0; i < n_nets && !failed; ++i) {
+      const StepArgs &a = nets[i];
+      const uint32_t n = *a.red_cnt;
+      const uint32_t xsz = a.wbf16 || a.wfp8 ? 4u : 8u;  // bytes per x word or record
+      unsigned long long ev = 0;
+      for (uint32_t r0 = blockIdx.x; r0 < n && !failed; r0 += 32 * gridDim.x) {
+        const uint32_t r = r0 + lane * gridDim.x;
+        uint32_t beg = 0, end = 0;
+        float scale = 1.0f;
+        if (r < n) {
+          const uint32_t gi = a.red_flat[r];
+          beg = __ldg(a.row_ptr + gi);
+          end = __ldg(a.row_ptr + gi + 1);
+          if (a.wfp8) scale = __ldg(a.row_scale + gi);
+        }
+        for (uint32_t k = 0; k < 32 && !failed; ++k) {
+          const uint32_t b = __shfl_sync(0xffffffffu, beg, k), e = __shfl_sync(0xffffffffu, end, k);
+          const float sc = __shfl_sync(0xffffffffu, scale, k);
+          if (lane == 0) {
+            ev += e - b;
+            for (uint32_t c = b; c < e;) {
+              if (!open && !open_stage()) {
+                failed = true;
+                break;
+              }
+              const uint32_t take = min(e - c, kRedChunk - cnt);
+              unsigned char *buf = S.buf[stage];
+              RedSeg &g = S.meta[stage].seg[nseg];
+              g.first = cnt;
+              g.net = i;
+              g.scale = sc;
+              g.x = bulk_elems(buf, &xc, xsz == 8 ? (const void *)a.edge : (const void *)a.edge_x, xsz, c, c + take,
+                               &S.full[stage], pf);
+              g.w = 0;
+              if (a.wbf16) g.w = bulk_elems(buf + kRedXBytes, &wc, a.w16, 2, c, c + take, &S.full[stage], pf);
+              if (a.wfp8) g.w = bulk_elems(buf + kRedXBytes, &wc, a.w8, 1, c, c + take, &S.full[stage], pf);
+              g.c = 0;
+              if (a.code)
+                g.c = bulk_elems(buf + kRedXBytes + kRedWBytes, &cc, a.code, 1, c, c + take, &S.full[stage], pf);
+              cnt += take;
+              c += take;
+              if (++nseg == kRedSegs || cnt == kRedChunk) close_stage();
             }
           }
+          failed = __shfl_sync(0xffffffffu, failed ? 1u : 0u, 0) != 0;
         }
-        failed = __shfl_sync(0xffffffffu, failed ? 1u : 0u, 0) != 0;
       }
+      if (lane == 0 && ev) atomicAdd(&S.ev[i], ev);
     }
     if (lane == 0) {
+      if (!failed && open) close_stage();
       // end marker: the consumers leave when they reach it
-      if (!failed && !a.debug_stall && mbar_wait(&S.empty[stage], eph)) {
+      if (!failed && open_stage()) {
         S.meta[stage].n = kEmpty;
+        S.meta[stage].n_seg = 0;
         mbar_arrive(&S.full[stage]);
       } else {
-        atomicOr(a.err, 1u);
-        // the copies issued into each stage land before the block ends
-        for (uint32_t k = 0; k < kRedStages; ++k)  // the last fill's phase has parity (fills - 1) & 1
+        atomicOr(err, 1u);
+        // the copies of every closed stage land before the block ends
+        // (the last close of a stage completes the phase of parity (closes - 1) & 1)
+        for (uint32_t k = 0; k < kRedStages; ++k)
           if ((filled >> k) & 1u) (void)mbar_wait(&S.full[k], ((fill_par >> k) & 1u) ^ 1u);
       }
     }
@@ -1327,28 +1421,34 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM) scatter_red_kern
     uint32_t stage = 0, fph = 0;
     for (;;) {
       if (!mbar_wait(&S.full[stage], fph)) {
-        if (ct == 0) atomicOr(a.err, 1u);
+        if (ct == 0) atomicOr(err, 1u);
         break;
       }
-      const RedStage m = S.meta[stage];
-      if (m.n == kEmpty) break;
-      const unsigned char *src = S.buf[stage];
+      const uint32_t n = S.meta[stage].n, n_seg = S.meta[stage].n_seg;
+      if (n == kEmpty) break;
+      const unsigned char *buf = S.buf[stage];
+      const RedSeg *segs = S.meta[stage].seg;
 #pragma unroll kRedUnroll
-      for (uint32_t k = ct; k < m.n; k += kRedConsumers) {
+      for (uint32_t k = ct; k < n; k += kRedConsumers) {
+        uint32_t q = 0;  // the piece holding synapse k
+        while (q + 1 < n_seg && segs[q + 1].first <= k) ++q;
+        const RedSeg &g = segs[q];
+        const uint32_t idx = k - g.first;
+        const RedNet &r = S.nets[g.net];
         uint32_t x, wbits;
-        if (xsz == 8) {
-          const uint2 rec = reinterpret_cast<const uint2 *>(src)[m.x_off + k];
+        if (r.fmt == 0) {
+          const uint2 rec = reinterpret_cast<const uint2 *>(buf)[g.x + idx];
           x = rec.x;
           wbits = rec.y;
         } else {
-          x = reinterpret_cast<const uint32_t *>(src)[m.x_off + k];
-          if (a.wbf16) wbits = (uint32_t)reinterpret_cast<const uint16_t *>(src + m.w_base)[m.w_off + k] << 16;
-          else wbits = __float_as_uint(e4m3_to_f32(src[m.w_base + m.w_off + k]) * m.scale);
+          x = reinterpret_cast<const uint32_t *>(buf)[g.x + idx];
+          if (r.fmt == 1) wbits = (uint32_t)reinterpret_cast<const uint16_t *>(buf + kRedXBytes)[g.w + idx] << 16;
+          else wbits = __float_as_uint(e4m3_to_f32(buf[kRedXBytes + g.w + idx]) * g.scale);
         }
-        const uint8_t code = a.code ? src[m.c_base + m.c_off + k] : (uint8_t)(x >> 24);
-        uint32_t slot = base + max(code_delay(code), 1u);
-        if (slot >= a.nslots) slot -= a.nslots;
-        red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + (x & a.post_mask),
+        const uint8_t code = r.code ? buf[kRedXBytes + kRedWBytes + g.c + idx] : (uint8_t)(x >> 24);
+        uint32_t slot = r.base + max(code_delay(code), 1u);
+        if (slot >= r.nslots) slot -= r.nslots;
+        red_add(r.ring + ((size_t)code_ring(code) * r.nslots + slot) * r.Nd + (x & r.post_mask),
                 __uint_as_float(wbits), pl);
       }
       __syncwarp();
@@ -1361,36 +1461,62 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM) scatter_red_kern
   }
   __syncthreads();
   // Poisson-source synapses in runs, source order free (exact sums)
-  for (uint32_t t = blockIdx.x * kRedThreads + tid; t < a.n_src_syn; t += gridDim.x * kRedThreads) {
-    uint32_t lo = 0, hi = a.n_runs - 1;  // largest run with run_off[run] <= t
-    while (lo < hi) {
-      const uint32_t mid = lo + ((hi - lo + 1) >> 1);
-      if (__ldg(a.run_off + mid) <= t) lo = mid;
-      else hi = mid - 1;
+  for (uint32_t i = 0; i < n_nets; ++i) {
+    const StepArgs &a = nets[i];
+    const uint32_t base = S.nets[i].base;
+    unsigned long long src_ev = 0;
+    for (uint32_t t = blockIdx.x * kRedThreads + tid; t < a.n_src_syn; t += gridDim.x * kRedThreads) {
+      uint32_t lo = 0, hi = a.n_runs - 1;  // largest run with run_off[run] <= t
+      while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+        if (__ldg(a.run_off + mid) <= t) lo = mid;
+        else hi = mid - 1;
+      }
+      const uint32_t off = t - __ldg(a.run_off + lo);
+      const float p = __ldg(a.run_p + lo);
+      if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + lo) + off, 0, *a.step, p)) {
+        const uint8_t code = __ldg(a.run_code + lo);
+        uint32_t slot = base + max(code_delay(code), 1u);
+        if (slot >= a.nslots) slot -= a.nslots;
+        red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + __ldg(a.run_post0 + lo) + off,
+                __ldg(a.run_w + lo), pl);
+        ++src_ev;
+      }
     }
-    const uint32_t off = t - __ldg(a.run_off + lo);
-    const float p = __ldg(a.run_p + lo);
-    if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + lo) + off, 0, step, p)) {
-      const uint8_t code = __ldg(a.run_code + lo);
-      uint32_t slot = base + max(code_delay(code), 1u);
-      if (slot >= a.nslots) slot -= a.nslots;
-      red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + __ldg(a.run_post0 + lo) + off,
-              __ldg(a.run_w + lo), pl);
-      ++src_ev;
-    }
-  }
-  ev += src_ev;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    ev += __shfl_xor_sync(0xffffffffu, ev, o);
-    src_ev += __shfl_xor_sync(0xffffffffu, src_ev, o);
+    for (int o = 16; o > 0; o >>= 1) src_ev += __shfl_xor_sync(0xffffffffu, src_ev, o);
+    if (lane == 0 && src_ev) atomicAdd(&S.src_ev[i], src_ev);
   }
-  if (lane == 0 && ev) atomicAdd(&S.events, ev);
-  if (lane == 0 && src_ev) atomicAdd(&S.src_events, src_ev);
   __syncthreads();
-  if (tid == 0 && S.events) atomicAdd(a.ev_step, S.events);
-  if (tid == 0 && S.src_events) atomicAdd(a.ev_src_step, S.src_events);
-  end_of_step(a, n);
+  for (uint32_t i = tid; i < n_nets; i += kRedThreads) {
+    const unsigned long long e = S.ev[i] + S.src_ev[i];
+    if (e) atomicAdd(nets[i].ev_step, e);
+    if (S.src_ev[i]) atomicAdd(nets[i].ev_src_step, S.src_ev[i]);
+  }
+  // the last block to finish closes the step of every network
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const uint32_t t = atomicAdd(done, 1u);
+    if (t == gridDim.x - 1) {
+      __threadfence();
+      for (uint32_t i = 0; i < n_nets; ++i) end_of_step_last(nets[i], *nets[i].red_cnt);
+      *done = 0;
+      __threadfence();
+    }
+  }
+}
+
+// One neuron launch per model over the populations of several networks (a
+// pool): block b takes map[b] = (network, population, block within it).
+template <int MODEL, bool FULL>
+__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCfg<MODEL>::MIN_BLOCKS)
+    neuron_pool_kernel(const StepArgs *__restrict__ nets, const PopArgs *__restrict__ pops,
+                       const uint4 *__restrict__ map) {
+  const uint4 m = map[blockIdx.x];
+  pdl_wait();
+  pdl_release();
+  neuron_block<MODEL, FULL>(nets[m.x], pops[m.y], m.z);
 }
 
 // Adds the deferred drive of step t - 1 (t >= 1) of one population into

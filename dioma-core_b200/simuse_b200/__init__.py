@@ -17,6 +17,7 @@ from .network import (  # noqa: F401
     W_F32,
     W_FP8,
     Network,
+    Pool,
 )
 from .kuramoto import KuramotoBatch  # noqa: F401,E402
 from . import taas  # noqa: F401,E402

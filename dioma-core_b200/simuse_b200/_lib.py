@@ -33,6 +33,13 @@ SIGNATURES = {
     "sg_net_destroy": [vp],
     "sg_synchronize": [vp],
     "sg_debug_stall_scatter": [vp, i32],
+    "sg_pool_create": [vp, i32],
+    "sg_pool_destroy": [vp],
+    "sg_pool_add": [vp, vp],
+    "sg_pool_remove": [vp, vp],
+    "sg_pool_size": [vp, vp],
+    "sg_pool_step": [vp, u32],
+    "sg_pool_synchronize": [vp],
     "sg_query": [vp, vp],
     "sg_pop_add": [vp, i32, u32, vp],
     "sg_pop_fill_param": [vp, u32, u32, f32],
@@ -50,6 +57,7 @@ SIGNATURES = {
     "sg_poisson_add": [vp, f32, f32, u32, vp],
     "sg_poisson_add_many": [vp, u32, f32, f32, vp, u32, vp],
     "sg_poisson_connect": [vp, u32, u32, vp, vp, vp, vp, u64],
+    "sg_poisson_connect_plastic": [vp, u32, u32, vp, vp, vp, vp, vp, u64],
     "sg_poisson_connect_one_to_one": [vp, u32, u32, u32, vp, f32, u8],
     "sg_stdp_config": [vp, f32, f32, f32, f32, f32, f32, f32],
     "sg_set_weight_format": [vp, i32],

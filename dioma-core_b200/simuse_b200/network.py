@@ -26,6 +26,14 @@ def _p(a):
     return None if a is None else a.ctypes.data
 
 
+def _random_w(r) -> int:
+    """random_w of the device generators: False/True, or an int b >= 2 (U on
+    the 2^-b grid)."""
+    if isinstance(r, bool):
+        return 1 if r else 0
+    return int(r)
+
+
 class Network:
     """One simulated network resident on one GPU (one CUDA stream)."""
 
@@ -128,7 +136,7 @@ class Network:
         (sg_connect_fixed_outdegree); weights w_exc/w_inh times U(0,1);
         delay uniform in [delay, d_max] (d_max defaults to delay)."""
         check(lib().sg_connect_fixed_outdegree(self._h, frm, to, k, seed, 1 if no_self else 0, n_exc,
-                                               float(w_exc), float(w_inh), 1 if random_w else 0, delay,
+                                               float(w_exc), float(w_inh), _random_w(random_w), delay,
                                                delay if d_max is None else d_max, syn_type_exc, syn_type_inh,
                                                EDGE_STDP if stdp_exc else 0))
 
@@ -139,7 +147,7 @@ class Network:
         device (sg_connect_lognormal_outdegree)."""
         check(lib().sg_connect_lognormal_outdegree(self._h, frm, to, float(mean), float(sd), seed,
                                                    1 if no_self else 0, n_exc, float(w_exc), float(w_inh),
-                                                   1 if random_w else 0, delay, delay if d_max is None else d_max,
+                                                   _random_w(random_w), delay, delay if d_max is None else d_max,
                                                    syn_type_exc, syn_type_inh, EDGE_STDP if stdp_exc else 0))
 
     def register_expone(self, tau_decay: float, erev: float, dt: float) -> int:
@@ -168,12 +176,13 @@ class Network:
         check(lib().sg_poisson_add_many(self._h, n, rate_hz, dt_ms, _p(s), seed0, C.byref(out)))
         return out.value
 
-    def connect_poisson_source(self, src, to, posts, weights, delays, syn_types=None):
+    def connect_poisson_source(self, src, to, posts, weights, delays, syn_types=None, plast_types=None):
         p = np.ascontiguousarray(posts, np.uint32)
         w = np.ascontiguousarray(weights, np.float32)
         d = np.ascontiguousarray(delays, np.uint8)
         st = None if syn_types is None else np.ascontiguousarray(syn_types, np.uint8)
-        check(lib().sg_poisson_connect(self._h, src, to, _p(p), _p(w), _p(d), _p(st), p.size))
+        pt = None if plast_types is None else np.ascontiguousarray(plast_types, np.uint8)
+        check(lib().sg_poisson_connect_plastic(self._h, src, to, _p(p), _p(w), _p(d), _p(st), _p(pt), p.size))
 
     def connect_poisson_one_to_one(self, first_src, n, to, weight, delay, posts=None):
         p = None if posts is None else np.ascontiguousarray(posts, np.uint32)
@@ -506,3 +515,49 @@ class Network:
         out = C.c_void_p()
         check(lib().sg_stream(self._h, C.byref(out)))
         return out.value or 0
+
+
+class Pool:
+    """Networks stepped together (continuous batching): per step one neuron
+    launch per model over every member's populations and one scatter launch
+    over every member (sg_pool_*).  Members stay independent networks; each
+    gives the same bits in the pool as alone."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().sg_pool_create(C.byref(h), device))
+        self._h = h
+        self.members: list[Network] = []
+        self.device = device
+
+    def add(self, net: Network):
+        check(lib().sg_pool_add(self._h, net._h))
+        self.members.append(net)
+
+    def remove(self, net: Network):
+        check(lib().sg_pool_remove(self._h, net._h))
+        self.members.remove(net)
+
+    def step(self, n_steps: int):
+        check(lib().sg_pool_step(self._h, n_steps))
+
+    def synchronize(self):
+        check(lib().sg_pool_synchronize(self._h))
+
+    def __len__(self) -> int:
+        out = C.c_uint32()
+        check(lib().sg_pool_size(self._h, C.byref(out)))
+        return out.value
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().sg_pool_destroy(h)
+        self._h = None
+        self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,21 +1,27 @@
 """A served stream of simulation requests on one GPU.
 
 Each request names a seeded network (LIF or Izhikevich, N neurons, lognormal
-out-degree) and a number of simulation steps, and gets back its spike events
-and per-neuron firing rates.  The server keeps every admitted network's state,
-synapses and delay rings resident in HBM until it finishes, and batches
-continuously: a request that arrives while others are running is admitted
-as soon as a resident slot and enough of the memory budget are free, and its
-steps then run beside theirs, each network on its own CUDA stream, so their
-kernels overlap on the device.  Admission is by resident footprint against
-the budget (an estimate at admission, replaced by the measured footprint of
-the built network).  Latency is measured per request from submission to
-completion.
+out-degree, BF16 weights) and a number of simulation steps, and gets back its
+spike events and per-neuron firing rates.  The server keeps every admitted
+network's state, synapses and delay rings resident in HBM until it finishes,
+and batches continuously: the resident networks are members of one pool
+(sg_pool), which steps them together, per step one neuron launch per model
+over every member's populations and one scatter launch over every member.  A
+request that arrives while others are running is admitted as soon as a
+resident slot and enough of the memory budget are free: it is built on its
+own stream beside the running pool and joins the pool at the next tick;
+finished requests leave it and release their budget.  Admission is by
+resident footprint against the budget (an estimate at admission, replaced by
+the measured footprint of the built network).  Latency is measured per
+request from submission to completion.
 
 Networks do not interact, and each one's random streams (Poisson drive,
 input noise) are keyed by its own seed and its own step counter, so a
 request's result does not depend on what else is resident: the same bits
-alone and in any mix.
+alone and in any mix.  Every served network's ring sums are exact (the LIF
+weights 20, -100 and 100; the Izhikevich weights 0.5 U and -U with U on the
+1/256 grid, which BF16 also holds exactly), so they all take the pre-centric
+scatter that a pool runs.
 
 The reference has no serving layer; this is a request loop over many
 simulations, written over the same builder/step API the reference's callers use
@@ -31,7 +37,7 @@ import time
 import numpy as np
 
 from . import workloads as W
-from .network import IZH, LIF, Network
+from .network import IZH, LIF, W_BF16, Network, Pool
 
 
 @dataclasses.dataclass
@@ -64,27 +70,21 @@ class Request:
 
 def estimate_footprint(req: Request) -> int:
     """Device bytes a request holds while it is built and resident: synapse
-    records, the per-row segment table, rings, state, spike lists and the
-    build-time sort buffers (the peak), rounded up generously."""
+    records (8 B while building, then x word + BF16 weight), the per-row
+    segment table, rings, state, spike lists and the build-time buffers (the
+    peak), rounded up generously."""
     n = req.n
     nd = -(-n // 1024) * 1024
     e = int(n * req.mean_degree * 1.05)
-    per_neuron = 32 * 4 + 16 * 4 + 8 + 148 * 2 + 64   # rings (<= 32 slots), state+params, spike list, segments
-    build_peak = e * 45                                # staged edges + radix-sort double buffers + records
-    # pending-event lists of the scatter: per block and ring slot, room for
-    # the block's heaviest step (bounded generously) up to 4 windows of 8192
-    g = max(1, min(148, nd // 32))
-    p = -(-(-(-nd // g)) // 32) * 32
-    g = -(-nd // p)
-    slots = 3 if req.kind == "lif" else 2
-    lcap = min(4 * 8192, -(-int(p * req.mean_degree * 4 + p) // 256) * 256)
-    lists = g * slots * (lcap * 6 + 4)
-    return int(nd * per_neuron + build_peak + lists + (64 << 20))
+    per_neuron = 32 * 4 + 16 * 4 + 16 + 148 * 2 + 64   # rings (<= 32 slots), state+params, spike lists, segments
+    build_peak = e * 45                                # staged edges + sort buffers + records
+    return int(nd * per_neuron + build_peak + (64 << 20))
 
 
 def build_request(req: Request, device: int = 0) -> Network:
     """The request's network through the builder API (not yet built)."""
     net = Network(device)
+    net.set_weight_format(W_BF16)
     n, n_exc = req.n, req.n * 4 // 5
     if req.kind == "lif":
         pop = net.add_population(LIF, n)
@@ -107,8 +107,9 @@ def build_request(req: Request, device: int = 0) -> Network:
         net.fill_param(pop, 6, 30.0)
         net.fill_state(pop, 0, -65.0)
         net.set_state(pop, 1, (b * np.float32(-65.0)).astype(np.float32))
+        # weights 0.5 U / -U with U on the 1/256 grid: exact ring sums, exact in BF16
         net.connect_lognormal_outdegree(pop, pop, req.mean_degree, req.sd_degree, req.seed, True, n_exc,
-                                        0.5, -1.0, random_w=True, delay=1)
+                                        0.5, -1.0, random_w=8, delay=1)
         net.set_noise(pop, req.seed, 5.0, 2.0, split=n_exc, stream=W.IZH_STREAM_NOISE, stride=n)
     else:
         raise ValueError(f"unknown request kind {req.kind!r}")
@@ -148,26 +149,27 @@ def _finish(req: Request, st, ix):
 
 
 class _Resident:
-    def __init__(self, req: Request, net: Network, chunk: int):
-        self.req, self.net, self.chunk = req, net, chunk
+    def __init__(self, req: Request, net: Network):
+        self.req, self.net = req, net
         self.done = 0
-        self.k = 0
         self.st: list[np.ndarray] = []
         self.ix: list[np.ndarray] = []
-        net.enable_raster(chunk)
 
 
 class Server:
     """Continuous-batching request loop on one GPU (see the module text).
 
     budget_bytes: device memory the resident networks may hold together.
-    max_resident: resident networks at most (streams in flight).
-    chunk: steps a resident network advances per scheduling round.
+    max_resident: resident networks at most (pool members; at most 64).
+    chunk: steps the pool advances per tick (a tick is shortened to the
+    fewest steps any resident network still needs).
+    builders: threads building admitted networks beside the running pool.
     """
 
     def __init__(self, device: int = 0, budget_bytes: int = 160 * 10**9, max_resident: int = 32,
-                 chunk: int = 256):
-        self.device, self.budget, self.max_resident, self.chunk = device, int(budget_bytes), max_resident, chunk
+                 chunk: int = 250, builders: int = 2):
+        self.device, self.budget, self.chunk = device, int(budget_bytes), chunk
+        self.max_resident = min(max_resident, 64)
         self._pending: queue.Queue[Request] = queue.Queue()
         self._built: queue.Queue[tuple[Request, Network | None]] = queue.Queue()
         self._to_build: queue.Queue[Request | None] = queue.Queue()
@@ -175,12 +177,14 @@ class Server:
         self._reserved = 0            # budget bytes held by building and resident networks
         self._next_id = 0
         self.completed: list[Request] = []
+        self.ticks = 0
         self._stop = threading.Event()
         self._idle = threading.Event()
         self._n_open = 0
-        self._builder = threading.Thread(target=self._build_loop, daemon=True)
+        self._builders = [threading.Thread(target=self._build_loop, daemon=True) for _ in range(max(1, builders))]
         self._stepper = threading.Thread(target=self._step_loop, daemon=True)
-        self._builder.start()
+        for b in self._builders:
+            b.start()
         self._stepper.start()
 
     # -- client side ----------------------------------------------------------
@@ -203,9 +207,11 @@ class Server:
 
     def close(self):
         self._stop.set()
-        self._to_build.put(None)
+        for _ in self._builders:
+            self._to_build.put(None)
         self._stepper.join()
-        self._builder.join()
+        for b in self._builders:
+            b.join()
 
     def latency_percentiles(self) -> dict:
         lat = np.array([r.latency for r in self.completed if r.error is None])
@@ -237,6 +243,7 @@ class Server:
                 self._built.put((req, None))
 
     def _step_loop(self):
+        pool = Pool(self.device)
         resident: list[_Resident] = []
         building = 0
         waiting: list[Request] = []
@@ -260,7 +267,7 @@ class Server:
                 waiting.pop(0)
                 building += 1
                 self._to_build.put(req)
-            # networks that finished building join the running set
+            # networks that finished building join the pool
             while True:
                 try:
                     req, net = self._built.get_nowait()
@@ -276,38 +283,31 @@ class Server:
                 with self._lock:                  # the measured footprint replaces the estimate
                     self._reserved += true_fp - req.footprint
                 req.footprint = true_fp
-                resident.append(_Resident(req, net, self.chunk))
+                net.enable_raster(self.chunk)
+                pool.add(net)
+                resident.append(_Resident(req, net))
             if not resident:
                 time.sleep(0.0005)
                 continue
-            # every resident network advances independently: when its last
-            # chunk has finished (non-blocking query) its spikes are read back
-            # and its next chunk is queued on its own stream, so the chunks of
-            # different networks overlap on the device and a small network is
-            # never held back by a large one
-            progressed = False
+            # one tick: every resident network advances k steps in the pool,
+            # then each one's spikes of the tick are read back
+            k = min(self.chunk, min(r.req.steps - r.done for r in resident))
+            pool.step(k)
+            self.ticks += 1
             finished = []
             for r in resident:
-                if r.k and not r.net.idle():
-                    continue
-                progressed = True
-                if r.k:
-                    s, i = r.net.read_spike_events()
-                    r.st.append(s)
-                    r.ix.append(i)
-                    r.done += r.k
-                    r.k = 0
+                s, i = r.net.read_spike_events()
+                r.st.append(s)
+                r.ix.append(i)
+                r.done += k
                 if r.done >= r.req.steps:
                     finished.append(r)
-                    continue
-                r.k = min(r.chunk, r.req.steps - r.done)
-                r.net.step(r.k)
             for r in finished:
                 resident.remove(r)
+                pool.remove(r.net)
                 _finish(r.req, r.st, r.ix)
                 r.net.close()
                 with self._lock:
                     self._reserved -= r.req.footprint
                 self._complete(r.req)
-            if not progressed:
-                time.sleep(0.0002)
+        pool.close()

@@ -119,7 +119,8 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
    draw q (j = m - k + q) takes t = hi32(h) * (j + 1) >> 32, or j when t was
    drawn before, h = splitmix64(seed ^ (i*k + q)*0x9E3779B97F4A7C15); without
    self-loops t >= i maps to t + 1 (k <= 4096).  Weight w_exc for i < n_exc
-   else w_inh, times lo32(h) / 2^32 when random_w; delay d_min +
+   else w_inh, times lo32(h) / 2^32 when random_w = 1, or times the top b
+   bits of lo32(h) / 2^b (a U on the 2^-b grid) when random_w = b in 2..24; delay d_min +
    lo32(splitmix64(h)) % (d_max - d_min + 1); synapse type st_exc / st_inh and,
    for excitatory sources, flags_exc (SG_EDGE_STDP).  Edges are appended in
    (source, draw) order.  The generator of the Izhikevich pulse network
@@ -176,6 +177,13 @@ int sg_poisson_add_many(sg_net *net, uint32_t n, float rate_hz, float dt_ms,
 int sg_poisson_connect(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts,
                        const float *weights, const uint8_t *delays, const uint8_t *syn_types,
                        uint64_t n);
+/* As sg_poisson_connect, each synapse with a Tsodyks-Markram profile
+   (plast_types[i], 0 none; registered with sg_register_plasticity): the
+   delivered weight is scaled by the synapse's own R and U at each source
+   spike (P/api/net/network/step.rs:166-180, core.rs:323-380). */
+int sg_poisson_connect_plastic(sg_net *net, uint32_t src, uint32_t to, const uint32_t *posts,
+                               const float *w, const uint8_t *delays, const uint8_t *syn_types,
+                               const uint8_t *plast_types, uint64_t n);
 /* Source first_src + i gets one synapse to post posts[i] (posts == NULL:
    post i), weight w, delay d: the "one source per neuron" drive. */
 int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first_src, uint32_t n, uint32_t to,
@@ -413,6 +421,29 @@ int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *we
 int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
                            const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
                            uint32_t n_active, uint64_t step, float *ring, void *stream);
+
+/* ---- pools of resident networks (continuous batching) ----------------------
+   No counterpart in the reference (its callers step one Network at a time;
+   dioma-engine's pooled dynamics, dioma-engine/src/brain/dynamics/gpu_pool.rs,
+   steps many creatures' networks as one).  A pool steps its member networks
+   together: per step one neuron launch per model over every member's
+   populations and one scatter launch over every member, on the pool's own
+   stream.  Members stay independent networks (own state, synapses, rings,
+   step counter, readbacks on their own stream); each gives the same bits in a
+   pool as alone.  Members must be built, on the pool's device, on the
+   pre-centric scatter (sg_scatter_mode EXACT or ATOMIC), without learning or
+   external populations; at most 64.  sg_pool_step orders itself after the
+   work queued on every member's stream and every member's later work after
+   it.  A network leaves its pool when removed or destroyed. */
+typedef struct sg_pool sg_pool;
+int sg_pool_create(sg_pool **out, int device);
+int sg_pool_destroy(sg_pool *pool);
+int sg_pool_add(sg_pool *pool, sg_net *net);
+int sg_pool_remove(sg_pool *pool, sg_net *net);
+int sg_pool_size(sg_pool *pool, uint32_t *out);
+int sg_pool_step(sg_pool *pool, uint32_t n_steps);
+/* Waits for the pool's stream; SG_E_CUDA if a scatter wait timed out. */
+int sg_pool_synchronize(sg_pool *pool);
 
 /* ---- batched Kuramoto populations ----------------------------------------- */
 /* A batch of independent all-to-all Kuramoto populations integrated by RK4:

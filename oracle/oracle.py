@@ -81,6 +81,7 @@ def lib():
             "or_learn_read": (i32, [vp, vp, vp, vp, vp]),
             "or_poisson_add": (i32, [vp, f32, f32, u32]),
             "or_poisson_connect": (i32, [vp, i32, i32, vp, vp, vp, vp, u64]),
+            "or_poisson_connect_plastic": (i32, [vp, i32, i32, vp, vp, vp, vp, vp, u64]),
             "or_poisson_add_many": (i32, [vp, u32, f32, f32, u32]),
             "or_poisson_connect_one_to_one": (i32, [vp, i32, u32, i32, f32, C.c_uint8]),
             "or_stdp_config": (i32, [vp, f32, f32, f32, f32, f32, f32, f32]),
@@ -295,12 +296,13 @@ class Network:
             return
         _chk(lib().or_poisson_connect_one_to_one(self._h, first_src, n, to, weight, delay))
 
-    def connect_poisson_source(self, src, to, posts, weights, delays, syn_types=None):
+    def connect_poisson_source(self, src, to, posts, weights, delays, syn_types=None, plast_types=None):
         p = np.ascontiguousarray(posts, np.uint32)
         w = np.ascontiguousarray(weights, np.float32)
         d = np.ascontiguousarray(delays, np.uint8)
         st = None if syn_types is None else np.ascontiguousarray(syn_types, np.uint8)
-        _chk(lib().or_poisson_connect(self._h, src, to, _p(p), _p(w), _p(d), _p(st), p.size))
+        pt = None if plast_types is None else np.ascontiguousarray(plast_types, np.uint8)
+        _chk(lib().or_poisson_connect_plastic(self._h, src, to, _p(p), _p(w), _p(d), _p(st), _p(pt), p.size))
 
     def stdp_config(self, dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max):
         _chk(lib().or_stdp_config(self._h, dt, tau_pre, tau_post, a_plus, a_minus, w_min, w_max))

@@ -475,6 +475,11 @@ template <typename T> struct Src {
   std::vector<uint32_t> post;
   std::vector<T> w;
   std::vector<uint8_t> d, st;
+  // Tsodyks-Markram profile per outgoing synapse (0 none) and its state
+  // R, U, last spike step (P/api/net/network/sources.rs:20-31, core.rs:372-378)
+  std::vector<uint8_t> pt;
+  std::vector<float> r, u;
+  std::vector<uint32_t> last;
 };
 
 struct Stdp {
@@ -789,7 +794,12 @@ template <typename T> void net_step_end(Net<T> &net) {
   // 5b. Poisson sources (step.rs:163-185)
   for (auto &src : net.srcs) {
     if (src.p <= 0.0f || !poisson_spike(src.seed, 0, s, src.p)) continue;
-    for (size_t i = 0; i < src.post.size(); ++i) deliver(src.post[i], src.d[i], src.st[i], src.w[i]);
+    for (size_t i = 0; i < src.post.size(); ++i) {
+      T w = src.w[i];
+      if (src.pt[i])  // step.rs:172-177: the synapse's short-term plasticity scales the weight
+        w = (T)tm_spike(net.tm[src.pt[i] - 1], src.r[i], src.u[i], src.last[i], (float)src.w[i], s);
+      deliver(src.post[i], src.d[i], src.st[i], w);
+    }
     net.events += src.post.size();
   }
   // Pair STDP with immediate weight updates (oracle-defined; trace order
@@ -1420,8 +1430,11 @@ int or_poisson_add_many(or_net *h, uint32_t n, float rate_hz, float dt_ms, uint3
 }
 
 // P/api/net/network/core.rs:323-381
-int or_poisson_connect(or_net *h, int src, int to, const uint32_t *posts, const float *w,
-                       const uint8_t *dl, const uint8_t *st, uint64_t n) {
+// Network::connect_poisson_source (core.rs:323-380), with the synapses'
+// plasticity profiles (plast_types; NULL = none): R = 1, U = U0 of the profile
+// registered when the synapse is connected, last = 0.
+int or_poisson_connect_plastic(or_net *h, int src, int to, const uint32_t *posts, const float *w,
+                               const uint8_t *dl, const uint8_t *st, const uint8_t *pt, uint64_t n) {
   DISPATCH(h, {
     if (net.built) return fail("Cannot connect after build()");
     if (src < 0 || (size_t)src >= net.srcs.size()) return fail("poisson source out of range");
@@ -1433,13 +1446,24 @@ int or_poisson_connect(or_net *h, int src, int to, const uint32_t *posts, const 
       if (posts[i] >= tc) return fail("post index out of bounds");
       if (!std::isfinite(w[i])) return fail("connect_poisson_source: weight must be finite");
       if (dl[i] >= kSlots) return fail("connect_poisson_source: delay >= MAX_DELAY_SLOTS");
+      const uint8_t p = pt ? pt[i] : 0;
+      if (p > net.tm.size()) return fail("plasticity profile out of range");
       s.post.push_back(tof + posts[i]);
       s.w.push_back(w[i]);
       s.d.push_back(dl[i]);
       s.st.push_back(st ? st[i] : 0);
+      s.pt.push_back(p);
+      s.r.push_back(1.0f);
+      s.u.push_back(p ? net.tm[p - 1].u0 : 0.0f);
+      s.last.push_back(0u);
     }
   });
   return 0;
+}
+
+int or_poisson_connect(or_net *h, int src, int to, const uint32_t *posts, const float *w,
+                       const uint8_t *dl, const uint8_t *st, uint64_t n) {
+  return or_poisson_connect_plastic(h, src, to, posts, w, dl, st, nullptr, n);
 }
 
 int or_poisson_connect_one_to_one(or_net *h, int first, uint32_t n, int to, float w, uint8_t dl) {

@@ -81,6 +81,9 @@ int or_poisson_connect_one_to_one(or_net *net, int first, uint32_t n, int to, fl
 int or_poisson_connect(or_net *net, int src, int to, const uint32_t *posts,
                        const float *w, const uint8_t *delay,
                        const uint8_t *syn_type, uint64_t n);
+int or_poisson_connect_plastic(or_net *net, int src, int to, const uint32_t *posts, const float *w,
+                               const uint8_t *delay, const uint8_t *syn_type, const uint8_t *plast_type,
+                               uint64_t n);
 int or_stdp_config(or_net *net, float dt, float tau_pre, float tau_post,
                    float a_plus, float a_minus, float w_min, float w_max);
 int or_build(or_net *net);
