@@ -107,10 +107,14 @@ struct HostPop {
 struct HostSrc {
   float p;
   uint32_t seed;
-  std::vector<uint32_t> post;  // device indices
-  std::vector<float> w;
-  std::vector<uint8_t> code;
-  std::vector<uint8_t> pt;     // Tsodyks-Markram profile per synapse (0 none)
+};
+// One Poisson-source synapse (all of them in one list, in connect order)
+struct SrcSyn {
+  uint32_t src;
+  uint32_t post;  // device index
+  float w;
+  uint8_t code;
+  uint8_t pt;     // Tsodyks-Markram profile (0 none)
 };
 
 // A kinetic synapse profile's per-step constants (P/api/net/network/step.rs:
@@ -151,6 +155,7 @@ struct sg_net {
   DVec<uint8_t> e_code;
   std::vector<Kin> kin;
   std::vector<HostSrc> srcs;
+  std::vector<SrcSyn> src_syn;
   bool stdp_on = false;
   float stdp_dt = 0, tau_pre = 0, tau_post = 0, a_plus = 0, a_minus = 0, w_min = 0, w_max = 0;
   int deterministic = 1;
@@ -977,6 +982,20 @@ void build_sources(sg_net *net) {
   const uint32_t G = net->G, P = net->P;
   std::vector<float> p(S);
   std::vector<uint32_t> seed(S);
+  for (size_t i = 0; i < S; ++i) {
+    p[i] = net->srcs[i].p;
+    seed[i] = net->srcs[i].seed;
+  }
+  // the source synapses in the reference's order: source ascending, then
+  // connect order (a counting sort by source, stable)
+  const std::vector<SrcSyn> &syn = net->src_syn;
+  std::vector<uint32_t> ord(syn.size());
+  {
+    std::vector<uint64_t> start(S + 1, 0);
+    for (const SrcSyn &y : syn) start[y.src + 1]++;
+    for (size_t i = 0; i < S; ++i) start[i + 1] += start[i];
+    for (size_t k = 0; k < syn.size(); ++k) ord[start[syn[k].src]++] = (uint32_t)k;
+  }
   std::vector<uint64_t> cnt((size_t)G + 1, 0);
   uint64_t tot = 0;
   // the source weights' part of the exact-sum test (rings_exact)
@@ -984,43 +1003,35 @@ void build_sources(sg_net *net) {
   net->src_lo = 1 << 20;
   net->src_bad = false;
   std::vector<uint8_t> deferred;
-  if (S) {
+  if (!syn.empty()) {
     std::vector<uint32_t> post_cnt(net->Nd, 0), post_src(net->Nd, 0);
     std::vector<float> post_w(net->Nd, 0.0f);
     std::vector<uint8_t> post_code(net->Nd, 0), post_pt(net->Nd, 0);
-    for (size_t i = 0; i < S; ++i)
-      for (size_t k = 0; k < net->srcs[i].post.size(); ++k) {
-        const uint32_t q = net->srcs[i].post[k];
-        post_cnt[q]++;
-        post_src[q] = (uint32_t)i;
-        post_w[q] = net->srcs[i].w[k];
-        post_code[q] = net->srcs[i].code[k];
-        post_pt[q] = net->srcs[i].pt[k];
-      }
+    for (const SrcSyn &y : syn) {
+      post_cnt[y.post]++;
+      post_src[y.post] = y.src;
+      post_w[y.post] = y.w;
+      post_code[y.post] = y.code;
+      post_pt[y.post] = y.pt;
+    }
     deferred.assign(net->Nd, 0);
     find_deferred_drive(net, post_cnt, post_src, post_w, post_code, post_pt, deferred);
   } else {
     net->any_drv = false;
     for (auto &pop : net->pops) pop.drv = false;
   }
-  for (size_t i = 0; i < S; ++i) {
-    p[i] = net->srcs[i].p;
-    seed[i] = net->srcs[i].seed;
-    for (size_t k = 0; k < net->srcs[i].post.size(); ++k) {
-      const uint32_t q = net->srcs[i].post[k];
-      const float w = net->srcs[i].w[k];
-      uint32_t bits;
-      std::memcpy(&bits, &w, 4);
-      if (!std::isfinite(w)) {
-        net->src_bad = true;
-      } else if (bits & 0x7FFFFFFFu) {
-        net->src_lo = std::min(net->src_lo, low_exponent(bits));
-        net->src_abs[q] += std::fabs((double)w);
-      }
-      if (deferred[q]) continue;  // taken by the neuron kernel
-      cnt[q / P]++;
-      tot++;
+  for (const SrcSyn &y : syn) {
+    uint32_t bits;
+    std::memcpy(&bits, &y.w, 4);
+    if (!std::isfinite(y.w)) {
+      net->src_bad = true;
+    } else if (bits & 0x7FFFFFFFu) {
+      net->src_lo = std::min(net->src_lo, low_exponent(bits));
+      net->src_abs[y.post] += std::fabs((double)y.w);
     }
+    if (deferred[y.post]) continue;  // taken by the neuron kernel
+    cnt[y.post / P]++;
+    tot++;
   }
   SG_REQUIRE(tot < 0xFFFFFFFFull, SG_E_OVERFLOW, "too many Poisson-source synapses");
   std::vector<uint32_t> lo((size_t)G + 1, 0);
@@ -1028,17 +1039,15 @@ void build_sources(sg_net *net) {
   std::vector<uint32_t> cur(lo.begin(), lo.end() - 1), se_src(tot), se_post(tot);
   std::vector<float> se_w(tot);
   std::vector<uint8_t> se_code(tot), se_pt(tot, 0);
-  for (size_t i = 0; i < S; ++i) {
-    const auto &sr = net->srcs[i];
-    for (size_t k = 0; k < sr.post.size(); ++k) {
-      if (deferred[sr.post[k]]) continue;
-      const uint32_t pos = cur[sr.post[k] / P]++;
-      se_src[pos] = (uint32_t)i;
-      se_post[pos] = sr.post[k];
-      se_w[pos] = sr.w[k];
-      se_code[pos] = sr.code[k];
-      se_pt[pos] = sr.pt[k];
-    }
+  for (uint32_t k : ord) {
+    const SrcSyn &y = syn[k];
+    if (deferred[y.post]) continue;
+    const uint32_t pos = cur[y.post / P]++;
+    se_src[pos] = y.src;
+    se_post[pos] = y.post;
+    se_w[pos] = y.w;
+    se_code[pos] = y.code;
+    se_pt[pos] = y.pt;
   }
   // run-length encoding per block (runs never cross blocks; <= 2^20 long)
   std::vector<uint32_t> run_lo((size_t)G + 1, 0), r_src0, r_post0, r_len, r_seed0;
@@ -1100,12 +1109,7 @@ void build_sources(sg_net *net) {
     net->d_src_tm_last.zero(net->stream);
   }
   SG_CUDA(cudaStreamSynchronize(net->stream));
-  for (auto &sr : net->srcs) {  // host copies are no longer needed
-    std::vector<uint32_t>().swap(sr.post);
-    std::vector<float>().swap(sr.w);
-    std::vector<uint8_t>().swap(sr.code);
-    std::vector<uint8_t>().swap(sr.pt);
-  }
+  std::vector<SrcSyn>().swap(net->src_syn);  // the host copy is no longer needed
 }
 
 // In-edges per post (CSC over the CSR records): in_ptr [Nd+1], and per
@@ -2298,7 +2302,6 @@ int sg_poisson_connect_plastic(sg_net *net, uint32_t src, uint32_t to, const uin
     require_local(net, to);
     SG_REQUIRE(n == 0 || (posts && w && d), SG_E_INVALID, "null slice");
     const auto &pt = net->pops[to];
-    auto &s = net->srcs[src];
     for (uint64_t i = 0; i < n; ++i) {
       SG_REQUIRE(posts[i] < pt.n, SG_E_INVALID, "post index out of bounds");
       SG_REQUIRE(std::isfinite(w[i]), SG_E_INVALID, "connect_poisson_source: weight must be finite");
@@ -2309,12 +2312,11 @@ int sg_poisson_connect_plastic(sg_net *net, uint32_t src, uint32_t to, const uin
       SG_REQUIRE(q <= net->tm_prof.size(), SG_E_INVALID,
                  "plasticity profile " + std::to_string(q) + " is not registered");
     }
+    net->src_syn.reserve(net->src_syn.size() + n);
     for (uint64_t i = 0; i < n; ++i) {
       net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
-      s.post.push_back(pt.dev_off + posts[i]);
-      s.w.push_back(w[i]);
-      s.code.push_back(edge_code(d[i], st ? st[i] : 0, false));
-      s.pt.push_back(plast ? plast[i] : 0);
+      net->src_syn.push_back(SrcSyn{src, pt.dev_off + posts[i], w[i], edge_code(d[i], st ? st[i] : 0, false),
+                                    (uint8_t)(plast ? plast[i] : 0)});
     }
   });
 }
@@ -2335,15 +2337,14 @@ int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint3
     SG_REQUIRE(delay < kSlots, SG_E_INVALID, "delay >= MAX_DELAY_SLOTS (32)");
     if (n) net->max_delay = std::max<uint32_t>(net->max_delay, delay);
     const auto &pt = net->pops[to];
-    for (uint32_t i = 0; i < n; ++i) {
-      const uint32_t q = posts ? posts[i] : i;
-      SG_REQUIRE(q < pt.n, SG_E_INVALID, "post index out of bounds");
-      auto &s = net->srcs[first + i];
-      s.post.push_back(pt.dev_off + q);
-      s.w.push_back(weight);
-      s.code.push_back(edge_code(delay, 0, false));
-      s.pt.push_back(0);
-    }
+    if (posts)
+      for (uint32_t i = 0; i < n; ++i) SG_REQUIRE(posts[i] < pt.n, SG_E_INVALID, "post index out of bounds");
+    else
+      SG_REQUIRE(n <= pt.n, SG_E_INVALID, "post index out of bounds");
+    const uint8_t code = edge_code(delay, 0, false);
+    net->src_syn.reserve(net->src_syn.size() + n);
+    for (uint32_t i = 0; i < n; ++i)
+      net->src_syn.push_back(SrcSyn{first + i, pt.dev_off + (posts ? posts[i] : i), weight, code, 0});
   });
 }
 
@@ -2401,7 +2402,7 @@ int sg_build(sg_net *net) {
     net->ln_consts = {sg_logf(10.0f / 140.0f), sg_logf(5.0f / 140.0f)};
     const uint64_t E = net->e_pre.n;
     uint64_t src_e = 0;
-    for (auto &s : net->srcs) src_e += s.post.size();
+    src_e = net->src_syn.size();
     SG_REQUIRE(E + src_e < 0xFFFFFFFFull, SG_E_OVERFLOW,
                "SparseGraph: too many synapses for a u32 CSR row_ptr / event key");
     build_graph(net);

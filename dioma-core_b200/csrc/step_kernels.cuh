@@ -241,7 +241,8 @@ __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 // is visible (a no-op for a kernel launched without the attribute); every
 // kernel calls it before it touches data an earlier kernel of the step wrote.
 // pdl_release() lets the next kernel launch (its blocks then run up to their
-// own pdl_wait()).
+// own pdl_wait()); the kernels call it when their main work is done, so that
+// the next kernel's launch overlaps their tail.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
@@ -628,13 +629,13 @@ template <int MODEL, bool FULL>
 __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCfg<MODEL>::MIN_BLOCKS)
     neuron_kernel(StepArgs a, PopArgs p0, const PopArgs *__restrict__ pops, const uint2 *__restrict__ map) {
   pdl_wait();
-  pdl_release();
   if (map == nullptr) {
     neuron_block<MODEL, FULL>(a, p0, blockIdx.x);
-    return;
+  } else {
+    const uint2 bm = map[blockIdx.x];
+    neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y);
   }
-  const uint2 bm = map[blockIdx.x];
-  neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y);
+  pdl_release();
 }
 
 // ---------------------------------------------------------------------------
@@ -846,7 +847,6 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   const uint32_t j = blockIdx.x;
   const uint32_t p0 = j * a.P;
   pdl_wait();
-  pdl_release();
   const unsigned long long step = *a.step;
   const uint32_t base = (uint32_t)(step % a.nslots);
   const uint32_t G1 = a.G + 1;
@@ -1139,6 +1139,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
     if (S.src_events) atomicAdd(a.ev_src_step, S.src_events);
     if (a.stdp && S.drift != 0.0) atomicAdd(a.drift, S.drift);
   }
+  pdl_release();
   end_of_step(a, n_spikes);
 }
 
@@ -1305,7 +1306,6 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   pdl_wait();
-  pdl_release();
   for (uint32_t i = tid; i < n_nets; i += kRedThreads) {
     const StepArgs &a = nets[i];
     RedNet r;
@@ -1460,6 +1460,7 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
     }
   }
   __syncthreads();
+  pdl_release();
   // Poisson-source synapses in runs, source order free (exact sums)
   for (uint32_t i = 0; i < n_nets; ++i) {
     const StepArgs &a = nets[i];
@@ -1515,8 +1516,8 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCf
                        const uint4 *__restrict__ map) {
   const uint4 m = map[blockIdx.x];
   pdl_wait();
-  pdl_release();
   neuron_block<MODEL, FULL>(nets[m.x], pops[m.y], m.z);
+  pdl_release();
 }
 
 // Adds the deferred drive of step t - 1 (t >= 1) of one population into

@@ -33,6 +33,7 @@ import dataclasses
 import queue
 import threading
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -167,7 +168,7 @@ class Server:
     """
 
     def __init__(self, device: int = 0, budget_bytes: int = 160 * 10**9, max_resident: int = 32,
-                 chunk: int = 250, builders: int = 2):
+                 chunk: int = 250, builders: int = 2, readers: int = 8):
         self.device, self.budget, self.chunk = device, int(budget_bytes), chunk
         self.max_resident = min(max_resident, 64)
         self._pending: queue.Queue[Request] = queue.Queue()
@@ -181,11 +182,18 @@ class Server:
         self._stop = threading.Event()
         self._idle = threading.Event()
         self._n_open = 0
+        # the networks' spikes of a tick are read back in parallel (each on its
+        # own stream); a finished request's results are assembled off the
+        # stepping thread
+        self._readers = ThreadPoolExecutor(max_workers=max(1, readers))
+        self._finishing: queue.Queue = queue.Queue()
         self._builders = [threading.Thread(target=self._build_loop, daemon=True) for _ in range(max(1, builders))]
         self._stepper = threading.Thread(target=self._step_loop, daemon=True)
+        self._finisher = threading.Thread(target=self._finish_loop, daemon=True)
         for b in self._builders:
             b.start()
         self._stepper.start()
+        self._finisher.start()
 
     # -- client side ----------------------------------------------------------
     def submit(self, req: Request) -> Request:
@@ -212,6 +220,9 @@ class Server:
         self._stepper.join()
         for b in self._builders:
             b.join()
+        self._finishing.put(None)
+        self._finisher.join()
+        self._readers.shutdown()
 
     def latency_percentiles(self) -> dict:
         lat = np.array([r.latency for r in self.completed if r.error is None])
@@ -227,6 +238,15 @@ class Server:
             self._n_open -= 1
             if self._n_open == 0:
                 self._idle.set()
+
+    def _finish_loop(self):
+        while True:
+            item = self._finishing.get()
+            if item is None:
+                return
+            r = item
+            _finish(r.req, r.st, r.ix)
+            self._complete(r.req)
 
     def _build_loop(self):
         while True:
@@ -294,20 +314,15 @@ class Server:
             k = min(self.chunk, min(r.req.steps - r.done for r in resident))
             pool.step(k)
             self.ticks += 1
-            finished = []
-            for r in resident:
-                s, i = r.net.read_spike_events()
+            for r, (s, i) in zip(resident, self._readers.map(lambda r: r.net.read_spike_events(), resident)):
                 r.st.append(s)
                 r.ix.append(i)
                 r.done += k
-                if r.done >= r.req.steps:
-                    finished.append(r)
-            for r in finished:
+            for r in [r for r in resident if r.done >= r.req.steps]:
                 resident.remove(r)
                 pool.remove(r.net)
-                _finish(r.req, r.st, r.ix)
                 r.net.close()
                 with self._lock:
                     self._reserved -= r.req.footprint
-                self._complete(r.req)
+                self._finishing.put(r)
         pool.close()
