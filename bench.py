@@ -31,6 +31,9 @@ Reported, one JSON line on rank 0:
           5..200 requests/s through the continuous-batching server (pooled
           steps): served sims/s, p50/p99 latency, against the one-at-a-time
           loop on the same arrivals.
+  sweep     (extra key) 1024 Kuramoto populations and 1024 Izhikevich
+          networks (BF16) advancing concurrently: each half alone, both
+          together, fixed against autotuned scatter schedule.
   precision_paths, hh_stdp_100k, kuramoto_sweep, lif_learn  (extra keys)
           BF16 / FP8 / ordered-path runs of the headline network, the 100k HH
           + STDP network, the Kuramoto sweep and learning.
@@ -82,10 +85,12 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--case", default="headline", choices=["headline", "kuramoto-sweep", "izh-batch", "hh-stdp",
-                                                           "lif-learn", "taas"],
+                                                           "lif-learn", "taas", "sweep"],
                     help="headline: the JSON line above; the others time one workload alone (also the "
                          "profiling entry points)")
-    ap.add_argument("--instances", type=int, default=1024)
+    ap.add_argument("--instances", type=int, default=1024,
+                    help="instances of the kuramoto-sweep and izh-batch cases; the sweep case takes half of "
+                         "each kind (2048: the 1024 + 1024 configuration)")
     ap.add_argument("--hh-wmax", type=float, default=0.01,
                     help="hh-stdp weights U(0, w_max) (raw conductance per synapse): the stated 0.5 "
                          "silences the network after its onset volley, 0.01 keeps it firing irregularly")
@@ -278,8 +283,7 @@ def run_batched(args, local):
     import simuse_b200 as sg
     from simuse_b200 import workloads as W
     K, steps = args.batch_instances, 1000
-    u = W.uniform01(7, 1, np.arange(K, dtype=np.uint64))
-    sizes = np.floor(np.exp(np.log(500) + u * (np.log(200001) - np.log(500)))).astype(int)
+    sizes = W.izh_sweep_sizes(K)
 
     def timed(net, n_steps):
         st = torch.cuda.ExternalStream(net.stream, device=local)
@@ -478,6 +482,70 @@ def run_kuramoto(args, local):
     return out
 
 
+def run_sweep(args, local, n_each: int = 1024, izh_steps: int = 1000, kura_steps: int = 10_000):
+    """The batched uneven sweep: n_each Kuramoto populations (N log-uniform
+    256..65,536, K linear 0..4, omega Lorentzian(0, 0.5), RK4 at dt 0.01,
+    kura_steps steps) and n_each Izhikevich pulse networks (N log-uniform
+    500..200,000, BF16 weights on the 1/256 grid, device thalamic noise,
+    izh_steps steps of 1 ms) advancing concurrently on two streams.  Timed
+    on the device: each half alone, both together, on the fixed scatter
+    schedule and again after the autotuner picked one."""
+    import torch
+
+    import simuse_b200 as sg
+    t0 = time.perf_counter()
+    sw = sg.Sweep.configured(n_each, n_each, device=local)
+    build_s = time.perf_counter() - t0
+    ks, ns = (torch.cuda.ExternalStream(h, device=local) for h in sw.streams)
+    sw.run(64, 20)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def timed(izh, kura):
+        e0, ei, ek, e1 = ev(), ev(), ev(), ev()
+        e0.record(ns)
+        ks.wait_event(e0)
+        ev0 = sw.events_total
+        sw.enqueue(0, kura)
+        ek.record(ks)
+        sw.enqueue(izh, 0)
+        ei.record(ns)
+        ns.wait_event(ek)
+        e1.record(ns)
+        e1.synchronize()
+        return {"total_ms": e0.elapsed_time(e1), "izh_ms": e0.elapsed_time(ei) if izh else 0.0,
+                "kura_ms": e0.elapsed_time(ek) if kura else 0.0, "izh_events": sw.events_total - ev0}
+
+    def schedule():
+        kura_alone = timed(0, kura_steps)
+        izh_alone = timed(izh_steps, 0)
+        both = timed(izh_steps, kura_steps)
+        return {"izh_alone_ms": izh_alone["izh_ms"], "kura_alone_ms": kura_alone["kura_ms"],
+                "sequential_ms": izh_alone["izh_ms"] + kura_alone["kura_ms"],
+                "concurrent_ms": both["total_ms"], "izh_ms_in_concurrent": both["izh_ms"],
+                "kura_ms_in_concurrent": both["kura_ms"],
+                "izh_events_per_s_alone": izh_alone["izh_events"] / (izh_alone["izh_ms"] / 1e3),
+                "izh_neuron_updates_per_s_alone": sw.neurons * izh_steps / (izh_alone["izh_ms"] / 1e3),
+                "kura_oscillator_steps_per_s_alone": sw.oscillators * kura_steps / (kura_alone["kura_ms"] / 1e3),
+                "instance_steps_per_s_concurrent": n_each * (izh_steps + kura_steps) / (both["total_ms"] / 1e3)}
+
+    fixed = schedule()
+    tune = sw.net.autotune(steps=100)
+    tuned = schedule()
+    rates = sw.izh_rates()
+    out = {"workload": f"{n_each} Kuramoto populations ({sw.oscillators} oscillators, N log-uniform 256..65536, K "
+                       f"0..4, RK4 dt 0.01, {kura_steps} steps) + {n_each} Izhikevich pulse networks "
+                       f"({sw.neurons} neurons, N log-uniform 500..200000, 100 targets each, BF16 weights on the "
+                       f"1/256 grid, {izh_steps} steps of 1 ms), concurrently on two streams",
+           "build_s": build_s, "synapses": sw.net.num_synapses, "footprint_gb": sw.footprint / 1e9,
+           "scatter": sw.net.scatter_mode, "weights": "bf16", "izh_rate_hz_mean": float(rates.mean()),
+           "fixed": fixed, "autotune": tune, "tuned": tuned,
+           "tuned_vs_fixed_izh": fixed["izh_alone_ms"] / tuned["izh_alone_ms"]}
+    sw.close()
+    return out
+
+
 def run_learn_short(args, local):
     """The headline network with dopamine learning on its 1e9 synapses: 200
     steps timed with learning after 300 learning steps, and one reward."""
@@ -648,7 +716,7 @@ def run_ours(args):
     if not args.no_extras and world == 1:
         for key, fn in (("precision_paths", run_precision_paths), ("hh_stdp_100k", run_hh_prefix),
                         ("kuramoto_sweep", run_kuramoto), ("lif_learn", run_learn_short),
-                        ("batched", run_batched), ("serving", run_serving)):
+                        ("batched", run_batched), ("sweep", run_sweep), ("serving", run_serving)):
             try:
                 out[key] = fn(args, local)
             except Exception as e:  # an extra measurement never takes the headline line down
@@ -742,6 +810,10 @@ def run_case(args):
         return
     if args.case == "lif-learn":
         run_lif_learn(args, local)
+        return
+    if args.case == "sweep":
+        print(json.dumps({"case": args.case, **run_sweep(args, local, n_each=args.instances // 2 or 1)}),
+              flush=True)
         return
     if args.case == "taas":
         run_taas(args, local)

@@ -43,6 +43,11 @@ __host__ __device__ inline uint64_t align_up(uint64_t x, uint64_t a) { return (x
 __host__ __device__ inline uint8_t edge_code(uint8_t delay, uint8_t syn_type, bool stdp) {
   return (uint8_t)((delay & 31u) | ((syn_type & 3u) << 5) | (stdp ? 0x80u : 0u));
 }
+// Receptor kinetics: an edge's code holds 1 + its receptor code (codes >= 7
+// are AMPA, 0) in the delay field, so that its event lands in ring slot 1 + r.
+__host__ __device__ inline uint8_t receptor_code(uint8_t receptor) {
+  return edge_code((uint8_t)(1u + (receptor < 7u ? receptor : 0u)), 0, false);
+}
 __host__ __device__ inline uint32_t code_delay(uint8_t c) { return c & 31u; }
 __host__ __device__ inline uint32_t code_ring(uint8_t c) { return (c >> 5) & 3u; }
 __host__ __device__ inline bool code_stdp(uint8_t c) { return (c & 0x80u) != 0; }

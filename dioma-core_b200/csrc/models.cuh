@@ -104,6 +104,28 @@ __device__ __forceinline__ float fast_exp(float x) {
   return __int_as_float((n + 127) << 23) * poly;
 }
 
+// Receptor kinetics of SynapticBrain (pillars-connectome/src/synaptic.rs):
+// receptor codes 0 AMPA, 1 NMDA, 2 GABA_A, 3 GABA_B, 4 nAChR, 5 GluCl,
+// 6 mAChR (any other code is AMPA, P/kernels/synapse/receptor.rs:103-115),
+// decay time constants (ms) and reversal potentials (mV) of :71-100.
+constexpr int kReceptors = 7;
+__host__ __device__ constexpr float rec_tau(int r) {
+  return r == 0 ? 2.0f : r == 1 ? 50.0f : r == 2 ? 10.0f : r == 3 ? 200.0f : r == 4 ? 3.0f : r == 5 ? 5.0f : 150.0f;
+}
+__host__ __device__ constexpr float rec_erev(int r) {
+  return r == 2 ? -65.0f : (r == 3 || r == 6) ? -90.0f : r == 5 ? -70.0f : 0.0f;
+}
+
+// P/kernels/synapse/receptor.rs:126-131 nmda_mg_block(v) =
+// 1 / (1 + 0.33 fast_exp(clamp(-0.06 v, -10, 10))); the SIMD form of :135-143
+// gives the same bits.  Correctly rounded division.
+__device__ __forceinline__ float nmda_mg_block(float v) {
+  float a = -0.06f * v;
+  a = a < -10.0f ? -10.0f : a;
+  a = a > 10.0f ? 10.0f : a;
+  return __fdiv_rn(1.0f, 1.0f + 0.33f * fast_exp(a));
+}
+
 // Exponential for the HH rates: Cody-Waite reduction by ln 2 (split in a
 // short high part and a low correction), degree-7 Taylor polynomial of e^r
 // on |r| <= ln2/2, and 2^k applied as two exact power-of-two factors.  The

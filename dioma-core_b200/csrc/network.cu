@@ -154,6 +154,11 @@ struct sg_net {
   DVec<float> e_w;
   DVec<uint8_t> e_code;
   std::vector<Kin> kin;
+  // receptor kinetics (SynapticBrain): the edges' syn_types are receptor
+  // codes, ring slot 0 is the external input and slot 1 + r the conductance
+  // of receptor r, decayed by rec_f[r] = fast_exp(-dt / tau_r) each step
+  bool receptor = false;
+  float rec_f[kReceptors] = {};
   std::vector<HostSrc> srcs;
   std::vector<SrcSyn> src_syn;
   bool stdp_on = false;
@@ -227,6 +232,8 @@ struct sg_net {
   StepArgs h_args{};
   bool args_uploaded = false;
   sg_pool *pool = nullptr;     // the pool this network steps in, if any
+  int red_variant = 0;         // pre-centric scatter schedule (sg_autotune)
+  uint32_t red_bps = kRedBlocksPerSM;
   unsigned long long drv_folded = ~0ull;
   bool any_drv = false;
   // short-term plasticity: profiles, staged per-edge ids (kept only once an
@@ -388,6 +395,8 @@ StepArgs make_args(sg_net *net) {
     a.kin_erev[k] = net->kin[k].erev;
   }
   a.kin_g = net->d_kin_g.p;
+  a.receptor = net->receptor ? 1 : 0;
+  for (int r = 0; r < kReceptors; ++r) a.rec_f[r] = net->rec_f[r];
   a.row_ptr = net->d_row_ptr.p;
   a.edge = net->d_edge.p;
   a.wbf16 = net->weight_format == SG_W_BF16 ? 1 : 0;
@@ -500,8 +509,8 @@ __global__ void sort_key_kernel(const uint32_t *pre, const uint32_t *post, unsig
 // Segment table: entry j of row `pre` = first position in the row whose post
 // is >= j*P (rows are sorted by post), entry G = row length.
 template <typename T>
-__global__ void seg_table_kernel(const uint32_t *row_ptr, const uint2 *edge, int packed, uint32_t Nd, uint32_t G,
-                                 uint32_t P, T *seg) {
+__global__ void seg_table_kernel(const uint32_t *row_ptr, const uint32_t *xw, uint32_t xstride, uint32_t post_mask,
+                                 uint32_t Nd, uint32_t G, uint32_t P, T *seg) {
   for (uint32_t pre = blockIdx.x * blockDim.x + threadIdx.x; pre < Nd; pre += gridDim.x * blockDim.x) {
     const uint32_t beg = row_ptr[pre], end = row_ptr[pre + 1];
     T *out = seg + (size_t)pre * (G + 1);
@@ -511,7 +520,7 @@ __global__ void seg_table_kernel(const uint32_t *row_ptr, const uint2 *edge, int
       uint32_t hi = end;
       while (lo < hi) {  // lower_bound of bound in [lo, end); no overflow past 2^31 edges
         const uint32_t mid = lo + ((hi - lo) >> 1);
-        if (edge_post(edge[mid], packed) < bound) lo = mid + 1;
+        if ((xw[(size_t)mid * xstride] & post_mask) < bound) lo = mid + 1;
         else hi = mid;
       }
       out[j] = (T)(lo - beg);
@@ -572,7 +581,8 @@ __global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, u
                                       uint64_t base, uint32_t n_post, uint32_t k_in, uint64_t seed,
                                       uint32_t from_off, uint32_t n_from, uint32_t to_off,
                                       uint32_t n_exc, float w_exc, float w_inh, uint32_t d_min,
-                                      uint32_t d_span, uint8_t st_e, uint8_t st_i, uint32_t flags_e) {
+                                      uint32_t d_span, uint8_t st_e, uint8_t st_i, uint32_t flags_e,
+                                      int recept) {
   const uint64_t total = (uint64_t)n_post * k_in;
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t h = splitmix64(seed ^ (t * 0x9E3779B97F4A7C15ull));
@@ -583,7 +593,8 @@ __global__ void synth_indegree_kernel(uint32_t *pre, uint32_t *post, float *w, u
     pre[base + t] = from_off + src;
     post[base + t] = to_off + j;
     w[base + t] = exc ? w_exc : w_inh;
-    code[base + t] = edge_code((uint8_t)d, exc ? st_e : st_i, exc && (flags_e & SG_EDGE_STDP));
+    code[base + t] = recept ? receptor_code(exc ? st_e : st_i)
+                            : edge_code((uint8_t)d, exc ? st_e : st_i, exc && (flags_e & SG_EDGE_STDP));
   }
 }
 
@@ -605,6 +616,7 @@ struct OutDegreeSpec {
   uint32_t d_min, d_span;       // delay uniform in [d_min, d_min + d_span)
   uint8_t st_exc, st_inh;       // synapse type (kinetic profile) by source class
   uint32_t flags_exc;           // SG_EDGE_STDP for excitatory sources
+  int receptor;                 // st_exc / st_inh are receptor codes (receptor kinetics)
 };
 
 __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, uint8_t *code, uint64_t base,
@@ -643,7 +655,8 @@ __global__ void synth_outdegree_kernel(uint32_t *pre, uint32_t *post, float *w, 
                                     : (float)lo * 2.3283064365386963e-10f;
       w[e] = random_w ? scale * u : scale;
       const uint32_t dly = sp.d_span > 1 ? sp.d_min + (uint32_t)(splitmix64(h) & 0xffffffffull) % sp.d_span : sp.d_min;
-      code[e] = edge_code((uint8_t)dly, exc ? sp.st_exc : sp.st_inh, exc && (sp.flags_exc & SG_EDGE_STDP));
+      code[e] = sp.receptor ? receptor_code(exc ? sp.st_exc : sp.st_inh)
+                            : edge_code((uint8_t)dly, exc ? sp.st_exc : sp.st_inh, exc && (sp.flags_exc & SG_EDGE_STDP));
     }
     // the row sorted by target (shell sort; the targets are distinct), so
     // that generated edges arrive in CSR order and the build needs no sort
@@ -892,8 +905,9 @@ void build_graph(sg_net *net) {
 }
 
 // Scatter geometry and the per-row segment table.
+// Scatter geometry: G blocks of P posts (the owner-computes scatter's post
+// ranges, and the grouping of Poisson-source synapses).
 void build_segments(sg_net *net) {
-  cudaStream_t s = net->stream;
   const uint32_t Nd = net->Nd;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, net->device);
@@ -906,6 +920,15 @@ void build_segments(sg_net *net) {
   while ((1u << pb) < P) ++pb;
   net->pbits = pb;
   SG_REQUIRE(((uint64_t)(4 * kSlots) << pb) < 0xFFFFFFFFull, SG_E_INVALID, "network too large for the cell encoding");
+}
+
+// The per-row segment table of the owner-computes scatter ([Nd][G+1] record
+// offsets where each block's post range starts); built when a network first
+// takes that path (networks on the pre-centric scatter never need it).
+void build_seg_table(sg_net *net) {
+  if (net->d_seg.p) return;
+  cudaStream_t s = net->stream;
+  const uint32_t Nd = net->Nd, G = net->G, P = net->P;
   // longest row decides the table width
   std::vector<uint32_t> rp((size_t)Nd + 1);
   SG_CUDA(cudaMemcpyAsync(rp.data(), net->d_row_ptr.p, rp.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -915,12 +938,15 @@ void build_segments(sg_net *net) {
   net->seg32 = longest >= 65536 ? 1 : 0;
   const size_t esz = net->seg32 ? 4 : 2;
   net->d_seg.alloc(std::max<size_t>((size_t)Nd * (G + 1) * esz, 1));
+  const bool split = net->weight_format != SG_W_F32 && !net->d_edge.p;
+  const uint32_t *xw = split ? net->d_edge_x.p : reinterpret_cast<const uint32_t *>(net->d_edge.p);
+  const uint32_t xstride = split ? 1u : 2u, mask = net->packed ? 0x00FFFFFFu : 0xFFFFFFFFu;
   launch_grid(Nd, [&](unsigned b) {
     if (net->seg32)
-      seg_table_kernel<uint32_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->packed, Nd, G, P,
+      seg_table_kernel<uint32_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, xw, xstride, mask, Nd, G, P,
                                                    (uint32_t *)net->d_seg.p);
     else
-      seg_table_kernel<uint16_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, net->d_edge.p, net->packed, Nd, G, P,
+      seg_table_kernel<uint16_t><<<b, 256, 0, s>>>(net->d_row_ptr.p, xw, xstride, mask, Nd, G, P,
                                                    (uint16_t *)net->d_seg.p);
   });
   SG_CUDA(cudaGetLastError());
@@ -1364,25 +1390,42 @@ void upload_args(sg_net *net, const StepArgs &a) {
   net->args_uploaded = true;
 }
 
-// The pre-centric scatter's shared memory (stage ring) exceeds the 48 KB
-// default: allowed once per device before its first launch.
+// The pre-centric scatter's schedules (stages x synapses per stage), the
+// first being the fixed one; sg_autotune picks one per network, with the
+// blocks per SM.
+// (4 x 1024, 8 x 512, 3 x 2048, 6 x 512: launch_step_red)
+constexpr int kNumRedVariants = 4;
+
+template <uint32_t ST, uint32_t CH> void allow_red_smem_v() {
+  SG_CUDA(cudaFuncSetAttribute(scatter_red_kernel<ST, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(RedSmemT<ST, CH>)));
+}
+// The stage rings exceed the 48 KB default of shared memory: allowed once
+// per device before the first launch.
 void allow_red_smem() {
-  SG_CUDA(cudaFuncSetAttribute(scatter_red_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RedSmem)));
+  allow_red_smem_v<4, 1024>();
+  allow_red_smem_v<8, 512>();
+  allow_red_smem_v<3, 2048>();
+  allow_red_smem_v<6, 512>();
 }
 
-unsigned red_grid(int device) {
+unsigned sm_count(int device) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return (unsigned)sms * kRedBlocksPerSM;
+  return (unsigned)sms;
 }
+
+void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
+                     uint32_t *done, uint32_t *err, uint32_t stall);
 
 void update_path(sg_net *net) {
   // the pre-centric scatter applies neither pair STDP nor short-term
   // plasticity: those networks keep the owner-computes scatter in any mode
-  const bool plain = !net->stdp_on && !net->tm_edges && !net->src_tm;
+  const bool plain = !net->stdp_on && !net->tm_edges && !net->src_tm && !net->receptor;
   const int red = plain && (!net->deterministic || net->exact) ? 1 : 0;
   if (red != net->red) drop_graph(net);
   net->red = red;
+  if (!red) build_seg_table(net);
 }
 
 void setup_scatter(sg_net *net) {
@@ -1455,7 +1498,7 @@ void finish_build(sg_net *net) {
   const size_t n_rings = 1 + net->kin.size();
   // a step's events land at most max(delay, 1) steps ahead, so that many
   // slots plus the one being read hold every pending arrival
-  net->nslots = std::max<uint32_t>(net->max_delay, 1u) + 1u;
+  net->nslots = net->receptor ? 1u + kReceptors : std::max<uint32_t>(net->max_delay, 1u) + 1u;
   net->d_ring.alloc(std::max<size_t>(n_rings * net->nslots * Nd, 1));
   net->d_ring.zero(s);
   net->d_kin_g.alloc(std::max<size_t>(net->kin.size() * 3 * Nd, 1));  // up to 3 state arrays per profile
@@ -1589,6 +1632,30 @@ void launch_step_kernel(void (*kernel)(KArgs...), unsigned grid, unsigned block,
   SG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
 }
 
+// One launch of the pre-centric scatter with schedule `variant` and `bps`
+// blocks per SM over a table of networks.
+void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
+                     uint32_t *done, uint32_t *err, uint32_t stall) {
+  const unsigned grid = sm_count(device) * bps;
+  switch (variant) {
+    case 1:
+      launch_step_kernel(scatter_red_kernel<8, 512>, grid, kRedThreads, sizeof(RedSmemT<8, 512>), s, nets, n_nets,
+                         done, err, stall);
+      break;
+    case 2:
+      launch_step_kernel(scatter_red_kernel<3, 2048>, grid, kRedThreads, sizeof(RedSmemT<3, 2048>), s, nets, n_nets,
+                         done, err, stall);
+      break;
+    case 3:
+      launch_step_kernel(scatter_red_kernel<6, 512>, grid, kRedThreads, sizeof(RedSmemT<6, 512>), s, nets, n_nets,
+                         done, err, stall);
+      break;
+    default:
+      launch_step_kernel(scatter_red_kernel<4, 1024>, grid, kRedThreads, sizeof(RedSmemT<4, 1024>), s, nets, n_nets,
+                         done, err, stall);
+  }
+}
+
 template <int M, bool FULL> void launch_neuron_form(sg_net *net, const StepArgs &a, uint32_t nb) {
   if (net->model_single[M] >= 0)
     launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M>::THREADS, 0, net->stream, a,
@@ -1601,7 +1668,7 @@ template <int M, bool FULL> void launch_neuron_form(sg_net *net, const StepArgs 
 // The lean neuron kernel serves steps without kinetic synapses, input
 // noise, neuron statistics, pair STDP or learning.
 bool needs_full_neuron_kernel(const sg_net *net, const StepArgs &a) {
-  if (a.n_kin || a.ns_count != nullptr || a.stdp || a.learn) return true;
+  if (a.n_kin || a.receptor || a.ns_count != nullptr || a.stdp || a.learn) return true;
   for (const auto &p : net->pops)
     if (p.noise) return true;
   return false;
@@ -1644,8 +1711,8 @@ void enqueue_rest(sg_net *net, const StepArgs &a) {
     if (p.external && p.n)
       ext_spikes_kernel<<<p.cap / kNeuronBlock, kNeuronBlock, 0, s>>>(a, p.dev_off, p.n, p.ext_src);
   if (a.red) {
-    launch_step_kernel(scatter_red_kernel, red_grid(net->device), kRedThreads, sizeof(RedSmem), s,
-                       (const StepArgs *)net->d_args.p, 1u, net->d_done.p, net->d_err.p, net->debug_stall);
+    launch_step_red(s, net->device, net->red_variant, net->red_bps, (const StepArgs *)net->d_args.p, 1u,
+                    net->d_done.p, net->d_err.p, net->debug_stall);
   } else {
     if (net->seg32) launch_step_kernel(scatter_kernel<true>, net->G, kScatterThreads, net->scatter_smem, s, a);
     else launch_step_kernel(scatter_kernel<false>, net->G, kScatterThreads, net->scatter_smem, s, a);
@@ -2014,13 +2081,15 @@ static int connect_impl(sg_net *net, uint32_t from, const uint32_t *fi, uint32_t
       SG_REQUIRE(d[i] < kSlots, SG_E_INVALID, "delay " + std::to_string(d[i]) + " >= MAX_DELAY_SLOTS (32)");
       net->max_delay = std::max<uint32_t>(net->max_delay, d[i]);
       const uint8_t s = st ? st[i] : 0;
-      SG_REQUIRE(s <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
+      SG_REQUIRE(net->receptor || s <= 3, SG_E_INVALID, "syn_type > 3 is not supported on the device path");
+      SG_REQUIRE(!net->receptor || (!(flags & SG_EDGE_STDP) && (!ptype || ptype[i] == 0)), SG_E_INVALID,
+                 "receptor kinetics: no pair-STDP or short-term plastic synapses");
       if (ptype)
         SG_REQUIRE(ptype[i] <= net->tm_prof.size(), SG_E_INVALID,
                    "Network::build: plast_type " + std::to_string(ptype[i]) + " exceeds registered plasticity profiles");
       pre[i] = pf.dev_off + fi[i];
       post[i] = pt.dev_off + ti[i];
-      code[i] = edge_code(d[i], s, (flags & SG_EDGE_STDP) != 0);
+      code[i] = net->receptor ? receptor_code(s) : edge_code(d[i], s, (flags & SG_EDGE_STDP) != 0);
     }
     DevGuard g(net->device);
     upload_staged_edges(net, pre.data(), post.data(), w, code.data(), n, ptype);
@@ -2071,7 +2140,8 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
     require_local(net, to);
     SG_REQUIRE(d_min <= d_max && d_max < kSlots, SG_E_INVALID, "delay range invalid");
     SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
-    SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
+    SG_REQUIRE(net->receptor || (st_e <= 3 && st_i <= 3), SG_E_INVALID, "syn_type > 3 is not supported");
+    SG_REQUIRE(!net->receptor || !(flags_e & SG_EDGE_STDP), SG_E_INVALID, "receptor kinetics: no pair-STDP synapses");
     const auto &pf = net->pops[from];
     const auto &pt = net->pops[to];
     SG_REQUIRE(pf.n > 0 || k_in == 0, SG_E_INVALID, "empty source population");
@@ -2087,7 +2157,8 @@ int sg_connect_fixed_indegree(sg_net *net, uint32_t from, uint32_t to, uint32_t 
     launch_grid(n, [&](unsigned b) {
       synth_indegree_kernel<<<b, 256, 0, net->stream>>>(net->e_pre.p, net->e_post.p, net->e_w.p, net->e_code.p, n0,
                                                         pt.n, k_in, seed, pf.dev_off, pf.n, pt.dev_off, n_exc, w_exc,
-                                                        w_inh, d_min, (uint32_t)(d_max - d_min + 1), st_e, st_i, flags_e);
+                                                        w_inh, d_min, (uint32_t)(d_max - d_min + 1), st_e, st_i, flags_e,
+                                                        net->receptor ? 1 : 0);
     });
     SG_CUDA(cudaGetLastError());
     SG_CUDA(cudaStreamSynchronize(net->stream));
@@ -2104,7 +2175,8 @@ static OutDegreeSpec outdegree_spec(sg_net *net, uint32_t from, uint32_t to, uin
   require_local(net, to);
   SG_REQUIRE(d_min <= d_max && d_max < kSlots, SG_E_INVALID, "delay range invalid (d_min <= d_max < 32)");
   SG_REQUIRE(std::isfinite(w_exc) && std::isfinite(w_inh), SG_E_INVALID, "weights must be finite");
-  SG_REQUIRE(st_e <= 3 && st_i <= 3, SG_E_INVALID, "syn_type > 3 is not supported");
+  SG_REQUIRE(net->receptor || (st_e <= 3 && st_i <= 3), SG_E_INVALID, "syn_type > 3 is not supported");
+  SG_REQUIRE(!net->receptor || !(flags_e & SG_EDGE_STDP), SG_E_INVALID, "receptor kinetics: no pair-STDP synapses");
   SG_REQUIRE(!no_self || from == to, SG_E_INVALID, "no_self needs from == to");
   SG_REQUIRE(random_w >= 0 && random_w <= 24, SG_E_INVALID, "random_w: 0, 1, or a grid of 2..24 bits");
   OutDegreeSpec sp{};
@@ -2122,6 +2194,7 @@ static OutDegreeSpec outdegree_spec(sg_net *net, uint32_t from, uint32_t to, uin
   sp.st_exc = st_e;
   sp.st_inh = st_i;
   sp.flags_exc = flags_e;
+  sp.receptor = net->receptor ? 1 : 0;
   return sp;
 }
 
@@ -2219,6 +2292,7 @@ int sg_register_kinetics(sg_net *net, int kind, const float *p, float erev, floa
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "register_kinetics must be called before build()");
+    SG_REQUIRE(!net->receptor, SG_E_STATE, "receptor kinetics: no kinetic profiles");
     SG_REQUIRE(p, SG_E_INVALID, "null parameters");
     SG_REQUIRE(std::isfinite(erev), SG_E_INVALID, "erev must be finite");
     SG_REQUIRE(std::isfinite(dt) && dt > 0, SG_E_INVALID, "register_kinetics: dt must be finite and > 0");
@@ -2274,6 +2348,7 @@ int sg_poisson_add_many(sg_net *net, uint32_t n, float rate_hz, float dt_ms, con
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "add_poisson_source must be called before build()");
+    SG_REQUIRE(!net->receptor, SG_E_STATE, "receptor kinetics: no Poisson sources");
     SG_REQUIRE(std::isfinite(rate_hz) && rate_hz >= 0, SG_E_INVALID, "add_poisson_source: rate_hz must be finite and >= 0");
     SG_REQUIRE(std::isfinite(dt_ms) && dt_ms > 0, SG_E_INVALID, "add_poisson_source: dt_ms must be finite and > 0");
     float p = rate_hz * dt_ms / 1000.0f;  // core.rs:301
@@ -2348,11 +2423,71 @@ int sg_poisson_connect_one_to_one(sg_net *net, uint32_t first, uint32_t n, uint3
   });
 }
 
+// SynapticBrain::from_sparse_graph(graph, receptor_types, dt)
+// (pillars-connectome/src/synaptic.rs:53-63): the syn_types of the edges
+// connected after this call are receptor codes, delays are ignored, and
+// every step decays the seven conductances and adds their ohmic current
+// (step order :94-130).  DecayFactors::new(dt), P/kernels/synapse/
+// kinetics.rs:27-38.
+int sg_set_receptor_kinetics(sg_net *net, float dt) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(!net->built, SG_E_STATE, "receptor kinetics must be set before build()");
+    SG_REQUIRE(std::isfinite(dt) && dt > 0.0f, SG_E_INVALID, "receptor kinetics: dt must be finite and > 0");
+    SG_REQUIRE(net->e_pre.n == 0 && net->kin.empty() && net->srcs.empty() && !net->stdp_on, SG_E_STATE,
+               "receptor kinetics: set before any synapse, kinetic profile, Poisson source or STDP");
+    net->receptor = true;
+    for (int r = 0; r < kReceptors; ++r) net->rec_f[r] = host_fast_exp(-dt / rec_tau(r));
+  });
+}
+
+// SynapticBrain::kinetics / set_kinetics (synaptic.rs:66-80): the seven
+// conductance arrays, g[r * total + i] for receptor r and neuron i.
+int sg_receptor_read(sg_net *net, float *g) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built && net->receptor, SG_E_STATE, "receptor kinetics are not on (or not built)");
+    SG_REQUIRE(g, SG_E_INVALID, "null output");
+    DevGuard gd(net->device);
+    const uint32_t Nd = net->Nd;
+    std::vector<float> r((size_t)kReceptors * Nd);
+    SG_CUDA(cudaMemcpyAsync(r.data(), net->d_ring.p + Nd, r.size() * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    const uint64_t N = net->total;
+    for (int k = 0; k < kReceptors; ++k)
+      for (size_t p = 0; p < net->pops.size(); ++p)
+        for (uint32_t i = 0; i < net->pops[p].n; ++i)
+          g[(size_t)k * N + net->offsets[p] + i] = r[(size_t)k * Nd + net->pops[p].dev_off + i];
+  });
+}
+
+int sg_receptor_write(sg_net *net, const float *g) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built && net->receptor, SG_E_STATE, "receptor kinetics are not on (or not built)");
+    SG_REQUIRE(g, SG_E_INVALID, "null input");
+    const uint64_t N = net->total;
+    for (uint64_t k = 0; k < (uint64_t)kReceptors * N; ++k)
+      SG_REQUIRE(std::isfinite(g[k]), SG_E_INVALID, "conductances must be finite");
+    DevGuard gd(net->device);
+    const uint32_t Nd = net->Nd;
+    std::vector<float> r((size_t)kReceptors * Nd, 0.0f);
+    for (int k = 0; k < kReceptors; ++k)
+      for (size_t p = 0; p < net->pops.size(); ++p)
+        for (uint32_t i = 0; i < net->pops[p].n; ++i)
+          r[(size_t)k * Nd + net->pops[p].dev_off + i] = g[(size_t)k * N + net->offsets[p] + i];
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    SG_CUDA(cudaMemcpyAsync(net->d_ring.p + Nd, r.data(), r.size() * 4, cudaMemcpyHostToDevice, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+  });
+}
+
 int sg_stdp_config(sg_net *net, float dt, float tau_pre, float tau_post, float a_plus, float a_minus, float w_min,
                    float w_max) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "stdp must be configured before build()");
+    SG_REQUIRE(!net->receptor, SG_E_STATE, "receptor kinetics: no pair STDP");
     SG_REQUIRE(dt > 0 && tau_pre > 0 && tau_post > 0 && w_min <= w_max, SG_E_INVALID, "invalid STDP config");
     net->stdp_on = true;
     net->stdp_dt = dt;
@@ -2397,6 +2532,9 @@ int sg_build(sg_net *net) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(!net->built, SG_E_STATE, "Network::build() called twice — the graph is already built");
+    SG_REQUIRE(!net->receptor || (net->kin.empty() && net->srcs.empty() && !net->stdp_on && !net->tm_edges),
+               SG_E_INVALID,
+               "receptor kinetics: no kinetic profiles, Poisson sources, pair-STDP or short-term plasticity");
     DevGuard g(net->device);
     // GPEA Nernst constants (gpea.rs:277-278), with the ln the kernels use
     net->ln_consts = {sg_logf(10.0f / 140.0f), sg_logf(5.0f / 140.0f)};
@@ -2439,7 +2577,7 @@ int sg_build_from_csr(sg_net *net, const uint32_t *row_ptr, const uint32_t *col,
         net->max_delay = std::max<uint32_t>(net->max_delay, d[e]);
         pre[e] = g2d[i];
         post[e] = g2d[col[e]];
-        code[e] = edge_code(d[e], 0, false);
+        code[e] = net->receptor ? receptor_code(0) : edge_code(d[e], 0, false);
       }
     DevGuard g(net->device);
     if (E) upload_staged_edges(net, pre.data(), post.data(), w, code.data(), E);
@@ -2529,7 +2667,8 @@ int sg_inject(sg_net *net, uint32_t pop, const uint32_t *idx, const float *vals,
     SG_CUDA(cudaMemcpyAsync(net->d_inj_val.p, vals, n * 4, cudaMemcpyHostToDevice, net->stream));
     fold_drive(net);  // the last step's deferred drive precedes this input in the slot
     unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 8);
-    inject_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->nslots, net->d_step.p, net->d_inj_idx.p,
+    inject_kernel<<<blocks, 256, 0, net->stream>>>(net->d_ring.p, net->Nd, net->receptor ? 1u : net->nslots,
+                                                   net->d_step.p, net->d_inj_idx.p,
                                                    net->d_inj_val.p, n, p.dev_off, dup ? 1 : 0);
     SG_CUDA(cudaGetLastError());
     // the staging buffers are reused by the next call
@@ -2546,6 +2685,68 @@ int sg_step(sg_net *net, uint32_t n_steps) {
     DevGuard g(net->device);
     if (net->profile && net->total > 0) do_steps_profiled(net, n_steps);
     else do_steps(net, n_steps);
+  });
+}
+
+// Autotuning of the pre-centric scatter's schedule on the network's own
+// steps: each candidate (stage ring of kRedVariants x 1..3 blocks per SM) runs
+// `steps` steps after one warm-up chunk, timed with CUDA events on the
+// network's stream; the fastest is kept.  On this path every schedule gives
+// the same bits (the ring sums are exact, or the order is free), so the
+// steps are ordinary steps of the simulation.
+int sg_autotune(sg_net *net, uint32_t steps, float *fixed_ms, float *best_ms, int *best_variant,
+                uint32_t *best_bps) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->built, SG_E_STATE, "autotune needs a built network");
+    SG_REQUIRE(steps > 0, SG_E_INVALID, "autotune: steps must be > 0");
+    SG_REQUIRE(!has_external(net) && !net->pool, SG_E_STATE,
+               "autotune: the network steps on its own (not split, not in a pool)");
+    DevGuard g(net->device);
+    const int v0 = net->red_variant;
+    const uint32_t b0 = net->red_bps;
+    float fixed = 0.0f, best = 0.0f;
+    int bv = 0;
+    uint32_t bb = kRedBlocksPerSM;
+    if (net->red) {
+      cudaEvent_t e0, e1;
+      SG_CUDA(cudaEventCreate(&e0));
+      SG_CUDA(cudaEventCreate(&e1));
+      bool first = true;
+      for (int v = 0; v < kNumRedVariants; ++v)
+        for (uint32_t bps = 1; bps <= 3; ++bps) {
+          net->red_variant = v;
+          net->red_bps = bps;
+          drop_graph(net);
+          do_steps(net, std::min<uint32_t>(steps, 64));  // warm-up (and the graph's capture)
+          SG_CUDA(cudaEventRecord(e0, net->stream));
+          do_steps(net, steps);
+          SG_CUDA(cudaEventRecord(e1, net->stream));
+          SG_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.0f;
+          SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          ms /= (float)steps;
+          if (v == 0 && bps == kRedBlocksPerSM) fixed = ms;
+          if (first || ms < best) {
+            best = ms;
+            bv = v;
+            bb = bps;
+            first = false;
+          }
+        }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      net->red_variant = bv;
+      net->red_bps = bb;
+      drop_graph(net);
+    } else {
+      net->red_variant = v0;
+      net->red_bps = b0;
+    }
+    if (fixed_ms) *fixed_ms = fixed;
+    if (best_ms) *best_ms = best;
+    if (best_variant) *best_variant = net->red_variant;
+    if (best_bps) *best_bps = net->red_bps;
   });
 }
 
@@ -2896,6 +3097,12 @@ static void read_csr_global(sg_net *net, uint32_t *row_ptr, uint32_t *col, float
     const uint32_t post = net->packed ? (ed[e].x & 0x00FFFFFFu) : ed[e].x;
     const uint8_t c = net->packed ? (uint8_t)(ed[e].x >> 24) : code[e];
     col[e] = d2g[post];
+    if (net->receptor) {  // the delay field holds 1 + the receptor code; delays are not kept
+      d[e] = 0;
+      if (syn) syn[e] = (uint8_t)(code_delay(c) - 1u);
+      if (plastic) plastic[e] = 0;
+      continue;
+    }
     d[e] = (uint8_t)code_delay(c);
     if (syn) syn[e] = (uint8_t)code_ring(c);
     if (plastic) plastic[e] = code_stdp(c) ? 1 : 0;
@@ -2941,6 +3148,7 @@ int sg_ring_read(sg_net *net, uint32_t ring, float *out) {
     SG_REQUIRE(net->built, SG_E_STATE, "not built");
     SG_REQUIRE(ring <= net->kin.size(), SG_E_INVALID, "ring out of range");
     SG_REQUIRE(out, SG_E_INVALID, "null output");
+    SG_REQUIRE(!net->receptor, SG_E_STATE, "receptor kinetics: read the conductances (sg_receptor_read)");
     DevGuard g(net->device);
     const uint32_t Nd = net->Nd, M = net->nslots;
     fold_drive(net);
@@ -3085,6 +3293,7 @@ int sg_learn_enable(sg_net *net, float dt, float tau_pre, float tau_post, float 
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "learning needs a built network");
     SG_REQUIRE(!net->learn_on, SG_E_STATE, "learning is already enabled");
+    SG_REQUIRE(!net->receptor, SG_E_STATE, "receptor kinetics: learning is not available");
     SG_REQUIRE(net->weight_format == SG_W_F32, SG_E_INVALID,
                "BF16 and FP8 weights are read-only: learning needs FP32 weights");
     const float v[9] = {dt, tau_pre, tau_post, tau_e, a_ltp, a_ltd, lr, w_min, w_max};
@@ -3630,8 +3839,8 @@ void pool_enqueue_step(sg_pool *pool) {
   pool_launch_neuron<kIZH>(pool);
   pool_launch_neuron<kGPEA>(pool);
   pool_launch_neuron<kHH>(pool);
-  launch_step_kernel(scatter_red_kernel, red_grid(pool->device), kRedThreads, sizeof(RedSmem), pool->stream,
-                     (const StepArgs *)pool->d_nets.p, (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u);
+  launch_step_red(pool->stream, pool->device, 0, kRedBlocksPerSM, (const StepArgs *)pool->d_nets.p,
+                  (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u);
 }
 
 }  // namespace

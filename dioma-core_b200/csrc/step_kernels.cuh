@@ -114,6 +114,12 @@ struct StepArgs {
   float kin_c[3][8];
   float kin_erev[3];
   float *kin_g;
+  // receptor kinetics (SynapticBrain): ring slot 0 holds the step's external
+  // input, slots 1..7 the conductances of receptors 0..6, never cleared and
+  // decayed by rec_f each step; spikes jump them with no delay (an edge's
+  // delay field is 1 + its receptor, and the ring base stays 0)
+  int receptor;
+  float rec_f[7];
   // CSR (device neuron indices), rows sorted by post; one 8-byte record per
   // synapse: x = post | code << 24 (packed) or post (code in `code`), y = weight
   const uint32_t *row_ptr;
@@ -234,6 +240,13 @@ struct PopArgs {
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// The ring slot a step reads (and the base its events count delays from):
+// step % nslots, or 0 under receptor kinetics, whose slots are fixed
+// (0 external input, 1 + r conductance of receptor r).
+__device__ __forceinline__ uint32_t ring_base(const StepArgs &a, unsigned long long step) {
+  return a.receptor ? 0u : (uint32_t)(step % a.nslots);
+}
 
 // Programmatic dependent launch: the step kernels are launched so that the
 // next kernel of the stream may start while this one drains.  pdl_wait()
@@ -374,7 +387,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   const uint32_t i0 = blk * kNeuronBlock + tid * NPT;  // population index of my first neuron
   const uint32_t gi0 = p.dev_off + i0;
   const unsigned long long step = *a.step;
-  const uint32_t slot = (uint32_t)(step % a.nslots);
+  const uint32_t slot = ring_base(a, step);
   // 1-2. read the slot, clear it (step.rs:27-34)
   float x[NPT], zero[NPT];
 #pragma unroll
@@ -455,6 +468,34 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     V::store(g0, s0);
     if (kind != 0) V::store(g1, s1);
     if (kind == 3) V::store(g2, s2);
+  }
+  // 2c. receptor kinetics (SynapticBrain::step, pillars-connectome/src/
+  // synaptic.rs:94-112): decay each conductance (P/kernels/synapse/
+  // kinetics.rs:112-147), I_syn = sum over receptors in code order of
+  // g_eff (E_rev - V) from zero with NMDA's g scaled by the Mg block of the
+  // pre-step V (:159-206), input = I_syn + the external input.
+  if (FULL && a.receptor) {
+    float cur[NPT], mg[NPT];
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) {
+      cur[q] = 0.0f;
+      mg[q] = nmda_mg_block(sv[0][q]);
+    }
+#pragma unroll
+    for (int r = 0; r < kReceptors; ++r) {
+      float g[NPT];
+      float *gp = a.ring + (size_t)(1 + r) * a.Nd + gi0;
+      V::load(gp, g);
+#pragma unroll
+      for (int q = 0; q < NPT; ++q) {
+        g[q] = g[q] * a.rec_f[r];
+        const float ge = r == 1 ? g[q] * mg[q] : g[q];
+        cur[q] = cur[q] + ge * (rec_erev(r) - sv[0][q]);
+      }
+      V::store(gp, g);
+    }
+#pragma unroll
+    for (int q = 0; q < NPT; ++q) x[q] = cur[q] + x[q];
   }
   float pv[NP][NPT];
 #pragma unroll
@@ -848,7 +889,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   const uint32_t p0 = j * a.P;
   pdl_wait();
   const unsigned long long step = *a.step;
-  const uint32_t base = (uint32_t)(step % a.nslots);
+  const uint32_t base = ring_base(a, step);
   const uint32_t G1 = a.G + 1;
   const uint32_t pj = min(a.P, a.Nd - p0);
   if (tid == 0) {
@@ -1153,16 +1194,21 @@ constexpr uint32_t kRedConsumers = kRedThreads - 32;
 #endif
 constexpr uint32_t kRedBlocksPerSM = SG_RED_BLOCKS_PER_SM;
 constexpr int kRedUnroll = SG_RED_UNROLL;  // consumer loop unroll
-constexpr uint32_t kRedStages = 4;
-constexpr uint32_t kRedChunk = 1024;         // synapses per stage
 constexpr uint32_t kRedSegs = 16;            // row pieces per stage (short rows share a stage)
-// Stage regions: x words or FP32 records, weights (split formats), code
-// bytes (networks whose code bytes are a separate array).  Each row piece is
-// widened to 16-byte boundaries: at most 32 extra bytes per piece and region.
-constexpr uint32_t kRedXBytes = kRedChunk * 8 + kRedSegs * 32;
-constexpr uint32_t kRedWBytes = kRedChunk * 2 + kRedSegs * 32;
-constexpr uint32_t kRedCBytes = kRedChunk + kRedSegs * 32;
-constexpr uint32_t kRedStageBytes = kRedXBytes + kRedWBytes + kRedCBytes;
+// A stage ring of STAGES stages of CHUNK synapses each.  Stage regions: x
+// words or FP32 records, weights (split formats), code bytes (networks whose
+// code bytes are a separate array).  Each row piece is widened to 16-byte
+// boundaries: at most 32 extra bytes per piece and region.
+template <uint32_t STAGES, uint32_t CHUNK> struct RedCfg {
+  static constexpr uint32_t kStages = STAGES;
+  static constexpr uint32_t kChunk = CHUNK;
+  static constexpr uint32_t kXBytes = CHUNK * 8 + kRedSegs * 32;
+  static constexpr uint32_t kWBytes = CHUNK * 2 + kRedSegs * 32;
+  static constexpr uint32_t kCBytes = CHUNK + kRedSegs * 32;
+  static constexpr uint32_t kStageBytes = kXBytes + kWBytes + kCBytes;
+};
+// the fixed schedule (the autotuner's other candidates: sg_autotune)
+constexpr uint32_t kRedStagesDefault = 4, kRedChunkDefault = 1024;
 constexpr unsigned long long kWaitNs = 1000000000ull;     // every pipeline wait gives up after ~1 s
 
 __device__ __forceinline__ void red_add(float *p, float v, unsigned long long pol) {
@@ -1239,17 +1285,17 @@ struct RedSeg {
   uint32_t net;     // the network it belongs to
   float scale;      // FP8 row scale
 };
-// One stage: up to kRedChunk synapses from up to kRedSegs row pieces.
+// One stage: up to CHUNK synapses from up to kRedSegs row pieces.
 struct RedStage {
   uint32_t n;       // synapses in the stage, or kEmpty: the producer is done
   uint32_t n_seg;
   RedSeg seg[kRedSegs];
 };
-struct RedSmem {
-  alignas(16) unsigned char buf[kRedStages][kRedStageBytes];
-  RedStage meta[kRedStages];
-  uint64_t full[kRedStages];
-  uint64_t empty[kRedStages];
+template <uint32_t STAGES, uint32_t CHUNK> struct RedSmemT {
+  alignas(16) unsigned char buf[STAGES][RedCfg<STAGES, CHUNK>::kStageBytes];
+  RedStage meta[STAGES];
+  uint64_t full[STAGES];
+  uint64_t empty[STAGES];
   RedNet nets[kPoolMax];
   unsigned long long ev[kPoolMax], src_ev[kPoolMax];  // this block's events per network
 };
@@ -1280,9 +1326,9 @@ __device__ __forceinline__ uint32_t bulk_elems(unsigned char *region, uint32_t *
 // with evict_last).  One launch serves a table of networks (a single network,
 // or every network of a pool): block b takes spiking rows b, b + G, ... of
 // each network in turn.  Warp 0 is the producer: its lanes look up 32 rows
-// at a time (flat list,
-// row bounds) and lane 0 copies each row, kRedChunk synapses per stage, into
-// a kRedStages-deep shared-memory ring with 1-D bulk copies (cp.async.bulk,
+// at a time (flat list, row bounds) and lane 0 copies the rows, CHUNK
+// synapses per stage (short rows share a stage), into a STAGES-deep
+// shared-memory ring with 1-D bulk copies (cp.async.bulk,
 // this GPU's memory, no multicast) that complete on the stage's mbarrier.
 // Warps 1-7 consume: per stage they read the synapses from shared memory and
 // issue the reds, then release the stage.  Every wait gives up after ~1 s,
@@ -1291,11 +1337,15 @@ __device__ __forceinline__ uint32_t bulk_elems(unsigned char *region, uint32_t *
 // take (deferred drive) follow, one per thread.  The last block to finish
 // closes the step of every network of the table.
 // ---------------------------------------------------------------------------
+template <uint32_t STAGES, uint32_t CHUNK>
 __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
     scatter_red_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done, uint32_t *err,
                        uint32_t stall) {
+  using Cfg = RedCfg<STAGES, CHUNK>;
+  constexpr uint32_t kRedStages = Cfg::kStages, kRedChunk = Cfg::kChunk, kRedXBytes = Cfg::kXBytes,
+                     kRedWBytes = Cfg::kWBytes;
   extern __shared__ __align__(128) unsigned char red_smem[];
-  RedSmem &S = *reinterpret_cast<RedSmem *>(red_smem);
+  RedSmemT<STAGES, CHUNK> &S = *reinterpret_cast<RedSmemT<STAGES, CHUNK> *>(red_smem);
   const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
   if (tid == 0) {
     for (uint32_t k = 0; k < kRedStages; ++k) {

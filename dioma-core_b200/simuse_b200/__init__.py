@@ -20,4 +20,6 @@ from .network import (  # noqa: F401
     Pool,
 )
 from .kuramoto import KuramotoBatch  # noqa: F401,E402
+from .sweep import Sweep  # noqa: F401,E402
+from .synaptic import SynapticBrain  # noqa: F401,E402
 from . import taas  # noqa: F401,E402

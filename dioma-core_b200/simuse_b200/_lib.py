@@ -33,6 +33,7 @@ SIGNATURES = {
     "sg_net_destroy": [vp],
     "sg_synchronize": [vp],
     "sg_debug_stall_scatter": [vp, i32],
+    "sg_autotune": [vp, u32, vp, vp, vp, vp],
     "sg_pool_create": [vp, i32],
     "sg_pool_destroy": [vp],
     "sg_pool_add": [vp, vp],
@@ -65,6 +66,9 @@ SIGNATURES = {
     "sg_scatter_mode": [vp, vp],
     "sg_register_plasticity": [vp, f32, f32, i32, f32, f32, vp],
     "sg_register_kinetics": [vp, i32, vp, f32, f32, vp],
+    "sg_set_receptor_kinetics": [vp, f32],
+    "sg_receptor_read": [vp, vp],
+    "sg_receptor_write": [vp, vp],
     "sg_connect_plastic": [vp, u32, vp, u32, vp, vp, vp, vp, vp, u64, u32],
     "sg_build": [vp],
     "sg_build_from_csr": [vp, vp, vp, vp, vp],

@@ -165,6 +165,24 @@ class Network:
         check(lib().sg_register_kinetics(self._h, int(kind), _p(p), erev, dt, C.byref(out)))
         return out.value
 
+    def set_receptor_kinetics(self, dt: float):
+        """SynapticBrain receptor kinetics (before any connect): syn_types
+        become receptor codes (RECEPTORS), delays are ignored."""
+        check(lib().sg_set_receptor_kinetics(self._h, dt))
+        self._receptor = True
+
+    def receptor_conductances(self) -> np.ndarray:
+        """The seven conductances, [receptor code][neuron]."""
+        out = np.empty((7, self.total_neurons), np.float32)
+        check(lib().sg_receptor_read(self._h, _p(out)))
+        return out
+
+    def set_receptor_conductances(self, g):
+        g = np.ascontiguousarray(g, np.float32)
+        if g.shape != (7, self.total_neurons):
+            raise ValueError("conductances must be [7][total neurons]")
+        check(lib().sg_receptor_write(self._h, _p(g)))
+
     def add_poisson_source(self, rate_hz: float, dt_ms: float, seed: int) -> int:
         out = C.c_uint32()
         check(lib().sg_poisson_add(self._h, rate_hz, dt_ms, seed, C.byref(out)))
@@ -253,6 +271,16 @@ class Network:
 
     def synchronize(self):
         check(lib().sg_synchronize(self._h))
+
+    def autotune(self, steps: int = 200) -> dict:
+        """Picks the pre-centric scatter's schedule on the next candidates x
+        `steps` simulation steps (they are ordinary steps); returns the per-step
+        times of the fixed and the chosen schedule."""
+        fixed, best = C.c_float(), C.c_float()
+        v, bps = C.c_int(), C.c_uint32()
+        check(lib().sg_autotune(self._h, steps, C.byref(fixed), C.byref(best), C.byref(v), C.byref(bps)))
+        return {"fixed_ms_per_step": fixed.value, "tuned_ms_per_step": best.value, "variant": v.value,
+                "blocks_per_sm": bps.value}
 
     def debug_stall_scatter(self, on: bool):
         """Test hook: the pre-centric scatter's producer stops feeding its

@@ -114,10 +114,21 @@ def outdegree_delays(h: np.ndarray, d_min: int, d_max: int) -> np.ndarray:
     return (d_min + (splitmix64(h) & np.uint64(0xFFFFFFFF)) % np.uint64(span)).astype(np.uint8)
 
 
+def _uniform_w(h, random_w) -> np.ndarray:
+    """The U of a weight draw from the low 32 bits of hash h (f32)."""
+    lo = h & np.uint64(0xFFFFFFFF)
+    if random_w is True or int(random_w) == 1:
+        return lo.astype(np.float32) * np.float32(2.3283064365386963e-10)
+    b = int(random_w)
+    return (lo >> np.uint64(32 - b)).astype(np.float32) * np.float32(2.0 ** -b)
+
+
 def fixed_outdegree_edges(n: int, k: int, seed: int, n_exc: int, w_exc: float, w_inh: float,
-                          no_self: bool = True, random_w: bool = True):
+                          no_self: bool = True, random_w=True):
     """NumPy twin of the device generator sg_connect_fixed_outdegree (same
-    hash, same Floyd draws, same (source, draw) edge order)."""
+    hash, same Floyd draws, same (source, draw) edge order).  random_w as
+    there: False, True (U = lo32 / 2^32) or b in 2..24 (U on the 2^-b grid,
+    the top b bits of lo32)."""
     m = n - (1 if no_self else 0)
     i = np.arange(n, dtype=np.uint64)
     sel = np.empty((n, k), np.uint64)
@@ -132,8 +143,7 @@ def fixed_outdegree_edges(n: int, k: int, seed: int, n_exc: int, w_exc: float, w
                 dup = (sel[:, :q] == t[:, None]).any(axis=1)
                 t = np.where(dup, j, t)
             sel[:, q] = t
-            u = (h & np.uint64(0xFFFFFFFF)).astype(np.float32) * np.float32(2.3283064365386963e-10)
-            w[:, q] = scale * u if random_w else scale
+            w[:, q] = scale * _uniform_w(h, random_w) if random_w else scale
     tgt = sel.copy()
     if no_self:
         tgt = np.where(tgt >= i[:, None], tgt + np.uint64(1), tgt)
@@ -158,8 +168,9 @@ def lognormal_degrees(n: int, mean: float, sd: float, seed: int, kmax: int) -> n
 
 
 def lognormal_outdegree_edges(n: int, mean: float, sd: float, seed: int, n_exc: int, w_exc: float,
-                              w_inh: float, no_self: bool = True, random_w: bool = True):
-    """NumPy twin of sg_connect_lognormal_outdegree (small n: loops per source)."""
+                              w_inh: float, no_self: bool = True, random_w=True):
+    """NumPy twin of sg_connect_lognormal_outdegree (small n: loops per
+    source); random_w as for fixed_outdegree_edges."""
     m = n - (1 if no_self else 0)
     deg = lognormal_degrees(n, mean, sd, seed, min(m, 4096))
     off = np.concatenate([[0], np.cumsum(deg)])
@@ -183,8 +194,7 @@ def lognormal_outdegree_edges(n: int, mean: float, sd: float, seed: int, n_exc: 
                 tt = np.where(tt >= i, tt + 1, tt)
             post[off[i]:off[i + 1]] = tt
             scale = np.float32(w_exc if i < n_exc else w_inh)
-            u = (h & np.uint64(0xFFFFFFFF)).astype(np.float32) * np.float32(2.3283064365386963e-10)
-            w[off[i]:off[i + 1]] = scale * u if random_w else scale
+            w[off[i]:off[i + 1]] = scale * _uniform_w(h, random_w) if random_w else scale
     return pre, post, w
 
 
@@ -200,12 +210,13 @@ def izhikevich_params(n: int, n_exc: int, seed: int):
 
 
 def add_izhikevich_instance(net, n: int, seed: int, k_out: int = 100, device_edges: bool = True,
-                            device_noise: bool = True, model_izh: int = 2) -> int:
+                            device_noise: bool = True, model_izh: int = 2, random_w=True) -> int:
     """One pulse-coupled Izhikevich network (the recipe of izhikevich_pulse,
     with the fixed-out-degree generator for its 100 distinct targets) added
     to `net` as its own population; several calls build a batch that steps
     as one network.  Device noise draws the thalamic input of
-    izhikevich_input on the GPU (same hash, counter i + step * n)."""
+    izhikevich_input on the GPU (same hash, counter i + step * n).
+    random_w = 8 draws the weights' U on the 1/256 grid (exact ring sums)."""
     n_exc = n * 4 // 5
     a, b, c, d = izhikevich_params(n, n_exc, seed)
     pop = net.add_population(model_izh, n)
@@ -220,9 +231,9 @@ def add_izhikevich_instance(net, n: int, seed: int, k_out: int = 100, device_edg
     net.set_state(pop, 1, (b * np.float32(-65.0)).astype(np.float32))
     k = min(k_out, n - 1)
     if device_edges:
-        net.connect_fixed_outdegree(pop, pop, k, seed, True, n_exc, 0.5, -1.0, True, 1)
+        net.connect_fixed_outdegree(pop, pop, k, seed, True, n_exc, 0.5, -1.0, random_w, 1)
     else:
-        pre, post, w = fixed_outdegree_edges(n, k, seed, n_exc, 0.5, -1.0)
+        pre, post, w = fixed_outdegree_edges(n, k, seed, n_exc, 0.5, -1.0, random_w=random_w)
         net.connect(pop, pre, pop, post, w, np.ones(pre.size, np.uint8))
     if device_noise:
         net.set_noise(pop, seed, 5.0, 2.0, split=n_exc, stream=IZH_STREAM_NOISE, stride=n)
@@ -335,6 +346,12 @@ def build_lif(net, spec: dict, model_lif: int = 1, device_generator: bool = True
 # ---------------------------------------------------------------------------
 # Kuramoto sweep (the oscillator half of the batched uneven sweep)
 # ---------------------------------------------------------------------------
+def izh_sweep_sizes(n_inst: int = 1024, n_min: int = 500, n_max: int = 200_000, seed: int = 7) -> np.ndarray:
+    """Sizes of the sweep's Izhikevich instances: N log-uniform in [n_min, n_max]."""
+    u = uniform01(seed, 1, np.arange(n_inst, dtype=np.uint64))
+    return np.floor(np.exp(np.log(n_min) + u * (np.log(n_max + 1) - np.log(n_min)))).astype(np.int64)
+
+
 def kuramoto_sweep(n_inst: int = 1024, n_min: int = 256, n_max: int = 65536, k_max: float = 4.0,
                    gamma: float = 0.5, seed: int = 0) -> dict:
     """``n_inst`` all-to-all Kuramoto populations: N log-uniform in

@@ -72,6 +72,16 @@ int sg_net_destroy(sg_net *net);                /* Drop for Network */
    pipeline gave up a wait on the device (its events are then incomplete);
    the condition is reported once. */
 int sg_synchronize(sg_net *net);
+/* No counterpart in the reference.  Tunes the pre-centric scatter's
+   schedule (its shared-memory stage ring: stages x synapses per stage, and
+   blocks per SM) on the network's own next steps: each candidate runs
+   `steps` steps (after a warm-up chunk), timed on the device, and the
+   fastest is kept.  Every schedule gives the same results, so these are
+   ordinary simulation steps (the step counter advances).  Reports the
+   per-step time of the fixed schedule and of the chosen one.  On the ordered
+   path there is nothing to tune (times 0). */
+int sg_autotune(sg_net *net, uint32_t steps, float *fixed_ms, float *best_ms, int *best_variant,
+                uint32_t *best_bps);
 /* Test hook (no reference counterpart): on != 0 makes the pre-centric
    scatter's producer stop feeding its consumers, whose waits then run out
    (~1 s per step) and set the device error that sg_synchronize reports. */
@@ -167,6 +177,22 @@ int sg_register_expone(sg_net *net, float tau_decay, float erev, float dt, uint3
 #define SG_KIN_ALPHA 2
 #define SG_KIN_EXPTHREE 3
 int sg_register_kinetics(sg_net *net, int kind, const float *params, float erev, float dt, uint32_t *out_id);
+
+/* SynapticBrain receptor kinetics (pillars-connectome/src/synaptic.rs:23-130;
+   P/kernels/synapse/{kinetics,receptor}.rs): call before any connect.  The
+   syn_types of later synapses are receptor codes (0 AMPA, 1 NMDA, 2 GABA_A,
+   3 GABA_B, 4 nAChR, 5 GluCl, 6 mAChR; others AMPA) and their delays are
+   ignored.  Each step decays the seven conductances by fast_exp(-dt/tau),
+   adds I_syn = sum g_eff (E_rev - V) (NMDA Mg-blocked, pre-step V) to the
+   step's external input (inject_current, bias, noise), steps the neurons,
+   then every spike jumps its targets' conductances in (pre ascending, row)
+   order: SynapticBrain::step.  No kinetic profiles, Poisson sources, STDP,
+   short-term plasticity or learning alongside; sg_clear_rings zeroes the
+   conductances too. */
+int sg_set_receptor_kinetics(sg_net *net, float dt);
+/* SynapticBrain::kinetics / set_kinetics: g[r * total + i], r = receptor code */
+int sg_receptor_read(sg_net *net, float *g);
+int sg_receptor_write(sg_net *net, const float *g);
 
 /* Network::add_poisson_source(rate_hz, dt_ms, seed) -> id, core.rs:288-312 */
 int sg_poisson_add(sg_net *net, float rate_hz, float dt_ms, uint32_t seed, uint32_t *out_id);

@@ -62,6 +62,12 @@ def lib():
             "or_tm_sequence": (i32, [f32, f32, f32, i32, f32, vp, u32, vp]),
             "or_register_expone": (i32, [vp, f32, f32, f32]),
             "or_register_kinetics": (i32, [vp, i32, vp, f32, f32]),
+            "or_set_receptor_kinetics": (i32, [vp, f32]),
+            "or_receptor_read": (i32, [vp, vp]),
+            "or_receptor_write": (i32, [vp, vp]),
+            "or_receptor_factors": (i32, [f32, vp]),
+            "or_receptor_currents": (i32, [u32, vp, vp, vp]),
+            "or_nmda_mg_block": (f32, [f32]),
             "or_pop_add_external": (i32, [vp, u32]),
             "or_step_begin": (i32, [vp]),
             "or_set_external_spikes": (i32, [vp, i32, vp, u32]),
@@ -201,6 +207,21 @@ class Network:
 
     def register_expone(self, tau_decay, erev, dt) -> int:
         return _chk(lib().or_register_expone(self._h, tau_decay, erev, dt))
+
+    def set_receptor_kinetics(self, dt):
+        """SynapticBrain receptor kinetics: syn_types are receptor codes."""
+        _chk(lib().or_set_receptor_kinetics(self._h, dt))
+
+    def receptor_conductances(self) -> np.ndarray:
+        out = np.empty((7, self.total_neurons), np.float32)
+        _chk(lib().or_receptor_read(self._h, _p(out)))
+        return out
+
+    def set_receptor_conductances(self, g):
+        g = np.ascontiguousarray(g, np.float32)
+        if g.shape != (7, self.total_neurons):
+            raise ValueError("conductances must be [7][total neurons]")
+        _chk(lib().or_receptor_write(self._h, _p(g)))
 
     def add_external_population(self, n):
         pid = _chk(lib().or_pop_add_external(self._h, n))
@@ -410,6 +431,24 @@ def sg_expf(x: float) -> float:
 
 def sg_logf(x: float) -> float:
     return float(lib().or_sg_logf(float(x)))
+
+
+def receptor_factors(dt: float) -> np.ndarray:
+    out = np.empty(7, np.float32)
+    _chk(lib().or_receptor_factors(dt, _p(out)))
+    return out
+
+
+def receptor_currents(g, v) -> np.ndarray:
+    g = np.ascontiguousarray(g, np.float32)
+    v = np.ascontiguousarray(v, np.float32)
+    out = np.empty(v.size, np.float32)
+    _chk(lib().or_receptor_currents(v.size, _p(g), _p(v), _p(out)))
+    return out
+
+
+def nmda_mg_block(v: float) -> float:
+    return lib().or_nmda_mg_block(v)
 
 
 def poisson_spike(seed, stream, step, p) -> bool:

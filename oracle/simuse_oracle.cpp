@@ -178,6 +178,44 @@ template <> struct M<double> {
   static double fma(double a, double b, double c) { return std::fma(a, b, c); }
 };
 
+// Receptor kinetics of SynapticBrain (pillars-connectome/src/synaptic.rs).
+// Decay time constant (ms) and reversal potential (mV) per receptor code,
+// P/kernels/synapse/receptor.rs:71-100: 0 AMPA, 1 NMDA, 2 GABA_A, 3 GABA_B,
+// 4 nAChR, 5 GluCl, 6 mAChR; any other code is AMPA (:103-115).
+constexpr int kReceptors = 7;
+constexpr float kRecTau[kReceptors] = {2.0f, 50.0f, 10.0f, 200.0f, 3.0f, 5.0f, 150.0f};
+constexpr float kRecErev[kReceptors] = {0.0f, 0.0f, -65.0f, -90.0f, 0.0f, -70.0f, -90.0f};
+inline int receptor_of(uint8_t code) { return code < kReceptors ? code : 0; }
+
+// P/kernels/synapse/receptor.rs:126-131 nmda_mg_block:
+// 1 / (1 + 0.33 exp(clamp(-0.06 v, -10, 10))) with the project's fast_exp
+// (the SIMD form of :135-143 gives the same bits).
+template <typename T> T nmda_mg_block(T v) {
+  T a = (T)-0.06f * v;
+  if (a < (T)-10.0f) a = (T)-10.0f;
+  if (a > (T)10.0f) a = (T)10.0f;
+  return (T)1.0f / ((T)1.0f + (T)0.33f * M<T>::fexp(a));
+}
+
+// DecayFactors::new(dt), P/kernels/synapse/kinetics.rs:27-38: fast_exp(-dt/tau).
+template <typename T> void receptor_factors(float dt, T f[kReceptors]) {
+  for (int r = 0; r < kReceptors; ++r) f[r] = M<T>::fexp(-(T)dt / (T)kRecTau[r]);
+}
+
+// One neuron of SynapticKinetics::compute_currents, P/kernels/synapse/
+// kinetics.rs:159-206: from zero, over the receptors in code order,
+// cur += g_eff (E_rev - v), g_eff = g * mg_block(v) for NMDA, g otherwise.
+// g[r] is the neuron's conductance of receptor r.
+template <typename T> T receptor_current(const T g[kReceptors], T v) {
+  const T b = nmda_mg_block(v);
+  T cur = (T)0;
+  for (int r = 0; r < kReceptors; ++r) {
+    const T ge = r == 1 ? g[r] * b : g[r];
+    cur += ge * ((T)kRecErev[r] - v);
+  }
+  return cur;
+}
+
 // P/api/net/network/sources.rs:5-14
 bool poisson_spike(uint32_t seed, uint32_t stream, uint64_t step, float p) {
   uint64_t z = ((uint64_t)seed << 32) | (uint64_t)stream;
@@ -522,6 +560,12 @@ template <typename T> struct Net : NetBase {
   std::vector<uint32_t> tm_last;    //   and the step of its last spike
   std::vector<Kin> kin;
   std::vector<T> g;     // [nk][N] kinetic conductances
+  // SynapticBrain mode: the edges' syn_types are receptor codes, every
+  // spike jumps the conductance rg[receptor][post] at once (no delay), and
+  // each step decays them and adds their ohmic current to the input
+  bool receptor = false;
+  float rec_dt = 0.0f;
+  std::vector<T> rg;    // [7][N]
   std::vector<T> ring;  // [1 + nk][32][N]
   std::vector<Src<T>> srcs;
   uint64_t step = 0, events = 0;
@@ -612,6 +656,7 @@ template <typename T> void alloc_runtime(Net<T> &net) {
   }
   net.ring.assign((1 + net.kin.size()) * kSlots * N, (T)0);
   net.g.assign(net.kin.size() * 3 * N, (T)0);  // up to three state arrays per profile
+  if (net.receptor) net.rg.assign((size_t)kReceptors * N, (T)0);
   net.i_in.assign(N, (T)0);
   net.v_scr.assign(N, (T)0);
   net.scratch.assign(N, (T)0);
@@ -711,6 +756,29 @@ template <typename T> void net_step_begin(Net<T> &net) {
       }
     }
   }
+  // 2c. SynapticBrain::step (pillars-connectome/src/synaptic.rs:94-112):
+  // decay every conductance by its factor (P/kernels/synapse/kinetics.rs:
+  // 112-147; factors fast_exp(-dt/tau), :27-38), then I_syn = sum over the
+  // receptors in code order of g_eff (E_rev - V) from zero, NMDA's g scaled
+  // by the Mg block of the pre-step V (:159-206), and i_in = I_syn + the
+  // external input (here the step's injected current).
+  if (net.receptor) {
+    T f[kReceptors];
+    receptor_factors(net.rec_dt, f);
+    for (size_t p = 0; p < net.pops.size(); ++p) {
+      auto &pop = net.pops[p];
+      for (uint32_t i = 0; i < pop.n; ++i) net.v_scr[net.offsets[p] + i] = pop.state[i];
+    }
+    for (size_t i = 0; i < N; ++i) {
+      T g[kReceptors];
+      for (int r = 0; r < kReceptors; ++r) {
+        T &gr = net.rg[(size_t)r * N + i];
+        gr = gr * f[r];
+        g[r] = gr;
+      }
+      net.i_in[i] = receptor_current(g, net.v_scr[i]) + net.i_in[i];
+    }
+  }
   // 3. populations (P/core/exec/population.rs:284-465).  dt is param column 0
   // of neuron 0, broadcast to the population (:307,:361).
   for (size_t p = 0; p < net.pops.size(); ++p) {
@@ -750,6 +818,10 @@ template <typename T> void net_step_end(Net<T> &net) {
   // sequentially, which is the same per-cell order).
   const uint64_t s = net.step;
   auto deliver = [&](uint32_t post, uint8_t dl, uint8_t st, T wv) {
+    if (net.receptor) {  // synaptic.rs:114-127: jump the receptor's conductance now
+      net.rg[(size_t)receptor_of(st) * N + post] += wv;
+      return;
+    }
     uint32_t ts = (uint32_t)((s + std::max<uint32_t>(dl, 1)) % kSlots);
     net.ring_slot(st, ts)[post] += wv;
   };
@@ -1401,6 +1473,58 @@ int or_register_expone(or_net *h, float tau_decay, float erev, float dt) {
   return id;
 }
 
+// SynapticBrain::from_sparse_graph(graph, receptor_types, dt)
+// (pillars-connectome/src/synaptic.rs:53-63) on this network: the edges'
+// syn_types become receptor codes (code >= 7 is AMPA), delays are ignored
+// (a spike jumps its targets' conductances at once), DecayFactors::new(dt).
+int or_set_receptor_kinetics(or_net *h, float dt) {
+  if (!(dt > 0) || !std::isfinite(dt)) return fail("receptor kinetics: dt must be finite and > 0");
+  DISPATCH(h, {
+    if (net.built) return fail("receptor kinetics must be set before build()");
+    net.receptor = true;
+    net.rec_dt = dt;
+  });
+  return 0;
+}
+
+// SynapticBrain::kinetics / set_kinetics (synaptic.rs:72-80): the seven
+// conductance arrays, [7][total] in receptor-code order.
+int or_receptor_read(or_net *h, float *g) {
+  DISPATCH(h, {
+    if (!net.built || !net.receptor) return fail("receptor kinetics are not on");
+    for (size_t k = 0; k < net.rg.size(); ++k) g[k] = (float)net.rg[k];
+  });
+  return 0;
+}
+
+int or_receptor_factors(float dt, float *f) {
+  if (!(dt > 0) || !std::isfinite(dt)) return fail("receptor kinetics: dt must be finite and > 0");
+  receptor_factors(dt, f);
+  return 0;
+}
+
+// I_out[i] = sum over receptors of g_eff (E_rev - v[i]) for n neurons with
+// conductances g[r * n + i] (SynapticKinetics::compute_currents into a zeroed
+// output).
+int or_receptor_currents(uint32_t n, const float *g, const float *v, float *i_out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    float gi[kReceptors];
+    for (int r = 0; r < kReceptors; ++r) gi[r] = g[(size_t)r * n + i];
+    i_out[i] = receptor_current(gi, v[i]);
+  }
+  return 0;
+}
+
+float or_nmda_mg_block(float v) { return nmda_mg_block(v); }
+
+int or_receptor_write(or_net *h, const float *g) {
+  DISPATCH(h, {
+    if (!net.built || !net.receptor) return fail("receptor kinetics are not on");
+    for (size_t k = 0; k < net.rg.size(); ++k) net.rg[k] = g[k];
+  });
+  return 0;
+}
+
 // P/api/net/network/core.rs:288-312
 int or_poisson_add(or_net *h, float rate_hz, float dt_ms, uint32_t seed) {
   if (!std::isfinite(rate_hz) || rate_hz < 0) return fail("add_poisson_source: rate_hz must be finite and >= 0");
@@ -1582,8 +1706,15 @@ int or_build_fixed_indegree(or_net *h, int from, int to, uint32_t k_in, uint64_t
 int or_build(or_net *h) {
   DISPATCH(h, {
     if (net.built) return fail("Network::build() called twice");
-    for (auto &e : net.edges)
-      if (e.st > net.kin.size()) return fail("Network::build: syn_type exceeds registered kinetics");
+    if (net.receptor) {
+      if (!net.kin.empty() || !net.srcs.empty() || !net.tm.empty() || net.stdp.on)
+        return fail("receptor kinetics: no kinetic profiles, Poisson sources, short-term or pair-STDP plasticity");
+      for (auto &e : net.edges)
+        if (e.flags & 1) return fail("receptor kinetics: no pair-STDP synapses");
+    } else {
+      for (auto &e : net.edges)
+        if (e.st > net.kin.size()) return fail("Network::build: syn_type exceeds registered kinetics");
+    }
     for (auto &s : net.srcs)
       for (auto st : s.st)
         if (st > net.kin.size()) return fail("Network::build: Poisson-source syn_type exceeds registered kinetics");

@@ -50,6 +50,17 @@ int or_register_plasticity(or_net *net, float u0, float tau_rec, int facilitatio
 int or_tm_sequence(float u0, float a_rec, float a_fac, int facilitation, float w, const uint64_t *steps,
                    uint32_t n, float *out);
 int or_register_expone(or_net *net, float tau_decay, float erev, float dt);
+/* SynapticBrain receptor kinetics (pillars-connectome/src/synaptic.rs):
+   syn_types are receptor codes 0..6 (others AMPA), delays ignored; the seven
+   conductances [7][total] read and written in receptor-code order */
+int or_set_receptor_kinetics(or_net *net, float dt);
+int or_receptor_read(or_net *net, float *g);
+int or_receptor_write(or_net *net, const float *g);
+/* the receptor kinetics' parts alone: DecayFactors::new(dt) in code order,
+   compute_currents of n neurons (g [7][n]) into i_out, nmda_mg_block(v) */
+int or_receptor_factors(float dt, float *f);
+int or_receptor_currents(uint32_t n, const float *g, const float *v, float *i_out);
+float or_nmda_mg_block(float v);
 /* kind 0 ExpOne {tau_decay}, 1 ExpTwo {tau_rise, tau_decay}, 2 Alpha {tau},
    3 ExpThree {tau_rise, tau_decay1, tau_decay2, gbase1, gbase2} */
 int or_register_kinetics(or_net *net, int kind, const float *params, float erev, float dt);

@@ -115,3 +115,29 @@ def test_exact_ring_readback_between_steps():
         assert np.array_equal(g.ring(0).view(np.uint32), c.ring(0).view(np.uint32))
     assert np.array_equal(g.state(gp, 0).view(np.uint32), c.state(cp, 0).view(np.uint32))
     g.close()
+
+
+def test_autotuned_schedule_keeps_the_oracle_bits():
+    """sg_autotune runs the network's next steps under every candidate
+    schedule of the pre-centric scatter and keeps the fastest; the steps are
+    ordinary simulation steps and every schedule gives the same bits."""
+    g = sg.Network(0)
+    gp = _balanced(g)
+    g.build()
+    c = O.Network(0)
+    cp = _balanced(c)
+    c.build()
+    rep = g.autotune(steps=20)
+    assert rep["fixed_ms_per_step"] > 0 and rep["tuned_ms_per_step"] > 0
+    assert rep["tuned_ms_per_step"] <= rep["fixed_ms_per_step"]
+    done = g.step_counter            # 12 candidates x (20 warm-up + 20 timed) steps
+    assert done == 12 * 40
+    c.step(done)
+    g.enable_raster(50)
+    g.step(50)
+    rg = g.read_raster()
+    rc = c.step(50, record=True)
+    assert np.array_equal(rg, rc)
+    assert np.array_equal(g.state(gp, 0).view(np.uint32), c.state(cp, 0).view(np.uint32))
+    assert g.events_total == c.events
+    g.close()

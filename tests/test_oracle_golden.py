@@ -254,3 +254,79 @@ def test_sg_logf_is_correctly_rounded():
     assert math.isnan(O.sg_logf(-1.0))
     assert O.sg_logf(math.inf) == math.inf
     assert O.sg_logf(1e-40) == float(np.float32(math.log(np.float32(1e-40))))
+
+
+def test_receptor_kinetics_known_answers():
+    """The reference's receptor-kinetics tests
+    (crates/SiMuse/crates/pillars/src/kernels/synapse/tests.rs) on the
+    oracle's restatement of DecayFactors, decay_all and compute_currents,
+    with the Mg-block values of the receptor.rs doc comment."""
+    assert abs(O.receptor_factors(0.5)[0] - 0.7788) < 1e-3            # test_decay_factors_precision
+    f = O.receptor_factors(2.0)                                          # test_decay_all_exponential
+    assert abs(np.float32(1.0) * f[0] - 0.3679) < 1e-3
+    assert abs(np.float32(2.0) * f[2] - 1.6375) < 1e-3
+    g = np.zeros((7, 2), np.float32)                                     # test_compute_currents_ohmic_direction
+    g[0, 0], g[2, 1] = 0.1, 0.2
+    i = O.receptor_currents(g, [-65.0, -65.0])
+    assert abs(i[0] - 6.5) < 0.01 and abs(i[1]) < 0.01
+    v = np.array([-80.0, -65.0, -40.0, -20.0, 0.0, 20.0, 40.0], np.float32)   # test_nmda_mg_block_voltage_profile
+    g = np.zeros((7, 7), np.float32)
+    g[1] = 1.0
+    i = O.receptor_currents(g, v)
+    assert i[0] < 5.0 and abs(i[4]) < 1.0 and i[5] < -5.0
+    g = np.zeros((7, 2), np.float32)                                     # test_gabab_and_machr_inhibitory
+    g[3, 0], g[6, 1] = 1.0, 1.0
+    i = O.receptor_currents(g, [-65.0, -65.0])
+    assert abs(i[0] + 25.0) < 0.1 and abs(i[1] + 25.0) < 0.1
+    n = 13                                                               # test_simd_tail_consistent
+    k = np.arange(n, dtype=np.float32) + 1.0
+    g = np.zeros((7, n), np.float32)
+    g[0], g[1], g[2], g[4] = 0.1 * k, 0.05 * k, 0.02, 0.01
+    v = -70.0 + np.arange(n, dtype=np.float32)
+    i = O.receptor_currents(g, v)
+    for idx in (0, 4, 12):
+        b = O.nmda_mg_block(float(v[idx]))
+        want = (0.1 * (idx + 1) * (0.0 - v[idx]) + 0.05 * (idx + 1) * b * (0.0 - v[idx])
+                + 0.02 * (-65.0 - v[idx]) + 0.01 * (0.0 - v[idx]))
+        assert abs(i[idx] - want) < 1e-4, idx
+    # the formula 1 / (1 + 0.33 exp(-0.06 v)): 0.058 at rest (the doc comment
+    # of receptor.rs rounds it to "0.02"), 0.95 at the spike peak
+    for vv in (-65.0, 30.0, -200.0, 200.0):
+        want = 1.0 / (1.0 + 0.33 * np.exp(np.clip(-0.06 * vv, -10, 10)))
+        assert abs(O.nmda_mg_block(vv) - want) < 1e-5 * max(1.0, want), vv
+    assert abs(O.nmda_mg_block(30.0) - 0.95) < 0.01
+
+
+def test_receptor_types_from_nt_signs():
+    """test_build_receptor_types_csr (kernels/synapse/tests.rs): rows of a
+    +1 and a -1 neuron give AMPA, AMPA, GABA_A, GABA_A; the insect phenotype
+    and the FlyWire table (pillars-connectome/src/data.rs:44-59, 465-523)."""
+    from simuse_b200.synaptic import receptor_types_flywire, receptor_types_from_nt
+    assert receptor_types_from_nt([0, 2, 4], [1.0, -1.0]).tolist() == [0, 0, 2, 2]
+    assert receptor_types_from_nt([0, 2, 4], [1.0, -1.0], "insect").tolist() == [4, 4, 5, 5]
+    assert receptor_types_from_nt([0, 1, 3], [-1.0]).tolist() == [2, 0, 0]     # missing NT: +1
+    assert receptor_types_flywire([0, 1, 2, 3, 4, 5], [1.0, -1.0, 2.0, -2.0, 0.0]).tolist() == [4, 2, 5, 6, 2]
+
+
+def test_receptor_network_step_order_on_the_oracle():
+    """SynapticBrain::step on the oracle network: a spike at step t jumps
+    its target's conductance, which is decayed once before it drives the
+    target at step t + 1 (synaptic.rs:94-130)."""
+    net = O.Network(0)
+    net.set_receptor_kinetics(1.0)
+    pop = net.add_population(2, 2)           # Izhikevich
+    for col, v in enumerate((1.0, 0.02, 0.2, -65.0, 8.0, 0.0, 30.0)):
+        net.fill_param(pop, col, v)
+    net.fill_state(pop, 0, -65.0)
+    net.fill_state(pop, 1, -13.0)
+    net.connect(pop, [0], pop, [1], [0.5], [7], syn_types=[4])   # nAChR, delay ignored
+    net.build()
+    net.inject_current(pop, np.array([0], np.uint32), np.array([100.0], np.float32))
+    net.step(1)
+    assert net.spikes(pop).tolist() == [1, 0]
+    g = net.receptor_conductances()
+    assert g[4, 1] == np.float32(0.5) and np.count_nonzero(g) == 1
+    net.step(1)
+    assert net.spikes(pop)[0] == 0
+    f = O.receptor_factors(1.0)
+    assert net.receptor_conductances()[4, 1] == np.float32(0.5) * f[4]
