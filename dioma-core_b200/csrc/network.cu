@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -264,6 +265,15 @@ struct sg_net {
   DBuf<unsigned long long> rr_cnt, rr_off;
   DBuf<uint8_t> rr_temp;
   DBuf<uint32_t> rr_step, rr_idx, rr_pd, rr_pg;
+  DBuf<uint32_t> rr_counts;  // spikes per device neuron over every read since the raster was enabled
+  // a staged read (sg_raster_stage / sg_raster_fetch): steps [rst_t0, rst_t1)
+  // compacted on rstream after the steps that wrote them; the network's
+  // later steps wait for that compaction (rdone)
+  cudaStream_t rstream = nullptr;
+  cudaEvent_t rev = nullptr, rdone = nullptr;
+  unsigned long long *rst_total = nullptr;  // pinned host word: the staged batch's spike count
+  bool rstaged = false;
+  uint64_t rst_t0 = 0, rst_nb = 0, rst_nw = 0;
   // neuron work table: per population its kernel arguments, per model the
   // (population, block) pairs its launch covers
   DBuf<PopArgs> d_pop_tab;
@@ -297,7 +307,7 @@ struct sg_pool {
   std::vector<PopArgs> h_pops;
   std::vector<uint4> h_map;  // (member, population of h_pops, block), grouped by model
   uint32_t model_off[5] = {}, model_cnt[5] = {};
-  bool full = false;
+  bool full[5] = {};  // per model: some member needs the full neuron kernel
   DBuf<StepArgs> d_nets;
   DBuf<PopArgs> d_pops;
   DBuf<uint4> d_map;
@@ -724,9 +734,15 @@ __global__ void raster_count_kernel(const uint32_t *bits, uint32_t cap, uint32_t
   }
 }
 
+// Writes the (step, global index) pairs at their scanned offsets and adds
+// one to counts[device index] per spike; does nothing when the total
+// (block_off[nb]) exceeds out_cap (the caller grows the outputs and runs it
+// again).
 __global__ void raster_write_kernel(const uint32_t *bits, uint32_t cap, uint32_t words, uint64_t t0, uint64_t nw,
-                                    const unsigned long long *block_off, const uint32_t *pop_dev, const uint32_t *pop_glob,
-                                    int npops, uint32_t *out_step, uint32_t *out_idx) {
+                                    const unsigned long long *block_off, uint64_t nb, uint64_t out_cap,
+                                    const uint32_t *pop_dev, const uint32_t *pop_glob, int npops, uint32_t *out_step,
+                                    uint32_t *out_idx, uint32_t *counts) {
+  if (block_off[nb] > out_cap) return;
   // each thread owns 4 consecutive words of the block's 1024
   __shared__ uint32_t warp_tot[32];
   const uint64_t w0 = (uint64_t)blockIdx.x * kRasterWordsPerBlock + threadIdx.x * 4;
@@ -773,6 +789,7 @@ __global__ void raster_write_kernel(const uint32_t *bits, uint32_t cap, uint32_t
       m &= m - 1;
       out_step[pos] = step;
       out_idx[pos] = gbase + b;
+      if (counts != nullptr) atomicAdd(counts + dbase + b, 1u);
       ++pos;
     }
   }
@@ -1667,17 +1684,19 @@ template <int M, bool FULL> void launch_neuron_form(sg_net *net, const StepArgs 
 
 // The lean neuron kernel serves steps without kinetic synapses, input
 // noise, neuron statistics, pair STDP or learning.
-bool needs_full_neuron_kernel(const sg_net *net, const StepArgs &a) {
+// The full neuron kernel (kinetics, receptors, noise, statistics, STDP,
+// learning) for the populations of model `model`, or the lean one.
+bool needs_full_neuron_kernel(const sg_net *net, const StepArgs &a, int model) {
   if (a.n_kin || a.receptor || a.ns_count != nullptr || a.stdp || a.learn) return true;
   for (const auto &p : net->pops)
-    if (p.noise) return true;
+    if (p.model == model && p.noise) return true;
   return false;
 }
 
 template <int M> void launch_neuron(sg_net *net, const StepArgs &a) {
   const uint32_t nb = net->model_blk_cnt[M];
   if (nb == 0) return;
-  if (needs_full_neuron_kernel(net, a)) launch_neuron_form<M, true>(net, a, nb);
+  if (needs_full_neuron_kernel(net, a, M)) launch_neuron_form<M, true>(net, a, nb);
   else launch_neuron_form<M, false>(net, a, nb);
 }
 
@@ -1868,6 +1887,13 @@ int sg_net_destroy(sg_net *net) {
     cudaStreamSynchronize(net->stream);
     drop_graph(net);
     for (auto e : net->prof_ev) cudaEventDestroy(e);
+    if (net->rstream) {
+      cudaStreamSynchronize(net->rstream);
+      cudaStreamDestroy(net->rstream);
+      cudaEventDestroy(net->rev);
+      cudaEventDestroy(net->rdone);
+      cudaFreeHost(net->rst_total);
+    }
     cudaStream_t s = net->stream;
     delete net;  // DBufs free their memory
     cudaStreamDestroy(s);
@@ -2709,6 +2735,7 @@ int sg_autotune(sg_net *net, uint32_t steps, float *fixed_ms, float *best_ms, in
     int bv = 0;
     uint32_t bb = kRedBlocksPerSM;
     if (net->red) {
+      const bool log = std::getenv("SG_AUTOTUNE_LOG") != nullptr;  // each candidate's time on stderr
       cudaEvent_t e0, e1;
       SG_CUDA(cudaEventCreate(&e0));
       SG_CUDA(cudaEventCreate(&e1));
@@ -2726,6 +2753,7 @@ int sg_autotune(sg_net *net, uint32_t steps, float *fixed_ms, float *best_ms, in
           float ms = 0.0f;
           SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
           ms /= (float)steps;
+          if (log) std::fprintf(stderr, "sg_autotune: variant %d, %u blocks per SM: %.4f ms per step\n", v, bps, ms);
           if (v == 0 && bps == kRedBlocksPerSM) fixed = ms;
           if (first || ms < best) {
             best = ms;
@@ -2832,6 +2860,7 @@ int sg_raster_enable(sg_net *net, uint32_t cap) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(net->built, SG_E_STATE, "raster recording needs a built network");
+    SG_REQUIRE(!net->rstaged, SG_E_STATE, "a staged raster read is not fetched yet");
     DevGuard g(net->device);
     SG_CUDA(cudaStreamSynchronize(net->stream));
     drop_graph(net);
@@ -2839,6 +2868,9 @@ int sg_raster_enable(sg_net *net, uint32_t cap) {
     if (cap) {
       net->d_raster.alloc((size_t)cap * (net->Nd / 32));
       net->d_raster.zero(net->stream);
+      net->rr_counts.ensure(std::max<uint32_t>(net->Nd, 1));
+      SG_CUDA(cudaMemsetAsync(net->rr_counts.p, 0, (size_t)std::max<uint32_t>(net->Nd, 1) * 4, net->stream));
+      SG_CUDA(cudaStreamSynchronize(net->stream));
     } else {
       net->d_raster.release();
     }
@@ -2878,19 +2910,65 @@ int sg_raster_read(sg_net *net, uint8_t *out, uint64_t cap_bytes, uint32_t *n_st
   });
 }
 
+namespace {
+
+// Queues on stream s the compaction of the raster steps [t0, t0 + k): per
+// block spike counts and their exclusive scan (off[nb] = the total).
+void enqueue_raster_count(sg_net *net, cudaStream_t s, uint64_t t0, uint64_t nw, uint64_t nb) {
+  const uint32_t words = net->Nd / 32;
+  auto &cnt = net->rr_cnt;
+  auto &off = net->rr_off;
+  cnt.ensure(nb + 1);
+  off.ensure(nb + 1);
+  SG_CUDA(cudaMemsetAsync(cnt.p, 0, (nb + 1) * sizeof(unsigned long long), s));
+  raster_count_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, t0, nw, cnt.p);
+  size_t tb = 0;
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, off.p, (int64_t)nb + 1, s));
+  auto &temp = net->rr_temp;
+  temp.ensure(std::max<size_t>(tb, 1));
+  SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, off.p, (int64_t)nb + 1, s));
+}
+
+// The population tables of the write kernel (device offset -> global offset).
+void upload_raster_pops(sg_net *net, cudaStream_t s) {
+  std::vector<uint32_t> pd, pgl;
+  for (size_t p = 0; p < net->pops.size(); ++p) {
+    pd.push_back(net->pops[p].dev_off);
+    pgl.push_back(net->offsets[p]);
+  }
+  net->rr_pd.ensure(pd.size());
+  net->rr_pg.ensure(pgl.size());
+  SG_CUDA(cudaMemcpyAsync(net->rr_pd.p, pd.data(), pd.size() * 4, cudaMemcpyHostToDevice, s));
+  SG_CUDA(cudaMemcpyAsync(net->rr_pg.p, pgl.data(), pgl.size() * 4, cudaMemcpyHostToDevice, s));
+  SG_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+}
+
+// Queues the write of the scanned batch into rr_step / rr_idx (which hold
+// `out_cap` pairs) and the per-neuron counts; skipped on the device when the
+// total exceeds out_cap.
+void enqueue_raster_write(sg_net *net, cudaStream_t s, uint64_t t0, uint64_t nw, uint64_t nb, uint64_t out_cap) {
+  raster_write_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, net->Nd / 32, t0, nw,
+                                                   net->rr_off.p, nb, out_cap, net->rr_pd.p, net->rr_pg.p,
+                                                   (int)net->pops.size(), net->rr_step.p, net->rr_idx.p,
+                                                   net->rr_counts.p);
+  SG_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
 int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap, uint64_t *n_out) {
   NET_CHECK(net);
   return run([&] {
     SG_REQUIRE(net->raster_cap > 0, SG_E_STATE, "raster recording is not enabled");
     SG_REQUIRE(n_out, SG_E_INVALID, "null output");
+    SG_REQUIRE(!net->rstaged, SG_E_STATE, "a staged raster read is not fetched yet");
     DevGuard g(net->device);
     cudaStream_t s = net->stream;
     const uint64_t k = net->host_step - net->raster_read_step;
     SG_REQUIRE(k <= net->raster_cap, SG_E_OVERFLOW,
                "raster overflow: " + std::to_string(k) + " steps since the last read, capacity " +
                    std::to_string(net->raster_cap));
-    const uint32_t words = net->Nd / 32;
-    const uint64_t nw = k * words;
+    const uint64_t nw = k * (net->Nd / 32);
     const uint64_t nb = (nw + kRasterWordsPerBlock - 1) / kRasterWordsPerBlock;
     *n_out = 0;
     if (nb == 0) {
@@ -2899,20 +2977,9 @@ int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t 
     }
     // work buffers live in the network and only grow: no allocation in a
     // steady read loop
-    auto &cnt = net->rr_cnt;
-    auto &off = net->rr_off;
-    cnt.ensure(nb + 1);
-    off.ensure(nb + 1);
-    SG_CUDA(cudaMemsetAsync(cnt.p, 0, (nb + 1) * sizeof(unsigned long long), s));
-    raster_count_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, net->raster_read_step, nw,
-                                                     cnt.p);
-    size_t tb = 0;
-    SG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, off.p, (int64_t)nb + 1, s));
-    auto &temp = net->rr_temp;
-    temp.ensure(std::max<size_t>(tb, 1));
-    SG_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt.p, off.p, (int64_t)nb + 1, s));
+    enqueue_raster_count(net, s, net->raster_read_step, nw, nb);
     unsigned long long total = 0;
-    SG_CUDA(cudaMemcpyAsync(&total, off.p + nb, 8, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaMemcpyAsync(&total, net->rr_off.p + nb, 8, cudaMemcpyDeviceToHost, s));
     SG_CUDA(cudaStreamSynchronize(s));
     *n_out = total;
     SG_REQUIRE(total <= cap, SG_E_INVALID, "output buffer too small: " + std::to_string(total) + " spikes");
@@ -2920,28 +2987,110 @@ int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t 
       net->raster_read_step = net->host_step;
       return;
     }
-    std::vector<uint32_t> pd, pgl;
-    for (size_t p = 0; p < net->pops.size(); ++p) {
-      pd.push_back(net->pops[p].dev_off);
-      pgl.push_back(net->offsets[p]);
-    }
-    auto &d_pd = net->rr_pd;
-    auto &d_pg = net->rr_pg;
-    auto &o_step = net->rr_step;
-    auto &o_idx = net->rr_idx;
-    d_pd.ensure(pd.size());
-    d_pg.ensure(pgl.size());
-    SG_CUDA(cudaMemcpyAsync(d_pd.p, pd.data(), pd.size() * 4, cudaMemcpyHostToDevice, s));
-    SG_CUDA(cudaMemcpyAsync(d_pg.p, pgl.data(), pgl.size() * 4, cudaMemcpyHostToDevice, s));
-    o_step.ensure(total);
-    o_idx.ensure(total);
-    raster_write_kernel<<<(unsigned)nb, 256, 0, s>>>(net->d_raster.p, net->raster_cap, words, net->raster_read_step, nw,
-                                                     off.p, d_pd.p, d_pg.p, (int)pd.size(), o_step.p, o_idx.p);
-    SG_CUDA(cudaGetLastError());
-    if (steps) SG_CUDA(cudaMemcpyAsync(steps, o_step.p, total * 4, cudaMemcpyDeviceToHost, s));
-    if (idx) SG_CUDA(cudaMemcpyAsync(idx, o_idx.p, total * 4, cudaMemcpyDeviceToHost, s));
+    upload_raster_pops(net, s);
+    net->rr_step.ensure(total);
+    net->rr_idx.ensure(total);
+    enqueue_raster_write(net, s, net->raster_read_step, nw, nb, total);
+    if (steps) SG_CUDA(cudaMemcpyAsync(steps, net->rr_step.p, total * 4, cudaMemcpyDeviceToHost, s));
+    if (idx) SG_CUDA(cudaMemcpyAsync(idx, net->rr_idx.p, total * 4, cudaMemcpyDeviceToHost, s));
     SG_CUDA(cudaStreamSynchronize(s));
     net->raster_read_step = net->host_step;
+  });
+}
+
+// Staged raster read, for a loop that keeps the GPU stepping while it reads:
+// the steps recorded since the last read are compacted on the network's read
+// stream right after the steps that wrote them (the network's next steps
+// wait for that compaction, so the raster slots may be reused at once), and
+// sg_raster_fetch later copies the pairs out.  Nothing here waits.
+int sg_raster_stage(sg_net *net) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->raster_cap > 0, SG_E_STATE, "raster recording is not enabled");
+    SG_REQUIRE(!net->rstaged, SG_E_STATE, "the last staged raster read is not fetched yet");
+    const uint64_t k = net->host_step - net->raster_read_step;
+    SG_REQUIRE(k <= net->raster_cap, SG_E_OVERFLOW,
+               "raster overflow: " + std::to_string(k) + " steps since the last read, capacity " +
+                   std::to_string(net->raster_cap));
+    DevGuard g(net->device);
+    if (!net->rstream) {
+      SG_CUDA(cudaStreamCreateWithFlags(&net->rstream, cudaStreamNonBlocking));
+      SG_CUDA(cudaEventCreateWithFlags(&net->rev, cudaEventDisableTiming));
+      SG_CUDA(cudaEventCreateWithFlags(&net->rdone, cudaEventDisableTiming));
+      SG_CUDA(cudaMallocHost(&net->rst_total, sizeof(unsigned long long)));
+      upload_raster_pops(net, net->rstream);
+    }
+    const uint64_t nw = k * (net->Nd / 32);
+    const uint64_t nb = (nw + kRasterWordsPerBlock - 1) / kRasterWordsPerBlock;
+    net->rst_t0 = net->raster_read_step;
+    net->rst_nw = nw;
+    net->rst_nb = nb;
+    *net->rst_total = 0;
+    net->raster_read_step = net->host_step;
+    net->rstaged = true;
+    if (nb == 0) return;
+    // the pool's steps of a member are followed on the member's stream (a
+    // pool step ends with the member streams waiting for it)
+    SG_CUDA(cudaEventRecord(net->rev, net->stream));
+    SG_CUDA(cudaStreamWaitEvent(net->rstream, net->rev, 0));
+    cudaStream_t rs = net->rstream;
+    enqueue_raster_count(net, rs, net->rst_t0, nw, nb);
+    // output room for 1/128 of the steps' neuron slots to begin with (fetch
+    // grows it when a batch has more spikes)
+    const uint64_t room = std::max<uint64_t>(net->rr_step.n, std::max<uint64_t>(nw / 4, 1u << 15));
+    net->rr_step.ensure(room);
+    net->rr_idx.ensure(room);
+    enqueue_raster_write(net, rs, net->rst_t0, nw, nb, net->rr_step.n);
+    SG_CUDA(cudaMemcpyAsync(net->rst_total, net->rr_off.p + nb, 8, cudaMemcpyDeviceToHost, rs));
+    SG_CUDA(cudaEventRecord(net->rdone, rs));
+    SG_CUDA(cudaStreamWaitEvent(net->stream, net->rdone, 0));
+  });
+}
+
+int sg_raster_fetch(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap, uint64_t *n_out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(n_out, SG_E_INVALID, "null output");
+    SG_REQUIRE(net->rstaged, SG_E_STATE, "no staged raster read");
+    *n_out = 0;
+    if (net->rst_nb == 0) {
+      net->rstaged = false;
+      return;
+    }
+    DevGuard g(net->device);
+    cudaStream_t rs = net->rstream;
+    SG_CUDA(cudaStreamSynchronize(rs));
+    const uint64_t total = *net->rst_total;
+    *n_out = total;
+    SG_REQUIRE(total <= cap, SG_E_INVALID, "output buffer too small: " + std::to_string(total) + " spikes");
+    if (total > net->rr_step.n) {  // the write was skipped: grow the room and write now
+      net->rr_step.ensure(total + total / 4);
+      net->rr_idx.ensure(total + total / 4);
+      enqueue_raster_write(net, rs, net->rst_t0, net->rst_nw, net->rst_nb, net->rr_step.n);
+    }
+    if (total) {
+      if (steps) SG_CUDA(cudaMemcpyAsync(steps, net->rr_step.p, total * 4, cudaMemcpyDeviceToHost, rs));
+      if (idx) SG_CUDA(cudaMemcpyAsync(idx, net->rr_idx.p, total * 4, cudaMemcpyDeviceToHost, rs));
+    }
+    SG_CUDA(cudaStreamSynchronize(rs));
+    net->rstaged = false;
+  });
+}
+
+// Spikes per neuron (reference order) over every event read since the
+// raster was enabled.
+int sg_raster_counts(sg_net *net, uint32_t *counts) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(net->raster_cap > 0 && net->rr_counts.p, SG_E_STATE, "raster recording is not enabled");
+    SG_REQUIRE(!net->rstaged, SG_E_STATE, "a staged raster read is not fetched yet");
+    SG_REQUIRE(counts, SG_E_INVALID, "null output");
+    DevGuard g(net->device);
+    std::vector<uint32_t> c(net->Nd);
+    SG_CUDA(cudaMemcpyAsync(c.data(), net->rr_counts.p, (size_t)net->Nd * 4, cudaMemcpyDeviceToHost, net->stream));
+    SG_CUDA(cudaStreamSynchronize(net->stream));
+    for (size_t p = 0; p < net->pops.size(); ++p)
+      for (uint32_t i = 0; i < net->pops[p].n; ++i) counts[net->offsets[p] + i] = c[net->pops[p].dev_off + i];
   });
 }
 
@@ -3770,7 +3919,7 @@ void pool_prepare(sg_pool *pool) {
   std::vector<StepArgs> nets;
   std::vector<PopArgs> pops;
   std::vector<uint4> map;
-  bool full = false;
+  bool full[5] = {};
   for (size_t i = 0; i < pool->members.size(); ++i) {
     sg_net *net = pool->members[i];
     upload_pop_table(net);
@@ -3779,7 +3928,7 @@ void pool_prepare(sg_pool *pool) {
                "pool: every member takes the pre-centric scatter (exact ring sums, or the atomic mode)");
     SG_REQUIRE(!net->learn_on && !has_external(net), SG_E_STATE,
                "pool: learning networks and networks split across GPUs step on their own");
-    full = full || needs_full_neuron_kernel(net, a);
+    for (int m = 1; m <= 4; ++m) full[m] = full[m] || needs_full_neuron_kernel(net, a, m);
     nets.push_back(a);
   }
   for (int m = 1; m <= 4; ++m) {
@@ -3797,7 +3946,7 @@ void pool_prepare(sg_pool *pool) {
     pool->model_cnt[m] = (uint32_t)map.size() - pool->model_off[m];
   }
   const bool same = nets.size() == pool->h_nets.size() && pops.size() == pool->h_pops.size() &&
-                    map.size() == pool->h_map.size() && full == pool->full &&
+                    map.size() == pool->h_map.size() && std::memcmp(full, pool->full, sizeof(full)) == 0 &&
                     std::memcmp(nets.data(), pool->h_nets.data(), nets.size() * sizeof(StepArgs)) == 0 &&
                     std::memcmp(pops.data(), pool->h_pops.data(), pops.size() * sizeof(PopArgs)) == 0 &&
                     std::memcmp(map.data(), pool->h_map.data(), map.size() * sizeof(uint4)) == 0;
@@ -3807,7 +3956,7 @@ void pool_prepare(sg_pool *pool) {
   pool->h_nets = std::move(nets);
   pool->h_pops = std::move(pops);
   pool->h_map = std::move(map);
-  pool->full = full;
+  std::memcpy(pool->full, full, sizeof(full));
   if (pool->d_nets.n < pool->h_nets.size()) pool->d_nets.alloc(pool->h_nets.size());
   if (pool->d_pops.n < std::max<size_t>(pool->h_pops.size(), 1)) pool->d_pops.alloc(std::max<size_t>(pool->h_pops.size(), 1));
   if (pool->d_map.n < std::max<size_t>(pool->h_map.size(), 1)) pool->d_map.alloc(std::max<size_t>(pool->h_map.size(), 1));
@@ -3826,7 +3975,7 @@ template <int M> void pool_launch_neuron(sg_pool *pool) {
   const uint32_t nb = pool->model_cnt[M];
   if (nb == 0) return;
   const uint4 *map = pool->d_map.p + pool->model_off[M];
-  if (pool->full)
+  if (pool->full[M])
     launch_step_kernel(neuron_pool_kernel<M, true>, nb, NeuronCfg<M>::THREADS, 0, pool->stream,
                        (const StepArgs *)pool->d_nets.p, (const PopArgs *)pool->d_pops.p, map);
   else

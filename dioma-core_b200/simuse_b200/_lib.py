@@ -81,6 +81,9 @@ SIGNATURES = {
     "sg_raster_read": [vp, vp, u64, vp],
     "sg_stats_read": [vp, vp, vp, u32, vp],
     "sg_raster_read_events": [vp, vp, vp, u64, vp],
+    "sg_raster_stage": [vp],
+    "sg_raster_fetch": [vp, vp, vp, u64, vp],
+    "sg_raster_counts": [vp, vp],
     "sg_profile_enable": [vp, i32],
     "sg_profile_read": [vp, vp, vp],
     "sg_spikes": [vp, u32, vp, u32],

@@ -318,6 +318,31 @@ class Network:
         self._raster_mark = self.step_counter
         return st[: n.value], ix[: n.value]
 
+    def raster_stage(self):
+        """Queue the compaction of the steps recorded since the last read,
+        right after them, without waiting (fetch with raster_fetch)."""
+        check(lib().sg_raster_stage(self._h))
+        self._raster_mark = self.step_counter
+
+    def raster_fetch(self, capacity: int = 1 << 20):
+        """(steps, indices) of the staged batch; waits for its compaction."""
+        n = C.c_uint64()
+        st = np.empty(capacity, np.uint32)
+        ix = np.empty(capacity, np.uint32)
+        rc = lib().sg_raster_fetch(self._h, _p(st), _p(ix), capacity, C.byref(n))
+        if rc < 0 and n.value > capacity:  # too small: the batch stays staged, fetch it at its size
+            st = np.empty(n.value, np.uint32)
+            ix = np.empty(n.value, np.uint32)
+            rc = lib().sg_raster_fetch(self._h, _p(st), _p(ix), n.value, C.byref(n))
+        check(rc)
+        return st[: n.value], ix[: n.value]
+
+    def raster_counts(self) -> np.ndarray:
+        """Spikes per neuron over every event read since the raster was enabled."""
+        out = np.empty(self.total_neurons, np.uint32)
+        check(lib().sg_raster_counts(self._h, _p(out)))
+        return out
+
     def read_spike_events_into(self, steps: np.ndarray, idx: np.ndarray) -> int:
         """Zero-allocation variant for preallocated (pinned) host buffers."""
         n = C.c_uint64()

@@ -21,6 +21,16 @@ spikes are the same.  A constant ``external_I`` is applied as a device bias
 (the same float add as the injection); Poisson groups are drawn on the host
 each step.  The reference draws them from ``StdRng`` (ChaCha12, seed 0),
 which no reference test pins: with Poisson groups only the statistics match.
+
+The conductance configurations ``NeuronConfig::LifSynaptic`` / ``::IzhSynaptic``
+(runner.rs:124-131, :156-163; run at :1365-1401 and :1695-1735) run the same
+neurons through ``SynapticBrain`` (receptor kinetics, pillars-connectome/src/
+synaptic.rs): the connectome's unsigned weights, its receptor types (or
+types from the presynaptic NT signs and the phenotype, data.rs:433-463), no
+delays, the conductances carried from one ``run`` to the next
+(``set_kinetics`` of the last run's ``kinetics``) and cleared by ``reset``.
+Here the network is built once in receptor mode and its conductances stay in
+HBM between calls, which is that carry-over.
 """
 from __future__ import annotations
 
@@ -29,6 +39,7 @@ import dataclasses
 import numpy as np
 
 from .network import IZH, LIF, Network
+from .synaptic import receptor_types_from_nt
 
 
 @dataclasses.dataclass
@@ -39,6 +50,8 @@ class ConnectomeData:
     col_indices: np.ndarray      # i32 [n_synapses]
     values: np.ndarray           # f32 [n_synapses]
     nt_types: np.ndarray | None = None   # f32 [n_neurons], < 0 = inhibitory presynapse
+    receptor_types: np.ndarray | None = None   # u8 [n_synapses] receptor codes (conductance configs)
+    phenotype: str = "mammal"            # NtPhenotype for types derived from nt_types
 
     @property
     def n_neurons(self) -> int:
@@ -47,8 +60,9 @@ class ConnectomeData:
 
 @dataclasses.dataclass
 class NeuronConfig:
-    """``NeuronConfig::Lif`` or ``::Izh`` (runner.rs:114-248)."""
-    model: str                   # "lif" or "izh"
+    """``NeuronConfig::Lif``, ``::Izh``, ``::LifSynaptic`` or ``::IzhSynaptic``
+    (runner.rs:114-248)."""
+    model: str                   # "lif", "izh", "lif_synaptic" or "izh_synaptic"
     dt_ms: float
     tau_ref: float
     tau_m: float = 20.0
@@ -71,6 +85,16 @@ def izh(dt_ms: float) -> NeuronConfig:
     return NeuronConfig("izh", dt_ms, tau_ref=2.0, a=0.02, b=0.2, c=-65.0, d=8.0)
 
 
+def lif_synaptic(dt_ms: float) -> NeuronConfig:
+    """BrainConfig::lif_synaptic (runner.rs:265-275)."""
+    return NeuronConfig("lif_synaptic", dt_ms, tau_ref=2.0, tau_m=20.0, v_rest=-70.0, v_thresh=-58.0, v_reset=-70.0)
+
+
+def izh_synaptic(dt_ms: float) -> NeuronConfig:
+    """NeuronConfig::IzhSynaptic with BrainConfig::izh's parameters."""
+    return NeuronConfig("izh_synaptic", dt_ms, tau_ref=2.0, a=0.02, b=0.2, c=-65.0, d=8.0)
+
+
 @dataclasses.dataclass
 class PoissonGroup:
     indices: np.ndarray
@@ -91,8 +115,9 @@ class BrainRunner:
         if len(connectome.col_indices) != len(connectome.values):
             raise ValueError(f"BrainRunner: col_indices length {len(connectome.col_indices)} != values "
                              f"length {len(connectome.values)}")
-        if config.model not in ("lif", "izh"):
+        if config.model not in ("lif", "izh", "lif_synaptic", "izh_synaptic"):
             raise ValueError(f"unsupported neuron model {config.model!r}")
+        self._synaptic = config.model.endswith("_synaptic")
         self.config, self.connectome, self.n_neurons = config, connectome, n
         self.poisson_groups: list[PoissonGroup] = []
         self._rng = np.random.default_rng(seed)
@@ -109,7 +134,9 @@ class BrainRunner:
         sign[:min(n, nt.size)] = np.where(nt[:n] < 0.0, np.float32(-1.0), np.float32(1.0))
         w *= np.repeat(sign, np.diff(rp32).astype(np.int64))
         self._net = Network(device)
-        self._model = LIF if config.model == "lif" else IZH
+        self._model = LIF if config.model.startswith("lif") else IZH
+        if self._synaptic:
+            self._net.set_receptor_kinetics(config.dt_ms)
         self._pop = self._net.add_population(self._model, n)
         c = config
         if self._model == LIF:
@@ -119,7 +146,19 @@ class BrainRunner:
             cols = [c.dt_ms, c.a, c.b, c.c, c.d, c.tau_ref, 30.0]
         for k, v in enumerate(cols):
             self._net.fill_param(self._pop, k, float(np.float32(v)))
-        self._net.build_from_csr(rp32, col, w, np.zeros(col.size, np.uint8))
+        if self._synaptic:
+            # SynapticBrain::from_connectome (synaptic.rs:36-50): unsigned
+            # weights, the given receptor types or ones from the NT signs
+            rt = connectome.receptor_types
+            if rt is None or len(rt) == 0:
+                rt = receptor_types_from_nt(rp32, [] if connectome.nt_types is None else connectome.nt_types,
+                                            connectome.phenotype)
+            pre = np.repeat(np.arange(n, dtype=np.uint32), np.diff(rp32.astype(np.int64)))
+            self._net.connect(self._pop, pre, self._pop, col, np.asarray(connectome.values, np.float32),
+                              np.ones(col.size, np.uint8), syn_types=np.asarray(rt, np.uint8))
+            self._net.build()
+        else:
+            self._net.build_from_csr(rp32, col, w, np.zeros(col.size, np.uint8))
         self._set_initial_state()
 
     def _set_initial_state(self):
@@ -147,7 +186,9 @@ class BrainRunner:
         e = np.asarray(external_I, np.float32).ravel()[:n]
         ext[:e.size] = e
         net = self._net
-        net.clear_rings()                 # the rebuilt Brain starts with empty rings
+        if not self._synaptic:
+            net.clear_rings()             # the rebuilt Brain starts with empty rings
+        # (the conductance configurations carry their kinetics over instead)
         if n_steps == 0:
             return self.spike_buffer[:0]
         net.enable_raster(n_steps)
@@ -249,6 +290,12 @@ class BrainRunner:
         self._net.set_state(self._pop, 0, (v + noise * np.float32(0.03)).astype(np.float32))
         self.spike_buffer[:] = 0
         self._step_counter = 0
+        if self._synaptic:               # SynapticKinetics::reset (runner.rs:1272-1274)
+            self._net.set_receptor_conductances(np.zeros((7, self.n_neurons), np.float32))
+
+    def kinetics(self) -> np.ndarray | None:
+        """The carried conductances [7][n] of a conductance configuration."""
+        return self._net.receptor_conductances() if self._synaptic else None
 
     def close(self):
         self._net.close()

@@ -139,13 +139,14 @@ def _run_to_end(net: Network, req: Request, chunk: int):
         st.append(s)
         ix.append(i)
         done += k
-    _finish(req, st, ix)
+    _finish(req, st, ix, net.raster_counts())
 
 
-def _finish(req: Request, st, ix):
+def _finish(req: Request, st, ix, counts):
+    """The request's results: its spike events in step order and its rates
+    from the per-neuron spike counts the device kept while reading."""
     req.spike_steps = np.concatenate(st) if st else np.empty(0, np.uint32)
     req.spike_index = np.concatenate(ix) if ix else np.empty(0, np.uint32)
-    counts = np.bincount(req.spike_index.astype(np.int64), minlength=req.n)
     req.rates_hz = counts / (req.steps * req.dt_ms * 1e-3)
 
 
@@ -155,6 +156,13 @@ class _Resident:
         self.done = 0
         self.st: list[np.ndarray] = []
         self.ix: list[np.ndarray] = []
+        self.counts: np.ndarray | None = None
+        self.cap = 1 << 16          # fetch buffer size: the last batch's size and a half
+
+    def fetch(self):
+        s, i = self.net.raster_fetch(self.cap)
+        self.cap = max(self.cap, s.size + s.size // 2)
+        return s, i
 
 
 class Server:
@@ -179,6 +187,8 @@ class Server:
         self._next_id = 0
         self.completed: list[Request] = []
         self.ticks = 0
+        # host seconds the stepping thread spent per phase (for tuning)
+        self.phase_s = {"admit": 0.0, "step": 0.0, "collect": 0.0, "stage": 0.0, "leave": 0.0, "idle": 0.0}
         self._stop = threading.Event()
         self._idle = threading.Event()
         self._n_open = 0
@@ -245,7 +255,7 @@ class Server:
             if item is None:
                 return
             r = item
-            _finish(r.req, r.st, r.ix)
+            _finish(r.req, r.st, r.ix, r.counts)
             self._complete(r.req)
 
     def _build_loop(self):
@@ -263,11 +273,21 @@ class Server:
                 self._built.put((req, None))
 
     def _step_loop(self):
+        """Ticks in a pipeline: tick t is queued, then the host collects the
+        spikes of tick t - 1 (copied out beside tick t), stages tick t's
+        spikes for compaction right after it and hands their copy to the
+        readers, so the GPU keeps stepping while results come back.  A
+        request that finished leaves the pool at once and completes when its
+        last batch is in."""
         pool = Pool(self.device)
         resident: list[_Resident] = []
+        draining: list[_Resident] = []   # out of the pool, last batch in flight
+        inflight: list = []              # (resident, future) of the last tick's fetches
         building = 0
         waiting: list[Request] = []
-        while not self._stop.is_set() or resident or building:
+        ph = self.phase_s
+        while not self._stop.is_set() or resident or building or inflight or draining:
+            t0 = time.perf_counter()
             # arrivals
             while True:
                 try:
@@ -275,7 +295,7 @@ class Server:
                 except queue.Empty:
                     break
             # admission in arrival order, by footprint and slot
-            while waiting and len(resident) + building < self.max_resident:
+            while waiting and len(resident) + len(draining) + building < self.max_resident:
                 req = waiting[0]
                 est = estimate_footprint(req)
                 with self._lock:
@@ -306,23 +326,48 @@ class Server:
                 net.enable_raster(self.chunk)
                 pool.add(net)
                 resident.append(_Resident(req, net))
-            if not resident:
+            t1 = time.perf_counter()
+            ph["admit"] += t1 - t0
+            if not resident and not inflight:
                 time.sleep(0.0005)
+                ph["idle"] += time.perf_counter() - t1
                 continue
-            # one tick: every resident network advances k steps in the pool,
-            # then each one's spikes of the tick are read back
-            k = min(self.chunk, min(r.req.steps - r.done for r in resident))
-            pool.step(k)
-            self.ticks += 1
-            for r, (s, i) in zip(resident, self._readers.map(lambda r: r.net.read_spike_events(), resident)):
+            # tick t: every resident network advances k steps in the pool
+            k = 0
+            if resident:
+                k = min(self.chunk, min(r.req.steps - r.done for r in resident))
+                pool.step(k)
+                self.ticks += 1
+            t2 = time.perf_counter()
+            ph["step"] += t2 - t1
+            # tick t - 1's spikes (their copies ran beside tick t)
+            for r, fut in inflight:
+                s, i = fut.result()
                 r.st.append(s)
                 r.ix.append(i)
-                r.done += k
-            for r in [r for r in resident if r.done >= r.req.steps]:
-                resident.remove(r)
-                pool.remove(r.net)
+            inflight = []
+            for r in draining:              # finished requests whose last batch is in
+                r.counts = r.net.raster_counts()
                 r.net.close()
                 with self._lock:
                     self._reserved -= r.req.footprint
                 self._finishing.put(r)
+            draining = []
+            t3 = time.perf_counter()
+            ph["collect"] += t3 - t2
+            if not resident:
+                continue
+            # tick t's spikes: compaction queued after the tick, copies to the readers
+            for r in resident:
+                r.net.raster_stage()
+                r.done += k
+            inflight = [(r, self._readers.submit(r.fetch)) for r in resident]
+            t4 = time.perf_counter()
+            ph["stage"] += t4 - t3
+            # finished requests leave the pool before the next tick
+            for r in [r for r in resident if r.done >= r.req.steps]:
+                resident.remove(r)
+                pool.remove(r.net)
+                draining.append(r)
+            ph["leave"] += time.perf_counter() - t4
         pool.close()

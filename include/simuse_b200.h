@@ -288,6 +288,20 @@ int sg_stats_read(sg_net *net, uint32_t *spikes, uint64_t *events, uint32_t cap,
    compacted on the device so only the spikes cross PCIe.  *n_out = spikes. */
 int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap,
                           uint64_t *n_out);
+/* Staged raster read for a loop that keeps the GPU stepping while it reads.
+   sg_raster_stage queues, right after the steps queued so far, the
+   compaction of the steps recorded since the last read (on the network's own
+   read stream; the network's later steps wait for it, so the raster slots are
+   reused at once) and returns without waiting.  sg_raster_fetch waits for
+   that compaction and copies its (step, index) pairs into the buffers
+   (cap pairs; when too small it fails with *n_out = the count and the batch
+   stays staged).  One staged batch per network at a time; plain reads,
+   sg_raster_enable and sg_raster_counts refuse while one is staged. */
+int sg_raster_stage(sg_net *net);
+int sg_raster_fetch(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap, uint64_t *n_out);
+/* Spikes per neuron over every event read (plain or staged) since the raster
+   was enabled; counts[total]. */
+int sg_raster_counts(sg_net *net, uint32_t *counts);
 /* Phase timing: when enabled, sg_step launches each step eagerly with CUDA
    events around its phases (0 neuron update, 1 expand, 2 STDP potentiation,
    3 apply) and accumulates the device time per phase. */

@@ -103,3 +103,40 @@ def test_pool_refuses_ordered_networks():
         pool.add(net)
     pool.close()
     net.close()
+
+
+def test_staged_raster_reads_equal_plain_reads():
+    """sg_raster_stage / sg_raster_fetch in a pipeline (the next steps are
+    queued before the last batch is fetched) give the events of plain reads,
+    and the device's per-neuron counts equal the counts of those events."""
+    chunks = [50, 13, 50, 1, 37, 50]
+    a, b = _build(S.Request("lif", 20000, 31, 0)), _build(S.Request("lif", 20000, 31, 0))
+    a.enable_raster(50)
+    b.enable_raster(50)
+    plain = []
+    for k in chunks:
+        a.step(k)
+        plain.append(a.read_spike_events())
+    staged = []
+    for j, k in enumerate(chunks):
+        b.step(k)
+        if j:
+            staged.append(b.raster_fetch(16))   # 16 pairs: too small, fetched again at the batch's size
+        b.raster_stage()
+    staged.append(b.raster_fetch())
+    for (s0, i0), (s1, i1) in zip(plain, staged):
+        assert s0.size > 100
+        assert np.array_equal(s0, s1) and np.array_equal(i0, i1)
+    idx = np.concatenate([i for _, i in plain]).astype(np.int64)
+    want = np.bincount(idx, minlength=a.total_neurons)
+    assert np.array_equal(a.raster_counts(), want)
+    assert np.array_equal(b.raster_counts(), want)
+    assert np.array_equal(a.state(0, 0).view(np.uint32), b.state(0, 0).view(np.uint32))
+    with pytest.raises(sg.SimuseError, match="no staged"):
+        b.raster_fetch()
+    b.raster_stage()
+    with pytest.raises(sg.SimuseError, match="not fetched"):
+        b.read_spike_events()
+    b.raster_fetch()
+    a.close()
+    b.close()

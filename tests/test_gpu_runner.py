@@ -122,3 +122,88 @@ def test_brain_runner_state_io_reset_and_errors():
     bad = R.ConnectomeData(np.array([0, 1, 2], np.int32), np.array([1, 0], np.int32), np.array([1.0], np.float32))
     with pytest.raises(ValueError, match="col_indices length"):
         R.BrainRunner(bad, R.lif(0.1))
+
+
+class _ReferenceSynapticRunner:
+    """The reference's conductance run() (runner.rs:1365-1401, :1695-1735)
+    through the oracle: a fresh SynapticBrain per call from the unsigned
+    connectome and its receptor types, the last call's kinetics restored,
+    state carried."""
+
+    def __init__(self, conn, cfg, receptor_types):
+        self.conn, self.cfg, self.n, self.rt = conn, cfg, conn.n_neurons, receptor_types
+        self.lif = cfg.model.startswith("lif")
+        self.v = np.full(self.n, -58.0 if self.lif else -65.0, np.float32)
+        self.u = np.full(self.n, -13.0, np.float32)
+        self.refr = np.zeros(self.n, np.float32)
+        self.kin = None
+
+    def run(self, n_steps, ext):
+        c, n = self.cfg, self.n
+        net = O.Network()
+        net.set_receptor_kinetics(c.dt_ms)
+        p = net.add_population(1 if self.lif else 2, n)
+        if self.lif:
+            cols = [c.dt_ms, np.float32(1.0) / np.float32(c.tau_m), c.v_rest, c.v_thresh, c.v_reset, c.tau_ref]
+        else:
+            cols = [c.dt_ms, c.a, c.b, c.c, c.d, c.tau_ref, 30.0]
+        for k, v in enumerate(cols):
+            net.fill_param(p, k, float(np.float32(v)))
+        net.set_state(p, 0, self.v)
+        if self.lif:
+            net.set_state(p, 1, self.refr)
+        else:
+            net.set_state(p, 1, self.u)
+            net.set_state(p, 2, self.refr)
+        rp = self.conn.row_ptr.astype(np.int64)
+        pre = np.repeat(np.arange(n, dtype=np.uint32), np.diff(rp))
+        net.connect(p, pre, p, self.conn.col_indices.astype(np.uint32), self.conn.values.astype(np.float32),
+                    np.ones(pre.size, np.uint8), syn_types=self.rt)
+        net.build()
+        if self.kin is not None:
+            net.set_receptor_conductances(self.kin)
+        e = np.zeros(n, np.float32)
+        ee = np.asarray(ext, np.float32)[:n]
+        e[:ee.size] = ee
+        idx = np.arange(n, dtype=np.uint32)
+        out = np.zeros((n_steps, n), np.int32)
+        for t in range(n_steps):
+            net.inject_current(p, idx, e)
+            net.step(1)
+            out[t] = net.spikes(p)
+        self.kin = net.receptor_conductances()
+        self.v = net.state(p, 0)
+        if self.lif:
+            self.refr = net.state(p, 1)
+        else:
+            self.u, self.refr = net.state(p, 1), net.state(p, 2)
+        return out.reshape(-1)
+
+
+@pytest.mark.parametrize("model", ["lif_synaptic", "izh_synaptic"])
+def test_brain_runner_conductance_configs_match_reference(model):
+    """LifSynaptic / IzhSynaptic: receptor types from the NT signs (AMPA /
+    GABA_A), conductances carried across calls and cleared by reset."""
+    cfg = R.lif_synaptic(0.1) if model == "lif_synaptic" else R.izh_synaptic(0.5)
+    conn = _connectome(w_hi=0.05 if model == "lif_synaptic" else 0.02)
+    n = conn.n_neurons
+    from simuse_b200.synaptic import receptor_types_from_nt
+    rt = receptor_types_from_nt(conn.row_ptr, conn.nt_types)
+    assert set(np.unique(rt)) == {0, 2}
+    rng = np.random.default_rng(3)
+    ext1 = rng.uniform(14.0, 20.0, n).astype(np.float32) if model == "lif_synaptic" else \
+        rng.uniform(0, 12, n).astype(np.float32)
+    gpu, ref = R.BrainRunner(conn, cfg), _ReferenceSynapticRunner(conn, cfg, rt)
+    total = 0
+    for steps, ext in ((150, ext1), (60, ext1[: n // 2]), (1, ext1), (200, ext1)):
+        a = gpu.run(steps, ext).copy()
+        b = ref.run(steps, ext)
+        total += a.sum()
+        assert np.array_equal(a, b), (model, steps)
+        assert np.array_equal(gpu.get_v().view(np.uint32), ref.v.view(np.uint32))
+        assert np.array_equal(gpu.kinetics().view(np.uint32), ref.kin.view(np.uint32))
+    assert total > 100
+    assert np.count_nonzero(gpu.kinetics()) > 0
+    gpu.reset()
+    assert np.count_nonzero(gpu.kinetics()) == 0
+    gpu.close()
