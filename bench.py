@@ -244,6 +244,17 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def probe_red_rate(device, n_cells, iters=64):
+    """Scattered 4-byte reductions per second this GPU completes into an
+    n_cells-float array (sg_probe_red_rate), or None."""
+    import ctypes as C
+
+    from simuse_b200 import _lib
+    r = C.c_double()
+    rc = _lib.lib().sg_probe_red_rate(device, int(n_cells), iters, C.byref(r))
+    return r.value if rc == 0 else None
+
+
 def profiled_traffic(kernel):
     """DRAM bytes (read + write) per launch of `kernel` on the bench workload,
     from the committed ncu summary profiles/dram_traffic.txt (lines
@@ -671,7 +682,9 @@ def run_ours(args):
     p_rec = p_events - p_src
     sp, _ = net.read_stats()
     p_spikes = float(sp[-p_steps:].mean()) if sp.size else 0.0
-    phases = ["neuron_kernel<LIF>", "scatter_red_kernel" if scatter_path != "ordered" else "scatter_kernel"]
+    scatter_kernel = ("scatter_kernel" if scatter_path == "ordered" else
+                      "scatter_walk_kernel" if net.scatter_schedule[0] == 4 else "scatter_red_kernel")
+    phases = ["neuron_kernel<LIF>", scatter_kernel]
     alg = [spec["n"] * B_NEURON,
            p_rec * (B_EVENT_EXPAND + B_EVENT_APPLY) + p_spikes * B_SPIKE]
     per_launch_ms = [ph_ms[i] / max(int(ph_launch[i]), 1) for i in range(2)]
@@ -681,6 +694,8 @@ def run_ours(args):
     step_alg = sum(alg)
     step_ms = ms / (args.steps * S)
 
+    # the pre-centric scatter's own ceiling: random reds into an array of the rings' size
+    red_peak = probe_red_rate(local, spec["n"] * (args.d_max + 1)) if scatter_path != "ordered" else None
     net.close()  # the headline network leaves HBM before the extra measurements
     if dist is not None:
         dist.destroy_process_group()
@@ -713,6 +728,14 @@ def run_ours(args):
         "clocks": clk.summary(),
         "gpu_launches": int(args.steps * S * 2),
     }
+    if red_peak:
+        red_ach = p_rec / (per_launch_ms[1] / 1e3)
+        out["roofline_l2"] = {"bound": "l2_red", "kernel": phases[1], "achieved": red_ach, "peak": red_peak,
+                              "unit": "reds/s", "frac": red_ach / red_peak,
+                              "peak_source": "sg_probe_red_rate on this GPU: random red.global.add.f32 from a "
+                                             "full-occupancy grid into an array of the rings' size",
+                              "what": "one red per recurrent event; the scatter's events per launch over its "
+                                      "launch time, against the measured red ceiling"}
     if not args.no_extras and world == 1:
         for key, fn in (("precision_paths", run_precision_paths), ("hh_stdp_100k", run_hh_prefix),
                         ("kuramoto_sweep", run_kuramoto), ("lif_learn", run_learn_short),

@@ -223,6 +223,7 @@ struct sg_net {
   int red = 0;
   bool exact = false;  // rings_exact at build (cleared when weights start changing)
   DBuf<uint32_t> d_red_flat, d_red_cnt, d_run_off;
+  DBuf<uint2> d_red_rows;
   // deferred drive: device record of the last folded step, and its host copy
   DBuf<unsigned long long> d_drv_fold;
   DBuf<uint32_t> d_err;        // device error word (scatter pipeline waits)
@@ -434,6 +435,7 @@ StepArgs make_args(sg_net *net) {
   a.deterministic = net->deterministic;
   a.red = net->red;
   a.red_flat = net->d_red_flat.p;
+  a.red_rows = net->d_red_rows.p;
   a.red_cnt = net->d_red_cnt.p;
   a.run_off = net->d_run_off.p;
   a.n_runs = (uint32_t)net->n_runs;
@@ -1410,8 +1412,10 @@ void upload_args(sg_net *net, const StepArgs &a) {
 // The pre-centric scatter's schedules (stages x synapses per stage), the
 // first being the fixed one; sg_autotune picks one per network, with the
 // blocks per SM.
-// (4 x 1024, 8 x 512, 3 x 2048, 6 x 512: launch_step_red)
-constexpr int kNumRedVariants = 4;
+// (4 x 1024, 8 x 512, 3 x 2048, 6 x 512: launch_step_red), and the warp walk
+// without stages (variant 4, scatter_walk_kernel).
+constexpr int kNumRedVariants = 5;
+constexpr int kWalkVariant = 4;
 
 template <uint32_t ST, uint32_t CH> void allow_red_smem_v() {
   SG_CUDA(cudaFuncSetAttribute(scatter_red_kernel<ST, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1435,6 +1439,17 @@ unsigned sm_count(int device) {
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
                      uint32_t *done, uint32_t *err, uint32_t stall);
 
+// The schedule a network or pool starts with: SG_RED_VARIANT (0..4) when set,
+// else the warp walk.
+int default_red_variant() {
+  static const int v = [] {
+    const char *e = std::getenv("SG_RED_VARIANT");
+    const int x = e ? std::atoi(e) : kWalkVariant;
+    return x >= 0 && x < kNumRedVariants ? x : kWalkVariant;
+  }();
+  return v;
+}
+
 void update_path(sg_net *net) {
   // the pre-centric scatter applies neither pair STDP nor short-term
   // plasticity: those networks keep the owner-computes scatter in any mode
@@ -1449,6 +1464,7 @@ void setup_scatter(sg_net *net) {
   cudaStream_t s = net->stream;
   net->exact = net->Nd > 0 && rings_exact(net);
   net->d_red_flat.alloc(std::max<uint32_t>(net->Nd, 1));
+  net->d_red_rows.alloc(std::max<uint32_t>(net->Nd, 1));
   net->d_red_cnt.alloc(1);
   net->d_red_cnt.zero(s);
   net->d_drv_fold.alloc(1);
@@ -1654,7 +1670,12 @@ void launch_step_kernel(void (*kernel)(KArgs...), unsigned grid, unsigned block,
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
                      uint32_t *done, uint32_t *err, uint32_t stall) {
   const unsigned grid = sm_count(device) * bps;
+  // the stall test hook acts on the staged pipeline's waits (the walk has none)
+  if (variant == kWalkVariant && stall) variant = 0;
   switch (variant) {
+    case kWalkVariant:
+      launch_step_kernel(scatter_walk_kernel, grid * 2, kWalkThreads, 0, s, nets, n_nets, done);
+      break;
     case 1:
       launch_step_kernel(scatter_red_kernel<8, 512>, grid, kRedThreads, sizeof(RedSmemT<8, 512>), s, nets, n_nets,
                          done, err, stall);
@@ -1675,10 +1696,10 @@ void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, cons
 
 template <int M, bool FULL> void launch_neuron_form(sg_net *net, const StepArgs &a, uint32_t nb) {
   if (net->model_single[M] >= 0)
-    launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M>::THREADS, 0, net->stream, a,
+    launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M, FULL>::THREADS, 0, net->stream, a,
                        net->pop_tab[net->model_single[M]], (const PopArgs *)nullptr, (const uint2 *)nullptr);
   else
-    launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M>::THREADS, 0, net->stream, a, PopArgs{},
+    launch_step_kernel(neuron_kernel<M, FULL>, nb, NeuronCfg<M, FULL>::THREADS, 0, net->stream, a, PopArgs{},
                        (const PopArgs *)net->d_pop_tab.p, (const uint2 *)(net->d_blk_map.p + net->model_blk_off[M]));
 }
 
@@ -1868,6 +1889,7 @@ int sg_net_create(sg_net **out, int device) {
     DevGuard g(device);
     auto *net = new sg_net();
     net->device = device;
+    net->red_variant = default_red_variant();
     cudaError_t e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
       delete net;
@@ -1929,6 +1951,15 @@ int sg_debug_stall_scatter(sg_net *net, int on) {
   return run([&] {
     net->debug_stall = on ? 1u : 0u;
     drop_graph(net);
+  });
+}
+
+int sg_scatter_schedule(sg_net *net, int *variant, uint32_t *blocks_per_sm) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(variant && blocks_per_sm, SG_E_INVALID, "null output");
+    *variant = net->red_variant;
+    *blocks_per_sm = net->red_bps;
   });
 }
 
@@ -2754,7 +2785,7 @@ int sg_autotune(sg_net *net, uint32_t steps, float *fixed_ms, float *best_ms, in
           SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
           ms /= (float)steps;
           if (log) std::fprintf(stderr, "sg_autotune: variant %d, %u blocks per SM: %.4f ms per step\n", v, bps, ms);
-          if (v == 0 && bps == kRedBlocksPerSM) fixed = ms;
+          if (v == default_red_variant() && bps == kRedBlocksPerSM) fixed = ms;
           if (first || ms < best) {
             best = ms;
             bv = v;
@@ -3883,7 +3914,7 @@ int sg_footprint(sg_net *net, uint64_t *out) {
          (net->packed ? 0 : net->d_code.n) + net->d_seg.n + net->d_spk.n * 8 + net->d_blk_cnt.n * 4 + net->d_last_bits.n * 4 +
          net->n_runs * 29 + net->d_raster.n * 4 +
          (net->d_in_edge.n + net->d_in_pre.n + net->d_in_ptr.n) * 4 + (net->d_x_pre.n + net->d_x_post.n) * 4 +
-         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_red_flat.n * 4 + net->d_run_off.n * 4 + net->d_w8.n + net->d_row_scale.n * 4 +
+         (net->d_stat_spk.n + net->d_stat_ev.n * 2) * 4 + net->d_red_flat.n * 4 + net->d_red_rows.n * 8 + net->d_run_off.n * 4 + net->d_w8.n + net->d_row_scale.n * 4 +
          (net->rr_cnt.n + net->rr_off.n) * 8 + net->rr_temp.n + (net->rr_step.n + net->rr_idx.n) * 4 +
          net->d_pt.n + (net->d_tm_r.n + net->d_tm_u.n + net->d_tm_last.n) * 4 +
          (net->d_l_tp.n + net->d_l_tq.n + net->d_l_baked.n + net->d_l_qb.n + net->d_l_in_ptr.n + net->d_l_in_edge.n +
@@ -3976,10 +4007,10 @@ template <int M> void pool_launch_neuron(sg_pool *pool) {
   if (nb == 0) return;
   const uint4 *map = pool->d_map.p + pool->model_off[M];
   if (pool->full[M])
-    launch_step_kernel(neuron_pool_kernel<M, true>, nb, NeuronCfg<M>::THREADS, 0, pool->stream,
+    launch_step_kernel(neuron_pool_kernel<M, true>, nb, NeuronCfg<M, true>::THREADS, 0, pool->stream,
                        (const StepArgs *)pool->d_nets.p, (const PopArgs *)pool->d_pops.p, map);
   else
-    launch_step_kernel(neuron_pool_kernel<M, false>, nb, NeuronCfg<M>::THREADS, 0, pool->stream,
+    launch_step_kernel(neuron_pool_kernel<M, false>, nb, NeuronCfg<M, false>::THREADS, 0, pool->stream,
                        (const StepArgs *)pool->d_nets.p, (const PopArgs *)pool->d_pops.p, map);
 }
 
@@ -3988,7 +4019,7 @@ void pool_enqueue_step(sg_pool *pool) {
   pool_launch_neuron<kIZH>(pool);
   pool_launch_neuron<kGPEA>(pool);
   pool_launch_neuron<kHH>(pool);
-  launch_step_red(pool->stream, pool->device, 0, kRedBlocksPerSM, (const StepArgs *)pool->d_nets.p,
+  launch_step_red(pool->stream, pool->device, default_red_variant(), kRedBlocksPerSM, (const StepArgs *)pool->d_nets.p,
                   (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u);
 }
 

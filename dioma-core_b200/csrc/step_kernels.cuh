@@ -65,12 +65,17 @@ constexpr uint32_t kMaxTm = 8;  // short-term plasticity profiles on the device
 // neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
 // GPEA/HH are compute heavy and keep one neuron per thread
 #ifndef SG_NEURON_MIN_BLOCKS
-#define SG_NEURON_MIN_BLOCKS 4  // resident 256-thread blocks per SM asked of the lean LIF/Izhikevich kernel
+#define SG_NEURON_MIN_BLOCKS 7  // resident 128-thread blocks per SM asked of the lean LIF kernel (7 x 148 >= 977 blocks of a million neurons)
 #endif
-template <int M> struct NeuronCfg {
-  static constexpr int NPT = (M == kLIF || M == kIZH) ? 4 : 1;
+// The lean LIF form moves 8 neurons per thread (two 128-bit accesses per
+// array): 128-thread blocks, 8 resident per SM, so a million-neuron
+// population updates in one wave of blocks.  Izhikevich (more state and
+// per-neuron parameters) and the full form keep 4 per thread (256-thread
+// blocks, 4 resident per SM in the lean form).
+template <int M, bool FULL> struct NeuronCfg {
+  static constexpr int NPT = (M == kLIF && !FULL) ? 8 : (M == kLIF || M == kIZH) ? 4 : 1;
   static constexpr int THREADS = (int)kNeuronBlock / NPT;
-  static constexpr int MIN_BLOCKS = (M == kLIF || M == kIZH) ? SG_NEURON_MIN_BLOCKS : 1;
+  static constexpr int MIN_BLOCKS = FULL ? 1 : NPT == 8 ? SG_NEURON_MIN_BLOCKS : NPT == 4 ? 4 : 1;
 };
 
 struct StepArgs {
@@ -163,6 +168,7 @@ struct StepArgs {
   int red;
   uint32_t *red_flat;
   uint32_t *red_cnt;
+  uint2 *red_rows;   // [Nd] synapse range [x, y) of each red_flat entry's row
   // Poisson-source synapses of the pre-centric scatter: run r covers source
   // synapses [run_off[r], run_off[r + 1]) of the n_src_syn in runs
   const uint32_t *run_off;
@@ -357,6 +363,20 @@ template <> struct VecF<1> {
   __device__ __forceinline__ static void ldg(const float *p, float *v) { v[0] = __ldg(p); }
   __device__ __forceinline__ static void store(float *p, const float *v) { *p = v[0]; }
 };
+template <> struct VecF<8> {
+  __device__ __forceinline__ static void load(const float *p, float *v) {
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  }
+  __device__ __forceinline__ static void ldg(const float *p, float *v) {
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(p)), b = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  }
+  __device__ __forceinline__ static void store(float *p, const float *v) {
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<float4 *>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+};
 template <> struct VecF<4> {
   __device__ __forceinline__ static void load(const float *p, float *v) {
     const float4 t = *reinterpret_cast<const float4 *>(p);
@@ -375,9 +395,22 @@ template <> struct VecF<4> {
 // FULL = false: the lean form for steps without kinetic synapses, input
 // noise, neuron statistics, pair STDP or learning (fewer registers: all blocks
 // of a large population resident at once).
+// Loads the state of this thread's neurons of block `blk` of population p.
 template <int MODEL, bool FULL>
-__device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p, uint32_t blk) {
-  constexpr int NPT = NeuronCfg<MODEL>::NPT;
+__device__ __forceinline__ void load_state(const PopArgs &p, uint32_t blk,
+                                           float (&sv)[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT]) {
+  constexpr int NPT = NeuronCfg<MODEL, FULL>::NPT;
+  const uint32_t i0 = blk * kNeuronBlock + threadIdx.x * NPT;
+#pragma unroll
+  for (int c = 0; c < n_state(MODEL); ++c) VecF<NPT>::load(p.state + (size_t)c * p.cap + i0, sv[c]);
+}
+
+// sv: the state of this thread's neurons (load_state), updated in place and
+// stored.
+template <int MODEL, bool FULL>
+__device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p, uint32_t blk,
+                                             float (&sv)[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT]) {
+  constexpr int NPT = NeuronCfg<MODEL, FULL>::NPT;
   constexpr int NS = n_state(MODEL), NP = n_params(MODEL);
   using V = VecF<NPT>;
   __shared__ uint32_t warp_cnt[32];
@@ -422,9 +455,6 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
         x[q] = x[q] + (float)((i < p.noise_split ? p.noise_sigma[0] : p.noise_sigma[1]) * z);
       }
   }
-  float sv[NS][NPT];
-#pragma unroll
-  for (int c = 0; c < NS; ++c) V::load(p.state + (size_t)c * p.cap + i0, sv[c]);
   // 2b. kinetic ExpOne rings (step.rs:56-70, :338-345); V from step start.
   // Unrolled over the (at most 3) profiles so that the profile constants are
   // indexed at compile time and stay in the kernel parameter space.
@@ -497,14 +527,20 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
 #pragma unroll
     for (int q = 0; q < NPT; ++q) x[q] = cur[q] + x[q];
   }
-  float pv[NP][NPT];
+  // per-neuron parameters: loaded for the block's NPT neurons at once, or
+  // (8 neurons per thread) one neuron at a time in the update loop, which
+  // keeps the register count down
+  constexpr bool kParamsPerNeuron = NPT == 8;
+  float pv[kParamsPerNeuron ? 1 : NP][kParamsPerNeuron ? 1 : NPT];
+  if (!kParamsPerNeuron) {
 #pragma unroll
-  for (int c = 0; c < NP; ++c) {
-    if ((p.umask >> c) & 1u) {
+    for (int c = 0; c < NP; ++c) {
+      if ((p.umask >> c) & 1u) {
 #pragma unroll
-      for (int q = 0; q < NPT; ++q) pv[c][q] = p.uval[c];
-    } else {
-      V::ldg(p.params + (size_t)c * p.cap + i0, pv[c]);
+        for (int q = 0; q < NPT; ++q) pv[c][q] = p.uval[c];
+      } else {
+        V::ldg(p.params + (size_t)c * p.cap + i0, pv[c]);
+      }
     }
   }
   // dt = param column 0 of neuron 0, broadcast (population.rs:307,361)
@@ -523,7 +559,10 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
 #pragma unroll
       for (int c = 0; c < NS; ++c) r.s[c] = sv[c][q];
 #pragma unroll
-      for (int c = 0; c < NP; ++c) r.p[c] = pv[c][q];
+      for (int c = 0; c < NP; ++c)
+        r.p[c] = !kParamsPerNeuron ? pv[kParamsPerNeuron ? 0 : c][kParamsPerNeuron ? 0 : q]
+                 : (p.umask >> c) & 1u ? p.uval[c]
+                                       : __ldg(p.params + (size_t)c * p.cap + i0 + q);
       bool sp;
       if (MODEL == kLIF) sp = lif_step(r, xi, dt);
       else if (MODEL == kIZH) sp = izh_step(r, xi, dt);
@@ -554,7 +593,15 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   }
   // 4. compaction: bitmask words (32 neurons each) and the block's spike list
   uint32_t word;
-  if (NPT == 4) {
+  if (NPT == 8) {
+    word = nib << (8 * (lane & 3));
+    word |= __shfl_xor_sync(0xffffffffu, word, 1);
+    word |= __shfl_xor_sync(0xffffffffu, word, 2);
+    if ((lane & 3) == 0) {
+      a.last_bits[gi0 >> 5] = word;
+      if (a.raster != nullptr) a.raster[(size_t)(step % a.raster_cap) * a.words + (gi0 >> 5)] = word;
+    }
+  } else if (NPT == 4) {
     word = nib << (4 * (lane & 7));
     word |= __shfl_xor_sync(0xffffffffu, word, 1);
     word |= __shfl_xor_sync(0xffffffffu, word, 2);
@@ -589,7 +636,7 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     warp_fire[wid] = fw;
   }
   __syncthreads();
-  constexpr uint32_t NW = NeuronCfg<MODEL>::THREADS / 32;
+  constexpr uint32_t NW = NeuronCfg<MODEL, FULL>::THREADS / 32;
   uint32_t before = incl - cnt, total = 0, clamp_tot = 0, fire_tot = 0;
 #pragma unroll
   for (uint32_t k = 0; k < NW; ++k) {
@@ -608,7 +655,11 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     uint32_t pos = red_base + before;
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
-      if (nib & (1u << q)) a.red_flat[pos++] = gi0 + q;
+      if (nib & (1u << q)) {  // the spiking neuron and its synapse range
+        a.red_flat[pos] = gi0 + q;
+        a.red_rows[pos] = make_uint2(__ldg(a.row_ptr + gi0 + q), __ldg(a.row_ptr + gi0 + q + 1));
+        ++pos;
+      }
   } else {
     uint2 *out = a.spk + (size_t)gblk * kNeuronBlock + before;
 #pragma unroll
@@ -667,14 +718,22 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
 // with a single population passes its arguments by value (map == null) and
 // block b is its block b.
 template <int MODEL, bool FULL>
-__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCfg<MODEL>::MIN_BLOCKS)
+__global__ void __launch_bounds__(NeuronCfg<MODEL, FULL>::THREADS, NeuronCfg<MODEL, FULL>::MIN_BLOCKS)
     neuron_kernel(StepArgs a, PopArgs p0, const PopArgs *__restrict__ pops, const uint2 *__restrict__ map) {
-  pdl_wait();
+  float sv[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT];
   if (map == nullptr) {
-    neuron_block<MODEL, FULL>(a, p0, blockIdx.x);
+    // Population state is written only by the neuron update, and the last
+    // one finished before the previous scatter passed its own wait (which
+    // is what let this kernel start): the state is read before the wait,
+    // so that its loads overlap the previous kernel's tail.
+    load_state<MODEL, FULL>(p0, blockIdx.x, sv);
+    pdl_wait();
+    neuron_block<MODEL, FULL>(a, p0, blockIdx.x, sv);
   } else {
+    pdl_wait();
     const uint2 bm = map[blockIdx.x];
-    neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y);
+    load_state<MODEL, FULL>(pops[bm.x], bm.y, sv);
+    neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y, sv);
   }
   pdl_release();
 }
@@ -1317,6 +1376,62 @@ __device__ __forceinline__ uint32_t bulk_elems(unsigned char *region, uint32_t *
   return at / esz + (b - b0);
 }
 
+// Poisson-source synapses (source order free) and the end of the step, for a
+// pre-centric scatter block of THREADS threads.  base[i]: network i's ring
+// slot base; ev / src_ev: this block's event counts per network (shared
+// memory; ev holds its recurrent events already).
+template <uint32_t THREADS>
+__device__ __forceinline__ void red_sources_and_close(const StepArgs *__restrict__ nets, uint32_t n_nets,
+                                                      const RedNet *rn, unsigned long long *ev,
+                                                      unsigned long long *src_ev, uint32_t *done,
+                                                      unsigned long long pl) {
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  for (uint32_t i = 0; i < n_nets; ++i) {
+    const StepArgs &a = nets[i];
+    const uint32_t base = rn[i].base;
+    unsigned long long sev = 0;
+    for (uint32_t t = blockIdx.x * THREADS + tid; t < a.n_src_syn; t += gridDim.x * THREADS) {
+      uint32_t lo = 0, hi = a.n_runs - 1;  // largest run with run_off[run] <= t
+      while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+        if (__ldg(a.run_off + mid) <= t) lo = mid;
+        else hi = mid - 1;
+      }
+      const uint32_t off = t - __ldg(a.run_off + lo);
+      const float p = __ldg(a.run_p + lo);
+      if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + lo) + off, 0, *a.step, p)) {
+        const uint8_t code = __ldg(a.run_code + lo);
+        uint32_t slot = base + max(code_delay(code), 1u);
+        if (slot >= a.nslots) slot -= a.nslots;
+        red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + __ldg(a.run_post0 + lo) + off,
+                __ldg(a.run_w + lo), pl);
+        ++sev;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sev += __shfl_xor_sync(0xffffffffu, sev, o);
+    if (lane == 0 && sev) atomicAdd(&src_ev[i], sev);
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < n_nets; i += THREADS) {
+    const unsigned long long e = ev[i] + src_ev[i];
+    if (e) atomicAdd(nets[i].ev_step, e);
+    if (src_ev[i]) atomicAdd(nets[i].ev_src_step, src_ev[i]);
+  }
+  // the last block to finish closes the step of every network
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const uint32_t t = atomicAdd(done, 1u);
+    if (t == gridDim.x - 1) {
+      __threadfence();
+      for (uint32_t i = 0; i < n_nets; ++i) end_of_step_last(nets[i], *nets[i].red_cnt);
+      *done = 0;
+      __threadfence();
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Pre-centric scatter (rings_exact networks, and the atomic mode).  When every
 // partial sum of a ring cell is exact, the order of the adds does not change
@@ -1511,62 +1626,154 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
   }
   __syncthreads();
   pdl_release();
-  // Poisson-source synapses in runs, source order free (exact sums)
+  red_sources_and_close<kRedThreads>(nets, n_nets, S.nets, S.ev, S.src_ev, done, pl);
+}
+
+// ---------------------------------------------------------------------------
+// Warp-walk scatter: the same sums as scatter_red_kernel (rings_exact
+// networks, and the atomic mode) without a staging ring, so nothing in it
+// waits on another warp.  Every warp of the grid takes spiking rows
+// round-robin: row r of a network's flat list goes to warp (r + rot) mod W,
+// where W is the number of warps and rot continues the round-robin from the
+// previous network of the table.  A warp holds up to 32 rows at a time (lane
+// k the bounds of its k-th row; a warp scan gives each row's offset in their
+// concatenation) and walks the concatenation kWalkU * 32 synapses per round:
+// each lane finds the row of each of its synapses (a binary search over the
+// lanes' offsets when the warp holds several rows), issues its kWalkU
+// coalesced record loads (evict_first in L2), then the kWalkU reds into the
+// ring cells (red.global.add, evict_last, so the rings stay L2-resident).
+// Poisson-source synapses that the neuron kernel does not take follow, one
+// per thread; the last block to finish closes the step of every network.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kWalkThreads = 256;
+constexpr uint32_t kWalkWarps = kWalkThreads / 32;
+constexpr int kWalkU = 8;  // record loads per lane in flight per round
+
+__global__ void __launch_bounds__(kWalkThreads, 4)
+    scatter_walk_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done) {
+  __shared__ RedNet rn[kPoolMax];
+  __shared__ unsigned long long ev[kPoolMax], src_ev[kPoolMax];
+  __shared__ uint32_t rot[kPoolMax];
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const uint32_t W = gridDim.x * kWalkWarps;
+  const uint32_t gw = blockIdx.x * kWalkWarps + (tid >> 5);
+  pdl_wait();
+  for (uint32_t i = tid; i < n_nets; i += kWalkThreads) {
+    const StepArgs &a = nets[i];
+    RedNet r;
+    r.ring = a.ring;
+    r.code = a.code;
+    r.Nd = a.Nd;
+    r.nslots = a.nslots;
+    r.base = (uint32_t)(*a.step % a.nslots);
+    r.post_mask = a.post_mask;
+    r.fmt = a.wbf16 ? 1 : a.wfp8 ? 2 : 0;
+    rn[i] = r;
+    ev[i] = 0;
+    src_ev[i] = 0;
+  }
+  if (tid == 0) {
+    uint32_t r0 = 0;
+    for (uint32_t i = 0; i < n_nets; ++i) {
+      rot[i] = r0;
+      r0 = (uint32_t)(((unsigned long long)r0 + *nets[i].red_cnt) % W);
+    }
+  }
+  __syncthreads();
+  const unsigned long long pl = policy_evict_last(), pf = policy_evict_first();
   for (uint32_t i = 0; i < n_nets; ++i) {
     const StepArgs &a = nets[i];
-    const uint32_t base = S.nets[i].base;
-    unsigned long long src_ev = 0;
-    for (uint32_t t = blockIdx.x * kRedThreads + tid; t < a.n_src_syn; t += gridDim.x * kRedThreads) {
-      uint32_t lo = 0, hi = a.n_runs - 1;  // largest run with run_off[run] <= t
-      while (lo < hi) {
-        const uint32_t mid = lo + ((hi - lo + 1) >> 1);
-        if (__ldg(a.run_off + mid) <= t) lo = mid;
-        else hi = mid - 1;
+    const RedNet r = rn[i];
+    const uint32_t n = *a.red_cnt;
+    unsigned long long wev = 0;
+    for (uint32_t g0 = (gw + W - rot[i]) % W; g0 < n; g0 += 32u * W) {
+      const uint32_t rr = g0 + lane * W;
+      uint32_t beg = 0, len = 0;
+      float scale = 1.0f;
+      if (rr < n) {
+        const uint2 rb = a.red_rows[rr];
+        beg = rb.x;
+        len = rb.y - rb.x;
+        if (r.fmt == 2) scale = __ldg(a.row_scale + a.red_flat[rr]);
       }
-      const uint32_t off = t - __ldg(a.run_off + lo);
-      const float p = __ldg(a.run_p + lo);
-      if (p > 0.0f && poisson_spike(__ldg(a.run_seed0 + lo) + off, 0, *a.step, p)) {
-        const uint8_t code = __ldg(a.run_code + lo);
-        uint32_t slot = base + max(code_delay(code), 1u);
-        if (slot >= a.nslots) slot -= a.nslots;
-        red_add(a.ring + ((size_t)code_ring(code) * a.nslots + slot) * a.Nd + __ldg(a.run_post0 + lo) + off,
-                __ldg(a.run_w + lo), pl);
-        ++src_ev;
-      }
-    }
+      uint32_t incl = len;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) src_ev += __shfl_xor_sync(0xffffffffu, src_ev, o);
-    if (lane == 0 && src_ev) atomicAdd(&S.src_ev[i], src_ev);
-  }
-  __syncthreads();
-  for (uint32_t i = tid; i < n_nets; i += kRedThreads) {
-    const unsigned long long e = S.ev[i] + S.src_ev[i];
-    if (e) atomicAdd(nets[i].ev_step, e);
-    if (S.src_ev[i]) atomicAdd(nets[i].ev_src_step, S.src_ev[i]);
-  }
-  // the last block to finish closes the step of every network
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    const uint32_t t = atomicAdd(done, 1u);
-    if (t == gridDim.x - 1) {
-      __threadfence();
-      for (uint32_t i = 0; i < n_nets; ++i) end_of_step_last(nets[i], *nets[i].red_cnt);
-      *done = 0;
-      __threadfence();
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t excl = incl - len;
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      const uint32_t nrows = min(32u, (n - g0 + W - 1) / W);  // lanes holding a row
+      wev += total;
+      for (uint32_t b0 = 0; b0 < total; b0 += 32u * kWalkU) {
+        uint32_t idx[kWalkU], ok = 0;
+        float sc[kWalkU];
+#pragma unroll
+        for (int u = 0; u < kWalkU; ++u) {
+          const uint32_t e = b0 + (uint32_t)u * 32u + lane;
+          uint32_t k = 0;  // the row holding synapse e: the last row whose offset is <= e
+          if (nrows > 1) {
+#pragma unroll
+            for (uint32_t st = 16; st > 0; st >>= 1) {
+              const uint32_t c = k + st;
+              const uint32_t ex = __shfl_sync(0xffffffffu, excl, c & 31u);
+              if (c < nrows && ex <= e) k = c;
+            }
+          }
+          idx[u] = __shfl_sync(0xffffffffu, beg, k) + (e - __shfl_sync(0xffffffffu, excl, k));
+          sc[u] = __shfl_sync(0xffffffffu, scale, k);
+          ok |= (e < total ? 1u : 0u) << u;
+        }
+        uint32_t xs[kWalkU], ws[kWalkU];
+#pragma unroll
+        for (int u = 0; u < kWalkU; ++u) {
+          xs[u] = 0;
+          ws[u] = 0;
+          if ((ok >> u) & 1u) {
+            if (r.fmt == 0) {
+              const uint2 rec = ld_stream_edge(a.edge + idx[u], pf);
+              xs[u] = rec.x;
+              ws[u] = rec.y;
+            } else {
+              xs[u] = ld_stream_u32(a.edge_x + idx[u], pf);
+              ws[u] = r.fmt == 1 ? ld_stream_u16(a.w16 + idx[u], pf) : ld_stream_u8(a.w8 + idx[u], pf);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kWalkU; ++u) {
+          if (!((ok >> u) & 1u)) continue;
+          const uint32_t x = xs[u];
+          uint32_t wbits = ws[u];
+          if (r.fmt == 1) wbits <<= 16;
+          else if (r.fmt == 2) wbits = __float_as_uint(e4m3_to_f32(wbits) * sc[u]);
+          const uint8_t code = r.code ? __ldg(r.code + idx[u]) : (uint8_t)(x >> 24);
+          uint32_t slot = r.base + max(code_delay(code), 1u);
+          if (slot >= r.nslots) slot -= r.nslots;
+          red_add(r.ring + ((size_t)code_ring(code) * r.nslots + slot) * r.Nd + (x & r.post_mask),
+                  __uint_as_float(wbits), pl);
+        }
+      }
     }
+    if (lane == 0 && wev) atomicAdd(&ev[i], wev);
   }
+  __syncthreads();
+  pdl_release();
+  red_sources_and_close<kWalkThreads>(nets, n_nets, rn, ev, src_ev, done, pl);
 }
 
 // One neuron launch per model over the populations of several networks (a
 // pool): block b takes map[b] = (network, population, block within it).
 template <int MODEL, bool FULL>
-__global__ void __launch_bounds__(NeuronCfg<MODEL>::THREADS, FULL ? 1 : NeuronCfg<MODEL>::MIN_BLOCKS)
+__global__ void __launch_bounds__(NeuronCfg<MODEL, FULL>::THREADS, NeuronCfg<MODEL, FULL>::MIN_BLOCKS)
     neuron_pool_kernel(const StepArgs *__restrict__ nets, const PopArgs *__restrict__ pops,
                        const uint4 *__restrict__ map) {
   const uint4 m = map[blockIdx.x];
   pdl_wait();
-  neuron_block<MODEL, FULL>(nets[m.x], pops[m.y], m.z);
+  float sv[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT];
+  load_state<MODEL, FULL>(pops[m.y], m.z, sv);
+  neuron_block<MODEL, FULL>(nets[m.x], pops[m.y], m.z, sv);
   pdl_release();
 }
 
@@ -1807,7 +2014,10 @@ __global__ void __launch_bounds__(kNeuronBlock) ext_spikes_kernel(StepArgs a, ui
     __shared__ uint32_t red_base;
     if (tid == 0) red_base = total ? atomicAdd(a.red_cnt, total) : 0u;
     __syncthreads();
-    if (sp) a.red_flat[red_base + before] = gi;
+    if (sp) {
+      a.red_flat[red_base + before] = gi;
+      a.red_rows[red_base + before] = make_uint2(__ldg(a.row_ptr + gi), __ldg(a.row_ptr + gi + 1));
+    }
   } else {
     if (sp) a.spk[(size_t)gblk * kNeuronBlock + before] = make_uint2(gi, __ldg(a.row_ptr + gi));
     if (tid == 0) a.blk_cnt[gblk] = total;

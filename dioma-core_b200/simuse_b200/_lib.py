@@ -34,6 +34,8 @@ SIGNATURES = {
     "sg_synchronize": [vp],
     "sg_debug_stall_scatter": [vp, i32],
     "sg_autotune": [vp, u32, vp, vp, vp, vp],
+    "sg_probe_red_rate": [i32, u64, u32, vp],
+    "sg_scatter_schedule": [vp, vp, vp],
     "sg_pool_create": [vp, i32],
     "sg_pool_destroy": [vp],
     "sg_pool_add": [vp, vp],

@@ -219,6 +219,14 @@ class Network:
         check(lib().sg_scatter_mode(self._h, C.byref(m)))
         return ("ordered", "exact", "atomic")[m.value]
 
+    @property
+    def scatter_schedule(self) -> tuple[int, int]:
+        """(variant, blocks per SM) of the pre-centric scatter: 0-3 the staged
+        pipeline's stage-ring shapes, 4 the warp walk."""
+        v, b = C.c_int(), C.c_uint32()
+        check(lib().sg_scatter_schedule(self._h, C.byref(v), C.byref(b)))
+        return v.value, b.value
+
     def set_deterministic(self, on: bool):
         check(lib().sg_set_deterministic(self._h, 1 if on else 0))
 

@@ -1,10 +1,11 @@
 """``Sweep`` — an uneven parameter sweep of Kuramoto populations and
 Izhikevich pulse networks advancing together on one GPU.
 
-Kuramoto half: a ``KuramotoBatch``.  Each instance runs on one CTA for all
-of a run's steps (phases and RK4 sums in registers up to 4096 oscillators,
-streamed through L2 above), so a run of any length is one persistent launch
-per CTA shape, largest instances first.
+Kuramoto half: a ``KuramotoBatch``.  Each instance runs on one CTA (up to
+4096 oscillators) or one thread-block cluster of 2-8 CTAs (up to 65,536) for
+all of a run's steps, phases and RK4 sums in registers, so a run of any
+length is one persistent launch per shape, each shape on its own stream,
+largest instances first.
 
 Izhikevich half: one ``Network`` holding every instance as its own
 population (the pulse-network recipe: 100 distinct targets per neuron,

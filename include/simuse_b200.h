@@ -73,8 +73,9 @@ int sg_net_destroy(sg_net *net);                /* Drop for Network */
    the condition is reported once. */
 int sg_synchronize(sg_net *net);
 /* No counterpart in the reference.  Tunes the pre-centric scatter's
-   schedule (its shared-memory stage ring: stages x synapses per stage, and
-   blocks per SM) on the network's own next steps: each candidate runs
+   schedule (variants 0-3: a shared-memory stage ring of stages x synapses
+   per stage; variant 4: the warp walk without stages; and blocks per SM)
+   on the network's own next steps: each candidate runs
    `steps` steps (after a warm-up chunk), timed on the device, and the
    fastest is kept.  Every schedule gives the same results, so these are
    ordinary simulation steps (the step counter advances).  Reports the
@@ -82,6 +83,10 @@ int sg_synchronize(sg_net *net);
    path there is nothing to tune (times 0). */
 int sg_autotune(sg_net *net, uint32_t steps, float *fixed_ms, float *best_ms, int *best_variant,
                 uint32_t *best_bps);
+/* No counterpart in the reference.  The pre-centric scatter's current
+   schedule (the variant and blocks per SM that sg_autotune reports; a new
+   network starts on variant 4, or on SG_RED_VARIANT when that is set). */
+int sg_scatter_schedule(sg_net *net, int *variant, uint32_t *blocks_per_sm);
 /* Test hook (no reference counterpart): on != 0 makes the pre-centric
    scatter's producer stop feeding its consumers, whose waits then run out
    (~1 s per step) and set the device error that sg_synchronize reports. */
@@ -461,6 +466,15 @@ int sg_push_spikes(const uint32_t *row_ptr, const uint32_t *col, const float *we
 int sg_push_spikes_noalloc(const uint32_t *row_ptr, const uint32_t *col, const float *weights,
                            const uint8_t *delays, uint32_t n_neurons, const uint32_t *active,
                            uint32_t n_active, uint64_t step, float *ring, void *stream);
+
+/* No counterpart in the reference: a measurement probe.  The rate
+   (reductions per second) at which this GPU completes independent
+   red.global.add.f32 operations on hashed cells of an n_cells-float array
+   (the size of a network's delay rings), from a full-occupancy grid of
+   `iters` reds per thread: the ceiling of the pre-centric scatter's event
+   adds, as a STREAM copy is the ceiling of a streaming kernel.  Allocates
+   and frees its own array. */
+int sg_probe_red_rate(int device, uint64_t n_cells, uint32_t iters, double *reds_per_s);
 
 /* ---- pools of resident networks (continuous batching) ----------------------
    No counterpart in the reference (its callers step one Network at a time;

@@ -119,8 +119,9 @@ def test_exact_ring_readback_between_steps():
 
 def test_autotuned_schedule_keeps_the_oracle_bits():
     """sg_autotune runs the network's next steps under every candidate
-    schedule of the pre-centric scatter and keeps the fastest; the steps are
-    ordinary simulation steps and every schedule gives the same bits."""
+    schedule of the pre-centric scatter (four stage-ring shapes and the warp
+    walk) and keeps the fastest; the steps are ordinary simulation steps and
+    every schedule gives the same bits."""
     g = sg.Network(0)
     gp = _balanced(g)
     g.build()
@@ -130,8 +131,8 @@ def test_autotuned_schedule_keeps_the_oracle_bits():
     rep = g.autotune(steps=20)
     assert rep["fixed_ms_per_step"] > 0 and rep["tuned_ms_per_step"] > 0
     assert rep["tuned_ms_per_step"] <= rep["fixed_ms_per_step"]
-    done = g.step_counter            # 12 candidates x (20 warm-up + 20 timed) steps
-    assert done == 12 * 40
+    done = g.step_counter            # 15 candidates (5 schedules x 1-3 blocks per SM) x (20 warm-up + 20 timed)
+    assert done == 15 * 40
     c.step(done)
     g.enable_raster(50)
     g.step(50)

@@ -35,9 +35,11 @@ def _sweep(sizes, ks, seed=4):
 
 
 # sizes reach every kernel shape: resident CTAs of 64 (partial and full),
-# 128, 256 and 512 threads, and streamed instances up to the 65,536 maximum
-SIZES = [256, 512, 1000, 2048, 4096, 4097, 9000, 20000, 65536]
-KS = [0.0, 1.5, 0.7, 1.2, 1.5, 2.0, 2.5, 3.0, 4.0]
+# 128, 256 and 512 threads; clusters of 2 (4097: one oscillator in the
+# second CTA), 4, 8 CTAs of 512 threads (16384 and 32768 fill them) and
+# 8 CTAs of 1024 threads up to the 65,536 maximum
+SIZES = [256, 512, 1000, 2048, 4096, 4097, 9000, 20000, 65536, 16384, 32769]
+KS = [0.0, 1.5, 0.7, 1.2, 1.5, 2.0, 2.5, 3.0, 4.0, 1.0, 3.5]
 
 
 def test_kuramoto_batch_vs_fp64_oracle():
@@ -81,7 +83,7 @@ def test_kuramoto_deterministic_and_alone_equals_batched():
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
     off = np.concatenate([[0], np.cumsum(sizes.astype(np.int64))])
-    for i in (1, 4, 6, 8):
+    for i in (1, 4, 5, 6, 8, 10):
         kb = KuramotoBatch(sizes[i:i + 1], ks[i:i + 1], dt)
         kb.set_state(th0[off[i]:off[i + 1]], om[off[i]:off[i + 1]])
         kb.record(steps)
@@ -89,6 +91,25 @@ def test_kuramoto_deterministic_and_alone_equals_batched():
         assert np.array_equal(kb.theta(), runs[0][0][off[i]:off[i + 1]])
         assert np.array_equal(kb.r()[0], runs[0][1][i])
         kb.close()
+
+
+def test_kuramoto_streamed_form_vs_fp64_oracle(monkeypatch):
+    """The streamed form (one CTA per instance, state re-read every stage),
+    which instances above 4096 oscillators take on a device that cannot hold
+    their cluster shape, forced here through SG_KURAMOTO_STREAMED."""
+    monkeypatch.setenv("SG_KURAMOTO_STREAMED", "1")
+    steps, dt = 300, 0.01
+    sizes, ks, th0, om = _sweep([5000, 40000], [2.0, 3.0], seed=5)
+    kb = KuramotoBatch(sizes, ks, dt)
+    kb.set_state(th0, om)
+    kb.record(steps)
+    kb.run(steps)
+    r = kb.r()
+    off = [0, 5000, 45000]
+    for i in range(2):
+        _, o_r = O.kuramoto_rk4(th0[off[i]:off[i + 1]], om[off[i]:off[i + 1]], float(ks[i]), dt, steps, precision=1)
+        assert np.abs(r[i].astype(np.float64) - o_r).max() <= R_TOL
+    kb.close()
 
 
 def test_kuramoto_uncoupled_is_rotation():
