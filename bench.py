@@ -365,7 +365,7 @@ def run_serving(args, local):
     for lam in (5.0, 20.0, 50.0, 100.0, 200.0):
         arrive = np.cumsum(-np.log(1.0 - W.uniform01(78, int(lam), np.arange(n_req, dtype=np.uint64))) / lam)
         reqs = make()
-        srv = S.Server(device=local, budget_bytes=160 * 10**9, max_resident=32, chunk=250)
+        srv = S.Server(device=local, budget_bytes=160 * 10**9, max_resident=32, chunk=256)
         t0 = time.perf_counter()
         for r, ta in zip(reqs, arrive):
             wait = t0 + ta - time.perf_counter()

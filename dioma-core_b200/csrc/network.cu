@@ -265,7 +265,7 @@ struct sg_net {
   // raster readback work buffers, kept from call to call (grow only)
   DBuf<unsigned long long> rr_cnt, rr_off;
   DBuf<uint8_t> rr_temp;
-  DBuf<uint32_t> rr_step, rr_idx, rr_pd, rr_pg;
+  DBuf<uint32_t> rr_step, rr_idx, rr_pd, rr_pg, rr_soff;
   DBuf<uint32_t> rr_counts;  // spikes per device neuron over every read since the raster was enabled
   // a staged read (sg_raster_stage / sg_raster_fetch): steps [rst_t0, rst_t1)
   // compacted on rstream after the steps that wrote them; the network's
@@ -795,6 +795,22 @@ __global__ void raster_write_kernel(const uint32_t *bits, uint32_t cap, uint32_t
       ++pos;
     }
   }
+}
+
+// off[s] = the first position of step t0 + s in the step-ordered out_step
+// (s = 0..k; off[k] = total): a lower-bound search per step.
+__global__ void raster_step_off_kernel(const uint32_t *out_step, uint64_t total, uint64_t t0, uint64_t k,
+                                       uint32_t *off) {
+  const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s > k) return;
+  const uint32_t want = (uint32_t)(t0 + s);
+  uint64_t lo = 0, hi = total;  // first position with out_step >= want
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if (out_step[mid] < want) lo = mid + 1;
+    else hi = mid;
+  }
+  off[s] = (uint32_t)(s == k ? total : lo);
 }
 
 template <typename F> void launch_grid(uint64_t n, F f) {
@@ -3105,6 +3121,64 @@ int sg_raster_fetch(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap, u
     }
     SG_CUDA(cudaStreamSynchronize(rs));
     net->rstaged = false;
+  });
+}
+
+int sg_raster_fetch_csr(sg_net *net, uint32_t *step_off, uint64_t off_cap, uint32_t *idx, uint64_t cap,
+                        uint64_t *t0, uint64_t *n_steps, uint64_t *n_out) {
+  NET_CHECK(net);
+  return run([&] {
+    SG_REQUIRE(t0 && n_steps && n_out, SG_E_INVALID, "null output");
+    SG_REQUIRE(net->rstaged, SG_E_STATE, "no staged raster read");
+    const uint64_t words = net->Nd / 32;
+    const uint64_t k = words ? net->rst_nw / words : 0;
+    *t0 = net->rst_t0;
+    *n_steps = k;
+    *n_out = 0;
+    SG_REQUIRE(off_cap >= k + 1, SG_E_INVALID, "step offset buffer too small: " + std::to_string(k + 1));
+    SG_REQUIRE(step_off, SG_E_INVALID, "null step offsets");
+    DevGuard g(net->device);
+    if (net->rst_nb == 0) {
+      for (uint64_t i = 0; i <= k; ++i) step_off[i] = 0;
+      net->rstaged = false;
+      return;
+    }
+    cudaStream_t rs = net->rstream;
+    SG_CUDA(cudaStreamSynchronize(rs));
+    const uint64_t total = *net->rst_total;
+    *n_out = total;
+    SG_REQUIRE(total <= cap, SG_E_INVALID, "output buffer too small: " + std::to_string(total) + " spikes");
+    SG_REQUIRE(total < 0xFFFFFFFFull, SG_E_OVERFLOW, "more than 2^32-2 spikes in one staged read");
+    if (total > net->rr_step.n) {  // the write was skipped: grow the room and write now
+      net->rr_step.ensure(total + total / 4);
+      net->rr_idx.ensure(total + total / 4);
+      enqueue_raster_write(net, rs, net->rst_t0, net->rst_nw, net->rst_nb, net->rr_step.n);
+    }
+    net->rr_soff.ensure(k + 1);
+    raster_step_off_kernel<<<(unsigned)((k + 256) / 256), 256, 0, rs>>>(net->rr_step.p, total, net->rst_t0, k,
+                                                                        net->rr_soff.p);
+    SG_CUDA(cudaGetLastError());
+    SG_CUDA(cudaMemcpyAsync(step_off, net->rr_soff.p, (k + 1) * 4, cudaMemcpyDeviceToHost, rs));
+    if (total) {
+      SG_REQUIRE(idx, SG_E_INVALID, "null output");
+      SG_CUDA(cudaMemcpyAsync(idx, net->rr_idx.p, total * 4, cudaMemcpyDeviceToHost, rs));
+    }
+    SG_CUDA(cudaStreamSynchronize(rs));
+    net->rstaged = false;
+  });
+}
+
+int sg_host_alloc(uint64_t bytes, void **out) {
+  return run([&] {
+    SG_REQUIRE(out, SG_E_INVALID, "null output");
+    *out = nullptr;
+    if (bytes) SG_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+  });
+}
+
+int sg_host_free(void *p) {
+  return run([&] {
+    if (p) SG_CUDA(cudaFreeHost(p));
   });
 }
 

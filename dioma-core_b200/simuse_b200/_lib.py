@@ -85,6 +85,9 @@ SIGNATURES = {
     "sg_raster_read_events": [vp, vp, vp, u64, vp],
     "sg_raster_stage": [vp],
     "sg_raster_fetch": [vp, vp, vp, u64, vp],
+    "sg_raster_fetch_csr": [vp, vp, u64, vp, u64, vp, vp, vp],
+    "sg_host_alloc": [u64, vp],
+    "sg_host_free": [vp],
     "sg_raster_counts": [vp, vp],
     "sg_profile_enable": [vp, i32],
     "sg_profile_read": [vp, vp, vp],

@@ -298,6 +298,24 @@ class Network:
     def enable_raster(self, capacity_steps: int):
         check(lib().sg_raster_enable(self._h, capacity_steps))
         self._raster_mark = self.step_counter
+        self._raster_cap = int(capacity_steps)
+
+    def raster_fetch_csr(self, off_buf: "PinnedU32", idx_buf: "PinnedU32"):
+        """The staged batch as (t0, step offsets, indices): the spikes of step
+        t0 + s are indices[offsets[s]:offsets[s + 1]].  Copied through the
+        page-locked buffers (grown when too small) into new arrays."""
+        t0, k, n = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        off_buf.ensure(getattr(self, "_raster_cap", 0) + 1)
+        while True:
+            rc = lib().sg_raster_fetch_csr(self._h, off_buf.ptr, off_buf.n, idx_buf.ptr, idx_buf.n, C.byref(t0),
+                                           C.byref(k), C.byref(n))
+            if rc < 0 and n.value > idx_buf.n:  # too small: the batch stays staged
+                idx_buf.ensure(n.value + n.value // 2)
+                continue
+            check(rc)
+            break
+        kk, nn = int(k.value), int(n.value)
+        return int(t0.value), off_buf.a[:kk + 1].copy(), idx_buf.a[:nn].copy()
 
     def read_raster(self) -> np.ndarray:
         """Spike raster [steps since the last read][total_neurons] as uint8."""
@@ -576,6 +594,45 @@ class Network:
         out = C.c_void_p()
         check(lib().sg_stream(self._h, C.byref(out)))
         return out.value or 0
+
+
+class PinnedU32:
+    """A page-locked host array of uint32 (sg_host_alloc) for readbacks that
+    the device copies into directly; grown on demand, freed by close()."""
+
+    def __init__(self, n: int = 0):
+        self._p = C.c_void_p()
+        self.n = 0
+        self.a = np.empty(0, np.uint32)
+        self.ensure(n)
+
+    @property
+    def ptr(self):
+        return self._p.value
+
+    def ensure(self, n: int) -> np.ndarray:
+        n = int(n)
+        if n <= self.n:
+            return self.a
+        self.close()
+        p = C.c_void_p()
+        check(lib().sg_host_alloc(n * 4, C.byref(p)))
+        self._p, self.n = p, n
+        self.a = np.ctypeslib.as_array((C.c_uint32 * n).from_address(p.value))
+        return self.a
+
+    def close(self):
+        if self._p is not None and self._p.value:
+            self.a = np.empty(0, np.uint32)
+            lib().sg_host_free(self._p)
+        self._p = C.c_void_p()
+        self.n = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Pool:

@@ -38,7 +38,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 from . import workloads as W
-from .network import IZH, LIF, W_BF16, Network, Pool
+from .network import IZH, LIF, W_BF16, Network, PinnedU32, Pool
 
 
 @dataclasses.dataclass
@@ -55,14 +55,37 @@ class Request:
     t_admit: float = 0.0
     t_done: float = 0.0
     footprint: int = 0
-    spike_steps: np.ndarray | None = None
-    spike_index: np.ndarray | None = None
+    # the spike raster as read, one (t0, step offsets, indices) chunk per read:
+    # the spikes of step t0 + s are indices[offsets[s]:offsets[s + 1]]
+    chunks: list | None = None
     rates_hz: np.ndarray | None = None
     error: str | None = None
+    _flat: tuple | None = dataclasses.field(default=None, repr=False)
 
     @property
     def latency(self) -> float:
         return self.t_done - self.t_submit
+
+    def _flatten(self):
+        if self._flat is None and self.chunks is not None:
+            st = [np.repeat(np.arange(t0, t0 + off.size - 1, dtype=np.uint32), np.diff(off)) for t0, off, _ in self.chunks]
+            ix = [i for _, _, i in self.chunks]
+            self._flat = (np.concatenate(st) if st else np.empty(0, np.uint32),
+                          np.concatenate(ix) if ix else np.empty(0, np.uint32))
+        return self._flat
+
+    @property
+    def spike_steps(self) -> np.ndarray | None:
+        """Step of every spike, in step then neuron order (built from the chunks
+        on first use)."""
+        f = self._flatten()
+        return None if f is None else f[0]
+
+    @property
+    def spike_index(self) -> np.ndarray | None:
+        """Global neuron index of every spike, in the order of spike_steps."""
+        f = self._flatten()
+        return None if f is None else f[1]
 
     @property
     def dt_ms(self) -> float:
@@ -128,41 +151,43 @@ def run_alone(req: Request, device: int = 0, chunk: int = 256) -> Request:
     return req
 
 
+_solo_bufs = threading.local()
+
+
 def _run_to_end(net: Network, req: Request, chunk: int):
+    bufs = getattr(_solo_bufs, "b", None)
+    if bufs is None:
+        bufs = _solo_bufs.b = (PinnedU32(), PinnedU32(1 << 20))
     net.enable_raster(chunk)
-    st, ix = [], []
+    chunks = []
     done = 0
     while done < req.steps:
         k = min(chunk, req.steps - done)
         net.step(k)
-        s, i = net.read_spike_events()
-        st.append(s)
-        ix.append(i)
+        net.raster_stage()
+        chunks.append(net.raster_fetch_csr(*bufs))
         done += k
-    _finish(req, st, ix, net.raster_counts())
+    _finish(req, chunks, net.raster_counts())
 
 
-def _finish(req: Request, st, ix, counts):
-    """The request's results: its spike events in step order and its rates
-    from the per-neuron spike counts the device kept while reading."""
-    req.spike_steps = np.concatenate(st) if st else np.empty(0, np.uint32)
-    req.spike_index = np.concatenate(ix) if ix else np.empty(0, np.uint32)
+def _finish(req: Request, chunks, counts):
+    """The request's results: its spike raster as read (chunks of step
+    offsets and indices) and its rates from the per-neuron spike counts the
+    device kept while reading."""
+    req.chunks = chunks
     req.rates_hz = counts / (req.steps * req.dt_ms * 1e-3)
 
 
 class _Resident:
-    def __init__(self, req: Request, net: Network):
+    def __init__(self, req: Request, net: Network, bufs):
         self.req, self.net = req, net
+        self.bufs = bufs            # page-locked (step offsets, indices) buffers, the server's
         self.done = 0
-        self.st: list[np.ndarray] = []
-        self.ix: list[np.ndarray] = []
+        self.chunks: list = []
         self.counts: np.ndarray | None = None
-        self.cap = 1 << 16          # fetch buffer size: the last batch's size and a half
 
     def fetch(self):
-        s, i = self.net.raster_fetch(self.cap)
-        self.cap = max(self.cap, s.size + s.size // 2)
-        return s, i
+        return self.net.raster_fetch_csr(*self.bufs)
 
 
 class Server:
@@ -171,12 +196,13 @@ class Server:
     budget_bytes: device memory the resident networks may hold together.
     max_resident: resident networks at most (pool members; at most 64).
     chunk: steps the pool advances per tick (a tick is shortened to the
-    fewest steps any resident network still needs).
+    fewest steps any resident network still needs); a multiple of 32 runs
+    as whole 32-step graphs.
     builders: threads building admitted networks beside the running pool.
     """
 
     def __init__(self, device: int = 0, budget_bytes: int = 160 * 10**9, max_resident: int = 32,
-                 chunk: int = 250, builders: int = 2, readers: int = 8):
+                 chunk: int = 256, builders: int = 2, readers: int = 8):
         self.device, self.budget, self.chunk = device, int(budget_bytes), chunk
         self.max_resident = min(max_resident, 64)
         self._pending: queue.Queue[Request] = queue.Queue()
@@ -197,6 +223,8 @@ class Server:
         # stepping thread
         self._readers = ThreadPoolExecutor(max_workers=max(1, readers))
         self._finishing: queue.Queue = queue.Queue()
+        # page-locked readback buffers, reused by the requests that follow
+        self._free_bufs: list = []
         self._builders = [threading.Thread(target=self._build_loop, daemon=True) for _ in range(max(1, builders))]
         self._stepper = threading.Thread(target=self._step_loop, daemon=True)
         self._finisher = threading.Thread(target=self._finish_loop, daemon=True)
@@ -255,7 +283,7 @@ class Server:
             if item is None:
                 return
             r = item
-            _finish(r.req, r.st, r.ix, r.counts)
+            _finish(r.req, r.chunks, r.counts)
             self._complete(r.req)
 
     def _build_loop(self):
@@ -325,7 +353,8 @@ class Server:
                 req.footprint = true_fp
                 net.enable_raster(self.chunk)
                 pool.add(net)
-                resident.append(_Resident(req, net))
+                bufs = self._free_bufs.pop() if self._free_bufs else (PinnedU32(), PinnedU32(1 << 20))
+                resident.append(_Resident(req, net, bufs))
             t1 = time.perf_counter()
             ph["admit"] += t1 - t0
             if not resident and not inflight:
@@ -342,13 +371,12 @@ class Server:
             ph["step"] += t2 - t1
             # tick t - 1's spikes (their copies ran beside tick t)
             for r, fut in inflight:
-                s, i = fut.result()
-                r.st.append(s)
-                r.ix.append(i)
+                r.chunks.append(fut.result())
             inflight = []
             for r in draining:              # finished requests whose last batch is in
                 r.counts = r.net.raster_counts()
                 r.net.close()
+                self._free_bufs.append(r.bufs)
                 with self._lock:
                     self._reserved -= r.req.footprint
                 self._finishing.put(r)
@@ -371,3 +399,7 @@ class Server:
                 draining.append(r)
             ph["leave"] += time.perf_counter() - t4
         pool.close()
+        for off, idx in self._free_bufs:
+            off.close()
+            idx.close()
+        self._free_bufs = []

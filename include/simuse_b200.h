@@ -304,6 +304,18 @@ int sg_raster_read_events(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t 
    sg_raster_enable and sg_raster_counts refuse while one is staged. */
 int sg_raster_stage(sg_net *net);
 int sg_raster_fetch(sg_net *net, uint32_t *steps, uint32_t *idx, uint64_t cap, uint64_t *n_out);
+/* The staged batch with its steps as offsets (4 bytes per spike instead of
+   8): *t0 = the batch's first step, *n_steps = its steps k, and the spikes
+   of step *t0 + s are idx[step_off[s] .. step_off[s + 1]), s < k
+   (step_off[k] = *n_out).  off_cap must be >= k + 1; when cap is too small
+   it fails with *n_out = the count and the batch stays staged. */
+int sg_raster_fetch_csr(sg_net *net, uint32_t *step_off, uint64_t off_cap, uint32_t *idx, uint64_t cap,
+                        uint64_t *t0, uint64_t *n_steps, uint64_t *n_out);
+/* No counterpart in the reference: page-locked host memory (cudaHostAlloc,
+   portable) for readback buffers, so that device-to-host copies are DMA
+   straight into them; *out = NULL for 0 bytes. */
+int sg_host_alloc(uint64_t bytes, void **out);
+int sg_host_free(void *p);
 /* Spikes per neuron over every event read (plain or staged) since the raster
    was enabled; counts[total]. */
 int sg_raster_counts(sg_net *net, uint32_t *counts);

@@ -55,3 +55,34 @@ def test_admission_by_budget_and_arrivals_during_run():
     assert srv2.wait_idle(60)
     srv2.close()
     assert big.error is not None   # larger than the whole budget: refused, not queued forever
+
+
+def test_csr_fetch_equals_event_pairs():
+    """sg_raster_fetch_csr (step offsets and indices, through page-locked
+    buffers) gives the spikes of the plain (step, index) read of the same
+    network, and the same per-neuron counts."""
+    from simuse_b200.network import PinnedU32
+    r = S.Request("lif", 20000, 31, 300)
+    a, b = S.build_request(r), S.build_request(r)
+    a.build()
+    b.build()
+    a.enable_raster(100)
+    b.enable_raster(100)
+    bufs = (PinnedU32(), PinnedU32(16))   # a tiny index buffer: the fetch grows it
+    total = 0
+    for _ in range(3):
+        a.step(100)
+        b.step(100)
+        s, i = a.read_spike_events()
+        b.raster_stage()
+        t0, off, ix = b.raster_fetch_csr(*bufs)
+        assert off.size == 101 and off[0] == 0 and off[-1] == ix.size == i.size
+        st = np.repeat(np.arange(t0, t0 + off.size - 1), np.diff(off))
+        assert np.array_equal(st, s) and np.array_equal(ix, i)
+        total += ix.size
+    assert total > 0
+    assert np.array_equal(a.raster_counts(), b.raster_counts())
+    for x in (a, b):
+        x.close()
+    for x in bufs:
+        x.close()
