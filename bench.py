@@ -683,7 +683,7 @@ def run_ours(args):
     sp, _ = net.read_stats()
     p_spikes = float(sp[-p_steps:].mean()) if sp.size else 0.0
     scatter_kernel = ("scatter_kernel" if scatter_path == "ordered" else
-                      "scatter_walk_kernel" if net.scatter_schedule[0] == 4 else "scatter_red_kernel")
+                      "scatter_walk_kernel" if net.scatter_schedule[0] >= 4 else "scatter_red_kernel")
     phases = ["neuron_kernel<LIF>", scatter_kernel]
     alg = [spec["n"] * B_NEURON,
            p_rec * (B_EVENT_EXPAND + B_EVENT_APPLY) + p_spikes * B_SPIKE]

@@ -236,6 +236,8 @@ struct sg_net {
   sg_pool *pool = nullptr;     // the pool this network steps in, if any
   int red_variant = 0;         // pre-centric scatter schedule (sg_autotune)
   uint32_t red_bps = kRedBlocksPerSM;
+  bool l2_reserved = false;    // holds a share of the device's L2 set-aside (setup_l2_setaside)
+  size_t l2_bytes = 0;         // the ring bytes counted for that share
   unsigned long long drv_folded = ~0ull;
   bool any_drv = false;
   // short-term plasticity: profiles, staged per-edge ids (kept only once an
@@ -1429,9 +1431,13 @@ void upload_args(sg_net *net, const StepArgs &a) {
 // first being the fixed one; sg_autotune picks one per network, with the
 // blocks per SM.
 // (4 x 1024, 8 x 512, 3 x 2048, 6 x 512: launch_step_red), and the warp walk
-// without stages (variant 4, scatter_walk_kernel).
-constexpr int kNumRedVariants = 5;
+// without stages (scatter_walk_kernel): variant 4 loads and reduces a round
+// at a time (8 records per lane), variants 5 and 6 load the next round's
+// records (4 or 8 per lane) before reducing the current one.
+constexpr int kNumRedVariants = 7;
 constexpr int kWalkVariant = 4;
+constexpr int kWalkPipeVariant = 5;
+bool is_walk_variant(int v) { return v >= kWalkVariant; }
 
 template <uint32_t ST, uint32_t CH> void allow_red_smem_v() {
   SG_CUDA(cudaFuncSetAttribute(scatter_red_kernel<ST, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1453,9 +1459,12 @@ unsigned sm_count(int device) {
 }
 
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
-                     uint32_t *done, uint32_t *err, uint32_t stall);
+                     uint32_t *done, uint32_t *err, uint32_t stall, bool plain);
+// FP32 weights in 8-byte records with the code byte inside: the walk's
+// compile-time form for such networks.
+bool plain_records(const StepArgs &a) { return !a.wbf16 && !a.wfp8 && a.code == nullptr; }
 
-// The schedule a network or pool starts with: SG_RED_VARIANT (0..4) when set,
+// The schedule a network or pool starts with: SG_RED_VARIANT (0..6) when set,
 // else the warp walk.
 int default_red_variant() {
   static const int v = [] {
@@ -1681,16 +1690,89 @@ void launch_step_kernel(void (*kernel)(KArgs...), unsigned grid, unsigned block,
   SG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
 }
 
+// L2 residency of the delay rings.  Both scatters add events into the rings
+// in L2 with the evict_last priority (random 4-byte reductions, or the
+// ordered path's loads and stores) while the spiking rows' records stream
+// through L2 with evict_first.  Lines marked evict_last are kept only within
+// the L2 set-aside for persisting accesses, which is empty by default, so
+// this process's context reserves up to the rings' size (at most the
+// device's maximum: 79 MiB of the B200's 126 MB L2) once a network steps
+// (the sum of the rings of every network that has stepped on the device).
+// The set-aside is a limit of this process's CUDA context on the device (it
+// ends with the context) and is put back to its earlier value when the last
+// network that reserved it is destroyed.  SG_L2_PERSIST=0 leaves it alone.
+bool l2_setaside_on() {
+  static const bool on = [] {
+    const char *e = std::getenv("SG_L2_PERSIST");
+    return e == nullptr || std::atoi(e) != 0;
+  }();
+  return on;
+}
+constexpr int kMaxDevices = 64;
+std::mutex g_l2_mu;
+int g_l2_refs[kMaxDevices];
+size_t g_l2_saved[kMaxDevices];
+size_t g_l2_rings[kMaxDevices];  // ring bytes of the networks holding a share
+
+void setup_l2_setaside(sg_net *net) {
+  if (net->l2_reserved || !l2_setaside_on() || net->d_ring.n == 0 || net->device < 0 ||
+      net->device >= kMaxDevices)
+    return;
+  int max_persist = 0;
+  SG_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, net->device));
+  if (max_persist <= 0) return;
+  std::lock_guard<std::mutex> lk(g_l2_mu);
+  const int d = net->device;
+  size_t cur = 0;
+  SG_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+  if (g_l2_refs[d] == 0) {
+    g_l2_saved[d] = cur;
+    g_l2_rings[d] = 0;
+  }
+  const size_t bytes = net->d_ring.n * sizeof(float);
+  const size_t want = std::min(g_l2_rings[d] + bytes, (size_t)max_persist);
+  if (cur < want) SG_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+  g_l2_rings[d] += bytes;
+  ++g_l2_refs[d];
+  net->l2_reserved = true;
+  net->l2_bytes = bytes;
+}
+
+// The device's set-aside goes back to its earlier value with the last
+// network that reserved it (lines still marked persisting become normal).
+void release_l2_setaside(sg_net *net) {
+  if (!net->l2_reserved) return;
+  std::lock_guard<std::mutex> lk(g_l2_mu);
+  net->l2_reserved = false;
+  g_l2_rings[net->device] -= net->l2_bytes;
+  if (--g_l2_refs[net->device] == 0) {
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_saved[net->device]);
+  }
+}
+
 // One launch of the pre-centric scatter with schedule `variant` and `bps`
 // blocks per SM over a table of networks.
+template <int U, bool PIPE>
+void launch_walk(cudaStream_t s, unsigned grid, bool plain, const StepArgs *nets, uint32_t n_nets, uint32_t *done) {
+  if (plain) launch_step_kernel(scatter_walk_kernel<U, PIPE, true>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+  else launch_step_kernel(scatter_walk_kernel<U, PIPE, false>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+}
+
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
-                     uint32_t *done, uint32_t *err, uint32_t stall) {
+                     uint32_t *done, uint32_t *err, uint32_t stall, bool plain) {
   const unsigned grid = sm_count(device) * bps;
   // the stall test hook acts on the staged pipeline's waits (the walk has none)
-  if (variant == kWalkVariant && stall) variant = 0;
+  if (is_walk_variant(variant) && stall) variant = 0;
   switch (variant) {
     case kWalkVariant:
-      launch_step_kernel(scatter_walk_kernel, grid * 2, kWalkThreads, 0, s, nets, n_nets, done);
+      launch_walk<8, false>(s, grid * 2, plain, nets, n_nets, done);
+      break;
+    case kWalkPipeVariant:
+      launch_walk<4, true>(s, grid * 2, plain, nets, n_nets, done);
+      break;
+    case kWalkPipeVariant + 1:  // 3 resident blocks per SM (more registers per thread)
+      launch_walk<8, true>(s, grid * 3 / 2, plain, nets, n_nets, done);
       break;
     case 1:
       launch_step_kernel(scatter_red_kernel<8, 512>, grid, kRedThreads, sizeof(RedSmemT<8, 512>), s, nets, n_nets,
@@ -1768,7 +1850,7 @@ void enqueue_rest(sg_net *net, const StepArgs &a) {
       ext_spikes_kernel<<<p.cap / kNeuronBlock, kNeuronBlock, 0, s>>>(a, p.dev_off, p.n, p.ext_src);
   if (a.red) {
     launch_step_red(s, net->device, net->red_variant, net->red_bps, (const StepArgs *)net->d_args.p, 1u,
-                    net->d_done.p, net->d_err.p, net->debug_stall);
+                    net->d_done.p, net->d_err.p, net->debug_stall, plain_records(a));
   } else {
     if (net->seg32) launch_step_kernel(scatter_kernel<true>, net->G, kScatterThreads, net->scatter_smem, s, a);
     else launch_step_kernel(scatter_kernel<false>, net->G, kScatterThreads, net->scatter_smem, s, a);
@@ -1852,6 +1934,7 @@ void do_steps(sg_net *net, uint32_t n) {
   if (net->learn_on) net->d_l_motor.zero(net->stream);  // motor counts are per step call
   const StepArgs a = make_args(net);
   upload_args(net, a);
+  setup_l2_setaside(net);
   const uint32_t G = 32;  // steps per graph launch
   uint32_t done = 0;
   if (n >= G) {
@@ -1924,6 +2007,7 @@ int sg_net_destroy(sg_net *net) {
     DevGuard g(net->device);
     cudaStreamSynchronize(net->stream);
     drop_graph(net);
+    release_l2_setaside(net);
     for (auto e : net->prof_ev) cudaEventDestroy(e);
     if (net->rstream) {
       cudaStreamSynchronize(net->rstream);
@@ -4093,8 +4177,10 @@ void pool_enqueue_step(sg_pool *pool) {
   pool_launch_neuron<kIZH>(pool);
   pool_launch_neuron<kGPEA>(pool);
   pool_launch_neuron<kHH>(pool);
+  bool plain = true;
+  for (const StepArgs &a : pool->h_nets) plain = plain && plain_records(a);
   launch_step_red(pool->stream, pool->device, default_red_variant(), kRedBlocksPerSM, (const StepArgs *)pool->d_nets.p,
-                  (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u);
+                  (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u, plain);
 }
 
 }  // namespace
@@ -4169,6 +4255,7 @@ int sg_pool_step(sg_pool *pool, uint32_t n_steps) {
     DevGuard g(pool->device);
     for (sg_net *net : pool->members) SG_REQUIRE(net->total > 0, SG_E_STATE, "pool: an empty network");
     pool_prepare(pool);
+    for (sg_net *net : pool->members) setup_l2_setaside(net);
     // the pool's steps follow everything queued on the members' streams
     for (sg_net *net : pool->members) {
       SG_CUDA(cudaEventRecord(pool->ev, net->stream));

@@ -1633,30 +1633,49 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
 // Warp-walk scatter: the same sums as scatter_red_kernel (rings_exact
 // networks, and the atomic mode) without a staging ring, so nothing in it
 // waits on another warp.  Every warp of the grid takes spiking rows
-// round-robin: row r of a network's flat list goes to warp (r + rot) mod W,
-// where W is the number of warps and rot continues the round-robin from the
-// previous network of the table.  A warp holds up to 32 rows at a time (lane
+// round-robin: row r of a network's flat list goes to warp place
+// (r + rot) mod W, where W is the number of warps, rot continues the
+// round-robin from the previous network of the table, and warp w of block b
+// has place w * G + b (G blocks).  A warp holds up to 32 rows at a time (lane
 // k the bounds of its k-th row; a warp scan gives each row's offset in their
-// concatenation) and walks the concatenation kWalkU * 32 synapses per round:
+// concatenation) and walks the concatenation U * 32 synapses per round:
 // each lane finds the row of each of its synapses (a binary search over the
-// lanes' offsets when the warp holds several rows), issues its kWalkU
-// coalesced record loads (evict_first in L2), then the kWalkU reds into the
-// ring cells (red.global.add, evict_last, so the rings stay L2-resident).
+// lanes' offsets when the warp holds several rows), issues its U coalesced
+// record loads (evict_first in L2), then the U reds into the ring cells
+// (red.global.add, evict_last, so the rings stay L2-resident).
 // Poisson-source synapses that the neuron kernel does not take follow, one
 // per thread; the last block to finish closes the step of every network.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kWalkThreads = 256;
 constexpr uint32_t kWalkWarps = kWalkThreads / 32;
-constexpr int kWalkU = 8;  // record loads per lane in flight per round
 
-__global__ void __launch_bounds__(kWalkThreads, 4)
+// One round of a warp's walk: the U synapses of each lane, as loaded.
+template <int U> struct WalkRound {
+  uint32_t x[U], w[U], c[U];  // record x word (post | code), weight bits, code byte (separate code array)
+  float s[U];                 // FP8 row scale
+  uint32_t ok;                // bit u: synapse u of this lane exists
+};
+
+// U: record loads per lane per round.  PIPE = false: each round loads its
+// records and then issues its reds.  PIPE = true: the records of the next
+// round are loaded before the reds of the current one are issued, so that
+// their memory latency runs under the reds instead of after them (a warp's
+// loads queue behind its earlier reds).  PLAIN: every network of the table
+// has FP32 weights in 8-byte records with the code byte inside (no BF16/FP8
+// arrays, no separate code array), known at compile time so that the
+// round's registers hold only the records.
+template <int U, bool PIPE, bool PLAIN>
+__global__ void __launch_bounds__(kWalkThreads, (PIPE && U > 4) ? 3 : 4)
     scatter_walk_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done) {
   __shared__ RedNet rn[kPoolMax];
   __shared__ unsigned long long ev[kPoolMax], src_ev[kPoolMax];
   __shared__ uint32_t rot[kPoolMax];
   const uint32_t tid = threadIdx.x, lane = lane_id();
   const uint32_t W = gridDim.x * kWalkWarps;
-  const uint32_t gw = blockIdx.x * kWalkWarps + (tid >> 5);
+  // the warp's place in the round-robin: warp w of block b is w * G + b, so
+  // that consecutive rows go to consecutive blocks and every SM gets its
+  // share of the step's rows (not the first blocks all of them)
+  const uint32_t gw = (tid >> 5) * gridDim.x + blockIdx.x;
   pdl_wait();
   for (uint32_t i = tid; i < n_nets; i += kWalkThreads) {
     const StepArgs &a = nets[i];
@@ -1684,6 +1703,8 @@ __global__ void __launch_bounds__(kWalkThreads, 4)
   for (uint32_t i = 0; i < n_nets; ++i) {
     const StepArgs &a = nets[i];
     const RedNet r = rn[i];
+    const uint32_t fmt = PLAIN ? 0u : r.fmt;
+    const uint8_t *code_arr = PLAIN ? nullptr : r.code;
     const uint32_t n = *a.red_cnt;
     unsigned long long wev = 0;
     for (uint32_t g0 = (gw + W - rot[i]) % W; g0 < n; g0 += 32u * W) {
@@ -1694,7 +1715,7 @@ __global__ void __launch_bounds__(kWalkThreads, 4)
         const uint2 rb = a.red_rows[rr];
         beg = rb.x;
         len = rb.y - rb.x;
-        if (r.fmt == 2) scale = __ldg(a.row_scale + a.red_flat[rr]);
+        if (fmt == 2) scale = __ldg(a.row_scale + a.red_flat[rr]);
       }
       uint32_t incl = len;
 #pragma unroll
@@ -1706,11 +1727,12 @@ __global__ void __launch_bounds__(kWalkThreads, 4)
       const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
       const uint32_t nrows = min(32u, (n - g0 + W - 1) / W);  // lanes holding a row
       wev += total;
-      for (uint32_t b0 = 0; b0 < total; b0 += 32u * kWalkU) {
-        uint32_t idx[kWalkU], ok = 0;
-        float sc[kWalkU];
+      // load the records of the round starting at synapse b0 of the concatenation
+      auto fetch = [&](uint32_t b0, WalkRound<U> &R) {
+        uint32_t idx[U];
+        R.ok = 0;
 #pragma unroll
-        for (int u = 0; u < kWalkU; ++u) {
+        for (int u = 0; u < U; ++u) {
           const uint32_t e = b0 + (uint32_t)u * 32u + lane;
           uint32_t k = 0;  // the row holding synapse e: the last row whose offset is <= e
           if (nrows > 1) {
@@ -1722,37 +1744,60 @@ __global__ void __launch_bounds__(kWalkThreads, 4)
             }
           }
           idx[u] = __shfl_sync(0xffffffffu, beg, k) + (e - __shfl_sync(0xffffffffu, excl, k));
-          sc[u] = __shfl_sync(0xffffffffu, scale, k);
-          ok |= (e < total ? 1u : 0u) << u;
+          R.s[u] = PLAIN ? 1.0f : __shfl_sync(0xffffffffu, scale, k);
+          R.ok |= (e < total ? 1u : 0u) << u;
         }
-        uint32_t xs[kWalkU], ws[kWalkU];
 #pragma unroll
-        for (int u = 0; u < kWalkU; ++u) {
-          xs[u] = 0;
-          ws[u] = 0;
-          if ((ok >> u) & 1u) {
-            if (r.fmt == 0) {
+        for (int u = 0; u < U; ++u) {
+          R.x[u] = 0;
+          R.w[u] = 0;
+          R.c[u] = 0;
+          if ((R.ok >> u) & 1u) {
+            if (fmt == 0) {
               const uint2 rec = ld_stream_edge(a.edge + idx[u], pf);
-              xs[u] = rec.x;
-              ws[u] = rec.y;
+              R.x[u] = rec.x;
+              R.w[u] = rec.y;
             } else {
-              xs[u] = ld_stream_u32(a.edge_x + idx[u], pf);
-              ws[u] = r.fmt == 1 ? ld_stream_u16(a.w16 + idx[u], pf) : ld_stream_u8(a.w8 + idx[u], pf);
+              R.x[u] = ld_stream_u32(a.edge_x + idx[u], pf);
+              R.w[u] = fmt == 1 ? ld_stream_u16(a.w16 + idx[u], pf) : ld_stream_u8(a.w8 + idx[u], pf);
             }
+            if (code_arr) R.c[u] = __ldg(code_arr + idx[u]);
           }
         }
+      };
+      // the reds of a loaded round
+      auto apply = [&](const WalkRound<U> &R) {
 #pragma unroll
-        for (int u = 0; u < kWalkU; ++u) {
-          if (!((ok >> u) & 1u)) continue;
-          const uint32_t x = xs[u];
-          uint32_t wbits = ws[u];
-          if (r.fmt == 1) wbits <<= 16;
-          else if (r.fmt == 2) wbits = __float_as_uint(e4m3_to_f32(wbits) * sc[u]);
-          const uint8_t code = r.code ? __ldg(r.code + idx[u]) : (uint8_t)(x >> 24);
+        for (int u = 0; u < U; ++u) {
+          if (!((R.ok >> u) & 1u)) continue;
+          const uint32_t x = R.x[u];
+          uint32_t wbits = R.w[u];
+          if (fmt == 1) wbits <<= 16;
+          else if (fmt == 2) wbits = __float_as_uint(e4m3_to_f32(wbits) * R.s[u]);
+          const uint8_t code = code_arr ? (uint8_t)R.c[u] : (uint8_t)(x >> 24);
           uint32_t slot = r.base + max(code_delay(code), 1u);
           if (slot >= r.nslots) slot -= r.nslots;
           red_add(r.ring + ((size_t)code_ring(code) * r.nslots + slot) * r.Nd + (x & r.post_mask),
                   __uint_as_float(wbits), pl);
+        }
+      };
+      constexpr uint32_t kRound = 32u * (uint32_t)U;
+      if (PIPE) {
+        WalkRound<U> A, B;
+        fetch(0, A);
+        for (uint32_t b0 = 0; b0 < total; b0 += 2u * kRound) {
+          if (b0 + kRound < total) fetch(b0 + kRound, B);
+          else B.ok = 0;
+          apply(A);
+          if (b0 + 2u * kRound < total) fetch(b0 + 2u * kRound, A);
+          else A.ok = 0;
+          apply(B);
+        }
+      } else {
+        for (uint32_t b0 = 0; b0 < total; b0 += kRound) {
+          WalkRound<U> A;
+          fetch(b0, A);
+          apply(A);
         }
       }
     }
