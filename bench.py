@@ -84,6 +84,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the scatter's fixed schedule (no sg_autotune before the timed steps)")
     ap.add_argument("--case", default="headline", choices=["headline", "kuramoto-sweep", "izh-batch", "hh-stdp",
                                                            "lif-learn", "taas", "sweep"],
                     help="headline: the JSON line above; the others time one workload alone (also the "
@@ -627,6 +629,10 @@ def run_ours(args):
         net.step(PARITY_STEPS)
         first_raster = net.read_raster()
         net.enable_raster(0)
+    # the scatter's schedule, picked by the library's autotuner on this
+    # network's own steps (ordinary simulation steps; every schedule gives
+    # the same bits on the pre-centric path)
+    tune = net.autotune(steps=200) if scatter_path != "ordered" and not args.no_autotune else None
     for _ in range(args.warmup):
         net.step(S)
     barrier()
@@ -682,8 +688,9 @@ def run_ours(args):
     p_rec = p_events - p_src
     sp, _ = net.read_stats()
     p_spikes = float(sp[-p_steps:].mean()) if sp.size else 0.0
+    net_schedule = net.scatter_schedule
     scatter_kernel = ("scatter_kernel" if scatter_path == "ordered" else
-                      "scatter_walk_kernel" if net.scatter_schedule[0] >= 4 else "scatter_red_kernel")
+                      "scatter_walk_kernel" if net_schedule[0] >= 4 else "scatter_red_kernel")
     phases = ["neuron_kernel<LIF>", scatter_kernel]
     alg = [spec["n"] * B_NEURON,
            p_rec * (B_EVENT_EXPAND + B_EVENT_APPLY) + p_spikes * B_SPIKE]
@@ -707,7 +714,11 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": config(args, name, spec, scatter_path),
+        "config": {**config(args, name, spec, scatter_path),
+                   "schedule": ({"autotuned": True, "variant": tune["variant"], "blocks_per_sm": tune["blocks_per_sm"],
+                                 "fixed_ms_per_sim_step": tune["fixed_ms_per_step"],
+                                 "tuned_ms_per_sim_step": tune["tuned_ms_per_step"]} if tune else
+                                {"autotuned": False, "variant": list(net_schedule)})},
         "sim": {"ms_per_sim_step": step_ms, "events_per_sim_step": events / (args.steps * S),
                 "recurrent_events_per_sim_step": p_rec, "source_events_per_sim_step": p_src,
                 "spikes_per_sim_step": mean_spk, "rate_hz": mean_spk / spec["n"] / (spec["dt"] * 1e-3),

@@ -1433,8 +1433,9 @@ void upload_args(sg_net *net, const StepArgs &a) {
 // (4 x 1024, 8 x 512, 3 x 2048, 6 x 512: launch_step_red), and the warp walk
 // without stages (scatter_walk_kernel): variant 4 loads and reduces a round
 // at a time (8 records per lane), variants 5 and 6 load the next round's
-// records (4 or 8 per lane) before reducing the current one.
-constexpr int kNumRedVariants = 7;
+// records (4 or 8 per lane) before reducing the current one, variant 7 cuts
+// every row into 4 pieces that different warps walk.
+constexpr int kNumRedVariants = 8;
 constexpr int kWalkVariant = 4;
 constexpr int kWalkPipeVariant = 5;
 bool is_walk_variant(int v) { return v >= kWalkVariant; }
@@ -1464,7 +1465,7 @@ void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, cons
 // compile-time form for such networks.
 bool plain_records(const StepArgs &a) { return !a.wbf16 && !a.wfp8 && a.code == nullptr; }
 
-// The schedule a network or pool starts with: SG_RED_VARIANT (0..6) when set,
+// The schedule a network or pool starts with: SG_RED_VARIANT (0..7) when set,
 // else the warp walk.
 int default_red_variant() {
   static const int v = [] {
@@ -1753,10 +1754,11 @@ void release_l2_setaside(sg_net *net) {
 
 // One launch of the pre-centric scatter with schedule `variant` and `bps`
 // blocks per SM over a table of networks.
-template <int U, bool PIPE>
+template <int U, bool PIPE, uint32_t P = 1>
 void launch_walk(cudaStream_t s, unsigned grid, bool plain, const StepArgs *nets, uint32_t n_nets, uint32_t *done) {
-  if (plain) launch_step_kernel(scatter_walk_kernel<U, PIPE, true>, grid, kWalkThreads, 0, s, nets, n_nets, done);
-  else launch_step_kernel(scatter_walk_kernel<U, PIPE, false>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+  if (plain)
+    launch_step_kernel(scatter_walk_kernel<U, PIPE, true, P>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+  else launch_step_kernel(scatter_walk_kernel<U, PIPE, false, P>, grid, kWalkThreads, 0, s, nets, n_nets, done);
 }
 
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
@@ -1773,6 +1775,9 @@ void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, cons
       break;
     case kWalkPipeVariant + 1:  // 3 resident blocks per SM (more registers per thread)
       launch_walk<8, true>(s, grid * 3 / 2, plain, nets, n_nets, done);
+      break;
+    case kWalkPipeVariant + 2:  // rows cut in 4 pieces
+      launch_walk<8, false, 4>(s, grid * 2, plain, nets, n_nets, done);
       break;
     case 1:
       launch_step_kernel(scatter_red_kernel<8, 512>, grid, kRedThreads, sizeof(RedSmemT<8, 512>), s, nets, n_nets,

@@ -618,6 +618,13 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     }
   }
   const uint32_t cnt = __popc(nib);
+  // the synapse range of this thread's first spiking neuron, loaded now so
+  // that its latency runs under the block's count exchange (pre-centric path)
+  uint2 rows0 = make_uint2(0u, 0u);
+  if (a.red && nib) {
+    const uint32_t q0 = (uint32_t)__ffs(nib) - 1u;
+    rows0 = make_uint2(__ldg(a.row_ptr + gi0 + q0), __ldg(a.row_ptr + gi0 + q0 + 1));
+  }
   uint32_t incl = cnt;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -653,11 +660,13 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
     if (tid == 0) red_base = total ? atomicAdd(a.red_cnt, total) : 0u;
     __syncthreads();
     uint32_t pos = red_base + before;
+    bool first = true;
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
       if (nib & (1u << q)) {  // the spiking neuron and its synapse range
         a.red_flat[pos] = gi0 + q;
-        a.red_rows[pos] = make_uint2(__ldg(a.row_ptr + gi0 + q), __ldg(a.row_ptr + gi0 + q + 1));
+        a.red_rows[pos] = first ? rows0 : make_uint2(__ldg(a.row_ptr + gi0 + q), __ldg(a.row_ptr + gi0 + q + 1));
+        first = false;
         ++pos;
       }
   } else {
@@ -1663,8 +1672,10 @@ template <int U> struct WalkRound {
 // loads queue behind its earlier reds).  PLAIN: every network of the table
 // has FP32 weights in 8-byte records with the code byte inside (no BF16/FP8
 // arrays, no separate code array), known at compile time so that the
-// round's registers hold only the records.
-template <int U, bool PIPE, bool PLAIN>
+// round's registers hold only the records.  P: each spiking row is cut into
+// P pieces of (nearly) equal length, and the pieces are the work items of
+// the round-robin (more warps busy on a step with few long rows).
+template <int U, bool PIPE, bool PLAIN, uint32_t P = 1>
 __global__ void __launch_bounds__(kWalkThreads, (PIPE && U > 4) ? 3 : 4)
     scatter_walk_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done) {
   __shared__ RedNet rn[kPoolMax];
@@ -1695,7 +1706,7 @@ __global__ void __launch_bounds__(kWalkThreads, (PIPE && U > 4) ? 3 : 4)
     uint32_t r0 = 0;
     for (uint32_t i = 0; i < n_nets; ++i) {
       rot[i] = r0;
-      r0 = (uint32_t)(((unsigned long long)r0 + *nets[i].red_cnt) % W);
+      r0 = (uint32_t)(((unsigned long long)r0 + (unsigned long long)*nets[i].red_cnt * P) % W);
     }
   }
   __syncthreads();
@@ -1705,16 +1716,23 @@ __global__ void __launch_bounds__(kWalkThreads, (PIPE && U > 4) ? 3 : 4)
     const RedNet r = rn[i];
     const uint32_t fmt = PLAIN ? 0u : r.fmt;
     const uint8_t *code_arr = PLAIN ? nullptr : r.code;
-    const uint32_t n = *a.red_cnt;
+    const unsigned long long n = (unsigned long long)*a.red_cnt * P;  // work items: row pieces
     unsigned long long wev = 0;
-    for (uint32_t g0 = (gw + W - rot[i]) % W; g0 < n; g0 += 32u * W) {
-      const uint32_t rr = g0 + lane * W;
+    for (unsigned long long g0 = (gw + W - rot[i]) % W; g0 < n; g0 += 32ull * W) {
+      const unsigned long long it = g0 + (unsigned long long)lane * W;
       uint32_t beg = 0, len = 0;
       float scale = 1.0f;
-      if (rr < n) {
+      if (it < n) {
+        const uint32_t rr = (uint32_t)(it / P);
         const uint2 rb = a.red_rows[rr];
-        beg = rb.x;
-        len = rb.y - rb.x;
+        if (P == 1) {
+          beg = rb.x;
+          len = rb.y - rb.x;
+        } else {
+          const unsigned long long L = rb.y - rb.x, j = it % P;
+          beg = rb.x + (uint32_t)(L * j / P);
+          len = rb.x + (uint32_t)(L * (j + 1) / P) - beg;
+        }
         if (fmt == 2) scale = __ldg(a.row_scale + a.red_flat[rr]);
       }
       uint32_t incl = len;
@@ -1725,7 +1743,7 @@ __global__ void __launch_bounds__(kWalkThreads, (PIPE && U > 4) ? 3 : 4)
       }
       const uint32_t excl = incl - len;
       const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-      const uint32_t nrows = min(32u, (n - g0 + W - 1) / W);  // lanes holding a row
+      const uint32_t nrows = (uint32_t)min(32ull, (n - g0 + W - 1) / W);  // lanes holding a row (piece)
       wev += total;
       // load the records of the round starting at synapse b0 of the concatenation
       auto fetch = [&](uint32_t b0, WalkRound<U> &R) {
