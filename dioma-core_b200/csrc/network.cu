@@ -1434,8 +1434,9 @@ void upload_args(sg_net *net, const StepArgs &a) {
 // without stages (scatter_walk_kernel): variant 4 loads and reduces a round
 // at a time (8 records per lane), variants 5 and 6 load the next round's
 // records (4 or 8 per lane) before reducing the current one, variant 7 cuts
-// every row into 4 pieces that different warps walk.
-constexpr int kNumRedVariants = 8;
+// every row into 4 pieces that different warps walk, variant 8 does that
+// with 4 records per lane and 6 blocks per SM (48 warps).
+constexpr int kNumRedVariants = 9;
 constexpr int kWalkVariant = 4;
 constexpr int kWalkPipeVariant = 5;
 bool is_walk_variant(int v) { return v >= kWalkVariant; }
@@ -1465,7 +1466,7 @@ void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, cons
 // compile-time form for such networks.
 bool plain_records(const StepArgs &a) { return !a.wbf16 && !a.wfp8 && a.code == nullptr; }
 
-// The schedule a network or pool starts with: SG_RED_VARIANT (0..7) when set,
+// The schedule a network or pool starts with: SG_RED_VARIANT (0..8) when set,
 // else the warp walk.
 int default_red_variant() {
   static const int v = [] {
@@ -1754,11 +1755,12 @@ void release_l2_setaside(sg_net *net) {
 
 // One launch of the pre-centric scatter with schedule `variant` and `bps`
 // blocks per SM over a table of networks.
-template <int U, bool PIPE, uint32_t P = 1>
+template <int U, bool PIPE, uint32_t P = 1, int MINB = (PIPE && U > 4) ? 3 : 4>
 void launch_walk(cudaStream_t s, unsigned grid, bool plain, const StepArgs *nets, uint32_t n_nets, uint32_t *done) {
   if (plain)
-    launch_step_kernel(scatter_walk_kernel<U, PIPE, true, P>, grid, kWalkThreads, 0, s, nets, n_nets, done);
-  else launch_step_kernel(scatter_walk_kernel<U, PIPE, false, P>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+    launch_step_kernel(scatter_walk_kernel<U, PIPE, true, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+  else
+    launch_step_kernel(scatter_walk_kernel<U, PIPE, false, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
 }
 
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
@@ -1778,6 +1780,9 @@ void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, cons
       break;
     case kWalkPipeVariant + 2:  // rows cut in 4 pieces
       launch_walk<8, false, 4>(s, grid * 2, plain, nets, n_nets, done);
+      break;
+    case kWalkPipeVariant + 3:  // rows cut in 4 pieces, 6 resident blocks per SM (fewer registers per thread)
+      launch_walk<4, false, 4, 6>(s, grid * 3, plain, nets, n_nets, done);
       break;
     case 1:
       launch_step_kernel(scatter_red_kernel<8, 512>, grid, kRedThreads, sizeof(RedSmemT<8, 512>), s, nets, n_nets,

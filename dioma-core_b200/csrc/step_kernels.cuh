@@ -1674,9 +1674,10 @@ template <int U> struct WalkRound {
 // arrays, no separate code array), known at compile time so that the
 // round's registers hold only the records.  P: each spiking row is cut into
 // P pieces of (nearly) equal length, and the pieces are the work items of
-// the round-robin (more warps busy on a step with few long rows).
-template <int U, bool PIPE, bool PLAIN, uint32_t P = 1>
-__global__ void __launch_bounds__(kWalkThreads, (PIPE && U > 4) ? 3 : 4)
+// the round-robin (more warps busy on a step with few long rows).  MINB:
+// resident blocks per SM the registers are sized for.
+template <int U, bool PIPE, bool PLAIN, uint32_t P = 1, int MINB = (PIPE && U > 4) ? 3 : 4>
+__global__ void __launch_bounds__(kWalkThreads, MINB)
     scatter_walk_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done) {
   __shared__ RedNet rn[kPoolMax];
   __shared__ unsigned long long ev[kPoolMax], src_ev[kPoolMax];

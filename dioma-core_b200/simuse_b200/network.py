@@ -222,8 +222,8 @@ class Network:
     @property
     def scatter_schedule(self) -> tuple[int, int]:
         """(variant, blocks per SM) of the pre-centric scatter: 0-3 the staged
-        pipeline's stage-ring shapes, 4-7 the warp walk (5 and 6 pipelined, 7
-        rows in 4 pieces)."""
+        pipeline's stage-ring shapes, 4-8 the warp walk (5 and 6 pipelined, 7
+        and 8 rows in 4 pieces)."""
         v, b = C.c_int(), C.c_uint32()
         check(lib().sg_scatter_schedule(self._h, C.byref(v), C.byref(b)))
         return v.value, b.value

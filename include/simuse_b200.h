@@ -74,9 +74,10 @@ int sg_net_destroy(sg_net *net);                /* Drop for Network */
 int sg_synchronize(sg_net *net);
 /* No counterpart in the reference.  Tunes the pre-centric scatter's
    schedule (variants 0-3: a shared-memory stage ring of stages x synapses
-   per stage; variants 4-7: the warp walk without stages, 5 and 6 loading
-   the next round of records before reducing the current one, 7 walking
-   each row as 4 pieces; and blocks per SM)
+   per stage; variants 4-8: the warp walk without stages, 5 and 6 loading
+   the next round of records before reducing the current one, 7 and 8
+   walking each row as 4 pieces (8 at 6 blocks per SM); and blocks per
+   SM)
    on the network's own next steps: each candidate runs
    `steps` steps (after a warm-up chunk), timed on the device, and the
    fastest is kept.  Every schedule gives the same results, so these are

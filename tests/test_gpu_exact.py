@@ -131,8 +131,8 @@ def test_autotuned_schedule_keeps_the_oracle_bits():
     rep = g.autotune(steps=20)
     assert rep["fixed_ms_per_step"] > 0 and rep["tuned_ms_per_step"] > 0
     assert rep["tuned_ms_per_step"] <= rep["fixed_ms_per_step"]
-    done = g.step_counter            # 24 candidates (8 schedules x 1-3 blocks per SM) x (20 warm-up + 20 timed)
-    assert done == 24 * 40
+    done = g.step_counter            # 27 candidates (9 schedules x 1-3 blocks per SM) x (20 warm-up + 20 timed)
+    assert done == 27 * 40
     c.step(done)
     g.enable_raster(50)
     g.step(50)

@@ -101,10 +101,10 @@ def test_sweep_autotuned_schedule_gives_the_fixed_schedule_bits():
     for tune in (True, False):
         sw = sg.Sweep(kura, sizes, izh_seed0=300)
         if tune:
-            res = sw.net.autotune(steps=10)      # 24 candidates x (10 warm-up + 10 timed) steps
+            res = sw.net.autotune(steps=10)      # 27 candidates x (10 warm-up + 10 timed) steps
             assert res["variant"] >= 0 and 1 <= res["blocks_per_sm"] <= 3
             tuned_steps = sw.net.step_counter
-            assert tuned_steps == 24 * 20
+            assert tuned_steps == 27 * 20
         else:
             sw.run(tuned_steps, 0)               # the same steps on the fixed schedule
         sw.run(IZH_STEPS, 100)
