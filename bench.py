@@ -392,6 +392,7 @@ def run_serving(args, local):
             "one_at_a_time_p50_latency_s": float(np.percentile(q_lat, 50)),
             "one_at_a_time_p99_latency_s": float(np.percentile(q_lat, 99)),
             "speedup_vs_one_at_a_time": (n_req / t_all) / (n_req / fin), "pool_ticks": srv.ticks,
+            "server_loop_s": {k: round(v, 3) for k, v in srv.phase_s.items()},
             "results_same_as_alone": bool(same), "errors": int(sum(r.error is not None for r in reqs))}
     return out
 

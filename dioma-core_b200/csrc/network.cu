@@ -1461,10 +1461,14 @@ unsigned sm_count(int device) {
 }
 
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
-                     uint32_t *done, uint32_t *err, uint32_t stall, bool plain);
-// FP32 weights in 8-byte records with the code byte inside: the walk's
-// compile-time form for such networks.
-bool plain_records(const StepArgs &a) { return !a.wbf16 && !a.wfp8 && a.code == nullptr; }
+                     uint32_t *done, uint32_t *err, uint32_t stall, int fmt);
+// The weight storage of a network as the walk's compile-time forms name it:
+// 1 FP32 records, 2 BF16, 3 FP8, each with the code byte in the x word; 0
+// with a separate code array.
+int walk_format(const StepArgs &a) {
+  if (a.code != nullptr) return 0;
+  return a.wbf16 ? 2 : a.wfp8 ? 3 : 1;
+}
 
 // The schedule a network or pool starts with: SG_RED_VARIANT (0..8) when set,
 // else the warp walk.
@@ -1756,33 +1760,42 @@ void release_l2_setaside(sg_net *net) {
 // One launch of the pre-centric scatter with schedule `variant` and `bps`
 // blocks per SM over a table of networks.
 template <int U, bool PIPE, uint32_t P = 1, int MINB = (PIPE && U > 4) ? 3 : 4>
-void launch_walk(cudaStream_t s, unsigned grid, bool plain, const StepArgs *nets, uint32_t n_nets, uint32_t *done) {
-  if (plain)
-    launch_step_kernel(scatter_walk_kernel<U, PIPE, true, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
-  else
-    launch_step_kernel(scatter_walk_kernel<U, PIPE, false, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+void launch_walk(cudaStream_t s, unsigned grid, int fmt, const StepArgs *nets, uint32_t n_nets, uint32_t *done) {
+  switch (fmt) {
+    case 1:
+      launch_step_kernel(scatter_walk_kernel<U, PIPE, 1, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+      break;
+    case 2:
+      launch_step_kernel(scatter_walk_kernel<U, PIPE, 2, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+      break;
+    case 3:
+      launch_step_kernel(scatter_walk_kernel<U, PIPE, 3, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+      break;
+    default:
+      launch_step_kernel(scatter_walk_kernel<U, PIPE, 0, P, MINB>, grid, kWalkThreads, 0, s, nets, n_nets, done);
+  }
 }
 
 void launch_step_red(cudaStream_t s, int device, int variant, uint32_t bps, const StepArgs *nets, uint32_t n_nets,
-                     uint32_t *done, uint32_t *err, uint32_t stall, bool plain) {
+                     uint32_t *done, uint32_t *err, uint32_t stall, int fmt) {
   const unsigned grid = sm_count(device) * bps;
   // the stall test hook acts on the staged pipeline's waits (the walk has none)
   if (is_walk_variant(variant) && stall) variant = 0;
   switch (variant) {
     case kWalkVariant:
-      launch_walk<8, false>(s, grid * 2, plain, nets, n_nets, done);
+      launch_walk<8, false>(s, grid * 2, fmt, nets, n_nets, done);
       break;
     case kWalkPipeVariant:
-      launch_walk<4, true>(s, grid * 2, plain, nets, n_nets, done);
+      launch_walk<4, true>(s, grid * 2, fmt, nets, n_nets, done);
       break;
     case kWalkPipeVariant + 1:  // 3 resident blocks per SM (more registers per thread)
-      launch_walk<8, true>(s, grid * 3 / 2, plain, nets, n_nets, done);
+      launch_walk<8, true>(s, grid * 3 / 2, fmt, nets, n_nets, done);
       break;
     case kWalkPipeVariant + 2:  // rows cut in 4 pieces
-      launch_walk<8, false, 4>(s, grid * 2, plain, nets, n_nets, done);
+      launch_walk<8, false, 4>(s, grid * 2, fmt, nets, n_nets, done);
       break;
     case kWalkPipeVariant + 3:  // rows cut in 4 pieces, 6 resident blocks per SM (fewer registers per thread)
-      launch_walk<4, false, 4, 6>(s, grid * 3, plain, nets, n_nets, done);
+      launch_walk<4, false, 4, 6>(s, grid * 3, fmt, nets, n_nets, done);
       break;
     case 1:
       launch_step_kernel(scatter_red_kernel<8, 512>, grid, kRedThreads, sizeof(RedSmemT<8, 512>), s, nets, n_nets,
@@ -1860,7 +1873,7 @@ void enqueue_rest(sg_net *net, const StepArgs &a) {
       ext_spikes_kernel<<<p.cap / kNeuronBlock, kNeuronBlock, 0, s>>>(a, p.dev_off, p.n, p.ext_src);
   if (a.red) {
     launch_step_red(s, net->device, net->red_variant, net->red_bps, (const StepArgs *)net->d_args.p, 1u,
-                    net->d_done.p, net->d_err.p, net->debug_stall, plain_records(a));
+                    net->d_done.p, net->d_err.p, net->debug_stall, walk_format(a));
   } else {
     if (net->seg32) launch_step_kernel(scatter_kernel<true>, net->G, kScatterThreads, net->scatter_smem, s, a);
     else launch_step_kernel(scatter_kernel<false>, net->G, kScatterThreads, net->scatter_smem, s, a);
@@ -4187,10 +4200,11 @@ void pool_enqueue_step(sg_pool *pool) {
   pool_launch_neuron<kIZH>(pool);
   pool_launch_neuron<kGPEA>(pool);
   pool_launch_neuron<kHH>(pool);
-  bool plain = true;
-  for (const StepArgs &a : pool->h_nets) plain = plain && plain_records(a);
+  int fmt = pool->h_nets.empty() ? 0 : walk_format(pool->h_nets[0]);
+  for (const StepArgs &a : pool->h_nets)
+    if (walk_format(a) != fmt) fmt = 0;  // mixed storage: read per network
   launch_step_red(pool->stream, pool->device, default_red_variant(), kRedBlocksPerSM, (const StepArgs *)pool->d_nets.p,
-                  (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u, plain);
+                  (uint32_t)pool->h_nets.size(), pool->d_done.p, pool->d_err.p, 0u, fmt);
 }
 
 }  // namespace

@@ -1669,14 +1669,15 @@ template <int U> struct WalkRound {
 // records and then issues its reds.  PIPE = true: the records of the next
 // round are loaded before the reds of the current one are issued, so that
 // their memory latency runs under the reds instead of after them (a warp's
-// loads queue behind its earlier reds).  PLAIN: every network of the table
-// has FP32 weights in 8-byte records with the code byte inside (no BF16/FP8
-// arrays, no separate code array), known at compile time so that the
-// round's registers hold only the records.  P: each spiking row is cut into
+// loads queue behind its earlier reds).  FMT: the weight storage of every
+// network of the table when it is known at compile time (1 FP32 in 8-byte
+// records, 2 BF16, 3 FP8; the code byte inside the x word, no separate code
+// array), so that the round's registers hold only what is loaded; 0: read
+// per network at run time.  P: each spiking row is cut into
 // P pieces of (nearly) equal length, and the pieces are the work items of
 // the round-robin (more warps busy on a step with few long rows).  MINB:
 // resident blocks per SM the registers are sized for.
-template <int U, bool PIPE, bool PLAIN, uint32_t P = 1, int MINB = (PIPE && U > 4) ? 3 : 4>
+template <int U, bool PIPE, int FMT, uint32_t P = 1, int MINB = (PIPE && U > 4) ? 3 : 4>
 __global__ void __launch_bounds__(kWalkThreads, MINB)
     scatter_walk_kernel(const StepArgs *__restrict__ nets, uint32_t n_nets, uint32_t *done) {
   __shared__ RedNet rn[kPoolMax];
@@ -1715,8 +1716,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
   for (uint32_t i = 0; i < n_nets; ++i) {
     const StepArgs &a = nets[i];
     const RedNet r = rn[i];
-    const uint32_t fmt = PLAIN ? 0u : r.fmt;
-    const uint8_t *code_arr = PLAIN ? nullptr : r.code;
+    const uint32_t fmt = FMT ? (uint32_t)(FMT - 1) : r.fmt;
+    const uint8_t *code_arr = FMT ? nullptr : r.code;
     const unsigned long long n = (unsigned long long)*a.red_cnt * P;  // work items: row pieces
     unsigned long long wev = 0;
     for (unsigned long long g0 = (gw + W - rot[i]) % W; g0 < n; g0 += 32ull * W) {
@@ -1763,7 +1764,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
             }
           }
           idx[u] = __shfl_sync(0xffffffffu, beg, k) + (e - __shfl_sync(0xffffffffu, excl, k));
-          R.s[u] = PLAIN ? 1.0f : __shfl_sync(0xffffffffu, scale, k);
+          R.s[u] = (FMT == 0 || FMT == 3) ? __shfl_sync(0xffffffffu, scale, k) : 1.0f;
           R.ok |= (e < total ? 1u : 0u) << u;
         }
 #pragma unroll
