@@ -139,7 +139,8 @@ def config(args, name, spec, scatter_path="ordered"):
         "scatter": SCATTER_TEXT[scatter_path],
         "l2": "inputs larger than L2: 8 GB of synapse records and "
               f"{(21 * spec['n'] * 4) / 1e6:.0f} MB of delay rings (21 slots for delays up to 20) against a "
-              "126 MB L2; each step reads the spiking rows",
+              "126 MB L2; each step reads the spiking rows; the rings are kept in the L2 set-aside for "
+              "persisting lines (at most 79 MiB on B200)",
         "parallelism": f"replicas x{args.gpus}",
     }
 

@@ -919,16 +919,22 @@ __device__ __forceinline__ uint32_t put_event(const StepArgs &a, ScatterSmem &S,
 
 // The last block of a step's scatter: per-step statistics, event totals,
 // the step counter (and the pre-centric scatter's spike count).
+// Every counter is loaded before anything is stored, so that the loads are
+// in flight together (this runs once per step, at the end of the scatter,
+// on the step's critical path).
 __device__ __forceinline__ void end_of_step_last(const StepArgs &a, uint32_t n_spikes) {
-  const unsigned long long step = *a.step;
+  const unsigned long long step = *(volatile unsigned long long *)a.step;
   const unsigned long long ev = *(volatile unsigned long long *)a.ev_step;
+  const unsigned long long ev_src = *(volatile unsigned long long *)a.ev_src_step;
+  const unsigned long long tot = *(volatile unsigned long long *)a.ev_total;
+  const unsigned long long tot_src = *(volatile unsigned long long *)a.ev_src_total;
   if (a.stat_cap) {
     a.stat_spk[step % a.stat_cap] = n_spikes;
     a.stat_ev[step % a.stat_cap] = ev;
   }
-  *a.ev_total += ev;
+  *a.ev_total = tot + ev;
   *a.ev_step = 0;
-  *a.ev_src_total += *(volatile unsigned long long *)a.ev_src_step;
+  *a.ev_src_total = tot_src + ev_src;
   *a.ev_src_step = 0;
   if (a.red) *a.red_cnt = 0;  // the next step's neuron kernel appends from 0
   *a.step = step + 1;
@@ -1434,7 +1440,7 @@ __device__ __forceinline__ void red_sources_and_close(const StepArgs *__restrict
     const uint32_t t = atomicAdd(done, 1u);
     if (t == gridDim.x - 1) {
       __threadfence();
-      for (uint32_t i = 0; i < n_nets; ++i) end_of_step_last(nets[i], *nets[i].red_cnt);
+      for (uint32_t i = 0; i < n_nets; ++i) end_of_step_last(nets[i], *(volatile uint32_t *)nets[i].red_cnt);
       *done = 0;
       __threadfence();
     }
@@ -1689,7 +1695,8 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
   // that consecutive rows go to consecutive blocks and every SM gets its
   // share of the step's rows (not the first blocks all of them)
   const uint32_t gw = (tid >> 5) * gridDim.x + blockIdx.x;
-  pdl_wait();
+  // the table of networks is host-written: read before the wait; the step
+  // counter and the spike list are the previous kernels' and read after it
   for (uint32_t i = tid; i < n_nets; i += kWalkThreads) {
     const StepArgs &a = nets[i];
     RedNet r;
@@ -1697,13 +1704,23 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
     r.code = a.code;
     r.Nd = a.Nd;
     r.nslots = a.nslots;
-    r.base = (uint32_t)(*a.step % a.nslots);
     r.post_mask = a.post_mask;
     r.fmt = a.wbf16 ? 1 : a.wfp8 ? 2 : 0;
+    r.base = 0;
     rn[i] = r;
     ev[i] = 0;
     src_ev[i] = 0;
   }
+  // the first network's list (Nd entries) and this lane's first item in it
+  // (the round-robin of the first network starts at place 0)
+  const uint2 *rows0 = n_nets ? nets[0].red_rows : nullptr;
+  const unsigned long long rr0 = (gw + (unsigned long long)lane * W) / P;
+  const bool spec = n_nets && rr0 < nets[0].Nd;
+  pdl_wait();
+  // that item's row range, loaded beside the counts instead of after them
+  // (used only when the item exists, i.e. lies below the step's count)
+  const uint2 rb_first = spec ? rows0[rr0] : make_uint2(0u, 0u);
+  for (uint32_t i = tid; i < n_nets; i += kWalkThreads) rn[i].base = (uint32_t)(*nets[i].step % rn[i].nslots);
   if (tid == 0) {
     uint32_t r0 = 0;
     for (uint32_t i = 0; i < n_nets; ++i) {
@@ -1720,13 +1737,14 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
     const uint8_t *code_arr = FMT ? nullptr : r.code;
     const unsigned long long n = (unsigned long long)*a.red_cnt * P;  // work items: row pieces
     unsigned long long wev = 0;
-    for (unsigned long long g0 = (gw + W - rot[i]) % W; g0 < n; g0 += 32ull * W) {
+    const unsigned long long g_first = (gw + W - rot[i]) % W;
+    for (unsigned long long g0 = g_first; g0 < n; g0 += 32ull * W) {
       const unsigned long long it = g0 + (unsigned long long)lane * W;
       uint32_t beg = 0, len = 0;
       float scale = 1.0f;
       if (it < n) {
         const uint32_t rr = (uint32_t)(it / P);
-        const uint2 rb = a.red_rows[rr];
+        const uint2 rb = (i == 0 && g0 == g_first && spec) ? rb_first : a.red_rows[rr];
         if (P == 1) {
           beg = rb.x;
           len = rb.y - rb.x;

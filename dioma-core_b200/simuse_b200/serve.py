@@ -195,9 +195,9 @@ class Server:
 
     budget_bytes: device memory the resident networks may hold together.
     max_resident: resident networks at most (pool members; at most 64).
-    chunk: steps the pool advances per tick (a tick is shortened to the
-    fewest steps any resident network still needs); a multiple of 32 runs
-    as whole 32-step graphs.
+    chunk: steps the pool advances per tick; a network that needs fewer
+    steps than that leaves the pool and runs them alone beside the tick; a
+    multiple of 32 runs as whole 32-step graphs.
     builders: threads building admitted networks beside the running pool.
     """
 
@@ -361,10 +361,18 @@ class Server:
                 time.sleep(0.0005)
                 ph["idle"] += time.perf_counter() - t1
                 continue
-            # tick t: every resident network advances k steps in the pool
+            # tick t: every resident network advances a full tick in the pool;
+            # one that needs fewer steps than that leaves the pool and runs its
+            # last steps alone on its own stream, beside the tick (a short tick
+            # would cost the whole pool a tick's host work for a few steps)
             k = 0
+            tail = [r for r in resident if r.req.steps - r.done < self.chunk]
+            for r in tail:
+                resident.remove(r)
+                pool.remove(r.net)
+                r.net.step(r.req.steps - r.done)
             if resident:
-                k = min(self.chunk, min(r.req.steps - r.done for r in resident))
+                k = self.chunk
                 pool.step(k)
                 self.ticks += 1
             t2 = time.perf_counter()
@@ -383,13 +391,16 @@ class Server:
             draining = []
             t3 = time.perf_counter()
             ph["collect"] += t3 - t2
-            if not resident:
+            if not resident and not tail:
                 continue
             # tick t's spikes: compaction queued after the tick, copies to the readers
             for r in resident:
                 r.net.raster_stage()
                 r.done += k
-            inflight = [(r, self._readers.submit(r.fetch)) for r in resident]
+            for r in tail:
+                r.net.raster_stage()
+                r.done = r.req.steps
+            inflight = [(r, self._readers.submit(r.fetch)) for r in resident + tail]
             t4 = time.perf_counter()
             ph["stage"] += t4 - t3
             # finished requests leave the pool before the next tick
@@ -397,6 +408,7 @@ class Server:
                 resident.remove(r)
                 pool.remove(r.net)
                 draining.append(r)
+            draining.extend(tail)
             ph["leave"] += time.perf_counter() - t4
         pool.close()
         for off, idx in self._free_bufs:
