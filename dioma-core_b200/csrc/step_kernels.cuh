@@ -62,6 +62,11 @@ constexpr unsigned long long kEmpty64 = ~0ull;
 constexpr uint32_t kMaxPops = 16;
 constexpr uint32_t kMaxTm = 8;  // short-term plasticity profiles on the device
 
+// a compile-time flag passed to a generic lambda (one instantiation per value)
+template <bool B> struct BoolC {
+  static constexpr bool value = B;
+};
+
 // neurons per thread: LIF/Izhikevich move 4 neighbours with 128-bit accesses;
 // GPEA/HH are compute heavy and keep one neuron per thread
 #ifndef SG_NEURON_MIN_BLOCKS
@@ -546,33 +551,43 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   // dt = param column 0 of neuron 0, broadcast (population.rs:307,361)
   const float dt = (p.umask & 1u) ? p.uval[0] : __ldg(p.params);
   uint32_t nib = 0, nclamp = 0;
+  // UNI: every parameter column is population-wide and all NPT neurons of
+  // the thread exist (the common case of a large homogeneous population):
+  // parameters straight from the kernel arguments, no per-neuron guards
+  auto update = [&](auto uni) {
+    constexpr bool UNI = decltype(uni)::value;
 #pragma unroll
-  for (int q = 0; q < NPT; ++q) {
-    if (i0 + q < p.n) {
-      float xi = x[q];
-      if (clamps(MODEL)) {
-        const float xc = fminf(fmaxf(xi, -100.0f), 100.0f);
-        nclamp += xc != xi;
-        xi = xc;
+    for (int q = 0; q < NPT; ++q) {
+      if (UNI || i0 + q < p.n) {
+        float xi = x[q];
+        if (clamps(MODEL)) {
+          const float xc = fminf(fmaxf(xi, -100.0f), 100.0f);
+          nclamp += xc != xi;
+          xi = xc;
+        }
+        RegNeuron<NS, NP> r;
+#pragma unroll
+        for (int c = 0; c < NS; ++c) r.s[c] = sv[c][q];
+#pragma unroll
+        for (int c = 0; c < NP; ++c)
+          r.p[c] = UNI ? p.uval[c]
+                   : !kParamsPerNeuron ? pv[kParamsPerNeuron ? 0 : c][kParamsPerNeuron ? 0 : q]
+                   : (p.umask >> c) & 1u ? p.uval[c]
+                                         : __ldg(p.params + (size_t)c * p.cap + i0 + q);
+        bool sp;
+        if (MODEL == kLIF) sp = lif_step(r, xi, dt);
+        else if (MODEL == kIZH) sp = izh_step(r, xi, dt);
+        else if (MODEL == kGPEA) sp = gpea_step(r, xi, dt, p.ln_na, p.ln_k);
+        else sp = hh_step(r, xi, dt);
+#pragma unroll
+        for (int c = 0; c < NS; ++c) sv[c][q] = r.s[c];
+        nib |= (sp ? 1u : 0u) << q;
       }
-      RegNeuron<NS, NP> r;
-#pragma unroll
-      for (int c = 0; c < NS; ++c) r.s[c] = sv[c][q];
-#pragma unroll
-      for (int c = 0; c < NP; ++c)
-        r.p[c] = !kParamsPerNeuron ? pv[kParamsPerNeuron ? 0 : c][kParamsPerNeuron ? 0 : q]
-                 : (p.umask >> c) & 1u ? p.uval[c]
-                                       : __ldg(p.params + (size_t)c * p.cap + i0 + q);
-      bool sp;
-      if (MODEL == kLIF) sp = lif_step(r, xi, dt);
-      else if (MODEL == kIZH) sp = izh_step(r, xi, dt);
-      else if (MODEL == kGPEA) sp = gpea_step(r, xi, dt, p.ln_na, p.ln_k);
-      else sp = hh_step(r, xi, dt);
-#pragma unroll
-      for (int c = 0; c < NS; ++c) sv[c][q] = r.s[c];
-      nib |= (sp ? 1u : 0u) << q;
     }
-  }
+  };
+  constexpr uint32_t kAllParams = (1u << NP) - 1u;
+  if (kParamsPerNeuron && (p.umask & kAllParams) == kAllParams && i0 + NPT <= p.n) update(BoolC<true>{});
+  else update(BoolC<false>{});
 #pragma unroll
   for (int c = 0; c < NS; ++c) V::store(p.state + (size_t)c * p.cap + i0, sv[c]);
   if (FULL && a.ns_count != nullptr && nib) {
