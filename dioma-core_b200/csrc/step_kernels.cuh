@@ -259,6 +259,35 @@ __device__ __forceinline__ uint32_t ring_base(const StepArgs &a, unsigned long l
   return a.receptor ? 0u : (uint32_t)(step % a.nslots);
 }
 
+// The step hint: the word after the step counter.  The pre-centric scatters
+// store step + 1 there as soon as they have read the step (long before they
+// finish), so that the next neuron kernel can roll its Poisson drive and
+// find its ring slot before its dependency wait.  It is only a guess: the
+// neuron kernel compares it with the step counter after the wait and redoes
+// that work when they differ (a step run another way, a host-set step).
+__device__ __forceinline__ unsigned long long *step_hint(const StepArgs &a) { return a.step + 1; }
+
+// The Poisson drive of NPT neurons from population index i0 for one step:
+// bit q = source of neuron i0 + q fires (P/api/net/network/sources.rs:5-14 roll).
+template <int NPT>
+__device__ __forceinline__ uint32_t drive_bits(const PopArgs &p, uint32_t i0, unsigned long long step) {
+  uint32_t b = 0;
+#pragma unroll
+  for (int q = 0; q < NPT; ++q)
+    if (i0 + q < p.n && poisson_spike(p.drv_seed0 + i0 + q, 0, step, p.drv_p)) b |= 1u << q;
+  return b;
+}
+
+// What the single-population neuron kernel works out before its wait from
+// the step hint (valid for step `step` only).
+struct PreWait {
+  unsigned long long step;
+  uint32_t slot;      // ring_base(step)
+  uint32_t drv_prev;  // drive_bits(step - 1)
+  uint32_t drv_now;   // drive_bits(step)
+  bool ok;
+};
+
 // Programmatic dependent launch: the step kernels are launched so that the
 // next kernel of the stream may start while this one drains.  pdl_wait()
 // returns once the previous kernel of the stream has completed and its memory
@@ -414,7 +443,8 @@ __device__ __forceinline__ void load_state(const PopArgs &p, uint32_t blk,
 // stored.
 template <int MODEL, bool FULL>
 __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p, uint32_t blk,
-                                             float (&sv)[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT]) {
+                                             float (&sv)[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT],
+                                             const PreWait &pre) {
   constexpr int NPT = NeuronCfg<MODEL, FULL>::NPT;
   constexpr int NS = n_state(MODEL), NP = n_params(MODEL);
   using V = VecF<NPT>;
@@ -425,7 +455,8 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   const uint32_t i0 = blk * kNeuronBlock + tid * NPT;  // population index of my first neuron
   const uint32_t gi0 = p.dev_off + i0;
   const unsigned long long step = *a.step;
-  const uint32_t slot = ring_base(a, step);
+  const bool hit = pre.ok && pre.step == step;  // the pre-wait work is this step's
+  const uint32_t slot = hit ? pre.slot : ring_base(a, step);
   // 1-2. read the slot, clear it (step.rs:27-34)
   float x[NPT], zero[NPT];
 #pragma unroll
@@ -436,13 +467,11 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   uint32_t nfire = 0;  // this step's deferred-drive events (counted now, applied next step)
   if (p.drv) {
     const bool take = step >= 1 && *a.drv_fold != step - 1;
+    const uint32_t prev = !take ? 0u : hit ? pre.drv_prev : drive_bits<NPT>(p, i0, step - 1);
 #pragma unroll
     for (int q = 0; q < NPT; ++q)
-      if (i0 + q < p.n) {
-        const uint32_t seed = p.drv_seed0 + i0 + q;
-        if (take && poisson_spike(seed, 0, step - 1, p.drv_p)) x[q] = x[q] + p.drv_w;
-        nfire += poisson_spike(seed, 0, step, p.drv_p) ? 1u : 0u;
-      }
+      if ((prev >> q) & 1u) x[q] = x[q] + p.drv_w;
+    nfire = __popc(hit ? pre.drv_now : drive_bits<NPT>(p, i0, step));
   }
   if (p.bias != nullptr) {
     float bv[NPT];
@@ -751,13 +780,28 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL, FULL>::THREADS, NeuronCfg<MOD
     // is what let this kernel start): the state is read before the wait,
     // so that its loads overlap the previous kernel's tail.
     load_state<MODEL, FULL>(p0, blockIdx.x, sv);
+    // this step's drive rolls and ring slot from the step hint (checked
+    // against the step counter after the wait)
+    PreWait pre;
+    pre.step = *(volatile unsigned long long *)step_hint(a);
+    pre.slot = ring_base(a, pre.step);
+    pre.ok = true;
+    pre.drv_prev = pre.drv_now = 0u;
+    if (p0.drv) {
+      constexpr int NPT = NeuronCfg<MODEL, FULL>::NPT;
+      const uint32_t i0 = blockIdx.x * kNeuronBlock + threadIdx.x * NPT;
+      pre.drv_prev = pre.step >= 1 ? drive_bits<NPT>(p0, i0, pre.step - 1) : 0u;
+      pre.drv_now = drive_bits<NPT>(p0, i0, pre.step);
+    }
     pdl_wait();
-    neuron_block<MODEL, FULL>(a, p0, blockIdx.x, sv);
+    neuron_block<MODEL, FULL>(a, p0, blockIdx.x, sv, pre);
   } else {
     pdl_wait();
     const uint2 bm = map[blockIdx.x];
     load_state<MODEL, FULL>(pops[bm.x], bm.y, sv);
-    neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y, sv);
+    PreWait none;
+    none.ok = false;
+    neuron_block<MODEL, FULL>(a, pops[bm.x], bm.y, sv, none);
   }
   pdl_release();
 }
@@ -1508,7 +1552,9 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
     r.code = a.code;
     r.Nd = a.Nd;
     r.nslots = a.nslots;
-    r.base = (uint32_t)(*a.step % a.nslots);
+    const unsigned long long st = *a.step;
+    if (blockIdx.x == 0) *step_hint(a) = st + 1;  // for the next neuron kernel's pre-wait work
+    r.base = (uint32_t)(st % a.nslots);
     r.post_mask = a.post_mask;
     r.fmt = a.wbf16 ? 1 : a.wfp8 ? 2 : 0;
     S.nets[i] = r;
@@ -1735,7 +1781,11 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
   // that item's row range, loaded beside the counts instead of after them
   // (used only when the item exists, i.e. lies below the step's count)
   const uint2 rb_first = spec ? rows0[rr0] : make_uint2(0u, 0u);
-  for (uint32_t i = tid; i < n_nets; i += kWalkThreads) rn[i].base = (uint32_t)(*nets[i].step % rn[i].nslots);
+  for (uint32_t i = tid; i < n_nets; i += kWalkThreads) {
+    const unsigned long long st = *nets[i].step;
+    if (blockIdx.x == 0) *step_hint(nets[i]) = st + 1;  // for the next neuron kernel's pre-wait work
+    rn[i].base = (uint32_t)(st % rn[i].nslots);
+  }
   if (tid == 0) {
     uint32_t r0 = 0;
     for (uint32_t i = 0; i < n_nets; ++i) {
@@ -1871,7 +1921,9 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL, FULL>::THREADS, NeuronCfg<MOD
   pdl_wait();
   float sv[n_state(MODEL)][NeuronCfg<MODEL, FULL>::NPT];
   load_state<MODEL, FULL>(pops[m.y], m.z, sv);
-  neuron_block<MODEL, FULL>(nets[m.x], pops[m.y], m.z, sv);
+  PreWait none;
+  none.ok = false;
+  neuron_block<MODEL, FULL>(nets[m.x], pops[m.y], m.z, sv, none);
   pdl_release();
 }
 
