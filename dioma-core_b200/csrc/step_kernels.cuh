@@ -454,15 +454,18 @@ __device__ __forceinline__ void neuron_block(const StepArgs &a, const PopArgs &p
   const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
   const uint32_t i0 = blk * kNeuronBlock + tid * NPT;  // population index of my first neuron
   const uint32_t gi0 = p.dev_off + i0;
-  const unsigned long long step = *a.step;
-  const bool hit = pre.ok && pre.step == step;  // the pre-wait work is this step's
-  const uint32_t slot = hit ? pre.slot : ring_base(a, step);
-  // 1-2. read the slot, clear it (step.rs:27-34)
+  // 1-2. read the slot, clear it (step.rs:27-34).  With a step hint the
+  // hinted slot (always a valid slot) is loaded beside the step counter and
+  // loaded again from the right slot only when the hint was wrong.
   float x[NPT], zero[NPT];
 #pragma unroll
   for (int q = 0; q < NPT; ++q) zero[q] = 0.0f;
+  if (pre.ok) V::load(a.ring + (size_t)pre.slot * a.Nd + gi0, x);
+  const unsigned long long step = *a.step;
+  const bool hit = pre.ok && pre.step == step;  // the pre-wait work is this step's
+  const uint32_t slot = hit ? pre.slot : ring_base(a, step);
   float *rs = a.ring + (size_t)slot * a.Nd + gi0;
-  V::load(rs, x);
+  if (!hit) V::load(rs, x);
   V::store(rs, zero);
   uint32_t nfire = 0;  // this step's deferred-drive events (counted now, applied next step)
   if (p.drv) {
