@@ -259,8 +259,8 @@ __device__ __forceinline__ uint32_t ring_base(const StepArgs &a, unsigned long l
   return a.receptor ? 0u : (uint32_t)(step % a.nslots);
 }
 
-// The step hint: the word after the step counter.  The pre-centric scatters
-// store step + 1 there as soon as they have read the step (long before they
+// The step hint: the word after the step counter.  The scatters store
+// step + 1 there as soon as they have read the step (long before they
 // finish), so that the next neuron kernel can roll its Poisson drive and
 // find its ring slot before its dependency wait.  It is only a guess: the
 // neuron kernel compares it with the step counter after the wait and redoes
@@ -1025,6 +1025,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   const uint32_t p0 = j * a.P;
   pdl_wait();
   const unsigned long long step = *a.step;
+  if (j == 0 && tid == 0) *step_hint(a) = step + 1;  // for the next neuron kernel's pre-wait work
   const uint32_t base = ring_base(a, step);
   const uint32_t G1 = a.G + 1;
   const uint32_t pj = min(a.P, a.Nd - p0);
