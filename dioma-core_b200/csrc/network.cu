@@ -1567,7 +1567,7 @@ void finish_build(sg_net *net) {
   net->d_ring.zero(s);
   net->d_kin_g.alloc(std::max<size_t>(net->kin.size() * 3 * Nd, 1));  // up to 3 state arrays per profile
   net->d_kin_g.zero(s);
-  net->d_step.alloc(2);  // [step counter, step hint] (step_hint in step_kernels.cuh)
+  net->d_step.alloc(2);  // [step counter, step hint] (hint_load / hint_store in step_kernels.cuh)
   net->d_step.zero(s);
   net->d_blk_cnt.alloc(std::max<uint32_t>(Nd / kNeuronBlock, 1));
   net->d_blk_cnt.zero(s);

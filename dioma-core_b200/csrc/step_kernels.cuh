@@ -265,7 +265,16 @@ __device__ __forceinline__ uint32_t ring_base(const StepArgs &a, unsigned long l
 // find its ring slot before its dependency wait.  It is only a guess: the
 // neuron kernel compares it with the step counter after the wait and redoes
 // that work when they differ (a step run another way, a host-set step).
-__device__ __forceinline__ unsigned long long *step_hint(const StepArgs &a) { return a.step + 1; }
+// The neuron kernel reads it while the scatter before it may still be
+// running, so both sides use relaxed GPU-scope accesses.
+__device__ __forceinline__ unsigned long long hint_load(const StepArgs &a) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a.step + 1));
+  return v;
+}
+__device__ __forceinline__ void hint_store(const StepArgs &a, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(a.step + 1), "l"(v) : "memory");
+}
 
 // The Poisson drive of NPT neurons from population index i0 for one step:
 // bit q = source of neuron i0 + q fires (P/api/net/network/sources.rs:5-14 roll).
@@ -786,7 +795,7 @@ __global__ void __launch_bounds__(NeuronCfg<MODEL, FULL>::THREADS, NeuronCfg<MOD
     // this step's drive rolls and ring slot from the step hint (checked
     // against the step counter after the wait)
     PreWait pre;
-    pre.step = *(volatile unsigned long long *)step_hint(a);
+    pre.step = hint_load(a);
     pre.slot = ring_base(a, pre.step);
     pre.ok = true;
     pre.drv_prev = pre.drv_now = 0u;
@@ -1025,7 +1034,7 @@ __global__ void __launch_bounds__(kScatterThreads, kScatterBlocksPerSM) scatter_
   const uint32_t p0 = j * a.P;
   pdl_wait();
   const unsigned long long step = *a.step;
-  if (j == 0 && tid == 0) *step_hint(a) = step + 1;  // for the next neuron kernel's pre-wait work
+  if (j == 0 && tid == 0) hint_store(a, step + 1);  // for the next neuron kernel's pre-wait work
   const uint32_t base = ring_base(a, step);
   const uint32_t G1 = a.G + 1;
   const uint32_t pj = min(a.P, a.Nd - p0);
@@ -1557,7 +1566,7 @@ __global__ void __launch_bounds__(kRedThreads, kRedBlocksPerSM)
     r.Nd = a.Nd;
     r.nslots = a.nslots;
     const unsigned long long st = *a.step;
-    if (blockIdx.x == 0) *step_hint(a) = st + 1;  // for the next neuron kernel's pre-wait work
+    if (blockIdx.x == 0) hint_store(a, st + 1);  // for the next neuron kernel's pre-wait work
     r.base = (uint32_t)(st % a.nslots);
     r.post_mask = a.post_mask;
     r.fmt = a.wbf16 ? 1 : a.wfp8 ? 2 : 0;
@@ -1787,7 +1796,7 @@ __global__ void __launch_bounds__(kWalkThreads, MINB)
   const uint2 rb_first = spec ? rows0[rr0] : make_uint2(0u, 0u);
   for (uint32_t i = tid; i < n_nets; i += kWalkThreads) {
     const unsigned long long st = *nets[i].step;
-    if (blockIdx.x == 0) *step_hint(nets[i]) = st + 1;  // for the next neuron kernel's pre-wait work
+    if (blockIdx.x == 0) hint_store(nets[i], st + 1);  // for the next neuron kernel's pre-wait work
     rn[i].base = (uint32_t)(st % rn[i].nslots);
   }
   if (tid == 0) {
